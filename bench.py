@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark of the explicit spectral BDF/IAEM generalized-momentum PIC step.
+
+Workload (the 512x512 Weibel configuration): 2D periodic grid 512x512 over
+[0, 2pi/0.3)^2, 256 electrons per cell (67,108,864 particles) at uniform
+random positions with a bi-Maxwellian in normalized momentum (thermal spread
+0.02c in x, 0.2c in y), fixed uniform ion background n0 = 1, quadratic
+B-spline, BDF1 field solve with the continuity-consistent charge update,
+dt = 0.05, FP64 throughout, diagnostics (energy history, gauge / Gauss /
+continuity residuals) every step as the reference's run loop does by default.
+A step is one pass of the hot path over all particles.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line.  value = whole-job particle-steps/s with inputs resident
+in HBM; e2e = the same metric through the public API from pinned host
+buffers (upload, start-up fields, K steps with a diagnostics row read back
+each step, particle state read back); roofline = the fused push/deposit
+kernel against the measured HBM copy bandwidth; cpu_baseline = the reference's
+own CPU code (oracle/_ref, compiled from the reference sources) on a bounded
+sample of the same workload.  N > 1 runs N independent replicas (the method
+runs on one GPU; it has no cross-GPU exchange).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s"
+WORKLOADS = {
+    "weibel512": dict(nx=512, ny=512, ppc=256, L=2 * np.pi / 0.3, dt=0.05, method="bdf1",
+                      charge_update="conserving", uth=(0.02, 0.2, 0.0), seed=2026),
+    "weibel64": dict(nx=64, ny=64, ppc=64, L=2 * np.pi / 0.3, dt=0.05, method="bdf1",
+                     charge_update="conserving", uth=(0.02, 0.2, 0.0), seed=2026),
+}
+# Algorithmic HBM bytes per particle per step of the fused push kernel: the
+# FP64 particle state x, y, P(3), v(3), v_prev(3) read once and written once.
+ALG_BYTES_PER_PARTICLE = 176
+# Reference CPU sample: same grid, 16 electrons per cell, timed step loop.
+REF_SAMPLE_PPC = 16
+REF_SAMPLE_STEPS = 2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="upic", choices=["upic", "reference"])
+    ap.add_argument("--workload", default="weibel512", choices=sorted(WORKLOADS))
+    ap.add_argument("--diag-stride", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def config_desc(w, extra=None):
+    d = {"workload": f"weibel_bimaxwellian_{w['nx']}x{w['ny']}_ppc{w['ppc']}",
+         "grid": [w["nx"], w["ny"]], "particles": w["nx"] * w["ny"] * w["ppc"],
+         "particles_per_cell": w["ppc"], "L": w["L"], "dt": w["dt"], "method": w["method"],
+         "charge_update": w["charge_update"], "shape": "quadratic B-spline",
+         "precision": "fp64", "l2": "inputs larger than L2 (particle state 5.9 GB)"
+         if w["ppc"] * w["nx"] * w["ny"] > 10_000_000 else "inputs smaller than L2",
+         "parallelism": "replicas"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid=None):
+        self.uuid = uuid
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.seek(0)
+        rows = [r.split(", ") for r in self.file.read().strip().splitlines() if r.strip()]
+        if self.uuid:
+            mine = [r for r in rows if len(r) >= 10 and self.uuid in r[1]]
+            rows = mine or rows
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 10:
+                continue
+            try:
+                sm.append(float(r[2]))
+                smax.append(float(r[3]))
+            except ValueError:
+                continue
+            for name, val in zip(names, r[6:10]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def measured_traffic(np_total):
+    """DRAM bytes per push launch from the committed ncu capture, scaled by
+    particle count (traffic grows in proportion to the particles streamed)."""
+    path = os.path.join(ROOT, "profiles", "push_deposit_traffic.json")
+    try:
+        with open(path) as fh:
+            t = json.load(fh)
+        return float(t["dram_bytes_per_launch"]) * np_total / float(t["particles"])
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+def reference_sample(ppc, steps, warmup, seed):
+    """Time the reference's own step loop (oracle/_ref/libref_p2.so, or the
+    oracle port when the reference build is absent) on a sample of the
+    workload: same grid, ppc electrons per cell.  Returns (particle-steps/s,
+    kind, particles, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import ctypes
+    import oracle_lib as ol
+    import unstaggered_pic_b200 as up
+    w = WORKLOADS["weibel512"]
+    lib = ol.ref_p2()
+    kind = "reference"
+    fn = lib.ref_p2_simulate if lib is not None else None
+    if fn is None:
+        fn = ol.oracle().o2_simulate
+        kind = "port"
+    p = up.generate_bimaxwellian(w["nx"], w["ny"], w["L"], w["L"], ppc, w["uth"], seed=seed)
+    parts = {"x": p["x"], "y": p["y"], "P": p["P"], "v": p["v"], "vprev": p["v_prev"], "q": p["q"],
+             "m": p["m"]}
+    if warmup > 0:
+        prob = ol.P2Problem(w["nx"], w["ny"], w["L"], w["L"], w["dt"], 1, True, n_steps=warmup)
+        parts, _, _, _ = ol.simulate(fn, prob, parts, want_fields=False)
+    prob = ol.P2Problem(w["nx"], w["ny"], w["L"], w["L"], w["dt"], 1, True, n_steps=steps)
+    _, _, _, secs = ol.simulate(fn, prob, parts, want_fields=False)
+    n = len(parts["x"])
+    del ctypes
+    return n * steps / secs, kind, n, secs
+
+
+def _ref_worker(args):
+    ppc, steps, warmup, seed = args
+    return reference_sample(ppc, steps, warmup, seed)
+
+
+def run_reference_arm(args):
+    """--impl reference: the reference's CPU step on all host cores (one
+    serial reference process per core, each on its own sample)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    w = WORKLOADS["weibel512"]
+    cores = min(os.cpu_count() or 1, 64)
+    ppc = 4  # per-process sample: 512x512 grid, 4 e-/cell (1,048,576 particles)
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_ref_worker, [(ppc, args.steps, args.warmup, 1000 + i) for i in range(cores)])
+    wall = time.perf_counter() - t0
+    n = res[0][2]
+    slowest = max(r[3] for r in res)
+    value = cores * n * args.steps / slowest
+    kind = res[0][1]
+    sample = (f"{cores} concurrent serial reference processes, each {w['nx']}x{w['ny']} grid with "
+              f"{ppc} e-/cell ({n} particles), {args.warmup} warm-up + {args.steps} timed steps, "
+              f"diagnostics every step; value = total particle-steps / slowest process time")
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * slowest / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_desc(w, {"reference_sample": sample}),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def run_upic(args):
+    import torch
+    import unstaggered_pic_b200 as up
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    w = WORKLOADS[args.workload]
+    np_total = w["nx"] * w["ny"] * w["ppc"]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # host inputs in pinned memory (seed differs per replica)
+    p = up.generate_bimaxwellian(w["nx"], w["ny"], w["L"], w["L"], w["ppc"], w["uth"],
+                                 seed=w["seed"] + rank)
+    pinned = {}
+    for k, a in p.items():
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        pinned[k] = t
+    del p
+    host = {k: t.numpy() for k, t in pinned.items()}
+    cfg = up.Config(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], method=w["method"],
+                    charge_update=w["charge_update"])
+    sim = up.Simulation(cfg)
+    stream = torch.cuda.current_stream()
+    sim.set_stream(stream.cuda_stream)
+
+    def load():
+        sim.set_particles(host["x"], host["y"], host["P"], host["v"], host["v_prev"], host["q"],
+                          host["m"])
+
+    # ---- device-resident throughput
+    load()
+    sim.init_fields(False)
+    sim.step(args.warmup, args.diag_stride)
+    torch.cuda.synchronize()
+    barrier()
+    sim.profile_enable(True)
+    _, _, launches0 = sim.profile_read()
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sim.step(args.steps, args.diag_stride)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_ms = allmax(e0.elapsed_time(e1))
+    push_ms, push_n, launches1 = sim.profile_read()
+    sim.profile_enable(False)
+    gpu_launches = launches1 - launches0
+    value = world * np_total * args.steps / (t_ms / 1e3)
+    push_avg_s = push_ms / max(push_n, 1) / 1e3
+    peak, peak_kind = measured_hbm_peak()
+    achieved = ALG_BYTES_PER_PARTICLE * np_total / push_avg_s / 1e9
+    traffic = measured_traffic(np_total)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                "kernel": "push_deposit_kernel (gather + IAEM push + next-step deposit)",
+                "kernel_ms": push_avg_s * 1e3, "kernel_share": push_ms / t_ms,
+                "algorithmic_bytes_per_particle": ALG_BYTES_PER_PARTICLE}
+
+    # ---- end to end through the public API from pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        load()
+        sim.init_fields(True)
+        sim.step(args.steps, 1)
+        out = sim.get_particles()
+        t_e2e = allmax(time.perf_counter() - t0)
+        del out
+        h2d = np_total * 13 * 8 / args.steps
+        d2h = (13 * 8 * (args.steps + 1) + np_total * 11 * 8) / args.steps
+        e2e = {"value": world * np_total * args.steps / t_e2e, "unit": METRIC,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "seconds": t_e2e,
+               "what": "upic_set_particles + upic_init_fields + upic_step(K, diagnostics every "
+                       "step) + upic_get_particles, host wall clock, max over ranks"}
+    sim.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, kind, n, secs = reference_sample(REF_SAMPLE_PPC, REF_SAMPLE_STEPS, 0, 7)
+            cpu = {"value": v, "unit": METRIC, "cores": 1, "kind": kind,
+                   "sample": f"{w['nx']}x{w['ny']} grid, {REF_SAMPLE_PPC} e-/cell ({n} particles), "
+                             f"{REF_SAMPLE_STEPS} steps of the serial reference step loop with "
+                             f"diagnostics every step ({secs:.1f} s)"}
+        except Exception as exc:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference",
+                   "sample": f"failed: {exc}"}
+
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_desc(w, {"diag_stride": args.diag_stride}),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
+            "clocks": clk}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_upic(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,224 @@
+/*
+ * upic.h -- C ABI of the B200-native unstaggered generalized-momentum PIC step.
+ *
+ * The reference (sgong11/Unstaggered_PIC) exposes this step only as
+ * single-file C++ solvers driven by `prog deck.txt`; its step functions are
+ * `static` inside one translation unit.  This header is the drop-in boundary
+ * a host driver (or an FFI binding: ctypes, cgo, JNI) calls instead.  Every
+ * entry point names the reference function(s) it replaces, as
+ * Project<N>/<file>:<line>.
+ *
+ * Conventions (those of the reference):
+ *   - grids are nx*ny doubles, node id = i*ny + j (x index i is the slow one),
+ *     Project2/spectral_pic_part3.cpp:313-317;
+ *   - explicit methods place particles in [0,Lx)x[0,Ly) with node i at x=i*dx
+ *     (spectral_pic_part3.cpp:537-552);
+ *   - per-particle 3-vectors (P, v, v_prev) are interleaved x,y,z triples,
+ *     the memory layout of the reference's std::vector<Vec3>;
+ *   - all arithmetic is FP64 unless the context is created with
+ *     UPIC_PRECISION_MIXED.
+ *
+ * Errors: every call returns 0 on success or a negative UPIC_ERR_* code;
+ * upic_last_error() returns the message.  No exception crosses the ABI.
+ * A context belongs to one host thread.  Work is ordered on the context's
+ * CUDA stream (upic_set_stream) and every call that returns host data
+ * synchronizes that stream.
+ */
+#ifndef UPIC_H
+#define UPIC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UPIC_ABI_VERSION 1
+
+/* Error codes. */
+enum {
+    UPIC_OK = 0,
+    UPIC_ERR_CONFIG = -1,         /* bad deck / config (reference throws in read_config) */
+    UPIC_ERR_ARGUMENT = -2,       /* bad pointer, size or enum */
+    UPIC_ERR_CUDA = -3,           /* a CUDA runtime call failed */
+    UPIC_ERR_STATE = -4,          /* call out of order (e.g. step before particles) */
+    UPIC_ERR_NONFINITE = -5,      /* non-finite particle or field value detected */
+    UPIC_ERR_NONCONVERGED = -6,   /* outer nonlinear solve failed (NonlinearSolveFailure) */
+    UPIC_ERR_LOCAL_PARTICLE = -7, /* per-particle local solve failed */
+    UPIC_ERR_SUPERLUMINAL = -8,   /* |v| >= c in a relativistic iterate */
+    UPIC_ERR_NOMEM = -9           /* device allocation failed */
+};
+
+/* Methods.  BDF1/BDF2: explicit spectral GM step with IAEM push,
+ * Project2/spectral_pic_part3.cpp:1094-1189. */
+enum { UPIC_METHOD_BDF1 = 1, UPIC_METHOD_BDF2 = 2 };
+
+/* Charge source: continuity-consistent (conserving) or redeposited (naive),
+ * spectral_pic_part3.cpp:1147-1152. */
+enum { UPIC_CHARGE_CONSERVING = 0, UPIC_CHARGE_NAIVE = 1 };
+
+enum { UPIC_PRECISION_FP64 = 0, UPIC_PRECISION_MIXED = 1 };
+
+/* Field selectors for upic_get_field / upic_set_field. */
+enum {
+    UPIC_FIELD_PHI = 0,
+    UPIC_FIELD_AX = 1,
+    UPIC_FIELD_AY = 2,
+    UPIC_FIELD_AZ = 3,
+    UPIC_FIELD_RHO = 4,
+    UPIC_FIELD_JX = 5,
+    UPIC_FIELD_JY = 6,
+    UPIC_FIELD_JZ = 7,
+    UPIC_FIELD_COUNT = 8
+};
+
+/* Diagnostics row, the column order of the reference's _diagnostics.csv after
+ * step,time,requested_method,active_method,charge_update
+ * (spectral_pic_part3.cpp:886-900, 1117-1119). */
+enum {
+    UPIC_DIAG_GAUGE_RMS = 0,
+    UPIC_DIAG_GAUSS_RMS,
+    UPIC_DIAG_CONTINUITY_RMS,
+    UPIC_DIAG_BZ_L2,
+    UPIC_DIAG_B_L2,
+    UPIC_DIAG_E_L2,
+    UPIC_DIAG_RHO_L2,
+    UPIC_DIAG_J_L2,
+    UPIC_DIAG_FIELD_ENERGY,
+    UPIC_DIAG_KINETIC_ENERGY,
+    UPIC_DIAG_TOTAL_ENERGY,
+    UPIC_DIAG_MAX_SPEED,
+    UPIC_DIAG_MEAN_GAMMA,
+    UPIC_DIAG_COUNT
+};
+
+/* Run configuration; mirrors the reference deck keys of
+ * spectral_pic_part3.cpp:174-231 (Config).  Fill with upic_config_default(). */
+typedef struct upic_config {
+    int nx, ny;              /* powers of two (radix-2 FFT), read_config:281 */
+    double Lx, Ly;
+    double dt;
+    int method;              /* UPIC_METHOD_* */
+    int charge_update;       /* UPIC_CHARGE_* */
+    double c, eps0, mu0;     /* normalized constants */
+    double n0;               /* fixed uniform ion background density */
+    int precision;           /* UPIC_PRECISION_* */
+    int sort_interval;       /* steps between particle re-sorts; 0 = automatic */
+    int tile;                /* deposit tile edge in cells; 0 = automatic */
+    int guard;               /* deposit window guard in cells; -1 = automatic */
+    int reserved[8];
+} upic_config;
+
+typedef struct upic_ctx upic_ctx;
+
+/* ABI version of the loaded library (UPIC_ABI_VERSION). */
+int upic_abi_version(void);
+
+/* Defaults of the reference Config (spectral_pic_part3.cpp:174-231). */
+int upic_config_default(upic_config* cfg);
+
+/* Validate cfg (read_config:281-293) and allocate a context on the current
+ * CUDA device.  Replaces make_grid (spectral_pic_part3.cpp:332). */
+int upic_create(const upic_config* cfg, upic_ctx** out);
+int upic_destroy(upic_ctx* ctx);
+
+/* Message of the last error on ctx (or of the last failed upic_create when
+ * ctx is NULL).  The pointer stays valid until the next call on ctx. */
+const char* upic_last_error(const upic_ctx* ctx);
+
+/* Order the context's work on a caller-provided cudaStream_t (NULL restores
+ * the context's own stream). */
+int upic_set_stream(upic_ctx* ctx, void* cuda_stream);
+
+/* Load the mobile electrons (ParticleSet::electrons,
+ * spectral_pic_part3.cpp:586-622): positions x,y; canonical momentum P,
+ * velocity v and previous velocity v_prev as xyz triples; per-particle
+ * charge q and mass m.  Copies host -> device. */
+int upic_set_particles(upic_ctx* ctx, long np, const double* x, const double* y,
+                       const double* P, const double* v, const double* v_prev,
+                       const double* q, const double* m);
+
+/* Copy the particle state back in the order it was given. */
+int upic_get_particles(upic_ctx* ctx, long np, double* x, double* y, double* P, double* v,
+                       double* v_prev);
+
+/* Start-up fields: rho0 = n0 + deposited electron charge, J0 = deposited
+ * current, phi0 from Poisson, A0 = 0, all BDF histories filled with copies
+ * (spectral_pic_part3.cpp:1100-1111).  If diag_row is not NULL it receives
+ * the step-0 diagnostics row (BDF1 derivatives, :1121-1131). */
+int upic_init_fields(upic_ctx* ctx, double* diag_row);
+
+/* Advance nsteps steps of the explicit BDF/IAEM method (loop body of
+ * run_simulation, spectral_pic_part3.cpp:1133-1189).  diag (optional):
+ * nsteps x UPIC_DIAG_COUNT rows; diagnostics are computed on steps where
+ * (global step % diag_stride == 0) or on the last step of this call, and
+ * other rows are filled with NaN.  diag_stride <= 0 disables diagnostics. */
+int upic_step(upic_ctx* ctx, int nsteps, int diag_stride, double* diag);
+
+/* Profiling of the dominant kernel: with on != 0, CUDA events are recorded
+ * on the context's stream around every particle push kernel of upic_step
+ * (gather + push + next-step deposit).  on = 0 disables and clears.  No
+ * reference counterpart (the reference only times whole runs with a wall
+ * clock, Project3/ec_pic_nyquist_projected.cpp:145-197). */
+int upic_profile_enable(upic_ctx* ctx, int on);
+
+/* Summed device time (ms) and count of the push kernels recorded since
+ * upic_profile_enable, and the number of kernels this library has launched
+ * since it was loaded (all contexts). */
+int upic_profile_read(upic_ctx* ctx, double* push_ms, long* push_launches, long* kernel_launches);
+
+/* Number of steps taken since upic_init_fields. */
+int upic_step_count(const upic_ctx* ctx, long* steps);
+
+/* Fields of the current time level (phi, A, rho, J), nx*ny doubles. */
+int upic_get_field(upic_ctx* ctx, int which, double* host);
+
+/* ---- Kernel-level entry points (host arrays in and out).  Each runs the
+ * same device kernels as upic_step on the context's grid. ------------- */
+
+/* J (3 x nx*ny) = sum_p q v S(x_p)/dA: deposit_current,
+ * spectral_pic_part3.cpp:747-755 (scatter_scalar :554). */
+int upic_deposit_current(upic_ctx* ctx, long np, const double* x, const double* y,
+                         const double* v, const double* q, double* J);
+
+/* rho = n0 + sum_p q S(x_p)/dA: deposit_total_charge_naive,
+ * spectral_pic_part3.cpp:739-745. */
+int upic_deposit_charge(upic_ctx* ctx, long np, const double* x, const double* y,
+                        const double* q, double* rho);
+
+/* out[p] = sum f S(x_p): gather_scalar, spectral_pic_part3.cpp:564-574. */
+int upic_gather(upic_ctx* ctx, const double* f, long np, const double* x, const double* y,
+                double* out);
+
+/* In-place complex 2D FFT (rows then columns), inverse scaled by 1/N:
+ * fft2d, spectral_pic_part3.cpp:406-424. */
+int upic_fft2d(upic_ctx* ctx, double* re, double* im, int inverse);
+
+/* Pseudo-spectral d/dx (dir 0) or d/dy (dir 1) with the Nyquist wave number
+ * zeroed: spectral_derivative, spectral_pic_part3.cpp:440-447. */
+int upic_spectral_derivative(upic_ctx* ctx, const double* f, int dir, double* out);
+
+/* phi = Poisson(rho), zero-mean: solve_initial_phi_from_poisson,
+ * spectral_pic_part3.cpp:819-827. */
+int upic_poisson(upic_ctx* ctx, const double* rho, double* phi);
+
+/* One BDF Helmholtz solve (solve_bdf_wave_scalar, spectral_pic_part3.cpp:829-848):
+ * hist holds u^n, u^{n-1}, ... (2 fields for BDF1, 4 for BDF2). */
+int upic_solve_bdf(upic_ctx* ctx, const double* source, const double* hist, double* out);
+
+/* Seeded synthetic plasma generator (splitmix64 + Box-Muller, independent of
+ * any C++ library's distributions): np_per_cell electrons per cell at uniform
+ * random positions in [0,Lx)x[0,Ly) with a drifting bi-Maxwellian in
+ * normalized momentum u = gamma v / c (thermal spreads uth[3], drift
+ * udrift[3]); P = m gamma v, v_prev = v, q = -n0*Lx*Ly/Np, m = |q|.
+ * Deterministic for a given seed, independent of thread count. */
+int upic_generate_bimaxwellian(int nx, int ny, double Lx, double Ly, int np_per_cell,
+                               double c, double n0, const double* uth, const double* udrift,
+                               uint64_t seed, double* x, double* y, double* P, double* v,
+                               double* v_prev, double* q, double* m);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UPIC_H */

@@ -1,0 +1,104 @@
+"""Regenerate the golden fixtures in tests/golden/ from the reference's own code.
+
+Runs the reference solver Project2/spectral_pic_part3.cpp through the C-ABI
+harness oracle/_ref/libref_p2.so (built by `make -C oracle` from the reference
+sources) on small seeded inputs and saves inputs and outputs, and copies the
+published validation numbers of Project2/docs/validation_summary.json.  The
+fixtures let the oracle and the GPU path be checked where the reference
+sources are absent.
+
+    python tests/golden/make_golden.py
+"""
+import ctypes
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+import oracle_lib as ol  # noqa: E402
+
+REF = "/root/reference"
+
+
+def seeded_particles(rng, n, Lx, Ly, vth=(0.02, 0.2, 0.05), edge=True):
+    """Random electrons (uniform positions, Maxwellian momenta) with q/m = -1."""
+    x = rng.uniform(0, Lx, n)
+    y = rng.uniform(0, Ly, n)
+    if edge and n >= 8:
+        # positions on and next to cell edges, the domain edge and node centres
+        x[:4] = [0.0, np.nextafter(Lx, 0), Lx / 2, 0.5 * Lx / 8]
+        y[:4] = [np.nextafter(Ly, 0), 0.0, 0.25 * Ly, Ly / 2]
+    u = rng.normal(size=(n, 3)) * np.asarray(vth)
+    gam = np.sqrt(1 + (u * u).sum(1))
+    v = u / gam[:, None]
+    w = Lx * Ly / n
+    q = np.full(n, -w)
+    m = np.full(n, w)
+    P = m[:, None] * u
+    vprev = v + rng.normal(size=(n, 3)) * 1e-3
+    return {"x": x, "y": y, "P": P, "v": v, "vprev": vprev, "q": q, "m": m}
+
+
+def main():
+    lib = ol.ref_p2()
+    if lib is None:
+        raise SystemExit("oracle/_ref/libref_p2.so missing: run make -C oracle")
+    rng = np.random.default_rng(20260101)
+    nx, ny, Lx, Ly = 32, 16, 3.0, 2.0
+    parts = seeded_particles(rng, 2000, Lx, Ly)
+    N = nx * ny
+    J = np.zeros(3 * N)
+    lib.ref_p2_deposit_current(nx, ny, ctypes.c_double(Lx), ctypes.c_double(Ly), ctypes.c_long(2000),
+                               ol.ptr(parts["x"]), ol.ptr(parts["y"]), ol.ptr(parts["v"]),
+                               ol.ptr(parts["q"]), ol.ptr(J))
+    rho = np.zeros(N)
+    lib.ref_p2_deposit_charge(nx, ny, ctypes.c_double(Lx), ctypes.c_double(Ly), ctypes.c_double(1.0),
+                              ctypes.c_long(2000), ol.ptr(parts["x"]), ol.ptr(parts["y"]),
+                              ol.ptr(parts["q"]), ol.ptr(rho))
+    f = rng.normal(size=N)
+    gat = np.zeros(2000)
+    lib.ref_p2_gather(nx, ny, ctypes.c_double(Lx), ctypes.c_double(Ly), ol.ptr(f), ctypes.c_long(2000),
+                      ol.ptr(parts["x"]), ol.ptr(parts["y"]), ol.ptr(gat))
+    re = rng.normal(size=N)
+    im = rng.normal(size=N)
+    fre, fim = re.copy(), im.copy()
+    lib.ref_p2_fft2d(nx, ny, ol.ptr(fre), ol.ptr(fim), 0)
+    ire, iim = re.copy(), im.copy()
+    lib.ref_p2_fft2d(nx, ny, ol.ptr(ire), ol.ptr(iim), 1)
+    ddx = np.zeros(N)
+    ddy = np.zeros(N)
+    lib.ref_p2_spectral_derivative(nx, ny, ctypes.c_double(Lx), ctypes.c_double(Ly), ol.ptr(f), 0, ol.ptr(ddx))
+    lib.ref_p2_spectral_derivative(nx, ny, ctypes.c_double(Lx), ctypes.c_double(Ly), ol.ptr(f), 1, ol.ptr(ddy))
+    phi = np.zeros(N)
+    lib.ref_p2_poisson(nx, ny, ctypes.c_double(Lx), ctypes.c_double(Ly), ctypes.c_double(1.0), ol.ptr(rho),
+                       ol.ptr(phi))
+    np.savez_compressed(os.path.join(HERE, "p2_kernels.npz"), nx=nx, ny=ny, Lx=Lx, Ly=Ly,
+                        **{"in_" + k: v for k, v in parts.items()}, J=J, rho=rho, f=f, gather=gat,
+                        re=re, im=im, fft_re=fre, fft_im=fim, ifft_re=ire, ifft_im=iim, ddx=ddx,
+                        ddy=ddy, phi=phi)
+
+    # short runs of the step loop, every method/charge variant
+    for order in (1, 2):
+        for conserving in (True, False):
+            prob = ol.P2Problem(16, 32, 2.5, 4.0, 0.05, order, conserving, n_steps=12)
+            p = seeded_particles(rng, 1024, prob.Lx, prob.Ly)
+            out, diag, fields, _ = ol.simulate(lib.ref_p2_simulate, prob, p)
+            name = f"p2_run_bdf{order}_{'conserving' if conserving else 'naive'}.npz"
+            np.savez_compressed(os.path.join(HERE, name), params=prob.params(), iparams=prob.iparams(),
+                                **{"in_" + k: v for k, v in p.items()},
+                                **{"out_" + k: v for k, v in out.items()}, diag=diag, fields=fields)
+
+    # published validation numbers of the four Weibel decks
+    with open(os.path.join(REF, "Project2/docs/validation_summary.json")) as fh:
+        summ = json.load(fh)
+    runs = {k: v for k, v in summ["runs"].items() if k.startswith("weibel")}
+    with open(os.path.join(HERE, "p2_weibel_published.json"), "w") as fh:
+        json.dump({"source": "Project2/docs/validation_summary.json", "runs": runs}, fh, indent=1)
+    print("fixtures written")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,205 @@
+"""GPU parity of the explicit BDF/IAEM path (libupic.so) against the oracle
+and the reference fixtures.  Tolerances (relative to the max magnitude of the
+reference quantity): 1e-13 for one deposit / gather / FFT solve / step, 1e-10
+after 50 steps."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+import unstaggered_pic_b200 as up
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL_ONE = 1e-13
+TOL_50 = 1e-10
+
+
+def relerr(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = np.max(np.abs(b))
+    if scale == 0.0:
+        return float(np.max(np.abs(a)))
+    return float(np.max(np.abs(a - b)) / scale)
+
+
+def gold(name):
+    return dict(np.load(os.path.join(GOLD, name)))
+
+
+@pytest.fixture(scope="module")
+def kern():
+    g = gold("p2_kernels.npz")
+    sim = up.Simulation(up.Config(nx=int(g["nx"]), ny=int(g["ny"]), Lx=float(g["Lx"]), Ly=float(g["Ly"])))
+    yield sim, g
+    sim.close()
+
+
+def test_fft_forward_inverse(kern):
+    sim, g = kern
+    re, im = sim.fft2d(g["re"], g["im"])
+    assert relerr(re.ravel() + 1j * im.ravel(), g["fft_re"] + 1j * g["fft_im"]) < TOL_ONE
+    re, im = sim.fft2d(g["re"], g["im"], inverse=True)
+    assert relerr(re.ravel() + 1j * im.ravel(), g["ifft_re"] + 1j * g["ifft_im"]) < TOL_ONE
+
+
+def test_deposit_current_and_charge(kern):
+    sim, g = kern
+    J = sim.deposit_current(g["in_x"], g["in_y"], g["in_v"], g["in_q"])
+    assert relerr(J.ravel(), g["J"]) < TOL_ONE
+    rho = sim.deposit_charge(g["in_x"], g["in_y"], g["in_q"])
+    assert relerr(rho.ravel(), g["rho"]) < TOL_ONE
+
+
+def test_gather_derivative_poisson(kern):
+    sim, g = kern
+    assert relerr(sim.gather(g["f"], g["in_x"], g["in_y"]), g["gather"]) < TOL_ONE
+    assert relerr(sim.spectral_derivative(g["f"], 0).ravel(), g["ddx"]) < TOL_ONE
+    assert relerr(sim.spectral_derivative(g["f"], 1).ravel(), g["ddy"]) < TOL_ONE
+    assert relerr(sim.poisson(g["rho"]).ravel(), g["phi"]) < TOL_ONE
+
+
+def test_deposit_edge_cases(kern):
+    sim, g = kern
+    nx, ny = int(g["nx"]), int(g["ny"])
+    # no particles: zero current, rho = n0
+    J = sim.deposit_current(np.zeros(0), np.zeros(0), np.zeros((0, 3)), np.zeros(0))
+    assert np.all(J == 0.0)
+    assert np.all(sim.deposit_charge(np.zeros(0), np.zeros(0), np.zeros(0)) == 1.0)
+    # one particle on the periodic seam, many particles in one cell
+    Lx, Ly = float(g["Lx"]), float(g["Ly"])
+    x = np.array([0.0, np.nextafter(Lx, 0)] + [0.3 * Lx] * 5000)
+    y = np.array([np.nextafter(Ly, 0), 0.0] + [0.7 * Ly] * 5000)
+    v = np.tile([0.1, -0.2, 0.3], (len(x), 1))
+    q = -np.ones(len(x))
+    J = sim.deposit_current(x, y, v, q)
+    ref = np.zeros(3 * nx * ny)
+    ol.oracle().o2_deposit_current(nx, ny, ctypes.c_double(Lx), ctypes.c_double(Ly),
+                                   ctypes.c_long(len(x)), ol.ptr(x), ol.ptr(y), ol.ptr(v), ol.ptr(q),
+                                   ol.ptr(ref))
+    assert relerr(J.ravel(), ref) < TOL_ONE
+
+
+def test_solve_bdf_against_numpy():
+    nx, ny, Lx, Ly, dt, c = 16, 32, 2.0, 5.0, 0.05, 1.3
+    rng = np.random.default_rng(3)
+    for method, a in (("bdf1", [1.0, -1.0]), ("bdf2", [1.5, -2.0, 0.5])):
+        sim = up.Simulation(up.Config(nx=nx, ny=ny, Lx=Lx, Ly=Ly, dt=dt, method=method, c=c))
+        b = np.convolve(a, a)
+        src = rng.normal(size=(nx, ny))
+        hist = rng.normal(size=(len(b) - 1, nx, ny))
+        out = sim.solve_bdf(src, hist)
+        kx = 2 * np.pi * np.array([0 if i == nx // 2 else (i if i < nx // 2 else i - nx) for i in range(nx)]) / Lx
+        ky = 2 * np.pi * np.array([0 if j == ny // 2 else (j if j < ny // 2 else j - ny) for j in range(ny)]) / Ly
+        k2 = kx[:, None] ** 2 + ky[None, :] ** 2
+        s = 1.0 / (c * c * dt * dt)
+        rhs = np.fft.fft2(src) - sum(s * b[l] * np.fft.fft2(hist[l - 1]) for l in range(1, len(b)))
+        ref = np.fft.ifft2(rhs / (s * b[0] + k2)).real
+        assert relerr(out, ref) < TOL_ONE
+        sim.close()
+
+
+def _run_gpu(prob, parts, nsteps, sort_interval=0, tile=0, guard=-1):
+    cfg = up.Config(nx=prob.nx, ny=prob.ny, Lx=prob.Lx, Ly=prob.Ly, dt=prob.dt,
+                    method="bdf2" if prob.bdf_order == 2 else "bdf1",
+                    charge_update="conserving" if prob.conserving else "naive", c=prob.c,
+                    eps0=prob.eps0, mu0=prob.mu0, n0=prob.n0, sort_interval=sort_interval, tile=tile,
+                    guard=guard)
+    with up.Simulation(cfg) as sim:
+        sim.set_particles(parts["x"], parts["y"], parts["P"], parts["v"], parts["vprev"], parts["q"],
+                          parts["m"])
+        d0 = sim.init_fields(True)
+        diag = sim.step(nsteps, 1) if nsteps else np.zeros((0, 13))
+        out = sim.get_particles()
+        fields = np.stack([sim.field(n) for n in ("phi", "Ax", "Ay", "Az", "rho", "Jx", "Jy", "Jz")])
+    return out, np.vstack([d0[None], diag]), fields
+
+
+# diagnostics columns with physical (non round-off) values
+PHYS_DIAG = [3, 4, 5, 6, 7, 8, 9, 10, 11, 12]
+
+
+@pytest.mark.parametrize("name", ["p2_run_bdf1_conserving.npz", "p2_run_bdf1_naive.npz",
+                                  "p2_run_bdf2_conserving.npz", "p2_run_bdf2_naive.npz"])
+def test_step_loop_matches_reference_fixture(name):
+    g = gold(name)
+    p, ip = g["params"], g["iparams"]
+    prob = ol.P2Problem(int(ip[0]), int(ip[1]), p[0], p[1], p[2], int(ip[2]), bool(ip[3]), p[3], p[4],
+                        p[5], p[6], int(ip[4]), int(ip[5]))
+    parts = {k[3:]: g[k] for k in g if k.startswith("in_")}
+    out, diag, fields = _run_gpu(prob, parts, prob.n_steps)
+    assert relerr(out["x"], g["out_x"]) < 1e-12
+    assert relerr(out["y"], g["out_y"]) < 1e-12
+    assert relerr(out["P"], g["out_P"]) < 1e-11
+    assert relerr(out["v"], g["out_v"]) < 1e-11
+    assert relerr(out["v_prev"], g["out_vprev"]) < 1e-11
+    for f in range(8):
+        assert relerr(fields[f], g["fields"][f].reshape(fields[f].shape)) < 1e-10, f
+    for k in PHYS_DIAG:
+        assert relerr(diag[:, k], g["diag"][:, k]) < 1e-10, k
+    # round-off level residuals: same order of magnitude as the reference's
+    if bool(ip[3]):
+        for k in (0, 1, 2):
+            assert np.all(diag[1:, k] < 1e-12), k
+
+
+def _bimax(nx, ny, ppc, L, seed):
+    p = up.generate_bimaxwellian(nx, ny, L, L, ppc, (0.02, 0.2, 0.0), seed=seed)
+    p["vprev"] = p.pop("v_prev")
+    return p
+
+
+@pytest.mark.parametrize("order,conserving", [(1, True), (2, False)])
+def test_weibel_64x64_one_and_fifty_steps(order, conserving):
+    """64x64 Weibel bi-Maxwellian, 64 electrons per cell (the CPU-runnable
+    workload): one step to 1e-13 and fifty steps to 1e-10 against the oracle."""
+    L = 2 * np.pi / 0.3
+    parts = _bimax(64, 64, 64, L, 11)
+    for nsteps, tol in ((1, TOL_ONE), (50, TOL_50)):
+        prob = ol.P2Problem(64, 64, L, L, 0.05, order, conserving, n_steps=nsteps)
+        ref, rdiag, rfields, _ = ol.simulate(ol.oracle().o2_simulate, prob, parts)
+        out, diag, fields = _run_gpu(prob, parts, nsteps)
+        for k, rk in (("x", "x"), ("y", "y"), ("P", "P"), ("v", "v"), ("v_prev", "vprev")):
+            assert relerr(out[k], ref[rk]) < tol, (nsteps, k, relerr(out[k], ref[rk]))
+        for f in range(8):
+            assert relerr(fields[f], rfields[f]) < tol * 10, (nsteps, f)
+        for k in PHYS_DIAG:
+            assert relerr(diag[:, k], rdiag[:, k]) < tol * 10, (nsteps, k)
+
+
+def test_bitwise_reproducible_and_sort_independent_physics():
+    L = 2 * np.pi / 0.3
+    parts = _bimax(64, 64, 16, L, 5)
+    prob = ol.P2Problem(64, 64, L, L, 0.05, 1, True, n_steps=20)
+    a = _run_gpu(prob, parts, 20)
+    b = _run_gpu(prob, parts, 20)
+    for k in a[0]:
+        assert np.array_equal(a[0][k], b[0][k]), k
+    assert np.array_equal(a[2], b[2])
+    # a different sort cadence / tiling changes only the summation order
+    c = _run_gpu(prob, parts, 20, sort_interval=1, tile=8, guard=1)
+    assert relerr(c[0]["v"], a[0]["v"]) < 1e-11
+    assert relerr(c[2][5], a[2][5]) < 1e-11
+
+
+def test_published_weibel_deck_on_gpu():
+    """Project2 Weibel BDF1 conserving deck (reference quiet start) on the GPU
+    against Project2/docs/validation_summary.json."""
+    import json
+    with open(os.path.join(GOLD, "p2_weibel_published.json")) as fh:
+        pub = json.load(fh)["runs"]["weibel_bdf1_conserving"]
+    o = ol.oracle()
+    o.o2_init_weibel.restype = ctypes.c_long
+    L = 6.283185307179586
+    parts = ol.init_weibel(o.o2_init_weibel, 32, 32, L, L, 4)
+    prob = ol.P2Problem(32, 32, L, L, 0.05, 1, True, n_steps=160)
+    _, diag, _ = _run_gpu(prob, parts, 160)
+    assert abs(diag[-1, 3] / pub["final_Bz_l2"] - 1) < 1e-9
+    assert abs(diag[-1, 10] / pub["final_total_energy"] - 1) < 1e-12
+    assert abs(diag[1:, 11].max() / pub["max_speed"] - 1) < 1e-12
+    # round-off residuals: same level as published (both far below the naive runs)
+    assert diag[1:, 0].max() < 100 * pub["max_gauge_rms"]
+    assert diag[1:, 1].max() < 100 * pub["max_gauss_rms"]

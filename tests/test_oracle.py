@@ -1,0 +1,102 @@
+"""CPU tests of the oracle: pinned to the reference's own code (bit for bit)
+and to the reference's published validation numbers."""
+import ctypes
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLD, name)))
+
+
+def test_oracle_kernels_match_reference_fixtures():
+    o = ol.oracle()
+    g = load("p2_kernels.npz")
+    nx, ny, Lx, Ly = int(g["nx"]), int(g["ny"]), float(g["Lx"]), float(g["Ly"])
+    n = len(g["in_x"])
+    cd = ctypes.c_double
+    J = np.zeros(3 * nx * ny)
+    o.o2_deposit_current(nx, ny, cd(Lx), cd(Ly), ctypes.c_long(n), ol.ptr(g["in_x"]), ol.ptr(g["in_y"]),
+                         ol.ptr(g["in_v"]), ol.ptr(g["in_q"]), ol.ptr(J))
+    assert np.array_equal(J, g["J"])
+    rho = np.zeros(nx * ny)
+    o.o2_deposit_charge(nx, ny, cd(Lx), cd(Ly), cd(1.0), ctypes.c_long(n), ol.ptr(g["in_x"]),
+                        ol.ptr(g["in_y"]), ol.ptr(g["in_q"]), ol.ptr(rho))
+    assert np.array_equal(rho, g["rho"])
+    gat = np.zeros(n)
+    o.o2_gather(nx, ny, cd(Lx), cd(Ly), ol.ptr(g["f"]), ctypes.c_long(n), ol.ptr(g["in_x"]),
+                ol.ptr(g["in_y"]), ol.ptr(gat))
+    assert np.array_equal(gat, g["gather"])
+    for inv, kr, ki in ((0, "fft_re", "fft_im"), (1, "ifft_re", "ifft_im")):
+        re, im = g["re"].copy(), g["im"].copy()
+        o.o2_fft2d(nx, ny, ol.ptr(re), ol.ptr(im), inv)
+        assert np.array_equal(re, g[kr]) and np.array_equal(im, g[ki])
+    for d, key in ((0, "ddx"), (1, "ddy")):
+        out = np.zeros(nx * ny)
+        o.o2_spectral_derivative(nx, ny, cd(Lx), cd(Ly), ol.ptr(g["f"]), d, ol.ptr(out))
+        assert np.array_equal(out, g[key])
+    phi = np.zeros(nx * ny)
+    o.o2_poisson(nx, ny, cd(Lx), cd(Ly), cd(1.0), ol.ptr(g["rho"]), ol.ptr(phi))
+    assert np.array_equal(phi, g["phi"])
+
+
+@pytest.mark.parametrize("name", ["p2_run_bdf1_conserving.npz", "p2_run_bdf1_naive.npz",
+                                  "p2_run_bdf2_conserving.npz", "p2_run_bdf2_naive.npz"])
+def test_oracle_step_loop_matches_reference_fixtures(name):
+    g = load(name)
+    p, ip = g["params"], g["iparams"]
+    prob = ol.P2Problem(int(ip[0]), int(ip[1]), p[0], p[1], p[2], int(ip[2]), bool(ip[3]), p[3], p[4],
+                        p[5], p[6], int(ip[4]), int(ip[5]))
+    parts = {k[3:]: g[k] for k in g if k.startswith("in_")}
+    out, diag, fields, _ = ol.simulate(ol.oracle().o2_simulate, prob, parts)
+    for k in out:
+        assert np.array_equal(out[k], g["out_" + k]), k
+    assert np.array_equal(diag, g["diag"], equal_nan=True)
+    assert np.array_equal(fields, g["fields"])
+
+
+@pytest.mark.parametrize("run,order,conserving", [("weibel_bdf1_conserving", 1, True),
+                                                  ("weibel_bdf2_conserving", 2, True),
+                                                  ("weibel_bdf1_naive", 1, False)])
+def test_oracle_reproduces_published_weibel_validation(run, order, conserving):
+    """Full Project2 Weibel decks (32x32, 4 samples/cell, 160 steps) against
+    Project2/docs/validation_summary.json."""
+    with open(os.path.join(GOLD, "p2_weibel_published.json")) as fh:
+        pub = json.load(fh)["runs"][run]
+    o = ol.oracle()
+    o.o2_init_weibel.restype = ctypes.c_long
+    L = 6.283185307179586
+    parts = ol.init_weibel(o.o2_init_weibel, 32, 32, L, L, 4)
+    prob = ol.P2Problem(32, 32, L, L, 0.05, order, conserving, n_steps=160)
+    _, diag, _, _ = ol.simulate(o.o2_simulate, prob, parts, want_fields=False)
+    # maxima skip the initial row, as Project2/tools/validate_against_paper.py:60,75 does
+    assert diag[1:, 0].max() == pub["max_gauge_rms"]
+    assert diag[1:, 1].max() == pub["max_gauss_rms"]
+    assert diag[1:, 2].max() == pub["max_continuity_rms"]
+    assert diag[-1, 3] == pub["final_Bz_l2"]
+    assert diag[-1, 10] == pub["final_total_energy"]
+    assert diag[1:, 11].max() == pub["max_speed"]
+
+
+def test_oracle_matches_live_reference_when_built():
+    """When the reference harness is available (this container), compare a
+    fresh random case directly."""
+    ref = ol.ref_p2()
+    if ref is None:
+        pytest.skip("reference harness not built (no reference sources)")
+    rng = np.random.default_rng(7)
+    from golden.make_golden import seeded_particles
+    prob = ol.P2Problem(8, 64, 1.0, 7.0, 0.1, 2, False, n_steps=5)
+    p = seeded_particles(rng, 300, prob.Lx, prob.Ly)
+    a = ol.simulate(ol.oracle().o2_simulate, prob, p)
+    b = ol.simulate(ref.ref_p2_simulate, prob, p)
+    for k in a[0]:
+        assert np.array_equal(a[0][k], b[0][k])
+    assert np.array_equal(a[1], b[1], equal_nan=True)

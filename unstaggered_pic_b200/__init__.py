@@ -1,0 +1,218 @@
+"""B200-native unstaggered generalized-momentum PIC step.
+
+Python mirror of the C ABI in include/upic.h.  The numerical work runs in
+libupic.so (hand-written CUDA for sm_100a); this module only marshals host
+arrays.  Names follow the reference solver (sgong11/Unstaggered_PIC,
+Project2/spectral_pic_part3.cpp): particles carry x, y, canonical momentum P,
+velocity v, previous velocity v_prev, charge q and mass m; grids are nx*ny
+doubles with node id = i*ny + j.
+"""
+import ctypes
+
+import numpy as np
+
+from ._native import UPIC_ERR, UpicConfig, c_dp, lib
+
+__all__ = ["UpicError", "Config", "Simulation", "generate_bimaxwellian", "DIAG_COLUMNS",
+           "METHODS", "FIELDS"]
+
+METHODS = {"bdf1": 1, "bdf2": 2}
+CHARGE_UPDATES = {"conserving": 0, "naive": 1}
+FIELDS = {"phi": 0, "Ax": 1, "Ay": 2, "Az": 3, "rho": 4, "Jx": 5, "Jy": 6, "Jz": 7}
+# Diagnostics columns of the reference's _diagnostics.csv (spectral_pic_part3.cpp:1117-1119).
+DIAG_COLUMNS = ["gauge_rms", "gauss_rms", "continuity_rms", "Bz_l2", "B_l2", "E_l2", "rho_l2",
+                "J_l2", "field_energy", "kinetic_energy", "total_energy", "max_speed",
+                "mean_gamma"]
+
+
+class UpicError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{UPIC_ERR.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(c_dp)
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None and a.shape != shape:
+        a = a.reshape(shape)
+    return a
+
+
+class Config:
+    """Run configuration with the reference deck's keys and defaults
+    (Config, spectral_pic_part3.cpp:174-231)."""
+
+    def __init__(self, nx=32, ny=32, Lx=2 * np.pi, Ly=2 * np.pi, dt=0.05, method="bdf1",
+                 charge_update="conserving", c=1.0, eps0=1.0, mu0=1.0, n0=1.0,
+                 sort_interval=0, tile=0, guard=-1):
+        self.nx, self.ny, self.Lx, self.Ly, self.dt = nx, ny, Lx, Ly, dt
+        self.method, self.charge_update = method, charge_update
+        self.c, self.eps0, self.mu0, self.n0 = c, eps0, mu0, n0
+        self.sort_interval, self.tile, self.guard = sort_interval, tile, guard
+
+    def to_c(self):
+        cfg = UpicConfig()
+        lib().upic_config_default(ctypes.byref(cfg))
+        cfg.nx, cfg.ny = int(self.nx), int(self.ny)
+        cfg.Lx, cfg.Ly, cfg.dt = float(self.Lx), float(self.Ly), float(self.dt)
+        cfg.method = METHODS[self.method] if isinstance(self.method, str) else int(self.method)
+        cu = self.charge_update
+        cfg.charge_update = CHARGE_UPDATES[cu] if isinstance(cu, str) else int(cu)
+        cfg.c, cfg.eps0, cfg.mu0, cfg.n0 = float(self.c), float(self.eps0), float(self.mu0), float(self.n0)
+        cfg.sort_interval, cfg.tile, cfg.guard = int(self.sort_interval), int(self.tile), int(self.guard)
+        return cfg
+
+
+class Simulation:
+    """One device context: particles + field state of the explicit BDF/IAEM step."""
+
+    def __init__(self, config):
+        self.config = config
+        self._ctx = ctypes.c_void_p()
+        cfg = config.to_c()
+        rc = lib().upic_create(ctypes.byref(cfg), ctypes.byref(self._ctx))
+        if rc != 0:
+            raise UpicError(rc, lib().upic_last_error(None).decode())
+        self.np = 0
+        self.N = config.nx * config.ny
+
+    def _check(self, rc):
+        if rc != 0:
+            raise UpicError(rc, lib().upic_last_error(self._ctx).decode())
+
+    def close(self):
+        if self._ctx:
+            lib().upic_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._ctx
+
+    def set_stream(self, stream_ptr):
+        self._check(lib().upic_set_stream(self._ctx, ctypes.c_void_p(stream_ptr)))
+
+    def set_particles(self, x, y, P, v, v_prev, q, m):
+        n = len(x)
+        arrs = [_f64(x), _f64(y), _f64(P, (n, 3)), _f64(v, (n, 3)), _f64(v_prev, (n, 3)), _f64(q),
+                _f64(m)]
+        self._check(lib().upic_set_particles(self._ctx, n, *[_p(a) for a in arrs]))
+        self.np = n
+
+    def get_particles(self):
+        n = self.np
+        out = {"x": np.empty(n), "y": np.empty(n), "P": np.empty((n, 3)), "v": np.empty((n, 3)),
+               "v_prev": np.empty((n, 3))}
+        self._check(lib().upic_get_particles(self._ctx, n, _p(out["x"]), _p(out["y"]), _p(out["P"]),
+                                             _p(out["v"]), _p(out["v_prev"])))
+        return out
+
+    def init_fields(self, diagnostics=True):
+        row = np.empty(13) if diagnostics else None
+        self._check(lib().upic_init_fields(self._ctx, _p(row)))
+        return row
+
+    def step(self, nsteps=1, diag_stride=1):
+        diag = np.empty((nsteps, 13)) if diag_stride > 0 else None
+        self._check(lib().upic_step(self._ctx, int(nsteps), int(diag_stride), _p(diag)))
+        return diag
+
+    def profile_enable(self, on=True):
+        self._check(lib().upic_profile_enable(self._ctx, int(bool(on))))
+
+    def profile_read(self):
+        """(summed push-kernel ms, push launches, library kernel launches)."""
+        ms = ctypes.c_double()
+        n = ctypes.c_long()
+        k = ctypes.c_long()
+        self._check(lib().upic_profile_read(self._ctx, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(k)))
+        return ms.value, n.value, k.value
+
+    def steps_taken(self):
+        s = ctypes.c_long()
+        self._check(lib().upic_step_count(self._ctx, ctypes.byref(s)))
+        return s.value
+
+    def field(self, name):
+        out = np.empty(self.N)
+        self._check(lib().upic_get_field(self._ctx, FIELDS[name], _p(out)))
+        return out.reshape(self.config.nx, self.config.ny)
+
+    # ---- kernel-level entry points (include/upic.h) -----------------------
+    def deposit_current(self, x, y, v, q):
+        n = len(x)
+        J = np.empty(3 * self.N)
+        arrs = [_f64(x), _f64(y), _f64(v, (n, 3)), _f64(q)]
+        self._check(lib().upic_deposit_current(self._ctx, n, *[_p(a) for a in arrs], _p(J)))
+        return J.reshape(3, self.config.nx, self.config.ny)
+
+    def deposit_charge(self, x, y, q):
+        n = len(x)
+        rho = np.empty(self.N)
+        arrs = [_f64(x), _f64(y), _f64(q)]
+        self._check(lib().upic_deposit_charge(self._ctx, n, *[_p(a) for a in arrs], _p(rho)))
+        return rho.reshape(self.config.nx, self.config.ny)
+
+    def gather(self, f, x, y):
+        n = len(x)
+        out = np.empty(n)
+        self._check(lib().upic_gather(self._ctx, _p(_f64(f).ravel()), n, _p(_f64(x)), _p(_f64(y)),
+                                      _p(out)))
+        return out
+
+    def fft2d(self, re, im, inverse=False):
+        re = _f64(re).ravel().copy()
+        im = _f64(im).ravel().copy()
+        self._check(lib().upic_fft2d(self._ctx, _p(re), _p(im), int(bool(inverse))))
+        shape = (self.config.nx, self.config.ny)
+        return re.reshape(shape), im.reshape(shape)
+
+    def spectral_derivative(self, f, direction):
+        out = np.empty(self.N)
+        self._check(lib().upic_spectral_derivative(self._ctx, _p(_f64(f).ravel()), int(direction),
+                                                   _p(out)))
+        return out.reshape(self.config.nx, self.config.ny)
+
+    def poisson(self, rho):
+        out = np.empty(self.N)
+        self._check(lib().upic_poisson(self._ctx, _p(_f64(rho).ravel()), _p(out)))
+        return out.reshape(self.config.nx, self.config.ny)
+
+    def solve_bdf(self, source, hist):
+        out = np.empty(self.N)
+        h = _f64(hist).ravel()
+        self._check(lib().upic_solve_bdf(self._ctx, _p(_f64(source).ravel()), _p(h), _p(out)))
+        return out.reshape(self.config.nx, self.config.ny)
+
+
+def generate_bimaxwellian(nx, ny, Lx, Ly, ppc, uth, udrift=(0.0, 0.0, 0.0), c=1.0, n0=1.0, seed=1):
+    """Seeded synthetic plasma (upic_generate_bimaxwellian): returns a dict of
+    x, y, P, v, v_prev, q, m in the reference's particle layout."""
+    n = nx * ny * ppc
+    out = {"x": np.empty(n), "y": np.empty(n), "P": np.empty((n, 3)), "v": np.empty((n, 3)),
+           "v_prev": np.empty((n, 3)), "q": np.empty(n), "m": np.empty(n)}
+    uth = _f64(uth)
+    ud = _f64(udrift)
+    rc = lib().upic_generate_bimaxwellian(int(nx), int(ny), float(Lx), float(Ly), int(ppc), float(c),
+                                          float(n0), _p(uth), _p(ud), ctypes.c_uint64(seed),
+                                          *[_p(out[k]) for k in ("x", "y", "P", "v", "v_prev", "q",
+                                                                 "m")])
+    if rc != 0:
+        raise UpicError(rc, "generate_bimaxwellian failed")
+    return out

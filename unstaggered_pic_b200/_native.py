@@ -1,0 +1,85 @@
+"""ctypes binding of libupic.so (include/upic.h).
+
+The library is the product: there is no CPU fallback.  Loading fails loudly
+when libupic.so has not been built (python -m unstaggered_pic_b200.build).
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libupic.so")
+
+c_dp = ctypes.POINTER(ctypes.c_double)
+c_ip = ctypes.POINTER(ctypes.c_int)
+
+UPIC_ERR = {
+    -1: "UPIC_ERR_CONFIG", -2: "UPIC_ERR_ARGUMENT", -3: "UPIC_ERR_CUDA", -4: "UPIC_ERR_STATE",
+    -5: "UPIC_ERR_NONFINITE", -6: "UPIC_ERR_NONCONVERGED", -7: "UPIC_ERR_LOCAL_PARTICLE",
+    -8: "UPIC_ERR_SUPERLUMINAL", -9: "UPIC_ERR_NOMEM",
+}
+
+# Exported C symbols with (restype, argtypes); the ABI test checks each one.
+SYMBOLS = {
+    "upic_abi_version": (ctypes.c_int, []),
+    "upic_config_default": (ctypes.c_int, [ctypes.c_void_p]),
+    "upic_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "upic_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "upic_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "upic_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "upic_set_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 7),
+    "upic_get_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 5),
+    "upic_init_fields": (ctypes.c_int, [ctypes.c_void_p, c_dp]),
+    "upic_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
+    "upic_step_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]),
+    "upic_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "upic_profile_read": (ctypes.c_int, [ctypes.c_void_p, c_dp, ctypes.POINTER(ctypes.c_long),
+                                         ctypes.POINTER(ctypes.c_long)]),
+    "upic_get_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp]),
+    "upic_deposit_current": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 5),
+    "upic_deposit_charge": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 4),
+    "upic_gather": (ctypes.c_int, [ctypes.c_void_p, c_dp, ctypes.c_long, c_dp, c_dp, c_dp]),
+    "upic_fft2d": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp, ctypes.c_int]),
+    "upic_spectral_derivative": (ctypes.c_int, [ctypes.c_void_p, c_dp, ctypes.c_int, c_dp]),
+    "upic_poisson": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp]),
+    "upic_solve_bdf": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp, c_dp]),
+    "upic_generate_bimaxwellian": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                  ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                                  ctypes.c_double, c_dp, c_dp, ctypes.c_uint64]
+                                   + [c_dp] * 7),
+}
+
+
+class UpicConfig(ctypes.Structure):
+    """Mirror of struct upic_config (include/upic.h)."""
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("Lx", ctypes.c_double), ("Ly", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("method", ctypes.c_int), ("charge_update", ctypes.c_int),
+        ("c", ctypes.c_double), ("eps0", ctypes.c_double), ("mu0", ctypes.c_double),
+        ("n0", ctypes.c_double),
+        ("precision", ctypes.c_int), ("sort_interval", ctypes.c_int),
+        ("tile", ctypes.c_int), ("guard", ctypes.c_int),
+        ("reserved", ctypes.c_int * 8),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libupic.so once; raise if it is missing (no fallback path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build the CUDA library with "
+            "`python -m unstaggered_pic_b200.build` (no CPU fallback exists)")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SYMBOLS.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L

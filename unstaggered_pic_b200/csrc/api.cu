@@ -1,0 +1,963 @@
+// C-ABI implementation (include/upic.h): device context, memory layout and
+// the explicit BDF/IAEM step driver.
+//
+// HBM layout of a context (N = nx*ny nodes, np particles):
+//   particles   2 x SoA {x, y, Px, Py, Pz, vx, vy, vz, wx, wy, wz (v_prev), id
+//               [, q, m when not uniform]}: the active set and a sort target
+//   acc         8 x N uint64: fixed-point (hi, lo) accumulators for J (3) and rho
+//   J, rho      3 x N, N doubles: current deposit of this time level
+//   gf          12 x N doubles: interleaved gather records (A, grad phi, grad A)
+//   spec        16 x N complex: J^ (3), deposited rho^ (1), gather spectra (11)
+//   hist        5 fields x 5 slots x N complex: phi^, A^ (3), rho^ ring buffers
+//   dspec/dreal 10 x N complex / real: diagnostics fields
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/upic.h"
+#include "kernels.h"
+#include "upic_common.cuh"
+
+using namespace upic;
+
+namespace {
+
+constexpr int kHistSlots = 5;
+constexpr int kDiagFields = 10;
+constexpr int kRedGrid = 148 * 2;
+
+thread_local std::string g_create_error;
+
+}  // namespace
+
+struct upic_ctx {
+    upic_config cfg{};
+    std::string err;
+    int nx = 0, ny = 0, N = 0;
+    double dx = 0, dy = 0, dA = 0;
+    cudaStream_t own = nullptr, st = nullptr;
+    int device = 0, nsm = 148;
+
+    FftPlan plan{};
+    double2* d_twx = nullptr;
+    double2* d_twy = nullptr;
+    double *d_kx = nullptr, *d_ky = nullptr, *d_k2 = nullptr;
+
+    // particle state
+    long np = 0, cap = 0;
+    ParticleSoA P[2];
+    int cur = 0;
+    bool uniform_qm = true;
+    double q0 = 0, m0 = 0;
+    double scale[4] = {1, 1, 1, 1};
+    double* d_tmp3 = nullptr;  // 3*cap staging for xyz triples
+
+    // kernel-level entry points use their own particle buffers
+    long kcap = 0;
+    ParticleSoA K[2];
+
+    // grid state
+    unsigned long long* d_acc = nullptr;
+    double* d_J = nullptr;
+    double* d_rho = nullptr;
+    double* d_gf = nullptr;
+    double2* d_spec = nullptr;
+    double2* d_hist = nullptr;
+    double2* d_dspec = nullptr;
+    double* d_dreal = nullptr;
+    double* d_partials = nullptr;
+    double* d_pdiag = nullptr;
+    double* d_row = nullptr;
+    double* h_row = nullptr;  // pinned
+
+    int head = 0;
+    long steps = 0;
+    bool fields_ready = false;
+    int steps_since_sort = 0;
+    int sort_interval = 4;
+
+    // profiling: CUDA events around every particle push kernel
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+
+    TileGeom tg{};
+    SortWork sw{};
+    SortWork ksw{};
+    int push_grid = 148;
+
+    std::vector<void*> allocs;
+};
+
+// ---------------------------------------------------------------------------
+namespace {
+
+int fail(upic_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define UPIC_CUDA(ctx, call)                                                               \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(ctx, UPIC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+int dalloc(upic_ctx* c, T** p, size_t count) {
+    void* v = nullptr;
+    cudaError_t e = cudaMalloc(&v, sizeof(T) * (count ? count : 1));
+    if (e != cudaSuccess)
+        return fail(c, UPIC_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    c->allocs.push_back(v);
+    *p = reinterpret_cast<T*>(v);
+    return 0;
+}
+
+void dfree(upic_ctx* c, void* p) {
+    if (!p) return;
+    for (auto& a : c->allocs)
+        if (a == p) {
+            cudaFree(p);
+            a = nullptr;
+        }
+}
+
+bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+int mode_number(int i, int n) {
+    // spectral_pic_part3.cpp:320-330: Nyquist wave number zeroed.
+    if (n > 1 && i == n / 2) return 0;
+    return (i < n / 2) ? i : i - n;
+}
+
+std::vector<double2> twiddles(int n) {
+    std::vector<double2> t(n > 1 ? n / 2 : 1);
+    for (int m = 0; m < (int)t.size(); ++m) {
+        const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)n;
+        t[m] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    return t;
+}
+
+TileGeom make_tiles(int nx, int ny, int tile, int guard) {
+    TileGeom g{};
+    g.nx = nx;
+    g.ny = ny;
+    g.guard = guard;
+    auto axis = [&](int n, int& t, int& nt, int& w, int& full) {
+        t = tile < n ? tile : n;
+        if (n <= tile + 2 * guard + 2) {
+            full = 1;
+            t = n;
+            w = n;
+        } else {
+            full = 0;
+            w = t + 2 * guard + 2;
+        }
+        nt = n / t;
+    };
+    axis(nx, g.tile_x, g.ntx, g.wx, g.full_x);
+    axis(ny, g.tile_y, g.nty, g.wy, g.full_y);
+    g.chunk = 2048;
+    return g;
+}
+
+int alloc_soa(upic_ctx* c, ParticleSoA& s, long cap, bool with_state, bool with_qm) {
+    int rc = 0;
+    double** arrs[] = {&s.x, &s.y, &s.vx, &s.vy, &s.vz};
+    for (double** a : arrs)
+        if ((rc = dalloc(c, a, cap))) return rc;
+    if (with_state) {
+        double** st[] = {&s.Px, &s.Py, &s.Pz, &s.wx, &s.wy, &s.wz};
+        for (double** a : st)
+            if ((rc = dalloc(c, a, cap))) return rc;
+    }
+    if (with_qm) {
+        if ((rc = dalloc(c, &s.q, cap))) return rc;
+        if ((rc = dalloc(c, &s.m, cap))) return rc;
+    }
+    return dalloc(c, &s.id, cap);
+}
+
+void free_soa(upic_ctx* c, ParticleSoA& s) {
+    void* ps[] = {s.x, s.y, s.Px, s.Py, s.Pz, s.vx, s.vy, s.vz, s.wx, s.wy, s.wz, s.q, s.m, s.id};
+    for (void* p : ps) dfree(c, p);
+    s = ParticleSoA{};
+}
+
+int alloc_sortwork(upic_ctx* c, SortWork& w, long cap, const TileGeom& tg) {
+    int rc;
+    if ((rc = dalloc(c, &w.keys, cap))) return rc;
+    if ((rc = dalloc(c, &w.keys_alt, cap))) return rc;
+    if ((rc = dalloc(c, &w.vals, cap))) return rc;
+    if ((rc = dalloc(c, &w.vals_alt, cap))) return rc;
+    const long nblocks = (cap + 4095) / 4096;
+    const long hist = 256 * nblocks;
+    if ((rc = dalloc(c, &w.hist, hist))) return rc;
+    const long scan_blocks = (hist + 1023) / 1024 + 16;
+    if ((rc = dalloc(c, &w.scan_tmp, scan_blocks))) return rc;
+    const int ntiles = tg.ntx * tg.nty;
+    if ((rc = dalloc(c, &w.tile_count, ntiles))) return rc;
+    if ((rc = dalloc(c, &w.tile_start, ntiles))) return rc;
+    if ((rc = dalloc(c, &w.tile_chunks, ntiles))) return rc;
+    const long chunks = cap / tg.chunk + ntiles + 1;
+    if ((rc = dalloc(c, &w.chunks, chunks))) return rc;
+    if ((rc = dalloc(c, &w.nchunks, 1))) return rc;
+    w.cap = cap;
+    return 0;
+}
+
+void free_sortwork(upic_ctx* c, SortWork& w) {
+    void* ps[] = {w.keys, w.keys_alt, w.vals, w.vals_alt, w.hist, w.scan_tmp, w.tile_count,
+                  w.tile_start, w.tile_chunks, w.chunks, w.nchunks};
+    for (void* p : ps) dfree(c, p);
+    w = SortWork{};
+}
+
+// Fixed-point scale 2^F with F = 91 - ceil(log2 B) for a node-value bound B.
+double fixed_scale(double bound) {
+    if (!(bound > 0.0) || !std::isfinite(bound)) return 1.0;
+    int e = 0;
+    std::frexp(bound, &e);  // bound < 2^e
+    int F = 91 - e;  // two bits of headroom over the bound
+    if (F > 1000) F = 1000;
+    if (F < -1000) F = -1000;
+    return std::ldexp(1.0, F);
+}
+
+int sync(upic_ctx* c) {
+    UPIC_CUDA(c, cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// Split host xyz triples into three device arrays.
+__global__ void split3_kernel(const double* t, long n, double* a, double* b, double* c) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        a[i] = t[3 * i];
+        b[i] = t[3 * i + 1];
+        c[i] = t[3 * i + 2];
+    }
+}
+
+__global__ void join3_kernel(double* t, long n, const double* a, const double* b, const double* c) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        t[3 * i] = a[i];
+        t[3 * i + 1] = b[i];
+        t[3 * i + 2] = c[i];
+    }
+}
+
+__global__ void iota_kernel(int* id, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        id[i] = (int)i;
+}
+
+__global__ void interleave_kernel(const double* re, const double* im, double2* out, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        out[i] = make_double2(re[i], im ? im[i] : 0.0);
+}
+
+__global__ void deinterleave_kernel(const double2* in, double* re, double* im, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        re[i] = in[i].x;
+        if (im) im[i] = in[i].y;
+    }
+}
+
+int gridn(long n) {
+    long g = (n + 255) / 256;
+    if (g > 148 * 16) g = 148 * 16;
+    return g < 1 ? 1 : (int)g;
+}
+
+int upload3(upic_ctx* c, const double* host, long n, double* a, double* b, double* d) {
+    UPIC_CUDA(c, cudaMemcpyAsync(c->d_tmp3, host, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->st));
+    split3_kernel<<<gridn(n), 256, 0, c->st>>>(c->d_tmp3, n, a, b, d);
+    count_launches(1);
+    UPIC_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+int download3(upic_ctx* c, double* host, long n, const double* a, const double* b, const double* d) {
+    join3_kernel<<<gridn(n), 256, 0, c->st>>>(c->d_tmp3, n, a, b, d);
+    count_launches(1);
+    UPIC_CUDA(c, cudaGetLastError());
+    UPIC_CUDA(c, cudaMemcpyAsync(host, c->d_tmp3, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
+    return 0;
+}
+
+int ensure_tmp3(upic_ctx* c, long n) {
+    static_assert(sizeof(long) == 8, "64-bit long expected");
+    if (c->d_tmp3 && n <= c->cap && n <= c->kcap) return 0;
+    long want = n;
+    if (c->cap > want) want = c->cap;
+    if (c->kcap > want) want = c->kcap;
+    dfree(c, c->d_tmp3);
+    c->d_tmp3 = nullptr;
+    return dalloc(c, &c->d_tmp3, 3 * want);
+}
+
+bool is_bdf(int m) { return m == UPIC_METHOD_BDF1 || m == UPIC_METHOD_BDF2; }
+
+void bdf_coeffs(int method, int& na, double* a, int& nb, double* b) {
+    if (method == UPIC_METHOD_BDF2) {
+        na = 3;
+        a[0] = 1.5; a[1] = -2.0; a[2] = 0.5;
+    } else {
+        na = 2;
+        a[0] = 1.0; a[1] = -1.0; a[2] = 0.0;
+    }
+    nb = 2 * na - 1;
+    for (int i = 0; i < 5; ++i) b[i] = 0.0;
+    for (int i = 0; i < na; ++i)
+        for (int j = 0; j < na; ++j) b[i + j] += a[i] * a[j];
+}
+
+PushArgs push_args(upic_ctx* c, const ParticleSoA& p, long np, bool uniform) {
+    PushArgs a{};
+    a.p = p;
+    a.np = np;
+    a.q0 = c->q0;
+    a.m0 = c->m0;
+    a.Lx = c->cfg.Lx;
+    a.Ly = c->cfg.Ly;
+    a.inv_dx = 1.0 / c->dx;
+    a.inv_dy = 1.0 / c->dy;
+    a.inv_dA = 1.0 / c->dA;
+    a.dt = c->cfg.dt;
+    a.c = c->cfg.c;
+    a.gfields = c->d_gf;
+    a.acc = c->d_acc;
+    for (int k = 0; k < 4; ++k) a.scale[k] = c->scale[k];
+    (void)uniform;
+    return a;
+}
+
+// Diagnostics row of the current spectra (hist slot_new with derivatives
+// against slot_prev0) into c->h_row.
+int run_diag(upic_ctx* c, int slot_new, int slot_prev0, int na, const double* acoef) {
+    DiagKArgs d{};
+    d.N = c->N;
+    d.kx = c->d_kx;
+    d.ky = c->d_ky;
+    d.k2 = c->d_k2;
+    d.Jhat = c->d_spec;
+    d.hist = c->d_hist;
+    d.R = kHistSlots;
+    d.slot_new = slot_new;
+    d.slot_prev0 = slot_prev0;
+    d.na = na;
+    for (int k = 0; k < 3; ++k) d.a[k] = acoef[k];
+    d.dt = c->cfg.dt;
+    d.c = c->cfg.c;
+    d.eps0 = c->cfg.eps0;
+    d.out = c->d_dspec;
+    UPIC_CUDA(c, launch_diag_kspace(d, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, c->d_dspec, kDiagFields, 1, c->st, nullptr, 1, c->d_dreal));
+    DiagReduceArgs r{};
+    r.N = c->N;
+    r.dfields = c->d_dreal;
+    r.J = c->d_J;
+    r.partials = c->d_partials;
+    r.grid = kRedGrid;
+    r.pdiag = c->d_pdiag;
+    r.pcount = c->push_grid;
+    r.np = c->np;
+    r.dA = c->dA;
+    r.eps0 = c->cfg.eps0;
+    r.mu0 = c->cfg.mu0;
+    r.row = c->d_row;
+    UPIC_CUDA(c, launch_diag_reduce(r, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(c->h_row, c->d_row, sizeof(double) * UPIC_DIAG_COUNT,
+                                 cudaMemcpyDeviceToHost, c->st));
+    return 0;
+}
+
+// Sort the active particle set by the cell of wrap(x + shift v) and make the
+// sorted copy active.
+int sort_active(upic_ctx* c, double shift) {
+    ParticleSoA& src = c->P[c->cur];
+    ParticleSoA& dst = c->P[1 - c->cur];
+    UPIC_CUDA(c, sort_particles_by_tile(c->tg, src, c->np, c->cfg.Lx, c->cfg.Ly, shift, c->sw, c->st));
+    UPIC_CUDA(c, permute_particles(src, dst, c->np, c->sw, c->st));
+    c->cur = 1 - c->cur;
+    c->steps_since_sort = 0;
+    return 0;
+}
+
+int launch_push(upic_ctx* c, int mode, int ncomp, const ParticleSoA& p, long np, bool uniform,
+                const SortWork& w, double* pdiag) {
+    PushArgs a = push_args(c, p, np, uniform);
+    a.chunks = w.chunks;
+    a.nchunks = w.nchunks;
+    a.diag_part = pdiag;
+    const bool prof = c->profiling && mode == kModePush;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof) {
+        UPIC_CUDA(c, cudaEventCreate(&e0));
+        UPIC_CUDA(c, cudaEventCreate(&e1));
+        UPIC_CUDA(c, cudaEventRecord(e0, c->st));
+    }
+    UPIC_CUDA(c, launch_push_deposit(mode, ncomp, uniform, c->tg, a, c->push_grid, c->st));
+    if (prof) {
+        UPIC_CUDA(c, cudaEventRecord(e1, c->st));
+        c->prof_events.emplace_back(e0, e1);
+    }
+    return 0;
+}
+
+void clear_profile(upic_ctx* c) {
+    for (auto& e : c->prof_events) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    c->prof_events.clear();
+}
+
+int grid_ncomp(const upic_ctx* c) { return c->cfg.charge_update == UPIC_CHARGE_NAIVE ? 4 : 3; }
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int upic_abi_version(void) { return UPIC_ABI_VERSION; }
+
+int upic_config_default(upic_config* cfg) {
+    if (!cfg) return UPIC_ERR_ARGUMENT;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->nx = 32;
+    cfg->ny = 32;
+    cfg->Lx = 2.0 * kPi;
+    cfg->Ly = 2.0 * kPi;
+    cfg->dt = 0.05;
+    cfg->method = UPIC_METHOD_BDF1;
+    cfg->charge_update = UPIC_CHARGE_CONSERVING;
+    cfg->c = 1.0;
+    cfg->eps0 = 1.0;
+    cfg->mu0 = 1.0;
+    cfg->n0 = 1.0;
+    cfg->precision = UPIC_PRECISION_FP64;
+    cfg->sort_interval = 0;
+    cfg->tile = 0;
+    cfg->guard = -1;
+    return UPIC_OK;
+}
+
+const char* upic_last_error(const upic_ctx* ctx) {
+    return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+int upic_create(const upic_config* cfg, upic_ctx** out) {
+    if (!cfg || !out) return fail(nullptr, UPIC_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    // read_config validation (spectral_pic_part3.cpp:281-293)
+    if (!pow2(cfg->nx) || !pow2(cfg->ny) || cfg->nx > 8192 || cfg->ny > 8192)
+        return fail(nullptr, UPIC_ERR_CONFIG,
+                    "the radix-2 FFT requires nx and ny to be powers of two (<= 8192)");
+    if (!is_bdf(cfg->method)) return fail(nullptr, UPIC_ERR_CONFIG, "method must be bdf1 or bdf2");
+    if (cfg->charge_update != UPIC_CHARGE_CONSERVING && cfg->charge_update != UPIC_CHARGE_NAIVE)
+        return fail(nullptr, UPIC_ERR_CONFIG, "charge_update must be conserving or naive");
+    if (!(cfg->Lx > 0) || !(cfg->Ly > 0) || !(cfg->dt > 0) || !(cfg->c > 0) || !(cfg->eps0 > 0) ||
+        !(cfg->mu0 > 0))
+        return fail(nullptr, UPIC_ERR_CONFIG, "Lx, Ly, dt, c, eps0, mu0 must be positive");
+    if (cfg->precision != UPIC_PRECISION_FP64)
+        return fail(nullptr, UPIC_ERR_CONFIG, "this build supports precision = fp64 only");
+
+    upic_ctx* c = new upic_ctx();
+    c->cfg = *cfg;
+    c->nx = cfg->nx;
+    c->ny = cfg->ny;
+    c->N = cfg->nx * cfg->ny;
+    c->dx = cfg->Lx / cfg->nx;
+    c->dy = cfg->Ly / cfg->ny;
+    c->dA = c->dx * c->dy;
+    c->sort_interval = cfg->sort_interval > 0 ? cfg->sort_interval : 4;
+    const int tile = cfg->tile > 0 ? cfg->tile : 16;
+    const int guard = cfg->guard >= 0 ? cfg->guard : 3;
+    c->tg = make_tiles(c->nx, c->ny, tile, guard);
+
+    auto bail = [&](int rc) {
+        g_create_error = c->err;
+        upic_destroy(c);
+        return rc;
+    };
+    int rc;
+    if (cudaGetDevice(&c->device) != cudaSuccess)
+        return bail(fail(c, UPIC_ERR_CUDA, "no CUDA device"));
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device);
+    if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(c, UPIC_ERR_CUDA, "cudaStreamCreate failed"));
+    c->st = c->own;
+    if (fft_configure_smem() != cudaSuccess || push_configure_smem(c->tg) != cudaSuccess)
+        return bail(fail(c, UPIC_ERR_CUDA, "cudaFuncSetAttribute failed"));
+    int occ = 0;
+    // occupancy of the push kernel bounds the persistent grid
+    occ = 227 * 1024 / (push_deposit_smem_bytes(c->tg, 4) + 1024);
+    if (occ < 1) occ = 1;
+    if (occ > 8) occ = 8;
+    c->push_grid = c->nsm * occ;
+
+    const int N = c->N;
+    auto tw_x = twiddles(c->nx), tw_y = twiddles(c->ny);
+    if ((rc = dalloc(c, &c->d_twx, tw_x.size())) || (rc = dalloc(c, &c->d_twy, tw_y.size())) ||
+        (rc = dalloc(c, &c->d_kx, N)) || (rc = dalloc(c, &c->d_ky, N)) || (rc = dalloc(c, &c->d_k2, N)) ||
+        (rc = dalloc(c, &c->d_acc, 8 * (size_t)N)) || (rc = dalloc(c, &c->d_J, 3 * (size_t)N)) ||
+        (rc = dalloc(c, &c->d_rho, N)) || (rc = dalloc(c, &c->d_gf, (size_t)kGFStride * N)) ||
+        (rc = dalloc(c, &c->d_spec, 16 * (size_t)N)) ||
+        (rc = dalloc(c, &c->d_hist, 5 * (size_t)kHistSlots * N)) ||
+        (rc = dalloc(c, &c->d_dspec, (size_t)kDiagFields * N)) ||
+        (rc = dalloc(c, &c->d_dreal, (size_t)kDiagFields * N)) ||
+        (rc = dalloc(c, &c->d_partials, (size_t)kRedGrid * 16)) ||
+        (rc = dalloc(c, &c->d_pdiag, (size_t)c->push_grid * kDiagPart)) ||
+        (rc = dalloc(c, &c->d_row, UPIC_DIAG_COUNT)))
+        return bail(rc);
+    if (cudaMallocHost(&c->h_row, sizeof(double) * UPIC_DIAG_COUNT) != cudaSuccess)
+        return bail(fail(c, UPIC_ERR_NOMEM, "cudaMallocHost failed"));
+    std::vector<double> kx(N), ky(N), k2(N);
+    for (int i = 0; i < c->nx; ++i) {
+        const double kxi = 2.0 * kPi * (double)mode_number(i, c->nx) / cfg->Lx;
+        for (int j = 0; j < c->ny; ++j) {
+            const double kyj = 2.0 * kPi * (double)mode_number(j, c->ny) / cfg->Ly;
+            const int id = i * c->ny + j;
+            kx[id] = kxi;
+            ky[id] = kyj;
+            k2[id] = kxi * kxi + kyj * kyj;
+        }
+    }
+    if (cudaMemcpy(c->d_twx, tw_x.data(), sizeof(double2) * tw_x.size(), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(c->d_twy, tw_y.data(), sizeof(double2) * tw_y.size(), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(c->d_kx, kx.data(), sizeof(double) * N, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(c->d_ky, ky.data(), sizeof(double) * N, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(c->d_k2, k2.data(), sizeof(double) * N, cudaMemcpyHostToDevice) ||
+        cudaMemset(c->d_acc, 0, sizeof(unsigned long long) * 8 * (size_t)N))
+        return bail(fail(c, UPIC_ERR_CUDA, "initial device copies failed"));
+    c->plan.nx = c->nx;
+    c->plan.ny = c->ny;
+    c->plan.tw_x = c->d_twx;
+    c->plan.tw_y = c->d_twy;
+    *out = c;
+    return UPIC_OK;
+}
+
+int upic_destroy(upic_ctx* c) {
+    if (!c) return UPIC_OK;
+    if (c->st) cudaStreamSynchronize(c->st);
+    clear_profile(c);
+    for (void* p : c->allocs)
+        if (p) cudaFree(p);
+    if (c->h_row) cudaFreeHost(c->h_row);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+    return UPIC_OK;
+}
+
+int upic_set_stream(upic_ctx* c, void* stream) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    UPIC_CUDA(c, cudaStreamSynchronize(c->st));
+    c->st = stream ? reinterpret_cast<cudaStream_t>(stream) : c->own;
+    return UPIC_OK;
+}
+
+int upic_set_particles(upic_ctx* c, long np, const double* x, const double* y, const double* P,
+                       const double* v, const double* v_prev, const double* q, const double* m) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (np < 0 || np > 0x7fffffffL) return fail(c, UPIC_ERR_ARGUMENT, "particle count out of range");
+    if (np > 0 && (!x || !y || !P || !v || !v_prev || !q || !m))
+        return fail(c, UPIC_ERR_ARGUMENT, "null particle array");
+    // uniform charge/mass (the reference stores them per particle)
+    bool uniform = true;
+    double qabs = 0.0, vmax = 0.0;
+    for (long p = 0; p < np; ++p) {
+        if (q[p] != q[0] || m[p] != m[0]) uniform = false;
+        qabs += std::fabs(q[p]);
+        const double s = std::sqrt(v[3 * p] * v[3 * p] + v[3 * p + 1] * v[3 * p + 1] + v[3 * p + 2] * v[3 * p + 2]);
+        if (!std::isfinite(s) || !std::isfinite(x[p]) || !std::isfinite(y[p]))
+            return fail(c, UPIC_ERR_NONFINITE, "non-finite particle position or velocity");
+        if (s > vmax) vmax = s;
+    }
+    int rc;
+    if (np > c->cap || (!uniform && !c->P[0].q)) {
+        free_soa(c, c->P[0]);
+        free_soa(c, c->P[1]);
+        free_sortwork(c, c->sw);
+        const long cap = np > c->cap ? np : c->cap;
+        if ((rc = alloc_soa(c, c->P[0], cap, true, !uniform)) || (rc = alloc_soa(c, c->P[1], cap, true, !uniform)) ||
+            (rc = alloc_sortwork(c, c->sw, cap, c->tg)))
+            return rc;
+        c->cap = cap;
+    }
+    if ((rc = ensure_tmp3(c, np))) return rc;
+    c->np = np;
+    c->cur = 0;
+    c->uniform_qm = uniform;
+    c->q0 = np ? q[0] : 0.0;
+    c->m0 = np ? m[0] : 0.0;
+    ParticleSoA& s = c->P[0];
+    if (np > 0) {
+        UPIC_CUDA(c, cudaMemcpyAsync(s.x, x, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.y, y, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        if ((rc = upload3(c, P, np, s.Px, s.Py, s.Pz))) return rc;
+        if ((rc = upload3(c, v, np, s.vx, s.vy, s.vz))) return rc;
+        if ((rc = upload3(c, v_prev, np, s.wx, s.wy, s.wz))) return rc;
+        if (!uniform) {
+            UPIC_CUDA(c, cudaMemcpyAsync(s.q, q, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+            UPIC_CUDA(c, cudaMemcpyAsync(s.m, m, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        }
+        iota_kernel<<<gridn(np), 256, 0, c->st>>>(s.id, np);
+        count_launches(1);
+        UPIC_CUDA(c, cudaGetLastError());
+    }
+    const double vb = vmax > c->cfg.c ? vmax : c->cfg.c;
+    const double bJ = qabs * vb / c->dA;
+    c->scale[0] = c->scale[1] = c->scale[2] = fixed_scale(bJ);
+    c->scale[3] = fixed_scale(qabs / c->dA);
+    c->fields_ready = false;
+    c->steps = 0;
+    return sync(c);
+}
+
+int upic_get_particles(upic_ctx* c, long np, double* x, double* y, double* P, double* v,
+                       double* v_prev) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (np != c->np) return fail(c, UPIC_ERR_ARGUMENT, "particle count does not match the context");
+    if (np == 0) return UPIC_OK;
+    ParticleSoA& s = c->P[c->cur];
+    ParticleSoA& d = c->P[1 - c->cur];
+    UPIC_CUDA(c, unpermute_particles(s, d, np, c->st));
+    int rc;
+    if (x) UPIC_CUDA(c, cudaMemcpyAsync(x, d.x, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    if (y) UPIC_CUDA(c, cudaMemcpyAsync(y, d.y, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    if (P && (rc = download3(c, P, np, d.Px, d.Py, d.Pz))) return rc;
+    if (P) { if ((rc = sync(c))) return rc; }
+    if (v && (rc = download3(c, v, np, d.vx, d.vy, d.vz))) return rc;
+    if (v) { if ((rc = sync(c))) return rc; }
+    if (v_prev && (rc = download3(c, v_prev, np, d.wx, d.wy, d.wz))) return rc;
+    return sync(c);
+}
+
+int upic_init_fields(upic_ctx* c, double* diag_row) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (c->cap == 0 && c->np == 0) return fail(c, UPIC_ERR_STATE, "upic_set_particles first");
+    const int N = c->N;
+    int rc;
+    // rho0 = n0 + electrons, J0 (spectral_pic_part3.cpp:1102-1103)
+    if (c->np > 0) {
+        if ((rc = sort_active(c, 0.0))) return rc;
+        UPIC_CUDA(c, cudaMemsetAsync(c->d_acc, 0, sizeof(unsigned long long) * 8 * (size_t)N, c->st));
+        if ((rc = launch_push(c, kModeDeposit, 4, c->P[c->cur], c->np, c->uniform_qm, c->sw, c->d_pdiag)))
+            return rc;
+    } else {
+        UPIC_CUDA(c, cudaMemsetAsync(c->d_pdiag, 0, sizeof(double) * c->push_grid * kDiagPart, c->st));
+    }
+    UPIC_CUDA(c, launch_convert_acc(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0, 3, c->st));
+    // phi0 from Poisson (:1104, :819-827), histories (:1107-1111)
+    double2* sp = c->d_spec;
+    UPIC_CUDA(c, fft2d_batched(c->plan, sp + 3 * (size_t)N, 1, 0, c->st, c->d_rho));
+    UPIC_CUDA(c, launch_poisson_kspace(N, c->d_k2, sp + 3 * (size_t)N, c->cfg.eps0, sp + 4 * (size_t)N, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, sp + 4 * (size_t)N, 1, 1, c->st, nullptr, 1, c->d_dreal));
+    UPIC_CUDA(c, fft2d_batched(c->plan, sp + 4 * (size_t)N, 1, 0, c->st, c->d_dreal));
+    double2* H = c->d_hist;
+    const size_t fs = (size_t)kHistSlots * N;
+    UPIC_CUDA(c, launch_fill_hist(H + 0 * fs, kHistSlots, N, sp + 4 * (size_t)N, c->st));
+    UPIC_CUDA(c, cudaMemsetAsync(H + 1 * fs, 0, sizeof(double2) * 3 * fs, c->st));
+    UPIC_CUDA(c, launch_fill_hist(H + 4 * fs, kHistSlots, N, sp + 3 * (size_t)N, c->st));
+    c->head = 0;
+    // J0 spectra for the step-0 diagnostics
+    UPIC_CUDA(c, fft2d_batched(c->plan, sp, 3, 0, c->st, c->d_J));
+    if (diag_row) {
+        const double a1[3] = {1.0, -1.0, 0.0};
+        if ((rc = run_diag(c, c->head, c->head, 2, a1))) return rc;
+    }
+    // first step's current, deposited one step ahead (:1137-1141)
+    if (c->np > 0) {
+        if ((rc = sort_active(c, c->cfg.dt))) return rc;
+        if ((rc = launch_push(c, kModeAdvanceDeposit, grid_ncomp(c), c->P[c->cur], c->np, c->uniform_qm,
+                              c->sw, nullptr)))
+            return rc;
+    }
+    c->steps = 0;
+    c->fields_ready = true;
+    if ((rc = sync(c))) return rc;
+    if (diag_row) std::memcpy(diag_row, c->h_row, sizeof(double) * UPIC_DIAG_COUNT);
+    return UPIC_OK;
+}
+
+int upic_step(upic_ctx* c, int nsteps, int diag_stride, double* diag) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (!c->fields_ready) return fail(c, UPIC_ERR_STATE, "upic_init_fields first");
+    if (nsteps < 0) return fail(c, UPIC_ERR_ARGUMENT, "nsteps < 0");
+    const int N = c->N;
+    int na, nb;
+    double a[3], b[5];
+    bdf_coeffs(c->cfg.method, na, a, nb, b);
+    const bool naive = c->cfg.charge_update == UPIC_CHARGE_NAIVE;
+    double2* sp = c->d_spec;
+    int rc;
+    for (int s = 0; s < nsteps; ++s) {
+        const long step = c->steps + 1;
+        const bool want_diag = diag && diag_stride > 0 && (step % diag_stride == 0 || s == nsteps - 1);
+        if (c->np > 0 && c->steps_since_sort >= c->sort_interval) {
+            if ((rc = sort_active(c, c->cfg.dt))) return rc;
+        }
+        // J^n (and rho^n) were deposited by the previous particle kernel
+        UPIC_CUDA(c, launch_convert_acc(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0,
+                                        naive ? 3 : 1, c->st));
+        UPIC_CUDA(c, fft2d_batched(c->plan, sp, 3, 0, c->st, c->d_J));
+        if (naive) UPIC_CUDA(c, fft2d_batched(c->plan, sp + 3 * (size_t)N, 1, 0, c->st, c->d_rho));
+        KspaceArgs k{};
+        k.N = N;
+        k.kx = c->d_kx;
+        k.ky = c->d_ky;
+        k.k2 = c->d_k2;
+        k.Jhat = sp;
+        k.rho_dep = naive ? sp + 3 * (size_t)N : nullptr;
+        k.hist = c->d_hist;
+        k.R = kHistSlots;
+        k.head = c->head;
+        k.na = na;
+        k.nb = nb;
+        for (int i = 0; i < 3; ++i) k.a[i] = a[i];
+        for (int i = 0; i < 5; ++i) k.b[i] = b[i];
+        k.dt = c->cfg.dt;
+        k.c = c->cfg.c;
+        k.eps0 = c->cfg.eps0;
+        k.mu0 = c->cfg.mu0;
+        k.conserving = naive ? 0 : 1;
+        k.gspec = sp + 4 * (size_t)N;
+        UPIC_CUDA(c, launch_bdf_kspace(k, c->st));
+        UPIC_CUDA(c, fft2d_batched(c->plan, sp + 4 * (size_t)N, kGF, 1, c->st, nullptr, 2, c->d_gf,
+                                   kGFStride, 0));
+        if (c->np > 0) {
+            if ((rc = launch_push(c, kModePush, grid_ncomp(c), c->P[c->cur], c->np, c->uniform_qm, c->sw,
+                                  c->d_pdiag)))
+                return rc;
+        } else {
+            UPIC_CUDA(c, cudaMemsetAsync(c->d_pdiag, 0, sizeof(double) * c->push_grid * kDiagPart, c->st));
+        }
+        const int snew = (c->head + kHistSlots - 1) % kHistSlots;
+        if (want_diag) {
+            if ((rc = run_diag(c, snew, c->head, na, a))) return rc;
+            if ((rc = sync(c))) return rc;
+            std::memcpy(diag + (size_t)s * UPIC_DIAG_COUNT, c->h_row, sizeof(double) * UPIC_DIAG_COUNT);
+        } else if (diag) {
+            for (int i = 0; i < UPIC_DIAG_COUNT; ++i) diag[(size_t)s * UPIC_DIAG_COUNT + i] = NAN;
+        }
+        c->head = snew;
+        c->steps = step;
+        c->steps_since_sort++;
+    }
+    return sync(c);
+}
+
+int upic_profile_enable(upic_ctx* c, int on) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    UPIC_CUDA(c, cudaStreamSynchronize(c->st));
+    clear_profile(c);
+    c->profiling = on != 0;
+    return UPIC_OK;
+}
+
+int upic_profile_read(upic_ctx* c, double* push_ms, long* push_launches, long* kernel_launches) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    UPIC_CUDA(c, cudaStreamSynchronize(c->st));
+    double total = 0.0;
+    for (auto& e : c->prof_events) {
+        float ms = 0.0f;
+        UPIC_CUDA(c, cudaEventElapsedTime(&ms, e.first, e.second));
+        total += ms;
+    }
+    if (push_ms) *push_ms = total;
+    if (push_launches) *push_launches = (long)c->prof_events.size();
+    if (kernel_launches) *kernel_launches = launches_total();
+    return UPIC_OK;
+}
+
+int upic_step_count(const upic_ctx* c, long* steps) {
+    if (!c || !steps) return UPIC_ERR_ARGUMENT;
+    *steps = c->steps;
+    return UPIC_OK;
+}
+
+int upic_get_field(upic_ctx* c, int which, double* host) {
+    if (!c || !host) return UPIC_ERR_ARGUMENT;
+    if (!c->fields_ready) return fail(c, UPIC_ERR_STATE, "upic_init_fields first");
+    const int N = c->N;
+    if (which >= UPIC_FIELD_JX && which <= UPIC_FIELD_JZ) {
+        UPIC_CUDA(c, cudaMemcpyAsync(host, c->d_J + (size_t)(which - UPIC_FIELD_JX) * N, sizeof(double) * N,
+                                     cudaMemcpyDeviceToHost, c->st));
+        return sync(c);
+    }
+    if (which < 0 || which > UPIC_FIELD_RHO) return fail(c, UPIC_ERR_ARGUMENT, "unknown field");
+    const int f = which;  // phi 0, A 1..3, rho 4 share the history field index
+    const double2* src = c->d_hist + ((size_t)f * kHistSlots + c->head) * N;
+    double2* tmp = c->d_dspec;
+    UPIC_CUDA(c, cudaMemcpyAsync(tmp, src, sizeof(double2) * N, cudaMemcpyDeviceToDevice, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, tmp, 1, 1, c->st, nullptr, 1, c->d_dreal));
+    UPIC_CUDA(c, cudaMemcpyAsync(host, c->d_dreal, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+
+// ---- kernel-level entry points --------------------------------------------
+namespace {
+
+int ensure_kparticles(upic_ctx* c, long np) {
+    if (np <= c->kcap) return 0;
+    free_soa(c, c->K[0]);
+    free_soa(c, c->K[1]);
+    free_sortwork(c, c->ksw);
+    int rc;
+    if ((rc = alloc_soa(c, c->K[0], np, false, true)) || (rc = alloc_soa(c, c->K[1], np, false, true)) ||
+        (rc = alloc_sortwork(c, c->ksw, np, c->tg)))
+        return rc;
+    c->kcap = np;
+    return ensure_tmp3(c, np);
+}
+
+// Upload (x, y, v, q), sort, deposit with ncomp (1 charge, 3 current).
+int kernel_deposit(upic_ctx* c, long np, const double* x, const double* y, const double* v,
+                   const double* q, int ncomp) {
+    int rc;
+    if ((rc = ensure_kparticles(c, np))) return rc;
+    const int N = c->N;
+    ParticleSoA& s = c->K[0];
+    double qabs = 0.0, vmax = 0.0;
+    for (long p = 0; p < np; ++p) {
+        qabs += std::fabs(q[p]);
+        if (v) {
+            const double sp = std::sqrt(v[3 * p] * v[3 * p] + v[3 * p + 1] * v[3 * p + 1] +
+                                        v[3 * p + 2] * v[3 * p + 2]);
+            if (sp > vmax) vmax = sp;
+        }
+    }
+    double scale[4];
+    scale[0] = scale[1] = scale[2] = fixed_scale(qabs * vmax / c->dA);
+    scale[3] = fixed_scale(qabs / c->dA);
+    UPIC_CUDA(c, cudaMemsetAsync(c->d_acc, 0, sizeof(unsigned long long) * 8 * (size_t)N, c->st));
+    if (np > 0) {
+        UPIC_CUDA(c, cudaMemcpyAsync(s.x, x, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.y, y, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.q, q, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        if (v) {
+            if ((rc = upload3(c, v, np, s.vx, s.vy, s.vz))) return rc;
+        } else {
+            UPIC_CUDA(c, cudaMemsetAsync(s.vx, 0, sizeof(double) * np, c->st));
+            UPIC_CUDA(c, cudaMemsetAsync(s.vy, 0, sizeof(double) * np, c->st));
+            UPIC_CUDA(c, cudaMemsetAsync(s.vz, 0, sizeof(double) * np, c->st));
+        }
+        iota_kernel<<<gridn(np), 256, 0, c->st>>>(s.id, np);
+        count_launches(1);
+        UPIC_CUDA(c, sort_particles_by_tile(c->tg, s, np, c->cfg.Lx, c->cfg.Ly, 0.0, c->ksw, c->st));
+        UPIC_CUDA(c, permute_particles(s, c->K[1], np, c->ksw, c->st));
+        PushArgs a = push_args(c, c->K[1], np, false);
+        for (int k = 0; k < 4; ++k) a.scale[k] = scale[k];
+        a.m0 = 1.0;
+        a.c = c->cfg.c;
+        a.chunks = c->ksw.chunks;
+        a.nchunks = c->ksw.nchunks;
+        a.diag_part = nullptr;
+        UPIC_CUDA(c, launch_push_deposit(kModeDeposit, ncomp, false, c->tg, a, c->push_grid, c->st));
+    }
+    UPIC_CUDA(c, launch_convert_acc(c->d_acc, N, scale, c->d_J, c->d_rho, c->cfg.n0,
+                                    ncomp == 1 ? 2 : 1, c->st));
+    return 0;
+}
+
+}  // namespace
+
+int upic_deposit_current(upic_ctx* c, long np, const double* x, const double* y, const double* v,
+                         const double* q, double* J) {
+    if (!c || !J || np < 0 || (np > 0 && (!x || !y || !v || !q))) return UPIC_ERR_ARGUMENT;
+    int rc = kernel_deposit(c, np, x, y, v, q, 3);
+    if (rc) return rc;
+    UPIC_CUDA(c, cudaMemcpyAsync(J, c->d_J, sizeof(double) * 3 * (size_t)c->N, cudaMemcpyDeviceToHost, c->st));
+    c->fields_ready = false;
+    return sync(c);
+}
+
+int upic_deposit_charge(upic_ctx* c, long np, const double* x, const double* y, const double* q,
+                        double* rho) {
+    if (!c || !rho || np < 0 || (np > 0 && (!x || !y || !q))) return UPIC_ERR_ARGUMENT;
+    int rc = kernel_deposit(c, np, x, y, nullptr, q, 1);
+    if (rc) return rc;
+    UPIC_CUDA(c, cudaMemcpyAsync(rho, c->d_rho, sizeof(double) * (size_t)c->N, cudaMemcpyDeviceToHost, c->st));
+    c->fields_ready = false;
+    return sync(c);
+}
+
+int upic_gather(upic_ctx* c, const double* f, long np, const double* x, const double* y, double* out) {
+    if (!c || !f || !out || np < 0 || (np > 0 && (!x || !y))) return UPIC_ERR_ARGUMENT;
+    int rc;
+    if ((rc = ensure_kparticles(c, np))) return rc;
+    double* df = c->d_dreal;
+    UPIC_CUDA(c, cudaMemcpyAsync(df, f, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+    if (np > 0) {
+        UPIC_CUDA(c, cudaMemcpyAsync(c->K[0].x, x, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(c->K[0].y, y, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, launch_gather_scalar(c->nx, c->ny, 1.0 / c->dx, 1.0 / c->dy, df, np, c->K[0].x,
+                                          c->K[0].y, c->K[0].vx, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(out, c->K[0].vx, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    }
+    return sync(c);
+}
+
+int upic_fft2d(upic_ctx* c, double* re, double* im, int inverse) {
+    if (!c || !re || !im) return UPIC_ERR_ARGUMENT;
+    const long N = c->N;
+    UPIC_CUDA(c, cudaMemcpyAsync(c->d_dreal, re, sizeof(double) * N, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(c->d_dreal + N, im, sizeof(double) * N, cudaMemcpyHostToDevice, c->st));
+    interleave_kernel<<<gridn(N), 256, 0, c->st>>>(c->d_dreal, c->d_dreal + N, c->d_dspec, N);
+    count_launches(1);
+    UPIC_CUDA(c, fft2d_batched(c->plan, c->d_dspec, 1, inverse ? 1 : 0, c->st));
+    deinterleave_kernel<<<gridn(N), 256, 0, c->st>>>(c->d_dspec, c->d_dreal, c->d_dreal + N, N);
+    count_launches(1);
+    UPIC_CUDA(c, cudaMemcpyAsync(re, c->d_dreal, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(im, c->d_dreal + N, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+
+int upic_spectral_derivative(upic_ctx* c, const double* f, int dir, double* out) {
+    if (!c || !f || !out || (dir != 0 && dir != 1)) return UPIC_ERR_ARGUMENT;
+    const long N = c->N;
+    UPIC_CUDA(c, cudaMemcpyAsync(c->d_dreal, f, sizeof(double) * N, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, c->d_dspec, 1, 0, c->st, c->d_dreal));
+    UPIC_CUDA(c, launch_derivative_kspace(N, dir == 0 ? c->d_kx : c->d_ky, c->d_dspec, c->d_dspec + N, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, c->d_dspec + N, 1, 1, c->st, nullptr, 1, c->d_dreal));
+    UPIC_CUDA(c, cudaMemcpyAsync(out, c->d_dreal, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+
+int upic_poisson(upic_ctx* c, const double* rho, double* phi) {
+    if (!c || !rho || !phi) return UPIC_ERR_ARGUMENT;
+    const long N = c->N;
+    UPIC_CUDA(c, cudaMemcpyAsync(c->d_dreal, rho, sizeof(double) * N, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, c->d_dspec, 1, 0, c->st, c->d_dreal));
+    UPIC_CUDA(c, launch_poisson_kspace(N, c->d_k2, c->d_dspec, c->cfg.eps0, c->d_dspec + N, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, c->d_dspec + N, 1, 1, c->st, nullptr, 1, c->d_dreal));
+    UPIC_CUDA(c, cudaMemcpyAsync(phi, c->d_dreal, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+
+int upic_solve_bdf(upic_ctx* c, const double* source, const double* hist, double* out) {
+    if (!c || !source || !hist || !out) return UPIC_ERR_ARGUMENT;
+    const long N = c->N;
+    int na, nb;
+    double a[3], b[5];
+    bdf_coeffs(c->cfg.method, na, a, nb, b);
+    const int nh = nb - 1;
+    UPIC_CUDA(c, cudaMemcpyAsync(c->d_dreal, source, sizeof(double) * N, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(c->d_dreal + N, hist, sizeof(double) * N * nh, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, c->d_dspec, 1 + nh, 0, c->st, c->d_dreal));
+    const double scale = 1.0 / (c->cfg.c * c->cfg.c * c->cfg.dt * c->cfg.dt);
+    UPIC_CUDA(c, launch_bdf_single(N, c->d_k2, c->d_dspec, c->d_dspec + N, nb, b, scale,
+                                   c->d_dspec + (size_t)(1 + nh) * N, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, c->d_dspec + (size_t)(1 + nh) * N, 1, 1, c->st, nullptr, 1, c->d_dreal));
+    UPIC_CUDA(c, cudaMemcpyAsync(out, c->d_dreal, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+
+}  // extern "C"

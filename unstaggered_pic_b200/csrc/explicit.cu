@@ -1,0 +1,731 @@
+// Explicit spectral BDF / IAEM step kernels (sm_100a).
+//
+// Reference: Project2/spectral_pic_part3.cpp (run_simulation :1094-1189).
+// One step of the reference is
+//   x += dt v; J = deposit(x, v); rho (continuity or redeposit); BDF wave
+//   solves for phi, A; spectral grad phi, grad A; IAEM push; diagnostics.
+// Here the particle work of a step is one fused kernel (push_deposit_kernel,
+// kModePush): it recomputes x^n = wrap(x^{n-1} + dt v^{n-1}), gathers the
+// eleven field records at x^n, pushes P and v, stores the step-n state, and
+// already deposits the NEXT step's current J^{n+1} at wrap(x^n + dt v^n) with
+// v^n (what the reference's next iteration deposits).  The field work of a
+// step is a handful of grid kernels in k-space (histories kept as spectra).
+#include "kernels.h"
+#include "upic_common.cuh"
+
+namespace upic {
+
+namespace {
+
+constexpr int kPushThreads = 256;
+constexpr int kPushWarps = kPushThreads / kWarp;
+constexpr int kKeyNone = -1;
+constexpr int kKeyEscape = -2;
+
+// Per-warp staging of 32 particles: 9 tensor-product weights and up to 4
+// deposit values per particle, plus window key and global stencil origin.
+template <int NCOMP>
+struct StageLayout {
+    static constexpr int kDoubles = 32 * (9 + NCOMP);
+    static constexpr int kInts = 32 * 3;
+};
+
+UPIC_D int acc_slot(int ncomp, int c) { return ncomp == 1 ? 3 : c; }
+
+// Window-local coordinate of a stencil origin node (tiled axis): -1 when the
+// three-node stencil does not fit in the window.
+UPIC_D int window_coord(int s, int origin, int n, int w) {
+    int d = (s - origin) % n;
+    if (d < 0) d += n;
+    return d <= w - 3 ? d : -1;
+}
+
+template <int MODE, int NCOMP, bool UNIFORM>
+__global__ void __launch_bounds__(kPushThreads)
+push_deposit_kernel(PushArgs a, TileGeom tg) {
+    extern __shared__ unsigned long long smem_u64[];
+    const int WN = tg.wx * tg.wy;
+    unsigned long long* whi = smem_u64;
+    unsigned long long* wlo = whi + NCOMP * WN;
+    double* sd = reinterpret_cast<double*>(wlo + NCOMP * WN);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* swab = sd + warp * StageLayout<NCOMP>::kDoubles;  // [32][9]
+    double* sval = swab + 32 * 9;                              // [32][NCOMP]
+    int* si = reinterpret_cast<int*>(sd + kPushWarps * StageLayout<NCOMP>::kDoubles);
+    int* skey = si + warp * StageLayout<NCOMP>::kInts;
+    int* sgx = skey + 32;
+    int* sgy = skey + 64;
+
+    const int nx = tg.nx, ny = tg.ny;
+    const int N = nx * ny;
+    const int nch = *a.nchunks;
+    const int c_begin = (int)(((long long)blockIdx.x * nch) / gridDim.x);
+    const int c_end = (int)(((long long)(blockIdx.x + 1) * nch) / gridDim.x);
+
+    DD kin{0.0, 0.0}, gsum{0.0, 0.0};
+    double vmax = 0.0;
+    const double c2 = a.c * a.c;
+
+    int cur_tile = -1, ox = 0, oy = 0;
+    for (int ci = c_begin; ci < c_end; ++ci) {
+        const Chunk ch = a.chunks[ci];
+        if (ch.tile != cur_tile) {
+            __syncthreads();
+            if (cur_tile >= 0) {
+                // fold the finished window into the global accumulators
+                for (int idx = threadIdx.x; idx < NCOMP * WN; idx += blockDim.x) {
+                    const unsigned long long hi = whi[idx], lo = wlo[idx];
+                    if ((hi | lo) == 0ull) continue;
+                    const int cc = idx / WN, widx = idx - cc * WN;
+                    const int lx = widx / tg.wy, ly = widx - lx * tg.wy;
+                    const int gx = tg.full_x ? lx : wrap_index(ox + lx, nx);
+                    const int gy = tg.full_y ? ly : wrap_index(oy + ly, ny);
+                    const int sl = acc_slot(NCOMP, cc);
+                    atomicAdd(&a.acc[(size_t)(2 * sl) * N + gx * ny + gy], hi);
+                    atomicAdd(&a.acc[(size_t)(2 * sl + 1) * N + gx * ny + gy], lo);
+                }
+                __syncthreads();
+            }
+            for (int idx = threadIdx.x; idx < 2 * NCOMP * WN; idx += blockDim.x) whi[idx] = 0ull;
+            cur_tile = ch.tile;
+            const int tx = cur_tile / tg.nty, ty = cur_tile - tx * tg.nty;
+            ox = tg.full_x ? 0 : tx * tg.tile_x - tg.guard - 1;
+            oy = tg.full_y ? 0 : ty * tg.tile_y - tg.guard - 1;
+            __syncthreads();
+        }
+        for (int base = ch.start; base < ch.end; base += kPushThreads) {
+            const int p = base + threadIdx.x;
+            int key = kKeyNone, gx0 = 0, gy0 = 0;
+            double wab[9];
+            double val[NCOMP];
+            if (p < ch.end) {
+                const double q = UNIFORM ? a.q0 : a.p.q[p];
+                double x = a.p.x[p], y = a.p.y[p];
+                double v0 = a.p.vx[p], v1 = a.p.vy[p], v2 = a.p.vz[p];
+                if (MODE == kModePush) {
+                    // spectral_pic_part3.cpp:1050-1055: x^n = x^{n-1} + dt v^{n-1}
+                    x = wrap_periodic(x + a.dt * v0, a.Lx);
+                    y = wrap_periodic(y + a.dt * v1, a.Ly);
+                    // gather A, grad phi, grad A at x^n (:1063-1078)
+                    const Quad1D qx = quadratic_weights(x, a.inv_dx);
+                    const Quad1D qy = quadratic_weights(y, a.inv_dy);
+                    const double wxs[3] = {qx.w0, qx.w1, qx.w2};
+                    const double wys[3] = {qy.w0, qy.w1, qy.w2};
+                    double G[12];
+#pragma unroll
+                    for (int f = 0; f < 12; ++f) G[f] = 0.0;
+#pragma unroll
+                    for (int ia = 0; ia < 3; ++ia) {
+                        const int gx = wrap_index(qx.ic - 1 + ia, nx);
+#pragma unroll
+                        for (int ib = 0; ib < 3; ++ib) {
+                            const int gy = wrap_index(qy.ic - 1 + ib, ny);
+                            const double w = wxs[ia] * wys[ib];
+                            const double2* rec = reinterpret_cast<const double2*>(
+                                a.gfields + (size_t)(gx * ny + gy) * kGFStride);
+#pragma unroll
+                            for (int f2 = 0; f2 < kGFStride / 2; ++f2) {
+                                const double2 r = __ldg(rec + f2);
+                                G[2 * f2] = fma(r.x, w, G[2 * f2]);
+                                G[2 * f2 + 1] = fma(r.y, w, G[2 * f2 + 1]);
+                            }
+                        }
+                    }
+                    // IAEM momentum update (:1072-1090)
+                    const double w0 = a.p.wx[p], w1 = a.p.wy[p], w2 = a.p.wz[p];
+                    const double vs0 = 2.0 * v0 - w0, vs1 = 2.0 * v1 - w1, vs2 = 2.0 * v2 - w2;
+                    const double gdx = G[5] * vs0 + G[7] * vs1 + G[9] * vs2;
+                    const double gdy = G[6] * vs0 + G[8] * vs1 + G[10] * vs2;
+                    const double qdt = q * a.dt;
+                    const double P0 = a.p.Px[p] + qdt * (gdx - G[3]);
+                    const double P1 = a.p.Py[p] + qdt * (gdy - G[4]);
+                    const double P2 = a.p.Pz[p];
+                    // velocity_from_canonical (:602-607)
+                    const double p0 = P0 - q * G[0], p1 = P1 - q * G[1], p2 = P2 - q * G[2];
+                    const double m = UNIFORM ? a.m0 : a.p.m[p];
+                    const double mc2 = m * c2;
+                    const double denom = sqrt(c2 * (p0 * p0 + p1 * p1 + p2 * p2) + mc2 * mc2);
+                    const double s = denom == 0.0 ? 0.0 : c2 / denom;
+                    const double n0v = s * p0, n1v = s * p1, n2v = s * p2;
+                    a.p.x[p] = x;
+                    a.p.y[p] = y;
+                    a.p.Px[p] = P0;
+                    a.p.Py[p] = P1;
+                    a.p.wx[p] = v0;
+                    a.p.wy[p] = v1;
+                    a.p.wz[p] = v2;
+                    a.p.vx[p] = n0v;
+                    a.p.vy[p] = n1v;
+                    a.p.vz[p] = n2v;
+                    v0 = n0v;
+                    v1 = n1v;
+                    v2 = n2v;
+                }
+                // particle diagnostics on the (new) velocity (:950-957)
+                if (a.diag_part) {
+                    const double m = UNIFORM ? a.m0 : a.p.m[p];
+                    const double sp2 = v0 * v0 + v1 * v1 + v2 * v2;
+                    const double one_m = 1.0 - sp2 / c2;
+                    const double gam = 1.0 / sqrt(one_m > 1.0e-14 ? one_m : 1.0e-14);
+                    gsum = dd_add(gsum, gam);
+                    kin = dd_add(kin, (gam - 1.0) * m * a.c * a.c);
+                    vmax = fmax(vmax, sqrt(sp2));
+                }
+                // deposit position: stored x (kModeDeposit) or one step ahead
+                if (MODE != kModeDeposit) {
+                    x = wrap_periodic(x + a.dt * v0, a.Lx);
+                    y = wrap_periodic(y + a.dt * v1, a.Ly);
+                }
+                const Quad1D dx_ = quadratic_weights(x, a.inv_dx);
+                const Quad1D dy_ = quadratic_weights(y, a.inv_dy);
+                const double wxs[3] = {dx_.w0, dx_.w1, dx_.w2};
+                const double wys[3] = {dy_.w0, dy_.w1, dy_.w2};
+#pragma unroll
+                for (int ia = 0; ia < 3; ++ia)
+#pragma unroll
+                    for (int ib = 0; ib < 3; ++ib) wab[ia * 3 + ib] = wxs[ia] * wys[ib];
+                const double qa = q * a.inv_dA;
+                if (NCOMP == 1) {
+                    val[0] = qa;
+                } else {
+                    val[0] = qa * v0;
+                    val[1] = qa * v1;
+                    val[2] = qa * v2;
+                    if (NCOMP == 4) val[NCOMP - 1] = qa;
+                }
+                gx0 = wrap_index(dx_.ic - 1, nx);
+                gy0 = wrap_index(dy_.ic - 1, ny);
+                const int lx = tg.full_x ? gx0 : window_coord(dx_.ic - 1, ox, nx, tg.wx);
+                const int ly = tg.full_y ? gy0 : window_coord(dy_.ic - 1, oy, ny, tg.wy);
+                key = (lx < 0 || ly < 0) ? kKeyEscape : lx * tg.wy + ly;
+            }
+            // stage
+            skey[lane] = key;
+            sgx[lane] = gx0;
+            sgy[lane] = gy0;
+            if (key != kKeyNone) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) swab[lane * 9 + k] = wab[k];
+#pragma unroll
+                for (int k = 0; k < NCOMP; ++k) sval[lane * NCOMP + k] = val[k];
+            }
+            __syncwarp();
+            // Warp-level segmented reduction: lane t owns value t (node ab, comp c)
+            // and sums it over runs of particles with the same window key, in
+            // particle order; each run end flushes one fixed-point add per value.
+            constexpr int NV = 9 * NCOMP;
+            constexpr int NPER = (NV + 31) / 32;
+            double run[NPER];
+#pragma unroll
+            for (int r = 0; r < NPER; ++r) run[r] = 0.0;
+            int cur = kKeyNone;
+            auto flush = [&](int k) {
+                const int lx = k / tg.wy, ly = k - (k / tg.wy) * tg.wy;
+#pragma unroll
+                for (int r = 0; r < NPER; ++r) {
+                    const int t = lane + 32 * r;
+                    if (t < NV && run[r] != 0.0) {
+                        const int ab = t / NCOMP, cc = t - ab * NCOMP;
+                        int nxl = lx + ab / 3, nyl = ly + ab % 3;
+                        if (tg.full_x) nxl %= tg.wx;
+                        if (tg.full_y) nyl %= tg.wy;
+                        const Fixed2 f = to_fixed(run[r], a.scale[acc_slot(NCOMP, cc)]);
+                        const int widx = cc * WN + nxl * tg.wy + nyl;
+                        atomicAdd(&whi[widx], f.hi);
+                        atomicAdd(&wlo[widx], f.lo);
+                    }
+                    run[r] = 0.0;
+                }
+            };
+            for (int j = 0; j < 32; ++j) {
+                const int k = skey[j];
+                if (k == kKeyNone) break;  // inactive lanes are trailing
+                if (k != cur) {
+                    if (cur >= 0) flush(cur);
+                    cur = k;
+                }
+                if (k == kKeyEscape) {
+                    // outside the window: exact fixed-point adds straight to the grid
+#pragma unroll
+                    for (int r = 0; r < NPER; ++r) {
+                        const int t = lane + 32 * r;
+                        if (t < NV) {
+                            const int ab = t / NCOMP, cc = t - ab * NCOMP;
+                            const double v = sval[j * NCOMP + cc] * swab[j * 9 + ab];
+                            if (v != 0.0) {
+                                const int gx = wrap_index(sgx[j] + ab / 3, nx);
+                                const int gy = wrap_index(sgy[j] + ab % 3, ny);
+                                const int sl = acc_slot(NCOMP, cc);
+                                const Fixed2 f = to_fixed(v, a.scale[sl]);
+                                atomicAdd(&a.acc[(size_t)(2 * sl) * N + gx * ny + gy], f.hi);
+                                atomicAdd(&a.acc[(size_t)(2 * sl + 1) * N + gx * ny + gy], f.lo);
+                            }
+                        }
+                    }
+                    continue;
+                }
+#pragma unroll
+                for (int r = 0; r < NPER; ++r) {
+                    const int t = lane + 32 * r;
+                    if (t < NV) {
+                        const int ab = t / NCOMP, cc = t - ab * NCOMP;
+                        run[r] = fma(sval[j * NCOMP + cc], swab[j * 9 + ab], run[r]);
+                    }
+                }
+            }
+            if (cur >= 0) flush(cur);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    if (cur_tile >= 0) {
+        for (int idx = threadIdx.x; idx < NCOMP * WN; idx += blockDim.x) {
+            const unsigned long long hi = whi[idx], lo = wlo[idx];
+            if ((hi | lo) == 0ull) continue;
+            const int cc = idx / WN, widx = idx - cc * WN;
+            const int lx = widx / tg.wy, ly = widx - lx * tg.wy;
+            const int gx = tg.full_x ? lx : wrap_index(ox + lx, nx);
+            const int gy = tg.full_y ? ly : wrap_index(oy + ly, ny);
+            const int sl = acc_slot(NCOMP, cc);
+            atomicAdd(&a.acc[(size_t)(2 * sl) * N + gx * ny + gy], hi);
+            atomicAdd(&a.acc[(size_t)(2 * sl + 1) * N + gx * ny + gy], lo);
+        }
+    }
+    // particle reductions: fixed order (lanes, then warps in index order)
+    if (a.diag_part) {
+        kin = warp_sum_dd(kin);
+        gsum = warp_sum_dd(gsum);
+        vmax = warp_max(vmax);
+        __syncthreads();
+        double* red = reinterpret_cast<double*>(smem_u64);
+        if (lane == 0) {
+            red[warp * 5 + 0] = kin.hi;
+            red[warp * 5 + 1] = kin.lo;
+            red[warp * 5 + 2] = gsum.hi;
+            red[warp * 5 + 3] = gsum.lo;
+            red[warp * 5 + 4] = vmax;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            DD k{0.0, 0.0}, g{0.0, 0.0};
+            double vm = 0.0;
+            for (int w = 0; w < kPushWarps; ++w) {
+                k = dd_add_dd(k, DD{red[w * 5 + 0], red[w * 5 + 1]});
+                g = dd_add_dd(g, DD{red[w * 5 + 2], red[w * 5 + 3]});
+                vm = fmax(vm, red[w * 5 + 4]);
+            }
+            double* out = a.diag_part + (size_t)blockIdx.x * kDiagPart;
+            out[0] = k.hi;
+            out[1] = k.lo;
+            out[2] = g.hi;
+            out[3] = g.lo;
+            out[4] = vm;
+        }
+    }
+}
+
+// acc -> doubles, then clear (kept on device for the next deposit).
+__global__ void convert_acc_kernel(unsigned long long* acc, int N, double s0, double s1, double s2,
+                                   double s3, double* J, double* rho, double n0, int mask) {
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        if (mask & 1) {
+            const double sc[3] = {s0, s1, s2};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                unsigned long long* h = acc + (size_t)(2 * c) * N;
+                unsigned long long* l = acc + (size_t)(2 * c + 1) * N;
+                J[(size_t)c * N + id] = from_fixed(h[id], l[id], 1.0 / sc[c]);
+                h[id] = 0ull;
+                l[id] = 0ull;
+            }
+        }
+        if (mask & 2) {
+            unsigned long long* h = acc + (size_t)6 * N;
+            unsigned long long* l = acc + (size_t)7 * N;
+            rho[id] = n0 + from_fixed(h[id], l[id], 1.0 / s3);
+            h[id] = 0ull;
+            l[id] = 0ull;
+        }
+    }
+}
+
+UPIC_D double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+UPIC_D double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+UPIC_D double2 cscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+// i*k*z
+UPIC_D double2 cik(double k, double2 z) { return make_double2(-k * z.y, k * z.x); }
+
+// k-space BDF step: continuity / naive charge, BDF Helmholtz solves for phi
+// and A (spectral_pic_part3.cpp:829-880, 1147-1164), spectra of the eleven
+// gathered fields (:1166-1168).
+__global__ void bdf_kspace_kernel(KspaceArgs a) {
+    const int N = a.N;
+    const double scale = 1.0 / (a.c * a.c * a.dt * a.dt);
+    const int snew = (a.head + a.R - 1) % a.R;
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        const double kx = a.kx[id], ky = a.ky[id];
+        const double denom = scale * a.b[0] + a.k2[id];
+        const double2 J0 = a.Jhat[id], J1 = a.Jhat[N + id], J2 = a.Jhat[2 * (size_t)N + id];
+        auto H = [&](int field, int past) -> double2 {
+            const int slot = (a.head + past) % a.R;
+            return a.hist[((size_t)field * a.R + slot) * N + id];
+        };
+        double2 rho_new;
+        if (a.conserving) {
+            const double2 div = cik(1.0, make_double2(kx * J0.x + ky * J1.x, kx * J0.y + ky * J1.y));
+            double2 hs = make_double2(0.0, 0.0);
+            for (int l = 1; l < a.na; ++l) hs = cadd(hs, cscale(a.a[l], H(4, l - 1)));
+            const double2 num = cadd(cscale(a.dt, div), hs);
+            rho_new = make_double2(-num.x / a.a[0], -num.y / a.a[0]);
+        } else {
+            rho_new = a.rho_dep[id];
+        }
+        // phi: (b0 s + k^2) phi = rho/eps0 - s sum b_l phi^{n+1-l}
+        double2 rhs = make_double2(rho_new.x / a.eps0, rho_new.y / a.eps0);
+        for (int l = 1; l < a.nb; ++l) rhs = csub(rhs, cscale(scale * a.b[l], H(0, l - 1)));
+        const double2 phi = make_double2(rhs.x / denom, rhs.y / denom);
+        double2 A[3];
+        const double2 J[3] = {J0, J1, J2};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double2 r = cscale(a.mu0, J[c]);
+            for (int l = 1; l < a.nb; ++l) r = csub(r, cscale(scale * a.b[l], H(1 + c, l - 1)));
+            A[c] = make_double2(r.x / denom, r.y / denom);
+        }
+        a.hist[((size_t)0 * a.R + snew) * N + id] = phi;
+        for (int c = 0; c < 3; ++c) a.hist[((size_t)(1 + c) * a.R + snew) * N + id] = A[c];
+        a.hist[((size_t)4 * a.R + snew) * N + id] = rho_new;
+        if (a.gspec) {
+            double2* g = a.gspec;
+            g[0 * (size_t)N + id] = A[0];
+            g[1 * (size_t)N + id] = A[1];
+            g[2 * (size_t)N + id] = A[2];
+            g[3 * (size_t)N + id] = cik(kx, phi);
+            g[4 * (size_t)N + id] = cik(ky, phi);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                g[(5 + 2 * c) * (size_t)N + id] = cik(kx, A[c]);
+                g[(6 + 2 * c) * (size_t)N + id] = cik(ky, A[c]);
+            }
+        }
+    }
+}
+
+// Diagnostics spectra (spectral_pic_part3.cpp:902-948): gauge, E, gauss,
+// continuity, B = curl A, rho, using BDF first derivatives of the histories.
+__global__ void diag_kspace_kernel(DiagKArgs a) {
+    const int N = a.N;
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        const double kx = a.kx[id], ky = a.ky[id];
+        auto H = [&](int field, int slot) -> double2 {
+            return a.hist[((size_t)field * a.R + slot) * N + id];
+        };
+        auto ddt = [&](int field) -> double2 {
+            double2 r = cscale(a.a[0], H(field, a.slot_new));
+            for (int l = 1; l < a.na; ++l) r = cadd(r, cscale(a.a[l], H(field, (a.slot_prev0 + l - 1) % a.R)));
+            return make_double2(r.x / a.dt, r.y / a.dt);
+        };
+        const double2 phi = H(0, a.slot_new);
+        const double2 Ax = H(1, a.slot_new), Ay = H(2, a.slot_new), Az = H(3, a.slot_new);
+        const double2 rho = H(4, a.slot_new);
+        const double2 phit = ddt(0);
+        const double2 divA = cik(1.0, make_double2(kx * Ax.x + ky * Ay.x, kx * Ax.y + ky * Ay.y));
+        const double c2 = a.c * a.c;
+        const double2 gauge = cadd(make_double2(phit.x / c2, phit.y / c2), divA);
+        const double2 Atx = ddt(1), Aty = ddt(2), Atz = ddt(3);
+        const double2 gpx = cik(kx, phi), gpy = cik(ky, phi);
+        const double2 Ex = make_double2(-gpx.x - Atx.x, -gpx.y - Atx.y);
+        const double2 Ey = make_double2(-gpy.x - Aty.x, -gpy.y - Aty.y);
+        const double2 Ez = make_double2(-Atz.x, -Atz.y);
+        const double2 divE = cik(1.0, make_double2(kx * Ex.x + ky * Ey.x, kx * Ex.y + ky * Ey.y));
+        const double2 gauss = csub(divE, make_double2(rho.x / a.eps0, rho.y / a.eps0));
+        const double2 J0 = a.Jhat[id], J1 = a.Jhat[N + id];
+        const double2 divJ = cik(1.0, make_double2(kx * J0.x + ky * J1.x, kx * J0.y + ky * J1.y));
+        const double2 cont = cadd(ddt(4), divJ);
+        const double2 Bx = cik(ky, Az);
+        const double2 gAzx = cik(kx, Az);
+        const double2 By = make_double2(-gAzx.x, -gAzx.y);
+        const double2 Bz = csub(cik(kx, Ay), cik(ky, Ax));
+        double2* o = a.out;
+        o[0 * (size_t)N + id] = gauge;
+        o[1 * (size_t)N + id] = Ex;
+        o[2 * (size_t)N + id] = Ey;
+        o[3 * (size_t)N + id] = Ez;
+        o[4 * (size_t)N + id] = gauss;
+        o[5 * (size_t)N + id] = cont;
+        o[6 * (size_t)N + id] = Bx;
+        o[7 * (size_t)N + id] = By;
+        o[8 * (size_t)N + id] = Bz;
+        o[9 * (size_t)N + id] = rho;
+    }
+}
+
+constexpr int kRedThreads = 256;
+constexpr int kNSums = 8;  // gauge, gauss, cont, Bz, B, E, rho, J
+
+__global__ void __launch_bounds__(kRedThreads) diag_reduce_kernel(DiagReduceArgs a) {
+    const int N = a.N;
+    const double* f = a.dfields;
+    DD s[kNSums];
+#pragma unroll
+    for (int k = 0; k < kNSums; ++k) s[k] = DD{0.0, 0.0};
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        const double gauge = f[id], Ex = f[N + id], Ey = f[2 * (size_t)N + id];
+        const double Ez = f[3 * (size_t)N + id], gauss = f[4 * (size_t)N + id];
+        const double cont = f[5 * (size_t)N + id], Bx = f[6 * (size_t)N + id];
+        const double By = f[7 * (size_t)N + id], Bz = f[8 * (size_t)N + id];
+        const double rho = f[9 * (size_t)N + id];
+        const double Jx = a.J[id], Jy = a.J[N + id], Jz = a.J[2 * (size_t)N + id];
+        s[0] = dd_add_dd(s[0], dd_sq(gauge));
+        s[1] = dd_add_dd(s[1], dd_sq(gauss));
+        s[2] = dd_add_dd(s[2], dd_sq(cont));
+        s[3] = dd_add_dd(s[3], dd_sq(Bz));
+        s[4] = dd_add_dd(dd_add_dd(dd_add_dd(s[4], dd_sq(Bx)), dd_sq(By)), dd_sq(Bz));
+        s[5] = dd_add_dd(dd_add_dd(dd_add_dd(s[5], dd_sq(Ex)), dd_sq(Ey)), dd_sq(Ez));
+        s[6] = dd_add_dd(s[6], dd_sq(rho));
+        s[7] = dd_add_dd(dd_add_dd(dd_add_dd(s[7], dd_sq(Jx)), dd_sq(Jy)), dd_sq(Jz));
+    }
+    __shared__ double red[kRedThreads / kWarp][kNSums * 2];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < kNSums; ++k) {
+        s[k] = warp_sum_dd(s[k]);
+        if (lane == 0) {
+            red[warp][2 * k] = s[k].hi;
+            red[warp][2 * k + 1] = s[k].lo;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < kNSums) {
+        DD t{0.0, 0.0};
+        for (int w = 0; w < kRedThreads / kWarp; ++w)
+            t = dd_add_dd(t, DD{red[w][2 * threadIdx.x], red[w][2 * threadIdx.x + 1]});
+        a.partials[(size_t)blockIdx.x * 16 + 2 * threadIdx.x] = t.hi;
+        a.partials[(size_t)blockIdx.x * 16 + 2 * threadIdx.x + 1] = t.lo;
+    }
+}
+
+__global__ void diag_final_kernel(DiagReduceArgs a) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    DD s[kNSums];
+    for (int k = 0; k < kNSums; ++k) {
+        s[k] = DD{0.0, 0.0};
+        for (int b = 0; b < a.grid; ++b)
+            s[k] = dd_add_dd(s[k], DD{a.partials[b * 16 + 2 * k], a.partials[b * 16 + 2 * k + 1]});
+    }
+    DD kin{0.0, 0.0}, gs{0.0, 0.0};
+    double vmax = 0.0;
+    for (int b = 0; b < a.pcount; ++b) {
+        const double* p = a.pdiag + (size_t)b * kDiagPart;
+        kin = dd_add_dd(kin, DD{p[0], p[1]});
+        gs = dd_add_dd(gs, DD{p[2], p[3]});
+        vmax = fmax(vmax, p[4]);
+    }
+    const double invN = 1.0 / (double)a.N;
+    auto rms = [&](DD v) { return sqrt((v.hi + v.lo) * invN); };
+    double* r = a.row;
+    r[0] = rms(s[0]);
+    r[1] = rms(s[1]);
+    r[2] = rms(s[2]);
+    r[3] = rms(s[3]);
+    r[4] = rms(s[4]);
+    r[5] = rms(s[5]);
+    r[6] = rms(s[6]);
+    r[7] = rms(s[7]);
+    r[8] = 0.5 * a.eps0 * ((s[5].hi + s[5].lo) * a.dA) + 0.5 / a.mu0 * ((s[4].hi + s[4].lo) * a.dA);
+    r[9] = kin.hi + kin.lo;
+    r[10] = r[8] + r[9];
+    r[11] = vmax;
+    r[12] = a.np > 0 ? (gs.hi + gs.lo) / (double)a.np : 0.0;
+}
+
+__global__ void poisson_kspace_kernel(int N, const double* k2, const double2* rh, double eps0,
+                                      double2* out) {
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        const double kk = k2[id];
+        if (kk > 0.0) {
+            const double d = eps0 * kk;
+            out[id] = make_double2(rh[id].x / d, rh[id].y / d);
+        } else {
+            out[id] = make_double2(0.0, 0.0);
+        }
+    }
+}
+
+__global__ void derivative_kspace_kernel(int N, const double* k, const double2* in, double2* out) {
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x)
+        out[id] = cik(k[id], in[id]);
+}
+
+__global__ void bdf_single_kernel(int N, const double* k2, const double2* src, const double2* hist,
+                                  int nb, double b0, double b1, double b2, double b3, double b4,
+                                  double scale, double2* out) {
+    const double b[5] = {b0, b1, b2, b3, b4};
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        double2 r = src[id];
+        for (int l = 1; l < nb; ++l) r = csub(r, cscale(scale * b[l], hist[(size_t)(l - 1) * N + id]));
+        const double d = scale * b[0] + k2[id];
+        out[id] = make_double2(r.x / d, r.y / d);
+    }
+}
+
+__global__ void gather_scalar_kernel(int nx, int ny, double inv_dx, double inv_dy, const double* f,
+                                     long np, const double* x, const double* y, double* out) {
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
+        const Quad1D qx = quadratic_weights(x[p], inv_dx);
+        const Quad1D qy = quadratic_weights(y[p], inv_dy);
+        const double wxs[3] = {qx.w0, qx.w1, qx.w2};
+        const double wys[3] = {qy.w0, qy.w1, qy.w2};
+        double v = 0.0;
+        for (int ia = 0; ia < 3; ++ia) {
+            const int gx = wrap_index(qx.ic - 1 + ia, nx);
+            for (int ib = 0; ib < 3; ++ib) {
+                const int gy = wrap_index(qy.ic - 1 + ib, ny);
+                v = fma(f[gx * ny + gy], wxs[ia] * wys[ib], v);
+            }
+        }
+        out[p] = v;
+    }
+}
+
+__global__ void fill_hist_kernel(double2* h, int R, int N, const double2* src) {
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        const double2 v = src[id];
+        for (int s = 0; s < R; ++s) h[(size_t)s * N + id] = v;
+    }
+}
+
+int grid_for(long n, int threads) {
+    long g = (n + threads - 1) / threads;
+    if (g > 148 * 16) g = 148 * 16;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+template <int MODE, int NCOMP, bool UNIFORM>
+cudaError_t launch_one(const TileGeom& tg, const PushArgs& a, int grid, cudaStream_t st) {
+    const int smem = push_deposit_smem_bytes(tg, NCOMP);
+    push_deposit_kernel<MODE, NCOMP, UNIFORM><<<grid, kPushThreads, smem, st>>>(a, tg);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+template <int MODE, int NCOMP, bool UNIFORM>
+cudaError_t set_smem_one(int bytes) {
+    return cudaFuncSetAttribute(push_deposit_kernel<MODE, NCOMP, UNIFORM>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+}  // namespace
+
+static long g_launches = 0;
+void count_launches(long n) { __atomic_fetch_add(&g_launches, n, __ATOMIC_RELAXED); }
+long launches_total() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+int push_deposit_smem_bytes(const TileGeom& tg, int ncomp) {
+    const int WN = tg.wx * tg.wy;
+    const int window = 2 * ncomp * WN * 8;
+    const int stage = kPushWarps * (32 * (9 + ncomp) * 8 + 32 * 3 * 4);
+    int bytes = window + stage;
+    const int red = kPushWarps * 5 * 8;
+    return bytes > red ? bytes : red;
+}
+
+cudaError_t push_configure_smem(const TileGeom& tg) {
+    cudaError_t e = cudaSuccess;
+#define UPIC_SET(MODE, NC, U)                                                   \
+    e = set_smem_one<MODE, NC, U>(push_deposit_smem_bytes(tg, NC));              \
+    if (e != cudaSuccess) return e;
+    UPIC_SET(kModeDeposit, 1, true) UPIC_SET(kModeDeposit, 1, false)
+    UPIC_SET(kModeDeposit, 3, true) UPIC_SET(kModeDeposit, 3, false)
+    UPIC_SET(kModeDeposit, 4, true) UPIC_SET(kModeDeposit, 4, false)
+    UPIC_SET(kModeAdvanceDeposit, 3, true) UPIC_SET(kModeAdvanceDeposit, 3, false)
+    UPIC_SET(kModeAdvanceDeposit, 4, true) UPIC_SET(kModeAdvanceDeposit, 4, false)
+    UPIC_SET(kModePush, 3, true) UPIC_SET(kModePush, 3, false)
+    UPIC_SET(kModePush, 4, true) UPIC_SET(kModePush, 4, false)
+#undef UPIC_SET
+    return e;
+}
+
+cudaError_t launch_push_deposit(int mode, int ncomp, bool uniform, const TileGeom& tg,
+                                const PushArgs& a, int grid, cudaStream_t st) {
+#define UPIC_CASE(MODE, NC)                                                     \
+    if (mode == MODE && ncomp == NC)                                            \
+        return uniform ? launch_one<MODE, NC, true>(tg, a, grid, st)            \
+                       : launch_one<MODE, NC, false>(tg, a, grid, st);
+    UPIC_CASE(kModeDeposit, 1)
+    UPIC_CASE(kModeDeposit, 3)
+    UPIC_CASE(kModeDeposit, 4)
+    UPIC_CASE(kModeAdvanceDeposit, 3)
+    UPIC_CASE(kModeAdvanceDeposit, 4)
+    UPIC_CASE(kModePush, 3)
+    UPIC_CASE(kModePush, 4)
+#undef UPIC_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_convert_acc(unsigned long long* acc, int N, const double* scale, double* J,
+                               double* rho, double n0, int mask, cudaStream_t st) {
+    convert_acc_kernel<<<grid_for(N, 256), 256, 0, st>>>(acc, N, scale[0], scale[1], scale[2],
+                                                         scale[3], J, rho, n0, mask);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bdf_kspace(const KspaceArgs& a, cudaStream_t st) {
+    bdf_kspace_kernel<<<grid_for(a.N, 256), 256, 0, st>>>(a);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diag_kspace(const DiagKArgs& a, cudaStream_t st) {
+    diag_kspace_kernel<<<grid_for(a.N, 256), 256, 0, st>>>(a);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diag_reduce(const DiagReduceArgs& a, cudaStream_t st) {
+    diag_reduce_kernel<<<a.grid, kRedThreads, 0, st>>>(a);
+    diag_final_kernel<<<1, 32, 0, st>>>(a);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_poisson_kspace(int N, const double* k2, const double2* rho_hat, double eps0,
+                                  double2* out, cudaStream_t st) {
+    poisson_kspace_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, k2, rho_hat, eps0, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_derivative_kspace(int N, const double* k, const double2* in, double2* out,
+                                     cudaStream_t st) {
+    derivative_kspace_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, k, in, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bdf_single(int N, const double* k2, const double2* src, const double2* hist,
+                              int nb, const double* b, double scale, double2* out,
+                              cudaStream_t st) {
+    bdf_single_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, k2, src, hist, nb, b[0], b[1], b[2], b[3],
+                                                        b[4], scale, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_scalar(int nx, int ny, double inv_dx, double inv_dy, const double* f,
+                                 long np, const double* x, const double* y, double* out,
+                                 cudaStream_t st) {
+    gather_scalar_kernel<<<grid_for(np, 256), 256, 0, st>>>(nx, ny, inv_dx, inv_dy, f, np, x, y, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_hist(double2* h, int R, int N, const double2* src, cudaStream_t st) {
+    fill_hist_kernel<<<grid_for(N, 256), 256, 0, st>>>(h, R, N, src);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace upic
