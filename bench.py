@@ -41,6 +41,9 @@ WORKLOADS = {
                       charge_update="conserving", uth=(0.02, 0.2, 0.0), seed=2026),
     "weibel64": dict(nx=64, ny=64, ppc=64, L=2 * np.pi / 0.3, dt=0.05, method="bdf1",
                      charge_update="conserving", uth=(0.02, 0.2, 0.0), seed=2026),
+    # profiling case: same grid and physics, 16 e-/cell (370 MB of particle state)
+    "weibel512_ppc16": dict(nx=512, ny=512, ppc=16, L=2 * np.pi / 0.3, dt=0.05, method="bdf1",
+                            charge_update="conserving", uth=(0.02, 0.2, 0.0), seed=2026),
 }
 # Algorithmic HBM bytes per particle per step of the fused push kernel: the
 # FP64 particle state x, y, P(3), v(3), v_prev(3) read once and written once.

@@ -140,10 +140,16 @@ def test_step_loop_matches_reference_fixture(name):
         assert relerr(fields[f], g["fields"][f].reshape(fields[f].shape)) < 1e-10, f
     for k in PHYS_DIAG:
         assert relerr(diag[:, k], g["diag"][:, k]) < 1e-10, k
-    # round-off level residuals: same order of magnitude as the reference's
-    if bool(ip[3]):
-        for k in (0, 1, 2):
-            assert np.all(diag[1:, k] < 1e-12), k
+    # residual columns: where the reference's residual is physical (random
+    # particles put charge on the Nyquist planes, whose zeroed wave number
+    # leaves Gauss's law and the gauge unenforced there) compare values;
+    # where it is round-off, both must be round-off.
+    for k in (0, 1, 2):
+        ref = g["diag"][1:, k]
+        if np.max(ref) > 1e-9:
+            assert relerr(diag[1:, k], ref) < 1e-9, k
+        else:
+            assert np.max(diag[1:, k]) < 1e-11, k
 
 
 def _bimax(nx, ny, ppc, L, seed):

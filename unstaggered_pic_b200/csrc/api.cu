@@ -202,7 +202,7 @@ int alloc_sortwork(upic_ctx* c, SortWork& w, long cap, const TileGeom& tg) {
     if ((rc = dalloc(c, &w.scan_tmp, scan_blocks))) return rc;
     const int ntiles = tg.ntx * tg.nty;
     if ((rc = dalloc(c, &w.tile_count, ntiles))) return rc;
-    if ((rc = dalloc(c, &w.tile_start, ntiles))) return rc;
+    if ((rc = dalloc(c, &w.tile_start, ntiles + 1))) return rc;
     if ((rc = dalloc(c, &w.tile_chunks, ntiles))) return rc;
     const long chunks = cap / tg.chunk + ntiles + 1;
     if ((rc = dalloc(c, &w.chunks, chunks))) return rc;
@@ -328,8 +328,11 @@ PushArgs push_args(upic_ctx* c, const ParticleSoA& p, long np, bool uniform) {
     a.inv_dx = 1.0 / c->dx;
     a.inv_dy = 1.0 / c->dy;
     a.inv_dA = 1.0 / c->dA;
+    a.inv_Lx = 1.0 / c->cfg.Lx;
+    a.inv_Ly = 1.0 / c->cfg.Ly;
     a.dt = c->cfg.dt;
     a.c = c->cfg.c;
+    a.inv_c2 = 1.0 / (c->cfg.c * c->cfg.c);
     a.gfields = c->d_gf;
     a.acc = c->d_acc;
     for (int k = 0; k < 4; ++k) a.scale[k] = c->scale[k];
@@ -495,12 +498,9 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
     c->st = c->own;
     if (fft_configure_smem() != cudaSuccess || push_configure_smem(c->tg) != cudaSuccess)
         return bail(fail(c, UPIC_ERR_CUDA, "cudaFuncSetAttribute failed"));
-    int occ = 0;
-    // occupancy of the push kernel bounds the persistent grid
-    occ = 227 * 1024 / (push_deposit_smem_bytes(c->tg, 4) + 1024);
-    if (occ < 1) occ = 1;
-    if (occ > 8) occ = 8;
-    c->push_grid = c->nsm * occ;
+    // persistent grid: as many push CTAs as fit on the GPU at once
+    const int occ = push_occupancy(c->tg, cfg->charge_update == UPIC_CHARGE_NAIVE ? 4 : 3);
+    c->push_grid = c->nsm * (occ > 0 ? occ : 1);
 
     const int N = c->N;
     auto tw_x = twiddles(c->nx), tw_y = twiddles(c->ny);

@@ -22,12 +22,12 @@ constexpr int kPushWarps = kPushThreads / kWarp;
 constexpr int kKeyNone = -1;
 constexpr int kKeyEscape = -2;
 
-// Per-warp staging of 32 particles: 9 tensor-product weights and up to 4
-// deposit values per particle, plus window key and global stencil origin.
+// Per-warp staging: the NV = 9*NCOMP deposit products of each of the warp's
+// 32 particles (weight of stencil node ab times deposit value c).
 template <int NCOMP>
 struct StageLayout {
-    static constexpr int kDoubles = 32 * (9 + NCOMP);
-    static constexpr int kInts = 32 * 3;
+    static constexpr int kNV = 9 * NCOMP;
+    static constexpr int kDoubles = 32 * kNV;
 };
 
 UPIC_D int acc_slot(int ncomp, int c) { return ncomp == 1 ? 3 : c; }
@@ -35,32 +35,64 @@ UPIC_D int acc_slot(int ncomp, int c) { return ncomp == 1 ? 3 : c; }
 // Window-local coordinate of a stencil origin node (tiled axis): -1 when the
 // three-node stencil does not fit in the window.
 UPIC_D int window_coord(int s, int origin, int n, int w) {
-    int d = (s - origin) % n;
-    if (d < 0) d += n;
+    const int d = (s - origin) & (n - 1);
     return d <= w - 3 ? d : -1;
 }
 
+// Fold a CTA's window into the global fixed-point accumulators (integer adds:
+// order-independent, hence deterministic).
+template <int NCOMP>
+UPIC_D void fold_window(const unsigned long long* whi, const unsigned long long* wlo, int WN,
+                        const TileGeom& tg, int ox, int oy, unsigned long long* acc) {
+    const int N = tg.nx * tg.ny;
+    for (int idx = threadIdx.x; idx < NCOMP * WN; idx += blockDim.x) {
+        const unsigned long long hi = whi[idx], lo = wlo[idx];
+        if ((hi | lo) == 0ull) continue;
+        const int cc = idx / WN, widx = idx - cc * WN;
+        const int lx = widx / tg.wy, ly = widx - lx * tg.wy;
+        const int gx = tg.full_x ? lx : wrap_index(ox + lx, tg.nx);
+        const int gy = tg.full_y ? ly : wrap_index(oy + ly, tg.ny);
+        const int sl = acc_slot(NCOMP, cc);
+        atomicAdd(&acc[(size_t)(2 * sl) * N + gx * tg.ny + gy], hi);
+        atomicAdd(&acc[(size_t)(2 * sl + 1) * N + gx * tg.ny + gy], lo);
+    }
+}
+
 template <int MODE, int NCOMP, bool UNIFORM>
-__global__ void __launch_bounds__(kPushThreads)
+__global__ void __launch_bounds__(kPushThreads, 2)
 push_deposit_kernel(PushArgs a, TileGeom tg) {
+    constexpr int NV = StageLayout<NCOMP>::kNV;
+    constexpr int NPER = (NV + 31) / 32;
     extern __shared__ unsigned long long smem_u64[];
     const int WN = tg.wx * tg.wy;
     unsigned long long* whi = smem_u64;
     unsigned long long* wlo = whi + NCOMP * WN;
-    double* sd = reinterpret_cast<double*>(wlo + NCOMP * WN);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double* swab = sd + warp * StageLayout<NCOMP>::kDoubles;  // [32][9]
-    double* sval = swab + 32 * 9;                              // [32][NCOMP]
-    int* si = reinterpret_cast<int*>(sd + kPushWarps * StageLayout<NCOMP>::kDoubles);
-    int* skey = si + warp * StageLayout<NCOMP>::kInts;
-    int* sgx = skey + 32;
-    int* sgy = skey + 64;
+    double* sprod = reinterpret_cast<double*>(wlo + NCOMP * WN) + warp * StageLayout<NCOMP>::kDoubles;
+    int* sgk = reinterpret_cast<int*>(reinterpret_cast<double*>(wlo + NCOMP * WN) +
+                                      kPushWarps * StageLayout<NCOMP>::kDoubles) + warp * 32;
 
     const int nx = tg.nx, ny = tg.ny;
     const int N = nx * ny;
     const int nch = *a.nchunks;
     const int c_begin = (int)(((long long)blockIdx.x * nch) / gridDim.x);
     const int c_end = (int)(((long long)(blockIdx.x + 1) * nch) / gridDim.x);
+
+    // values owned by this lane in the segmented reduction: t = lane + 32 r is
+    // stencil node ab = t / NCOMP (a = ab/3 along x, b = ab%3 along y) and
+    // deposit component c = t % NCOMP
+    int t_off[NPER], t_a[NPER], t_b[NPER], t_c[NPER];
+    double t_scale[NPER];
+#pragma unroll
+    for (int r = 0; r < NPER; ++r) {
+        const int t = lane + 32 * r;
+        const int ab = t < NV ? t / NCOMP : 0;
+        t_a[r] = ab / 3;
+        t_b[r] = ab % 3;
+        t_c[r] = t < NV ? t - ab * NCOMP : 0;
+        t_off[r] = t_a[r] * tg.wy + t_b[r];
+        t_scale[r] = a.scale[acc_slot(NCOMP, t_c[r])];
+    }
 
     DD kin{0.0, 0.0}, gsum{0.0, 0.0};
     double vmax = 0.0;
@@ -72,18 +104,7 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
         if (ch.tile != cur_tile) {
             __syncthreads();
             if (cur_tile >= 0) {
-                // fold the finished window into the global accumulators
-                for (int idx = threadIdx.x; idx < NCOMP * WN; idx += blockDim.x) {
-                    const unsigned long long hi = whi[idx], lo = wlo[idx];
-                    if ((hi | lo) == 0ull) continue;
-                    const int cc = idx / WN, widx = idx - cc * WN;
-                    const int lx = widx / tg.wy, ly = widx - lx * tg.wy;
-                    const int gx = tg.full_x ? lx : wrap_index(ox + lx, nx);
-                    const int gy = tg.full_y ? ly : wrap_index(oy + ly, ny);
-                    const int sl = acc_slot(NCOMP, cc);
-                    atomicAdd(&a.acc[(size_t)(2 * sl) * N + gx * ny + gy], hi);
-                    atomicAdd(&a.acc[(size_t)(2 * sl + 1) * N + gx * ny + gy], lo);
-                }
+                fold_window<NCOMP>(whi, wlo, WN, tg, ox, oy, a.acc);
                 __syncthreads();
             }
             for (int idx = threadIdx.x; idx < 2 * NCOMP * WN; idx += blockDim.x) whi[idx] = 0ull;
@@ -95,17 +116,17 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
         }
         for (int base = ch.start; base < ch.end; base += kPushThreads) {
             const int p = base + threadIdx.x;
+            const bool active = p < ch.end;
             int key = kKeyNone, gx0 = 0, gy0 = 0;
-            double wab[9];
-            double val[NCOMP];
-            if (p < ch.end) {
+            double dwx[3], dwy[3], dval[NCOMP];
+            if (active) {
                 const double q = UNIFORM ? a.q0 : a.p.q[p];
                 double x = a.p.x[p], y = a.p.y[p];
                 double v0 = a.p.vx[p], v1 = a.p.vy[p], v2 = a.p.vz[p];
                 if (MODE == kModePush) {
                     // spectral_pic_part3.cpp:1050-1055: x^n = x^{n-1} + dt v^{n-1}
-                    x = wrap_periodic(x + a.dt * v0, a.Lx);
-                    y = wrap_periodic(y + a.dt * v1, a.Ly);
+                    x = wrap_periodic(x + a.dt * v0, a.Lx, a.inv_Lx);
+                    y = wrap_periodic(y + a.dt * v1, a.Ly, a.inv_Ly);
                     // gather A, grad phi, grad A at x^n (:1063-1078)
                     const Quad1D qx = quadratic_weights(x, a.inv_dx);
                     const Quad1D qy = quadratic_weights(y, a.inv_dy);
@@ -141,11 +162,11 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                     const double P1 = a.p.Py[p] + qdt * (gdy - G[4]);
                     const double P2 = a.p.Pz[p];
                     // velocity_from_canonical (:602-607)
-                    const double p0 = P0 - q * G[0], p1 = P1 - q * G[1], p2 = P2 - q * G[2];
                     const double m = UNIFORM ? a.m0 : a.p.m[p];
+                    const double p0 = P0 - q * G[0], p1 = P1 - q * G[1], p2 = P2 - q * G[2];
                     const double mc2 = m * c2;
-                    const double denom = sqrt(c2 * (p0 * p0 + p1 * p1 + p2 * p2) + mc2 * mc2);
-                    const double s = denom == 0.0 ? 0.0 : c2 / denom;
+                    const double arg = c2 * (p0 * p0 + p1 * p1 + p2 * p2) + mc2 * mc2;
+                    const double s = arg == 0.0 ? 0.0 : c2 * rsqrt(arg);
                     const double n0v = s * p0, n1v = s * p1, n2v = s * p2;
                     a.p.x[p] = x;
                     a.p.y[p] = y;
@@ -165,132 +186,150 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                 if (a.diag_part) {
                     const double m = UNIFORM ? a.m0 : a.p.m[p];
                     const double sp2 = v0 * v0 + v1 * v1 + v2 * v2;
-                    const double one_m = 1.0 - sp2 / c2;
-                    const double gam = 1.0 / sqrt(one_m > 1.0e-14 ? one_m : 1.0e-14);
+                    const double one_m = 1.0 - sp2 * a.inv_c2;
+                    const double gam = rsqrt(one_m > 1.0e-14 ? one_m : 1.0e-14);
                     gsum = dd_add(gsum, gam);
                     kin = dd_add(kin, (gam - 1.0) * m * a.c * a.c);
                     vmax = fmax(vmax, sqrt(sp2));
                 }
                 // deposit position: stored x (kModeDeposit) or one step ahead
                 if (MODE != kModeDeposit) {
-                    x = wrap_periodic(x + a.dt * v0, a.Lx);
-                    y = wrap_periodic(y + a.dt * v1, a.Ly);
+                    x = wrap_periodic(x + a.dt * v0, a.Lx, a.inv_Lx);
+                    y = wrap_periodic(y + a.dt * v1, a.Ly, a.inv_Ly);
                 }
                 const Quad1D dx_ = quadratic_weights(x, a.inv_dx);
                 const Quad1D dy_ = quadratic_weights(y, a.inv_dy);
                 const double wxs[3] = {dx_.w0, dx_.w1, dx_.w2};
                 const double wys[3] = {dy_.w0, dy_.w1, dy_.w2};
-#pragma unroll
-                for (int ia = 0; ia < 3; ++ia)
-#pragma unroll
-                    for (int ib = 0; ib < 3; ++ib) wab[ia * 3 + ib] = wxs[ia] * wys[ib];
                 const double qa = q * a.inv_dA;
                 if (NCOMP == 1) {
-                    val[0] = qa;
+                    dval[0] = qa;
                 } else {
-                    val[0] = qa * v0;
-                    val[1] = qa * v1;
-                    val[2] = qa * v2;
-                    if (NCOMP == 4) val[NCOMP - 1] = qa;
+                    dval[0] = qa * v0;
+                    dval[1] = qa * v1;
+                    dval[2] = qa * v2;
+                    if (NCOMP == 4) dval[NCOMP - 1] = qa;
                 }
                 gx0 = wrap_index(dx_.ic - 1, nx);
                 gy0 = wrap_index(dy_.ic - 1, ny);
                 const int lx = tg.full_x ? gx0 : window_coord(dx_.ic - 1, ox, nx, tg.wx);
                 const int ly = tg.full_y ? gy0 : window_coord(dy_.ic - 1, oy, ny, tg.wy);
                 key = (lx < 0 || ly < 0) ? kKeyEscape : lx * tg.wy + ly;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    dwx[k] = wxs[k];
+                    dwy[k] = wys[k];
+                }
             }
-            // stage
-            skey[lane] = key;
-            sgx[lane] = gx0;
-            sgy[lane] = gy0;
-            if (key != kKeyNone) {
+            // Group the warp's particles by window key: groups in the order of
+            // their first particle, particles in index order inside a group
+            // (deterministic), escapes after all groups.
+            const unsigned full = 0xffffffffu;
+            const unsigned lt = (1u << lane) - 1u;
+            const unsigned valid = __ballot_sync(full, key >= 0);
+            const unsigned esc = __ballot_sync(full, key == kKeyEscape);
+            const unsigned peers = __match_any_sync(full, key);
+            int row = -1, nvalid = 0, ngroups = 0;
+            unsigned heads = 0u;
+            for (unsigned rem = valid; rem;) {
+                const int l = __ffs(rem) - 1;
+                const unsigned g = __shfl_sync(full, peers, l);
+                const int gk = __shfl_sync(full, key, l);
+                if ((g >> lane) & 1u) row = nvalid + __popc(g & lt);
+                if (lane == 0) sgk[ngroups] = gk;
+                heads |= 1u << nvalid;
+                nvalid += __popc(g);
+                rem &= ~g;
+                ++ngroups;
+            }
+            if (key == kKeyEscape) row = nvalid + __popc(esc & lt);
+            if (row >= 0) {
+                // stage the products q v_c S_ab / dA of this particle in its row
+                double* mine = sprod + row * NV;
 #pragma unroll
-                for (int k = 0; k < 9; ++k) swab[lane * 9 + k] = wab[k];
+                for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
-                for (int k = 0; k < NCOMP; ++k) sval[lane * NCOMP + k] = val[k];
+                    for (int ib = 0; ib < 3; ++ib) {
+                        const double w = dwx[ia] * dwy[ib];
+#pragma unroll
+                        for (int cc = 0; cc < NCOMP; ++cc) mine[(ia * 3 + ib) * NCOMP + cc] = dval[cc] * w;
+                    }
             }
             __syncwarp();
-            // Warp-level segmented reduction: lane t owns value t (node ab, comp c)
-            // and sums it over runs of particles with the same window key, in
-            // particle order; each run end flushes one fixed-point add per value.
-            constexpr int NV = 9 * NCOMP;
-            constexpr int NPER = (NV + 31) / 32;
-            double run[NPER];
-#pragma unroll
-            for (int r = 0; r < NPER; ++r) run[r] = 0.0;
-            int cur = kKeyNone;
-            auto flush = [&](int k) {
-                const int lx = k / tg.wy, ly = k - (k / tg.wy) * tg.wy;
-#pragma unroll
-                for (int r = 0; r < NPER; ++r) {
-                    const int t = lane + 32 * r;
-                    if (t < NV && run[r] != 0.0) {
-                        const int ab = t / NCOMP, cc = t - ab * NCOMP;
-                        int nxl = lx + ab / 3, nyl = ly + ab % 3;
-                        if (tg.full_x) nxl %= tg.wx;
-                        if (tg.full_y) nyl %= tg.wy;
-                        const Fixed2 f = to_fixed(run[r], a.scale[acc_slot(NCOMP, cc)]);
-                        const int widx = cc * WN + nxl * tg.wy + nyl;
-                        atomicAdd(&whi[widx], f.hi);
-                        atomicAdd(&wlo[widx], f.lo);
-                    }
-                    run[r] = 0.0;
-                }
-            };
-            for (int j = 0; j < 32; ++j) {
-                const int k = skey[j];
-                if (k == kKeyNone) break;  // inactive lanes are trailing
-                if (k != cur) {
-                    if (cur >= 0) flush(cur);
-                    cur = k;
-                }
-                if (k == kKeyEscape) {
-                    // outside the window: exact fixed-point adds straight to the grid
+            // Particles whose stencil leaves the window (rare): exact fixed-point
+            // adds straight to the grid.
+            {
+                unsigned e = esc;
+                int erow = nvalid;
+                while (e) {
+                    const int j = __ffs(e) - 1;
+                    e &= e - 1;
+                    const int gxj = __shfl_sync(full, gx0, j);
+                    const int gyj = __shfl_sync(full, gy0, j);
 #pragma unroll
                     for (int r = 0; r < NPER; ++r) {
                         const int t = lane + 32 * r;
                         if (t < NV) {
-                            const int ab = t / NCOMP, cc = t - ab * NCOMP;
-                            const double v = sval[j * NCOMP + cc] * swab[j * 9 + ab];
+                            const double v = sprod[erow * NV + t];
                             if (v != 0.0) {
-                                const int gx = wrap_index(sgx[j] + ab / 3, nx);
-                                const int gy = wrap_index(sgy[j] + ab % 3, ny);
-                                const int sl = acc_slot(NCOMP, cc);
-                                const Fixed2 f = to_fixed(v, a.scale[sl]);
-                                atomicAdd(&a.acc[(size_t)(2 * sl) * N + gx * ny + gy], f.hi);
-                                atomicAdd(&a.acc[(size_t)(2 * sl + 1) * N + gx * ny + gy], f.lo);
+                                const int g = wrap_index(gxj + t_a[r], nx) * ny + wrap_index(gyj + t_b[r], ny);
+                                const int sl = acc_slot(NCOMP, t_c[r]);
+                                const Fixed2 f = to_fixed(v, t_scale[r]);
+                                atomicAdd(&a.acc[(size_t)(2 * sl) * N + g], f.hi);
+                                atomicAdd(&a.acc[(size_t)(2 * sl + 1) * N + g], f.lo);
                             }
                         }
                     }
-                    continue;
+                    ++erow;
                 }
+            }
+            // Warp-level segmented reduction: lane t owns value t and sums it over
+            // the rows of each key group (two interleaved partial sums, fixed
+            // order); each group adds its sum to the window once per value.
+            {
+                unsigned h = heads;
+                int gi = 0;
+                while (h) {
+                    const int rs = __ffs(h) - 1;
+                    h &= h - 1;
+                    const int re = h ? __ffs(h) - 1 : nvalid;
+                    const int k = sgk[gi++];
 #pragma unroll
-                for (int r = 0; r < NPER; ++r) {
-                    const int t = lane + 32 * r;
-                    if (t < NV) {
-                        const int ab = t / NCOMP, cc = t - ab * NCOMP;
-                        run[r] = fma(sval[j * NCOMP + cc], swab[j * 9 + ab], run[r]);
+                    for (int r = 0; r < NPER; ++r) {
+                        const int t = lane + 32 * r;
+                        if (t < NV) {
+                            double s0 = 0.0, s1 = 0.0;
+                            int j = rs;
+                            for (; j + 1 < re; j += 2) {
+                                s0 += sprod[j * NV + t];
+                                s1 += sprod[(j + 1) * NV + t];
+                            }
+                            if (j < re) s0 += sprod[j * NV + t];
+                            const double sum = s0 + s1;
+                            if (sum != 0.0) {
+                                int widx;
+                                if (tg.full_x || tg.full_y) {
+                                    const int kx = k / tg.wy, ky = k - kx * tg.wy;
+                                    int nxl = kx + t_a[r], nyl = ky + t_b[r];
+                                    if (tg.full_x) nxl &= tg.wx - 1;
+                                    if (tg.full_y) nyl &= tg.wy - 1;
+                                    widx = nxl * tg.wy + nyl;
+                                } else {
+                                    widx = k + t_off[r];
+                                }
+                                const Fixed2 f = to_fixed(sum, t_scale[r]);
+                                atomicAdd(&whi[t_c[r] * WN + widx], f.hi);
+                                atomicAdd(&wlo[t_c[r] * WN + widx], f.lo);
+                            }
+                        }
                     }
                 }
             }
-            if (cur >= 0) flush(cur);
             __syncwarp();
         }
     }
     __syncthreads();
-    if (cur_tile >= 0) {
-        for (int idx = threadIdx.x; idx < NCOMP * WN; idx += blockDim.x) {
-            const unsigned long long hi = whi[idx], lo = wlo[idx];
-            if ((hi | lo) == 0ull) continue;
-            const int cc = idx / WN, widx = idx - cc * WN;
-            const int lx = widx / tg.wy, ly = widx - lx * tg.wy;
-            const int gx = tg.full_x ? lx : wrap_index(ox + lx, nx);
-            const int gy = tg.full_y ? ly : wrap_index(oy + ly, ny);
-            const int sl = acc_slot(NCOMP, cc);
-            atomicAdd(&a.acc[(size_t)(2 * sl) * N + gx * ny + gy], hi);
-            atomicAdd(&a.acc[(size_t)(2 * sl + 1) * N + gx * ny + gy], lo);
-        }
-    }
+    if (cur_tile >= 0) fold_window<NCOMP>(whi, wlo, WN, tg, ox, oy, a.acc);
     // particle reductions: fixed order (lanes, then warps in index order)
     if (a.diag_part) {
         kin = warp_sum_dd(kin);
@@ -505,38 +544,46 @@ __global__ void __launch_bounds__(kRedThreads) diag_reduce_kernel(DiagReduceArgs
     }
 }
 
+// Final reduction in a fixed order: lane l sums blocks l, l+32, ... and the
+// 32 lane sums are combined by a fixed butterfly; then thread 0 forms the row.
 __global__ void diag_final_kernel(DiagReduceArgs a) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    DD s[kNSums];
+    const int lane = threadIdx.x;
+    __shared__ double sums[kNSums + 2][2];
+    __shared__ double svmax;
     for (int k = 0; k < kNSums; ++k) {
-        s[k] = DD{0.0, 0.0};
-        for (int b = 0; b < a.grid; ++b)
-            s[k] = dd_add_dd(s[k], DD{a.partials[b * 16 + 2 * k], a.partials[b * 16 + 2 * k + 1]});
+        DD s{0.0, 0.0};
+        for (int b = lane; b < a.grid; b += 32)
+            s = dd_add_dd(s, DD{a.partials[b * 16 + 2 * k], a.partials[b * 16 + 2 * k + 1]});
+        s = warp_sum_dd(s);
+        if (lane == 0) { sums[k][0] = s.hi; sums[k][1] = s.lo; }
     }
     DD kin{0.0, 0.0}, gs{0.0, 0.0};
     double vmax = 0.0;
-    for (int b = 0; b < a.pcount; ++b) {
+    for (int b = lane; b < a.pcount; b += 32) {
         const double* p = a.pdiag + (size_t)b * kDiagPart;
         kin = dd_add_dd(kin, DD{p[0], p[1]});
         gs = dd_add_dd(gs, DD{p[2], p[3]});
         vmax = fmax(vmax, p[4]);
     }
+    kin = warp_sum_dd(kin);
+    gs = warp_sum_dd(gs);
+    vmax = warp_max(vmax);
+    if (lane == 0) {
+        sums[kNSums][0] = kin.hi; sums[kNSums][1] = kin.lo;
+        sums[kNSums + 1][0] = gs.hi; sums[kNSums + 1][1] = gs.lo;
+        svmax = vmax;
+    }
+    __syncwarp();
+    if (lane != 0) return;
     const double invN = 1.0 / (double)a.N;
-    auto rms = [&](DD v) { return sqrt((v.hi + v.lo) * invN); };
+    auto tot = [&](int k) { return sums[k][0] + sums[k][1]; };
     double* r = a.row;
-    r[0] = rms(s[0]);
-    r[1] = rms(s[1]);
-    r[2] = rms(s[2]);
-    r[3] = rms(s[3]);
-    r[4] = rms(s[4]);
-    r[5] = rms(s[5]);
-    r[6] = rms(s[6]);
-    r[7] = rms(s[7]);
-    r[8] = 0.5 * a.eps0 * ((s[5].hi + s[5].lo) * a.dA) + 0.5 / a.mu0 * ((s[4].hi + s[4].lo) * a.dA);
-    r[9] = kin.hi + kin.lo;
+    for (int k = 0; k < kNSums; ++k) r[k] = sqrt(tot(k) * invN);
+    r[8] = 0.5 * a.eps0 * (tot(5) * a.dA) + 0.5 / a.mu0 * (tot(4) * a.dA);
+    r[9] = tot(kNSums);
     r[10] = r[8] + r[9];
-    r[11] = vmax;
-    r[12] = a.np > 0 ? (gs.hi + gs.lo) / (double)a.np : 0.0;
+    r[11] = svmax;
+    r[12] = a.np > 0 ? tot(kNSums + 1) / (double)a.np : 0.0;
 }
 
 __global__ void poisson_kspace_kernel(int N, const double* k2, const double2* rh, double eps0,
@@ -625,8 +672,8 @@ long launches_total() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 int push_deposit_smem_bytes(const TileGeom& tg, int ncomp) {
     const int WN = tg.wx * tg.wy;
     const int window = 2 * ncomp * WN * 8;
-    const int stage = kPushWarps * (32 * (9 + ncomp) * 8 + 32 * 3 * 4);
-    int bytes = window + stage;
+    const int stage = kPushWarps * (32 * 9 * ncomp * 8 + 32 * 4);
+    const int bytes = window + stage;
     const int red = kPushWarps * 5 * 8;
     return bytes > red ? bytes : red;
 }
@@ -645,6 +692,17 @@ cudaError_t push_configure_smem(const TileGeom& tg) {
     UPIC_SET(kModePush, 4, true) UPIC_SET(kModePush, 4, false)
 #undef UPIC_SET
     return e;
+}
+
+int push_occupancy(const TileGeom& tg, int ncomp) {
+    int n = 0;
+    if (ncomp == 4)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, push_deposit_kernel<kModePush, 4, true>, kPushThreads,
+                                                      push_deposit_smem_bytes(tg, 4));
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, push_deposit_kernel<kModePush, 3, true>, kPushThreads,
+                                                      push_deposit_smem_bytes(tg, 3));
+    return n;
 }
 
 cudaError_t launch_push_deposit(int mode, int ncomp, bool uniform, const TileGeom& tg,

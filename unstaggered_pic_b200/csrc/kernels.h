@@ -97,7 +97,8 @@ struct PushArgs {
     long np;
     double q0, m0;          // uniform charge and mass when p.q / p.m are null
     double Lx, Ly, inv_dx, inv_dy, inv_dA;
-    double dt, c;
+    double inv_Lx, inv_Ly;
+    double dt, c, inv_c2;
     const double* gfields;  // interleaved node records, kGFStride doubles
     const Chunk* chunks;
     const int* nchunks;
@@ -112,6 +113,8 @@ cudaError_t launch_push_deposit(int mode, int ncomp, bool uniform_qm, const Tile
                                 const PushArgs& a, int grid, cudaStream_t st);
 int push_deposit_smem_bytes(const TileGeom& tg, int ncomp);
 cudaError_t push_configure_smem(const TileGeom& tg);
+// Resident CTAs per SM of the step's push kernel (ncomp 3 or 4).
+int push_occupancy(const TileGeom& tg, int ncomp);
 
 // acc -> real fields: J (3 x N) from slots 0..2 when ncomp_mask & 1;
 // rho = n0 + slot 3 when ncomp_mask & 2.  Zeroes the converted slots.

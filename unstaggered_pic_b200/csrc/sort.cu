@@ -32,8 +32,8 @@ __global__ void make_keys_kernel(TileGeom tg, ParticleSoA p, long np, double Lx,
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < np; q += (long)gridDim.x * blockDim.x) {
         double x = p.x[q], y = p.y[q];
         if (shift != 0.0) {
-            x = wrap_periodic(x + shift * p.vx[q], Lx);
-            y = wrap_periodic(y + shift * p.vy[q], Ly);
+            x = wrap_periodic(x + shift * p.vx[q], Lx, 1.0 / Lx);
+            y = wrap_periodic(y + shift * p.vy[q], Ly, 1.0 / Ly);
         }
         const int icx = wrap_index(quadratic_weights(x, inv_dx).ic, tg.nx);
         const int icy = wrap_index(quadratic_weights(y, inv_dy).ic, tg.ny);
@@ -179,9 +179,20 @@ cudaError_t exclusive_scan(const int* in, int* out, long n, int* tmp, int* grand
 }
 
 // ---- chunk table ----------------------------------------------------------
-__global__ void tile_count_kernel(const unsigned* keys, long n, unsigned cells_per_tile, int* cnt) {
-    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
-        atomicAdd(&cnt[keys[q] / cells_per_tile], 1);
+// Tile extents of the sorted keys without atomics: position q opens every
+// tile in (tile(key[q-1]), tile(key[q])]; tile_start[ntiles] = n.
+__global__ void tile_bounds_kernel(const unsigned* keys, long n, unsigned cells_per_tile, int ntiles,
+                                   int* tstart) {
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q <= n; q += (long)gridDim.x * blockDim.x) {
+        const int t = q < n ? (int)(keys[q] / cells_per_tile) : ntiles;
+        const int tp = q > 0 ? (int)(keys[q - 1] / cells_per_tile) : -1;
+        for (int k = tp + 1; k <= t; ++k) tstart[k] = (int)q;
+    }
+}
+
+__global__ void tile_counts_kernel(const int* tstart, int ntiles, int* cnt) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < ntiles) cnt[t] = tstart[t + 1] - tstart[t];
 }
 
 __global__ void tile_chunks_kernel(const int* cnt, int ntiles, int chunk, int* nch) {
@@ -276,15 +287,15 @@ cudaError_t sort_particles_by_tile(const TileGeom& tg, const ParticleSoA& p, lon
     }
     // chunk table
     const int ntiles = tg.ntx * tg.nty;
-    cudaMemsetAsync(w.tile_count, 0, sizeof(int) * ntiles, st);
-    tile_count_kernel<<<grid_for(np), 256, 0, st>>>(w.keys, np, (unsigned)(tg.tile_x * tg.tile_y),
-                                                    w.tile_count);
-    exclusive_scan(w.tile_count, w.tile_start, ntiles, w.scan_tmp, nullptr, st);
+    tile_bounds_kernel<<<grid_for(np + 1), 256, 0, st>>>(w.keys, np, (unsigned)(tg.tile_x * tg.tile_y),
+                                                         ntiles, w.tile_start);
+    tile_counts_kernel<<<(ntiles + 255) / 256, 256, 0, st>>>(w.tile_start, ntiles, w.tile_count);
+    count_launches(2);
     tile_chunks_kernel<<<(ntiles + 255) / 256, 256, 0, st>>>(w.tile_count, ntiles, tg.chunk, w.tile_chunks);
     exclusive_scan(w.tile_chunks, w.tile_chunks, ntiles, w.scan_tmp, w.nchunks, st);
     fill_chunks_kernel<<<(ntiles + 255) / 256, 256, 0, st>>>(w.tile_count, w.tile_start, w.tile_chunks,
                                                              ntiles, tg.chunk, w.chunks);
-    count_launches(3);
+    count_launches(2);
     return cudaGetLastError();
 }
 

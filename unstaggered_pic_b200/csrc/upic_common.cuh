@@ -27,6 +27,16 @@ UPIC_HD double wrap_periodic(double x, double L) {
     return x;
 }
 
+// Same result with a precomputed 1/L: floor(x*invL) can differ from
+// floor(x/L) only when x is within an ulp of a multiple of L, and the two
+// correction branches then produce the identical wrapped value.
+UPIC_HD double wrap_periodic(double x, double L, double invL) {
+    x -= floor(x * invL) * L;
+    if (x >= L) x -= L;
+    if (x < 0.0) x += L;
+    return x;
+}
+
 // Quadratic B-spline weights centred on the nearest node:
 // spectral_pic_part3.cpp:537-552.  ic is the nearest node (unwrapped).
 struct Quad1D {
@@ -47,10 +57,9 @@ UPIC_HD Quad1D quadratic_weights(double x, double inv_dx) {
     return q;
 }
 
-UPIC_HD int wrap_index(int i, int n) {
-    i %= n;
-    return i < 0 ? i + n : i;
-}
+// Periodic node index; n is a power of two (radix-2 grids), so the wrap is a
+// mask (two's complement handles negative i).
+UPIC_HD int wrap_index(int i, int n) { return i & (n - 1); }
 
 // ---------------------------------------------------------------------------
 // Deterministic fixed-point accumulation.
