@@ -153,6 +153,23 @@ def measured_traffic(np_total):
         return None
 
 
+def max_over_ranks(x, dist, device):
+    """Max of a per-rank scalar over all ranks (device time is taken as the
+    slowest rank's); identity without a process group."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, particles_per_rank, steps, max_ms):
+    """Whole-job particle-steps/s of `world` independent replicas timed by
+    the slowest one."""
+    return world * particles_per_rank * steps / (max_ms / 1e3)
+
+
 # ---------------------------------------------------------------------------
 def reference_sample(ppc, steps, warmup, seed):
     """Time the reference's own step loop (oracle/_ref/libref_p2.so, or the
@@ -248,11 +265,7 @@ def run_upic(args):
             dist.barrier()
 
     def allmax(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(x, dist, "cuda")
 
     # host inputs in pinned memory (seed differs per replica)
     p = up.generate_bimaxwellian(w["nx"], w["ny"], w["L"], w["L"], w["ppc"], w["uth"],
@@ -302,7 +315,7 @@ def run_upic(args):
     push_ms, push_n, launches1 = sim.profile_read()
     sim.profile_enable(False)
     gpu_launches = launches1 - launches0
-    value = world * np_total * args.steps / (t_ms / 1e3)
+    value = replica_throughput(world, np_total, args.steps, t_ms)
     push_avg_s = push_ms / max(push_n, 1) / 1e3
     peak, peak_kind = measured_hbm_peak()
     achieved = ALG_BYTES_PER_PARTICLE * np_total / push_avg_s / 1e9

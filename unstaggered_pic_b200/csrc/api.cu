@@ -479,9 +479,11 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
     c->dx = cfg->Lx / cfg->nx;
     c->dy = cfg->Ly / cfg->ny;
     c->dA = c->dx * c->dy;
+    // Defaults from a sweep on the 512x512, 256 e-/cell workload: re-sort
+    // every 4 steps, 8x8-cell tiles, 2 guard cells.
     c->sort_interval = cfg->sort_interval > 0 ? cfg->sort_interval : 4;
-    const int tile = cfg->tile > 0 ? cfg->tile : 16;
-    const int guard = cfg->guard >= 0 ? cfg->guard : 3;
+    const int tile = cfg->tile > 0 ? cfg->tile : 8;
+    const int guard = cfg->guard >= 0 ? cfg->guard : 2;
     c->tg = make_tiles(c->nx, c->ny, tile, guard);
 
     auto bail = [&](int rc) {

@@ -22,12 +22,13 @@ constexpr int kPushWarps = kPushThreads / kWarp;
 constexpr int kKeyNone = -1;
 constexpr int kKeyEscape = -2;
 
-// Per-warp staging: the NV = 9*NCOMP deposit products of each of the warp's
-// 32 particles (weight of stencil node ab times deposit value c).
+// Per-warp staging: one row per particle with its 9 tensor-product stencil
+// weights S_ab and its NCOMP deposit values (q v_c / dA, or q / dA).
 template <int NCOMP>
 struct StageLayout {
-    static constexpr int kNV = 9 * NCOMP;
-    static constexpr int kDoubles = 32 * kNV;
+    static constexpr int kNV = 9 * NCOMP;   // values reduced per particle
+    static constexpr int kRow = 9 + NCOMP;  // doubles staged per particle
+    static constexpr int kDoubles = 32 * kRow;
 };
 
 UPIC_D int acc_slot(int ncomp, int c) { return ncomp == 1 ? 3 : c; }
@@ -59,9 +60,10 @@ UPIC_D void fold_window(const unsigned long long* whi, const unsigned long long*
 }
 
 template <int MODE, int NCOMP, bool UNIFORM>
-__global__ void __launch_bounds__(kPushThreads, 2)
+__global__ void __launch_bounds__(kPushThreads, 3)
 push_deposit_kernel(PushArgs a, TileGeom tg) {
     constexpr int NV = StageLayout<NCOMP>::kNV;
+    constexpr int RW = StageLayout<NCOMP>::kRow;
     constexpr int NPER = (NV + 31) / 32;
     extern __shared__ unsigned long long smem_u64[];
     const int WN = tg.wx * tg.wy;
@@ -81,12 +83,13 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
     // values owned by this lane in the segmented reduction: t = lane + 32 r is
     // stencil node ab = t / NCOMP (a = ab/3 along x, b = ab%3 along y) and
     // deposit component c = t % NCOMP
-    int t_off[NPER], t_a[NPER], t_b[NPER], t_c[NPER];
+    int t_off[NPER], t_a[NPER], t_b[NPER], t_c[NPER], t_ab[NPER];
     double t_scale[NPER];
 #pragma unroll
     for (int r = 0; r < NPER; ++r) {
         const int t = lane + 32 * r;
         const int ab = t < NV ? t / NCOMP : 0;
+        t_ab[r] = ab;
         t_a[r] = ab / 3;
         t_b[r] = ab % 3;
         t_c[r] = t < NV ? t - ab * NCOMP : 0;
@@ -121,8 +124,8 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
             double dwx[3], dwy[3], dval[NCOMP];
             if (active) {
                 const double q = UNIFORM ? a.q0 : a.p.q[p];
-                double x = a.p.x[p], y = a.p.y[p];
-                double v0 = a.p.vx[p], v1 = a.p.vy[p], v2 = a.p.vz[p];
+                double x = __ldcs(a.p.x + p), y = __ldcs(a.p.y + p);
+                double v0 = __ldcs(a.p.vx + p), v1 = __ldcs(a.p.vy + p), v2 = __ldcs(a.p.vz + p);
                 if (MODE == kModePush) {
                     // spectral_pic_part3.cpp:1050-1055: x^n = x^{n-1} + dt v^{n-1}
                     x = wrap_periodic(x + a.dt * v0, a.Lx, a.inv_Lx);
@@ -153,14 +156,14 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                         }
                     }
                     // IAEM momentum update (:1072-1090)
-                    const double w0 = a.p.wx[p], w1 = a.p.wy[p], w2 = a.p.wz[p];
+                    const double w0 = __ldcs(a.p.wx + p), w1 = __ldcs(a.p.wy + p), w2 = __ldcs(a.p.wz + p);
                     const double vs0 = 2.0 * v0 - w0, vs1 = 2.0 * v1 - w1, vs2 = 2.0 * v2 - w2;
                     const double gdx = G[5] * vs0 + G[7] * vs1 + G[9] * vs2;
                     const double gdy = G[6] * vs0 + G[8] * vs1 + G[10] * vs2;
                     const double qdt = q * a.dt;
-                    const double P0 = a.p.Px[p] + qdt * (gdx - G[3]);
-                    const double P1 = a.p.Py[p] + qdt * (gdy - G[4]);
-                    const double P2 = a.p.Pz[p];
+                    const double P0 = __ldcs(a.p.Px + p) + qdt * (gdx - G[3]);
+                    const double P1 = __ldcs(a.p.Py + p) + qdt * (gdy - G[4]);
+                    const double P2 = __ldcs(a.p.Pz + p);
                     // velocity_from_canonical (:602-607)
                     const double m = UNIFORM ? a.m0 : a.p.m[p];
                     const double p0 = P0 - q * G[0], p1 = P1 - q * G[1], p2 = P2 - q * G[2];
@@ -168,16 +171,16 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                     const double arg = c2 * (p0 * p0 + p1 * p1 + p2 * p2) + mc2 * mc2;
                     const double s = arg == 0.0 ? 0.0 : c2 * rsqrt(arg);
                     const double n0v = s * p0, n1v = s * p1, n2v = s * p2;
-                    a.p.x[p] = x;
-                    a.p.y[p] = y;
-                    a.p.Px[p] = P0;
-                    a.p.Py[p] = P1;
-                    a.p.wx[p] = v0;
-                    a.p.wy[p] = v1;
-                    a.p.wz[p] = v2;
-                    a.p.vx[p] = n0v;
-                    a.p.vy[p] = n1v;
-                    a.p.vz[p] = n2v;
+                    __stcs(a.p.x + p, x);
+                    __stcs(a.p.y + p, y);
+                    __stcs(a.p.Px + p, P0);
+                    __stcs(a.p.Py + p, P1);
+                    __stcs(a.p.wx + p, v0);
+                    __stcs(a.p.wy + p, v1);
+                    __stcs(a.p.wz + p, v2);
+                    __stcs(a.p.vx + p, n0v);
+                    __stcs(a.p.vy + p, n1v);
+                    __stcs(a.p.vz + p, n2v);
                     v0 = n0v;
                     v1 = n1v;
                     v2 = n2v;
@@ -244,16 +247,14 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
             }
             if (key == kKeyEscape) row = nvalid + __popc(esc & lt);
             if (row >= 0) {
-                // stage the products q v_c S_ab / dA of this particle in its row
-                double* mine = sprod + row * NV;
+                // stage S_ab and q v_c / dA of this particle in its row
+                double* mine = sprod + row * RW;
 #pragma unroll
                 for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
-                    for (int ib = 0; ib < 3; ++ib) {
-                        const double w = dwx[ia] * dwy[ib];
+                    for (int ib = 0; ib < 3; ++ib) mine[ia * 3 + ib] = dwx[ia] * dwy[ib];
 #pragma unroll
-                        for (int cc = 0; cc < NCOMP; ++cc) mine[(ia * 3 + ib) * NCOMP + cc] = dval[cc] * w;
-                    }
+                for (int cc = 0; cc < NCOMP; ++cc) mine[9 + cc] = dval[cc];
             }
             __syncwarp();
             // Particles whose stencil leaves the window (rare): exact fixed-point
@@ -270,7 +271,7 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                     for (int r = 0; r < NPER; ++r) {
                         const int t = lane + 32 * r;
                         if (t < NV) {
-                            const double v = sprod[erow * NV + t];
+                            const double v = sprod[erow * RW + 9 + t_c[r]] * sprod[erow * RW + t_ab[r]];
                             if (v != 0.0) {
                                 const int g = wrap_index(gxj + t_a[r], nx) * ny + wrap_index(gyj + t_b[r], ny);
                                 const int sl = acc_slot(NCOMP, t_c[r]);
@@ -300,11 +301,12 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                         if (t < NV) {
                             double s0 = 0.0, s1 = 0.0;
                             int j = rs;
+                            const int iw = t_ab[r], iv = 9 + t_c[r];
                             for (; j + 1 < re; j += 2) {
-                                s0 += sprod[j * NV + t];
-                                s1 += sprod[(j + 1) * NV + t];
+                                s0 = fma(sprod[j * RW + iv], sprod[j * RW + iw], s0);
+                                s1 = fma(sprod[(j + 1) * RW + iv], sprod[(j + 1) * RW + iw], s1);
                             }
-                            if (j < re) s0 += sprod[j * NV + t];
+                            if (j < re) s0 = fma(sprod[j * RW + iv], sprod[j * RW + iw], s0);
                             const double sum = s0 + s1;
                             if (sum != 0.0) {
                                 int widx;
@@ -672,7 +674,7 @@ long launches_total() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 int push_deposit_smem_bytes(const TileGeom& tg, int ncomp) {
     const int WN = tg.wx * tg.wy;
     const int window = 2 * ncomp * WN * 8;
-    const int stage = kPushWarps * (32 * 9 * ncomp * 8 + 32 * 4);
+    const int stage = kPushWarps * (32 * (9 + ncomp) * 8 + 32 * 4);
     const int bytes = window + stage;
     const int red = kPushWarps * 5 * 8;
     return bytes > red ? bytes : red;
