@@ -47,7 +47,8 @@ enum {
     UPIC_ERR_NONCONVERGED = -6,   /* outer nonlinear solve failed (NonlinearSolveFailure) */
     UPIC_ERR_LOCAL_PARTICLE = -7, /* per-particle local solve failed */
     UPIC_ERR_SUPERLUMINAL = -8,   /* |v| >= c in a relativistic iterate */
-    UPIC_ERR_NOMEM = -9           /* device allocation failed */
+    UPIC_ERR_NOMEM = -9,          /* device allocation failed */
+    UPIC_ERR_TOO_LARGE = -10      /* size exceeds a fixed capacity (UPIC_NOALLOC_MAX_NODES) */
 };
 
 /* Methods.  BDF1/BDF2: explicit spectral GM step with IAEM push,
@@ -206,6 +207,29 @@ int upic_poisson(upic_ctx* ctx, const double* rho, double* phi);
 /* One BDF Helmholtz solve (solve_bdf_wave_scalar, spectral_pic_part3.cpp:829-848):
  * hist holds u^n, u^{n-1}, ... (2 fields for BDF1, 4 for BDF2). */
 int upic_solve_bdf(upic_ctx* ctx, const double* source, const double* hist, double* out);
+
+/* Largest grid (nx*ny nodes) upic_deposit_current_noalloc accepts: its
+ * scratch is a fixed 6*UPIC_NOALLOC_MAX_NODES+2 uint64 array (3 MiB). */
+#define UPIC_NOALLOC_MAX_NODES 65536
+
+/* Current deposit that allocates nothing -- no counterpart in the reference.
+ * Same result as upic_deposit_current (J = sum_p q v S(x_p)/dA, quadratic
+ * B-spline, x in [0,Lx)), for callers that may not call cudaMalloc: hosts
+ * that reserve all device memory up front through their own allocator, or
+ * loops that cannot risk the device synchronization an allocation may
+ * cause.  x, y (np), v (3*np xyz triples), q (np) and J (3*nx*ny) are DEVICE
+ * pointers owned by the caller; work is queued on `stream` (a cudaStream_t,
+ * NULL = default stream) and J is complete when the stream reaches it.
+ * Scratch lives in one fixed __device__ array per GPU (3 MiB, held by every
+ * GPU that loads the library until exit).  The first call on a device
+ * resolves that array's device address, so make the first call on each
+ * device before any stream capture.  Every call uses the same array and
+ * clears it first: calls that overlap on the GPU (different streams, or
+ * host threads sharing a device) race and must be serialized by the caller.
+ * Returns UPIC_ERR_TOO_LARGE when nx*ny > UPIC_NOALLOC_MAX_NODES. */
+int upic_deposit_current_noalloc(int nx, int ny, double Lx, double Ly, long np, const double* x,
+                                 const double* y, const double* v, const double* q, double* J,
+                                 void* stream);
 
 /* Seeded synthetic plasma generator (splitmix64 + Box-Muller, independent of
  * any C++ library's distributions): np_per_cell electrons per cell at uniform

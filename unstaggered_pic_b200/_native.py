@@ -15,7 +15,7 @@ c_ip = ctypes.POINTER(ctypes.c_int)
 UPIC_ERR = {
     -1: "UPIC_ERR_CONFIG", -2: "UPIC_ERR_ARGUMENT", -3: "UPIC_ERR_CUDA", -4: "UPIC_ERR_STATE",
     -5: "UPIC_ERR_NONFINITE", -6: "UPIC_ERR_NONCONVERGED", -7: "UPIC_ERR_LOCAL_PARTICLE",
-    -8: "UPIC_ERR_SUPERLUMINAL", -9: "UPIC_ERR_NOMEM",
+    -8: "UPIC_ERR_SUPERLUMINAL", -9: "UPIC_ERR_NOMEM", -10: "UPIC_ERR_TOO_LARGE",
 }
 
 # Exported C symbols with (restype, argtypes); the ABI test checks each one.
@@ -42,6 +42,10 @@ SYMBOLS = {
     "upic_spectral_derivative": (ctypes.c_int, [ctypes.c_void_p, c_dp, ctypes.c_int, c_dp]),
     "upic_poisson": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp]),
     "upic_solve_bdf": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp, c_dp]),
+    "upic_deposit_current_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                    ctypes.c_double, ctypes.c_long, ctypes.c_void_p,
+                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_void_p, ctypes.c_void_p]),
     "upic_generate_bimaxwellian": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                                   ctypes.c_double, c_dp, c_dp, ctypes.c_uint64]
