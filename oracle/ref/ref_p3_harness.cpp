@@ -1,0 +1,219 @@
+// Test infrastructure only: a C-ABI harness around the reference's implicit
+// energy-conserving GM-HC-CN solver (Project3/ec_pic_nyquist_projected.cpp).
+//
+// Same pattern as the reference's own regression harness
+// (Project3/tests/test_solver.cpp:3-5): the solver translation unit is
+// included with `main` renamed, and the `static` functions run unmodified on
+// injected particles and fields.  Built by oracle/Makefile into
+// oracle/_ref/libref_p3.so (serial: no -fopenmp).
+
+#include <new>
+
+#define main upic_ref_p3_cli_main
+#include "ec_pic_nyquist_projected.cpp"
+#undef main
+
+#include <chrono>
+#include <cstring>
+
+namespace {
+
+// dparams / iparams layout shared with oracle/p3_oracle.c and the tests.
+enum {
+    D_LX, D_LY, D_LZ, D_DT, D_KAPPA, D_SIGMA1, D_SIGMA2, D_N0, D_NL_RTOL, D_NL_ATOL,
+    D_AND_DAMP, D_AND_REG, D_AND_GROWTH, D_LOC_RTOL, D_LOC_ATOL, D_LOC_DAMP, D_COUNT
+};
+enum {
+    I_NX, I_NY, I_NZ, I_ORDER, I_NQ, I_SPLIT, I_NYQ, I_NL_MAXIT, I_AND_MEM, I_AND_START,
+    I_LOC_MAXIT, I_SOLVER, I_NSTEPS, I_MODE, I_COUNT
+};
+constexpr int kDiag = 22;
+constexpr int kInfo = 8;
+
+Config make_cfg(const double* d, const int* ip) {
+    Config c;
+    c.nx = ip[I_NX]; c.ny = ip[I_NY]; c.nz = ip[I_NZ];
+    c.Lx = d[D_LX]; c.Ly = d[D_LY]; c.Lz = d[D_LZ];
+    c.dt = d[D_DT];
+    c.kappa = d[D_KAPPA]; c.sigma1 = d[D_SIGMA1]; c.sigma2 = d[D_SIGMA2];
+    c.n0 = d[D_N0];
+    c.spline_order = ip[I_ORDER];
+    c.orbit_quad_order = ip[I_NQ];
+    c.split_orbit_at_knots = ip[I_SPLIT] != 0;
+    c.nyquist_projection = ip[I_NYQ] != 0;
+    c.nonlinear_solver = ip[I_SOLVER] == 1 ? "picard" : "anderson_quasi_newton";
+    c.nonlinear_rtol = d[D_NL_RTOL];
+    c.nonlinear_atol = d[D_NL_ATOL];
+    c.nonlinear_max_iter = ip[I_NL_MAXIT];
+    c.anderson_memory = ip[I_AND_MEM];
+    c.anderson_start = ip[I_AND_START];
+    c.anderson_damping = d[D_AND_DAMP];
+    c.anderson_regularization = d[D_AND_REG];
+    c.anderson_growth_limit = d[D_AND_GROWTH];
+    c.uniform_local_rtol = d[D_LOC_RTOL];
+    c.uniform_local_atol = d[D_LOC_ATOL];
+    c.uniform_local_max_iter = ip[I_LOC_MAXIT];
+    c.uniform_local_damping = d[D_LOC_DAMP];
+    c.uniform_particle_subcycling = false;
+    c.selective_particle_fallback = false;
+    c.adaptive_dt = false;
+    c.run_unit_tests = false;
+    c.output_prefix = "/tmp/upic_ref_p3";
+    return c;
+}
+
+void store_diag(const Diagnostics& d, double* o) {
+    const double v[kDiag] = {d.gauss_rms, d.gauss_max, d.divE_rms, d.sigma1_rho_rms,
+                             d.gauss_normalization_rms, d.gauss_relative, d.gauge_rms,
+                             d.gauge_max, d.psi_over_kappa2_rms, d.divA_rms,
+                             d.gauge_normalization_rms, d.gauge_relative, d.field_energy,
+                             d.kinetic_energy, d.total_energy, d.rho_mode, d.E_mode_re,
+                             d.E_mode_im, d.E_mode_abs, d.Bz_y_mode_re, d.Bz_y_mode_im,
+                             d.Bz_y_mode_abs};
+    std::memcpy(o, v, sizeof(v));
+}
+
+void copy_vec3(const std::vector<Vec3>& a, double* out) {
+    for (std::size_t p = 0; p < a.size(); ++p)
+        for (int d = 0; d < 3; ++d) out[3 * p + d] = a[p][d];
+}
+
+}  // namespace
+
+extern "C" {
+
+// Gauss-Legendre nodes and weights on [0,1] (gauss_legendre_01, :2479).
+int ref_p3_gauss_legendre(int n, double* s, double* w) {
+    Quadrature q = gauss_legendre_01(n);
+    for (int i = 0; i < n; ++i) { s[i] = q.s[i]; w[i] = q.w[i]; }
+    return 0;
+}
+
+// Orbit-averaged current deposit (path_average_deposit_current, :2784).
+int ref_p3_orbit_deposit(const double* d, const int* ip, long np, const double* x0,
+                         const double* dx, const double* vbar, const double* q, double* J) {
+    Config c = make_cfg(d, ip);
+    Grid g = make_grid(c);
+    Quadrature quad = gauss_legendre_01(c.orbit_quad_order);
+    std::vector<Vec3> X(np), DX(np), V(np);
+    std::vector<Real> Q(q, q + np);
+    for (long p = 0; p < np; ++p)
+        for (int k = 0; k < 3; ++k) {
+            X[p][k] = x0[3 * p + k];
+            DX[p][k] = dx[3 * p + k];
+            V[p][k] = vbar[3 * p + k];
+        }
+    VecField Jf = path_average_deposit_current(X, DX, V, Q, g, c.spline_order, quad,
+                                               c.split_orbit_at_knots, nullptr);
+    for (int k = 0; k < 3; ++k) std::memcpy(J + (std::size_t)k * g.N, Jf[k].data(), sizeof(double) * g.N);
+    return 0;
+}
+
+// Fused orbit gather + D_A (path_average_gather_and_gradient, :3016):
+// gathered (3 per particle) and gradient (9 per particle, [comp][dir]).
+int ref_p3_orbit_gather(const double* d, const int* ip, long np, const double* x0,
+                        const double* dx, const double* mesh, const double* An,
+                        const double* Anp1, double* gathered, double* grad) {
+    Config c = make_cfg(d, ip);
+    Grid g = make_grid(c);
+    Quadrature quad = gauss_legendre_01(c.orbit_quad_order);
+    std::vector<Vec3> X(np), DX(np);
+    for (long p = 0; p < np; ++p)
+        for (int k = 0; k < 3; ++k) {
+            X[p][k] = x0[3 * p + k];
+            DX[p][k] = dx[3 * p + k];
+        }
+    VecField M, A0, A1;
+    for (int k = 0; k < 3; ++k) {
+        M[k].assign(mesh + (std::size_t)k * g.N, mesh + (std::size_t)(k + 1) * g.N);
+        A0[k].assign(An + (std::size_t)k * g.N, An + (std::size_t)(k + 1) * g.N);
+        A1[k].assign(Anp1 + (std::size_t)k * g.N, Anp1 + (std::size_t)(k + 1) * g.N);
+    }
+    OrbitGatherGradient o = path_average_gather_and_gradient(X, DX, M, A0, A1, g, c.spline_order,
+                                                             quad, c.split_orbit_at_knots);
+    for (long p = 0; p < np; ++p) {
+        for (int k = 0; k < 3; ++k) gathered[3 * p + k] = o.gathered[p][k];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) grad[9 * p + 3 * a + b] = o.gradient[p][a][b];
+    }
+    return 0;
+}
+
+// Injected start-up state (the tail of initialize_weibel_filamentation_3d,
+// :4061-4123, with the caller's particles, A = U = 0) followed by n_steps of
+// nonlinear_step_orbit (:6477) and compute_diagnostics (:3521) per step.
+//   x, v: 3*np in/out (positions in [-L/2, L/2)); P, v_prev, vbar: 3*np out
+//   diag: (n_steps+1) x 22; info: n_steps x 8 {iterations, converged,
+//   final_rms_residual, final_max_particle_residual, local_iter_max,
+//   local_iter_mean, anderson_steps, picard_steps}; fields (optional): phi,
+//   psi, rho, A(3), U(3), J(3) = 12 x N after the last step.
+int ref_p3_run(const double* d, const int* ip, long np, double* x, double* v, double* P,
+               double* v_prev, double* vbar, const double* q, const double* m, double* diag,
+               double* info, double* fields, double* seconds) {
+    try {
+        Config c = make_cfg(d, ip);
+        Grid g = make_grid(c);
+        Quadrature quad = gauss_legendre_01(c.orbit_quad_order);
+        State st;
+        st.x.resize(np); st.v.resize(np); st.v_prev.resize(np); st.vbar_last.resize(np);
+        st.P.resize(np); st.q.assign(q, q + np); st.m.assign(m, m + np);
+        for (long p = 0; p < np; ++p)
+            for (int k = 0; k < 3; ++k) {
+                st.x[p][k] = x[3 * p + k];
+                st.v[p][k] = v[3 * p + k];
+            }
+        for (auto& xx : st.x) xx = wrap_pos(xx, g.L);
+        Field rho_e = deposit_scalar_to_mesh(st.x, st.q, g, c.spline_order, true);
+        st.rho.assign(g.N, 0.0);
+        for (int id = 0; id < g.N; ++id) st.rho[id] = rho_e[id] + c.n0;
+        subtract_mean(st.rho);
+        st.phi = solve_periodic_poisson_for_phi(st.rho, g, c.sigma1);
+        st.psi.assign(g.N, 0.0);
+        st.A = zero_vecfield(g.N);
+        st.U = zero_vecfield(g.N);
+        st.J = deposit_current_to_mesh(st.x, st.v, st.q, g, c.spline_order);
+        for (long p = 0; p < np; ++p) {
+            const Vec3 pm = momentum_from_v(st.v[p], st.m[p], c.kappa);
+            const Vec3 A0p = gather_vector_at(st.A, st.x[p], g, c.spline_order);
+            st.P[p] = add3(pm, mul3(st.q[p], A0p));
+        }
+        project_initial_state(st, g, c);
+        initialize_relativistic_history_velocity(st, g, c);
+        const int mode = ip[I_MODE];
+        if (diag) store_diag(compute_diagnostics(st, g, c.sigma1, c.sigma2, c.kappa, mode), diag);
+        const auto t0 = std::chrono::steady_clock::now();
+        for (int s = 1; s <= ip[I_NSTEPS]; ++s) {
+            std::vector<NonlinearHistoryEntry> hist;
+            NonlinearSolveInfo si;
+            st = nonlinear_step_orbit(st, g, c, quad, hist, &si, (s - 1) * c.dt);
+            if (diag) store_diag(compute_diagnostics(st, g, c.sigma1, c.sigma2, c.kappa, mode),
+                                 diag + (std::size_t)kDiag * s);
+            if (info) {
+                double* o = info + (std::size_t)kInfo * (s - 1);
+                o[0] = si.iterations; o[1] = si.converged; o[2] = si.final_rms_residual;
+                o[3] = si.final_max_particle_residual; o[4] = si.local_particle_iterations_max;
+                o[5] = si.local_particle_iterations_mean; o[6] = si.anderson_steps;
+                o[7] = si.picard_fallback_steps;
+            }
+        }
+        const auto t1 = std::chrono::steady_clock::now();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+        copy_vec3(st.x, x);
+        copy_vec3(st.v, v);
+        copy_vec3(st.P, P);
+        copy_vec3(st.v_prev, v_prev);
+        copy_vec3(st.vbar_last, vbar);
+        if (fields) {
+            const Field* f[12] = {&st.phi, &st.psi, &st.rho, &st.A[0], &st.A[1], &st.A[2],
+                                  &st.U[0], &st.U[1], &st.U[2], &st.J[0], &st.J[1], &st.J[2]};
+            for (int k = 0; k < 12; ++k)
+                std::memcpy(fields + (std::size_t)k * g.N, f[k]->data(), sizeof(double) * g.N);
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_p3_run: %s\n", e.what());
+        return -1;
+    }
+}
+
+}  // extern "C"

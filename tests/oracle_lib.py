@@ -94,3 +94,80 @@ def init_weibel(lib_fn, nx, ny, Lx, Ly, ppc, c=1.0, n0=1.0, vx=0.5, vy_max=0.01,
                ptr(a["v"]), ptr(a["vprev"]), ptr(a["q"]), ptr(a["m"]))
     assert n == cap, (n, cap)
     return a
+
+
+# ---------------------------------------------------------------------------
+# Project3 (implicit GM-HC-CN) runs: dparams / iparams layout of
+# oracle/ref/ref_p3_harness.cpp and oracle/p3_oracle.c.
+REF_P3_SO = os.path.join(ROOT, "oracle", "_ref", "libref_p3.so")
+P3_NDIAG = 22
+P3_NINFO = 8
+P3_DIAG_NAMES = ["gauss_rms", "gauss_max", "divE_rms", "sigma1_rho_rms", "gauss_normalization_rms",
+                 "gauss_relative", "gauge_rms", "gauge_max", "psi_over_kappa2_rms", "divA_rms",
+                 "gauge_normalization_rms", "gauge_relative", "field_energy", "kinetic_energy",
+                 "total_energy", "rho_mode", "E_mode_re", "E_mode_im", "E_mode_abs", "Bz_y_mode_re",
+                 "Bz_y_mode_im", "Bz_y_mode_abs"]
+
+
+def ref_p3():
+    return _load(REF_P3_SO)
+
+
+class P3Problem:
+    def __init__(self, nx, ny, Lx, Ly, dt, nz=1, Lz=1.0, kappa=1.0, sigma1=1.0, sigma2=1.0, n0=1.0,
+                 order=2, nq=8, split=True, nyquist=True, nl_rtol=1e-11, nl_atol=1e-13,
+                 nl_maxit=80, and_mem=4, and_start=2, and_damp=0.5, and_reg=1e-12,
+                 and_growth=1.2, loc_rtol=1e-12, loc_atol=1e-14, loc_maxit=64, loc_damp=1.0,
+                 solver="anderson", n_steps=1, mode=1):
+        self.__dict__.update(locals())
+        del self.__dict__["self"]
+
+    def dparams(self):
+        return np.array([self.Lx, self.Ly, self.Lz, self.dt, self.kappa, self.sigma1, self.sigma2,
+                         self.n0, self.nl_rtol, self.nl_atol, self.and_damp, self.and_reg,
+                         self.and_growth, self.loc_rtol, self.loc_atol, self.loc_damp])
+
+    def iparams(self):
+        return np.array([self.nx, self.ny, self.nz, self.order, self.nq, int(self.split),
+                         int(self.nyquist), self.nl_maxit, self.and_mem, self.and_start,
+                         self.loc_maxit, 1 if self.solver == "picard" else 0, self.n_steps,
+                         self.mode], dtype=np.int32)
+
+
+def p3_run(fn, prob, x, v, q, m, want_fields=True):
+    """Run fn (ref_p3_run / o3_run) on copies: x, v (np, 3).  Returns dict
+    with x, v, P, v_prev, vbar, diag (n_steps+1, 22), info (n_steps, 8),
+    fields (12, nx, ny) and seconds."""
+    n = len(q)
+    out = {"x": np.ascontiguousarray(x, dtype=np.float64).copy(),
+           "v": np.ascontiguousarray(v, dtype=np.float64).copy(),
+           "P": np.zeros((n, 3)), "v_prev": np.zeros((n, 3)), "vbar": np.zeros((n, 3))}
+    diag = np.full((prob.n_steps + 1, P3_NDIAG), np.nan)
+    info = np.full((max(prob.n_steps, 1), P3_NINFO), np.nan)
+    N = prob.nx * prob.ny * prob.nz
+    fields = np.zeros((12, N)) if want_fields else None
+    secs = np.zeros(1)
+    rc = fn(ptr(prob.dparams()), ptr(prob.iparams()), ctypes.c_long(n), ptr(out["x"]), ptr(out["v"]),
+            ptr(out["P"]), ptr(out["v_prev"]), ptr(out["vbar"]),
+            ptr(np.ascontiguousarray(q, dtype=np.float64)), ptr(np.ascontiguousarray(m, dtype=np.float64)),
+            ptr(diag), ptr(info), ptr(fields), ptr(secs))
+    if rc != 0:
+        raise RuntimeError("p3 run failed")
+    out.update(diag=diag, info=info[:prob.n_steps], seconds=float(secs[0]))
+    if fields is not None:
+        out["fields"] = fields.reshape(12, prob.nx, prob.ny * prob.nz)
+    return out
+
+
+def p3_particles(rng, nx, ny, ppc, Lx, Ly, uth=(0.02, 0.2, 0.0), n0=1.0, Lz=1.0):
+    """Random electrons in [-L/2, L/2) (Project3's coordinates), normalized
+    momentum u = gamma v Maxwellian with spreads uth, q/m = -1, neutralizing n0."""
+    n = nx * ny * ppc
+    x = np.zeros((n, 3))
+    x[:, 0] = rng.uniform(-Lx / 2, Lx / 2, n)
+    x[:, 1] = rng.uniform(-Ly / 2, Ly / 2, n)
+    u = rng.normal(size=(n, 3)) * np.asarray(uth)
+    gam = np.sqrt(1 + (u * u).sum(1))
+    v = u / gam[:, None]
+    q = np.full(n, -n0 * Lx * Ly * Lz / n)
+    return x, v, q, np.abs(q)

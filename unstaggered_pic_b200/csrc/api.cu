@@ -16,82 +16,18 @@
 #include <string>
 #include <vector>
 
-#include "../../include/upic.h"
-#include "kernels.h"
 #include "upic_common.cuh"
 
+#include "context.h"
+
 using namespace upic;
+using namespace upic_host;
 
 namespace {
-
-constexpr int kHistSlots = 5;
-constexpr int kDiagFields = 10;
-constexpr int kRedGrid = 148 * 2;
-
 thread_local std::string g_create_error;
-
 }  // namespace
 
-struct upic_ctx {
-    upic_config cfg{};
-    std::string err;
-    int nx = 0, ny = 0, N = 0;
-    double dx = 0, dy = 0, dA = 0;
-    cudaStream_t own = nullptr, st = nullptr;
-    int device = 0, nsm = 148;
-
-    FftPlan plan{};
-    double2* d_twx = nullptr;
-    double2* d_twy = nullptr;
-    double *d_kx = nullptr, *d_ky = nullptr, *d_k2 = nullptr;
-
-    // particle state
-    long np = 0, cap = 0;
-    ParticleSoA P[2];
-    int cur = 0;
-    bool uniform_qm = true;
-    double q0 = 0, m0 = 0;
-    double scale[4] = {1, 1, 1, 1};
-    double* d_tmp3 = nullptr;  // 3*cap staging for xyz triples
-
-    // kernel-level entry points use their own particle buffers
-    long kcap = 0;
-    ParticleSoA K[2];
-
-    // grid state
-    unsigned long long* d_acc = nullptr;
-    double* d_J = nullptr;
-    double* d_rho = nullptr;
-    double* d_gf = nullptr;
-    double2* d_spec = nullptr;
-    double2* d_hist = nullptr;
-    double2* d_dspec = nullptr;
-    double* d_dreal = nullptr;
-    double* d_partials = nullptr;
-    double* d_pdiag = nullptr;
-    double* d_row = nullptr;
-    double* h_row = nullptr;  // pinned
-
-    int head = 0;
-    long steps = 0;
-    bool fields_ready = false;
-    int steps_since_sort = 0;
-    int sort_interval = 4;
-
-    // profiling: CUDA events around every particle push kernel
-    bool profiling = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
-
-    TileGeom tg{};
-    SortWork sw{};
-    SortWork ksw{};
-    int push_grid = 148;
-
-    std::vector<void*> allocs;
-};
-
-// ---------------------------------------------------------------------------
-namespace {
+namespace upic_host {
 
 int fail(upic_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
@@ -99,21 +35,13 @@ int fail(upic_ctx* c, int code, const std::string& msg) {
     return code;
 }
 
-#define UPIC_CUDA(ctx, call)                                                               \
-    do {                                                                                   \
-        cudaError_t e_ = (call);                                                           \
-        if (e_ != cudaSuccess)                                                             \
-            return fail(ctx, UPIC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-template <typename T>
-int dalloc(upic_ctx* c, T** p, size_t count) {
+int dalloc_bytes(upic_ctx* c, void** p, size_t bytes) {
     void* v = nullptr;
-    cudaError_t e = cudaMalloc(&v, sizeof(T) * (count ? count : 1));
+    cudaError_t e = cudaMalloc(&v, bytes);
     if (e != cudaSuccess)
         return fail(c, UPIC_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     c->allocs.push_back(v);
-    *p = reinterpret_cast<T*>(v);
+    *p = v;
     return 0;
 }
 
@@ -143,20 +71,27 @@ std::vector<double2> twiddles(int n) {
     return t;
 }
 
-TileGeom make_tiles(int nx, int ny, int tile, int guard) {
+// A tiled axis' window covers the nodes that the stencils of particles in
+// the tile, or up to `guard` cells outside it, can touch: `lo` nodes below
+// and `hi` nodes above a particle's key cell.  An axis whose window would
+// cover the whole axis becomes one periodic window.
+TileGeom make_tiles(int nx, int ny, int tile, int guard, int lo, int hi) {
     TileGeom g{};
     g.nx = nx;
     g.ny = ny;
     g.guard = guard;
+    g.lo = lo;
+    g.span = lo + hi + 1;
     auto axis = [&](int n, int& t, int& nt, int& w, int& full) {
         t = tile < n ? tile : n;
-        if (n <= tile + 2 * guard + 2) {
+        const int wt = t + 2 * guard + lo + hi;
+        if (n <= wt) {
             full = 1;
             t = n;
             w = n;
         } else {
             full = 0;
-            w = t + 2 * guard + 2;
+            w = wt;
         }
         nt = n / t;
     };
@@ -165,6 +100,8 @@ TileGeom make_tiles(int nx, int ny, int tile, int guard) {
     g.chunk = 2048;
     return g;
 }
+
+int iota(upic_ctx* c, int* id, long n);
 
 int alloc_soa(upic_ctx* c, ParticleSoA& s, long cap, bool with_state, bool with_qm) {
     int rc = 0;
@@ -423,7 +360,7 @@ void clear_profile(upic_ctx* c) {
 
 int grid_ncomp(const upic_ctx* c) { return c->cfg.charge_update == UPIC_CHARGE_NAIVE ? 4 : 3; }
 
-}  // namespace
+}  // namespace upic_host
 
 // ===========================================================================
 extern "C" {
@@ -484,7 +421,7 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
     c->sort_interval = cfg->sort_interval > 0 ? cfg->sort_interval : 4;
     const int tile = cfg->tile > 0 ? cfg->tile : 8;
     const int guard = cfg->guard >= 0 ? cfg->guard : 2;
-    c->tg = make_tiles(c->nx, c->ny, tile, guard);
+    c->tg = make_tiles(c->nx, c->ny, tile, guard, 1, 1);
 
     auto bail = [&](int rc) {
         g_create_error = c->err;

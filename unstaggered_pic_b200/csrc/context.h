@@ -1,0 +1,138 @@
+// Device context shared by the C-ABI implementation files (api.cu for the
+// explicit BDF/IAEM method, api_implicit.cu for the implicit orbit-averaged
+// GM-HC-CN method).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/upic.h"
+#include "kernels.h"
+
+namespace upic_host {
+
+constexpr int kHistSlots = 5;
+constexpr int kDiagFields = 10;
+constexpr int kRedGrid = 148 * 2;
+
+struct ImplicitState;  // api_implicit.cu
+
+}  // namespace upic_host
+
+using upic::FftPlan;
+using upic::ParticleSoA;
+using upic::SortWork;
+using upic::TileGeom;
+
+struct upic_ctx {
+    upic_config cfg{};
+    std::string err;
+    int nx = 0, ny = 0, N = 0;
+    double dx = 0, dy = 0, dA = 0;
+    cudaStream_t own = nullptr, st = nullptr;
+    int device = 0, nsm = 148;
+
+    FftPlan plan{};
+    double2* d_twx = nullptr;
+    double2* d_twy = nullptr;
+    double *d_kx = nullptr, *d_ky = nullptr, *d_k2 = nullptr;
+
+    // particle state
+    long np = 0, cap = 0;
+    ParticleSoA P[2];
+    int cur = 0;
+    bool uniform_qm = true;
+    double q0 = 0, m0 = 0;
+    double scale[4] = {1, 1, 1, 1};
+    double* d_tmp3 = nullptr;  // 3*cap staging for xyz triples
+
+    // kernel-level entry points use their own particle buffers
+    long kcap = 0;
+    ParticleSoA K[2];
+
+    // grid state
+    unsigned long long* d_acc = nullptr;
+    double* d_J = nullptr;
+    double* d_rho = nullptr;
+    double* d_gf = nullptr;
+    double2* d_spec = nullptr;
+    double2* d_hist = nullptr;
+    double2* d_dspec = nullptr;
+    double* d_dreal = nullptr;
+    double* d_partials = nullptr;
+    double* d_pdiag = nullptr;
+    double* d_row = nullptr;
+    double* h_row = nullptr;  // pinned
+
+    int head = 0;
+    long steps = 0;
+    bool fields_ready = false;
+    int steps_since_sort = 0;
+    int sort_interval = 4;
+
+    // profiling: CUDA events around every particle push kernel
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+
+    TileGeom tg{};
+    SortWork sw{};
+    SortWork ksw{};
+    int push_grid = 148;
+
+    std::vector<void*> allocs;
+
+    // implicit orbit-averaged method (api_implicit.cu); null for BDF methods
+    upic_host::ImplicitState* imp = nullptr;
+};
+
+namespace upic_host {
+
+using upic::ParticleSoA;
+using upic::SortWork;
+using upic::TileGeom;
+
+int fail(upic_ctx* c, int code, const std::string& msg);
+
+#define UPIC_CUDA(ctx, call)                                                                     \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return ::upic_host::fail(ctx, UPIC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int dalloc_bytes(upic_ctx* c, void** p, size_t bytes);
+template <typename T>
+int dalloc(upic_ctx* c, T** p, size_t count) {
+    void* v = nullptr;
+    const int rc = dalloc_bytes(c, &v, sizeof(T) * (count ? count : 1));
+    if (rc == 0) *p = reinterpret_cast<T*>(v);
+    return rc;
+}
+void dfree(upic_ctx* c, void* p);
+int sync(upic_ctx* c);
+int gridn(long n);
+int upload3(upic_ctx* c, const double* host, long n, double* a, double* b, double* d);
+int download3(upic_ctx* c, double* host, long n, const double* a, const double* b, const double* d);
+int ensure_tmp3(upic_ctx* c, long n);
+double fixed_scale(double bound);
+TileGeom make_tiles(int nx, int ny, int tile, int guard, int lo, int hi);
+int alloc_soa(upic_ctx* c, ParticleSoA& s, long cap, bool with_state, bool with_qm);
+void free_soa(upic_ctx* c, ParticleSoA& s);
+int alloc_sortwork(upic_ctx* c, SortWork& w, long cap, const TileGeom& tg);
+void free_sortwork(upic_ctx* c, SortWork& w);
+int iota(upic_ctx* c, int* id, long n);
+
+// implicit method (api_implicit.cu)
+int implicit_create(upic_ctx* c);
+void implicit_destroy(upic_ctx* c);
+int implicit_set_particles(upic_ctx* c, long np, const double* x, const double* y, const double* P,
+                           const double* v, const double* v_prev, const double* q, const double* m);
+int implicit_get_particles(upic_ctx* c, long np, double* x, double* y, double* P, double* v,
+                           double* v_prev);
+int implicit_init_fields(upic_ctx* c, double* diag_row);
+int implicit_get_field(upic_ctx* c, int which, double* host);
+
+}  // namespace upic_host

@@ -49,6 +49,8 @@ struct TileGeom {
     int tile_x, tile_y;   // cells per tile
     int ntx, nty;         // tiles per axis
     int guard;            // guard cells around a tile (tiled axes)
+    int lo;               // stencil nodes below a particle's key cell
+    int span;             // stencil nodes per axis
     int wx, wy;           // window extents in nodes
     int full_x, full_y;   // 1 if the axis window is the whole periodic axis
     int chunk;            // particles per chunk
