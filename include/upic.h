@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define UPIC_ABI_VERSION 1
+#define UPIC_ABI_VERSION 2
 
 /* Error codes. */
 enum {
@@ -52,8 +52,16 @@ enum {
 };
 
 /* Methods.  BDF1/BDF2: explicit spectral GM step with IAEM push,
- * Project2/spectral_pic_part3.cpp:1094-1189. */
-enum { UPIC_METHOD_BDF1 = 1, UPIC_METHOD_BDF2 = 2 };
+ * Project2/spectral_pic_part3.cpp:1094-1189.  CN_ORBIT: implicit
+ * energy-conserving orbit-averaged GM-HC-CN step (relativistic
+ * Higuera-Cary rotation, Crank-Nicolson potentials, outer Anderson/Picard
+ * iteration on the mesh current), Project3/ec_pic_nyquist_projected.cpp
+ * nonlinear_step_orbit:6477; runs in 2D (nz = 1). */
+enum { UPIC_METHOD_BDF1 = 1, UPIC_METHOD_BDF2 = 2, UPIC_METHOD_CN_ORBIT = 3 };
+
+/* Outer nonlinear solver of the implicit method (Config::nonlinear_solver,
+ * ec_pic_nyquist_projected.cpp:891). */
+enum { UPIC_SOLVER_ANDERSON = 0, UPIC_SOLVER_PICARD = 1 };
 
 /* Charge source: continuity-consistent (conserving) or redeposited (naive),
  * spectral_pic_part3.cpp:1147-1152. */
@@ -71,7 +79,11 @@ enum {
     UPIC_FIELD_JX = 5,
     UPIC_FIELD_JY = 6,
     UPIC_FIELD_JZ = 7,
-    UPIC_FIELD_COUNT = 8
+    UPIC_FIELD_PSI = 8,
+    UPIC_FIELD_UX = 9,
+    UPIC_FIELD_UY = 10,
+    UPIC_FIELD_UZ = 11,
+    UPIC_FIELD_COUNT = 12
 };
 
 /* Diagnostics row, the column order of the reference's _diagnostics.csv after
@@ -109,9 +121,46 @@ typedef struct upic_config {
     int tile;                /* deposit tile edge in cells; 0 = automatic */
     int guard;               /* deposit window guard in cells; -1 = automatic */
     int reserved[8];
+    /* Implicit method (UPIC_METHOD_CN_ORBIT): the Project3 deck keys
+     * (Config, ec_pic_nyquist_projected.cpp:837-1005).  Positions are in
+     * [-L/2, L/2) with node i at -L/2 + i*dx, as in Project3. */
+    double Lz;                     /* cell volume dV = dx*dy*Lz (nz = 1) */
+    double kappa, sigma1, sigma2;  /* nondimensional light speed and sources */
+    int spline_order;              /* 1..4 */
+    int orbit_quad_order;          /* Gauss-Legendre points per orbit segment */
+    int split_orbit_at_knots;
+    int nyquist_projection;
+    int nonlinear_solver;          /* UPIC_SOLVER_* */
+    int nonlinear_max_iter;
+    int anderson_memory;           /* 1..4 */
+    int anderson_start;
+    int local_max_iter;            /* particle_local_max_iter */
+    double nonlinear_rtol, nonlinear_atol;
+    double anderson_damping, anderson_regularization, anderson_growth_limit;
+    double local_rtol, local_atol, local_damping;  /* particle_local_* */
+    int perturbation_mode;         /* x (and y) Fourier mode of the diagnostics */
 } upic_config;
 
 typedef struct upic_ctx upic_ctx;
+
+/* Diagnostics row of the implicit method: the Diagnostics struct of
+ * ec_pic_nyquist_projected.cpp:3469-3519 (columns of its _diagnostics.csv). */
+enum {
+    UPIC_P3_GAUSS_RMS = 0, UPIC_P3_GAUSS_MAX, UPIC_P3_DIVE_RMS, UPIC_P3_SIGMA1_RHO_RMS,
+    UPIC_P3_GAUSS_NORM_RMS, UPIC_P3_GAUSS_RELATIVE, UPIC_P3_GAUGE_RMS, UPIC_P3_GAUGE_MAX,
+    UPIC_P3_PSI_OVER_KAPPA2_RMS, UPIC_P3_DIVA_RMS, UPIC_P3_GAUGE_NORM_RMS, UPIC_P3_GAUGE_RELATIVE,
+    UPIC_P3_FIELD_ENERGY, UPIC_P3_KINETIC_ENERGY, UPIC_P3_TOTAL_ENERGY, UPIC_P3_RHO_MODE,
+    UPIC_P3_E_MODE_RE, UPIC_P3_E_MODE_IM, UPIC_P3_E_MODE_ABS, UPIC_P3_BZ_Y_MODE_RE,
+    UPIC_P3_BZ_Y_MODE_IM, UPIC_P3_BZ_Y_MODE_ABS, UPIC_P3_DIAG_COUNT
+};
+
+/* Per-step solve report of the implicit method (NonlinearSolveInfo,
+ * ec_pic_nyquist_projected.cpp:5493-5533). */
+enum {
+    UPIC_INFO_ITERATIONS = 0, UPIC_INFO_CONVERGED, UPIC_INFO_FINAL_RMS_RESIDUAL,
+    UPIC_INFO_FINAL_MAX_PARTICLE_RESIDUAL, UPIC_INFO_LOCAL_ITER_MAX, UPIC_INFO_LOCAL_ITER_MEAN,
+    UPIC_INFO_ANDERSON_STEPS, UPIC_INFO_PICARD_STEPS, UPIC_INFO_COUNT
+};
 
 /* ABI version of the loaded library (UPIC_ABI_VERSION). */
 int upic_abi_version(void);
@@ -147,8 +196,20 @@ int upic_get_particles(upic_ctx* ctx, long np, double* x, double* y, double* P, 
 /* Start-up fields: rho0 = n0 + deposited electron charge, J0 = deposited
  * current, phi0 from Poisson, A0 = 0, all BDF histories filled with copies
  * (spectral_pic_part3.cpp:1100-1111).  If diag_row is not NULL it receives
- * the step-0 diagnostics row (BDF1 derivatives, :1121-1131). */
+ * the step-0 diagnostics row (BDF1 derivatives, :1121-1131).
+ * Implicit method: rho = deposited charge + n0 (zero mean), phi from
+ * Poisson, psi = A = U = 0, J deposited, P = m gamma v, v_prev from a
+ * backward Lorentz step (ec_pic_nyquist_projected.cpp:4061-4123, 3423);
+ * diag_row then has UPIC_P3_DIAG_COUNT entries. */
 int upic_init_fields(upic_ctx* ctx, double* diag_row);
+
+/* Advance nsteps implicit steps (nonlinear_step_orbit,
+ * ec_pic_nyquist_projected.cpp:6477, then compute_diagnostics :3521).
+ * diag (optional): nsteps x UPIC_P3_DIAG_COUNT; info (optional): nsteps x
+ * UPIC_INFO_COUNT.  A step that does not converge returns
+ * UPIC_ERR_NONCONVERGED, one whose per-particle solve fails returns
+ * UPIC_ERR_LOCAL_PARTICLE; the state then stays at the last accepted step. */
+int upic_step_implicit(upic_ctx* ctx, int nsteps, double* diag, double* info);
 
 /* Advance nsteps steps of the explicit BDF/IAEM method (loop body of
  * run_simulation, spectral_pic_part3.cpp:1133-1189).  diag (optional):
@@ -172,7 +233,8 @@ int upic_profile_read(upic_ctx* ctx, double* push_ms, long* push_launches, long*
 /* Number of steps taken since upic_init_fields. */
 int upic_step_count(const upic_ctx* ctx, long* steps);
 
-/* Fields of the current time level (phi, A, rho, J), nx*ny doubles. */
+/* Fields of the current time level (phi, A, rho, J; implicit method also
+ * psi = d phi/dt and U = dA/dt), nx*ny doubles. */
 int upic_get_field(upic_ctx* ctx, int which, double* host);
 
 /* ---- Kernel-level entry points (host arrays in and out).  Each runs the

@@ -1,13 +1,16 @@
 """Regenerate the golden fixtures in tests/golden/ from the reference's own code.
 
-Runs the reference solver Project2/spectral_pic_part3.cpp through the C-ABI
-harness oracle/_ref/libref_p2.so (built by `make -C oracle` from the reference
-sources) on small seeded inputs and saves inputs and outputs, and copies the
-published validation numbers of Project2/docs/validation_summary.json.  The
+Runs the reference solvers Project2/spectral_pic_part3.cpp and
+Project3/ec_pic_nyquist_projected.cpp through the C-ABI harnesses
+oracle/_ref/libref_p2.so and oracle/_ref/libref_p3.so (built by `make -C
+oracle` from the reference sources) on small seeded inputs and saves inputs
+and outputs, and copies the published validation numbers of
+Project2/docs/validation_summary.json.  The
 fixtures let the oracle and the GPU path be checked where the reference
 sources are absent.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py        # all fixtures
+    python tests/golden/make_golden.py p3     # the implicit-method runs only
 """
 import ctypes
 import json
@@ -97,8 +100,61 @@ def main():
     runs = {k: v for k, v in summ["runs"].items() if k.startswith("weibel")}
     with open(os.path.join(HERE, "p2_weibel_published.json"), "w") as fh:
         json.dump({"source": "Project2/docs/validation_summary.json", "runs": runs}, fh, indent=1)
+    p3_main()
     print("fixtures written")
 
 
+def p3_edge_positions(x, Lx, Ly, nx, ny):
+    """Put the first particles on the domain edge, on nodes and next to them."""
+    dx, dy = Lx / nx, Ly / ny
+    x[:6, 0] = [-Lx / 2, np.nextafter(Lx / 2, 0), 0.0, -Lx / 2 + dx, np.nextafter(-Lx / 2 + 3 * dx, 0),
+                0.5 * dx]
+    x[:6, 1] = [np.nextafter(Ly / 2, 0), -Ly / 2, -Ly / 2 + 2 * dy, 0.0, 0.25 * dy,
+                np.nextafter(-Ly / 2 + 5 * dy, 0)]
+
+
+# Implicit (Project3) runs: (name, problem keywords, particles per cell, thermal
+# spreads of u = gamma v, two species).
+P3_CASES = [
+    ("p3_run_o2_anderson", dict(nx=16, ny=16, Lx=2 * np.pi / 0.3, Ly=2 * np.pi / 0.3, dt=0.05, order=2,
+                                nq=8, nyquist=True, n_steps=4), 8, (0.02, 0.2, 0.0), False),
+    ("p3_run_o3_picard", dict(nx=16, ny=16, Lx=2 * np.pi / 0.3, Ly=2 * np.pi / 0.3, dt=0.2, order=3,
+                              nq=8, nyquist=False, solver="picard", n_steps=3), 8, (0.02, 0.2, 0.0),
+     False),
+    ("p3_run_o1_nosplit", dict(nx=16, ny=16, Lx=2 * np.pi, Ly=2 * np.pi, dt=0.1, order=1, nq=4,
+                               split=False, nyquist=True, n_steps=3), 8, (0.05, 0.05, 0.05), False),
+    ("p3_run_o4", dict(nx=8, ny=16, Lx=2 * np.pi, Ly=2 * np.pi, dt=0.1, order=4, nq=8, nyquist=True,
+                       n_steps=2), 16, (0.05, 0.05, 0.05), False),
+    ("p3_run_two_species", dict(nx=16, ny=8, Lx=2 * np.pi, Ly=np.pi, dt=0.1, order=2, nq=8,
+                                nyquist=True, n_steps=2, Lz=0.5), 16, (0.1, 0.05, 0.02), True),
+]
+
+
+def p3_main():
+    """Fixtures of the implicit GM-HC-CN step from oracle/_ref/libref_p3.so."""
+    lib = ol.ref_p3()
+    if lib is None:
+        raise SystemExit("oracle/_ref/libref_p3.so missing: run make -C oracle")
+    for k, (name, kw, ppc, uth, two) in enumerate(P3_CASES):
+        rng = np.random.default_rng(20261203 + k)
+        prob = ol.P3Problem(**kw)
+        x, v, q, m = ol.p3_particles(rng, prob.nx, prob.ny, ppc, prob.Lx, prob.Ly, uth=uth, Lz=prob.Lz)
+        p3_edge_positions(x, prob.Lx, prob.Ly, prob.nx, prob.ny)
+        if two:
+            # every other particle a heavier positive species
+            q[1::2] = -q[1::2]
+            m[1::2] = 4.0 * m[1::2]
+            v[1::2] *= 0.5
+        out = ol.p3_run(lib.ref_p3_run, prob, x, v, q, m)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), dparams=prob.dparams(),
+                            iparams=prob.iparams(), in_x=x, in_v=v, in_q=q, in_m=m,
+                            **{"out_" + k: out[k] for k in ("x", "v", "P", "v_prev", "vbar")},
+                            diag=out["diag"], info=out["info"], fields=out["fields"])
+        print(name, "iterations", out["info"][:, 0].tolist())
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "p3":
+        p3_main()
+    else:
+        main()

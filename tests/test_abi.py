@@ -30,13 +30,41 @@ def test_every_declared_symbol_is_exported_and_bound():
 
 def test_abi_version_and_config_defaults():
     L = _native.lib()
-    assert L.upic_abi_version() == 1
+    assert L.upic_abi_version() == 2
     cfg = _native.UpicConfig()
     assert L.upic_config_default(ctypes.byref(cfg)) == 0
     # reference Config defaults (spectral_pic_part3.cpp:174-231)
     assert (cfg.nx, cfg.ny, cfg.method, cfg.charge_update) == (32, 32, 1, 0)
     assert cfg.dt == 0.05 and cfg.c == 1.0 and cfg.eps0 == 1.0 and cfg.mu0 == 1.0 and cfg.n0 == 1.0
     assert abs(cfg.Lx - 2 * np.pi) < 1e-15
+    # implicit-method defaults (ec_pic_nyquist_projected.cpp:837-1005)
+    assert (cfg.spline_order, cfg.orbit_quad_order, cfg.split_orbit_at_knots, cfg.nyquist_projection) == \
+        (2, 16, 1, 0)
+    assert (cfg.nonlinear_solver, cfg.nonlinear_max_iter, cfg.anderson_memory, cfg.anderson_start,
+            cfg.local_max_iter, cfg.perturbation_mode) == (0, 32, 4, 2, 24, 1)
+    assert (cfg.kappa, cfg.sigma1, cfg.sigma2) == (1.0, 1.0, 1.0)
+    assert (cfg.nonlinear_rtol, cfg.nonlinear_atol, cfg.anderson_damping, cfg.anderson_regularization,
+            cfg.anderson_growth_limit) == (1e-12, 1e-13, 0.7, 1e-12, 1.2)
+    assert (cfg.local_rtol, cfg.local_atol, cfg.local_damping) == (1e-11, 1e-13, 1.0)
+
+
+def test_config_struct_layout_matches_header():
+    """The ctypes mirror has the C struct's size and field offsets."""
+    import subprocess
+    import tempfile
+    fields = [f[0] for f in _native.UpicConfig._fields_]
+    src = "#include <stdio.h>\n#include <stddef.h>\n#include \"upic.h\"\nint main(void){printf(\"%zu\"" + \
+        "".join(' \" %zu\"' for _ in fields) + ", sizeof(upic_config)" + \
+        "".join(f", offsetof(upic_config, {f})" for f in fields) + ");return 0;}\n"
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "layout.c")
+        exe = os.path.join(d, "layout")
+        open(c, "w").write(src)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        out = [int(t) for t in subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()]
+    assert out[0] == ctypes.sizeof(_native.UpicConfig)
+    for f, off in zip(fields, out[1:]):
+        assert getattr(_native.UpicConfig, f).offset == off, f
 
 
 @pytest.mark.parametrize("kw,code", [(dict(nx=48), -1), (dict(method="bdf3"), None),

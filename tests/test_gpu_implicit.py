@@ -1,0 +1,204 @@
+"""GPU parity of the implicit orbit-averaged GM-HC-CN path (libupic.so,
+UPIC_METHOD_CN_ORBIT) against runs of the reference's own solver
+(Project3/ec_pic_nyquist_projected.cpp through oracle/_ref/libref_p3.so),
+committed as tests/golden/p3_*.npz.
+
+Both sides iterate the outer current map to the same mixed tolerance
+(nonlinear_rtol 1e-11, nonlinear_atol 1e-13) and the particle map to
+1e-12/1e-14, so a converged step agrees to about that tolerance, not to
+round-off: the tests bound the relative difference of every field and
+particle array by TOL_STEP per step taken.  Round-off-level diagnostics (Gauss
+and gauge residuals) are compared in absolute terms against TOL_ROUNDOFF."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+import unstaggered_pic_b200 as up
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL_STEP = 2e-10      # relative difference per step, fields and particle state
+TOL_ROUNDOFF = 1e-12  # absolute, residual diagnostics at round-off level
+CASES = ["p3_run_o2_anderson", "p3_run_o3_picard", "p3_run_o1_nosplit", "p3_run_o4",
+         "p3_run_two_species"]
+FIELD_ORDER = ["phi", "psi", "rho", "Ax", "Ay", "Az", "Ux", "Uy", "Uz", "Jx", "Jy", "Jz"]
+
+
+def relerr(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = np.max(np.abs(b))
+    if scale == 0.0:
+        return float(np.max(np.abs(a)))
+    return float(np.max(np.abs(a - b)) / scale)
+
+
+def periodic_err(a, b, L):
+    d = np.asarray(a) - np.asarray(b)
+    d -= L * np.round(d / L)
+    return float(np.max(np.abs(d)))
+
+
+def config_from(dp, ip):
+    """ImplicitConfig of a fixture's (dparams, iparams) (oracle_lib.P3Problem layout)."""
+    return up.ImplicitConfig(
+        nx=int(ip[0]), ny=int(ip[1]), Lx=dp[0], Ly=dp[1], Lz=dp[2], dt=dp[3], kappa=dp[4], sigma1=dp[5],
+        sigma2=dp[6], n0=dp[7], spline_order=int(ip[3]), orbit_quad_order=int(ip[4]),
+        split_orbit_at_knots=bool(ip[5]), nyquist_projection=bool(ip[6]),
+        nonlinear_solver="picard" if ip[11] == 1 else "anderson", nonlinear_rtol=dp[8],
+        nonlinear_atol=dp[9], nonlinear_max_iter=int(ip[7]), anderson_memory=int(ip[8]),
+        anderson_start=int(ip[9]), anderson_damping=dp[10], anderson_regularization=dp[11],
+        anderson_growth_limit=dp[12], uniform_local_rtol=dp[13], uniform_local_atol=dp[14],
+        uniform_local_max_iter=int(ip[10]), uniform_local_damping=dp[15], perturbation_mode=int(ip[13]))
+
+
+def load_sim(g):
+    cfg = config_from(g["dparams"], g["iparams"])
+    sim = up.Simulation(cfg)
+    x, v = g["in_x"], g["in_v"]
+    n = len(g["in_q"])
+    sim.set_particles(x[:, 0], x[:, 1], np.zeros((n, 3)), v, v, g["in_q"], g["in_m"])
+    return sim, cfg
+
+
+def compare_diag(row, ref, nyquist, tol):
+    names = up.IMPLICIT_DIAG_COLUMNS
+    for k, name in enumerate(names):
+        a, b = row[k], ref[k]
+        roundoff = name in ("gauss_rms", "gauss_max", "gauge_rms", "gauge_max", "gauss_relative",
+                            "gauge_relative")
+        if roundoff and (nyquist or abs(b) < 1e-9):
+            assert abs(a - b) < TOL_ROUNDOFF * max(1.0, abs(b)) or abs(a) < 1e-11, (name, a, b)
+        else:
+            assert abs(a - b) <= tol * max(abs(b), 1e-300) + 1e-14, (name, a, b)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_implicit_run_matches_reference(case):
+    g = dict(np.load(os.path.join(GOLD, case + ".npz")))
+    sim, cfg = load_sim(g)
+    nsteps = int(g["iparams"][12])
+    nyq = bool(g["iparams"][6])
+    try:
+        row0 = sim.init_fields()
+        compare_diag(row0, g["diag"][0], nyq, 1e-12)
+        diag, info = sim.step_implicit(nsteps)
+        for s in range(nsteps):
+            compare_diag(diag[s], g["diag"][s + 1], nyq, TOL_STEP * (s + 1))
+        # same outer iteration path
+        assert np.all(np.abs(info[:, 0] - g["info"][:, 0]) <= 1), (info[:, 0], g["info"][:, 0])
+        assert np.all(info[:, 1] == 1.0)
+        tol = TOL_STEP * nsteps
+        fields = np.stack([sim.field(f) for f in FIELD_ORDER])
+        for k, f in enumerate(FIELD_ORDER):
+            assert relerr(fields[k], g["fields"][k]) < tol, (f, relerr(fields[k], g["fields"][k]))
+        p = sim.get_particles()
+        assert periodic_err(p["x"], g["out_x"][:, 0], cfg.Lx) < tol * cfg.Lx
+        assert periodic_err(p["y"], g["out_x"][:, 1], cfg.Ly) < tol * cfg.Ly
+        assert relerr(p["v"], g["out_v"]) < tol
+        assert relerr(p["P"], g["out_P"]) < tol
+        assert relerr(p["v_prev"], g["out_v_prev"]) < tol
+    finally:
+        sim.close()
+
+
+def test_implicit_energy_conserved_and_deterministic():
+    """Energy of the knot-split orbit-averaged scheme is conserved to the
+    solver tolerance, and two runs from the same input are bitwise equal."""
+    g = dict(np.load(os.path.join(GOLD, "p3_run_o2_anderson.npz")))
+    results = []
+    for _ in range(2):
+        sim, _ = load_sim(g)
+        try:
+            row0 = sim.init_fields()
+            diag, info = sim.step_implicit(6)
+            results.append((row0, diag, sim.field("Jx"), sim.get_particles()["v"]))
+        finally:
+            sim.close()
+    row0, diag, jx, v = results[0]
+    e0 = row0[up.IMPLICIT_DIAG_COLUMNS.index("total_energy")]
+    drift = np.abs(diag[:, up.IMPLICIT_DIAG_COLUMNS.index("total_energy")] - e0) / e0
+    assert drift.max() < 1e-10
+    assert np.array_equal(results[1][1], diag)
+    assert np.array_equal(results[1][2], jx)
+    assert np.array_equal(results[1][3], v)
+
+
+def test_implicit_errors():
+    g = dict(np.load(os.path.join(GOLD, "p3_run_o2_anderson.npz")))
+    sim, cfg = load_sim(g)
+    try:
+        with pytest.raises(up.UpicError) as e:
+            sim.step_implicit(1)
+        assert e.value.code == -4  # UPIC_ERR_STATE: init_fields first
+        sim.init_fields()
+        with pytest.raises(up.UpicError) as e:
+            sim.step(1)
+        assert e.value.code == -4  # the explicit step on an implicit context
+        # superluminal input velocity (gamma_from_v throws in the reference)
+        n = 4
+        with pytest.raises(up.UpicError) as e:
+            sim.set_particles(np.zeros(n), np.zeros(n), np.zeros((n, 3)), np.full((n, 3), 0.6),
+                              np.zeros((n, 3)), -np.ones(n), np.ones(n))
+        assert e.value.code == -8
+    finally:
+        sim.close()
+    # a local solve that cannot converge in one iteration fails loudly
+    cfg.uniform_local_max_iter = 1
+    sim = up.Simulation(cfg)
+    try:
+        x, v = g["in_x"], g["in_v"]
+        n = len(g["in_q"])
+        sim.set_particles(x[:, 0], x[:, 1], np.zeros((n, 3)), v, v, g["in_q"], g["in_m"])
+        sim.init_fields()
+        with pytest.raises(up.UpicError) as e:
+            sim.step_implicit(1)
+        assert e.value.code == -7  # UPIC_ERR_LOCAL_PARTICLE
+        assert "maximum_iterations" in str(e.value)
+    finally:
+        sim.close()
+
+
+def test_implicit_empty_and_bad_config():
+    cfg = up.ImplicitConfig(nx=8, ny=8, dt=0.1)
+    sim = up.Simulation(cfg)
+    try:
+        sim.set_particles(np.zeros(0), np.zeros(0), np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 3)),
+                          np.zeros(0), np.zeros(0))
+        row0 = sim.init_fields()
+        diag, info = sim.step_implicit(2)
+        assert np.all(sim.field("phi") == 0.0)
+        assert info[0, 0] == 1  # the zero current is a fixed point
+    finally:
+        sim.close()
+    for bad in (dict(spline_order=5), dict(orbit_quad_order=0), dict(anderson_memory=5), dict(nx=12),
+                dict(kappa=0.0)):
+        kw = dict(nx=8, ny=8, dt=0.1)
+        kw.update(bad)
+        with pytest.raises(up.UpicError) as e:
+            up.Simulation(up.ImplicitConfig(**kw))
+        assert e.value.code == -1
+
+
+@pytest.mark.skipif(not os.path.exists(ol.REF_P3_SO), reason="oracle/_ref/libref_p3.so not built")
+def test_implicit_larger_case_against_reference_build():
+    """A 32x32 grid, 16 particles per cell, 3 steps, compared with the
+    reference build directly (when oracle/_ref travels with the tree)."""
+    rng = np.random.default_rng(7)
+    prob = ol.P3Problem(32, 32, 2 * np.pi / 0.3, 2 * np.pi / 0.3, 0.05, order=2, nq=8, n_steps=3)
+    x, v, q, m = ol.p3_particles(rng, 32, 32, 16, prob.Lx, prob.Ly, uth=(0.02, 0.2, 0.0), Lz=prob.Lz)
+    ref = ol.p3_run(ol.ref_p3().ref_p3_run, prob, x, v, q, m)
+    g = {"dparams": prob.dparams(), "iparams": prob.iparams(), "in_x": x, "in_v": v, "in_q": q, "in_m": m}
+    sim, cfg = load_sim(g)
+    try:
+        sim.init_fields()
+        diag, info = sim.step_implicit(3)
+        for s in range(3):
+            compare_diag(diag[s], ref["diag"][s + 1], True, TOL_STEP * (s + 1))
+        for k, f in enumerate(FIELD_ORDER):
+            assert relerr(sim.field(f), ref["fields"][k]) < 3 * TOL_STEP, f
+    finally:
+        sim.close()

@@ -100,3 +100,25 @@ def test_oracle_matches_live_reference_when_built():
     for k in a[0]:
         assert np.array_equal(a[0][k], b[0][k])
     assert np.array_equal(a[1], b[1], equal_nan=True)
+
+
+@pytest.mark.parametrize("case", [0, 4])
+def test_implicit_fixtures_regenerate_from_reference_build(case):
+    """The committed implicit-method fixtures (tests/golden/p3_*.npz) are
+    outputs of the reference's own solver: rerunning the reference build on
+    the stored inputs reproduces them bit for bit.  Skipped where the
+    reference sources (and so oracle/_ref/libref_p3.so) are absent."""
+    ref = ol.ref_p3()
+    if ref is None:
+        pytest.skip("reference harness not built (no reference sources)")
+    from golden.make_golden import P3_CASES
+    name = P3_CASES[case][0]
+    g = dict(np.load(os.path.join(GOLD, name + ".npz")))
+    prob = ol.P3Problem(**P3_CASES[case][1])
+    assert np.array_equal(prob.dparams(), g["dparams"]) and np.array_equal(prob.iparams(), g["iparams"])
+    out = ol.p3_run(ref.ref_p3_run, prob, g["in_x"], g["in_v"], g["in_q"], g["in_m"])
+    for k in ("x", "v", "P", "v_prev", "vbar"):
+        assert np.array_equal(out[k], g["out_" + k]), k
+    assert np.array_equal(out["diag"], g["diag"])
+    assert np.array_equal(out["info"], g["info"])
+    assert np.array_equal(out["fields"], g["fields"])

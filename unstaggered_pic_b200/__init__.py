@@ -13,16 +13,29 @@ import numpy as np
 
 from ._native import UPIC_ERR, UpicConfig, c_dp, lib
 
-__all__ = ["UpicError", "Config", "Simulation", "generate_bimaxwellian", "DIAG_COLUMNS",
-           "METHODS", "FIELDS"]
+__all__ = ["UpicError", "Config", "ImplicitConfig", "Simulation", "generate_bimaxwellian",
+           "DIAG_COLUMNS", "IMPLICIT_DIAG_COLUMNS", "SOLVE_INFO_COLUMNS", "METHODS", "FIELDS"]
 
-METHODS = {"bdf1": 1, "bdf2": 2}
+METHODS = {"bdf1": 1, "bdf2": 2, "cn_orbit": 3}
 CHARGE_UPDATES = {"conserving": 0, "naive": 1}
-FIELDS = {"phi": 0, "Ax": 1, "Ay": 2, "Az": 3, "rho": 4, "Jx": 5, "Jy": 6, "Jz": 7}
+NONLINEAR_SOLVERS = {"anderson_quasi_newton": 0, "anderson": 0, "picard": 1}
+FIELDS = {"phi": 0, "Ax": 1, "Ay": 2, "Az": 3, "rho": 4, "Jx": 5, "Jy": 6, "Jz": 7,
+          "psi": 8, "Ux": 9, "Uy": 10, "Uz": 11}
 # Diagnostics columns of the reference's _diagnostics.csv (spectral_pic_part3.cpp:1117-1119).
 DIAG_COLUMNS = ["gauge_rms", "gauss_rms", "continuity_rms", "Bz_l2", "B_l2", "E_l2", "rho_l2",
                 "J_l2", "field_energy", "kinetic_energy", "total_energy", "max_speed",
                 "mean_gamma"]
+# Diagnostics of the implicit method (Diagnostics, ec_pic_nyquist_projected.cpp:3469-3519).
+IMPLICIT_DIAG_COLUMNS = [
+    "gauss_rms", "gauss_max", "divE_rms", "sigma1_rho_rms", "gauss_normalization_rms",
+    "gauss_relative", "gauge_rms", "gauge_max", "psi_over_kappa2_rms", "divA_rms",
+    "gauge_normalization_rms", "gauge_relative", "field_energy", "kinetic_energy", "total_energy",
+    "rho_mode", "E_mode_re", "E_mode_im", "E_mode_abs", "Bz_y_mode_re", "Bz_y_mode_im",
+    "Bz_y_mode_abs"]
+# Per-step outer-solve report (NonlinearSolveInfo, ec_pic_nyquist_projected.cpp:5493-5533).
+SOLVE_INFO_COLUMNS = ["iterations", "converged", "final_rms_residual", "final_max_particle_residual",
+                      "local_particle_iterations_max", "local_particle_iterations_mean",
+                      "anderson_steps", "picard_fallback_steps"]
 
 
 class UpicError(RuntimeError):
@@ -67,8 +80,65 @@ class Config:
         return cfg
 
 
+class ImplicitConfig:
+    """Deck of the implicit orbit-averaged GM-HC-CN method with the keys and
+    defaults of the reference Config (ec_pic_nyquist_projected.cpp:837-1005),
+    2D (nz = 1; Lz sets the cell volume).  Positions live in [-L/2, L/2)."""
+
+    def __init__(self, nx=4, ny=4, Lx=2 * np.pi, Ly=2 * np.pi, Lz=2 * np.pi, dt=0.00625, kappa=1.0,
+                 sigma1=1.0, sigma2=1.0, n0=1.0, spline_order=2, orbit_quad_order=16,
+                 split_orbit_at_knots=True, nyquist_projection=False,
+                 nonlinear_solver="anderson_quasi_newton", nonlinear_rtol=1.0e-12,
+                 nonlinear_atol=1.0e-13, nonlinear_max_iter=32, anderson_memory=4, anderson_start=2,
+                 anderson_damping=0.7, anderson_regularization=1.0e-12, anderson_growth_limit=1.2,
+                 uniform_local_rtol=1.0e-11, uniform_local_atol=1.0e-13, uniform_local_max_iter=24,
+                 uniform_local_damping=1.0, perturbation_mode=1, tile=0, guard=-1):
+        self.method = "cn_orbit"
+        self.nx, self.ny, self.Lx, self.Ly, self.Lz, self.dt = nx, ny, Lx, Ly, Lz, dt
+        self.kappa, self.sigma1, self.sigma2, self.n0 = kappa, sigma1, sigma2, n0
+        self.spline_order, self.orbit_quad_order = spline_order, orbit_quad_order
+        self.split_orbit_at_knots, self.nyquist_projection = split_orbit_at_knots, nyquist_projection
+        self.nonlinear_solver = nonlinear_solver
+        self.nonlinear_rtol, self.nonlinear_atol = nonlinear_rtol, nonlinear_atol
+        self.nonlinear_max_iter = nonlinear_max_iter
+        self.anderson_memory, self.anderson_start = anderson_memory, anderson_start
+        self.anderson_damping, self.anderson_regularization = anderson_damping, anderson_regularization
+        self.anderson_growth_limit = anderson_growth_limit
+        self.uniform_local_rtol, self.uniform_local_atol = uniform_local_rtol, uniform_local_atol
+        self.uniform_local_max_iter, self.uniform_local_damping = uniform_local_max_iter, uniform_local_damping
+        self.perturbation_mode, self.tile, self.guard = perturbation_mode, tile, guard
+
+    def to_c(self):
+        cfg = UpicConfig()
+        lib().upic_config_default(ctypes.byref(cfg))
+        cfg.nx, cfg.ny = int(self.nx), int(self.ny)
+        cfg.Lx, cfg.Ly, cfg.Lz, cfg.dt = float(self.Lx), float(self.Ly), float(self.Lz), float(self.dt)
+        cfg.method = METHODS["cn_orbit"]
+        cfg.n0 = float(self.n0)
+        cfg.kappa, cfg.sigma1, cfg.sigma2 = float(self.kappa), float(self.sigma1), float(self.sigma2)
+        cfg.spline_order, cfg.orbit_quad_order = int(self.spline_order), int(self.orbit_quad_order)
+        cfg.split_orbit_at_knots = int(bool(self.split_orbit_at_knots))
+        cfg.nyquist_projection = int(bool(self.nyquist_projection))
+        ns = self.nonlinear_solver
+        cfg.nonlinear_solver = NONLINEAR_SOLVERS[ns] if isinstance(ns, str) else int(ns)
+        cfg.nonlinear_rtol, cfg.nonlinear_atol = float(self.nonlinear_rtol), float(self.nonlinear_atol)
+        cfg.nonlinear_max_iter = int(self.nonlinear_max_iter)
+        cfg.anderson_memory, cfg.anderson_start = int(self.anderson_memory), int(self.anderson_start)
+        cfg.anderson_damping = float(self.anderson_damping)
+        cfg.anderson_regularization = float(self.anderson_regularization)
+        cfg.anderson_growth_limit = float(self.anderson_growth_limit)
+        cfg.local_rtol, cfg.local_atol = float(self.uniform_local_rtol), float(self.uniform_local_atol)
+        cfg.local_max_iter = int(self.uniform_local_max_iter)
+        cfg.local_damping = float(self.uniform_local_damping)
+        cfg.perturbation_mode = int(self.perturbation_mode)
+        cfg.tile, cfg.guard = int(self.tile), int(self.guard)
+        return cfg
+
+
 class Simulation:
-    """One device context: particles + field state of the explicit BDF/IAEM step."""
+    """One device context: particles + field state of the explicit BDF/IAEM
+    step (Config) or of the implicit orbit-averaged GM-HC-CN step
+    (ImplicitConfig)."""
 
     def __init__(self, config):
         self.config = config
@@ -79,6 +149,7 @@ class Simulation:
             raise UpicError(rc, lib().upic_last_error(None).decode())
         self.np = 0
         self.N = config.nx * config.ny
+        self.implicit = cfg.method == METHODS["cn_orbit"]
 
     def _check(self, rc):
         if rc != 0:
@@ -124,9 +195,17 @@ class Simulation:
         return out
 
     def init_fields(self, diagnostics=True):
-        row = np.empty(13) if diagnostics else None
+        ncol = len(IMPLICIT_DIAG_COLUMNS) if self.implicit else len(DIAG_COLUMNS)
+        row = np.empty(ncol) if diagnostics else None
         self._check(lib().upic_init_fields(self._ctx, _p(row)))
         return row
+
+    def step_implicit(self, nsteps=1, diagnostics=True):
+        """nsteps implicit steps; returns (diag rows, solve-info rows)."""
+        diag = np.empty((nsteps, len(IMPLICIT_DIAG_COLUMNS))) if diagnostics else None
+        info = np.empty((nsteps, len(SOLVE_INFO_COLUMNS)))
+        self._check(lib().upic_step_implicit(self._ctx, int(nsteps), _p(diag), _p(info)))
+        return diag, info
 
     def step(self, nsteps=1, diag_stride=1):
         diag = np.empty((nsteps, 13)) if diag_stride > 0 else None

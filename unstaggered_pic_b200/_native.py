@@ -30,6 +30,7 @@ SYMBOLS = {
     "upic_get_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 5),
     "upic_init_fields": (ctypes.c_int, [ctypes.c_void_p, c_dp]),
     "upic_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
+    "upic_step_implicit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, c_dp]),
     "upic_step_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]),
     "upic_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "upic_profile_read": (ctypes.c_int, [ctypes.c_void_p, c_dp, ctypes.POINTER(ctypes.c_long),
@@ -65,6 +66,19 @@ class UpicConfig(ctypes.Structure):
         ("precision", ctypes.c_int), ("sort_interval", ctypes.c_int),
         ("tile", ctypes.c_int), ("guard", ctypes.c_int),
         ("reserved", ctypes.c_int * 8),
+        ("Lz", ctypes.c_double),
+        ("kappa", ctypes.c_double), ("sigma1", ctypes.c_double), ("sigma2", ctypes.c_double),
+        ("spline_order", ctypes.c_int), ("orbit_quad_order", ctypes.c_int),
+        ("split_orbit_at_knots", ctypes.c_int), ("nyquist_projection", ctypes.c_int),
+        ("nonlinear_solver", ctypes.c_int), ("nonlinear_max_iter", ctypes.c_int),
+        ("anderson_memory", ctypes.c_int), ("anderson_start", ctypes.c_int),
+        ("local_max_iter", ctypes.c_int),
+        ("nonlinear_rtol", ctypes.c_double), ("nonlinear_atol", ctypes.c_double),
+        ("anderson_damping", ctypes.c_double), ("anderson_regularization", ctypes.c_double),
+        ("anderson_growth_limit", ctypes.c_double),
+        ("local_rtol", ctypes.c_double), ("local_atol", ctypes.c_double),
+        ("local_damping", ctypes.c_double),
+        ("perturbation_mode", ctypes.c_int),
     ]
 
 

@@ -17,7 +17,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libupic.so")
 BUILD = os.path.join(ROOT, "_build")
 
-SOURCES = ["fft.cu", "sort.cu", "explicit.cu", "api.cu", "noalloc.cu", "generate.cpp"]
+SOURCES = ["fft.cu", "sort.cu", "explicit.cu", "implicit.cu", "api.cu", "api_implicit.cu", "noalloc.cu",
+           "generate.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -98,6 +98,9 @@ TileGeom make_tiles(int nx, int ny, int tile, int guard, int lo, int hi) {
     axis(nx, g.tile_x, g.ntx, g.wx, g.full_x);
     axis(ny, g.tile_y, g.nty, g.wy, g.full_y);
     g.chunk = 2048;
+    g.key_origin_x = 0.0;
+    g.key_origin_y = 0.0;
+    g.key_shift = 0.5;
     return g;
 }
 
@@ -191,6 +194,14 @@ __global__ void join3_kernel(double* t, long n, const double* a, const double* b
 __global__ void iota_kernel(int* id, long n) {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         id[i] = (int)i;
+}
+
+int iota(upic_ctx* c, int* id, long n) {
+    if (n <= 0) return 0;
+    iota_kernel<<<gridn(n), 256, 0, c->st>>>(id, n);
+    count_launches(1);
+    UPIC_CUDA(c, cudaGetLastError());
+    return 0;
 }
 
 __global__ void interleave_kernel(const double* re, const double* im, double2* out, long n) {
@@ -385,6 +396,29 @@ int upic_config_default(upic_config* cfg) {
     cfg->sort_interval = 0;
     cfg->tile = 0;
     cfg->guard = -1;
+    // implicit method: the Config defaults of ec_pic_nyquist_projected.cpp:837-1005
+    cfg->Lz = 2.0 * kPi;
+    cfg->kappa = 1.0;
+    cfg->sigma1 = 1.0;
+    cfg->sigma2 = 1.0;
+    cfg->spline_order = 2;
+    cfg->orbit_quad_order = 16;
+    cfg->split_orbit_at_knots = 1;
+    cfg->nyquist_projection = 0;
+    cfg->nonlinear_solver = UPIC_SOLVER_ANDERSON;
+    cfg->nonlinear_max_iter = 32;
+    cfg->anderson_memory = 4;
+    cfg->anderson_start = 2;
+    cfg->local_max_iter = 24;
+    cfg->nonlinear_rtol = 1.0e-12;
+    cfg->nonlinear_atol = 1.0e-13;
+    cfg->anderson_damping = 0.7;
+    cfg->anderson_regularization = 1.0e-12;
+    cfg->anderson_growth_limit = 1.2;
+    cfg->local_rtol = 1.0e-11;
+    cfg->local_atol = 1.0e-13;
+    cfg->local_damping = 1.0;
+    cfg->perturbation_mode = 1;
     return UPIC_OK;
 }
 
@@ -399,12 +433,38 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
     if (!pow2(cfg->nx) || !pow2(cfg->ny) || cfg->nx > 8192 || cfg->ny > 8192)
         return fail(nullptr, UPIC_ERR_CONFIG,
                     "the radix-2 FFT requires nx and ny to be powers of two (<= 8192)");
-    if (!is_bdf(cfg->method)) return fail(nullptr, UPIC_ERR_CONFIG, "method must be bdf1 or bdf2");
-    if (cfg->charge_update != UPIC_CHARGE_CONSERVING && cfg->charge_update != UPIC_CHARGE_NAIVE)
-        return fail(nullptr, UPIC_ERR_CONFIG, "charge_update must be conserving or naive");
-    if (!(cfg->Lx > 0) || !(cfg->Ly > 0) || !(cfg->dt > 0) || !(cfg->c > 0) || !(cfg->eps0 > 0) ||
-        !(cfg->mu0 > 0))
-        return fail(nullptr, UPIC_ERR_CONFIG, "Lx, Ly, dt, c, eps0, mu0 must be positive");
+    const bool implicit = cfg->method == UPIC_METHOD_CN_ORBIT;
+    if (!is_bdf(cfg->method) && !implicit)
+        return fail(nullptr, UPIC_ERR_CONFIG, "method must be bdf1, bdf2 or cn_orbit");
+    if (implicit) {
+        // validation of ec_pic_nyquist_projected.cpp read_config / make_grid
+        if (!(cfg->Lx > 0) || !(cfg->Ly > 0) || !(cfg->Lz > 0) || !(cfg->dt > 0) || !(cfg->kappa > 0) ||
+            !(cfg->sigma1 > 0) || !(cfg->sigma2 > 0))
+            return fail(nullptr, UPIC_ERR_CONFIG, "Lx, Ly, Lz, dt, kappa, sigma1, sigma2 must be positive");
+        if (cfg->spline_order < 1 || cfg->spline_order > 4)
+            return fail(nullptr, UPIC_ERR_CONFIG, "spline_order must be 1, 2, 3 or 4");
+        if (cfg->orbit_quad_order < 1 || cfg->orbit_quad_order > 32)
+            return fail(nullptr, UPIC_ERR_CONFIG, "orbit_quad_order must be in 1..32");
+        if (cfg->nonlinear_solver != UPIC_SOLVER_ANDERSON && cfg->nonlinear_solver != UPIC_SOLVER_PICARD)
+            return fail(nullptr, UPIC_ERR_CONFIG, "nonlinear_solver must be anderson or picard");
+        if (cfg->anderson_memory < 1 || cfg->anderson_memory > 4)
+            return fail(nullptr, UPIC_ERR_CONFIG, "anderson_memory must be in 1..4");
+        if (cfg->nonlinear_max_iter < 1 || cfg->local_max_iter < 1 || cfg->anderson_start < 0)
+            return fail(nullptr, UPIC_ERR_CONFIG, "iteration limits must be positive");
+        if (!(cfg->nonlinear_rtol >= 0) || !(cfg->nonlinear_atol >= 0) || !(cfg->local_rtol >= 0) ||
+            !(cfg->local_atol >= 0) || !(cfg->nonlinear_rtol + cfg->nonlinear_atol > 0) ||
+            !(cfg->local_rtol + cfg->local_atol > 0))
+            return fail(nullptr, UPIC_ERR_CONFIG, "tolerances must be non-negative and not both zero");
+        if (!(cfg->anderson_damping > 0) || !(cfg->local_damping > 0) || !(cfg->anderson_growth_limit > 0) ||
+            !(cfg->anderson_regularization >= 0))
+            return fail(nullptr, UPIC_ERR_CONFIG, "damping and growth limits must be positive");
+    } else {
+        if (cfg->charge_update != UPIC_CHARGE_CONSERVING && cfg->charge_update != UPIC_CHARGE_NAIVE)
+            return fail(nullptr, UPIC_ERR_CONFIG, "charge_update must be conserving or naive");
+        if (!(cfg->Lx > 0) || !(cfg->Ly > 0) || !(cfg->dt > 0) || !(cfg->c > 0) || !(cfg->eps0 > 0) ||
+            !(cfg->mu0 > 0))
+            return fail(nullptr, UPIC_ERR_CONFIG, "Lx, Ly, dt, c, eps0, mu0 must be positive");
+    }
     if (cfg->precision != UPIC_PRECISION_FP64)
         return fail(nullptr, UPIC_ERR_CONFIG, "this build supports precision = fp64 only");
 
@@ -479,6 +539,7 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
     c->plan.ny = c->ny;
     c->plan.tw_x = c->d_twx;
     c->plan.tw_y = c->d_twy;
+    if (implicit && (rc = implicit_create(c))) return bail(rc);
     *out = c;
     return UPIC_OK;
 }
@@ -487,6 +548,7 @@ int upic_destroy(upic_ctx* c) {
     if (!c) return UPIC_OK;
     if (c->st) cudaStreamSynchronize(c->st);
     clear_profile(c);
+    implicit_destroy(c);
     for (void* p : c->allocs)
         if (p) cudaFree(p);
     if (c->h_row) cudaFreeHost(c->h_row);
@@ -508,6 +570,15 @@ int upic_set_particles(upic_ctx* c, long np, const double* x, const double* y, c
     if (np < 0 || np > 0x7fffffffL) return fail(c, UPIC_ERR_ARGUMENT, "particle count out of range");
     if (np > 0 && (!x || !y || !P || !v || !v_prev || !q || !m))
         return fail(c, UPIC_ERR_ARGUMENT, "null particle array");
+    if (c->imp) {
+        const int rc = implicit_set_particles(c, np, x, y, P, v, v_prev, q, m);
+        if (rc == 0) {
+            c->np = np;
+            c->fields_ready = false;
+            c->steps = 0;
+        }
+        return rc;
+    }
     // uniform charge/mass (the reference stores them per particle)
     bool uniform = true;
     double qabs = 0.0, vmax = 0.0;
@@ -547,9 +618,7 @@ int upic_set_particles(upic_ctx* c, long np, const double* x, const double* y, c
             UPIC_CUDA(c, cudaMemcpyAsync(s.q, q, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
             UPIC_CUDA(c, cudaMemcpyAsync(s.m, m, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
         }
-        iota_kernel<<<gridn(np), 256, 0, c->st>>>(s.id, np);
-        count_launches(1);
-        UPIC_CUDA(c, cudaGetLastError());
+        if ((rc = iota(c, s.id, np))) return rc;
     }
     const double vb = vmax > c->cfg.c ? vmax : c->cfg.c;
     const double bJ = qabs * vb / c->dA;
@@ -564,6 +633,7 @@ int upic_get_particles(upic_ctx* c, long np, double* x, double* y, double* P, do
                        double* v_prev) {
     if (!c) return UPIC_ERR_ARGUMENT;
     if (np != c->np) return fail(c, UPIC_ERR_ARGUMENT, "particle count does not match the context");
+    if (c->imp) return implicit_get_particles(c, np, x, y, P, v, v_prev);
     if (np == 0) return UPIC_OK;
     ParticleSoA& s = c->P[c->cur];
     ParticleSoA& d = c->P[1 - c->cur];
@@ -581,6 +651,7 @@ int upic_get_particles(upic_ctx* c, long np, double* x, double* y, double* P, do
 
 int upic_init_fields(upic_ctx* c, double* diag_row) {
     if (!c) return UPIC_ERR_ARGUMENT;
+    if (c->imp) return implicit_init_fields(c, diag_row);
     if (c->cap == 0 && c->np == 0) return fail(c, UPIC_ERR_STATE, "upic_set_particles first");
     const int N = c->N;
     int rc;
@@ -628,6 +699,7 @@ int upic_init_fields(upic_ctx* c, double* diag_row) {
 
 int upic_step(upic_ctx* c, int nsteps, int diag_stride, double* diag) {
     if (!c) return UPIC_ERR_ARGUMENT;
+    if (c->imp) return fail(c, UPIC_ERR_STATE, "the implicit method advances with upic_step_implicit");
     if (!c->fields_ready) return fail(c, UPIC_ERR_STATE, "upic_init_fields first");
     if (nsteps < 0) return fail(c, UPIC_ERR_ARGUMENT, "nsteps < 0");
     const int N = c->N;
@@ -725,6 +797,7 @@ int upic_step_count(const upic_ctx* c, long* steps) {
 int upic_get_field(upic_ctx* c, int which, double* host) {
     if (!c || !host) return UPIC_ERR_ARGUMENT;
     if (!c->fields_ready) return fail(c, UPIC_ERR_STATE, "upic_init_fields first");
+    if (c->imp) return implicit_get_field(c, which, host);
     const int N = c->N;
     if (which >= UPIC_FIELD_JX && which <= UPIC_FIELD_JZ) {
         UPIC_CUDA(c, cudaMemcpyAsync(host, c->d_J + (size_t)(which - UPIC_FIELD_JX) * N, sizeof(double) * N,

@@ -1,0 +1,871 @@
+// Host side of the implicit energy-conserving orbit-averaged GM-HC-CN method
+// (UPIC_METHOD_CN_ORBIT): state, start-up, the outer Anderson/Picard
+// iteration on the mesh current, and diagnostics.
+//
+// Reference: Project3/ec_pic_nyquist_projected.cpp.  The outer iteration
+// restates nonlinear_step_uniform_subcycled (:5878) for the level-one
+// particle layout that nonlinear_step_orbit (:6477) uses: map evaluations
+// J -> J_map run on the GPU (api: eval_map), the small dense Anderson solve
+// and the acceptance logic run here, with every vector reduction computed on
+// the device in double-double in a fixed order.
+//
+// HBM layout (N nodes, np particles): particle SoA x2 {x, y, P(3), v(3),
+// v_prev(3), vbar(3), id[, q, m]}; state spectra phi, psi, rho, A(3), U(3)
+// and their trial copies (2 x 9 complex per node); map records (8 doubles per
+// node: grad phi_mid, A^n, A^{n+1}); node currents J, J_field, guesses,
+// map values and the Anderson history (3 doubles per node each).
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "context.h"
+#include "implicit_kernels.h"
+#include "upic_common.cuh"
+
+using namespace upic;
+
+namespace upic_host {
+
+constexpr int kHist = 5;         // Anderson memory + 1 (memory <= 4)
+constexpr int kNormGrid = 296;
+
+struct ImplicitState {
+    int order = 2, nq = 8;
+    double dx = 0, dy = 0, dV = 0;
+    // particles: two sorted copies (the second is the sort / trial target)
+    ParticleSoA P[2];
+    double *bx[2] = {}, *by[2] = {}, *bz[2] = {};
+    int cur = 0;
+    long np = 0, cap = 0;
+    bool uniform = true;
+    double q0 = 0, m0 = 0, qabs = 0;
+    // fields
+    double2* spec = nullptr;      // state spectra (9 x N)
+    double2* spec_out = nullptr;  // trial spectra (9 x N)
+    double2* Jhat = nullptr;      // 3 x N
+    double2* gspec = nullptr;     // 5 x N
+    double2* dspec = nullptr;     // 10 x N
+    double* dreal = nullptr;      // 10 x N
+    double* rec = nullptr;        // 8 x N
+    unsigned char* excl = nullptr;
+    unsigned long long* acc = nullptr;  // 8 x N (J 3 comps + rho)
+    double* J = nullptr;          // state current (3 x N)
+    double* Jf = nullptr;         // projected current guess (3 x N)
+    double* guess = nullptr;
+    double* map = nullptr;
+    double* trial = nullptr;
+    double* trial_map = nullptr;
+    double* cand = nullptr;
+    double* resid = nullptr;
+    double* hx[kHist] = {};
+    double* hr[kHist] = {};
+    int hcount = 0;
+    double* partials = nullptr;
+    NormSums* dnorm = nullptr;
+    NormSums* hnorm = nullptr;    // pinned
+    MapStats* dstats = nullptr;
+    MapStats* hstats = nullptr;   // pinned
+    int* dflag = nullptr;
+    int* hflag = nullptr;         // pinned
+    double* ddots = nullptr;
+    double* hdots = nullptr;      // pinned (32)
+    double scaleJ[4] = {1, 1, 1, 1};
+    TileGeom tg{};
+    SortWork sw{};
+    int grid = 148;
+    long steps = 0;
+    bool loaded = false;  // upic_set_particles has succeeded
+    bool ready = false;   // upic_init_fields has succeeded
+};
+
+namespace {
+
+// Gauss-Legendre nodes and weights on [0,1] by Newton iteration on the
+// Legendre polynomial from the Chebyshev-like start cos(pi (i+3/4)/(n+1/2)),
+// the scheme of gauss_legendre_01 (ec_pic_nyquist_projected.cpp:2479).
+void gauss_legendre_01(int n, std::vector<double>& s, std::vector<double>& w) {
+    s.assign(n, 0.0);
+    w.assign(n, 0.0);
+    auto legendre = [&](double x, double& pn, double& dp) {
+        double p0 = 1.0, p1 = x;
+        if (n == 0) { pn = 1.0; dp = 0.0; return; }
+        if (n == 1) { pn = x; dp = 1.0; return; }
+        for (int k = 2; k <= n; ++k) {
+            const double pk = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / (double)k;
+            p0 = p1;
+            p1 = pk;
+        }
+        pn = p1;
+        dp = (double)n * (x * p1 - p0) / (x * x - 1.0);
+    };
+    const int m = (n + 1) / 2;
+    for (int i = 0; i < m; ++i) {
+        double x = std::cos(kPi * ((double)i + 0.75) / ((double)n + 0.5));
+        for (int it = 0; it < 80; ++it) {
+            double pn, dp;
+            legendre(x, pn, dp);
+            const double d = -pn / dp;
+            x += d;
+            if (std::fabs(d) < 1.0e-15) break;
+        }
+        double pn, dp;
+        legendre(x, pn, dp);
+        const double wt = 2.0 / ((1.0 - x * x) * dp * dp);
+        s[i] = 0.5 * (1.0 - x);
+        w[i] = 0.5 * wt;
+        s[n - 1 - i] = 0.5 * (1.0 + x);
+        w[n - 1 - i] = 0.5 * wt;
+    }
+}
+
+// solve_small_dense_system (ec_pic_nyquist_projected.cpp:5706): Gaussian
+// elimination with partial pivoting and the reference's singularity tests.
+bool solve_small_dense(std::vector<std::vector<double>> A, std::vector<double> b, std::vector<double>& x) {
+    const int n = (int)b.size();
+    double scale = 0.0;
+    for (const auto& row : A)
+        for (double v : row) scale = std::max(scale, std::fabs(v));
+    if (!(scale > 0.0) || !std::isfinite(scale)) return false;
+    double largest = 0.0, smallest = INFINITY;
+    for (int col = 0; col < n; ++col) {
+        int pr = col;
+        for (int r = col + 1; r < n; ++r)
+            if (std::fabs(A[r][col]) > std::fabs(A[pr][col])) pr = r;
+        const double piv = std::fabs(A[pr][col]);
+        if (!std::isfinite(piv) || piv <= 100.0 * DBL_EPSILON * scale) return false;
+        largest = std::max(largest, piv);
+        smallest = std::min(smallest, piv);
+        if (pr != col) {
+            std::swap(A[pr], A[col]);
+            std::swap(b[pr], b[col]);
+        }
+        for (int r = col + 1; r < n; ++r) {
+            const double f = A[r][col] / A[col][col];
+            for (int j = col; j < n; ++j) A[r][j] -= f * A[col][j];
+            b[r] -= f * b[col];
+        }
+    }
+    if (smallest <= 1.0e-12 * largest) return false;
+    x.assign(n, 0.0);
+    for (int r = n - 1; r >= 0; --r) {
+        double rhs = b[r];
+        for (int j = r + 1; j < n; ++j) rhs -= A[r][j] * x[j];
+        x[r] = rhs / A[r][r];
+        if (!std::isfinite(x[r])) return false;
+    }
+    return true;
+}
+
+struct Norms {
+    double rms_relative = INFINITY, max_relative = INFINITY, rms_absolute = INFINITY;
+    double rms_scaled = INFINITY, max_scaled = INFINITY;
+};
+
+bool is_even_nyquist(int i, int n) { return n > 1 && n % 2 == 0 && i == n / 2; }
+
+int alloc_particles(upic_ctx* c, ImplicitState& s, long cap, bool with_qm) {
+    int rc;
+    for (int k = 0; k < 2; ++k) {
+        if ((rc = alloc_soa(c, s.P[k], cap, true, with_qm))) return rc;
+        if ((rc = dalloc(c, &s.bx[k], cap)) || (rc = dalloc(c, &s.by[k], cap)) || (rc = dalloc(c, &s.bz[k], cap)))
+            return rc;
+    }
+    if ((rc = alloc_sortwork(c, s.sw, cap, s.tg))) return rc;
+    s.cap = cap;
+    return ensure_tmp3(c, cap);
+}
+
+void free_particles(upic_ctx* c, ImplicitState& s) {
+    for (int k = 0; k < 2; ++k) {
+        free_soa(c, s.P[k]);
+        dfree(c, s.bx[k]);
+        dfree(c, s.by[k]);
+        dfree(c, s.bz[k]);
+        s.bx[k] = s.by[k] = s.bz[k] = nullptr;
+    }
+    free_sortwork(c, s.sw);
+    s.cap = 0;
+}
+
+// Sort the active set by cell of x (shift 0) and make the sorted copy active.
+int sort_active(upic_ctx* c, ImplicitState& s) {
+    ParticleSoA& src = s.P[s.cur];
+    ParticleSoA& dst = s.P[1 - s.cur];
+    UPIC_CUDA(c, sort_particles_by_tile(s.tg, src, s.np, c->cfg.Lx, c->cfg.Ly, 0.0, s.sw, c->st));
+    UPIC_CUDA(c, permute_particles(src, dst, s.np, s.sw, c->st));
+    // vbar arrays ride along through the spare velocity slots of a temporary SoA
+    ParticleSoA vs{}, vd{};
+    vs.vx = s.bx[s.cur];
+    vs.vy = s.by[s.cur];
+    vs.vz = s.bz[s.cur];
+    vd.vx = s.bx[1 - s.cur];
+    vd.vy = s.by[1 - s.cur];
+    vd.vz = s.bz[1 - s.cur];
+    UPIC_CUDA(c, permute_particles(vs, vd, s.np, s.sw, c->st));
+    s.cur = 1 - s.cur;
+    return 0;
+}
+
+// One evaluation of the outer map at `guess` (evaluate_selective_current_map_at_layout
+// :5235 with every particle at level one).  Result in `out` (3 x N).  With
+// write_state the particles' trial end state goes to the spare set and the
+// trial spectra to spec_out.  Returns UPIC_ERR_LOCAL_PARTICLE when a local
+// solve fails (the step then fails, as SelectiveParticleRefinementNeeded
+// propagates in the reference), with the failure described in c->err.
+int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bool write_state,
+             MapStats* stats_out, bool* map_finite = nullptr) {
+    const upic_config& cf = c->cfg;
+    const int N = c->N;
+    // J_field = projected guess (:5264-5265), its spectra
+    UPIC_CUDA(c, cudaMemcpyAsync(s.Jf, guess, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, c->st));
+    if (cf.nyquist_projection) UPIC_CUDA(c, launch_project_nyquist(s.Jf, 3, c->nx, c->ny, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.Jhat, 3, 0, c->st, s.Jf));
+    // continuity + CN update + grad phi_mid and A^{n+1} spectra
+    CnArgs k{};
+    k.nx = c->nx;
+    k.ny = c->ny;
+    k.N = N;
+    k.kx = c->d_kx;
+    k.ky = c->d_ky;
+    k.k2 = c->d_k2;
+    k.excl = cf.nyquist_projection ? s.excl : nullptr;
+    k.Jhat = s.Jhat;
+    k.st = s.spec;
+    k.out = s.spec_out;
+    k.gspec = s.gspec;
+    k.dt = cf.dt;
+    k.kappa = cf.kappa;
+    k.sigma1 = cf.sigma1;
+    k.sigma2 = cf.sigma2;
+    UPIC_CUDA(c, launch_cn_kspace(k, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.gspec, 2, 1, c->st, nullptr, 2, s.rec, kIRec, kIRecGpm));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.gspec + 2 * (size_t)N, 3, 1, c->st, nullptr, 2, s.rec, kIRec, kIRecAe));
+    // particles: local fixed points and the orbit-averaged deposit
+    UPIC_CUDA(c, cudaMemsetAsync(s.acc, 0, sizeof(unsigned long long) * 6 * (size_t)N, c->st));
+    UPIC_CUDA(c, cudaMemsetAsync(s.dstats, 0, sizeof(MapStats), c->st));
+    UPIC_CUDA(c, cudaMemsetAsync(&s.dstats->first_fail_key, 0xff, sizeof(unsigned long long), c->st));
+    const ParticleSoA& p = s.P[s.cur];
+    const ParticleSoA& o = s.P[1 - s.cur];
+    ImplicitMapArgs a{};
+    a.x = p.x; a.y = p.y; a.Px = p.Px; a.Py = p.Py; a.Pz = p.Pz; a.vx = p.vx; a.vy = p.vy; a.vz = p.vz;
+    a.q = p.q; a.m = p.m; a.q0 = s.q0; a.m0 = s.m0; a.id = p.id;
+    a.ox = o.x; a.oy = o.y; a.oPx = o.Px; a.oPy = o.Py; a.oPz = o.Pz; a.ovx = o.vx; a.ovy = o.vy; a.ovz = o.vz;
+    a.obx = s.bx[1 - s.cur]; a.oby = s.by[1 - s.cur]; a.obz = s.bz[1 - s.cur];
+    a.np = s.np;
+    a.write_state = write_state ? 1 : 0;
+    a.Lx = cf.Lx; a.Ly = cf.Ly; a.inv_dx = 1.0 / s.dx; a.inv_dy = 1.0 / s.dy; a.inv_dV = 1.0 / s.dV;
+    a.dt = cf.dt; a.kappa = cf.kappa;
+    a.rec = s.rec;
+    a.split = cf.split_orbit_at_knots;
+    a.loc_rtol = cf.local_rtol; a.loc_atol = cf.local_atol; a.loc_damp = cf.local_damping;
+    a.loc_maxit = cf.local_max_iter;
+    a.chunks = s.sw.chunks;
+    a.nchunks = s.sw.nchunks;
+    a.acc = s.acc;
+    for (int d = 0; d < 3; ++d) a.scale[d] = s.scaleJ[d];
+    a.stats = s.dstats;
+    if (s.np > 0) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (c->profiling) {
+            UPIC_CUDA(c, cudaEventCreate(&e0));
+            UPIC_CUDA(c, cudaEventCreate(&e1));
+            UPIC_CUDA(c, cudaEventRecord(e0, c->st));
+        }
+        UPIC_CUDA(c, launch_implicit_map(s.order, s.uniform, s.tg, a, s.grid, c->st));
+        if (c->profiling) {
+            UPIC_CUDA(c, cudaEventRecord(e1, c->st));
+            c->prof_events.emplace_back(e0, e1);
+        }
+    }
+    UPIC_CUDA(c, launch_convert_acc(s.acc, N, s.scaleJ, out, nullptr, 0.0, 1, c->st));
+    if (cf.nyquist_projection) UPIC_CUDA(c, launch_project_nyquist(out, 3, c->nx, c->ny, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hstats, s.dstats, sizeof(MapStats), cudaMemcpyDeviceToHost, c->st));
+    if (map_finite) {
+        UPIC_CUDA(c, cudaMemsetAsync(s.dflag, 0, sizeof(int), c->st));
+        UPIC_CUDA(c, launch_nonfinite_flag(3 * N, out, s.dflag, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.hflag, s.dflag, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    }
+    int rc = sync(c);
+    if (rc) return rc;
+    if (stats_out) *stats_out = *s.hstats;
+    if (map_finite) *map_finite = *s.hflag == 0;
+    if (s.hstats->failures > 0) {
+        static const char* names[] = {"none", "nonfinite_map", "superluminal_map", "nonfinite_iterate",
+                                      "superluminal_iterate", "maximum_iterations", "too_many_knot_crossings"};
+        const unsigned long long key = s.hstats->first_fail_key;
+        const int reason = (int)(key & 0xffu);
+        char buf[256];
+        std::snprintf(buf, sizeof(buf),
+                      "local particle solve failed for %d particles (first: particle %llu, %s; "
+                      "local_max_iter=%d)",
+                      s.hstats->failures, key >> 8, reason < 7 ? names[reason] : "?", cf.local_max_iter);
+        return fail(c, UPIC_ERR_LOCAL_PARTICLE, buf);
+    }
+    return 0;
+}
+
+// finite_node_vector (:5051) of a 3 x N node vector.
+int all_finite(upic_ctx* c, ImplicitState& s, const double* v, bool& finite) {
+    UPIC_CUDA(c, cudaMemsetAsync(s.dflag, 0, sizeof(int), c->st));
+    UPIC_CUDA(c, launch_nonfinite_flag(3 * c->N, v, s.dflag, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hflag, s.dflag, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    const int rc = sync(c);
+    if (rc) return rc;
+    finite = *s.hflag == 0;
+    return 0;
+}
+
+// nonlinear_residual_norms (:5576) on node vectors.
+int residual_norms(upic_ctx* c, ImplicitState& s, const double* map, const double* guess, Norms& n) {
+    const upic_config& cf = c->cfg;
+    const double floor_rel = 64.0 * DBL_EPSILON * cf.kappa;
+    UPIC_CUDA(c, launch_residual_norms(c->N, map, guess, floor_rel, cf.nonlinear_atol, cf.nonlinear_rtol,
+                                       s.partials, kNormGrid, s.dnorm, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hnorm, s.dnorm, sizeof(NormSums), cudaMemcpyDeviceToHost, c->st));
+    int rc = sync(c);
+    if (rc) return rc;
+    const double cnt = 3.0 * c->N;
+    const NormSums& h = *s.hnorm;
+    n.rms_absolute = std::sqrt((h.r2[0] + h.r2[1]) / cnt);
+    const double map_rms = std::sqrt((h.map2[0] + h.map2[1]) / cnt);
+    const double guess_rms = std::sqrt((h.guess2[0] + h.guess2[1]) / cnt);
+    const double vrms = 0.5 * (map_rms + guess_rms);
+    n.rms_relative = n.rms_absolute / (vrms + floor_rel);
+    n.rms_scaled = n.rms_absolute / (cf.nonlinear_atol + cf.nonlinear_rtol * vrms);
+    n.max_relative = h.max_rel;
+    n.max_scaled = h.max_scaled;
+    return 0;
+}
+
+// anderson_type2_candidate (:5763) over the last m+1 history entries.
+int anderson_candidate(upic_ctx* c, ImplicitState& s, bool& ok) {
+    const upic_config& cf = c->cfg;
+    ok = false;
+    const int available = s.hcount - 1;
+    const int m = std::min(cf.anderson_memory, available);
+    if (m <= 0) return 0;
+    const int first = s.hcount - m - 1;
+    const double* r[kHist];
+    const double* x[kHist];
+    for (int k = 0; k <= m; ++k) {
+        r[k] = s.hr[first + k];
+        x[k] = s.hx[first + k];
+    }
+    const int n3 = 3 * c->N;
+    UPIC_CUDA(c, launch_anderson_dots(n3, r, m, s.partials, kNormGrid, s.ddots, c->st));
+    const int ndots = m * (m + 1) / 2 + m;
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hdots, s.ddots, sizeof(double) * ndots, cudaMemcpyDeviceToHost, c->st));
+    int rc = sync(c);
+    if (rc) return rc;
+    std::vector<std::vector<double>> gram(m, std::vector<double>(m, 0.0));
+    std::vector<double> rhs(m, 0.0);
+    int k = 0;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j <= i; ++j) {
+            gram[i][j] = gram[j][i] = s.hdots[k++];
+        }
+    double trace = 0.0;
+    for (int i = 0; i < m; ++i) {
+        rhs[i] = s.hdots[k++];
+        trace += gram[i][i];
+    }
+    if (!(trace > 0.0) || !std::isfinite(trace)) return 0;
+    std::vector<double> unreg;
+    if (!solve_small_dense(gram, rhs, unreg)) return 0;
+    const double regs = trace / (double)m;
+    for (int i = 0; i < m; ++i) gram[i][i] += cf.anderson_regularization * regs;
+    std::vector<double> gamma;
+    if (!solve_small_dense(gram, rhs, gamma)) return 0;
+    UPIC_CUDA(c, launch_anderson_candidate(n3, x, r, m, cf.anderson_damping, gamma.data(), s.cand, c->st));
+    ok = true;
+    return 0;
+}
+
+void push_history(upic_ctx* c, ImplicitState& s, const double* x, const double* r) {
+    const int keep = c->cfg.anderson_memory + 1;
+    if (s.hcount == keep) {
+        double* tx = s.hx[0];
+        double* tr = s.hr[0];
+        for (int k = 0; k + 1 < s.hcount; ++k) {
+            s.hx[k] = s.hx[k + 1];
+            s.hr[k] = s.hr[k + 1];
+        }
+        s.hx[s.hcount - 1] = tx;
+        s.hr[s.hcount - 1] = tr;
+        --s.hcount;
+    }
+    const size_t bytes = sizeof(double) * 3 * (size_t)c->N;
+    cudaMemcpyAsync(s.hx[s.hcount], x, bytes, cudaMemcpyDeviceToDevice, c->st);
+    cudaMemcpyAsync(s.hr[s.hcount], r, bytes, cudaMemcpyDeviceToDevice, c->st);
+    ++s.hcount;
+}
+
+void reset_history(upic_ctx* c, ImplicitState& s, const double* x, const double* r) {
+    s.hcount = 0;
+    push_history(c, s, x, r);
+}
+
+// The diagnostics row of the current state (compute_diagnostics :3521).
+int state_diagnostics(upic_ctx* c, ImplicitState& s, double* row) {
+    const upic_config& cf = c->cfg;
+    const int N = c->N;
+    UPIC_CUDA(c, launch_diag_spectra(N, c->d_kx, c->d_ky, s.spec, s.dspec, c->st));
+    // mode amplitudes from the spectra before the inverse transforms overwrite them
+    const int mode = cf.perturbation_mode;
+    const int im = ((mode % c->nx) + c->nx) % c->nx, jm = ((mode % c->ny) + c->ny) % c->ny;
+    const int idx = im * c->ny, idy = jm;
+    double2 modes[3];
+    UPIC_CUDA(c, cudaMemcpyAsync(&modes[0], s.spec + 2 * (size_t)N + idx, sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(&modes[1], s.dspec + idx, sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(&modes[2], s.dspec + 5 * (size_t)N + idy, sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 10, 1, c->st, nullptr, 1, s.dreal));
+    ImplicitDiagArgs d{};
+    d.N = N;
+    d.E = s.dreal;
+    d.B = s.dreal + 3 * (size_t)N;
+    d.divE = s.dreal + 6 * (size_t)N;
+    d.divA = s.dreal + 7 * (size_t)N;
+    d.psi = s.dreal + 8 * (size_t)N;
+    d.rho = s.dreal + 9 * (size_t)N;
+    d.sigma1 = cf.sigma1;
+    d.kappa = cf.kappa;
+    d.partials = s.partials;
+    d.grid = kNormGrid;
+    UPIC_CUDA(c, launch_implicit_diag(d, s.ddots, c->st));
+    const ParticleSoA& p = s.P[s.cur];
+    UPIC_CUDA(c, launch_kinetic(s.np, p.vx, p.vy, p.vz, s.uniform ? nullptr : p.m, s.m0, cf.kappa,
+                                s.partials + 32 * kNormGrid, kNormGrid, s.ddots + 20, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hdots, s.ddots, sizeof(double) * 22, cudaMemcpyDeviceToHost, c->st));
+    int rc = sync(c);
+    if (rc) return rc;
+    const double* h = s.hdots;
+    const double invN = 1.0 / N;
+    auto tot = [&](int k) { return h[2 * k] + h[2 * k + 1]; };
+    auto rel = [](double a, double b) { return b > 0.0 ? a / b : (a == 0.0 ? 0.0 : INFINITY); };
+    double* r = row;
+    r[UPIC_P3_GAUSS_RMS] = std::sqrt(tot(0) * invN);
+    r[UPIC_P3_GAUSS_MAX] = h[18];
+    r[UPIC_P3_DIVE_RMS] = std::sqrt(tot(1) * invN);
+    r[UPIC_P3_SIGMA1_RHO_RMS] = std::fabs(cf.sigma1) * std::sqrt(tot(2) * invN);
+    r[UPIC_P3_GAUSS_NORM_RMS] = r[UPIC_P3_DIVE_RMS] + r[UPIC_P3_SIGMA1_RHO_RMS];
+    r[UPIC_P3_GAUSS_RELATIVE] = rel(r[UPIC_P3_GAUSS_RMS], r[UPIC_P3_GAUSS_NORM_RMS]);
+    r[UPIC_P3_GAUGE_RMS] = std::sqrt(tot(3) * invN);
+    r[UPIC_P3_GAUGE_MAX] = h[19];
+    r[UPIC_P3_PSI_OVER_KAPPA2_RMS] = std::sqrt(tot(4) * invN) / (cf.kappa * cf.kappa);
+    r[UPIC_P3_DIVA_RMS] = std::sqrt(tot(5) * invN);
+    r[UPIC_P3_GAUGE_NORM_RMS] = r[UPIC_P3_PSI_OVER_KAPPA2_RMS] + r[UPIC_P3_DIVA_RMS];
+    r[UPIC_P3_GAUGE_RELATIVE] = rel(r[UPIC_P3_GAUGE_RMS], r[UPIC_P3_GAUGE_NORM_RMS]);
+    r[UPIC_P3_FIELD_ENERGY] = (0.5 / cf.sigma1 * tot(6) + 0.5 / cf.sigma2 * tot(7)) * s.dV;
+    r[UPIC_P3_KINETIC_ENERGY] = h[20] + h[21];
+    r[UPIC_P3_TOTAL_ENERGY] = r[UPIC_P3_FIELD_ENERGY] + r[UPIC_P3_KINETIC_ENERGY];
+    r[UPIC_P3_RHO_MODE] = std::hypot(modes[0].x, modes[0].y) * invN;
+    r[UPIC_P3_E_MODE_RE] = modes[1].x * invN;
+    r[UPIC_P3_E_MODE_IM] = modes[1].y * invN;
+    r[UPIC_P3_E_MODE_ABS] = std::hypot(modes[1].x, modes[1].y) * invN;
+    r[UPIC_P3_BZ_Y_MODE_RE] = modes[2].x * invN;
+    r[UPIC_P3_BZ_Y_MODE_IM] = modes[2].y * invN;
+    r[UPIC_P3_BZ_Y_MODE_ABS] = std::hypot(modes[2].x, modes[2].y) * invN;
+    return 0;
+}
+
+// One implicit step (nonlinear_step_uniform_subcycled :5878); info: the
+// UPIC_INFO_* entries.
+int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
+    const upic_config& cf = c->cfg;
+    const int N = c->N, n3 = 3 * N;
+    int rc;
+    if (s.np > 0 && (rc = sort_active(c, s))) return rc;
+    // A^n records for the orbit D_A and the start-point gather
+    UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec + 3 * (size_t)N, sizeof(double2) * 3 * N,
+                                 cudaMemcpyDeviceToDevice, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 3, 1, c->st, nullptr, 2, s.rec, kIRec, kIRecAn));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.guess, s.J, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
+    bool finite = true;
+    if ((rc = all_finite(c, s, s.guess, finite))) return rc;
+    if (!finite) return fail(c, UPIC_ERR_NONFINITE, "nonfinite initial macro-current predictor");
+    const bool anderson = cf.nonlinear_solver == UPIC_SOLVER_ANDERSON;
+    s.hcount = 0;
+    double prev_rms = INFINITY;
+    bool have_prefetched = false, converged = false;
+    int iterations = 0, anderson_steps = 0, picard_steps = 0;
+    Norms norms;
+    MapStats ms{};
+    for (int it = 0; it < cf.nonlinear_max_iter; ++it) {
+        if (!have_prefetched) {
+            if ((rc = eval_map(c, s, s.guess, s.map, false, &ms, &finite))) return rc;
+            if (!finite)
+                return fail(c, UPIC_ERR_NONCONVERGED, "uniform particle map returned a nonfinite macro current");
+        }
+        have_prefetched = false;
+        UPIC_CUDA(c, launch_axpy(n3, s.map, s.guess, -1.0, s.resid, c->st));
+        if ((rc = residual_norms(c, s, s.map, s.guess, norms))) return rc;
+        iterations = it + 1;
+        if (norms.rms_scaled <= 1.0 && norms.max_scaled <= 1.0) {
+            converged = true;
+            break;
+        }
+        if (anderson && std::isfinite(prev_rms) && norms.rms_relative > cf.anderson_growth_limit * prev_rms)
+            s.hcount = 0;
+        push_history(c, s, s.guess, s.resid);
+        bool used_anderson = false;
+        if (anderson && it >= cf.anderson_start && s.hcount >= 2) {
+            if ((rc = anderson_candidate(c, s, used_anderson))) return rc;
+            if (used_anderson) {
+                if ((rc = all_finite(c, s, s.cand, finite))) return rc;
+                used_anderson = finite;
+            }
+            if (!used_anderson) reset_history(c, s, s.guess, s.resid);
+        }
+        const double cur_rms = norms.rms_scaled, cur_max = norms.max_scaled;
+        // backtracking line search on the candidate (:6044-6084)
+        auto try_update = [&](bool& accepted) -> int {
+            accepted = false;
+            for (int bt = 0; bt <= 6; ++bt) {
+                const double alpha = std::ldexp(1.0, -bt);
+                UPIC_CUDA(c, launch_lerp(n3, s.guess, s.cand, alpha, s.trial, c->st));
+                bool tf = true;
+                int r2 = all_finite(c, s, s.trial, tf);
+                if (r2) return r2;
+                if (!tf) continue;
+                r2 = eval_map(c, s, s.trial, s.trial_map, false, &ms);
+                if (r2) return r2;
+                Norms tn;
+                if ((r2 = residual_norms(c, s, s.trial_map, s.trial, tn))) return r2;
+                if (!std::isfinite(tn.rms_scaled)) continue;
+                const bool dec = tn.rms_scaled <= (1.0 - 1.0e-4 * alpha) * cur_rms;
+                const bool safe = tn.max_scaled <= cf.anderson_growth_limit * cur_max;
+                if (dec && safe) {
+                    accepted = true;
+                    return 0;
+                }
+            }
+            return 0;
+        };
+        bool accepted = false, as_anderson = false;
+        if (used_anderson) {
+            if ((rc = try_update(accepted))) return rc;
+            as_anderson = accepted;
+            if (!accepted) reset_history(c, s, s.guess, s.resid);
+        }
+        if (!accepted) {
+            const double damping = anderson ? cf.anderson_damping : 1.0;
+            UPIC_CUDA(c, launch_axpy(n3, s.guess, s.resid, damping, s.cand, c->st));
+            if ((rc = try_update(accepted))) return rc;
+        }
+        if (!accepted)
+            return fail(c, UPIC_ERR_NONCONVERGED,
+                        "outer current Anderson/Picard backtracking failed at the prescribed macro dt");
+        if (as_anderson) ++anderson_steps;
+        else ++picard_steps;
+        prev_rms = norms.rms_relative;
+        std::swap(s.guess, s.trial);
+        std::swap(s.map, s.trial_map);
+        have_prefetched = true;
+    }
+    if (!converged) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "outer macro-current solve failed at dt=%g after %d iterations", cf.dt,
+                      iterations);
+        return fail(c, UPIC_ERR_NONCONVERGED, buf);
+    }
+    // final consistency evaluation (:6160) produces the accepted state
+    if ((rc = eval_map(c, s, s.guess, s.map, true, &ms))) return rc;
+    Norms fin;
+    if ((rc = residual_norms(c, s, s.map, s.guess, fin))) return rc;
+    if (!(fin.rms_scaled <= 1.0 && fin.max_scaled <= 1.0))
+        return fail(c, UPIC_ERR_NONCONVERGED,
+                    "final outer macro-current consistency evaluation failed at the prescribed macro dt");
+    // accept: particles from the trial set, v_prev = v^n, fields from the trial spectra
+    ParticleSoA& old = s.P[s.cur];
+    ParticleSoA& nw = s.P[1 - s.cur];
+    const size_t pb = sizeof(double) * s.np;
+    if (s.np > 0) {
+        UPIC_CUDA(c, cudaMemcpyAsync(nw.wx, old.vx, pb, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(nw.wy, old.vy, pb, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(nw.wz, old.vz, pb, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(nw.id, old.id, sizeof(int) * s.np, cudaMemcpyDeviceToDevice, c->st));
+        if (!s.uniform) {
+            UPIC_CUDA(c, cudaMemcpyAsync(nw.q, old.q, pb, cudaMemcpyDeviceToDevice, c->st));
+            UPIC_CUDA(c, cudaMemcpyAsync(nw.m, old.m, pb, cudaMemcpyDeviceToDevice, c->st));
+        }
+    }
+    s.cur = 1 - s.cur;
+    std::swap(s.spec, s.spec_out);
+    UPIC_CUDA(c, cudaMemcpyAsync(s.J, s.map, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
+    if (info) {
+        info[UPIC_INFO_ITERATIONS] = iterations;
+        info[UPIC_INFO_CONVERGED] = 1.0;
+        info[UPIC_INFO_FINAL_RMS_RESIDUAL] = fin.rms_relative;
+        info[UPIC_INFO_FINAL_MAX_PARTICLE_RESIDUAL] = fin.max_relative;
+        info[UPIC_INFO_LOCAL_ITER_MAX] = ms.iter_max;
+        info[UPIC_INFO_LOCAL_ITER_MEAN] = s.np > 0 ? (double)ms.iter_total / (double)s.np : 0.0;
+        info[UPIC_INFO_ANDERSON_STEPS] = anderson_steps;
+        info[UPIC_INFO_PICARD_STEPS] = picard_steps;
+    }
+    ++s.steps;
+    return sync(c);
+}
+
+__global__ void wrap_positions_kernel(double* x, double* y, long n, double Lx, double Ly) {
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+        double a = fmod(x[p] + 0.5 * Lx, Lx);
+        if (a < 0.0) a += Lx;
+        x[p] = a - 0.5 * Lx;
+        double b = fmod(y[p] + 0.5 * Ly, Ly);
+        if (b < 0.0) b += Ly;
+        y[p] = b - 0.5 * Ly;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+int implicit_create(upic_ctx* c) {
+    const upic_config& cf = c->cfg;
+    auto* s = new ImplicitState();
+    c->imp = s;
+    s->order = cf.spline_order;
+    s->nq = cf.orbit_quad_order;
+    s->dx = cf.Lx / c->nx;
+    s->dy = cf.Ly / c->ny;
+    s->dV = s->dx * s->dy * cf.Lz;
+    const int N = c->N;
+    // window guard: the orbit reaches kappa*dt from its start; sorting every
+    // step leaves no drift on top of that
+    const double reach = cf.kappa * cf.dt / std::min(s->dx, s->dy);
+    const int guard = cf.guard >= 0 ? cf.guard : (int)std::ceil(reach) + 1;
+    const int tile = cf.tile > 0 ? cf.tile : 8;
+    s->tg = make_tiles(c->nx, c->ny, tile, guard, s->order / 2, s->order / 2 + 1);
+    s->tg.key_origin_x = 0.5 * cf.Lx;
+    s->tg.key_origin_y = 0.5 * cf.Ly;
+    s->tg.key_shift = 0.0;
+    s->tg.chunk = 1024;
+    if (implicit_configure_smem(s->tg, s->order) != cudaSuccess)
+        return fail(c, UPIC_ERR_CUDA, "cudaFuncSetAttribute (implicit map) failed");
+    const int occ = implicit_map_occupancy(s->tg, s->order);
+    s->grid = c->nsm * (occ > 0 ? occ : 1);
+    std::vector<double> qs, qw;
+    gauss_legendre_01(s->nq, qs, qw);
+    if (implicit_set_quadrature(qs.data(), qw.data(), s->nq) != cudaSuccess)
+        return fail(c, UPIC_ERR_CUDA, "quadrature upload failed");
+    int rc;
+    if ((rc = dalloc(c, &s->spec, 9 * (size_t)N)) || (rc = dalloc(c, &s->spec_out, 9 * (size_t)N)) ||
+        (rc = dalloc(c, &s->Jhat, 3 * (size_t)N)) || (rc = dalloc(c, &s->gspec, 5 * (size_t)N)) ||
+        (rc = dalloc(c, &s->dspec, 10 * (size_t)N)) || (rc = dalloc(c, &s->dreal, 10 * (size_t)N)) ||
+        (rc = dalloc(c, &s->rec, (size_t)kIRec * N)) || (rc = dalloc(c, &s->excl, (size_t)N)) ||
+        (rc = dalloc(c, &s->acc, 8 * (size_t)N)) || (rc = dalloc(c, &s->J, 3 * (size_t)N)) ||
+        (rc = dalloc(c, &s->Jf, 3 * (size_t)N)) || (rc = dalloc(c, &s->guess, 3 * (size_t)N)) ||
+        (rc = dalloc(c, &s->map, 3 * (size_t)N)) || (rc = dalloc(c, &s->trial, 3 * (size_t)N)) ||
+        (rc = dalloc(c, &s->trial_map, 3 * (size_t)N)) || (rc = dalloc(c, &s->cand, 3 * (size_t)N)) ||
+        (rc = dalloc(c, &s->resid, 3 * (size_t)N)) || (rc = dalloc(c, &s->partials, 64 * (size_t)kNormGrid)) ||
+        (rc = dalloc(c, &s->dnorm, 1)) || (rc = dalloc(c, &s->dstats, 1)) || (rc = dalloc(c, &s->ddots, 32)) ||
+        (rc = dalloc(c, &s->dflag, 1)))
+        return rc;
+    for (int k = 0; k < kHist; ++k)
+        if ((rc = dalloc(c, &s->hx[k], 3 * (size_t)N)) || (rc = dalloc(c, &s->hr[k], 3 * (size_t)N))) return rc;
+    if (cudaMallocHost(&s->hnorm, sizeof(NormSums)) != cudaSuccess ||
+        cudaMallocHost(&s->hstats, sizeof(MapStats)) != cudaSuccess ||
+        cudaMallocHost(&s->hdots, sizeof(double) * 32) != cudaSuccess ||
+        cudaMallocHost(&s->hflag, sizeof(int)) != cudaSuccess)
+        return fail(c, UPIC_ERR_NOMEM, "cudaMallocHost failed");
+    std::vector<unsigned char> ex(N, 0);
+    for (int i = 0; i < c->nx; ++i)
+        for (int j = 0; j < c->ny; ++j)
+            ex[i * c->ny + j] = (is_even_nyquist(i, c->nx) || is_even_nyquist(j, c->ny)) ? 1 : 0;
+    if (cudaMemcpy(s->excl, ex.data(), N, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(c, UPIC_ERR_CUDA, "mask upload failed");
+    return 0;
+}
+
+void implicit_destroy(upic_ctx* c) {
+    if (!c || !c->imp) return;
+    ImplicitState* s = c->imp;
+    if (s->hnorm) cudaFreeHost(s->hnorm);
+    if (s->hstats) cudaFreeHost(s->hstats);
+    if (s->hdots) cudaFreeHost(s->hdots);
+    if (s->hflag) cudaFreeHost(s->hflag);
+    delete s;
+    c->imp = nullptr;
+}
+
+int implicit_set_particles(upic_ctx* c, long np, const double* x, const double* y, const double* P,
+                           const double* v, const double* v_prev, const double* q, const double* m) {
+    ImplicitState& s = *c->imp;
+    bool uniform = true;
+    double qabs = 0.0;
+    for (long p = 0; p < np; ++p) {
+        if (q[p] != q[0] || m[p] != m[0]) uniform = false;
+        qabs += std::fabs(q[p]);
+        const double* vp = v + 3 * p;
+        if (!std::isfinite(x[p]) || !std::isfinite(y[p]) || !std::isfinite(vp[0]) || !std::isfinite(vp[1]) ||
+            !std::isfinite(vp[2]))
+            return fail(c, UPIC_ERR_NONFINITE, "non-finite particle position or velocity");
+        // gamma_from_v (:623)
+        if ((vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]) / (c->cfg.kappa * c->cfg.kappa) >= 1.0)
+            return fail(c, UPIC_ERR_SUPERLUMINAL, "relativistic initial velocity must satisfy |v| < kappa");
+        if (!(m[p] > 0.0)) return fail(c, UPIC_ERR_ARGUMENT, "particle masses must be positive");
+    }
+    int rc;
+    if (np > s.cap || (!uniform && !s.P[0].q)) {
+        free_particles(c, s);
+        if ((rc = alloc_particles(c, s, std::max(np, s.cap), !uniform))) return rc;
+    }
+    if ((rc = ensure_tmp3(c, np))) return rc;
+    s.np = np;
+    s.cur = 0;
+    s.uniform = uniform;
+    s.q0 = np ? q[0] : 0.0;
+    s.m0 = np ? m[0] : 0.0;
+    s.qabs = qabs;
+    ParticleSoA& d = s.P[0];
+    if (np > 0) {
+        UPIC_CUDA(c, cudaMemcpyAsync(d.x, x, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(d.y, y, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        wrap_positions_kernel<<<gridn(np), 256, 0, c->st>>>(d.x, d.y, np, c->cfg.Lx, c->cfg.Ly);
+        count_launches(1);
+        if ((rc = upload3(c, P, np, d.Px, d.Py, d.Pz))) return rc;
+        if ((rc = upload3(c, v, np, d.vx, d.vy, d.vz))) return rc;
+        if ((rc = upload3(c, v_prev, np, d.wx, d.wy, d.wz))) return rc;
+        UPIC_CUDA(c, cudaMemcpyAsync(s.bx[0], d.vx, sizeof(double) * np, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.by[0], d.vy, sizeof(double) * np, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.bz[0], d.vz, sizeof(double) * np, cudaMemcpyDeviceToDevice, c->st));
+        if (!uniform) {
+            UPIC_CUDA(c, cudaMemcpyAsync(d.q, q, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+            UPIC_CUDA(c, cudaMemcpyAsync(d.m, m, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        }
+        if ((rc = iota(c, d.id, np))) return rc;
+    }
+    // fixed-point bound of the orbit-averaged current: |v| < kappa
+    const double bJ = qabs * c->cfg.kappa / s.dV;
+    s.scaleJ[0] = s.scaleJ[1] = s.scaleJ[2] = fixed_scale(bJ);
+    s.scaleJ[3] = fixed_scale(qabs / s.dV);
+    s.ready = false;
+    s.loaded = true;
+    s.steps = 0;
+    return sync(c);
+}
+
+int implicit_get_particles(upic_ctx* c, long np, double* x, double* y, double* P, double* v, double* v_prev) {
+    ImplicitState& s = *c->imp;
+    if (np != s.np) return fail(c, UPIC_ERR_ARGUMENT, "particle count does not match the context");
+    if (np == 0) return UPIC_OK;
+    ParticleSoA src = s.P[s.cur];
+    ParticleSoA dst = s.P[1 - s.cur];
+    UPIC_CUDA(c, unpermute_particles(src, dst, np, c->st));
+    int rc;
+    if (x) UPIC_CUDA(c, cudaMemcpyAsync(x, dst.x, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    if (y) UPIC_CUDA(c, cudaMemcpyAsync(y, dst.y, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    if (P && (rc = download3(c, P, np, dst.Px, dst.Py, dst.Pz))) return rc;
+    if ((rc = sync(c))) return rc;
+    if (v && (rc = download3(c, v, np, dst.vx, dst.vy, dst.vz))) return rc;
+    if ((rc = sync(c))) return rc;
+    if (v_prev && (rc = download3(c, v_prev, np, dst.wx, dst.wy, dst.wz))) return rc;
+    return sync(c);
+}
+
+int implicit_init_fields(upic_ctx* c, double* diag_row) {
+    ImplicitState& s = *c->imp;
+    const upic_config& cf = c->cfg;
+    const int N = c->N;
+    if (!s.loaded) return fail(c, UPIC_ERR_STATE, "upic_set_particles first");
+    int rc;
+    if (s.np > 0 && (rc = sort_active(c, s))) return rc;
+    ParticleSoA& p = s.P[s.cur];
+    // rho_e, J by point deposit (deposit_scalar_to_mesh :2117, deposit_current_to_mesh :2182)
+    UPIC_CUDA(c, cudaMemsetAsync(s.acc, 0, sizeof(unsigned long long) * 8 * (size_t)N, c->st));
+    if (s.np > 0) {
+        PointDepositArgs d{};
+        d.x = p.x; d.y = p.y; d.vx = p.vx; d.vy = p.vy; d.vz = p.vz;
+        d.q = s.uniform ? nullptr : p.q;
+        d.q0 = s.q0;
+        d.np = s.np;
+        d.nx = c->nx; d.ny = c->ny;
+        d.Lx = cf.Lx; d.Ly = cf.Ly; d.inv_dx = 1.0 / s.dx; d.inv_dy = 1.0 / s.dy; d.inv_dV = 1.0 / s.dV;
+        d.acc = s.acc;
+        for (int k = 0; k < 4; ++k) d.scale[k] = s.scaleJ[k];
+        UPIC_CUDA(c, launch_point_deposit(s.order, d, c->st));
+    }
+    // rho = rho_e + n0 with its mean subtracted and the Nyquist planes
+    // projected out (project_initial_state :3399) is, in k-space, the
+    // spectrum of rho_e with the k = 0 and excluded modes zeroed: the
+    // uniform background only enters the k = 0 mode.
+    double* rho = s.dreal;
+    UPIC_CUDA(c, launch_convert_acc(s.acc, N, s.scaleJ, s.J, rho, 0.0, 3, c->st));
+    if (cf.nyquist_projection) UPIC_CUDA(c, launch_project_nyquist(s.J, 3, c->nx, c->ny, c->st));
+    // spectra: phi from Poisson (solve_periodic_poisson_for_phi :3196), psi = A = U = 0
+    UPIC_CUDA(c, cudaMemsetAsync(s.spec, 0, sizeof(double2) * 9 * (size_t)N, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.spec + 2 * (size_t)N, 1, 0, c->st, rho));
+    UPIC_CUDA(c, launch_kspace_mask(s.spec + 2 * (size_t)N, 1, N, cf.nyquist_projection ? s.excl : nullptr, 1,
+                                    c->st));
+    UPIC_CUDA(c, launch_poisson_kspace(N, c->d_k2, s.spec + 2 * (size_t)N, 1.0 / cf.sigma1, s.spec, c->st));
+    UPIC_CUDA(c, launch_kspace_mask(s.spec, 1, N, cf.nyquist_projection ? s.excl : nullptr, 1, c->st));
+    // P = m gamma v (A = 0); v_prev from one backward Lorentz step; vbar = v
+    if (s.np > 0) {
+        UPIC_CUDA(c, launch_momentum_from_v(s.np, p.vx, p.vy, p.vz, s.uniform ? nullptr : p.m, s.m0, cf.kappa,
+                                            p.Px, p.Py, p.Pz, c->st));
+        UPIC_CUDA(c, launch_diag_spectra(N, c->d_kx, c->d_ky, s.spec, s.dspec, c->st));
+        UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 6, 1, c->st, nullptr, 1, s.dreal));
+        UPIC_CUDA(c, launch_history_velocity(s.order, c->nx, c->ny, cf.Lx, cf.Ly, s.dreal, s.dreal + 3 * (size_t)N,
+                                             s.np, p.x, p.y, p.vx, p.vy, p.vz, s.uniform ? nullptr : p.q, s.q0,
+                                             s.uniform ? nullptr : p.m, s.m0, cf.kappa, cf.dt, p.wx, p.wy, p.wz,
+                                             c->st));
+        const size_t pb = sizeof(double) * s.np;
+        UPIC_CUDA(c, cudaMemcpyAsync(s.bx[s.cur], p.vx, pb, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.by[s.cur], p.vy, pb, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.bz[s.cur], p.vz, pb, cudaMemcpyDeviceToDevice, c->st));
+    }
+    s.ready = true;
+    s.steps = 0;
+    c->steps = 0;
+    c->fields_ready = true;
+    if ((rc = sync(c))) return rc;
+    if (diag_row && (rc = state_diagnostics(c, s, diag_row))) return rc;
+    return UPIC_OK;
+}
+
+int implicit_get_field(upic_ctx* c, int which, double* host) {
+    ImplicitState& s = *c->imp;
+    const int N = c->N;
+    if (which >= UPIC_FIELD_JX && which <= UPIC_FIELD_JZ) {
+        UPIC_CUDA(c, cudaMemcpyAsync(host, s.J + (size_t)(which - UPIC_FIELD_JX) * N, sizeof(double) * N,
+                                     cudaMemcpyDeviceToHost, c->st));
+        return sync(c);
+    }
+    // spectra slot of each field: phi 0, psi 1, rho 2, A 3..5, U 6..8
+    int slot;
+    switch (which) {
+        case UPIC_FIELD_PHI: slot = 0; break;
+        case UPIC_FIELD_PSI: slot = 1; break;
+        case UPIC_FIELD_RHO: slot = 2; break;
+        case UPIC_FIELD_AX: case UPIC_FIELD_AY: case UPIC_FIELD_AZ: slot = 3 + which - UPIC_FIELD_AX; break;
+        case UPIC_FIELD_UX: case UPIC_FIELD_UY: case UPIC_FIELD_UZ: slot = 6 + which - UPIC_FIELD_UX; break;
+        default: return fail(c, UPIC_ERR_ARGUMENT, "unknown field");
+    }
+    UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec + (size_t)slot * N, sizeof(double2) * N, cudaMemcpyDeviceToDevice,
+                                 c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 1, 1, c->st, nullptr, 1, s.dreal));
+    UPIC_CUDA(c, cudaMemcpyAsync(host, s.dreal, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+
+}  // namespace upic_host
+
+using namespace upic_host;
+
+extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double* info) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (!c->imp) return fail(c, UPIC_ERR_STATE, "context was not created with UPIC_METHOD_CN_ORBIT");
+    ImplicitState& s = *c->imp;
+    if (!s.ready) return fail(c, UPIC_ERR_STATE, "upic_init_fields first");
+    if (nsteps < 0) return fail(c, UPIC_ERR_ARGUMENT, "nsteps < 0");
+    for (int k = 0; k < nsteps; ++k) {
+        int rc = implicit_one_step(c, s, info ? info + (size_t)k * UPIC_INFO_COUNT : nullptr);
+        if (rc) return rc;
+        c->steps = s.steps;
+        if (diag && (rc = state_diagnostics(c, s, diag + (size_t)k * UPIC_P3_DIAG_COUNT))) return rc;
+    }
+    return UPIC_OK;
+}

@@ -1,0 +1,1340 @@
+// Implicit energy-conserving orbit-averaged GM-HC-CN step kernels (sm_100a).
+//
+// Reference: Project3/ec_pic_nyquist_projected.cpp, the manuscript path
+// nonlinear_step_orbit (:6477) -> nonlinear_step_uniform_subcycled (:5878)
+// with a level-one layout -> evaluate_selective_current_map_at_layout
+// (:5235).  One evaluation of the outer map J -> J_map is: continuity and CN
+// potential update in k-space (cn_kspace_kernel), then per particle the
+// damped local fixed point on the orbit velocity vbar
+// (solve_local_particle_substep :4930, evaluate_local_particle_substep :4843)
+// followed by the orbit-averaged current deposit of the accepted orbit
+// (path_average_deposit_current :2784) -- all in implicit_map_kernel, one
+// thread per particle.  The grid runs in 2D (nz = 1): the z stencil of the
+// reference then sums to one, so its z factors and z-knot splits only change
+// rounding and are dropped here.
+#include <climits>
+
+#include "implicit_kernels.h"
+#include "upic_common.cuh"
+
+namespace upic {
+
+namespace {
+
+constexpr int kMapThreads = 128;
+constexpr int kMapWarps = kMapThreads / kWarp;
+constexpr int kKeyNone = -1;
+constexpr int kKeyEscape = -2;
+
+__constant__ double c_qs[kMaxQuad];
+__constant__ double c_qw[kMaxQuad];
+__constant__ int c_nq;
+
+// wrap1 (:704): x -> [-L/2, L/2)
+UPIC_D double wrap1(double x, double L) {
+    double y = fmod(x + 0.5 * L, L);
+    if (y < 0.0) y += L;
+    return y - 0.5 * L;
+}
+
+// Centered B-spline of degree ORDER on the stencil of grid coordinate u
+// (centered_bspline :1856, centered_bspline_derivative :1912, axis_stencil
+// :1971).  The stencil's first node is il = floor(u - (ORDER-1)/2); with
+// f = u - il each node's offset r_a = f - a lies on a fixed polynomial piece,
+// evaluated directly.  dw holds dS/dx = S'(r) / h.
+template <int ORDER>
+struct Stencil {
+    int il;
+    double w[ORDER + 1];
+    double dw[ORDER + 1];
+};
+
+template <int ORDER>
+UPIC_D void bspline(double u, double inv_h, Stencil<ORDER>& s) {
+    const double fl = floor(u - 0.5 * (double)(ORDER - 1));
+    s.il = (int)fl;
+    const double f = u - fl;
+    if (ORDER == 1) {
+        s.w[0] = 1.0 - f;
+        s.w[1] = f;
+        s.dw[0] = -inv_h;
+        s.dw[1] = inv_h;
+    } else if (ORDER == 2) {
+        const double z0 = 1.5 - f, r1 = f - 1.0, z2 = f - 0.5;
+        s.w[0] = 0.5 * z0 * z0;
+        s.w[1] = 0.75 - r1 * r1;
+        s.w[2] = 0.5 * z2 * z2;
+        s.dw[0] = -z0 * inv_h;
+        s.dw[1] = -2.0 * r1 * inv_h;
+        s.dw[2] = z2 * inv_h;
+    } else if (ORDER == 3) {
+        const double z0 = 2.0 - f, a1 = f - 1.0, a2 = 2.0 - f, z3 = f - 1.0;
+        s.w[0] = z0 * z0 * z0 / 6.0;
+        s.w[1] = (2.0 / 3.0) - a1 * a1 + 0.5 * a1 * a1 * a1;
+        s.w[2] = (2.0 / 3.0) - a2 * a2 + 0.5 * a2 * a2 * a2;
+        s.w[3] = z3 * z3 * z3 / 6.0;
+        s.dw[0] = -0.5 * z0 * z0 * inv_h;
+        s.dw[1] = (-2.0 * a1 + 1.5 * a1 * a1) * inv_h;
+        s.dw[2] = (2.0 * a2 - 1.5 * a2 * a2) * inv_h;
+        s.dw[3] = 0.5 * z3 * z3 * inv_h;
+    } else {
+        const double z0 = 2.5 - f, a1 = f - 1.0, r2 = f - 2.0, a3 = 3.0 - f, z4 = f - 1.5;
+        const double r22 = r2 * r2;
+        s.w[0] = z0 * z0 * z0 * z0 / 24.0;
+        s.w[1] = 55.0 / 96.0 + (5.0 / 24.0) * a1 - 1.25 * a1 * a1 + (5.0 / 6.0) * a1 * a1 * a1 -
+                 (1.0 / 6.0) * a1 * a1 * a1 * a1;
+        s.w[2] = 115.0 / 192.0 - (5.0 / 8.0) * r22 + 0.25 * r22 * r22;
+        s.w[3] = 55.0 / 96.0 + (5.0 / 24.0) * a3 - 1.25 * a3 * a3 + (5.0 / 6.0) * a3 * a3 * a3 -
+                 (1.0 / 6.0) * a3 * a3 * a3 * a3;
+        s.w[4] = z4 * z4 * z4 * z4 / 24.0;
+        s.dw[0] = -(z0 * z0 * z0 / 6.0) * inv_h;
+        s.dw[1] = (5.0 / 24.0 - 2.5 * a1 + 2.5 * a1 * a1 - (2.0 / 3.0) * a1 * a1 * a1) * inv_h;
+        s.dw[2] = r2 * (r22 - 1.25) * inv_h;
+        s.dw[3] = -(5.0 / 24.0 - 2.5 * a3 + 2.5 * a3 * a3 - (2.0 / 3.0) * a3 * a3 * a3) * inv_h;
+        s.dw[4] = (z4 * z4 * z4 / 6.0) * inv_h;
+    }
+}
+
+struct Geo {
+    int nx, ny;
+    double Lx, Ly, inv_dx, inv_dy;
+};
+
+template <int ORDER>
+UPIC_D void stencil_xy(const Geo& g, double x, double y, Stencil<ORDER>& sx, Stencil<ORDER>& sy) {
+    bspline<ORDER>((x + 0.5 * g.Lx) * g.inv_dx, g.inv_dx, sx);
+    bspline<ORDER>((y + 0.5 * g.Ly) * g.inv_dy, g.inv_dy, sy);
+}
+
+// Sum of record component block [off, off+3) at a wrapped position.
+template <int ORDER>
+UPIC_D void gather_rec3(const Geo& g, const double* __restrict__ rec, int off, double x, double y,
+                        double out[3]) {
+    Stencil<ORDER> sx, sy;
+    stencil_xy<ORDER>(g, x, y, sx, sy);
+    out[0] = out[1] = out[2] = 0.0;
+#pragma unroll
+    for (int a = 0; a <= ORDER; ++a) {
+        const int gx = wrap_index(sx.il + a, g.nx);
+#pragma unroll
+        for (int b = 0; b <= ORDER; ++b) {
+            const double* r = rec + (size_t)(gx * g.ny + wrap_index(sy.il + b, g.ny)) * kIRec + off;
+            const double w = sx.w[a] * sy.w[b];
+            out[0] = fma(__ldg(r), w, out[0]);
+            out[1] = fma(__ldg(r + 1), w, out[1]);
+            out[2] = fma(__ldg(r + 2), w, out[2]);
+        }
+    }
+}
+
+// Knot-split breakpoints of the orbit x0 + s dx, s in [0, 1]
+// (path_breakpoints_for_particle :2555); returns the count, or -1 when more
+// than kMaxBreaks are needed.
+template <int ORDER>
+UPIC_D int breakpoints(const Geo& g, double x0, double y0, double dxx, double dxy, int split,
+                       double* b) {
+    int nb = 0;
+    b[nb++] = 0.0;
+    b[nb++] = 1.0;
+    if (split) {
+        const double tol = 1.0e-13;
+        const double offset = 0.5 * (double)(ORDER - 1);
+#pragma unroll
+        for (int d = 0; d < 2; ++d) {
+            const double L = d == 0 ? g.Lx : g.Ly;
+            const double h = L / (double)(d == 0 ? g.nx : g.ny);
+            const double u0 = (wrap1(d == 0 ? x0 : y0, L) + 0.5 * L) / h;
+            const double du = (d == 0 ? dxx : dxy) / h;
+            if (fabs(du) < 1.0e-300) continue;
+            const double a0 = u0 - offset;
+            const double a1 = a0 + du;
+            const double lo = fmin(a0, a1), hi = fmax(a0, a1);
+            const long long first = (long long)floor(lo) + 1;
+            const long long last = (long long)ceil(hi) - 1;
+            for (long long m = first; m <= last; ++m) {
+                const double s = ((double)m - a0) / du;
+                if (s > tol && s < 1.0 - tol) {
+                    if (nb >= kMaxBreaks) return -1;
+                    b[nb++] = s;
+                }
+            }
+        }
+        // insertion sort, then drop near-duplicates
+        for (int i = 1; i < nb; ++i) {
+            const double v = b[i];
+            int j = i - 1;
+            while (j >= 0 && b[j] > v) {
+                b[j + 1] = b[j];
+                --j;
+            }
+            b[j + 1] = v;
+        }
+        int n = 0;
+        for (int i = 0; i < nb; ++i)
+            if (n == 0 || fabs(b[i] - b[n - 1]) > 1.0e-12) b[n++] = b[i];
+        nb = n;
+    }
+    return nb;
+}
+
+UPIC_D double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+UPIC_D double norm3(const double* a) { return sqrt(dot3(a, a)); }
+
+// gamma_from_p (:584)
+UPIC_D double gamma_p(const double* p, double mk) { return sqrt(1.0 + dot3(p, p) / (mk * mk)); }
+
+// Higuera-Cary rotation by B_eff (higuera_cary_rotate_with_K :4636,
+// beff_from_skew_K :4605).
+UPIC_D void hc_rotate(const double* pm, const double* B, double q, double m, double kappa, double dt,
+                      double* out) {
+    const double mk = m * kappa;
+    double u[3] = {pm[0] * (1.0 / mk), pm[1] * (1.0 / mk), pm[2] * (1.0 / mk)};
+    const double gm = sqrt(1.0 + dot3(u, u));
+    const double c = q * dt / (2.0 * m);
+    const double tau[3] = {c * B[0], c * B[1], c * B[2]};
+    const double tau2 = dot3(tau, tau);
+    const double udt = dot3(u, tau);
+    const double sigma = gm * gm - tau2;
+    const double ghc2 = 0.5 * (sigma + sqrt(sigma * sigma + 4.0 * (tau2 + udt * udt)));
+    const double ghc = sqrt(fmax(ghc2, 1.0));
+    const double t[3] = {tau[0] / ghc, tau[1] / ghc, tau[2] / ghc};
+    const double sf = 2.0 / (1.0 + dot3(t, t));
+    const double sv[3] = {sf * t[0], sf * t[1], sf * t[2]};
+    const double up[3] = {u[0] + (u[1] * t[2] - u[2] * t[1]), u[1] + (u[2] * t[0] - u[0] * t[2]),
+                          u[2] + (u[0] * t[1] - u[1] * t[0])};
+    const double upl[3] = {u[0] + (up[1] * sv[2] - up[2] * sv[1]), u[1] + (up[2] * sv[0] - up[0] * sv[2]),
+                           u[2] + (up[0] * sv[1] - up[1] * sv[0])};
+    out[0] = mk * upl[0];
+    out[1] = mk * upl[1];
+    out[2] = mk * upl[2];
+}
+
+// kinetic_secant_velocity (:682)
+UPIC_D void secant(const double* a, const double* b, double m, double kappa, double* v) {
+    const double mk = m * kappa;
+    const double s = 1.0 / (m * (gamma_p(a, mk) + gamma_p(b, mk)));
+    v[0] = s * (a[0] + b[0]);
+    v[1] = s * (a[1] + b[1]);
+    v[2] = s * (a[2] + b[2]);
+}
+
+struct LocalIn {
+    double x0, y0;
+    double P0[3];
+    double A0p[3];
+    double pstart[3];
+    double q, m;
+};
+
+struct LocalOut {
+    double vbar_map[3];
+    double P_end[3];
+    double v_end[3];
+    double x1, y1;
+};
+
+// One evaluation of the particle map at guess vbar (evaluate_local_particle_substep
+// :4843 with h = dt, theta0 = 0, theta1 = 1).  b/nb: breakpoints of the orbit.
+template <int ORDER>
+UPIC_D bool evaluate(const Geo& g, const double* __restrict__ rec, double dt, double kappa, int split,
+                     const LocalIn& in, const double* guess, LocalOut& o, double* b, int& nb) {
+    const double dxx = dt * guess[0], dxy = dt * guess[1];
+    o.x1 = wrap1(in.x0 + dxx, g.Lx);
+    o.y1 = wrap1(in.y0 + dxy, g.Ly);
+    double A1p[3];
+    gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, A1p);
+    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
+                           0.5 * (in.A0p[2] + A1p[2])};
+    nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
+    if (nb < 0) return false;
+    // orbit averages: grad phi_mid along the path and D_A (:2738, :2958)
+    double gp0 = 0.0, gp1 = 0.0;
+    double D[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    const int nq = c_nq;
+    for (int k = 0; k + 1 < nb; ++k) {
+        const double sa = b[k], len = b[k + 1] - b[k];
+        if (len <= 0.0) continue;
+        for (int iq = 0; iq < nq; ++iq) {
+            const double s = sa + len * c_qs[iq];
+            const double wq = len * c_qw[iq];
+            const double xs = wrap1(in.x0 + s * dxx, g.Lx);
+            const double ys = wrap1(in.y0 + s * dxy, g.Ly);
+            Stencil<ORDER> sx, sy;
+            stencil_xy<ORDER>(g, xs, ys, sx, sy);
+            double g0 = 0.0, g1 = 0.0;
+            double d[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+            const double s1 = 1.0 - s;
+#pragma unroll
+            for (int a = 0; a <= ORDER; ++a) {
+                const int gx = wrap_index(sx.il + a, g.nx);
+#pragma unroll
+                for (int bb = 0; bb <= ORDER; ++bb) {
+                    const double* r = rec + (size_t)(gx * g.ny + wrap_index(sy.il + bb, g.ny)) * kIRec;
+                    const double2 r01 = __ldg(reinterpret_cast<const double2*>(r));
+                    const double2 r23 = __ldg(reinterpret_cast<const double2*>(r + 2));
+                    const double2 r45 = __ldg(reinterpret_cast<const double2*>(r + 4));
+                    const double2 r67 = __ldg(reinterpret_cast<const double2*>(r + 6));
+                    const double sh = sx.w[a] * sy.w[bb];
+                    const double dsx = sx.dw[a] * sy.w[bb];
+                    const double dsy = sx.w[a] * sy.dw[bb];
+                    g0 = fma(r01.x, sh, g0);
+                    g1 = fma(r01.y, sh, g1);
+                    const double av[3] = {s1 * r23.x + s * r45.y, s1 * r23.y + s * r67.x, s1 * r45.x + s * r67.y};
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        d[c][0] = fma(av[c], dsx, d[c][0]);
+                        d[c][1] = fma(av[c], dsy, d[c][1]);
+                    }
+                }
+            }
+            gp0 = fma(wq, g0, gp0);
+            gp1 = fma(wq, g1, gp1);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                D[c][0] = fma(wq, d[c][0], D[c][0]);
+                D[c][1] = fma(wq, d[c][1], D[c][1]);
+            }
+        }
+    }
+    // D vbar and the skew part K = D^T - D as B_eff (:4585-4620); the z
+    // columns of D vanish in 2D.
+    const double Dv[3] = {D[0][0] * guess[0] + D[0][1] * guess[1], D[1][0] * guess[0] + D[1][1] * guess[1],
+                          D[2][0] * guess[0] + D[2][1] * guess[1]};
+    const double B[3] = {D[2][1], -D[2][0], D[1][0] - D[0][1]};
+    const double q = in.q, m = in.m, hq = 0.5 * q * dt;
+    const double gpb[3] = {gp0, gp1, 0.0};
+    double pm[3], pp[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pm[c] = ((in.P0[c] - q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
+    hc_rotate(pm, B, q, m, kappa, dt, pp);
+    double pend[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        o.P_end[c] = ((pp[c] + q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
+        pend[c] = o.P_end[c] - q * A1p[c];
+    }
+    const double gam = gamma_p(pend, m * kappa);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.v_end[c] = pend[c] * (1.0 / (m * gam));
+    double vm[3], vp[3];
+    secant(pm, in.pstart, m, kappa, vm);
+    secant(pend, pp, m, kappa, vp);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.vbar_map[c] = 0.5 * (vm[c] + vp[c]);
+    return true;
+}
+
+UPIC_D bool finite3(const double* v) { return isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]); }
+
+UPIC_D int window_coord(int s, int origin, int n, int w, int span) {
+    const int d = (s - origin) & (n - 1);
+    return d <= w - span ? d : -1;
+}
+
+template <int ORDER, bool UNIFORM>
+__global__ void __launch_bounds__(kMapThreads)
+implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
+    constexpr int S = ORDER + 1;
+    constexpr int SS = S * S;
+    constexpr int NV = 3 * SS;
+    constexpr int RW = SS + 3;
+    constexpr int NPER = (NV + 31) / 32;
+    extern __shared__ unsigned long long smem_u64[];
+    const int WN = tg.wx * tg.wy;
+    unsigned long long* whi = smem_u64;
+    unsigned long long* wlo = whi + 3 * WN;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* srow = reinterpret_cast<double*>(wlo + 3 * WN) + warp * 32 * RW;
+    int* sgk = reinterpret_cast<int*>(reinterpret_cast<double*>(wlo + 3 * WN) + kMapWarps * 32 * RW) + warp * 32;
+
+    const Geo g{tg.nx, tg.ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    const int nx = tg.nx, ny = tg.ny, N = nx * ny;
+    const int nch = *a.nchunks;
+    const int c_begin = (int)(((long long)blockIdx.x * nch) / gridDim.x);
+    const int c_end = (int)(((long long)(blockIdx.x + 1) * nch) / gridDim.x);
+
+    // values owned by this lane in the grouped reduction
+    int t_ab[NPER], t_a[NPER], t_b[NPER], t_c[NPER], t_off[NPER];
+#pragma unroll
+    for (int r = 0; r < NPER; ++r) {
+        const int t = lane + 32 * r;
+        const int ab = t < NV ? t / 3 : 0;
+        t_ab[r] = ab;
+        t_a[r] = ab / S;
+        t_b[r] = ab % S;
+        t_c[r] = t < NV ? t - 3 * ab : 0;
+        t_off[r] = t_a[r] * tg.wy + t_b[r];
+    }
+
+    unsigned long long it_total = 0;
+    int it_max = 0, nfail = 0;
+    unsigned long long first_fail = ~0ull;
+    double worst = 0.0;
+
+    int cur_tile = -1, ox = 0, oy = 0;
+    for (int ci = c_begin; ci < c_end; ++ci) {
+        const Chunk ch = a.chunks[ci];
+        if (ch.tile != cur_tile) {
+            __syncthreads();
+            if (cur_tile >= 0) {
+                for (int idx = threadIdx.x; idx < 3 * WN; idx += blockDim.x) {
+                    const unsigned long long hi = whi[idx], lo = wlo[idx];
+                    if ((hi | lo) == 0ull) continue;
+                    const int cc = idx / WN, widx = idx - cc * WN;
+                    const int lx = widx / tg.wy, ly = widx - lx * tg.wy;
+                    const int gx = tg.full_x ? lx : wrap_index(ox + lx, nx);
+                    const int gy = tg.full_y ? ly : wrap_index(oy + ly, ny);
+                    atomicAdd(&a.acc[(size_t)(2 * cc) * N + gx * ny + gy], hi);
+                    atomicAdd(&a.acc[(size_t)(2 * cc + 1) * N + gx * ny + gy], lo);
+                }
+                __syncthreads();
+            }
+            for (int idx = threadIdx.x; idx < 6 * WN; idx += blockDim.x) whi[idx] = 0ull;
+            cur_tile = ch.tile;
+            const int tx = cur_tile / tg.nty, ty = cur_tile - tx * tg.nty;
+            ox = tg.full_x ? 0 : tx * tg.tile_x - tg.guard - tg.lo;
+            oy = tg.full_y ? 0 : ty * tg.tile_y - tg.guard - tg.lo;
+            __syncthreads();
+        }
+        for (int base = ch.start; base < ch.end; base += kMapThreads) {
+            const int p = base + threadIdx.x;
+            const bool active = p < ch.end;
+            bool ok = false;
+            double vb[3] = {0.0, 0.0, 0.0};
+            double bk[kMaxBreaks];
+            int nb = 0;
+            LocalIn in;
+            if (active) {
+                in.x0 = a.x[p];
+                in.y0 = a.y[p];
+                in.P0[0] = a.Px[p];
+                in.P0[1] = a.Py[p];
+                in.P0[2] = a.Pz[p];
+                in.q = UNIFORM ? a.q0 : a.q[p];
+                in.m = UNIFORM ? a.m0 : a.m[p];
+                gather_rec3<ORDER>(g, a.rec, kIRecAn, in.x0, in.y0, in.A0p);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) in.pstart[c] = in.P0[c] - in.q * in.A0p[c];
+                double guess[3] = {a.vx[p], a.vy[p], a.vz[p]};
+                // solve_local_particle_substep (:4930)
+                int reason = kLocalMaxIter;
+                int iters = 0;
+                double scaled = INFINITY;
+                LocalOut o;
+                for (int it = 0; it < a.loc_maxit; ++it) {
+                    if (!evaluate<ORDER>(g, a.rec, a.dt, a.kappa, a.split, in, guess, o, bk, nb)) {
+                        reason = kLocalTooManyCrossings;
+                        break;
+                    }
+                    ++iters;
+                    if (!finite3(o.vbar_map)) {
+                        reason = kLocalNonfiniteMap;
+                        break;
+                    }
+                    if (norm3(o.vbar_map) >= a.kappa) {
+                        reason = kLocalSuperluminalMap;
+                        break;
+                    }
+                    const double res[3] = {o.vbar_map[0] - guess[0], o.vbar_map[1] - guess[1],
+                                           o.vbar_map[2] - guess[2]};
+                    const double sc = 0.5 * (norm3(o.vbar_map) + norm3(guess));
+                    scaled = norm3(res) / (a.loc_atol + a.loc_rtol * sc);
+                    if (scaled <= 1.0) {
+                        reason = kLocalOk;
+                        break;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) guess[c] += a.loc_damp * res[c];
+                    if (!finite3(guess)) {
+                        reason = kLocalNonfiniteIterate;
+                        break;
+                    }
+                    if (norm3(guess) >= a.kappa) {
+                        reason = kLocalSuperluminalIterate;
+                        break;
+                    }
+                }
+                it_total += (unsigned long long)iters;
+                it_max = max(it_max, iters);
+                worst = fmax(worst, isfinite(scaled) ? scaled : 1.0e300);
+                ok = reason == kLocalOk;
+                if (!ok) {
+                    ++nfail;
+                    const unsigned long long key = ((unsigned long long)(unsigned)a.id[p] << 8) | (unsigned)reason;
+                    first_fail = key < first_fail ? key : first_fail;
+                } else {
+                    vb[0] = guess[0];
+                    vb[1] = guess[1];
+                    vb[2] = guess[2];
+                    if (a.write_state) {
+                        a.ox[p] = o.x1;
+                        a.oy[p] = o.y1;
+                        a.oPx[p] = o.P_end[0];
+                        a.oPy[p] = o.P_end[1];
+                        a.oPz[p] = o.P_end[2];
+                        a.ovx[p] = o.v_end[0];
+                        a.ovy[p] = o.v_end[1];
+                        a.ovz[p] = o.v_end[2];
+                        a.obx[p] = guess[0];
+                        a.oby[p] = guess[1];
+                        a.obz[p] = guess[2];
+                    }
+                }
+            }
+            // Orbit-averaged deposit of the accepted orbit (:2784): item k of a
+            // particle is its k-th (segment, quadrature point); the warp works
+            // through the items in rounds and reduces equal window keys.
+            const double dxx = a.dt * vb[0], dxy = a.dt * vb[1];
+            const double qa = ok ? in.q * a.inv_dV : 0.0;
+            const double val[3] = {qa * vb[0], qa * vb[1], qa * vb[2]};
+            const int nq = c_nq;
+            const int nitems = ok ? (nb - 1) * nq : 0;
+            const int rounds = __reduce_max_sync(0xffffffffu, nitems);
+            for (int rd = 0; rd < rounds; ++rd) {
+                int key = kKeyNone, gx0 = 0, gy0 = 0;
+                Stencil<ORDER> sx, sy;
+                double wq = 0.0;
+                if (rd < nitems) {
+                    const int k = rd / nq, iq = rd - k * nq;
+                    const double sa = bk[k], len = bk[k + 1] - bk[k];
+                    if (len > 0.0) {
+                        const double s = sa + len * c_qs[iq];
+                        wq = len * c_qw[iq];
+                        const double xs = wrap1(in.x0 + s * dxx, g.Lx);
+                        const double ys = wrap1(in.y0 + s * dxy, g.Ly);
+                        stencil_xy<ORDER>(g, xs, ys, sx, sy);
+                        gx0 = wrap_index(sx.il, nx);
+                        gy0 = wrap_index(sy.il, ny);
+                        const int lx = tg.full_x ? gx0 : window_coord(sx.il, ox, nx, tg.wx, S);
+                        const int ly = tg.full_y ? gy0 : window_coord(sy.il, oy, ny, tg.wy, S);
+                        key = (lx < 0 || ly < 0) ? kKeyEscape : lx * tg.wy + ly;
+                    }
+                }
+                const unsigned full = 0xffffffffu;
+                const unsigned lt = (1u << lane) - 1u;
+                const unsigned valid = __ballot_sync(full, key >= 0);
+                const unsigned esc = __ballot_sync(full, key == kKeyEscape);
+                const unsigned peers = __match_any_sync(full, key);
+                int row = -1, nvalid = 0, ngroups = 0;
+                unsigned heads = 0u;
+                for (unsigned rem = valid; rem;) {
+                    const int l = __ffs(rem) - 1;
+                    const unsigned gm = __shfl_sync(full, peers, l);
+                    const int gk = __shfl_sync(full, key, l);
+                    if ((gm >> lane) & 1u) row = nvalid + __popc(gm & lt);
+                    if (lane == 0) sgk[ngroups] = gk;
+                    heads |= 1u << nvalid;
+                    nvalid += __popc(gm);
+                    rem &= ~gm;
+                    ++ngroups;
+                }
+                if (key == kKeyEscape) row = nvalid + __popc(esc & lt);
+                if (row >= 0) {
+                    double* mine = srow + row * RW;
+#pragma unroll
+                    for (int ia = 0; ia < S; ++ia)
+#pragma unroll
+                        for (int ib = 0; ib < S; ++ib) mine[ia * S + ib] = wq * sx.w[ia] * sy.w[ib];
+                    mine[SS + 0] = val[0];
+                    mine[SS + 1] = val[1];
+                    mine[SS + 2] = val[2];
+                }
+                __syncwarp();
+                {
+                    unsigned e = esc;
+                    int erow = nvalid;
+                    while (e) {
+                        const int j = __ffs(e) - 1;
+                        e &= e - 1;
+                        const int gxj = __shfl_sync(full, gx0, j);
+                        const int gyj = __shfl_sync(full, gy0, j);
+#pragma unroll
+                        for (int r = 0; r < NPER; ++r) {
+                            const int t = lane + 32 * r;
+                            if (t < NV) {
+                                const double v = srow[erow * RW + SS + t_c[r]] * srow[erow * RW + t_ab[r]];
+                                if (v != 0.0) {
+                                    const int gi = wrap_index(gxj + t_a[r], nx) * ny + wrap_index(gyj + t_b[r], ny);
+                                    const Fixed2 f = to_fixed(v, a.scale[t_c[r]]);
+                                    atomicAdd(&a.acc[(size_t)(2 * t_c[r]) * N + gi], f.hi);
+                                    atomicAdd(&a.acc[(size_t)(2 * t_c[r] + 1) * N + gi], f.lo);
+                                }
+                            }
+                        }
+                        ++erow;
+                    }
+                }
+                {
+                    unsigned h = heads;
+                    int gi = 0;
+                    while (h) {
+                        const int rs = __ffs(h) - 1;
+                        h &= h - 1;
+                        const int re = h ? __ffs(h) - 1 : nvalid;
+                        const int kk = sgk[gi++];
+#pragma unroll
+                        for (int r = 0; r < NPER; ++r) {
+                            const int t = lane + 32 * r;
+                            if (t < NV) {
+                                double s0 = 0.0;
+                                const int iw = t_ab[r], iv = SS + t_c[r];
+                                for (int j = rs; j < re; ++j) s0 = fma(srow[j * RW + iv], srow[j * RW + iw], s0);
+                                if (s0 != 0.0) {
+                                    int widx;
+                                    if (tg.full_x || tg.full_y) {
+                                        const int kx = kk / tg.wy, ky = kk - kx * tg.wy;
+                                        int nxl = kx + t_a[r], nyl = ky + t_b[r];
+                                        if (tg.full_x) nxl &= tg.wx - 1;
+                                        if (tg.full_y) nyl &= tg.wy - 1;
+                                        widx = nxl * tg.wy + nyl;
+                                    } else {
+                                        widx = kk + t_off[r];
+                                    }
+                                    const Fixed2 f = to_fixed(s0, a.scale[t_c[r]]);
+                                    atomicAdd(&whi[t_c[r] * WN + widx], f.hi);
+                                    atomicAdd(&wlo[t_c[r] * WN + widx], f.lo);
+                                }
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+    }
+    __syncthreads();
+    if (cur_tile >= 0) {
+        for (int idx = threadIdx.x; idx < 3 * WN; idx += blockDim.x) {
+            const unsigned long long hi = whi[idx], lo = wlo[idx];
+            if ((hi | lo) == 0ull) continue;
+            const int cc = idx / WN, widx = idx - cc * WN;
+            const int lx = widx / tg.wy, ly = widx - lx * tg.wy;
+            const int gx = tg.full_x ? lx : wrap_index(ox + lx, nx);
+            const int gy = tg.full_y ? ly : wrap_index(oy + ly, ny);
+            atomicAdd(&a.acc[(size_t)(2 * cc) * N + gx * ny + gy], hi);
+            atomicAdd(&a.acc[(size_t)(2 * cc + 1) * N + gx * ny + gy], lo);
+        }
+    }
+    // statistics (integer atomics and max over bit patterns: order independent)
+    MapStats* st = a.stats;
+    for (int o = 16; o > 0; o >>= 1) {
+        it_total += __shfl_xor_sync(0xffffffffu, it_total, o);
+        it_max = max(it_max, __shfl_xor_sync(0xffffffffu, it_max, o));
+        nfail += __shfl_xor_sync(0xffffffffu, nfail, o);
+        const unsigned long long ff = __shfl_xor_sync(0xffffffffu, first_fail, o);
+        first_fail = ff < first_fail ? ff : first_fail;
+        worst = fmax(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+    }
+    if (lane == 0) {
+        if (it_total) atomicAdd(&st->iter_total, it_total);
+        atomicMax(&st->iter_max, it_max);
+        if (nfail) {
+            atomicAdd(&st->failures, nfail);
+            atomicMin(&st->first_fail_key, first_fail);
+        }
+        atomicMax(&st->worst_scaled_bits, (unsigned long long)__double_as_longlong(worst));
+    }
+}
+
+// ---- start-up point deposit -------------------------------------------------
+template <int ORDER>
+__global__ void point_deposit_kernel(PointDepositArgs a) {
+    const Geo g{a.nx, a.ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    const int N = a.nx * a.ny;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < a.np; p += (long)gridDim.x * blockDim.x) {
+        Stencil<ORDER> sx, sy;
+        stencil_xy<ORDER>(g, a.x[p], a.y[p], sx, sy);
+        const double q = a.q ? a.q[p] : a.q0;
+        const double qa = q * a.inv_dV;
+        const double val[4] = {qa * a.vx[p], qa * a.vy[p], qa * a.vz[p], qa};
+        for (int ia = 0; ia <= ORDER; ++ia) {
+            const int gx = wrap_index(sx.il + ia, a.nx);
+            for (int ib = 0; ib <= ORDER; ++ib) {
+                const int node = gx * a.ny + wrap_index(sy.il + ib, a.ny);
+                const double w = sx.w[ia] * sy.w[ib];
+                for (int c = 0; c < 4; ++c) {
+                    const double v = val[c] * w;
+                    if (v == 0.0) continue;
+                    const Fixed2 f = to_fixed(v, a.scale[c]);
+                    atomicAdd(&a.acc[(size_t)(2 * c) * N + node], f.hi);
+                    atomicAdd(&a.acc[(size_t)(2 * c + 1) * N + node], f.lo);
+                }
+            }
+        }
+    }
+}
+
+template <int ORDER>
+__global__ void gather3_kernel(int nx, int ny, double Lx, double Ly, const double* f3, long np,
+                               const double* x, const double* y, double* out3) {
+    const Geo g{nx, ny, Lx, Ly, nx / Lx, ny / Ly};
+    const int N = nx * ny;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
+        Stencil<ORDER> sx, sy;
+        stencil_xy<ORDER>(g, x[p], y[p], sx, sy);
+        double o[3] = {0.0, 0.0, 0.0};
+        for (int ia = 0; ia <= ORDER; ++ia) {
+            const int gx = wrap_index(sx.il + ia, nx);
+            for (int ib = 0; ib <= ORDER; ++ib) {
+                const int node = gx * ny + wrap_index(sy.il + ib, ny);
+                const double w = sx.w[ia] * sy.w[ib];
+                for (int c = 0; c < 3; ++c) o[c] = fma(f3[(size_t)c * N + node], w, o[c]);
+            }
+        }
+        for (int c = 0; c < 3; ++c) out3[3 * p + c] = o[c];
+    }
+}
+
+template <int ORDER>
+__global__ void history_velocity_kernel(int nx, int ny, double Lx, double Ly, const double* E3,
+                                        const double* B3, long np, const double* x, const double* y,
+                                        const double* vx, const double* vy, const double* vz,
+                                        const double* qa, double q0, const double* ma, double m0,
+                                        double kappa, double dt, double* wx, double* wy, double* wz) {
+    const Geo g{nx, ny, Lx, Ly, nx / Lx, ny / Ly};
+    const int N = nx * ny;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
+        Stencil<ORDER> sx, sy;
+        stencil_xy<ORDER>(g, x[p], y[p], sx, sy);
+        double E[3] = {0.0, 0.0, 0.0}, B[3] = {0.0, 0.0, 0.0};
+        for (int ia = 0; ia <= ORDER; ++ia) {
+            const int gx = wrap_index(sx.il + ia, nx);
+            for (int ib = 0; ib <= ORDER; ++ib) {
+                const int node = gx * ny + wrap_index(sy.il + ib, ny);
+                const double w = sx.w[ia] * sy.w[ib];
+                for (int c = 0; c < 3; ++c) {
+                    E[c] = fma(E3[(size_t)c * N + node], w, E[c]);
+                    B[c] = fma(B3[(size_t)c * N + node], w, B[c]);
+                }
+            }
+        }
+        const double q = qa ? qa[p] : q0, m = ma ? ma[p] : m0;
+        const double v[3] = {vx[p], vy[p], vz[p]};
+        const double beta2 = dot3(v, v) / (kappa * kappa);
+        const double gam = 1.0 / sqrt(fmax(1.0e-300, 1.0 - beta2));
+        const double pn[3] = {m * gam * v[0], m * gam * v[1], m * gam * v[2]};
+        const double vxb[3] = {v[1] * B[2] - v[2] * B[1], v[2] * B[0] - v[0] * B[2], v[0] * B[1] - v[1] * B[0]};
+        const double pp[3] = {pn[0] - dt * (q * (E[0] + vxb[0])), pn[1] - dt * (q * (E[1] + vxb[1])),
+                              pn[2] - dt * (q * (E[2] + vxb[2]))};
+        const double gp = gamma_p(pp, m * kappa);
+        wx[p] = pp[0] * (1.0 / (m * gp));
+        wy[p] = pp[1] * (1.0 / (m * gp));
+        wz[p] = pp[2] * (1.0 / (m * gp));
+    }
+}
+
+// ---- k-space map fields -----------------------------------------------------
+UPIC_D double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+UPIC_D double2 cscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+UPIC_D double2 cik(double k, double2 z) { return make_double2(-k * z.y, k * z.x); }
+
+__global__ void cn_kspace_kernel(CnArgs a) {
+    const int N = a.N;
+    const double c2 = a.kappa * a.kappa;
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        const bool ex = a.excl && a.excl[id];
+        const double kx = a.kx[id], ky = a.ky[id], k2 = a.k2[id];
+        double2 J[3];
+        for (int c = 0; c < 3; ++c) J[c] = ex ? make_double2(0.0, 0.0) : a.Jhat[(size_t)c * N + id];
+        const double2 phi = a.st[0 * (size_t)N + id], psi = a.st[1 * (size_t)N + id];
+        const double2 rho = a.st[2 * (size_t)N + id];
+        // continuity_charge_update (:3288): rho - dt div J, zero mean, Nyquist projection
+        const double2 divJ = cik(1.0, make_double2(kx * J[0].x + ky * J[1].x, kx * J[0].y + ky * J[1].y));
+        double2 rho_end = make_double2(rho.x - a.dt * divJ.x, rho.y - a.dt * divJ.y);
+        if (id == 0 || ex) rho_end = make_double2(0.0, 0.0);
+        const double2 rho_mid = cscale(0.5, cadd(rho, rho_end));
+        // CN step (cn_fft_wave_step_from_spectra :3131)
+        const double theta = 0.25 * c2 * a.dt * a.dt * k2;
+        const double den = 1.0 + theta;
+        auto cn = [&](double2 u, double2 v, double2 S, double sigma, double2& un, double2& vn) {
+            if (ex) {
+                un = vn = make_double2(0.0, 0.0);
+                return;
+            }
+            const double sc = c2 * sigma;
+            un = make_double2(((1.0 - theta) * u.x + a.dt * v.x + 0.5 * sc * a.dt * a.dt * S.x) / den,
+                              ((1.0 - theta) * u.y + a.dt * v.y + 0.5 * sc * a.dt * a.dt * S.y) / den);
+            vn = make_double2(((1.0 - theta) * v.x - c2 * a.dt * k2 * u.x + sc * a.dt * S.x) / den,
+                              ((1.0 - theta) * v.y - c2 * a.dt * k2 * u.y + sc * a.dt * S.y) / den);
+        };
+        double2 phin, psin;
+        cn(phi, psi, rho_mid, a.sigma1, phin, psin);
+        if (id == 0) {  // subtract_mean of phi and psi
+            phin = make_double2(0.0, 0.0);
+            psin = make_double2(0.0, 0.0);
+        }
+        double2 An[3], Un[3];
+        for (int c = 0; c < 3; ++c)
+            cn(a.st[(size_t)(3 + c) * N + id], a.st[(size_t)(6 + c) * N + id], J[c], a.sigma2, An[c], Un[c]);
+        a.out[0 * (size_t)N + id] = phin;
+        a.out[1 * (size_t)N + id] = psin;
+        a.out[2 * (size_t)N + id] = rho_end;
+        for (int c = 0; c < 3; ++c) {
+            a.out[(size_t)(3 + c) * N + id] = An[c];
+            a.out[(size_t)(6 + c) * N + id] = Un[c];
+        }
+        // grad phi_mid = (grad phi^n + grad phi^{n+1}) / 2, and A^{n+1}
+        const double2 gx = cscale(0.5, cadd(cik(kx, phi), cik(kx, phin)));
+        const double2 gy = cscale(0.5, cadd(cik(ky, phi), cik(ky, phin)));
+        a.gspec[0 * (size_t)N + id] = gx;
+        a.gspec[1 * (size_t)N + id] = gy;
+        for (int c = 0; c < 3; ++c) a.gspec[(size_t)(2 + c) * N + id] = An[c];
+    }
+}
+
+// Diagnostics spectra of a state (compute_E :3338, spectral_curl :1780,
+// compute_diagnostics :3521): E (3), B (3), div E, div A, psi, rho.
+__global__ void diag_spectra_kernel(int N, const double* kx, const double* ky, const double2* st,
+                                    double2* out) {
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        const double kxx = kx[id], kyy = ky[id];
+        const double2 phi = st[id], psi = st[N + id], rho = st[2 * (size_t)N + id];
+        const double2 A0 = st[3 * (size_t)N + id], A1 = st[4 * (size_t)N + id], A2 = st[5 * (size_t)N + id];
+        const double2 U0 = st[6 * (size_t)N + id], U1 = st[7 * (size_t)N + id], U2 = st[8 * (size_t)N + id];
+        const double2 gx = cik(kxx, phi), gy = cik(kyy, phi);
+        const double2 E0 = make_double2(-gx.x - U0.x, -gx.y - U0.y);
+        const double2 E1 = make_double2(-gy.x - U1.x, -gy.y - U1.y);
+        const double2 E2 = make_double2(-U2.x, -U2.y);
+        out[0 * (size_t)N + id] = E0;
+        out[1 * (size_t)N + id] = E1;
+        out[2 * (size_t)N + id] = E2;
+        out[3 * (size_t)N + id] = cik(kyy, A2);
+        out[4 * (size_t)N + id] = cik(-kxx, A2);
+        out[5 * (size_t)N + id] = cik(1.0, make_double2(kxx * A1.x - kyy * A0.x, kxx * A1.y - kyy * A0.y));
+        out[6 * (size_t)N + id] = cik(1.0, make_double2(kxx * E0.x + kyy * E1.x, kxx * E0.y + kyy * E1.y));
+        out[7 * (size_t)N + id] = cik(1.0, make_double2(kxx * A0.x + kyy * A1.x, kxx * A0.y + kyy * A1.y));
+        out[8 * (size_t)N + id] = psi;
+        out[9 * (size_t)N + id] = rho;
+    }
+}
+
+// P = m gamma(v) v + q A(x) with A = 0 at start-up (momentum_from_v :645).
+__global__ void momentum_from_v_kernel(long np, const double* vx, const double* vy, const double* vz,
+                                       const double* m, double m0, double kappa, double* Px, double* Py,
+                                       double* Pz) {
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
+        const double v[3] = {vx[p], vy[p], vz[p]};
+        const double beta2 = dot3(v, v) / (kappa * kappa);
+        const double gam = 1.0 / sqrt(fmax(1.0e-300, 1.0 - beta2));
+        const double mg = (m ? m[p] : m0) * gam;
+        Px[p] = mg * v[0];
+        Py[p] = mg * v[1];
+        Pz[p] = mg * v[2];
+    }
+}
+
+// project_nyquist (:2044): per line, subtract the alternating mean.
+__global__ void project_lines_kernel(double* f, int ncomp, int nx, int ny, int axis) {
+    const int n = axis == 0 ? nx : ny;
+    const int lines = axis == 0 ? ny : nx;
+    const int stride = axis == 0 ? ny : 1;
+    const int total = ncomp * lines;
+    for (int L = blockIdx.x * blockDim.x + threadIdx.x; L < total; L += gridDim.x * blockDim.x) {
+        const int c = L / lines, l = L - c * lines;
+        double* base = f + (size_t)c * nx * ny + (axis == 0 ? l : (size_t)l * ny);
+        DD s{0.0, 0.0};
+        for (int j = 0; j < n; ++j) s = dd_add(s, (j & 1) ? -base[(size_t)j * stride] : base[(size_t)j * stride]);
+        const double mean = (s.hi + s.lo) / (double)n;
+        for (int j = 0; j < n; ++j) base[(size_t)j * stride] -= (j & 1) ? -mean : mean;
+    }
+}
+
+__global__ void kspace_mask_kernel(double2* f, int ncomp, int N, const unsigned char* excl, int zero_mean) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncomp * N; i += gridDim.x * blockDim.x) {
+        const int id = i % N;
+        if ((zero_mean && id == 0) || (excl && excl[id])) f[i] = make_double2(0.0, 0.0);
+    }
+}
+
+// ---- outer iteration algebra ------------------------------------------------
+constexpr int kRed = 256;
+
+__global__ void __launch_bounds__(kRed)
+residual_norms_kernel(int N, const double* map, const double* guess, double floor_rel, double atol,
+                      double rtol, double* partials) {
+    DD r2{0, 0}, m2{0, 0}, g2{0, 0};
+    double mrel = 0.0, msc = 0.0;
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        double mv[3], gv[3], rv[3];
+        for (int c = 0; c < 3; ++c) {
+            mv[c] = map[(size_t)c * N + id];
+            gv[c] = guess[(size_t)c * N + id];
+            rv[c] = mv[c] - gv[c];
+            r2 = dd_add_dd(r2, dd_sq(rv[c]));
+            m2 = dd_add_dd(m2, dd_sq(mv[c]));
+            g2 = dd_add_dd(g2, dd_sq(gv[c]));
+        }
+        const double rn = norm3(rv);
+        const double vs = 0.5 * (norm3(mv) + norm3(gv));
+        mrel = fmax(mrel, rn / fmax(floor_rel, vs));
+        msc = fmax(msc, rn / (atol + rtol * vs));
+    }
+    r2 = warp_sum_dd(r2);
+    m2 = warp_sum_dd(m2);
+    g2 = warp_sum_dd(g2);
+    mrel = warp_max(mrel);
+    msc = warp_max(msc);
+    __shared__ double red[kRed / kWarp][8];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[w][0] = r2.hi; red[w][1] = r2.lo; red[w][2] = m2.hi; red[w][3] = m2.lo;
+        red[w][4] = g2.hi; red[w][5] = g2.lo; red[w][6] = mrel; red[w][7] = msc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD a{0, 0}, b{0, 0}, c{0, 0};
+        double x = 0.0, y = 0.0;
+        for (int k = 0; k < kRed / kWarp; ++k) {
+            a = dd_add_dd(a, DD{red[k][0], red[k][1]});
+            b = dd_add_dd(b, DD{red[k][2], red[k][3]});
+            c = dd_add_dd(c, DD{red[k][4], red[k][5]});
+            x = fmax(x, red[k][6]);
+            y = fmax(y, red[k][7]);
+        }
+        double* o = partials + (size_t)blockIdx.x * 8;
+        o[0] = a.hi; o[1] = a.lo; o[2] = b.hi; o[3] = b.lo; o[4] = c.hi; o[5] = c.lo; o[6] = x; o[7] = y;
+    }
+}
+
+__global__ void residual_final_kernel(const double* partials, int grid, NormSums* out) {
+    if (threadIdx.x != 0) return;
+    DD a{0, 0}, b{0, 0}, c{0, 0};
+    double x = 0.0, y = 0.0;
+    for (int k = 0; k < grid; ++k) {
+        const double* o = partials + (size_t)k * 8;
+        a = dd_add_dd(a, DD{o[0], o[1]});
+        b = dd_add_dd(b, DD{o[2], o[3]});
+        c = dd_add_dd(c, DD{o[4], o[5]});
+        x = fmax(x, o[6]);
+        y = fmax(y, o[7]);
+    }
+    out->r2[0] = a.hi; out->r2[1] = a.lo;
+    out->map2[0] = b.hi; out->map2[1] = b.lo;
+    out->guess2[0] = c.hi; out->guess2[1] = c.lo;
+    out->max_rel = x;
+    out->max_scaled = y;
+}
+
+struct RPtrs {
+    const double* r[8];
+};
+
+constexpr int kMaxDots = 14;
+
+__global__ void __launch_bounds__(kRed)
+anderson_dots_kernel(int n, RPtrs rp, int m, double* partials) {
+    DD s[kMaxDots];
+    for (int k = 0; k < kMaxDots; ++k) s[k] = DD{0, 0};
+    const int ndots = m * (m + 1) / 2 + m;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double dr[4];
+        for (int j = 0; j < m; ++j) dr[j] = rp.r[j + 1][i] - rp.r[j][i];
+        const double rl = rp.r[m][i];
+        int k = 0;
+        for (int a = 0; a < m; ++a)
+            for (int b = 0; b <= a; ++b) {
+                const double pr = dr[a] * dr[b];
+                s[k] = dd_add_dd(s[k], DD{pr, fma(dr[a], dr[b], -pr)});
+                ++k;
+            }
+        for (int a = 0; a < m; ++a) {
+            const double pr = dr[a] * rl;
+            s[k] = dd_add_dd(s[k], DD{pr, fma(dr[a], rl, -pr)});
+            ++k;
+        }
+    }
+    __shared__ double red[kRed / kWarp][2 * kMaxDots];
+    const int w = threadIdx.x >> 5;
+    for (int k = 0; k < ndots; ++k) {
+        s[k] = warp_sum_dd(s[k]);
+        if ((threadIdx.x & 31) == 0) {
+            red[w][2 * k] = s[k].hi;
+            red[w][2 * k + 1] = s[k].lo;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < ndots) {
+        DD t{0, 0};
+        for (int q = 0; q < kRed / kWarp; ++q) t = dd_add_dd(t, DD{red[q][2 * threadIdx.x], red[q][2 * threadIdx.x + 1]});
+        partials[(size_t)blockIdx.x * 2 * kMaxDots + 2 * threadIdx.x] = t.hi;
+        partials[(size_t)blockIdx.x * 2 * kMaxDots + 2 * threadIdx.x + 1] = t.lo;
+    }
+}
+
+__global__ void dots_final_kernel(const double* partials, int grid, int ndots, double* out) {
+    const int k = threadIdx.x;
+    if (k >= ndots) return;
+    DD t{0, 0};
+    for (int b = 0; b < grid; ++b) t = dd_add_dd(t, DD{partials[(size_t)b * 2 * kMaxDots + 2 * k],
+                                                       partials[(size_t)b * 2 * kMaxDots + 2 * k + 1]});
+    out[k] = t.hi + t.lo;
+}
+
+struct GPtrs {
+    const double* x[8];
+    const double* r[8];
+    double gamma[4];
+};
+
+__global__ void anderson_candidate_kernel(int n, GPtrs g, int m, double beta, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double c = g.x[m][i] + beta * g.r[m][i];
+        for (int j = 0; j < m; ++j) {
+            const double dx = g.x[j + 1][i] - g.x[j][i];
+            const double dr = g.r[j + 1][i] - g.r[j][i];
+            c -= g.gamma[j] * (dx + beta * dr);
+        }
+        out[i] = c;
+    }
+}
+
+__global__ void nonfinite_kernel(int n, const double* v, int* flag) {
+    int bad = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        bad |= !isfinite(v[i]);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+__global__ void lerp_kernel(int n, const double* a, const double* b, double s, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = a[i] + s * (b[i] - a[i]);
+}
+
+__global__ void axpy_kernel(int n, const double* a, const double* b, double s, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = a[i] + s * b[i];
+}
+
+// ---- diagnostics ----------------------------------------------------------------
+constexpr int kDiagSums = 9;
+
+__global__ void __launch_bounds__(kRed) implicit_diag_kernel(ImplicitDiagArgs a) {
+    const int N = a.N;
+    DD s[kDiagSums];
+    for (int k = 0; k < kDiagSums; ++k) s[k] = DD{0, 0};
+    double gmax = 0.0, gamax = 0.0;
+    const double ik2 = 1.0 / (a.kappa * a.kappa);
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        const double gauss = a.divE[id] - a.sigma1 * a.rho[id];
+        const double gauge = a.psi[id] * ik2 + a.divA[id];
+        gmax = fmax(gmax, fabs(gauss));
+        gamax = fmax(gamax, fabs(gauge));
+        s[0] = dd_add_dd(s[0], dd_sq(gauss));
+        s[1] = dd_add_dd(s[1], dd_sq(a.divE[id]));
+        s[2] = dd_add_dd(s[2], dd_sq(a.rho[id]));
+        s[3] = dd_add_dd(s[3], dd_sq(gauge));
+        s[4] = dd_add_dd(s[4], dd_sq(a.psi[id]));
+        s[5] = dd_add_dd(s[5], dd_sq(a.divA[id]));
+        for (int c = 0; c < 3; ++c) {
+            s[6] = dd_add_dd(s[6], dd_sq(a.E[(size_t)c * N + id]));
+            s[7] = dd_add_dd(s[7], dd_sq(a.B[(size_t)c * N + id]));
+        }
+        s[8] = dd_add(s[8], a.rho[id]);
+    }
+    __shared__ double red[kRed / kWarp][2 * kDiagSums + 2];
+    const int w = threadIdx.x >> 5;
+    for (int k = 0; k < kDiagSums; ++k) {
+        s[k] = warp_sum_dd(s[k]);
+        if ((threadIdx.x & 31) == 0) {
+            red[w][2 * k] = s[k].hi;
+            red[w][2 * k + 1] = s[k].lo;
+        }
+    }
+    gmax = warp_max(gmax);
+    gamax = warp_max(gamax);
+    if ((threadIdx.x & 31) == 0) {
+        red[w][2 * kDiagSums] = gmax;
+        red[w][2 * kDiagSums + 1] = gamax;
+    }
+    __syncthreads();
+    if (threadIdx.x < kDiagSums + 2) {
+        const int k = threadIdx.x;
+        double* o = a.partials + (size_t)blockIdx.x * 32;
+        if (k < kDiagSums) {
+            DD t{0, 0};
+            for (int q = 0; q < kRed / kWarp; ++q) t = dd_add_dd(t, DD{red[q][2 * k], red[q][2 * k + 1]});
+            o[2 * k] = t.hi;
+            o[2 * k + 1] = t.lo;
+        } else {
+            double mx = 0.0;
+            for (int q = 0; q < kRed / kWarp; ++q) mx = fmax(mx, red[q][2 * kDiagSums + (k - kDiagSums)]);
+            o[2 * kDiagSums + (k - kDiagSums)] = mx;
+        }
+    }
+}
+
+__global__ void implicit_diag_final_kernel(const double* partials, int grid, double* out) {
+    const int k = threadIdx.x;
+    if (k < kDiagSums) {
+        DD t{0, 0};
+        for (int b = 0; b < grid; ++b) t = dd_add_dd(t, DD{partials[(size_t)b * 32 + 2 * k], partials[(size_t)b * 32 + 2 * k + 1]});
+        out[2 * k] = t.hi;
+        out[2 * k + 1] = t.lo;
+    } else if (k < kDiagSums + 2) {
+        double mx = 0.0;
+        for (int b = 0; b < grid; ++b) mx = fmax(mx, partials[(size_t)b * 32 + 2 * kDiagSums + (k - kDiagSums)]);
+        out[2 * kDiagSums + (k - kDiagSums)] = mx;
+    }
+}
+
+__global__ void __launch_bounds__(kRed)
+kinetic_kernel(long np, const double* vx, const double* vy, const double* vz, const double* m, double m0,
+               double kappa, double* partials) {
+    DD s{0, 0};
+    const double k2 = kappa * kappa;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
+        const double v[3] = {vx[p], vy[p], vz[p]};
+        const double beta2 = dot3(v, v) / k2;
+        const double gam = 1.0 / sqrt(fmax(1.0e-300, 1.0 - beta2));
+        const double mm = m ? m[p] : m0;
+        s = dd_add(s, mm * kappa * kappa * (gam - 1.0));
+    }
+    s = warp_sum_dd(s);
+    __shared__ double red[kRed / kWarp][2];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[w][0] = s.hi;
+        red[w][1] = s.lo;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD t{0, 0};
+        for (int q = 0; q < kRed / kWarp; ++q) t = dd_add_dd(t, DD{red[q][0], red[q][1]});
+        partials[2 * blockIdx.x] = t.hi;
+        partials[2 * blockIdx.x + 1] = t.lo;
+    }
+}
+
+__global__ void pair_final_kernel(const double* partials, int grid, double* out) {
+    if (threadIdx.x != 0) return;
+    DD t{0, 0};
+    for (int b = 0; b < grid; ++b) t = dd_add_dd(t, DD{partials[2 * b], partials[2 * b + 1]});
+    out[0] = t.hi;
+    out[1] = t.lo;
+}
+
+int gsize(long n, int threads = 256) {
+    long g = (n + threads - 1) / threads;
+    if (g > 148 * 8) g = 148 * 8;
+    return g < 1 ? 1 : (int)g;
+}
+
+template <int ORDER, bool U>
+cudaError_t map_one(const TileGeom& tg, const ImplicitMapArgs& a, int grid, cudaStream_t st) {
+    implicit_map_kernel<ORDER, U><<<grid, kMapThreads, implicit_map_smem_bytes(tg, ORDER), st>>>(a, tg);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+template <int ORDER, bool U>
+cudaError_t map_attr(int bytes) {
+    return cudaFuncSetAttribute(implicit_map_kernel<ORDER, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                bytes);
+}
+
+}  // namespace
+
+cudaError_t implicit_set_quadrature(const double* s, const double* w, int nq) {
+    if (nq < 1 || nq > kMaxQuad) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemcpyToSymbol(c_qs, s, sizeof(double) * nq);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_qw, w, sizeof(double) * nq);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(c_nq, &nq, sizeof(int));
+}
+
+int implicit_map_smem_bytes(const TileGeom& tg, int order) {
+    const int S = order + 1;
+    const int RW = S * S + 3;
+    return 2 * 3 * tg.wx * tg.wy * 8 + kMapWarps * (32 * RW * 8 + 32 * 4);
+}
+
+cudaError_t implicit_configure_smem(const TileGeom& tg, int order) {
+    const int b = implicit_map_smem_bytes(tg, order);
+    cudaError_t e;
+    switch (order) {
+        case 1: if ((e = map_attr<1, true>(b)) != cudaSuccess) return e; return map_attr<1, false>(b);
+        case 2: if ((e = map_attr<2, true>(b)) != cudaSuccess) return e; return map_attr<2, false>(b);
+        case 3: if ((e = map_attr<3, true>(b)) != cudaSuccess) return e; return map_attr<3, false>(b);
+        case 4: if ((e = map_attr<4, true>(b)) != cudaSuccess) return e; return map_attr<4, false>(b);
+    }
+    return cudaErrorInvalidValue;
+}
+
+int implicit_map_occupancy(const TileGeom& tg, int order) {
+    int n = 0;
+    const int b = implicit_map_smem_bytes(tg, order);
+    switch (order) {
+        case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, implicit_map_kernel<1, true>, kMapThreads, b); break;
+        case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, implicit_map_kernel<2, true>, kMapThreads, b); break;
+        case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, implicit_map_kernel<3, true>, kMapThreads, b); break;
+        case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, implicit_map_kernel<4, true>, kMapThreads, b); break;
+    }
+    return n;
+}
+
+cudaError_t launch_implicit_map(int order, bool uniform, const TileGeom& tg, const ImplicitMapArgs& a, int grid,
+                                cudaStream_t st) {
+    switch (order) {
+        case 1: return uniform ? map_one<1, true>(tg, a, grid, st) : map_one<1, false>(tg, a, grid, st);
+        case 2: return uniform ? map_one<2, true>(tg, a, grid, st) : map_one<2, false>(tg, a, grid, st);
+        case 3: return uniform ? map_one<3, true>(tg, a, grid, st) : map_one<3, false>(tg, a, grid, st);
+        case 4: return uniform ? map_one<4, true>(tg, a, grid, st) : map_one<4, false>(tg, a, grid, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_point_deposit(int order, const PointDepositArgs& a, cudaStream_t st) {
+    const int g = gsize(a.np);
+    switch (order) {
+        case 1: point_deposit_kernel<1><<<g, 256, 0, st>>>(a); break;
+        case 2: point_deposit_kernel<2><<<g, 256, 0, st>>>(a); break;
+        case 3: point_deposit_kernel<3><<<g, 256, 0, st>>>(a); break;
+        case 4: point_deposit_kernel<4><<<g, 256, 0, st>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather3(int order, int nx, int ny, double Lx, double Ly, const double* f3, long np,
+                           const double* x, const double* y, double* out3, cudaStream_t st) {
+    const int g = gsize(np);
+    switch (order) {
+        case 1: gather3_kernel<1><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, f3, np, x, y, out3); break;
+        case 2: gather3_kernel<2><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, f3, np, x, y, out3); break;
+        case 3: gather3_kernel<3><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, f3, np, x, y, out3); break;
+        case 4: gather3_kernel<4><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, f3, np, x, y, out3); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_history_velocity(int order, int nx, int ny, double Lx, double Ly, const double* E3,
+                                    const double* B3, long np, const double* x, const double* y,
+                                    const double* vx, const double* vy, const double* vz,
+                                    const double* q, double q0, const double* m, double m0, double kappa,
+                                    double dt, double* wx, double* wy, double* wz, cudaStream_t st) {
+    const int g = gsize(np);
+#define UPIC_HV(O)                                                                                        \
+    history_velocity_kernel<O><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, E3, B3, np, x, y, vx, vy, vz, q, q0, m, m0, \
+                                                  kappa, dt, wx, wy, wz)
+    switch (order) {
+        case 1: UPIC_HV(1); break;
+        case 2: UPIC_HV(2); break;
+        case 3: UPIC_HV(3); break;
+        case 4: UPIC_HV(4); break;
+        default: return cudaErrorInvalidValue;
+    }
+#undef UPIC_HV
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cn_kspace(const CnArgs& a, cudaStream_t st) {
+    cn_kspace_kernel<<<gsize(a.N), 256, 0, st>>>(a);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diag_spectra(int N, const double* kx, const double* ky, const double2* st_spec, double2* out,
+                                cudaStream_t st) {
+    diag_spectra_kernel<<<gsize(N), 256, 0, st>>>(N, kx, ky, st_spec, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_momentum_from_v(long np, const double* vx, const double* vy, const double* vz, const double* m,
+                                   double m0, double kappa, double* Px, double* Py, double* Pz, cudaStream_t st) {
+    momentum_from_v_kernel<<<gsize(np), 256, 0, st>>>(np, vx, vy, vz, m, m0, kappa, Px, Py, Pz);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_project_nyquist(double* f, int ncomp, int nx, int ny, cudaStream_t st) {
+    if (nx > 1 && nx % 2 == 0) {
+        project_lines_kernel<<<gsize((long)ncomp * ny, 128), 128, 0, st>>>(f, ncomp, nx, ny, 0);
+        count_launches(1);
+    }
+    if (ny > 1 && ny % 2 == 0) {
+        project_lines_kernel<<<gsize((long)ncomp * nx, 128), 128, 0, st>>>(f, ncomp, nx, ny, 1);
+        count_launches(1);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kspace_mask(double2* f, int ncomp, int N, const unsigned char* excl, int zero_mean,
+                               cudaStream_t st) {
+    kspace_mask_kernel<<<gsize((long)ncomp * N), 256, 0, st>>>(f, ncomp, N, excl, zero_mean);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual_norms(int N, const double* map, const double* guess, double floor_rel, double atol,
+                                  double rtol, double* partials, int grid, NormSums* out, cudaStream_t st) {
+    residual_norms_kernel<<<grid, kRed, 0, st>>>(N, map, guess, floor_rel, atol, rtol, partials);
+    residual_final_kernel<<<1, 32, 0, st>>>(partials, grid, out);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_anderson_dots(int n, const double* const* r, int m, double* partials, int grid, double* out,
+                                 cudaStream_t st) {
+    if (m < 1 || m > 4) return cudaErrorInvalidValue;
+    RPtrs rp{};
+    for (int k = 0; k <= m; ++k) rp.r[k] = r[k];
+    anderson_dots_kernel<<<grid, kRed, 0, st>>>(n, rp, m, partials);
+    dots_final_kernel<<<1, 32, 0, st>>>(partials, grid, m * (m + 1) / 2 + m, out);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_anderson_candidate(int n, const double* const* x, const double* const* r, int m, double beta,
+                                      const double* gamma, double* out, cudaStream_t st) {
+    if (m < 0 || m > 4) return cudaErrorInvalidValue;
+    GPtrs g{};
+    for (int k = 0; k <= m; ++k) {
+        g.x[k] = x[k];
+        g.r[k] = r[k];
+    }
+    for (int k = 0; k < m; ++k) g.gamma[k] = gamma[k];
+    anderson_candidate_kernel<<<gsize(n), 256, 0, st>>>(n, g, m, beta, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nonfinite_flag(int n, const double* v, int* flag, cudaStream_t st) {
+    nonfinite_kernel<<<gsize(n), 256, 0, st>>>(n, v, flag);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lerp(int n, const double* a, const double* b, double s, double* out, cudaStream_t st) {
+    lerp_kernel<<<gsize(n), 256, 0, st>>>(n, a, b, s, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_axpy(int n, const double* a, const double* b, double s, double* out, cudaStream_t st) {
+    axpy_kernel<<<gsize(n), 256, 0, st>>>(n, a, b, s, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_implicit_diag(const ImplicitDiagArgs& a, double* out20, cudaStream_t st) {
+    implicit_diag_kernel<<<a.grid, kRed, 0, st>>>(a);
+    implicit_diag_final_kernel<<<1, 32, 0, st>>>(a.partials, a.grid, out20);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kinetic(long np, const double* vx, const double* vy, const double* vz, const double* m,
+                           double m0, double kappa, double* partials, int grid, double* out, cudaStream_t st) {
+    kinetic_kernel<<<grid, kRed, 0, st>>>(np, vx, vy, vz, m, m0, kappa, partials);
+    pair_final_kernel<<<1, 32, 0, st>>>(partials, grid, out);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
+}  // namespace upic

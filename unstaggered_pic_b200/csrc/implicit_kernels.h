@@ -1,0 +1,180 @@
+// Launch interface of the implicit orbit-averaged GM-HC-CN kernels
+// (implicit.cu), used by api_implicit.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace upic {
+
+// Gather record of the implicit map, per node: grad phi_mid (x, y), A^n (3),
+// A^{n+1} trial (3).
+constexpr int kIRec = 8;
+constexpr int kIRecGpm = 0;
+constexpr int kIRecAn = 2;
+constexpr int kIRecAe = 5;
+constexpr int kMaxQuad = 32;
+// Knot crossings per particle orbit that the device kernel can hold
+// (breakpoints of both axes plus the two ends).
+constexpr int kMaxBreaks = 40;
+
+// Failure reasons of the per-particle local fixed point
+// (LocalParticleFailureReason, Project3/ec_pic_nyquist_projected.cpp:204-211).
+enum LocalFailure {
+    kLocalOk = 0,
+    kLocalNonfiniteMap = 1,
+    kLocalSuperluminalMap = 2,
+    kLocalNonfiniteIterate = 3,
+    kLocalSuperluminalIterate = 4,
+    kLocalMaxIter = 5,
+    kLocalTooManyCrossings = 6
+};
+
+struct MapStats {
+    unsigned long long iter_total;
+    int iter_max;
+    int failures;
+    // smallest (original particle index << 8 | LocalFailure) over failing
+    // particles, ~0 when none failed
+    unsigned long long first_fail_key;
+    unsigned long long worst_scaled_bits;  // max final scaled residual (bit pattern)
+};
+
+struct ImplicitMapArgs {
+    // current state (sorted order)
+    const double *x, *y, *Px, *Py, *Pz, *vx, *vy, *vz;
+    const double *q, *m;
+    double q0, m0;
+    const int* id;
+    // trial end state, written by the final (consistency) evaluation
+    double *ox, *oy, *oPx, *oPy, *oPz, *ovx, *ovy, *ovz, *obx, *oby, *obz;
+    long np;
+    int write_state;
+    // grid (Project3 coordinates: x in [-L/2, L/2), node i at x = -L/2 + i dx)
+    double Lx, Ly, inv_dx, inv_dy, inv_dV;
+    double dt, kappa;
+    const double* rec;  // kIRec doubles per node
+    int split;
+    double loc_rtol, loc_atol, loc_damp;
+    int loc_maxit;
+    // deposit of the orbit-averaged current
+    const Chunk* chunks;
+    const int* nchunks;
+    unsigned long long* acc;  // [comp][hi,lo][N]
+    double scale[3];
+    MapStats* stats;
+};
+
+cudaError_t implicit_set_quadrature(const double* s, const double* w, int nq);
+cudaError_t launch_implicit_map(int order, bool uniform, const TileGeom& tg, const ImplicitMapArgs& a,
+                                int grid, cudaStream_t st);
+int implicit_map_smem_bytes(const TileGeom& tg, int order);
+cudaError_t implicit_configure_smem(const TileGeom& tg, int order);
+int implicit_map_occupancy(const TileGeom& tg, int order);
+
+// Point deposit of rho (q S / dV, slot 3) and J (q v S / dV, slots 0..2) at
+// the particle positions (deposit_scalar_to_mesh :2117, deposit_current_to_mesh
+// :2182), for the start-up state.
+struct PointDepositArgs {
+    const double *x, *y, *vx, *vy, *vz, *q;
+    double q0;
+    long np;
+    int nx, ny;
+    double Lx, Ly, inv_dx, inv_dy, inv_dV;
+    unsigned long long* acc;
+    double scale[4];
+};
+cudaError_t launch_point_deposit(int order, const PointDepositArgs& a, cudaStream_t st);
+
+// Gather of planar 3-vector fields at particle positions (gather_vector_at :2267).
+cudaError_t launch_gather3(int order, int nx, int ny, double Lx, double Ly, const double* f3,
+                           long np, const double* x, const double* y, double* out3,
+                           cudaStream_t st);
+
+// k-space map step: J_field spectra -> rho_end, rho_mid, CN (phi, psi), (A, U)
+// and the spectra of grad phi_mid and A_end (continuity_charge_update :3288,
+// cn_potential_update :3249, cn_fft_wave_step_from_spectra :3131).
+struct CnArgs {
+    int nx, ny, N;
+    const double *kx, *ky, *k2;
+    const unsigned char* excl;  // Nyquist-plane mask (projection on) or null
+    const double2* Jhat;        // 3 x N (J_field)
+    const double2* st;          // state spectra: phi, psi, rho, A(3), U(3) (9 x N)
+    double2* out;               // end spectra: phi, psi, rho, A(3), U(3) (9 x N)
+    double2* gspec;             // grad phi_mid (2), A_end (3): 5 x N
+    double dt, kappa, sigma1, sigma2;
+};
+cudaError_t launch_cn_kspace(const CnArgs& a, cudaStream_t st);
+
+// Spectra of E (3), B (3), div E, div A, psi, rho (10 x N) from the state
+// spectra phi, psi, rho, A(3), U(3).
+cudaError_t launch_diag_spectra(int N, const double* kx, const double* ky, const double2* st_spec, double2* out,
+                                cudaStream_t st);
+// P = m gamma(v) v (start-up canonical momentum with A = 0).
+cudaError_t launch_momentum_from_v(long np, const double* vx, const double* vy, const double* vz, const double* m,
+                                   double m0, double kappa, double* Px, double* Py, double* Pz, cudaStream_t st);
+
+// Project every even-grid Nyquist plane out of real fields (project_nyquist
+// :2044): alternating-mean subtraction along x lines then y lines.
+cudaError_t launch_project_nyquist(double* f, int ncomp, int nx, int ny, cudaStream_t st);
+
+// Zero the k = 0 mode and the excluded Nyquist modes of spectra.
+cudaError_t launch_kspace_mask(double2* f, int ncomp, int N, const unsigned char* excl, int zero_mean,
+                               cudaStream_t st);
+
+// Outer-iteration vector algebra on node currents (3 x N planar).
+struct NormSums {
+    double r2[2], map2[2], guess2[2];  // double-double sums
+    double max_rel, max_scaled;
+};
+cudaError_t launch_residual_norms(int N, const double* map, const double* guess, double floor_rel,
+                                  double atol, double rtol, double* partials, int grid,
+                                  NormSums* out, cudaStream_t st);
+// Gram dots of the Anderson history: dr_i = r[i+1]-r[i] for i < m; sums
+// dr_i.dr_j (i>=j, packed) and dr_i.r[m], in double-double.
+cudaError_t launch_anderson_dots(int N3, const double* const* r, int m, double* partials, int grid,
+                                 double* out, cudaStream_t st);
+// out = x[m] + beta r[m] - sum_j gamma_j (dx_j + beta dr_j)
+cudaError_t launch_anderson_candidate(int N3, const double* const* x, const double* const* r, int m,
+                                      double beta, const double* gamma, double* out, cudaStream_t st);
+// *flag |= 1 when any of v[0..n) is not finite (finite_node_vector :5051);
+// the caller clears *flag.
+cudaError_t launch_nonfinite_flag(int n, const double* v, int* flag, cudaStream_t st);
+// out = a + s (b - a)
+cudaError_t launch_lerp(int n, const double* a, const double* b, double s, double* out, cudaStream_t st);
+// out = a + s b
+cudaError_t launch_axpy(int n, const double* a, const double* b, double s, double* out, cudaStream_t st);
+
+// Diagnostics of the implicit method (compute_diagnostics :3521): real fields
+// planar in `f` (phi, psi, rho, A(3), U(3) real; E(3), B(3), divE, divA
+// appended by the caller), particle kinetic energy.
+struct ImplicitDiagArgs {
+    int N;
+    const double* psi;
+    const double* rho;
+    const double* E;     // 3 x N
+    const double* B;     // 3 x N
+    const double* divE;
+    const double* divA;
+    double sigma1, kappa;
+    double* partials;    // grid x 32
+    int grid;
+};
+// sums: [0..1] gauss^2, [2..3] divE^2, [4..5] rho^2, [6..7] gauge^2, [8..9] psi^2,
+// [10..11] divA^2, [12..13] E^2, [14..15] B^2, [16..17] rho; [18] gauss max, [19] gauge max
+cudaError_t launch_implicit_diag(const ImplicitDiagArgs& a, double* out20, cudaStream_t st);
+// kinetic energy and gamma sum over particles (double-double): out[0..1] kinetic
+cudaError_t launch_kinetic(long np, const double* vx, const double* vy, const double* vz,
+                           const double* m, double m0, double kappa, double* partials, int grid,
+                           double* out, cudaStream_t st);
+
+// Lorentz backward start-up of v_prev (initialize_relativistic_history_velocity :3423)
+cudaError_t launch_history_velocity(int order, int nx, int ny, double Lx, double Ly, const double* E3,
+                                    const double* B3, long np, const double* x, const double* y,
+                                    const double* vx, const double* vy, const double* vz,
+                                    const double* q, double q0, const double* m, double m0,
+                                    double kappa, double dt, double* wx, double* wy, double* wz,
+                                    cudaStream_t st);
+
+}  // namespace upic

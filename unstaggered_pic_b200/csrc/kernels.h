@@ -54,6 +54,10 @@ struct TileGeom {
     int wx, wy;           // window extents in nodes
     int full_x, full_y;   // 1 if the axis window is the whole periodic axis
     int chunk;            // particles per chunk
+    // particle key cell = floor((x + key_origin) / dx + key_shift): the
+    // nearest node for the explicit method (origin 0, shift 1/2), the cell
+    // floor((x + L/2) / dx) for the implicit method (origin L/2, shift 0)
+    double key_origin_x, key_origin_y, key_shift;
 };
 
 struct Chunk {

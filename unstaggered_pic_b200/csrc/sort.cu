@@ -35,8 +35,8 @@ __global__ void make_keys_kernel(TileGeom tg, ParticleSoA p, long np, double Lx,
             x = wrap_periodic(x + shift * p.vx[q], Lx, 1.0 / Lx);
             y = wrap_periodic(y + shift * p.vy[q], Ly, 1.0 / Ly);
         }
-        const int icx = wrap_index(quadratic_weights(x, inv_dx).ic, tg.nx);
-        const int icy = wrap_index(quadratic_weights(y, inv_dy).ic, tg.ny);
+        const int icx = wrap_index((int)floor((x + tg.key_origin_x) * inv_dx + tg.key_shift), tg.nx);
+        const int icy = wrap_index((int)floor((y + tg.key_origin_y) * inv_dy + tg.key_shift), tg.ny);
         const int tx = icx / tg.tile_x, lx = icx - tx * tg.tile_x;
         const int ty = icy / tg.tile_y, ly = icy - ty * tg.tile_y;
         const unsigned tile = (unsigned)(tx * tg.nty + ty);
