@@ -36,6 +36,19 @@ def relerr(a, b):
     return float(np.max(np.abs(a - b)) / scale)
 
 
+# Vector fields are compared against the magnitude of the whole vector: a
+# component that is zero in exact arithmetic (A_z of a run with v_z = 0)
+# holds only rounding noise on both sides.
+FAMILIES = {0: [0], 1: [1], 2: [2], 3: [3, 4, 5], 4: [3, 4, 5], 5: [3, 4, 5], 6: [6, 7, 8], 7: [6, 7, 8],
+            8: [6, 7, 8], 9: [9, 10, 11], 10: [9, 10, 11], 11: [9, 10, 11]}
+
+
+def family_err(fields, ref, k):
+    scale = max(np.max(np.abs(ref[j])) for j in FAMILIES[k])
+    d = np.max(np.abs(np.asarray(fields[k]) - ref[k]))
+    return float(d / scale) if scale > 0 else float(d)
+
+
 def periodic_err(a, b, L):
     d = np.asarray(a) - np.asarray(b)
     d -= L * np.round(d / L)
@@ -94,7 +107,8 @@ def test_implicit_run_matches_reference(case):
         tol = TOL_STEP * nsteps
         fields = np.stack([sim.field(f) for f in FIELD_ORDER])
         for k, f in enumerate(FIELD_ORDER):
-            assert relerr(fields[k], g["fields"][k]) < tol, (f, relerr(fields[k], g["fields"][k]))
+            err = family_err(fields, g["fields"], k)
+            assert err < tol, (f, err)
         p = sim.get_particles()
         assert periodic_err(p["x"], g["out_x"][:, 0], cfg.Lx) < tol * cfg.Lx
         assert periodic_err(p["y"], g["out_x"][:, 1], cfg.Ly) < tol * cfg.Ly
@@ -198,7 +212,8 @@ def test_implicit_larger_case_against_reference_build():
         diag, info = sim.step_implicit(3)
         for s in range(3):
             compare_diag(diag[s], ref["diag"][s + 1], True, TOL_STEP * (s + 1))
+        fields = np.stack([sim.field(f) for f in FIELD_ORDER])
         for k, f in enumerate(FIELD_ORDER):
-            assert relerr(sim.field(f), ref["fields"][k]) < 3 * TOL_STEP, f
+            assert family_err(fields, ref["fields"], k) < 3 * TOL_STEP, f
     finally:
         sim.close()
