@@ -44,7 +44,24 @@ WORKLOADS = {
     # profiling case: same grid and physics, 16 e-/cell (370 MB of particle state)
     "weibel512_ppc16": dict(nx=512, ny=512, ppc=16, L=2 * np.pi / 0.3, dt=0.05, method="bdf1",
                             charge_update="conserving", uth=(0.02, 0.2, 0.0), seed=2026),
+    # the same Weibel decks advanced by the implicit orbit-averaged GM-HC-CN step
+    "weibel512_implicit": dict(nx=512, ny=512, ppc=256, L=2 * np.pi / 0.3, dt=0.05, method="cn_orbit",
+                               charge_update="-", uth=(0.02, 0.2, 0.0), seed=2026),
+    "weibel64_implicit": dict(nx=64, ny=64, ppc=64, L=2 * np.pi / 0.3, dt=0.05, method="cn_orbit",
+                              charge_update="-", uth=(0.02, 0.2, 0.0), seed=2026),
+    "weibel512_ppc16_implicit": dict(nx=512, ny=512, ppc=16, L=2 * np.pi / 0.3, dt=0.05,
+                                     method="cn_orbit", charge_update="-", uth=(0.02, 0.2, 0.0),
+                                     seed=2026),
 }
+# Solver settings of the implicit workloads: the reference's manuscript deck
+# (Project3/inputs/manuscript/weibel_main_dt02_T100.txt) in 2D (nz = 1, Lz = 1).
+IMPLICIT_DECK = dict(Lz=1.0, kappa=1.0, sigma1=1.0, sigma2=1.0, n0=1.0, spline_order=2,
+                     orbit_quad_order=8, split_orbit_at_knots=True, nyquist_projection=True,
+                     nonlinear_solver="anderson_quasi_newton", nonlinear_rtol=1e-11,
+                     nonlinear_atol=1e-13, nonlinear_max_iter=80, anderson_memory=4,
+                     anderson_start=2, anderson_damping=0.5, anderson_regularization=1e-12,
+                     anderson_growth_limit=1.2, uniform_local_rtol=1e-12, uniform_local_atol=1e-14,
+                     uniform_local_max_iter=64, uniform_local_damping=1.0)
 # Algorithmic HBM bytes per particle per step of the fused push kernel: the
 # FP64 particle state x, y, P(3), v(3), v_prev(3) read once and written once.
 ALG_BYTES_PER_PARTICLE = 176
@@ -71,9 +88,12 @@ def config_desc(w, extra=None):
          "grid": [w["nx"], w["ny"]], "particles": w["nx"] * w["ny"] * w["ppc"],
          "particles_per_cell": w["ppc"], "L": w["L"], "dt": w["dt"], "method": w["method"],
          "charge_update": w["charge_update"], "shape": "quadratic B-spline",
-         "precision": "fp64", "l2": "inputs larger than L2 (particle state 5.9 GB)"
+         "precision": "fp64",
+         "l2": f"inputs larger than L2 (particle state {w['ppc'] * w['nx'] * w['ny'] * 88 / 1e9:.1f} GB)"
          if w["ppc"] * w["nx"] * w["ny"] > 10_000_000 else "inputs smaller than L2",
          "parallelism": "replicas"}
+    if w["method"] == "cn_orbit":
+        d["implicit_deck"] = dict(IMPLICIT_DECK)
     if extra:
         d.update(extra)
     return d
@@ -171,16 +191,49 @@ def replica_throughput(world, particles_per_rank, steps, max_ms):
 
 
 # ---------------------------------------------------------------------------
-def reference_sample(ppc, steps, warmup, seed):
-    """Time the reference's own step loop (oracle/_ref/libref_p2.so, or the
-    oracle port when the reference build is absent) on a sample of the
-    workload: same grid, ppc electrons per cell.  Returns (particle-steps/s,
-    kind, particles, seconds)."""
+def reference_sample(w, ppc, steps, warmup, seed):
+    """Time the reference's own step loop on a sample of workload w and
+    return (particle-steps/s, kind, particles, seconds, what).
+
+    Explicit workloads: Project2's run loop (oracle/_ref/libref_p2.so, or the
+    oracle port when the reference build is absent) on the same grid with
+    ppc electrons per cell.  Implicit workloads: Project3's
+    nonlinear_step_orbit loop (oracle/_ref/libref_p3.so) on a 64x64 sub-box
+    with the workload's cell size and physics and ppc electrons per cell (the
+    per-particle cost of the implicit step does not depend on the box)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import ctypes
     import oracle_lib as ol
     import unstaggered_pic_b200 as up
-    w = WORKLOADS["weibel512"]
+    if w["method"] == "cn_orbit":
+        lib = ol.ref_p3()
+        if lib is None:
+            raise RuntimeError("oracle/_ref/libref_p3.so is not built (make -C oracle ref)")
+        nsub = 64
+        Ls = w["L"] * nsub / w["nx"]
+        d = IMPLICIT_DECK
+        p = up.generate_bimaxwellian(nsub, nsub, Ls, Ls, ppc, w["uth"], seed=seed)
+        x = np.zeros((len(p["x"]), 3))
+        x[:, 0] = p["x"] - Ls / 2
+        x[:, 1] = p["y"] - Ls / 2
+        q = p["q"] * d["Lz"]
+        m = np.abs(q)
+
+        def prob(n_steps):
+            return ol.P3Problem(nsub, nsub, Ls, Ls, w["dt"], Lz=d["Lz"], kappa=d["kappa"], order=2,
+                                nq=d["orbit_quad_order"], split=True, nyquist=True,
+                                nl_rtol=d["nonlinear_rtol"], nl_atol=d["nonlinear_atol"],
+                                nl_maxit=d["nonlinear_max_iter"], and_damp=d["anderson_damping"],
+                                loc_rtol=d["uniform_local_rtol"], loc_atol=d["uniform_local_atol"],
+                                loc_maxit=d["uniform_local_max_iter"], n_steps=n_steps)
+        if warmup > 0:
+            ol.p3_run(lib.ref_p3_run, prob(1), x, p["v"], q, m, want_fields=False)
+        out = ol.p3_run(lib.ref_p3_run, prob(steps), x, p["v"], q, m, want_fields=False)
+        n = len(q)
+        secs = out["seconds"]
+        what = (f"serial reference nonlinear_step_orbit loop, {nsub}x{nsub} sub-box with the "
+                f"workload's cell size, {ppc} e-/cell ({n} particles), {steps} steps "
+                f"(mean {out['info'][:, 0].mean():.1f} outer iterations)")
+        return n * steps / secs, "reference", n, secs, what
     lib = ol.ref_p2()
     kind = "reference"
     fn = lib.ref_p2_simulate if lib is not None else None
@@ -196,13 +249,14 @@ def reference_sample(ppc, steps, warmup, seed):
     prob = ol.P2Problem(w["nx"], w["ny"], w["L"], w["L"], w["dt"], 1, True, n_steps=steps)
     _, _, _, secs = ol.simulate(fn, prob, parts, want_fields=False)
     n = len(parts["x"])
-    del ctypes
-    return n * steps / secs, kind, n, secs
+    what = (f"serial reference step loop, {w['nx']}x{w['ny']} grid, {ppc} e-/cell ({n} particles), "
+            f"{steps} steps with diagnostics every step")
+    return n * steps / secs, kind, n, secs, what
 
 
 def _ref_worker(args):
-    ppc, steps, warmup, seed = args
-    return reference_sample(ppc, steps, warmup, seed)
+    name, ppc, steps, warmup, seed = args
+    return reference_sample(WORKLOADS[name], ppc, steps, warmup, seed)
 
 
 def run_reference_arm(args):
@@ -212,21 +266,23 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     import multiprocessing as mp
-    w = WORKLOADS["weibel512"]
+    w = WORKLOADS[args.workload]
     cores = min(os.cpu_count() or 1, 64)
-    ppc = 4  # per-process sample: 512x512 grid, 4 e-/cell (1,048,576 particles)
+    # per-process sample: explicit 512x512 grid with 4 e-/cell (1,048,576
+    # particles); implicit 64x64 sub-box with 2 e-/cell (8,192 particles)
+    ppc = 2 if w["method"] == "cn_orbit" else 4
+    warm = min(args.warmup, 1) if w["method"] == "cn_orbit" else args.warmup
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(cores) as pool:
-        res = pool.map(_ref_worker, [(ppc, args.steps, args.warmup, 1000 + i) for i in range(cores)])
+        res = pool.map(_ref_worker, [(args.workload, ppc, args.steps, warm, 1000 + i) for i in range(cores)])
     wall = time.perf_counter() - t0
     n = res[0][2]
     slowest = max(r[3] for r in res)
     value = cores * n * args.steps / slowest
     kind = res[0][1]
-    sample = (f"{cores} concurrent serial reference processes, each {w['nx']}x{w['ny']} grid with "
-              f"{ppc} e-/cell ({n} particles), {args.warmup} warm-up + {args.steps} timed steps, "
-              f"diagnostics every step; value = total particle-steps / slowest process time")
+    sample = (f"{cores} concurrent processes, each a {res[0][4]}; value = total particle-steps / "
+              f"slowest process time")
     line = {"metric": METRIC, "value": value, "unit": METRIC, "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * slowest / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -241,6 +297,31 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+def make_simulation(up, w):
+    if w["method"] == "cn_orbit":
+        cfg = up.ImplicitConfig(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], **IMPLICIT_DECK)
+    else:
+        cfg = up.Config(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], method=w["method"],
+                        charge_update=w["charge_update"])
+    return up.Simulation(cfg)
+
+
+def advance(sim, w, steps, diag_stride):
+    """K steps of the workload's method; returns the implicit solve reports."""
+    if w["method"] == "cn_orbit":
+        _, info = sim.step_implicit(steps, diagnostics=diag_stride > 0)
+        return info
+    sim.step(steps, diag_stride)
+    return None
+
+
+# Implicit map kernel: per launch it streams x, y, P(3), v(3) of every
+# particle (64 B); the final consistency launch of a step also writes the end
+# state x, y, P(3), v(3), vbar(3) (88 B).
+IMPLICIT_READ_BYTES = 64
+IMPLICIT_WRITE_BYTES = 88
+
+
 def run_upic(args):
     import torch
     import unstaggered_pic_b200 as up
@@ -258,6 +339,7 @@ def run_upic(args):
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
     w = WORKLOADS[args.workload]
+    implicit = w["method"] == "cn_orbit"
     np_total = w["nx"] * w["ny"] * w["ppc"]
 
     def barrier():
@@ -277,9 +359,7 @@ def run_upic(args):
         pinned[k] = t
     del p
     host = {k: t.numpy() for k, t in pinned.items()}
-    cfg = up.Config(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], method=w["method"],
-                    charge_update=w["charge_update"])
-    sim = up.Simulation(cfg)
+    sim = make_simulation(up, w)
     stream = torch.cuda.current_stream()
     sim.set_stream(stream.cuda_stream)
 
@@ -290,7 +370,7 @@ def run_upic(args):
     # ---- device-resident throughput
     load()
     sim.init_fields(False)
-    sim.step(args.warmup, args.diag_stride)
+    advance(sim, w, args.warmup, args.diag_stride)
     torch.cuda.synchronize()
     barrier()
     sim.profile_enable(True)
@@ -307,24 +387,43 @@ def run_upic(args):
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
-    sim.step(args.steps, args.diag_stride)
+    info = advance(sim, w, args.steps, args.diag_stride)
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
     t_ms = allmax(e0.elapsed_time(e1))
-    push_ms, push_n, launches1 = sim.profile_read()
+    kern_ms, kern_n, launches1 = sim.profile_read()
     sim.profile_enable(False)
     gpu_launches = launches1 - launches0
     value = replica_throughput(world, np_total, args.steps, t_ms)
-    push_avg_s = push_ms / max(push_n, 1) / 1e3
     peak, peak_kind = measured_hbm_peak()
-    achieved = ALG_BYTES_PER_PARTICLE * np_total / push_avg_s / 1e9
-    traffic = measured_traffic(np_total)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                "kernel": "push_deposit_kernel (gather + IAEM push + next-step deposit)",
-                "kernel_ms": push_avg_s * 1e3, "kernel_share": push_ms / t_ms,
-                "algorithmic_bytes_per_particle": ALG_BYTES_PER_PARTICLE}
+    if implicit:
+        alg_bytes = np_total * (IMPLICIT_READ_BYTES * kern_n + IMPLICIT_WRITE_BYTES * args.steps)
+        achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                    "kernel": "implicit_map_kernel (per-particle local GM-HC solve + orbit-averaged "
+                              "current deposit)",
+                    "kernel_ms": kern_ms / max(kern_n, 1), "kernel_launches": kern_n,
+                    "kernel_share": kern_ms / t_ms,
+                    "algorithmic_bytes_per_particle_launch": IMPLICIT_READ_BYTES,
+                    "note": "FP64-issue bound (local fixed point with orbit quadrature per particle "
+                            "per launch); HBM fraction stated for the streamed particle state"}
+        solve = {"outer_iterations_per_step": float(np.mean(info[:, 0])),
+                 "map_evaluations_per_step": kern_n / args.steps,
+                 "local_iterations_mean": float(np.mean(info[:, 5])),
+                 "local_iterations_max": float(np.max(info[:, 4])),
+                 "final_rms_residual_max": float(np.max(info[:, 2]))}
+    else:
+        push_avg_s = kern_ms / max(kern_n, 1) / 1e3
+        achieved = ALG_BYTES_PER_PARTICLE * np_total / push_avg_s / 1e9
+        traffic = measured_traffic(np_total)
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                    "kernel": "push_deposit_kernel (gather + IAEM push + next-step deposit)",
+                    "kernel_ms": push_avg_s * 1e3, "kernel_share": kern_ms / t_ms,
+                    "algorithmic_bytes_per_particle": ALG_BYTES_PER_PARTICLE}
+        solve = None
 
     # ---- end to end through the public API from pinned host buffers
     e2e = None
@@ -334,26 +433,27 @@ def run_upic(args):
         t0 = time.perf_counter()
         load()
         sim.init_fields(True)
-        sim.step(args.steps, 1)
+        advance(sim, w, args.steps, 1)
         out = sim.get_particles()
         t_e2e = allmax(time.perf_counter() - t0)
         del out
+        ncol = len(up.IMPLICIT_DIAG_COLUMNS) + len(up.SOLVE_INFO_COLUMNS) if implicit else len(up.DIAG_COLUMNS)
         h2d = np_total * 13 * 8 / args.steps
-        d2h = (13 * 8 * (args.steps + 1) + np_total * 11 * 8) / args.steps
+        d2h = (ncol * 8 * (args.steps + 1) + np_total * 11 * 8) / args.steps
+        api = "upic_step_implicit(K)" if implicit else "upic_step(K, diagnostics every step)"
         e2e = {"value": world * np_total * args.steps / t_e2e, "unit": METRIC,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "seconds": t_e2e,
-               "what": "upic_set_particles + upic_init_fields + upic_step(K, diagnostics every "
-                       "step) + upic_get_particles, host wall clock, max over ranks"}
+               "what": f"upic_set_particles + upic_init_fields + {api} with a diagnostics row per "
+                       "step + upic_get_particles, host wall clock, max over ranks"}
     sim.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            v, kind, n, secs = reference_sample(REF_SAMPLE_PPC, REF_SAMPLE_STEPS, 0, 7)
+            ppc, steps = (4, 2) if implicit else (REF_SAMPLE_PPC, REF_SAMPLE_STEPS)
+            v, kind, n, secs, what = reference_sample(w, ppc, steps, 0, 7)
             cpu = {"value": v, "unit": METRIC, "cores": 1, "kind": kind,
-                   "sample": f"{w['nx']}x{w['ny']} grid, {REF_SAMPLE_PPC} e-/cell ({n} particles), "
-                             f"{REF_SAMPLE_STEPS} steps of the serial reference step loop with "
-                             f"diagnostics every step ({secs:.1f} s)"}
+                   "sample": f"{what} ({secs:.1f} s)"}
         except Exception as exc:  # the baseline is reported, not required
             cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference",
                    "sample": f"failed: {exc}"}
@@ -368,6 +468,8 @@ def run_upic(args):
             "config": config_desc(w, {"diag_stride": args.diag_stride}),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
             "clocks": clk}
+    if solve is not None:
+        line["implicit_solve"] = solve
     print(json.dumps(line))
     return 0
 

@@ -33,7 +33,8 @@ constexpr int kHist = 5;         // Anderson memory + 1 (memory <= 4)
 constexpr int kNormGrid = 296;
 
 struct ImplicitState {
-    int order = 2, nq = 8;
+    int order = 2, nq = 8, mnq = 8;
+    double* qtab = nullptr;  // Gauss rules (ImplicitMapArgs::qtab)
     double dx = 0, dy = 0, dV = 0;
     // particles: two sorted copies (the second is the sort / trial target)
     ParticleSoA P[2];
@@ -267,6 +268,9 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
     a.acc = s.acc;
     for (int d = 0; d < 3; ++d) a.scale[d] = s.scaleJ[d];
     a.stats = s.dstats;
+    a.qtab = s.qtab;
+    a.nq = s.nq;
+    a.mnq = s.mnq;
     if (s.np > 0) {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (c->profiling) {
@@ -274,7 +278,7 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
             UPIC_CUDA(c, cudaEventCreate(&e1));
             UPIC_CUDA(c, cudaEventRecord(e0, c->st));
         }
-        UPIC_CUDA(c, launch_implicit_map(s.order, s.uniform, s.tg, a, s.grid, c->st));
+        UPIC_CUDA(c, launch_implicit_map(s.order, s.uniform, a.split != 0, s.tg, a, s.grid, c->st));
         if (c->profiling) {
             UPIC_CUDA(c, cudaEventRecord(e1, c->st));
             c->prof_events.emplace_back(e0, e1);
@@ -643,15 +647,34 @@ int implicit_create(upic_ctx* c) {
     s->tg.key_origin_y = 0.5 * cf.Ly;
     s->tg.key_shift = 0.0;
     s->tg.chunk = 1024;
-    if (implicit_configure_smem(s->tg, s->order) != cudaSuccess)
+    const bool split = cf.split_orbit_at_knots != 0;
+    if (implicit_configure_smem(s->tg, s->order, split) != cudaSuccess)
         return fail(c, UPIC_ERR_CUDA, "cudaFuncSetAttribute (implicit map) failed");
-    const int occ = implicit_map_occupancy(s->tg, s->order);
+    const int occ = implicit_map_occupancy(s->tg, s->order, split);
     s->grid = c->nsm * (occ > 0 ? occ : 1);
-    std::vector<double> qs, qw;
+    // Gauss rules: the deck's nq points, and for segment moments (order <= 2
+    // with knot splitting) the (order+1)-point rule.  Within a knot-split
+    // segment every orbit integrand -- S_a S_b, (1-s) S'_a S_b, s S'_a S_b --
+    // is a polynomial of degree <= 2 order in s, which an (order+1)-point
+    // Gauss rule integrates exactly, as the deck's rule does when nq >=
+    // order+1; the two then differ by rounding only.
+    std::vector<double> qs, qw, ms, mw;
     gauss_legendre_01(s->nq, qs, qw);
-    if (implicit_set_quadrature(qs.data(), qw.data(), s->nq) != cudaSuccess)
-        return fail(c, UPIC_ERR_CUDA, "quadrature upload failed");
+    s->mnq = (split && s->order <= 2 && s->nq > s->order + 1) ? s->order + 1 : s->nq;
+    gauss_legendre_01(s->mnq, ms, mw);
+    std::vector<double> tab(4 * kMaxQuad, 0.0);
+    for (int i = 0; i < s->nq; ++i) {
+        tab[i] = qs[i];
+        tab[kMaxQuad + i] = qw[i];
+    }
+    for (int i = 0; i < s->mnq; ++i) {
+        tab[2 * kMaxQuad + i] = ms[i];
+        tab[3 * kMaxQuad + i] = mw[i];
+    }
     int rc;
+    if ((rc = dalloc(c, &s->qtab, tab.size()))) return rc;
+    if (cudaMemcpy(s->qtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(c, UPIC_ERR_CUDA, "quadrature upload failed");
     if ((rc = dalloc(c, &s->spec, 9 * (size_t)N)) || (rc = dalloc(c, &s->spec_out, 9 * (size_t)N)) ||
         (rc = dalloc(c, &s->Jhat, 3 * (size_t)N)) || (rc = dalloc(c, &s->gspec, 5 * (size_t)N)) ||
         (rc = dalloc(c, &s->dspec, 10 * (size_t)N)) || (rc = dalloc(c, &s->dreal, 10 * (size_t)N)) ||

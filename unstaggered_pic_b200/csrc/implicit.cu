@@ -22,18 +22,29 @@ namespace upic {
 namespace {
 
 constexpr int kMapThreads = 128;
+// Resident CTAs per SM the map kernel is compiled for (register budget
+// 65536 / (128 * kMapMinBlocks) per thread).
+#ifndef UPIC_MAP_MIN_BLOCKS
+#define UPIC_MAP_MIN_BLOCKS 3
+#endif
+constexpr int kMapMinBlocks = UPIC_MAP_MIN_BLOCKS;
 constexpr int kMapWarps = kMapThreads / kWarp;
 constexpr int kKeyNone = -1;
 constexpr int kKeyEscape = -2;
 
-__constant__ double c_qs[kMaxQuad];
-__constant__ double c_qw[kMaxQuad];
-__constant__ int c_nq;
 
-// wrap1 (:704): x -> [-L/2, L/2)
+// wrap1 (:704): x -> [-L/2, L/2), fmod(x + L/2, L) shifted into [0, L).
+// For t = x + L/2 in [-L, 2L) -- every orbit point, whose excursion is below
+// kappa dt -- fmod(t, L) is t itself or t - L, which is exact (Sterbenz), so
+// the branches below return fmod's value without its remainder loop.
 UPIC_D double wrap1(double x, double L) {
-    double y = fmod(x + 0.5 * L, L);
-    if (y < 0.0) y += L;
+    double y = x + 0.5 * L;
+    if (y >= L) {
+        y = y < 2.0 * L ? y - L : fmod(y, L);
+    } else if (y < 0.0) {
+        if (y < -L) y = fmod(y, L);
+        if (y < 0.0) y += L;
+    }
     return y - 0.5 * L;
 }
 
@@ -49,11 +60,20 @@ struct Stencil {
     double dw[ORDER + 1];
 };
 
+// Weights and dS/dx of the stencil whose first node is il, at f = u - il.
+template <int ORDER>
+UPIC_D void bspline_f(double f, double inv_h, double* w, double* dw);
+
 template <int ORDER>
 UPIC_D void bspline(double u, double inv_h, Stencil<ORDER>& s) {
     const double fl = floor(u - 0.5 * (double)(ORDER - 1));
     s.il = (int)fl;
-    const double f = u - fl;
+    bspline_f<ORDER>(u - fl, inv_h, s.w, s.dw);
+}
+
+template <int ORDER>
+UPIC_D void bspline_f(double f, double inv_h, double* w, double* dw) {
+    Stencil<ORDER> s;
     if (ORDER == 1) {
         s.w[0] = 1.0 - f;
         s.w[1] = f;
@@ -93,11 +113,21 @@ UPIC_D void bspline(double u, double inv_h, Stencil<ORDER>& s) {
         s.dw[3] = -(5.0 / 24.0 - 2.5 * a3 + 2.5 * a3 * a3 - (2.0 / 3.0) * a3 * a3 * a3) * inv_h;
         s.dw[4] = (z4 * z4 * z4 / 6.0) * inv_h;
     }
+#pragma unroll
+    for (int a = 0; a <= ORDER; ++a) {
+        w[a] = s.w[a];
+        dw[a] = s.dw[a];
+    }
 }
 
 struct Geo {
     int nx, ny;
     double Lx, Ly, inv_dx, inv_dy;
+    // orbit quadrature (map kernel only, in shared memory): the deck's
+    // Gauss rule for point-wise orbit sums, and the rule used for segment
+    // moments
+    const double *qs = nullptr, *qw = nullptr, *ms = nullptr, *mw = nullptr;
+    int nq = 0, mnq = 0;
 };
 
 template <int ORDER>
@@ -250,13 +280,13 @@ UPIC_D bool evaluate(const Geo& g, const double* __restrict__ rec, double dt, do
     // orbit averages: grad phi_mid along the path and D_A (:2738, :2958)
     double gp0 = 0.0, gp1 = 0.0;
     double D[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-    const int nq = c_nq;
+    const int nq = g.nq;
     for (int k = 0; k + 1 < nb; ++k) {
         const double sa = b[k], len = b[k + 1] - b[k];
         if (len <= 0.0) continue;
         for (int iq = 0; iq < nq; ++iq) {
-            const double s = sa + len * c_qs[iq];
-            const double wq = len * c_qw[iq];
+            const double s = sa + len * g.qs[iq];
+            const double wq = len * g.qw[iq];
             const double xs = wrap1(in.x0 + s * dxx, g.Lx);
             const double ys = wrap1(in.y0 + s * dxy, g.Ly);
             Stencil<ORDER> sx, sy;
@@ -324,6 +354,137 @@ UPIC_D bool evaluate(const Geo& g, const double* __restrict__ rec, double dt, do
     return true;
 }
 
+// Shape moments of one knot-split orbit segment [sa, sa + len].  Inside a
+// segment every point of the orbit has the same stencil (its first node per
+// axis is ilx, ily, taken at the segment midpoint), so the Gauss sums
+//   sum_q wq S_a S_b,  sum_q wq (1-s_q) S'_a S_b,  sum_q wq s_q S'_a S_b, ...
+// are accumulated once per segment and contracted with each node record
+// once, instead of gathering the node records at every quadrature point.
+// The algebra is that of path_average_gather_vector_one (:2738) and
+// orbit_discrete_gradient_A_interval (:2958) with the node and quadrature
+// sums exchanged.
+template <int ORDER>
+struct SegMoments {
+    static constexpr int SS = (ORDER + 1) * (ORDER + 1);
+    int ilx, ily;
+    double m[SS];               // sum wq Sx_a Sy_b
+    double x0[SS], x1[SS];      // sum wq (1-s) dSx_a Sy_b, sum wq s dSx_a Sy_b
+    double y0[SS], y1[SS];      // sum wq (1-s) Sx_a dSy_b, sum wq s Sx_a dSy_b
+};
+
+// Segment stencil origin and the weighted shape sums of one segment.  With
+// GRAD false only m is formed (the deposit needs no derivatives).
+template <int ORDER, bool GRAD>
+UPIC_D void segment_moments(const Geo& g, double x0, double y0, double dxx, double dxy, double sa,
+                            double len, SegMoments<ORDER>& M) {
+    constexpr int S = ORDER + 1;
+    const double off = 0.5 * (double)(ORDER - 1);
+    const double ox = x0 + 0.5 * g.Lx, oy = y0 + 0.5 * g.Ly;
+    const double sm = sa + 0.5 * len;
+    M.ilx = (int)floor((ox + sm * dxx) * g.inv_dx - off);
+    M.ily = (int)floor((oy + sm * dxy) * g.inv_dy - off);
+    const double fx0 = (double)M.ilx, fy0 = (double)M.ily;
+#pragma unroll
+    for (int k = 0; k < S * S; ++k) {
+        M.m[k] = 0.0;
+        if (GRAD) M.x0[k] = M.x1[k] = M.y0[k] = M.y1[k] = 0.0;
+    }
+    const int nq = g.mnq;
+    for (int iq = 0; iq < nq; ++iq) {
+        const double s = sa + len * g.ms[iq];
+        const double wq = len * g.mw[iq];
+        double wx[S], dwx[S], wy[S], dwy[S];
+        bspline_f<ORDER>((ox + s * dxx) * g.inv_dx - fx0, g.inv_dx, wx, dwx);
+        bspline_f<ORDER>((oy + s * dxy) * g.inv_dy - fy0, g.inv_dy, wy, dwy);
+        const double w1 = wq * s, w0 = wq * (1.0 - s);
+#pragma unroll
+        for (int a = 0; a < S; ++a) {
+            const double ta = wq * wx[a];
+#pragma unroll
+            for (int b = 0; b < S; ++b) M.m[a * S + b] = fma(ta, wy[b], M.m[a * S + b]);
+            if (GRAD) {
+                const double t0 = w0 * dwx[a], t1 = w1 * dwx[a], u0 = w0 * wx[a], u1 = w1 * wx[a];
+#pragma unroll
+                for (int b = 0; b < S; ++b) {
+                    M.x0[a * S + b] = fma(t0, wy[b], M.x0[a * S + b]);
+                    M.x1[a * S + b] = fma(t1, wy[b], M.x1[a * S + b]);
+                    M.y0[a * S + b] = fma(u0, dwy[b], M.y0[a * S + b]);
+                    M.y1[a * S + b] = fma(u1, dwy[b], M.y1[a * S + b]);
+                }
+            }
+        }
+    }
+}
+
+// evaluate() for ORDER <= 2 with knot splitting on, through segment moments.
+template <int ORDER>
+UPIC_D bool evaluate_moments(const Geo& g, const double* __restrict__ rec, double dt, double kappa, int split,
+                             const LocalIn& in, const double* guess, LocalOut& o, double* b, int& nb) {
+    constexpr int S = ORDER + 1;
+    const double dxx = dt * guess[0], dxy = dt * guess[1];
+    o.x1 = wrap1(in.x0 + dxx, g.Lx);
+    o.y1 = wrap1(in.y0 + dxy, g.Ly);
+    double A1p[3];
+    gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, A1p);
+    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
+                           0.5 * (in.A0p[2] + A1p[2])};
+    nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
+    if (nb < 0) return false;
+    double gp0 = 0.0, gp1 = 0.0;
+    double D[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    for (int k = 0; k + 1 < nb; ++k) {
+        const double len = b[k + 1] - b[k];
+        if (len <= 0.0) continue;
+        SegMoments<ORDER> M;
+        segment_moments<ORDER, true>(g, in.x0, in.y0, dxx, dxy, b[k], len, M);
+#pragma unroll
+        for (int a = 0; a < S; ++a) {
+            const int gx = wrap_index(M.ilx + a, g.nx);
+#pragma unroll
+            for (int bb = 0; bb < S; ++bb) {
+                const double* r = rec + (size_t)(gx * g.ny + wrap_index(M.ily + bb, g.ny)) * kIRec;
+                const double2 r01 = __ldg(reinterpret_cast<const double2*>(r));
+                const double2 r23 = __ldg(reinterpret_cast<const double2*>(r + 2));
+                const double2 r45 = __ldg(reinterpret_cast<const double2*>(r + 4));
+                const double2 r67 = __ldg(reinterpret_cast<const double2*>(r + 6));
+                const int j = a * S + bb;
+                gp0 = fma(r01.x, M.m[j], gp0);
+                gp1 = fma(r01.y, M.m[j], gp1);
+                const double An[3] = {r23.x, r23.y, r45.x}, Ae[3] = {r45.y, r67.x, r67.y};
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    D[c][0] = fma(An[c], M.x0[j], fma(Ae[c], M.x1[j], D[c][0]));
+                    D[c][1] = fma(An[c], M.y0[j], fma(Ae[c], M.y1[j], D[c][1]));
+                }
+            }
+        }
+    }
+    const double Dv[3] = {D[0][0] * guess[0] + D[0][1] * guess[1], D[1][0] * guess[0] + D[1][1] * guess[1],
+                          D[2][0] * guess[0] + D[2][1] * guess[1]};
+    const double B[3] = {D[2][1], -D[2][0], D[1][0] - D[0][1]};
+    const double q = in.q, m = in.m, hq = 0.5 * q * dt;
+    const double gpb[3] = {gp0, gp1, 0.0};
+    double pm[3], pp[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pm[c] = ((in.P0[c] - q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
+    hc_rotate(pm, B, q, m, kappa, dt, pp);
+    double pend[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        o.P_end[c] = ((pp[c] + q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
+        pend[c] = o.P_end[c] - q * A1p[c];
+    }
+    const double gam = gamma_p(pend, m * kappa);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.v_end[c] = pend[c] * (1.0 / (m * gam));
+    double vm[3], vp[3];
+    secant(pm, in.pstart, m, kappa, vm);
+    secant(pend, pp, m, kappa, vp);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.vbar_map[c] = 0.5 * (vm[c] + vp[c]);
+    return true;
+}
+
 UPIC_D bool finite3(const double* v) { return isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]); }
 
 UPIC_D int window_coord(int s, int origin, int n, int w, int span) {
@@ -331,8 +492,10 @@ UPIC_D int window_coord(int s, int origin, int n, int w, int span) {
     return d <= w - span ? d : -1;
 }
 
-template <int ORDER, bool UNIFORM>
-__global__ void __launch_bounds__(kMapThreads)
+// MOM: segment moments (ORDER <= 2 with knot splitting on); otherwise the
+// orbit integrals are gathered point by point.
+template <int ORDER, bool UNIFORM, bool MOM>
+__global__ void __launch_bounds__(kMapThreads, kMapMinBlocks)
 implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
     constexpr int S = ORDER + 1;
     constexpr int SS = S * S;
@@ -346,8 +509,18 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double* srow = reinterpret_cast<double*>(wlo + 3 * WN) + warp * 32 * RW;
     int* sgk = reinterpret_cast<int*>(reinterpret_cast<double*>(wlo + 3 * WN) + kMapWarps * 32 * RW) + warp * 32;
+    double* squad = reinterpret_cast<double*>(reinterpret_cast<int*>(reinterpret_cast<double*>(wlo + 3 * WN) +
+                                                                       kMapWarps * 32 * RW) + kMapWarps * 32);
+    for (int i = threadIdx.x; i < 4 * kMaxQuad; i += blockDim.x) squad[i] = a.qtab[i];
+    __syncthreads();
 
-    const Geo g{tg.nx, tg.ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    Geo g{tg.nx, tg.ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    g.qs = squad;
+    g.qw = squad + kMaxQuad;
+    g.ms = squad + 2 * kMaxQuad;
+    g.mw = squad + 3 * kMaxQuad;
+    g.nq = a.nq;
+    g.mnq = a.mnq;
     const int nx = tg.nx, ny = tg.ny, N = nx * ny;
     const int nch = *a.nchunks;
     const int c_begin = (int)(((long long)blockIdx.x * nch) / gridDim.x);
@@ -422,7 +595,12 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                 double scaled = INFINITY;
                 LocalOut o;
                 for (int it = 0; it < a.loc_maxit; ++it) {
-                    if (!evaluate<ORDER>(g, a.rec, a.dt, a.kappa, a.split, in, guess, o, bk, nb)) {
+                    bool okev;
+                    if constexpr (MOM)
+                        okev = evaluate_moments<ORDER>(g, a.rec, a.dt, a.kappa, a.split, in, guess, o, bk, nb);
+                    else
+                        okev = evaluate<ORDER>(g, a.rec, a.dt, a.kappa, a.split, in, guess, o, bk, nb);
+                    if (!okev) {
                         reason = kLocalTooManyCrossings;
                         break;
                     }
@@ -481,32 +659,51 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                     }
                 }
             }
-            // Orbit-averaged deposit of the accepted orbit (:2784): item k of a
-            // particle is its k-th (segment, quadrature point); the warp works
-            // through the items in rounds and reduces equal window keys.
+            // Orbit-averaged deposit of the accepted orbit (:2784).  Item k of
+            // a particle is its k-th segment (MOM: the segment's shape sums,
+            // one stencil per segment) or its k-th (segment, quadrature point)
+            // pair; the warp works through the items in rounds and reduces
+            // equal window keys.
             const double dxx = a.dt * vb[0], dxy = a.dt * vb[1];
             const double qa = ok ? in.q * a.inv_dV : 0.0;
             const double val[3] = {qa * vb[0], qa * vb[1], qa * vb[2]};
-            const int nq = c_nq;
+            const int nq = MOM ? 1 : g.nq;
             const int nitems = ok ? (nb - 1) * nq : 0;
             const int rounds = __reduce_max_sync(0xffffffffu, nitems);
             for (int rd = 0; rd < rounds; ++rd) {
                 int key = kKeyNone, gx0 = 0, gy0 = 0;
-                Stencil<ORDER> sx, sy;
-                double wq = 0.0;
+                double wgt[SS];
                 if (rd < nitems) {
                     const int k = rd / nq, iq = rd - k * nq;
                     const double sa = bk[k], len = bk[k + 1] - bk[k];
                     if (len > 0.0) {
-                        const double s = sa + len * c_qs[iq];
-                        wq = len * c_qw[iq];
-                        const double xs = wrap1(in.x0 + s * dxx, g.Lx);
-                        const double ys = wrap1(in.y0 + s * dxy, g.Ly);
-                        stencil_xy<ORDER>(g, xs, ys, sx, sy);
-                        gx0 = wrap_index(sx.il, nx);
-                        gy0 = wrap_index(sy.il, ny);
-                        const int lx = tg.full_x ? gx0 : window_coord(sx.il, ox, nx, tg.wx, S);
-                        const int ly = tg.full_y ? gy0 : window_coord(sy.il, oy, ny, tg.wy, S);
+                        int ilx, ily;
+                        if constexpr (MOM) {
+                            (void)iq;
+                            SegMoments<ORDER> M;
+                            segment_moments<ORDER, false>(g, in.x0, in.y0, dxx, dxy, sa, len, M);
+                            ilx = M.ilx;
+                            ily = M.ily;
+#pragma unroll
+                            for (int j = 0; j < SS; ++j) wgt[j] = M.m[j];
+                        } else {
+                            const double s = sa + len * g.qs[iq];
+                            const double wq = len * g.qw[iq];
+                            const double xs = wrap1(in.x0 + s * dxx, g.Lx);
+                            const double ys = wrap1(in.y0 + s * dxy, g.Ly);
+                            Stencil<ORDER> sx, sy;
+                            stencil_xy<ORDER>(g, xs, ys, sx, sy);
+                            ilx = sx.il;
+                            ily = sy.il;
+#pragma unroll
+                            for (int ia = 0; ia < S; ++ia)
+#pragma unroll
+                                for (int ib = 0; ib < S; ++ib) wgt[ia * S + ib] = wq * sx.w[ia] * sy.w[ib];
+                        }
+                        gx0 = wrap_index(ilx, nx);
+                        gy0 = wrap_index(ily, ny);
+                        const int lx = tg.full_x ? gx0 : window_coord(ilx, ox, nx, tg.wx, S);
+                        const int ly = tg.full_y ? gy0 : window_coord(ily, oy, ny, tg.wy, S);
                         key = (lx < 0 || ly < 0) ? kKeyEscape : lx * tg.wy + ly;
                     }
                 }
@@ -532,9 +729,7 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                 if (row >= 0) {
                     double* mine = srow + row * RW;
 #pragma unroll
-                    for (int ia = 0; ia < S; ++ia)
-#pragma unroll
-                        for (int ib = 0; ib < S; ++ib) mine[ia * S + ib] = wq * sx.w[ia] * sy.w[ib];
+                    for (int j = 0; j < SS; ++j) mine[j] = wgt[j];
                     mine[SS + 0] = val[0];
                     mine[SS + 1] = val[1];
                     mine[SS + 2] = val[2];
@@ -1119,69 +1314,61 @@ int gsize(long n, int threads = 256) {
     return g < 1 ? 1 : (int)g;
 }
 
-template <int ORDER, bool U>
-cudaError_t map_one(const TileGeom& tg, const ImplicitMapArgs& a, int grid, cudaStream_t st) {
-    implicit_map_kernel<ORDER, U><<<grid, kMapThreads, implicit_map_smem_bytes(tg, ORDER), st>>>(a, tg);
-    count_launches(1);
-    return cudaGetLastError();
-}
+using MapKernel = void (*)(ImplicitMapArgs, TileGeom);
 
-template <int ORDER, bool U>
-cudaError_t map_attr(int bytes) {
-    return cudaFuncSetAttribute(implicit_map_kernel<ORDER, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                bytes);
+// The map kernel instance of (order, uniform q/m, knot splitting).
+MapKernel map_kernel(int order, bool uniform, bool split) {
+    const bool mom = split && order <= 2;
+#define UPIC_K(O, U, M) &implicit_map_kernel<O, U, M>
+    switch (order) {
+        case 1:
+            return mom ? (uniform ? UPIC_K(1, true, true) : UPIC_K(1, false, true))
+                       : (uniform ? UPIC_K(1, true, false) : UPIC_K(1, false, false));
+        case 2:
+            return mom ? (uniform ? UPIC_K(2, true, true) : UPIC_K(2, false, true))
+                       : (uniform ? UPIC_K(2, true, false) : UPIC_K(2, false, false));
+        case 3: return uniform ? UPIC_K(3, true, false) : UPIC_K(3, false, false);
+        case 4: return uniform ? UPIC_K(4, true, false) : UPIC_K(4, false, false);
+    }
+#undef UPIC_K
+    return nullptr;
 }
 
 }  // namespace
 
-cudaError_t implicit_set_quadrature(const double* s, const double* w, int nq) {
-    if (nq < 1 || nq > kMaxQuad) return cudaErrorInvalidValue;
-    cudaError_t e = cudaMemcpyToSymbol(c_qs, s, sizeof(double) * nq);
-    if (e != cudaSuccess) return e;
-    e = cudaMemcpyToSymbol(c_qw, w, sizeof(double) * nq);
-    if (e != cudaSuccess) return e;
-    return cudaMemcpyToSymbol(c_nq, &nq, sizeof(int));
-}
-
 int implicit_map_smem_bytes(const TileGeom& tg, int order) {
     const int S = order + 1;
     const int RW = S * S + 3;
-    return 2 * 3 * tg.wx * tg.wy * 8 + kMapWarps * (32 * RW * 8 + 32 * 4);
+    return 2 * 3 * tg.wx * tg.wy * 8 + kMapWarps * (32 * RW * 8 + 32 * 4) + 4 * kMaxQuad * 8;
 }
 
-cudaError_t implicit_configure_smem(const TileGeom& tg, int order) {
+cudaError_t implicit_configure_smem(const TileGeom& tg, int order, bool split) {
     const int b = implicit_map_smem_bytes(tg, order);
-    cudaError_t e;
-    switch (order) {
-        case 1: if ((e = map_attr<1, true>(b)) != cudaSuccess) return e; return map_attr<1, false>(b);
-        case 2: if ((e = map_attr<2, true>(b)) != cudaSuccess) return e; return map_attr<2, false>(b);
-        case 3: if ((e = map_attr<3, true>(b)) != cudaSuccess) return e; return map_attr<3, false>(b);
-        case 4: if ((e = map_attr<4, true>(b)) != cudaSuccess) return e; return map_attr<4, false>(b);
+    for (int u = 0; u < 2; ++u) {
+        MapKernel k = map_kernel(order, u != 0, split);
+        if (!k) return cudaErrorInvalidValue;
+        const cudaError_t e =
+            cudaFuncSetAttribute(reinterpret_cast<const void*>(k), cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        if (e != cudaSuccess) return e;
     }
-    return cudaErrorInvalidValue;
+    return cudaSuccess;
 }
 
-int implicit_map_occupancy(const TileGeom& tg, int order) {
+int implicit_map_occupancy(const TileGeom& tg, int order, bool split) {
     int n = 0;
-    const int b = implicit_map_smem_bytes(tg, order);
-    switch (order) {
-        case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, implicit_map_kernel<1, true>, kMapThreads, b); break;
-        case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, implicit_map_kernel<2, true>, kMapThreads, b); break;
-        case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, implicit_map_kernel<3, true>, kMapThreads, b); break;
-        case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, implicit_map_kernel<4, true>, kMapThreads, b); break;
-    }
+    MapKernel k = map_kernel(order, true, split);
+    if (!k) return 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kMapThreads, implicit_map_smem_bytes(tg, order));
     return n;
 }
 
-cudaError_t launch_implicit_map(int order, bool uniform, const TileGeom& tg, const ImplicitMapArgs& a, int grid,
-                                cudaStream_t st) {
-    switch (order) {
-        case 1: return uniform ? map_one<1, true>(tg, a, grid, st) : map_one<1, false>(tg, a, grid, st);
-        case 2: return uniform ? map_one<2, true>(tg, a, grid, st) : map_one<2, false>(tg, a, grid, st);
-        case 3: return uniform ? map_one<3, true>(tg, a, grid, st) : map_one<3, false>(tg, a, grid, st);
-        case 4: return uniform ? map_one<4, true>(tg, a, grid, st) : map_one<4, false>(tg, a, grid, st);
-    }
-    return cudaErrorInvalidValue;
+cudaError_t launch_implicit_map(int order, bool uniform, bool split, const TileGeom& tg,
+                                const ImplicitMapArgs& a, int grid, cudaStream_t st) {
+    MapKernel k = map_kernel(order, uniform, split);
+    if (!k) return cudaErrorInvalidValue;
+    k<<<grid, kMapThreads, implicit_map_smem_bytes(tg, order), st>>>(a, tg);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_point_deposit(int order, const PointDepositArgs& a, cudaStream_t st) {

@@ -64,14 +64,20 @@ struct ImplicitMapArgs {
     unsigned long long* acc;  // [comp][hi,lo][N]
     double scale[3];
     MapStats* stats;
+    // Gauss rules on [0, 1] (device, 4 x kMaxQuad doubles: nodes and
+    // weights of the deck's nq-point rule, then of the mnq-point rule used
+    // for segment moments)
+    const double* qtab;
+    int nq, mnq;
 };
 
-cudaError_t implicit_set_quadrature(const double* s, const double* w, int nq);
-cudaError_t launch_implicit_map(int order, bool uniform, const TileGeom& tg, const ImplicitMapArgs& a,
-                                int grid, cudaStream_t st);
+// split: knot splitting of the orbit (ImplicitMapArgs::split), which selects
+// the kernel instance.
+cudaError_t launch_implicit_map(int order, bool uniform, bool split, const TileGeom& tg,
+                                const ImplicitMapArgs& a, int grid, cudaStream_t st);
 int implicit_map_smem_bytes(const TileGeom& tg, int order);
-cudaError_t implicit_configure_smem(const TileGeom& tg, int order);
-int implicit_map_occupancy(const TileGeom& tg, int order);
+cudaError_t implicit_configure_smem(const TileGeom& tg, int order, bool split);
+int implicit_map_occupancy(const TileGeom& tg, int order, bool split);
 
 // Point deposit of rho (q S / dV, slot 3) and J (q v S / dV, slots 0..2) at
 // the particle positions (deposit_scalar_to_mesh :2117, deposit_current_to_mesh
