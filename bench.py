@@ -1,25 +1,31 @@
 #!/usr/bin/env python
-"""Benchmark of the explicit spectral BDF/IAEM generalized-momentum PIC step.
+"""Benchmark of the unstaggered generalized-momentum PIC step on one plasma.
 
 Workload (the 512x512 Weibel configuration): 2D periodic grid 512x512 over
 [0, 2pi/0.3)^2, 256 electrons per cell (67,108,864 particles) at uniform
 random positions with a bi-Maxwellian in normalized momentum (thermal spread
 0.02c in x, 0.2c in y), fixed uniform ion background n0 = 1, quadratic
-B-spline, BDF1 field solve with the continuity-consistent charge update,
-dt = 0.05, FP64 throughout, diagnostics (energy history, gauge / Gauss /
-continuity residuals) every step as the reference's run loop does by default.
-A step is one pass of the hot path over all particles.
+B-spline, dt = 0.05, FP64 throughout.  A step is one pass of the hot path
+over all particles.
+
+The headline line times the explicit spectral BDF1/IAEM step (continuity-
+consistent charge update, diagnostics -- energy history, gauge / Gauss /
+continuity residuals -- every step as the reference's run loop does).  Its
+"implicit" object times the implicit energy-conserving orbit-averaged
+GM-HC-CN step (Anderson outer iteration on the mesh current to 1e-11, local
+particle fixed points to 1e-12, knot-split orbits, Nyquist projection: the
+reference's manuscript deck in 2D) on the same plasma.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 Prints one JSON line.  value = whole-job particle-steps/s with inputs resident
 in HBM; e2e = the same metric through the public API from pinned host
 buffers (upload, start-up fields, K steps with a diagnostics row read back
-each step, particle state read back); roofline = the fused push/deposit
-kernel against the measured HBM copy bandwidth; cpu_baseline = the reference's
-own CPU code (oracle/_ref, compiled from the reference sources) on a bounded
-sample of the same workload.  N > 1 runs N independent replicas (the method
-runs on one GPU; it has no cross-GPU exchange).
+each step, particle state read back); roofline = the dominant kernel against
+the measured HBM copy bandwidth; cpu_baseline = the reference's own CPU code
+(oracle/_ref, compiled from the reference sources) on a bounded sample of the
+same workload.  N > 1 runs N independent replicas (the method runs on one
+GPU; it has no cross-GPU exchange).
 """
 import argparse
 import json
@@ -80,6 +86,10 @@ def parse():
     ap.add_argument("--diag-stride", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--implicit-workload", default="weibel512_implicit",
+                    help="implicit-method workload reported beside an explicit headline ('none' skips)")
+    ap.add_argument("--implicit-steps", type=int, default=3,
+                    help="timed steps of the implicit companion run (at most --steps)")
     return ap.parse_args()
 
 
@@ -259,39 +269,51 @@ def _ref_worker(args):
     return reference_sample(WORKLOADS[name], ppc, steps, warmup, seed)
 
 
-def run_reference_arm(args):
-    """--impl reference: the reference's CPU step on all host cores (one
-    serial reference process per core, each on its own sample)."""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return 0
+def reference_pool(name, steps, warmup):
+    """The reference's CPU step on all host cores (one serial reference
+    process per core, each on its own sample of workload `name`)."""
     import multiprocessing as mp
-    w = WORKLOADS[args.workload]
+    w = WORKLOADS[name]
     cores = min(os.cpu_count() or 1, 64)
     # per-process sample: explicit 512x512 grid with 4 e-/cell (1,048,576
     # particles); implicit 64x64 sub-box with 2 e-/cell (8,192 particles)
     ppc = 2 if w["method"] == "cn_orbit" else 4
-    warm = min(args.warmup, 1) if w["method"] == "cn_orbit" else args.warmup
+    warm = min(warmup, 1) if w["method"] == "cn_orbit" else warmup
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(cores) as pool:
-        res = pool.map(_ref_worker, [(args.workload, ppc, args.steps, warm, 1000 + i) for i in range(cores)])
+        res = pool.map(_ref_worker, [(name, ppc, steps, warm, 1000 + i) for i in range(cores)])
     wall = time.perf_counter() - t0
     n = res[0][2]
     slowest = max(r[3] for r in res)
-    value = cores * n * args.steps / slowest
-    kind = res[0][1]
+    value = cores * n * steps / slowest
     sample = (f"{cores} concurrent processes, each a {res[0][4]}; value = total particle-steps / "
               f"slowest process time")
-    line = {"metric": METRIC, "value": value, "unit": METRIC, "impl": "reference",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * slowest / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+    return {"value": value, "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * slowest / steps,
             "config": config_desc(w, {"reference_sample": sample}),
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind,
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": res[0][1],
                              "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
+
+
+def run_reference_arm(args):
+    """--impl reference: rank 0 times the reference's own CPU step; other
+    ranks exit without work."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    main = reference_pool(args.workload, args.steps, args.warmup)
+    line = {"metric": METRIC, "value": main["value"], "unit": METRIC, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": main["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
+    for k in ("config", "cpu_baseline", "e2e", "wall_s"):
+        line[k] = main[k]
+    if args.implicit_workload != "none" and WORKLOADS[args.workload]["method"] != "cn_orbit":
+        imp = reference_pool(args.implicit_workload, min(args.steps, args.implicit_steps), args.warmup)
+        imp.update({"metric": METRIC, "unit": METRIC, "impl": "reference", "dtype": "f64"})
+        line["implicit"] = imp
     print(json.dumps(line))
     return 0
 
@@ -322,23 +344,14 @@ IMPLICIT_READ_BYTES = 64
 IMPLICIT_WRITE_BYTES = 88
 
 
-def run_upic(args):
+def measure(args, name, steps, warmup, world, rank, dist, dev):
+    """Device-resident and end-to-end throughput of workload `name` (one
+    replica per rank), the dominant kernel's roofline and the reference CPU
+    sample; returns the bench-line fields."""
     import torch
     import unstaggered_pic_b200 as up
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(0)
-    dev = torch.cuda.current_device()
-    w = WORKLOADS[args.workload]
+    w = WORKLOADS[name]
     implicit = w["method"] == "cn_orbit"
     np_total = w["nx"] * w["ny"] * w["ppc"]
 
@@ -370,7 +383,7 @@ def run_upic(args):
     # ---- device-resident throughput
     load()
     sim.init_fields(False)
-    advance(sim, w, args.warmup, args.diag_stride)
+    advance(sim, w, warmup, args.diag_stride)
     torch.cuda.synchronize()
     barrier()
     sim.profile_enable(True)
@@ -387,7 +400,7 @@ def run_upic(args):
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
-    info = advance(sim, w, args.steps, args.diag_stride)
+    info = advance(sim, w, steps, args.diag_stride)
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -395,10 +408,10 @@ def run_upic(args):
     kern_ms, kern_n, launches1 = sim.profile_read()
     sim.profile_enable(False)
     gpu_launches = launches1 - launches0
-    value = replica_throughput(world, np_total, args.steps, t_ms)
+    value = replica_throughput(world, np_total, steps, t_ms)
     peak, peak_kind = measured_hbm_peak()
     if implicit:
-        alg_bytes = np_total * (IMPLICIT_READ_BYTES * kern_n + IMPLICIT_WRITE_BYTES * args.steps)
+        alg_bytes = np_total * (IMPLICIT_READ_BYTES * kern_n + IMPLICIT_WRITE_BYTES * steps)
         achieved = alg_bytes / (kern_ms / 1e3) / 1e9
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
@@ -410,7 +423,7 @@ def run_upic(args):
                     "note": "FP64-issue bound (local fixed point with orbit quadrature per particle "
                             "per launch); HBM fraction stated for the streamed particle state"}
         solve = {"outer_iterations_per_step": float(np.mean(info[:, 0])),
-                 "map_evaluations_per_step": kern_n / args.steps,
+                 "map_evaluations_per_step": kern_n / steps,
                  "local_iterations_mean": float(np.mean(info[:, 5])),
                  "local_iterations_max": float(np.max(info[:, 4])),
                  "final_rms_residual_max": float(np.max(info[:, 2]))}
@@ -433,15 +446,15 @@ def run_upic(args):
         t0 = time.perf_counter()
         load()
         sim.init_fields(True)
-        advance(sim, w, args.steps, 1)
+        advance(sim, w, steps, 1)
         out = sim.get_particles()
         t_e2e = allmax(time.perf_counter() - t0)
         del out
         ncol = len(up.IMPLICIT_DIAG_COLUMNS) + len(up.SOLVE_INFO_COLUMNS) if implicit else len(up.DIAG_COLUMNS)
-        h2d = np_total * 13 * 8 / args.steps
-        d2h = (ncol * 8 * (args.steps + 1) + np_total * 11 * 8) / args.steps
+        h2d = np_total * 13 * 8 / steps
+        d2h = (ncol * 8 * (steps + 1) + np_total * 11 * 8) / steps
         api = "upic_step_implicit(K)" if implicit else "upic_step(K, diagnostics every step)"
-        e2e = {"value": world * np_total * args.steps / t_e2e, "unit": METRIC,
+        e2e = {"value": world * np_total * steps / t_e2e, "unit": METRIC,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "seconds": t_e2e,
                "what": f"upic_set_particles + upic_init_fields + {api} with a diagnostics row per "
                        "step + upic_get_particles, host wall clock, max over ranks"}
@@ -450,26 +463,58 @@ def run_upic(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            ppc, steps = (4, 2) if implicit else (REF_SAMPLE_PPC, REF_SAMPLE_STEPS)
-            v, kind, n, secs, what = reference_sample(w, ppc, steps, 0, 7)
+            ref_ppc, ref_steps = (4, 2) if implicit else (REF_SAMPLE_PPC, REF_SAMPLE_STEPS)
+            v, kind, n, secs, what = reference_sample(w, ref_ppc, ref_steps, 0, 7)
             cpu = {"value": v, "unit": METRIC, "cores": 1, "kind": kind,
                    "sample": f"{what} ({secs:.1f} s)"}
         except Exception as exc:  # the baseline is reported, not required
             cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference",
                    "sample": f"failed: {exc}"}
 
+    out = {"value": value, "steps": steps, "warmup": warmup, "ms_per_step": t_ms / steps,
+           "config": config_desc(w, {"diag_stride": args.diag_stride}), "roofline": roofline,
+           "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk}
+    if solve is not None:
+        out["implicit_solve"] = solve
+    return out
+
+
+def run_upic(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    main = measure(args, args.workload, args.steps, args.warmup, world, rank, dist, dev)
+    companion = None
+    if args.implicit_workload != "none" and WORKLOADS[args.workload]["method"] != "cn_orbit":
+        torch.cuda.empty_cache()
+        companion = measure(args, args.implicit_workload, min(args.steps, args.implicit_steps),
+                            args.warmup, world, rank, dist, dev)
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_desc(w, {"diag_stride": args.diag_stride}),
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
-            "clocks": clk}
-    if solve is not None:
-        line["implicit_solve"] = solve
+    line = {"metric": METRIC, "value": main["value"], "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": main["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic"}
+    for k in ("config", "roofline", "cpu_baseline", "e2e", "gpu_launches", "clocks", "implicit_solve"):
+        if k in main:
+            line[k] = main[k]
+    if companion is not None:
+        companion.update({"metric": METRIC, "unit": METRIC, "n_gpus": world, "dtype": "f64",
+                          "method": "implicit orbit-averaged GM-HC-CN step on the same plasma"})
+        line["implicit"] = companion
     print(json.dumps(line))
     return 0
 
