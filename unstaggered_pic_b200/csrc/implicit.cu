@@ -1018,19 +1018,29 @@ __global__ void momentum_from_v_kernel(long np, const double* vx, const double* 
     }
 }
 
-// project_nyquist (:2044): per line, subtract the alternating mean.
+// project_nyquist (:2044): per line, subtract the alternating mean.  One
+// warp per line: lane l sums entries l, l+32, ... in double-double, then a
+// fixed xor tree combines the lanes (the same order on every run).
+// Axis 1 (lines along y) reads rows contiguously; axis 0 (lines along x)
+// makes 32 lines of consecutive j share each warp's columns via the grid.
 __global__ void project_lines_kernel(double* f, int ncomp, int nx, int ny, int axis) {
     const int n = axis == 0 ? nx : ny;
     const int lines = axis == 0 ? ny : nx;
     const int stride = axis == 0 ? ny : 1;
-    const int total = ncomp * lines;
-    for (int L = blockIdx.x * blockDim.x + threadIdx.x; L < total; L += gridDim.x * blockDim.x) {
-        const int c = L / lines, l = L - c * lines;
+    const long total = (long)ncomp * lines;
+    const int lane = threadIdx.x & 31;
+    const long warps = (long)gridDim.x * (blockDim.x >> 5);
+    for (long L = blockIdx.x * (long)(blockDim.x >> 5) + (threadIdx.x >> 5); L < total; L += warps) {
+        const int c = (int)(L / lines), l = (int)(L - (long)c * lines);
         double* base = f + (size_t)c * nx * ny + (axis == 0 ? l : (size_t)l * ny);
         DD s{0.0, 0.0};
-        for (int j = 0; j < n; ++j) s = dd_add(s, (j & 1) ? -base[(size_t)j * stride] : base[(size_t)j * stride]);
+        for (int j = lane; j < n; j += 32) {
+            const double v = base[(size_t)j * stride];
+            s = dd_add(s, (j & 1) ? -v : v);
+        }
+        s = warp_sum_dd(s);
         const double mean = (s.hi + s.lo) / (double)n;
-        for (int j = 0; j < n; ++j) base[(size_t)j * stride] -= (j & 1) ? -mean : mean;
+        for (int j = lane; j < n; j += 32) base[(size_t)j * stride] -= (j & 1) ? -mean : mean;
     }
 }
 
@@ -1091,11 +1101,12 @@ residual_norms_kernel(int N, const double* map, const double* guess, double floo
     }
 }
 
+// One warp: lane l combines the partials l, l+32, ...; a fixed xor tree
+// combines the lanes.
 __global__ void residual_final_kernel(const double* partials, int grid, NormSums* out) {
-    if (threadIdx.x != 0) return;
     DD a{0, 0}, b{0, 0}, c{0, 0};
     double x = 0.0, y = 0.0;
-    for (int k = 0; k < grid; ++k) {
+    for (int k = threadIdx.x; k < grid; k += 32) {
         const double* o = partials + (size_t)k * 8;
         a = dd_add_dd(a, DD{o[0], o[1]});
         b = dd_add_dd(b, DD{o[2], o[3]});
@@ -1103,6 +1114,12 @@ __global__ void residual_final_kernel(const double* partials, int grid, NormSums
         x = fmax(x, o[6]);
         y = fmax(y, o[7]);
     }
+    a = warp_sum_dd(a);
+    b = warp_sum_dd(b);
+    c = warp_sum_dd(c);
+    x = warp_max(x);
+    y = warp_max(y);
+    if (threadIdx.x != 0) return;
     out->r2[0] = a.hi; out->r2[1] = a.lo;
     out->map2[0] = b.hi; out->map2[1] = b.lo;
     out->guess2[0] = c.hi; out->guess2[1] = c.lo;
@@ -1156,13 +1173,15 @@ anderson_dots_kernel(int n, RPtrs rp, int m, double* partials) {
     }
 }
 
+// One warp per dot (blockDim = 32 * ndots), lanes over the partials.
 __global__ void dots_final_kernel(const double* partials, int grid, int ndots, double* out) {
-    const int k = threadIdx.x;
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (k >= ndots) return;
     DD t{0, 0};
-    for (int b = 0; b < grid; ++b) t = dd_add_dd(t, DD{partials[(size_t)b * 2 * kMaxDots + 2 * k],
-                                                       partials[(size_t)b * 2 * kMaxDots + 2 * k + 1]});
-    out[k] = t.hi + t.lo;
+    for (int b = lane; b < grid; b += 32)
+        t = dd_add_dd(t, DD{partials[(size_t)b * 2 * kMaxDots + 2 * k], partials[(size_t)b * 2 * kMaxDots + 2 * k + 1]});
+    t = warp_sum_dd(t);
+    if (lane == 0) out[k] = t.hi + t.lo;
 }
 
 struct GPtrs {
@@ -1258,17 +1277,24 @@ __global__ void __launch_bounds__(kRed) implicit_diag_kernel(ImplicitDiagArgs a)
     }
 }
 
+// One warp per quantity (blockDim = 32 * (kDiagSums + 2)), lanes over the
+// partials.
 __global__ void implicit_diag_final_kernel(const double* partials, int grid, double* out) {
-    const int k = threadIdx.x;
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (k < kDiagSums) {
         DD t{0, 0};
-        for (int b = 0; b < grid; ++b) t = dd_add_dd(t, DD{partials[(size_t)b * 32 + 2 * k], partials[(size_t)b * 32 + 2 * k + 1]});
-        out[2 * k] = t.hi;
-        out[2 * k + 1] = t.lo;
+        for (int b = lane; b < grid; b += 32)
+            t = dd_add_dd(t, DD{partials[(size_t)b * 32 + 2 * k], partials[(size_t)b * 32 + 2 * k + 1]});
+        t = warp_sum_dd(t);
+        if (lane == 0) {
+            out[2 * k] = t.hi;
+            out[2 * k + 1] = t.lo;
+        }
     } else if (k < kDiagSums + 2) {
         double mx = 0.0;
-        for (int b = 0; b < grid; ++b) mx = fmax(mx, partials[(size_t)b * 32 + 2 * kDiagSums + (k - kDiagSums)]);
-        out[2 * kDiagSums + (k - kDiagSums)] = mx;
+        for (int b = lane; b < grid; b += 32) mx = fmax(mx, partials[(size_t)b * 32 + 2 * kDiagSums + (k - kDiagSums)]);
+        mx = warp_max(mx);
+        if (lane == 0) out[2 * kDiagSums + (k - kDiagSums)] = mx;
     }
 }
 
@@ -1301,9 +1327,10 @@ kinetic_kernel(long np, const double* vx, const double* vy, const double* vz, co
 }
 
 __global__ void pair_final_kernel(const double* partials, int grid, double* out) {
-    if (threadIdx.x != 0) return;
     DD t{0, 0};
-    for (int b = 0; b < grid; ++b) t = dd_add_dd(t, DD{partials[2 * b], partials[2 * b + 1]});
+    for (int b = threadIdx.x; b < grid; b += 32) t = dd_add_dd(t, DD{partials[2 * b], partials[2 * b + 1]});
+    t = warp_sum_dd(t);
+    if (threadIdx.x != 0) return;
     out[0] = t.hi;
     out[1] = t.lo;
 }
@@ -1441,11 +1468,11 @@ cudaError_t launch_momentum_from_v(long np, const double* vx, const double* vy, 
 
 cudaError_t launch_project_nyquist(double* f, int ncomp, int nx, int ny, cudaStream_t st) {
     if (nx > 1 && nx % 2 == 0) {
-        project_lines_kernel<<<gsize((long)ncomp * ny, 128), 128, 0, st>>>(f, ncomp, nx, ny, 0);
+        project_lines_kernel<<<gsize((long)ncomp * ny, 8), 256, 0, st>>>(f, ncomp, nx, ny, 0);
         count_launches(1);
     }
     if (ny > 1 && ny % 2 == 0) {
-        project_lines_kernel<<<gsize((long)ncomp * nx, 128), 128, 0, st>>>(f, ncomp, nx, ny, 1);
+        project_lines_kernel<<<gsize((long)ncomp * nx, 8), 256, 0, st>>>(f, ncomp, nx, ny, 1);
         count_launches(1);
     }
     return cudaGetLastError();
@@ -1472,7 +1499,7 @@ cudaError_t launch_anderson_dots(int n, const double* const* r, int m, double* p
     RPtrs rp{};
     for (int k = 0; k <= m; ++k) rp.r[k] = r[k];
     anderson_dots_kernel<<<grid, kRed, 0, st>>>(n, rp, m, partials);
-    dots_final_kernel<<<1, 32, 0, st>>>(partials, grid, m * (m + 1) / 2 + m, out);
+    dots_final_kernel<<<1, 32 * (m * (m + 1) / 2 + m), 0, st>>>(partials, grid, m * (m + 1) / 2 + m, out);
     count_launches(2);
     return cudaGetLastError();
 }
@@ -1511,7 +1538,7 @@ cudaError_t launch_axpy(int n, const double* a, const double* b, double s, doubl
 
 cudaError_t launch_implicit_diag(const ImplicitDiagArgs& a, double* out20, cudaStream_t st) {
     implicit_diag_kernel<<<a.grid, kRed, 0, st>>>(a);
-    implicit_diag_final_kernel<<<1, 32, 0, st>>>(a.partials, a.grid, out20);
+    implicit_diag_final_kernel<<<1, 32 * (kDiagSums + 2), 0, st>>>(a.partials, a.grid, out20);
     count_launches(2);
     return cudaGetLastError();
 }
