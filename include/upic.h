@@ -270,6 +270,23 @@ int upic_poisson(upic_ctx* ctx, const double* rho, double* phi);
  * hist holds u^n, u^{n-1}, ... (2 fields for BDF1, 4 for BDF2). */
 int upic_solve_bdf(upic_ctx* ctx, const double* source, const double* hist, double* out);
 
+/* Kernel-level orbit integrals of the implicit method (context created with
+ * UPIC_METHOD_CN_ORBIT; its grid, spline order, Gauss rule, knot splitting
+ * and Nyquist projection apply).  Orbits are x0 + s*dx, s in [0,1], with x0
+ * = (x[p], y[p]) and dx, vbar as xyz triples (2D: their z components are not
+ * used).
+ * J (3 x nx*ny) = sum_p q vbar <S(x0 + s dx)>_s / dV, Nyquist-projected:
+ * path_average_deposit_current, Project3/ec_pic_nyquist_projected.cpp:2784. */
+int upic_orbit_deposit(upic_ctx* ctx, long np, const double* x, const double* y, const double* dx,
+                       const double* vbar, const double* q, double* J);
+
+/* gathered[3p+c] = <mesh_c S>_s and grad[9p+3c+d] = <((1-s) An_c + s Anp1_c)
+ * dS/dx_d>_s (d = z column 0 in 2D), mesh/An/Anp1 3 x nx*ny planar:
+ * path_average_gather_and_gradient, ec_pic_nyquist_projected.cpp:3016. */
+int upic_orbit_gather(upic_ctx* ctx, long np, const double* x, const double* y, const double* dx,
+                      const double* mesh, const double* An, const double* Anp1, double* gathered,
+                      double* grad);
+
 /* Largest grid (nx*ny nodes) upic_deposit_current_noalloc accepts: its
  * scratch is a fixed 6*UPIC_NOALLOC_MAX_NODES+2 uint64 array (3 MiB). */
 #define UPIC_NOALLOC_MAX_NODES 65536

@@ -130,11 +130,56 @@ P3_CASES = [
 ]
 
 
+# Orbit kernels: (order, knot splitting, Gauss points)
+P3_ORBIT_CASES = [(2, True, 8), (2, False, 8), (1, True, 4), (3, True, 6)]
+
+
+def p3_orbit_main(lib):
+    """Fixtures of the reference's orbit integrals path_average_deposit_current
+    and path_average_gather_and_gradient on a 16x32 grid: 1000 orbits of up
+    to ~3 cells (several knot crossings, the periodic seam), z components 0."""
+    rng = np.random.default_rng(20261204)
+    nx, ny, Lx, Ly = 16, 32, 5.0, 7.0
+    n = 1000
+    x0 = np.zeros((n, 3))
+    x0[:, 0] = rng.uniform(-Lx / 2, Lx / 2, n)
+    x0[:, 1] = rng.uniform(-Ly / 2, Ly / 2, n)
+    p3_edge_positions(x0, Lx, Ly, nx, ny)
+    vbar = rng.uniform(-0.9, 0.9, (n, 3)) / np.sqrt(3)
+    dt = 2.5
+    dx = dt * vbar
+    dx[:, 2] = 0.0
+    q = rng.uniform(-1.5, 0.5, n)
+    N = nx * ny
+    mesh = rng.normal(size=(3, N))
+    An = rng.normal(size=(3, N))
+    Anp1 = An + 0.1 * rng.normal(size=(3, N))
+    out = {"x0": x0, "dx": dx, "vbar": vbar, "q": q, "mesh": mesh, "An": An, "Anp1": Anp1,
+           "cases": np.array([[o, int(sp), nq] for o, sp, nq in P3_ORBIT_CASES]),
+           "grid": np.array([nx, ny]), "box": np.array([Lx, Ly])}
+    for k, (order, split, nq) in enumerate(P3_ORBIT_CASES):
+        prob = ol.P3Problem(nx, ny, Lx, Ly, dt, order=order, nq=nq, split=split, nyquist=True)
+        J = np.zeros(3 * N)
+        lib.ref_p3_orbit_deposit(ol.ptr(prob.dparams()), ol.ptr(prob.iparams()), ctypes.c_long(n),
+                                 ol.ptr(x0), ol.ptr(dx), ol.ptr(vbar), ol.ptr(q), ol.ptr(J))
+        gat = np.zeros(3 * n)
+        grad = np.zeros(9 * n)
+        lib.ref_p3_orbit_gather(ol.ptr(prob.dparams()), ol.ptr(prob.iparams()), ctypes.c_long(n), ol.ptr(x0),
+                                ol.ptr(dx), ol.ptr(np.ascontiguousarray(mesh)), ol.ptr(np.ascontiguousarray(An)),
+                                ol.ptr(np.ascontiguousarray(Anp1)), ol.ptr(gat), ol.ptr(grad))
+        out[f"J_{k}"] = J
+        out[f"gathered_{k}"] = gat.reshape(n, 3)
+        out[f"grad_{k}"] = grad.reshape(n, 3, 3)
+    np.savez_compressed(os.path.join(HERE, "p3_orbit_kernels.npz"), **out)
+    print("p3_orbit_kernels written")
+
+
 def p3_main():
     """Fixtures of the implicit GM-HC-CN step from oracle/_ref/libref_p3.so."""
     lib = ol.ref_p3()
     if lib is None:
         raise SystemExit("oracle/_ref/libref_p3.so missing: run make -C oracle")
+    p3_orbit_main(lib)
     for k, (name, kw, ppc, uth, two) in enumerate(P3_CASES):
         rng = np.random.default_rng(20261203 + k)
         prob = ol.P3Problem(**kw)

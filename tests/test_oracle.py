@@ -122,3 +122,19 @@ def test_implicit_fixtures_regenerate_from_reference_build(case):
     assert np.array_equal(out["diag"], g["diag"])
     assert np.array_equal(out["info"], g["info"])
     assert np.array_equal(out["fields"], g["fields"])
+
+
+def test_orbit_fixtures_regenerate_from_reference_build(tmp_path, monkeypatch):
+    """tests/golden/p3_orbit_kernels.npz is the reference's own orbit
+    integrals: regenerating it from the reference build is bit-exact."""
+    ref = ol.ref_p3()
+    if ref is None:
+        pytest.skip("reference harness not built (no reference sources)")
+    import golden.make_golden as mg
+    monkeypatch.setattr(mg, "HERE", str(tmp_path))
+    mg.p3_orbit_main(ref)
+    a = dict(np.load(os.path.join(GOLD, "p3_orbit_kernels.npz")))
+    b = dict(np.load(os.path.join(str(tmp_path), "p3_orbit_kernels.npz")))
+    assert a.keys() == b.keys()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k

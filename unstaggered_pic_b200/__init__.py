@@ -273,6 +273,24 @@ class Simulation:
         self._check(lib().upic_poisson(self._ctx, _p(_f64(rho).ravel()), _p(out)))
         return out.reshape(self.config.nx, self.config.ny)
 
+    def orbit_deposit(self, x, y, dx, vbar, q):
+        """Orbit-averaged current of orbits (x, y) + s dx (implicit context)."""
+        n = len(x)
+        J = np.empty(3 * self.N)
+        arrs = [_f64(x), _f64(y), _f64(dx, (n, 3)), _f64(vbar, (n, 3)), _f64(q)]
+        self._check(lib().upic_orbit_deposit(self._ctx, n, *[_p(a) for a in arrs], _p(J)))
+        return J.reshape(3, self.config.nx, self.config.ny)
+
+    def orbit_gather(self, x, y, dx, mesh, An, Anp1):
+        """Orbit averages of mesh (3 fields) and of the A gradient (implicit context):
+        returns gathered (n, 3) and grad (n, 3, 3) [component][direction]."""
+        n = len(x)
+        gat = np.empty((n, 3))
+        grad = np.empty((n, 3, 3))
+        arrs = [_f64(x), _f64(y), _f64(dx, (n, 3)), _f64(mesh).ravel(), _f64(An).ravel(), _f64(Anp1).ravel()]
+        self._check(lib().upic_orbit_gather(self._ctx, n, *[_p(a) for a in arrs], _p(gat), _p(grad)))
+        return gat, grad
+
     def solve_bdf(self, source, hist):
         out = np.empty(self.N)
         h = _f64(hist).ravel()

@@ -43,6 +43,8 @@ SYMBOLS = {
     "upic_spectral_derivative": (ctypes.c_int, [ctypes.c_void_p, c_dp, ctypes.c_int, c_dp]),
     "upic_poisson": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp]),
     "upic_solve_bdf": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp, c_dp]),
+    "upic_orbit_deposit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 6),
+    "upic_orbit_gather": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 8),
     "upic_deposit_current_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                     ctypes.c_double, ctypes.c_long, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

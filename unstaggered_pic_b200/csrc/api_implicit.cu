@@ -78,6 +78,12 @@ struct ImplicitState {
     SortWork sw{};
     int grid = 148;
     long steps = 0;
+    // kernel-level orbit entry points: host-array staging (grown on demand)
+    long ocap = 0;
+    double *ox = nullptr, *oy = nullptr, *odx = nullptr, *ovb = nullptr, *oq = nullptr, *ogat = nullptr,
+           *ograd = nullptr;
+    double* ogrid = nullptr;  // mesh, A^n, A^{n+1}: 9 x N
+    int* oerr = nullptr;
     bool loaded = false;  // upic_set_particles has succeeded
     bool ready = false;   // upic_init_fields has succeeded
 };
@@ -874,9 +880,122 @@ int implicit_get_field(upic_ctx* c, int which, double* host) {
     return sync(c);
 }
 
+int orbit_stage(upic_ctx* c, ImplicitState& s, long np) {
+    int rc;
+    if (!s.ogrid) {
+        if ((rc = dalloc(c, &s.ogrid, 9 * (size_t)c->N)) || (rc = dalloc(c, &s.oerr, 1))) return rc;
+    }
+    if (np <= s.ocap) return 0;
+    double** bufs[] = {&s.ox, &s.oy, &s.odx, &s.ovb, &s.oq, &s.ogat, &s.ograd};
+    const long sizes[] = {1, 1, 3, 3, 1, 3, 9};
+    for (int k = 0; k < 7; ++k) {
+        dfree(c, *bufs[k]);
+        *bufs[k] = nullptr;
+        if ((rc = dalloc(c, bufs[k], sizes[k] * (size_t)np))) return rc;
+    }
+    s.ocap = np;
+    return 0;
+}
+
+OrbitArgs orbit_args(upic_ctx* c, ImplicitState& s, long np) {
+    const upic_config& cf = c->cfg;
+    OrbitArgs a{};
+    a.x = s.ox; a.y = s.oy; a.dx = s.odx; a.vbar = s.ovb; a.q = s.oq;
+    a.np = np;
+    a.nx = c->nx; a.ny = c->ny;
+    a.Lx = cf.Lx; a.Ly = cf.Ly; a.inv_dx = 1.0 / s.dx; a.inv_dy = 1.0 / s.dy; a.inv_dV = 1.0 / s.dV;
+    a.split = cf.split_orbit_at_knots;
+    a.nq = s.nq;
+    a.qtab = s.qtab;
+    a.acc = s.acc;
+    a.err = s.oerr;
+    return a;
+}
+
+int orbit_check(upic_ctx* c, ImplicitState& s) {
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hflag, s.oerr, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    const int rc = sync(c);
+    if (rc) return rc;
+    if (*s.hflag)
+        return fail(c, UPIC_ERR_TOO_LARGE, "an orbit crosses more spline knots than the kernel holds (38)");
+    return 0;
+}
+
 }  // namespace upic_host
 
 using namespace upic_host;
+
+extern "C" int upic_orbit_deposit(upic_ctx* c, long np, const double* x, const double* y, const double* dx,
+                                  const double* vbar, const double* q, double* J) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (!c->imp) return fail(c, UPIC_ERR_STATE, "context was not created with UPIC_METHOD_CN_ORBIT");
+    if (!J || np < 0 || (np > 0 && (!x || !y || !dx || !vbar || !q)))
+        return fail(c, UPIC_ERR_ARGUMENT, "null array or negative particle count");
+    ImplicitState& s = *c->imp;
+    const int N = c->N;
+    int rc;
+    if ((rc = orbit_stage(c, s, np))) return rc;
+    double qabs = 0.0, vmax = 0.0;
+    for (long p = 0; p < np; ++p) {
+        qabs += std::fabs(q[p]);
+        for (int d = 0; d < 3; ++d) vmax = std::max(vmax, std::fabs(vbar[3 * p + d]));
+        if (!std::isfinite(q[p]) || !std::isfinite(x[p]) || !std::isfinite(y[p]))
+            return fail(c, UPIC_ERR_NONFINITE, "non-finite particle input");
+    }
+    if (!std::isfinite(vmax)) return fail(c, UPIC_ERR_NONFINITE, "non-finite orbit velocity");
+    OrbitArgs a = orbit_args(c, s, np);
+    const double scale = fixed_scale(qabs * vmax / s.dV);
+    double sc4[4] = {scale, scale, scale, 1.0};
+    for (int k = 0; k < 3; ++k) a.scale[k] = scale;
+    UPIC_CUDA(c, cudaMemsetAsync(s.acc, 0, sizeof(unsigned long long) * 6 * (size_t)N, c->st));
+    UPIC_CUDA(c, cudaMemsetAsync(s.oerr, 0, sizeof(int), c->st));
+    if (np > 0) {
+        UPIC_CUDA(c, cudaMemcpyAsync(s.ox, x, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.oy, y, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.odx, dx, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.ovb, vbar, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.oq, q, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, launch_orbit_deposit(s.order, a, c->st));
+    }
+    double* out = s.dreal;
+    UPIC_CUDA(c, launch_convert_acc(s.acc, N, sc4, out, nullptr, 0.0, 1, c->st));
+    if (c->cfg.nyquist_projection) UPIC_CUDA(c, launch_project_nyquist(out, 3, c->nx, c->ny, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(J, out, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, c->st));
+    return orbit_check(c, s);
+}
+
+extern "C" int upic_orbit_gather(upic_ctx* c, long np, const double* x, const double* y, const double* dx,
+                                 const double* mesh, const double* An, const double* Anp1, double* gathered,
+                                 double* grad) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (!c->imp) return fail(c, UPIC_ERR_STATE, "context was not created with UPIC_METHOD_CN_ORBIT");
+    if (!mesh || !An || !Anp1 || np < 0 || (np > 0 && (!x || !y || !dx || !gathered || !grad)))
+        return fail(c, UPIC_ERR_ARGUMENT, "null array or negative particle count");
+    ImplicitState& s = *c->imp;
+    const int N = c->N;
+    int rc;
+    if ((rc = orbit_stage(c, s, np))) return rc;
+    OrbitArgs a = orbit_args(c, s, np);
+    a.mesh = s.ogrid;
+    a.An = s.ogrid + 3 * (size_t)N;
+    a.Ae = s.ogrid + 6 * (size_t)N;
+    a.gathered = s.ogat;
+    a.grad = s.ograd;
+    UPIC_CUDA(c, cudaMemsetAsync(s.oerr, 0, sizeof(int), c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.ogrid, mesh, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.ogrid + 3 * (size_t)N, An, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.ogrid + 6 * (size_t)N, Anp1, sizeof(double) * 3 * N, cudaMemcpyHostToDevice,
+                                 c->st));
+    if (np > 0) {
+        UPIC_CUDA(c, cudaMemcpyAsync(s.ox, x, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.oy, y, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.odx, dx, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, launch_orbit_gather(s.order, a, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(gathered, s.ogat, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(grad, s.ograd, sizeof(double) * 9 * np, cudaMemcpyDeviceToHost, c->st));
+    }
+    return orbit_check(c, s);
+}
 
 extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double* info) {
     if (!c) return UPIC_ERR_ARGUMENT;

@@ -859,6 +859,105 @@ __global__ void point_deposit_kernel(PointDepositArgs a) {
     }
 }
 
+// ---- kernel-level orbit entry points ---------------------------------------
+// Orbit x0 + s dx, s in [0, 1], split at knots and summed with the deck's
+// Gauss rule point by point, in the reference's order of quadrature points
+// (path_average_deposit_current :2784, path_average_gather_and_gradient
+// :3016).  One thread per particle; the deposit adds fixed-point integers,
+// so its result does not depend on the order of the atomics.
+template <int ORDER>
+__global__ void orbit_deposit_kernel(OrbitArgs a) {
+    constexpr int S = ORDER + 1;
+    Geo g{a.nx, a.ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    const int N = a.nx * a.ny;
+    const double* qs = a.qtab;
+    const double* qw = a.qtab + kMaxQuad;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < a.np; p += (long)gridDim.x * blockDim.x) {
+        const double x0 = a.x[p], y0 = a.y[p];
+        const double dxx = a.dx[3 * p], dxy = a.dx[3 * p + 1];
+        double b[kMaxBreaks];
+        const int nb = breakpoints<ORDER>(g, x0, y0, dxx, dxy, a.split, b);
+        if (nb < 0) {
+            atomicOr(a.err, 1);
+            continue;
+        }
+        const double qa = (a.q ? a.q[p] : a.q0) * a.inv_dV;
+        const double val[3] = {qa * a.vbar[3 * p], qa * a.vbar[3 * p + 1], qa * a.vbar[3 * p + 2]};
+        for (int k = 0; k + 1 < nb; ++k) {
+            const double sa = b[k], len = b[k + 1] - b[k];
+            if (len <= 0.0) continue;
+            for (int iq = 0; iq < a.nq; ++iq) {
+                const double s = sa + len * qs[iq];
+                const double wq = len * qw[iq];
+                Stencil<ORDER> sx, sy;
+                stencil_xy<ORDER>(g, wrap1(x0 + s * dxx, g.Lx), wrap1(y0 + s * dxy, g.Ly), sx, sy);
+                for (int ia = 0; ia < S; ++ia) {
+                    const int gx = wrap_index(sx.il + ia, a.nx);
+                    for (int ib = 0; ib < S; ++ib) {
+                        const int node = gx * a.ny + wrap_index(sy.il + ib, a.ny);
+                        const double w = wq * sx.w[ia] * sy.w[ib];
+                        for (int c = 0; c < 3; ++c) {
+                            const double v = val[c] * w;
+                            if (v == 0.0) continue;
+                            const Fixed2 f = to_fixed(v, a.scale[c]);
+                            atomicAdd(&a.acc[(size_t)(2 * c) * N + node], f.hi);
+                            atomicAdd(&a.acc[(size_t)(2 * c + 1) * N + node], f.lo);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int ORDER>
+__global__ void orbit_gather_kernel(OrbitArgs a) {
+    constexpr int S = ORDER + 1;
+    Geo g{a.nx, a.ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    const int N = a.nx * a.ny;
+    const double* qs = a.qtab;
+    const double* qw = a.qtab + kMaxQuad;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < a.np; p += (long)gridDim.x * blockDim.x) {
+        const double x0 = a.x[p], y0 = a.y[p];
+        const double dxx = a.dx[3 * p], dxy = a.dx[3 * p + 1];
+        double b[kMaxBreaks];
+        const int nb = breakpoints<ORDER>(g, x0, y0, dxx, dxy, a.split, b);
+        double gat[3] = {0.0, 0.0, 0.0};
+        double D[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+        if (nb < 0) atomicOr(a.err, 1);
+        for (int k = 0; k + 1 < nb; ++k) {
+            const double sa = b[k], len = b[k + 1] - b[k];
+            if (len <= 0.0) continue;
+            for (int iq = 0; iq < a.nq; ++iq) {
+                const double s = sa + len * qs[iq];
+                const double wq = len * qw[iq];
+                Stencil<ORDER> sx, sy;
+                stencil_xy<ORDER>(g, wrap1(x0 + s * dxx, g.Lx), wrap1(y0 + s * dxy, g.Ly), sx, sy);
+                for (int ia = 0; ia < S; ++ia) {
+                    const int gx = wrap_index(sx.il + ia, a.nx);
+                    for (int ib = 0; ib < S; ++ib) {
+                        const int node = gx * a.ny + wrap_index(sy.il + ib, a.ny);
+                        const double shape = sx.w[ia] * sy.w[ib];
+                        const double dsx = sx.dw[ia] * sy.w[ib], dsy = sx.w[ia] * sy.dw[ib];
+                        for (int c = 0; c < 3; ++c) {
+                            gat[c] += wq * a.mesh[(size_t)c * N + node] * shape;
+                            const double av = (1.0 - s) * a.An[(size_t)c * N + node] + s * a.Ae[(size_t)c * N + node];
+                            D[c][0] += wq * av * dsx;
+                            D[c][1] += wq * av * dsy;
+                        }
+                    }
+                }
+            }
+        }
+        for (int c = 0; c < 3; ++c) {
+            a.gathered[3 * p + c] = gat[c];
+            a.grad[9 * p + 3 * c] = D[c][0];
+            a.grad[9 * p + 3 * c + 1] = D[c][1];
+            a.grad[9 * p + 3 * c + 2] = 0.0;  // nz = 1: no z derivative
+        }
+    }
+}
+
 template <int ORDER>
 __global__ void gather3_kernel(int nx, int ny, double Lx, double Ly, const double* f3, long np,
                                const double* x, const double* y, double* out3) {
@@ -1394,6 +1493,32 @@ cudaError_t launch_implicit_map(int order, bool uniform, bool split, const TileG
     MapKernel k = map_kernel(order, uniform, split);
     if (!k) return cudaErrorInvalidValue;
     k<<<grid, kMapThreads, implicit_map_smem_bytes(tg, order), st>>>(a, tg);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_orbit_deposit(int order, const OrbitArgs& a, cudaStream_t st) {
+    const int g = gsize(a.np);
+    switch (order) {
+        case 1: orbit_deposit_kernel<1><<<g, 128, 0, st>>>(a); break;
+        case 2: orbit_deposit_kernel<2><<<g, 128, 0, st>>>(a); break;
+        case 3: orbit_deposit_kernel<3><<<g, 128, 0, st>>>(a); break;
+        case 4: orbit_deposit_kernel<4><<<g, 128, 0, st>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_orbit_gather(int order, const OrbitArgs& a, cudaStream_t st) {
+    const int g = gsize(a.np);
+    switch (order) {
+        case 1: orbit_gather_kernel<1><<<g, 128, 0, st>>>(a); break;
+        case 2: orbit_gather_kernel<2><<<g, 128, 0, st>>>(a); break;
+        case 3: orbit_gather_kernel<3><<<g, 128, 0, st>>>(a); break;
+        case 4: orbit_gather_kernel<4><<<g, 128, 0, st>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
     count_launches(1);
     return cudaGetLastError();
 }

@@ -93,6 +93,26 @@ struct PointDepositArgs {
 };
 cudaError_t launch_point_deposit(int order, const PointDepositArgs& a, cudaStream_t st);
 
+// Kernel-level orbit integrals (path_average_deposit_current :2784,
+// path_average_gather_and_gradient :3016) over orbits x0 + s dx, s in [0,1],
+// 2D (the third components of dx are not used; the z column of grad is 0).
+struct OrbitArgs {
+    const double *x, *y, *dx, *vbar, *q;   // dx, vbar: xyz triples; q null = q0
+    double q0;
+    long np;
+    int nx, ny;
+    double Lx, Ly, inv_dx, inv_dy, inv_dV;
+    int split, nq;
+    const double* qtab;                    // Gauss rule (nodes, then weights at +kMaxQuad)
+    unsigned long long* acc;               // deposit: [comp][hi,lo][N]
+    double scale[3];
+    const double *mesh, *An, *Ae;          // gather: 3 x N planar fields
+    double *gathered, *grad;               // gather: 3 and 9 ([comp][dir]) per particle
+    int* err;                              // set to 1 when an orbit crosses too many knots
+};
+cudaError_t launch_orbit_deposit(int order, const OrbitArgs& a, cudaStream_t st);
+cudaError_t launch_orbit_gather(int order, const OrbitArgs& a, cudaStream_t st);
+
 // Gather of planar 3-vector fields at particle positions (gather_vector_at :2267).
 cudaError_t launch_gather3(int order, int nx, int ny, double Lx, double Ly, const double* f3,
                            long np, const double* x, const double* y, double* out3,
