@@ -162,6 +162,18 @@ enum {
     UPIC_INFO_ANDERSON_STEPS, UPIC_INFO_PICARD_STEPS, UPIC_INFO_COUNT
 };
 
+/* Step diagnostics of the implicit method: StepDiagnostics of
+ * compute_step_diagnostics, ec_pic_nyquist_projected.cpp:4501 (:4303-4321),
+ * in the column order of its _step_diagnostics.csv (:8462-8473). */
+enum {
+    UPIC_SD_A_CHAIN_ABS_RMS = 0, UPIC_SD_A_CHAIN_REL_RMS, UPIC_SD_A_CHAIN_MAX_NORM,
+    UPIC_SD_A_CHAIN_MEAN_NORM, UPIC_SD_A_CHAIN_WORK_DEFECT, UPIC_SD_DELTA_K, UPIC_SD_DELTA_W,
+    UPIC_SD_DELTA_TOTAL_ENERGY, UPIC_SD_PARTICLE_WORK, UPIC_SD_GRID_WORK,
+    UPIC_SD_DEPOSIT_GATHER_WORK_RESIDUAL, UPIC_SD_PARTICLE_ENERGY_RESIDUAL,
+    UPIC_SD_FIELD_ENERGY_RESIDUAL, UPIC_SD_CROSSING_PARTICLES, UPIC_SD_TOTAL_CROSSINGS,
+    UPIC_SD_AVERAGE_PATH_SEGMENTS, UPIC_SD_MAX_PATH_SEGMENTS, UPIC_SD_COUNT
+};
+
 /* ABI version of the loaded library (UPIC_ABI_VERSION). */
 int upic_abi_version(void);
 
@@ -204,12 +216,14 @@ int upic_get_particles(upic_ctx* ctx, long np, double* x, double* y, double* P, 
 int upic_init_fields(upic_ctx* ctx, double* diag_row);
 
 /* Advance nsteps implicit steps (nonlinear_step_orbit,
- * ec_pic_nyquist_projected.cpp:6477, then compute_diagnostics :3521).
+ * ec_pic_nyquist_projected.cpp:6477, then compute_diagnostics :3521 and, the
+ * run loop's per-step record, compute_step_diagnostics :4501 at :8835).
  * diag (optional): nsteps x UPIC_P3_DIAG_COUNT; info (optional): nsteps x
- * UPIC_INFO_COUNT.  A step that does not converge returns
+ * UPIC_INFO_COUNT; step_diag (optional, one extra orbit pass per step):
+ * nsteps x UPIC_SD_COUNT.  A step that does not converge returns
  * UPIC_ERR_NONCONVERGED, one whose per-particle solve fails returns
  * UPIC_ERR_LOCAL_PARTICLE; the state then stays at the last accepted step. */
-int upic_step_implicit(upic_ctx* ctx, int nsteps, double* diag, double* info);
+int upic_step_implicit(upic_ctx* ctx, int nsteps, double* diag, double* info, double* step_diag);
 
 /* Advance nsteps steps of the explicit BDF/IAEM method (loop body of
  * run_simulation, spectral_pic_part3.cpp:1133-1189).  diag (optional):

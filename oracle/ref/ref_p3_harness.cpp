@@ -29,6 +29,7 @@ enum {
 };
 constexpr int kDiag = 22;
 constexpr int kInfo = 8;
+constexpr int kStepDiag = 17;
 
 Config make_cfg(const double* d, const int* ip) {
     Config c;
@@ -70,6 +71,17 @@ void store_diag(const Diagnostics& d, double* o) {
                              d.kinetic_energy, d.total_energy, d.rho_mode, d.E_mode_re,
                              d.E_mode_im, d.E_mode_abs, d.Bz_y_mode_re, d.Bz_y_mode_im,
                              d.Bz_y_mode_abs};
+    std::memcpy(o, v, sizeof(v));
+}
+
+void store_step_diag(const StepDiagnostics& d, double* o) {
+    const double v[kStepDiag] = {d.A_chain_abs_rms, d.A_chain_rel_rms, d.A_chain_max_norm,
+                                 d.A_chain_mean_norm, d.A_chain_work_defect, d.delta_K, d.delta_W,
+                                 d.delta_total_energy, d.particle_work, d.grid_work,
+                                 d.deposit_gather_work_residual, d.particle_energy_residual,
+                                 d.field_energy_residual, (double)d.crossing_particles,
+                                 (double)d.total_crossings, d.average_path_segments,
+                                 (double)d.max_path_segments};
     std::memcpy(o, v, sizeof(v));
 }
 
@@ -146,10 +158,13 @@ int ref_p3_orbit_gather(const double* d, const int* ip, long np, const double* x
 //   diag: (n_steps+1) x 22; info: n_steps x 8 {iterations, converged,
 //   final_rms_residual, final_max_particle_residual, local_iter_max,
 //   local_iter_mean, anderson_steps, picard_steps}; fields (optional): phi,
-//   psi, rho, A(3), U(3), J(3) = 12 x N after the last step.
+//   psi, rho, A(3), U(3), J(3) = 12 x N after the last step; step_diag
+//   (optional): n_steps x 17, compute_step_diagnostics (:4501) of each step
+//   as the run loop calls it (:8835), StepDiagnostics members in the column
+//   order of _step_diagnostics.csv (:8462-8473).
 int ref_p3_run(const double* d, const int* ip, long np, double* x, double* v, double* P,
                double* v_prev, double* vbar, const double* q, const double* m, double* diag,
-               double* info, double* fields, double* seconds) {
+               double* info, double* fields, double* seconds, double* step_diag) {
     try {
         Config c = make_cfg(d, ip);
         Grid g = make_grid(c);
@@ -185,7 +200,12 @@ int ref_p3_run(const double* d, const int* ip, long np, double* x, double* v, do
         for (int s = 1; s <= ip[I_NSTEPS]; ++s) {
             std::vector<NonlinearHistoryEntry> hist;
             NonlinearSolveInfo si;
+            const State s0 = step_diag ? st : State{};
             st = nonlinear_step_orbit(st, g, c, quad, hist, &si, (s - 1) * c.dt);
+            if (step_diag)
+                store_step_diag(compute_step_diagnostics(s0, st, g, c.dt, c.spline_order, quad, c.sigma1,
+                                                         c.sigma2, c.kappa, c.split_orbit_at_knots),
+                                step_diag + (std::size_t)kStepDiag * (s - 1));
             if (diag) store_diag(compute_diagnostics(st, g, c.sigma1, c.sigma2, c.kappa, mode),
                                  diag + (std::size_t)kDiag * s);
             if (info) {

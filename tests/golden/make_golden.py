@@ -190,11 +190,12 @@ def p3_main():
             q[1::2] = -q[1::2]
             m[1::2] = 4.0 * m[1::2]
             v[1::2] *= 0.5
-        out = ol.p3_run(lib.ref_p3_run, prob, x, v, q, m)
+        out = ol.p3_run(lib.ref_p3_run, prob, x, v, q, m, want_step_diag=True)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), dparams=prob.dparams(),
                             iparams=prob.iparams(), in_x=x, in_v=v, in_q=q, in_m=m,
                             **{"out_" + k: out[k] for k in ("x", "v", "P", "v_prev", "vbar")},
-                            diag=out["diag"], info=out["info"], fields=out["fields"])
+                            diag=out["diag"], info=out["info"], fields=out["fields"],
+                            step_diag=out["step_diag"])
         print(name, "iterations", out["info"][:, 0].tolist())
 
 

@@ -102,6 +102,7 @@ def init_weibel(lib_fn, nx, ny, Lx, Ly, ppc, c=1.0, n0=1.0, vx=0.5, vy_max=0.01,
 REF_P3_SO = os.path.join(ROOT, "oracle", "_ref", "libref_p3.so")
 P3_NDIAG = 22
 P3_NINFO = 8
+P3_NSTEPDIAG = 17
 P3_DIAG_NAMES = ["gauss_rms", "gauss_max", "divE_rms", "sigma1_rho_rms", "gauss_normalization_rms",
                  "gauss_relative", "gauge_rms", "gauge_max", "psi_over_kappa2_rms", "divA_rms",
                  "gauge_normalization_rms", "gauge_relative", "field_energy", "kinetic_energy",
@@ -134,10 +135,11 @@ class P3Problem:
                          self.mode], dtype=np.int32)
 
 
-def p3_run(fn, prob, x, v, q, m, want_fields=True):
-    """Run fn (ref_p3_run / o3_run) on copies: x, v (np, 3).  Returns dict
-    with x, v, P, v_prev, vbar, diag (n_steps+1, 22), info (n_steps, 8),
-    fields (12, nx, ny) and seconds."""
+def p3_run(fn, prob, x, v, q, m, want_fields=True, want_step_diag=False):
+    """Run fn (ref_p3_run) on copies: x, v (np, 3).  Returns dict with x,
+    v, P, v_prev, vbar, diag (n_steps+1, 22), info (n_steps, 8), fields
+    (12, nx, ny), step_diag (n_steps, 17) and seconds (of the step loop,
+    step diagnostics included when requested)."""
     n = len(q)
     out = {"x": np.ascontiguousarray(x, dtype=np.float64).copy(),
            "v": np.ascontiguousarray(v, dtype=np.float64).copy(),
@@ -147,13 +149,16 @@ def p3_run(fn, prob, x, v, q, m, want_fields=True):
     N = prob.nx * prob.ny * prob.nz
     fields = np.zeros((12, N)) if want_fields else None
     secs = np.zeros(1)
+    sdiag = np.full((max(prob.n_steps, 1), P3_NSTEPDIAG), np.nan) if want_step_diag else None
     rc = fn(ptr(prob.dparams()), ptr(prob.iparams()), ctypes.c_long(n), ptr(out["x"]), ptr(out["v"]),
             ptr(out["P"]), ptr(out["v_prev"]), ptr(out["vbar"]),
             ptr(np.ascontiguousarray(q, dtype=np.float64)), ptr(np.ascontiguousarray(m, dtype=np.float64)),
-            ptr(diag), ptr(info), ptr(fields), ptr(secs))
+            ptr(diag), ptr(info), ptr(fields), ptr(secs), ptr(sdiag))
     if rc != 0:
         raise RuntimeError("p3 run failed")
     out.update(diag=diag, info=info[:prob.n_steps], seconds=float(secs[0]))
+    if sdiag is not None:
+        out["step_diag"] = sdiag[:prob.n_steps]
     if fields is not None:
         out["fields"] = fields.reshape(12, prob.nx, prob.ny * prob.nz)
     return out

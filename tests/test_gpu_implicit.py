@@ -247,3 +247,34 @@ def test_orbit_kernels_match_reference(k):
         # no orbits: zero current
         Z = sim.orbit_deposit(np.zeros(0), np.zeros(0), np.zeros((0, 3)), np.zeros((0, 3)), np.zeros(0))
         assert np.all(Z == 0.0)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_step_diagnostics_match_reference(case):
+    """upic_step_implicit's step diagnostics against the reference's
+    compute_step_diagnostics of the same steps: the work/energy balances,
+    the A-chain residual and the knot-crossing statistics."""
+    g = dict(np.load(os.path.join(GOLD, case + ".npz")))
+    sim, cfg = load_sim(g)
+    nsteps = int(g["iparams"][12])
+    np_ = len(g["in_q"])
+    names = up.STEP_DIAG_COLUMNS
+    try:
+        sim.init_fields(diagnostics=False)  # energies of the start state computed on demand
+        _, info, sd = sim.step_implicit(nsteps, diagnostics=False, step_diagnostics=True)
+        ref = g["step_diag"]
+        for s in range(nsteps):
+            for k, name in enumerate(names):
+                a, b = sd[s, k], ref[s, k]
+                if name in ("crossing_particles", "total_crossings"):
+                    assert abs(a - b) <= 1, (s, name, a, b)
+                elif name == "avg_path_segments":
+                    assert abs(a - b) <= 1.0 / np_ + 1e-15, (s, name, a, b)
+                elif name == "max_path_segments":
+                    assert a == b, (s, name, a, b)
+                elif abs(b) < 1e-10:
+                    assert abs(a - b) < TOL_ROUNDOFF, (s, name, a, b)  # round-off residuals
+                else:
+                    assert abs(a - b) <= TOL_STEP * (s + 1) * abs(b) + TOL_ROUNDOFF, (s, name, a, b)
+    finally:
+        sim.close()

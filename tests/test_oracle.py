@@ -116,12 +116,13 @@ def test_implicit_fixtures_regenerate_from_reference_build(case):
     g = dict(np.load(os.path.join(GOLD, name + ".npz")))
     prob = ol.P3Problem(**P3_CASES[case][1])
     assert np.array_equal(prob.dparams(), g["dparams"]) and np.array_equal(prob.iparams(), g["iparams"])
-    out = ol.p3_run(ref.ref_p3_run, prob, g["in_x"], g["in_v"], g["in_q"], g["in_m"])
+    out = ol.p3_run(ref.ref_p3_run, prob, g["in_x"], g["in_v"], g["in_q"], g["in_m"], want_step_diag=True)
     for k in ("x", "v", "P", "v_prev", "vbar"):
         assert np.array_equal(out[k], g["out_" + k]), k
     assert np.array_equal(out["diag"], g["diag"])
     assert np.array_equal(out["info"], g["info"])
     assert np.array_equal(out["fields"], g["fields"])
+    assert np.array_equal(out["step_diag"], g["step_diag"])
 
 
 def test_orbit_fixtures_regenerate_from_reference_build(tmp_path, monkeypatch):

@@ -14,7 +14,8 @@ import numpy as np
 from ._native import UPIC_ERR, UpicConfig, c_dp, lib
 
 __all__ = ["UpicError", "Config", "ImplicitConfig", "Simulation", "generate_bimaxwellian",
-           "DIAG_COLUMNS", "IMPLICIT_DIAG_COLUMNS", "SOLVE_INFO_COLUMNS", "METHODS", "FIELDS"]
+           "DIAG_COLUMNS", "IMPLICIT_DIAG_COLUMNS", "SOLVE_INFO_COLUMNS", "STEP_DIAG_COLUMNS", "METHODS",
+           "FIELDS"]
 
 METHODS = {"bdf1": 1, "bdf2": 2, "cn_orbit": 3}
 CHARGE_UPDATES = {"conserving": 0, "naive": 1}
@@ -32,6 +33,13 @@ IMPLICIT_DIAG_COLUMNS = [
     "gauge_normalization_rms", "gauge_relative", "field_energy", "kinetic_energy", "total_energy",
     "rho_mode", "E_mode_re", "E_mode_im", "E_mode_abs", "Bz_y_mode_re", "Bz_y_mode_im",
     "Bz_y_mode_abs"]
+# Step diagnostics of the implicit method (StepDiagnostics, ec_pic_nyquist_projected.cpp:4303-4321),
+# the column order of its _step_diagnostics.csv.
+STEP_DIAG_COLUMNS = ["A_chain_abs_rms", "A_chain_rel_rms", "A_chain_max_norm", "A_chain_mean_norm",
+                     "A_chain_work_defect", "delta_K", "delta_W", "delta_total_energy", "particle_work",
+                     "grid_work", "deposit_gather_work_residual", "particle_energy_residual",
+                     "field_energy_residual", "crossing_particles", "total_crossings", "avg_path_segments",
+                     "max_path_segments"]
 # Per-step outer-solve report (NonlinearSolveInfo, ec_pic_nyquist_projected.cpp:5493-5533).
 SOLVE_INFO_COLUMNS = ["iterations", "converged", "final_rms_residual", "final_max_particle_residual",
                       "local_particle_iterations_max", "local_particle_iterations_mean",
@@ -200,12 +208,15 @@ class Simulation:
         self._check(lib().upic_init_fields(self._ctx, _p(row)))
         return row
 
-    def step_implicit(self, nsteps=1, diagnostics=True):
-        """nsteps implicit steps; returns (diag rows, solve-info rows)."""
+    def step_implicit(self, nsteps=1, diagnostics=True, step_diagnostics=False):
+        """nsteps implicit steps; returns (diag rows, solve-info rows), and
+        the step-diagnostics rows (STEP_DIAG_COLUMNS) as a third item when
+        step_diagnostics is set."""
         diag = np.empty((nsteps, len(IMPLICIT_DIAG_COLUMNS))) if diagnostics else None
         info = np.empty((nsteps, len(SOLVE_INFO_COLUMNS)))
-        self._check(lib().upic_step_implicit(self._ctx, int(nsteps), _p(diag), _p(info)))
-        return diag, info
+        sd = np.empty((nsteps, len(STEP_DIAG_COLUMNS))) if step_diagnostics else None
+        self._check(lib().upic_step_implicit(self._ctx, int(nsteps), _p(diag), _p(info), _p(sd)))
+        return (diag, info, sd) if step_diagnostics else (diag, info)
 
     def step(self, nsteps=1, diag_stride=1):
         diag = np.empty((nsteps, 13)) if diag_stride > 0 else None

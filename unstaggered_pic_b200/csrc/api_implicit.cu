@@ -84,6 +84,13 @@ struct ImplicitState {
            *ograd = nullptr;
     double* ogrid = nullptr;  // mesh, A^n, A^{n+1}: 9 x N
     int* oerr = nullptr;
+    // step diagnostics (grown on first use)
+    double2* sd_spec = nullptr;             // 12 x N
+    double* sd_rec = nullptr;               // 12 doubles per node
+    unsigned long long* sd_counts = nullptr;  // 4
+    // field and kinetic energy of the current state, when known
+    bool energy_valid = false;
+    double energy_W = 0.0, energy_K = 0.0;
     bool loaded = false;  // upic_set_particles has succeeded
     bool ready = false;   // upic_init_fields has succeeded
 };
@@ -418,17 +425,20 @@ void reset_history(upic_ctx* c, ImplicitState& s, const double* x, const double*
     push_history(c, s, x, r);
 }
 
-// The diagnostics row of the current state (compute_diagnostics :3521).
-int state_diagnostics(upic_ctx* c, ImplicitState& s, double* row) {
+// The diagnostics row (compute_diagnostics :3521) of a state: its spectra
+// and particle set (default: the current state).
+int state_diagnostics(upic_ctx* c, ImplicitState& s, double* row, const double2* spec = nullptr, int pset = -1) {
     const upic_config& cf = c->cfg;
     const int N = c->N;
-    UPIC_CUDA(c, launch_diag_spectra(N, c->d_kx, c->d_ky, s.spec, s.dspec, c->st));
+    if (!spec) spec = s.spec;
+    if (pset < 0) pset = s.cur;
+    UPIC_CUDA(c, launch_diag_spectra(N, c->d_kx, c->d_ky, spec, s.dspec, c->st));
     // mode amplitudes from the spectra before the inverse transforms overwrite them
     const int mode = cf.perturbation_mode;
     const int im = ((mode % c->nx) + c->nx) % c->nx, jm = ((mode % c->ny) + c->ny) % c->ny;
     const int idx = im * c->ny, idy = jm;
     double2 modes[3];
-    UPIC_CUDA(c, cudaMemcpyAsync(&modes[0], s.spec + 2 * (size_t)N + idx, sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(&modes[0], spec + 2 * (size_t)N + idx, sizeof(double2), cudaMemcpyDeviceToHost, c->st));
     UPIC_CUDA(c, cudaMemcpyAsync(&modes[1], s.dspec + idx, sizeof(double2), cudaMemcpyDeviceToHost, c->st));
     UPIC_CUDA(c, cudaMemcpyAsync(&modes[2], s.dspec + 5 * (size_t)N + idy, sizeof(double2), cudaMemcpyDeviceToHost, c->st));
     UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 10, 1, c->st, nullptr, 1, s.dreal));
@@ -445,7 +455,7 @@ int state_diagnostics(upic_ctx* c, ImplicitState& s, double* row) {
     d.partials = s.partials;
     d.grid = kNormGrid;
     UPIC_CUDA(c, launch_implicit_diag(d, s.ddots, c->st));
-    const ParticleSoA& p = s.P[s.cur];
+    const ParticleSoA& p = s.P[pset];
     UPIC_CUDA(c, launch_kinetic(s.np, p.vx, p.vy, p.vz, s.uniform ? nullptr : p.m, s.m0, cf.kappa,
                                 s.partials + 32 * kNormGrid, kNormGrid, s.ddots + 20, c->st));
     UPIC_CUDA(c, cudaMemcpyAsync(s.hdots, s.ddots, sizeof(double) * 22, cudaMemcpyDeviceToHost, c->st));
@@ -772,6 +782,7 @@ int implicit_set_particles(upic_ctx* c, long np, const double* x, const double* 
     s.scaleJ[0] = s.scaleJ[1] = s.scaleJ[2] = fixed_scale(bJ);
     s.scaleJ[3] = fixed_scale(qabs / s.dV);
     s.ready = false;
+    s.energy_valid = false;
     s.loaded = true;
     s.steps = 0;
     return sync(c);
@@ -851,7 +862,13 @@ int implicit_init_fields(upic_ctx* c, double* diag_row) {
     c->steps = 0;
     c->fields_ready = true;
     if ((rc = sync(c))) return rc;
-    if (diag_row && (rc = state_diagnostics(c, s, diag_row))) return rc;
+    s.energy_valid = false;
+    if (diag_row) {
+        if ((rc = state_diagnostics(c, s, diag_row))) return rc;
+        s.energy_W = diag_row[UPIC_P3_FIELD_ENERGY];
+        s.energy_K = diag_row[UPIC_P3_KINETIC_ENERGY];
+        s.energy_valid = true;
+    }
     return UPIC_OK;
 }
 
@@ -878,6 +895,75 @@ int implicit_get_field(upic_ctx* c, int which, double* host) {
     UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 1, 1, c->st, nullptr, 1, s.dreal));
     UPIC_CUDA(c, cudaMemcpyAsync(host, s.dreal, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
     return sync(c);
+}
+
+// compute_step_diagnostics (:4501 -> :4340) of the step just accepted: the
+// state before it is the spare particle set and spec_out, the state after it
+// the current set and spec.  W0, K0, W1, K1: field and kinetic energies.
+int step_diagnostics(upic_ctx* c, ImplicitState& s, double W0, double K0, double W1, double K1, double* out) {
+    const upic_config& cf = c->cfg;
+    const int N = c->N;
+    int rc;
+    if (!s.sd_spec) {
+        if ((rc = dalloc(c, &s.sd_spec, 12 * (size_t)N)) || (rc = dalloc(c, &s.sd_rec, 12 * (size_t)N)) ||
+            (rc = dalloc(c, &s.sd_counts, 4)))
+            return rc;
+    }
+    UPIC_CUDA(c, launch_step_diag_spectra(N, c->d_kx, c->d_ky, s.spec_out, s.spec, s.sd_spec, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.sd_spec, 12, 1, c->st, nullptr, 2, s.sd_rec, 12, 0));
+    UPIC_CUDA(c, cudaMemsetAsync(s.sd_counts, 0, sizeof(unsigned long long) * 4, c->st));
+    const ParticleSoA& p0 = s.P[1 - s.cur];
+    StepDiagArgs a{};
+    a.x = p0.x;
+    a.y = p0.y;
+    a.bx = s.bx[s.cur];
+    a.by = s.by[s.cur];
+    a.bz = s.bz[s.cur];
+    a.q = s.uniform ? nullptr : s.P[s.cur].q;
+    a.q0 = s.q0;
+    a.np = s.np;
+    a.nx = c->nx;
+    a.ny = c->ny;
+    a.Lx = cf.Lx;
+    a.Ly = cf.Ly;
+    a.inv_dx = 1.0 / s.dx;
+    a.inv_dy = 1.0 / s.dy;
+    a.dt = cf.dt;
+    a.split = cf.split_orbit_at_knots;
+    a.nq = s.nq;
+    a.qtab = s.qtab;
+    a.rec = s.sd_rec;
+    a.partials = s.partials;
+    a.counts = s.sd_counts;
+    UPIC_CUDA(c, launch_step_diag(s.order, a, kNormGrid, s.ddots, c->st));
+    UPIC_CUDA(c, launch_grid_work(N, s.J, s.sd_rec, s.partials + 16 * kNormGrid, kNormGrid, s.ddots + 14, c->st));
+    unsigned long long cnt[4];
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hdots, s.ddots, sizeof(double) * 16, cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(cnt, s.sd_counts, sizeof(cnt), cudaMemcpyDeviceToHost, c->st));
+    if ((rc = sync(c))) return rc;
+    const double* h = s.hdots;
+    auto tot = [&](int k) { return h[2 * k] + h[2 * k + 1]; };
+    const double denom = (double)std::max<long>(1, 3 * s.np);
+    const double arms = std::sqrt(tot(1) / denom), rhsrms = std::sqrt(tot(2) / denom);
+    double* o = out;
+    o[UPIC_SD_A_CHAIN_ABS_RMS] = std::sqrt(tot(0) / denom);
+    o[UPIC_SD_A_CHAIN_REL_RMS] = o[UPIC_SD_A_CHAIN_ABS_RMS] / (0.5 * (arms + rhsrms) + 1.0e-300);
+    o[UPIC_SD_A_CHAIN_MAX_NORM] = h[12];
+    o[UPIC_SD_A_CHAIN_MEAN_NORM] = tot(3) / (double)std::max<long>(1, s.np);
+    o[UPIC_SD_A_CHAIN_WORK_DEFECT] = tot(4);
+    o[UPIC_SD_DELTA_K] = K1 - K0;
+    o[UPIC_SD_DELTA_W] = W1 - W0;
+    o[UPIC_SD_DELTA_TOTAL_ENERGY] = o[UPIC_SD_DELTA_K] + o[UPIC_SD_DELTA_W];
+    o[UPIC_SD_PARTICLE_WORK] = tot(5);
+    o[UPIC_SD_GRID_WORK] = cf.dt * (h[14] + h[15]) * s.dV;
+    o[UPIC_SD_DEPOSIT_GATHER_WORK_RESIDUAL] = o[UPIC_SD_PARTICLE_WORK] - o[UPIC_SD_GRID_WORK];
+    o[UPIC_SD_PARTICLE_ENERGY_RESIDUAL] = o[UPIC_SD_DELTA_K] - o[UPIC_SD_PARTICLE_WORK];
+    o[UPIC_SD_FIELD_ENERGY_RESIDUAL] = o[UPIC_SD_DELTA_W] + o[UPIC_SD_GRID_WORK];
+    o[UPIC_SD_CROSSING_PARTICLES] = (double)cnt[2];
+    o[UPIC_SD_TOTAL_CROSSINGS] = (double)cnt[1];
+    o[UPIC_SD_AVERAGE_PATH_SEGMENTS] = s.np ? (double)cnt[0] / (double)s.np : 1.0;
+    o[UPIC_SD_MAX_PATH_SEGMENTS] = (double)(s.np ? cnt[3] : 1);
+    return 0;
 }
 
 int orbit_stage(upic_ctx* c, ImplicitState& s, long np) {
@@ -997,17 +1083,36 @@ extern "C" int upic_orbit_gather(upic_ctx* c, long np, const double* x, const do
     return orbit_check(c, s);
 }
 
-extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double* info) {
+extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double* info, double* step_diag) {
     if (!c) return UPIC_ERR_ARGUMENT;
     if (!c->imp) return fail(c, UPIC_ERR_STATE, "context was not created with UPIC_METHOD_CN_ORBIT");
     ImplicitState& s = *c->imp;
     if (!s.ready) return fail(c, UPIC_ERR_STATE, "upic_init_fields first");
     if (nsteps < 0) return fail(c, UPIC_ERR_ARGUMENT, "nsteps < 0");
+    double row[UPIC_P3_DIAG_COUNT];
     for (int k = 0; k < nsteps; ++k) {
-        int rc = implicit_one_step(c, s, info ? info + (size_t)k * UPIC_INFO_COUNT : nullptr);
+        int rc;
+        if (step_diag && !s.energy_valid) {
+            if ((rc = state_diagnostics(c, s, row))) return rc;
+            s.energy_W = row[UPIC_P3_FIELD_ENERGY];
+            s.energy_K = row[UPIC_P3_KINETIC_ENERGY];
+            s.energy_valid = true;
+        }
+        const double W0 = s.energy_W, K0 = s.energy_K;
+        s.energy_valid = false;
+        rc = implicit_one_step(c, s, info ? info + (size_t)k * UPIC_INFO_COUNT : nullptr);
         if (rc) return rc;
         c->steps = s.steps;
-        if (diag && (rc = state_diagnostics(c, s, diag + (size_t)k * UPIC_P3_DIAG_COUNT))) return rc;
+        if (diag || step_diag) {
+            double* r = diag ? diag + (size_t)k * UPIC_P3_DIAG_COUNT : row;
+            if ((rc = state_diagnostics(c, s, r))) return rc;
+            s.energy_W = r[UPIC_P3_FIELD_ENERGY];
+            s.energy_K = r[UPIC_P3_KINETIC_ENERGY];
+            s.energy_valid = true;
+        }
+        if (step_diag &&
+            (rc = step_diagnostics(c, s, W0, K0, s.energy_W, s.energy_K, step_diag + (size_t)k * UPIC_SD_COUNT)))
+            return rc;
     }
     return UPIC_OK;
 }

@@ -137,7 +137,7 @@ UPIC_D void stencil_xy(const Geo& g, double x, double y, Stencil<ORDER>& sx, Ste
 }
 
 // Sum of record component block [off, off+3) at a wrapped position.
-template <int ORDER>
+template <int ORDER, int STRIDE = kIRec>
 UPIC_D void gather_rec3(const Geo& g, const double* __restrict__ rec, int off, double x, double y,
                         double out[3]) {
     Stencil<ORDER> sx, sy;
@@ -148,7 +148,7 @@ UPIC_D void gather_rec3(const Geo& g, const double* __restrict__ rec, int off, d
         const int gx = wrap_index(sx.il + a, g.nx);
 #pragma unroll
         for (int b = 0; b <= ORDER; ++b) {
-            const double* r = rec + (size_t)(gx * g.ny + wrap_index(sy.il + b, g.ny)) * kIRec + off;
+            const double* r = rec + (size_t)(gx * g.ny + wrap_index(sy.il + b, g.ny)) * STRIDE + off;
             const double w = sx.w[a] * sy.w[b];
             out[0] = fma(__ldg(r), w, out[0]);
             out[1] = fma(__ldg(r + 1), w, out[1]);
@@ -1318,6 +1318,189 @@ __global__ void axpy_kernel(int n, const double* a, const double* b, double s, d
         out[i] = a[i] + s * b[i];
 }
 
+// ---- step diagnostics (compute_subcycled_step_diagnostics :4340 with one
+// level per particle, the layout of nonlinear_step_orbit) ---------------------
+constexpr int kSdRec = 12;   // An(3), Ae(3), U_mid(3), E_mid(3) per node
+constexpr int kSdPart = 16;  // per-CTA partials: 6 double-double sums + max
+
+// Spectra of A^n, A^{n+1}, U_mid = (U^n + U^{n+1})/2 and
+// E_mid = -(grad phi^n + grad phi^{n+1})/2 - U_mid.
+__global__ void step_diag_spectra_kernel(int N, const double* kx, const double* ky, const double2* s0,
+                                         const double2* s1, double2* out) {
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        const double kxx = kx[id], kyy = ky[id];
+        const double2 phi0 = s0[id], phi1 = s1[id];
+        double2 um[3];
+        for (int c = 0; c < 3; ++c) {
+            out[(size_t)c * N + id] = s0[(size_t)(3 + c) * N + id];
+            out[(size_t)(3 + c) * N + id] = s1[(size_t)(3 + c) * N + id];
+            const double2 u0 = s0[(size_t)(6 + c) * N + id], u1 = s1[(size_t)(6 + c) * N + id];
+            um[c] = make_double2(0.5 * u0.x + 0.5 * u1.x, 0.5 * u0.y + 0.5 * u1.y);
+            out[(size_t)(6 + c) * N + id] = um[c];
+        }
+        const double2 g0 = cik(kxx, phi0), g1 = cik(kxx, phi1), h0 = cik(kyy, phi0), h1 = cik(kyy, phi1);
+        out[(size_t)9 * N + id] = make_double2(-0.5 * (g0.x + g1.x) - um[0].x, -0.5 * (g0.y + g1.y) - um[0].y);
+        out[(size_t)10 * N + id] = make_double2(-0.5 * (h0.x + h1.x) - um[1].x, -0.5 * (h0.y + h1.y) - um[1].y);
+        out[(size_t)11 * N + id] = make_double2(-um[2].x, -um[2].y);
+    }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(kRed) step_diag_kernel(StepDiagArgs a) {
+    constexpr int S = ORDER + 1;
+    Geo g{a.nx, a.ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    const double* qs = a.qtab;
+    const double* qw = a.qtab + kMaxQuad;
+    DD r2{0, 0}, a2{0, 0}, rhs2{0, 0}, nsum{0, 0}, wdef{0, 0}, pw{0, 0};
+    double nmax = 0.0;
+    unsigned long long segs = 0, cross = 0, cpart = 0;
+    int maxseg = 1;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < a.np; p += (long)gridDim.x * blockDim.x) {
+        const double x0 = a.x[p], y0 = a.y[p];
+        const double vb[3] = {a.bx[p], a.by[p], a.bz[p]};
+        const double q = a.q ? a.q[p] : a.q0;
+        const double h = a.dt;
+        const double dxx = h * vb[0], dxy = h * vb[1];
+        const double x1 = wrap1(x0 + dxx, g.Lx), y1 = wrap1(y0 + dxy, g.Ly);
+        double A0p[3], A1p[3];
+        gather_rec3<ORDER, kSdRec>(g, a.rec, 0, x0, y0, A0p);
+        gather_rec3<ORDER, kSdRec>(g, a.rec, 3, x1, y1, A1p);
+        double b[kMaxBreaks];
+        const int nb = breakpoints<ORDER>(g, x0, y0, dxx, dxy, a.split, b);
+        double Ub[3] = {0.0, 0.0, 0.0}, Eb[3] = {0.0, 0.0, 0.0};
+        double D[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+        for (int k = 0; k + 1 < nb; ++k) {
+            const double sa = b[k], len = b[k + 1] - b[k];
+            if (len <= 0.0) continue;
+            for (int iq = 0; iq < a.nq; ++iq) {
+                const double s = sa + len * qs[iq];
+                const double wq = len * qw[iq];
+                Stencil<ORDER> sx, sy;
+                stencil_xy<ORDER>(g, wrap1(x0 + s * dxx, g.Lx), wrap1(y0 + s * dxy, g.Ly), sx, sy);
+                for (int ia = 0; ia < S; ++ia) {
+                    const int gx = wrap_index(sx.il + ia, a.nx);
+                    for (int ib = 0; ib < S; ++ib) {
+                        const double* r = a.rec + (size_t)(gx * a.ny + wrap_index(sy.il + ib, a.ny)) * kSdRec;
+                        const double shape = sx.w[ia] * sy.w[ib];
+                        const double dsx = sx.dw[ia] * sy.w[ib], dsy = sx.w[ia] * sy.dw[ib];
+                        for (int c = 0; c < 3; ++c) {
+                            Ub[c] += wq * r[6 + c] * shape;
+                            Eb[c] += wq * r[9 + c] * shape;
+                            const double av = (1.0 - s) * r[c] + s * r[3 + c];
+                            D[c][0] += wq * av * dsx;
+                            D[c][1] += wq * av * dsy;
+                        }
+                    }
+                }
+            }
+        }
+        double R[3], Ad[3], rhs[3];
+        for (int c = 0; c < 3; ++c) {
+            Ad[c] = A1p[c] - A0p[c];
+            rhs[c] = h * (Ub[c] + (D[c][0] * vb[0] + D[c][1] * vb[1]));
+            R[c] = Ad[c] - rhs[c];
+        }
+        r2 = dd_add(r2, dot3(R, R));
+        a2 = dd_add(a2, dot3(Ad, Ad));
+        rhs2 = dd_add(rhs2, dot3(rhs, rhs));
+        const double nr = norm3(R);
+        nmax = fmax(nmax, nr);
+        nsum = dd_add(nsum, nr);
+        wdef = dd_add(wdef, -q * dot3(vb, R));
+        pw = dd_add(pw, (h * q) * dot3(vb, Eb));
+        const int nseg = nb - 1 > 1 ? nb - 1 : 1;
+        segs += (unsigned long long)nseg;
+        cross += (unsigned long long)(nseg - 1);
+        cpart += nseg > 1 ? 1ull : 0ull;
+        maxseg = max(maxseg, nseg);
+    }
+    DD v[6] = {r2, a2, rhs2, nsum, wdef, pw};
+    __shared__ double red[kRed / kWarp][kSdPart];
+    const int w = threadIdx.x >> 5;
+    for (int k = 0; k < 6; ++k) {
+        v[k] = warp_sum_dd(v[k]);
+        if ((threadIdx.x & 31) == 0) {
+            red[w][2 * k] = v[k].hi;
+            red[w][2 * k + 1] = v[k].lo;
+        }
+    }
+    nmax = warp_max(nmax);
+    if ((threadIdx.x & 31) == 0) red[w][12] = nmax;
+    for (int o = 16; o > 0; o >>= 1) {
+        segs += __shfl_xor_sync(0xffffffffu, segs, o);
+        cross += __shfl_xor_sync(0xffffffffu, cross, o);
+        cpart += __shfl_xor_sync(0xffffffffu, cpart, o);
+        maxseg = max(maxseg, __shfl_xor_sync(0xffffffffu, maxseg, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&a.counts[0], segs);
+        atomicAdd(&a.counts[1], cross);
+        atomicAdd(&a.counts[2], cpart);
+        atomicMax(&a.counts[3], (unsigned long long)maxseg);
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        const int k = threadIdx.x;
+        double* o = a.partials + (size_t)blockIdx.x * kSdPart;
+        if (k < 6) {
+            DD t{0, 0};
+            for (int q = 0; q < kRed / kWarp; ++q) t = dd_add_dd(t, DD{red[q][2 * k], red[q][2 * k + 1]});
+            o[2 * k] = t.hi;
+            o[2 * k + 1] = t.lo;
+        } else {
+            double mx = 0.0;
+            for (int q = 0; q < kRed / kWarp; ++q) mx = fmax(mx, red[q][12]);
+            o[12] = mx;
+        }
+    }
+}
+
+// One warp per quantity: out[0..11] the six double-double sums, out[12] max.
+__global__ void step_diag_final_kernel(const double* partials, int grid, double* out) {
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (k < 6) {
+        DD t{0, 0};
+        for (int b = lane; b < grid; b += 32)
+            t = dd_add_dd(t, DD{partials[(size_t)b * kSdPart + 2 * k], partials[(size_t)b * kSdPart + 2 * k + 1]});
+        t = warp_sum_dd(t);
+        if (lane == 0) {
+            out[2 * k] = t.hi;
+            out[2 * k + 1] = t.lo;
+        }
+    } else if (k == 6) {
+        double mx = 0.0;
+        for (int b = lane; b < grid; b += 32) mx = fmax(mx, partials[(size_t)b * kSdPart + 12]);
+        mx = warp_max(mx);
+        if (lane == 0) out[12] = mx;
+    }
+}
+
+// sum_m sum_id J_m(id) E_mid,m(id) in double-double (exact products).
+__global__ void __launch_bounds__(kRed) grid_work_kernel(int N, const double* J, const double* rec, double* partials) {
+    DD s{0, 0};
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
+        for (int c = 0; c < 3; ++c) {
+            const double a = J[(size_t)c * N + id], b = rec[(size_t)id * kSdRec + 9 + c];
+            const double pr = a * b;
+            s = dd_add_dd(s, DD{pr, fma(a, b, -pr)});
+        }
+    }
+    s = warp_sum_dd(s);
+    __shared__ double red[kRed / kWarp][2];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[w][0] = s.hi;
+        red[w][1] = s.lo;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD t{0, 0};
+        for (int q = 0; q < kRed / kWarp; ++q) t = dd_add_dd(t, DD{red[q][0], red[q][1]});
+        partials[2 * blockIdx.x] = t.hi;
+        partials[2 * blockIdx.x + 1] = t.lo;
+    }
+}
+
 // ---- diagnostics ----------------------------------------------------------------
 constexpr int kDiagSums = 9;
 
@@ -1520,6 +1703,34 @@ cudaError_t launch_orbit_gather(int order, const OrbitArgs& a, cudaStream_t st) 
         default: return cudaErrorInvalidValue;
     }
     count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step_diag_spectra(int N, const double* kx, const double* ky, const double2* s0,
+                                     const double2* s1, double2* out12, cudaStream_t st) {
+    step_diag_spectra_kernel<<<gsize(N), 256, 0, st>>>(N, kx, ky, s0, s1, out12);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step_diag(int order, const StepDiagArgs& a, int grid, double* out13, cudaStream_t st) {
+    switch (order) {
+        case 1: step_diag_kernel<1><<<grid, kRed, 0, st>>>(a); break;
+        case 2: step_diag_kernel<2><<<grid, kRed, 0, st>>>(a); break;
+        case 3: step_diag_kernel<3><<<grid, kRed, 0, st>>>(a); break;
+        case 4: step_diag_kernel<4><<<grid, kRed, 0, st>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    step_diag_final_kernel<<<1, 32 * 7, 0, st>>>(a.partials, grid, out13);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grid_work(int N, const double* J, const double* rec12, double* partials, int grid, double* out2,
+                             cudaStream_t st) {
+    grid_work_kernel<<<grid, kRed, 0, st>>>(N, J, rec12, partials);
+    pair_final_kernel<<<1, 32, 0, st>>>(partials, grid, out2);
+    count_launches(2);
     return cudaGetLastError();
 }
 

@@ -113,6 +113,33 @@ struct OrbitArgs {
 cudaError_t launch_orbit_deposit(int order, const OrbitArgs& a, cudaStream_t st);
 cudaError_t launch_orbit_gather(int order, const OrbitArgs& a, cudaStream_t st);
 
+// Step diagnostics (compute_subcycled_step_diagnostics :4340, one level per
+// particle): A-chain residual R = (A^{n+1}(x1) - A^n(x0)) - dt (<U_mid> +
+// D_A vbar), particle work dt q vbar.<E_mid>, knot-crossing counts.
+struct StepDiagArgs {
+    const double *x, *y;              // orbit starts (state n, sorted order)
+    const double *bx, *by, *bz;       // accepted orbit velocities (same order)
+    const double* q;                  // per particle, or null (q0)
+    double q0;
+    long np;
+    int nx, ny;
+    double Lx, Ly, inv_dx, inv_dy, dt;
+    int split, nq;
+    const double* qtab;
+    const double* rec;                // 12 doubles per node: An, Ae, U_mid, E_mid
+    double* partials;                 // grid x 16
+    unsigned long long* counts;       // segments, crossings, crossing particles, max segments
+};
+// Spectra (12 x N) of A^n, A^{n+1}, U_mid, E_mid from the two states' spectra.
+cudaError_t launch_step_diag_spectra(int N, const double* kx, const double* ky, const double2* s0,
+                                     const double2* s1, double2* out12, cudaStream_t st);
+// out13: double-double sums R.R, A_delta.A_delta, rhs.rhs, |R|, -q vbar.R,
+// dt q vbar.<E_mid> ([0..11]) and max |R| ([12]).
+cudaError_t launch_step_diag(int order, const StepDiagArgs& a, int grid, double* out13, cudaStream_t st);
+// out2: double-double sum of J . E_mid over nodes and components.
+cudaError_t launch_grid_work(int N, const double* J, const double* rec12, double* partials, int grid,
+                             double* out2, cudaStream_t st);
+
 // Gather of planar 3-vector fields at particle positions (gather_vector_at :2267).
 cudaError_t launch_gather3(int order, int nx, int ny, double Lx, double Ly, const double* f3,
                            long np, const double* x, const double* y, double* out3,
