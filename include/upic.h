@@ -205,6 +205,14 @@ int upic_set_particles(upic_ctx* ctx, long np, const double* x, const double* y,
 int upic_get_particles(upic_ctx* ctx, long np, double* x, double* y, double* P, double* v,
                        double* v_prev);
 
+/* Fixed background charge density (explicit methods): rho_bg, nx*ny doubles,
+ * replaces the uniform ion density n0 in rho0 and in every naive charge
+ * re-deposit -- the reference's ParticleSet::fixed_ion_rho, which the cloud
+ * example fills from stationary ions (spectral_pic_part3.cpp:618-621,
+ * 720-724, deposit_total_charge_naive :739).  NULL restores n0.  Call it
+ * before upic_init_fields. */
+int upic_set_background(upic_ctx* ctx, const double* rho_bg);
+
 /* Start-up fields: rho0 = n0 + deposited electron charge, J0 = deposited
  * current, phi0 from Poisson, A0 = 0, all BDF histories filled with copies
  * (spectral_pic_part3.cpp:1100-1111).  If diag_row is not NULL it receives

@@ -202,6 +202,12 @@ class Simulation:
                                              _p(out["v"]), _p(out["v_prev"])))
         return out
 
+    def set_background(self, rho_bg):
+        """Fixed background charge (nx, ny) in place of the uniform n0
+        (explicit methods); None restores n0."""
+        arr = None if rho_bg is None else _f64(rho_bg).ravel()
+        self._check(lib().upic_set_background(self._ctx, _p(arr)))
+
     def init_fields(self, diagnostics=True):
         ncol = len(IMPLICIT_DIAG_COLUMNS) if self.implicit else len(DIAG_COLUMNS)
         row = np.empty(ncol) if diagnostics else None

@@ -29,6 +29,7 @@ SYMBOLS = {
     "upic_set_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 7),
     "upic_get_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 5),
     "upic_init_fields": (ctypes.c_int, [ctypes.c_void_p, c_dp]),
+    "upic_set_background": (ctypes.c_int, [ctypes.c_void_p, c_dp]),
     "upic_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
     "upic_step_implicit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, c_dp, c_dp]),
     "upic_step_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]),

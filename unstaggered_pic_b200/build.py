@@ -1,6 +1,6 @@
 """Build recipe for libupic.so, the sm_100a CUDA library behind include/upic.h.
 
-    python -m unstaggered_pic_b200.build          # builds unstaggered_pic_b200/libupic.so
+    python -m unstaggered_pic_b200.build          # builds unstaggered_pic_b200/libupic.so and upic_run
 
 nvcc compiles every source for sm_100a (it cross-compiles without a GPU);
 the library links the CUDA runtime statically, so it loads next to any
@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libupic.so")
+RUN = os.path.join(HERE, "upic_run")
 BUILD = os.path.join(ROOT, "_build")
 
 SOURCES = ["fft.cu", "sort.cu", "explicit.cu", "implicit.cu", "api.cu", "api_implicit.cu", "noalloc.cu",
@@ -61,6 +62,14 @@ def build(verbose=False, ptxas_info=False):
         subprocess.run(cmd, check=True)
     if not _newer(OUT, objs) or ptxas_info:
         cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", OUT] + objs
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    # upic_run: the deck-driven driver (host C++ over the C ABI)
+    src = os.path.join(CSRC, "upic_run.cpp")
+    if not _newer(RUN, [src, OUT, os.path.join(ROOT, "include", "upic.h")]):
+        cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), src, "-o", RUN,
+               "-L", HERE, "-lupic", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -108,6 +108,9 @@ int iota(upic_ctx* c, int* id, long n);
 
 int alloc_soa(upic_ctx* c, ParticleSoA& s, long cap, bool with_state, bool with_qm) {
     int rc = 0;
+    // two elements of padding: bulk prefetches widen their ranges to 16-byte
+    // boundaries (explicit.cu prefetch_l2)
+    cap += 2;
     double** arrs[] = {&s.x, &s.y, &s.vx, &s.vy, &s.vz};
     for (double** a : arrs)
         if ((rc = dalloc(c, a, cap))) return rc;
@@ -664,7 +667,7 @@ int upic_init_fields(upic_ctx* c, double* diag_row) {
     } else {
         UPIC_CUDA(c, cudaMemsetAsync(c->d_pdiag, 0, sizeof(double) * c->push_grid * kDiagPart, c->st));
     }
-    UPIC_CUDA(c, launch_convert_acc(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0, 3, c->st));
+    UPIC_CUDA(c, launch_convert_acc(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0, 3, c->st, c->d_bg));
     // phi0 from Poisson (:1104, :819-827), histories (:1107-1111)
     double2* sp = c->d_spec;
     UPIC_CUDA(c, fft2d_batched(c->plan, sp + 3 * (size_t)N, 1, 0, c->st, c->d_rho));
@@ -717,7 +720,7 @@ int upic_step(upic_ctx* c, int nsteps, int diag_stride, double* diag) {
         }
         // J^n (and rho^n) were deposited by the previous particle kernel
         UPIC_CUDA(c, launch_convert_acc(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0,
-                                        naive ? 3 : 1, c->st));
+                                        naive ? 3 : 1, c->st, c->d_bg));
         UPIC_CUDA(c, fft2d_batched(c->plan, sp, 3, 0, c->st, c->d_J));
         if (naive) UPIC_CUDA(c, fft2d_batched(c->plan, sp + 3 * (size_t)N, 1, 0, c->st, c->d_rho));
         KspaceArgs k{};
@@ -785,6 +788,24 @@ int upic_profile_read(upic_ctx* c, double* push_ms, long* push_launches, long* k
     if (push_ms) *push_ms = total;
     if (push_launches) *push_launches = (long)c->prof_events.size();
     if (kernel_launches) *kernel_launches = launches_total();
+    return UPIC_OK;
+}
+
+int upic_set_background(upic_ctx* c, const double* rho_bg) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (c->imp) return fail(c, UPIC_ERR_STATE, "the implicit method has a uniform background (n0)");
+    if (!rho_bg) {
+        dfree(c, c->d_bg);
+        c->d_bg = nullptr;
+    } else {
+        for (int id = 0; id < c->N; ++id)
+            if (!std::isfinite(rho_bg[id])) return fail(c, UPIC_ERR_NONFINITE, "non-finite background charge");
+        int rc;
+        if (!c->d_bg && (rc = dalloc(c, &c->d_bg, c->N))) return rc;
+        UPIC_CUDA(c, cudaMemcpyAsync(c->d_bg, rho_bg, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+        if ((rc = sync(c))) return rc;
+    }
+    c->fields_ready = false;
     return UPIC_OK;
 }
 

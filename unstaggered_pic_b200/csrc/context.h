@@ -65,6 +65,7 @@ struct upic_ctx {
     double* d_partials = nullptr;
     double* d_pdiag = nullptr;
     double* d_row = nullptr;
+    double* d_bg = nullptr;   // fixed background charge (upic_set_background) or null: uniform n0
     double* h_row = nullptr;  // pinned
 
     int head = 0;

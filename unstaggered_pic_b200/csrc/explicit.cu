@@ -59,6 +59,54 @@ UPIC_D void fold_window(const unsigned long long* whi, const unsigned long long*
     }
 }
 
+// Bulk L2 prefetch (sm_90+ TMA unit) of elements [i0, i1) of a particle
+// array.  The range is widened to 16-byte boundaries; particle arrays carry
+// two elements of padding (alloc_soa), so the widened range stays inside
+// the allocation.  A prefetch is a hint: it moves no data into the SM.
+UPIC_D void prefetch_l2(const double* base, int i0, int i1) {
+    if (!base || i1 <= i0) return;
+    const unsigned long long a0 = reinterpret_cast<unsigned long long>(base + i0) & ~15ull;
+    const unsigned long long a1 = (reinterpret_cast<unsigned long long>(base + i1) + 15ull) & ~15ull;
+    const unsigned bytes = (unsigned)(a1 - a0);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"(bytes) : "memory");
+}
+
+// Prefetch of the particle state the CTA reads in its next batch of
+// kPushThreads particles: the rest of this chunk, else the next chunk.
+template <int MODE, bool UNIFORM>
+UPIC_D void prefetch_next_batch(const PushArgs& a, const Chunk& ch, int base, int ci, int c_end) {
+    int n0, n1;
+    if (base + kPushThreads < ch.end) {
+        n0 = base + kPushThreads;
+        n1 = min(n0 + kPushThreads, ch.end);
+    } else if (ci + 1 < c_end) {
+        const Chunk nx = a.chunks[ci + 1];
+        n0 = nx.start;
+        n1 = min(nx.start + kPushThreads, nx.end);
+    } else {
+        return;
+    }
+    const int t = threadIdx.x;
+    const double* arr = nullptr;
+    switch (t) {
+        case 0: arr = a.p.x; break;
+        case 1: arr = a.p.y; break;
+        case 2: arr = a.p.vx; break;
+        case 3: arr = a.p.vy; break;
+        case 4: arr = a.p.vz; break;
+        case 5: arr = MODE == kModePush ? a.p.wx : nullptr; break;
+        case 6: arr = MODE == kModePush ? a.p.wy : nullptr; break;
+        case 7: arr = MODE == kModePush ? a.p.wz : nullptr; break;
+        case 8: arr = MODE == kModePush ? a.p.Px : nullptr; break;
+        case 9: arr = MODE == kModePush ? a.p.Py : nullptr; break;
+        case 10: arr = MODE == kModePush ? a.p.Pz : nullptr; break;
+        case 11: arr = UNIFORM ? nullptr : a.p.q; break;
+        case 12: arr = UNIFORM ? nullptr : a.p.m; break;
+        default: break;
+    }
+    prefetch_l2(arr, n0, n1);
+}
+
 template <int MODE, int NCOMP, bool UNIFORM>
 __global__ void __launch_bounds__(kPushThreads, 3)
 push_deposit_kernel(PushArgs a, TileGeom tg) {
@@ -120,6 +168,7 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
         for (int base = ch.start; base < ch.end; base += kPushThreads) {
             const int p = base + threadIdx.x;
             const bool active = p < ch.end;
+            if (threadIdx.x < 13) prefetch_next_batch<MODE, UNIFORM>(a, ch, base, ci, c_end);
             int key = kKeyNone, gx0 = 0, gy0 = 0;
             double dwx[3], dwy[3], dval[NCOMP];
             if (active) {
@@ -367,7 +416,8 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
 
 // acc -> doubles, then clear (kept on device for the next deposit).
 __global__ void convert_acc_kernel(unsigned long long* acc, int N, double s0, double s1, double s2,
-                                   double s3, double* J, double* rho, double n0, int mask) {
+                                   double s3, double* J, double* rho, double n0, int mask,
+                                   const double* bg) {
     for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x) {
         if (mask & 1) {
             const double sc[3] = {s0, s1, s2};
@@ -383,7 +433,7 @@ __global__ void convert_acc_kernel(unsigned long long* acc, int N, double s0, do
         if (mask & 2) {
             unsigned long long* h = acc + (size_t)6 * N;
             unsigned long long* l = acc + (size_t)7 * N;
-            rho[id] = n0 + from_fixed(h[id], l[id], 1.0 / s3);
+            rho[id] = (bg ? bg[id] : n0) + from_fixed(h[id], l[id], 1.0 / s3);
             h[id] = 0ull;
             l[id] = 0ull;
         }
@@ -725,9 +775,9 @@ cudaError_t launch_push_deposit(int mode, int ncomp, bool uniform, const TileGeo
 }
 
 cudaError_t launch_convert_acc(unsigned long long* acc, int N, const double* scale, double* J,
-                               double* rho, double n0, int mask, cudaStream_t st) {
+                               double* rho, double n0, int mask, cudaStream_t st, const double* bg) {
     convert_acc_kernel<<<grid_for(N, 256), 256, 0, st>>>(acc, N, scale[0], scale[1], scale[2],
-                                                         scale[3], J, rho, n0, mask);
+                                                         scale[3], J, rho, n0, mask, bg);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -123,10 +123,12 @@ cudaError_t push_configure_smem(const TileGeom& tg);
 int push_occupancy(const TileGeom& tg, int ncomp);
 
 // acc -> real fields: J (3 x N) from slots 0..2 when ncomp_mask & 1;
-// rho = n0 + slot 3 when ncomp_mask & 2.  Zeroes the converted slots.
+// rho = background + slot 3 when ncomp_mask & 2, the background being bg[id]
+// (a fixed charge field) or, with bg null, the uniform n0.  Zeroes the
+// converted slots.
 cudaError_t launch_convert_acc(unsigned long long* acc, int N, const double* scale,
                                double* J, double* rho, double n0, int ncomp_mask,
-                               cudaStream_t st);
+                               cudaStream_t st, const double* bg = nullptr);
 
 struct KspaceArgs {
     int N;
