@@ -56,8 +56,12 @@ enum {
  * energy-conserving orbit-averaged GM-HC-CN step (relativistic
  * Higuera-Cary rotation, Crank-Nicolson potentials, outer Anderson/Picard
  * iteration on the mesh current), Project3/ec_pic_nyquist_projected.cpp
- * nonlinear_step_orbit:6477; runs in 2D (nz = 1). */
-enum { UPIC_METHOD_BDF1 = 1, UPIC_METHOD_BDF2 = 2, UPIC_METHOD_CN_ORBIT = 3 };
+ * nonlinear_step_orbit:6477.  CN_ORBIT_NONREL: the non-relativistic
+ * orbit-averaged CN step with Picard iteration on the particle velocities,
+ * Project1/ec_pic_serial_demo.cpp picard_step_orbit:1509 (c, eps0, mu0 as in
+ * the explicit methods; no Nyquist projection, Nyquist wave numbers kept).
+ * The implicit methods run in 2D (nz = 1). */
+enum { UPIC_METHOD_BDF1 = 1, UPIC_METHOD_BDF2 = 2, UPIC_METHOD_CN_ORBIT = 3, UPIC_METHOD_CN_ORBIT_NONREL = 4 };
 
 /* Outer nonlinear solver of the implicit method (Config::nonlinear_solver,
  * ec_pic_nyquist_projected.cpp:891). */
@@ -139,6 +143,11 @@ typedef struct upic_config {
     double anderson_damping, anderson_regularization, anderson_growth_limit;
     double local_rtol, local_atol, local_damping;  /* particle_local_* */
     int perturbation_mode;         /* x (and y) Fourier mode of the diagnostics */
+    /* Non-relativistic implicit method (UPIC_METHOD_CN_ORBIT_NONREL): the
+     * Project1 deck keys (Config, ec_pic_serial_demo.cpp:232-301). */
+    double picard_tol;
+    int picard_max_iter;
+    int final_consistency_sweep;
 } upic_config;
 
 typedef struct upic_ctx upic_ctx;
@@ -151,15 +160,27 @@ enum {
     UPIC_P3_PSI_OVER_KAPPA2_RMS, UPIC_P3_DIVA_RMS, UPIC_P3_GAUGE_NORM_RMS, UPIC_P3_GAUGE_RELATIVE,
     UPIC_P3_FIELD_ENERGY, UPIC_P3_KINETIC_ENERGY, UPIC_P3_TOTAL_ENERGY, UPIC_P3_RHO_MODE,
     UPIC_P3_E_MODE_RE, UPIC_P3_E_MODE_IM, UPIC_P3_E_MODE_ABS, UPIC_P3_BZ_Y_MODE_RE,
-    UPIC_P3_BZ_Y_MODE_IM, UPIC_P3_BZ_Y_MODE_ABS, UPIC_P3_DIAG_COUNT
+    UPIC_P3_BZ_Y_MODE_IM, UPIC_P3_BZ_Y_MODE_ABS, UPIC_P3_MEAN_RHO, UPIC_P3_DIAG_COUNT
 };
+/* UPIC_METHOD_CN_ORBIT_NONREL fills the same row with Project1's
+ * definitions (compute_diagnostics, ec_pic_serial_demo.cpp:1057): Gauss law
+ * div E - rho/eps0, gauge psi/c^2 + div A, field energy eps0/2 E^2 + B^2/(2
+ * mu0), kinetic energy sum m v^2/2; Project1's columns are gauss_rms,
+ * gauss_max, gauge_rms, field/kinetic/total energy, rho_mode, E_mode_*,
+ * mean_rho. */
 
 /* Per-step solve report of the implicit method (NonlinearSolveInfo,
  * ec_pic_nyquist_projected.cpp:5493-5533). */
 enum {
     UPIC_INFO_ITERATIONS = 0, UPIC_INFO_CONVERGED, UPIC_INFO_FINAL_RMS_RESIDUAL,
     UPIC_INFO_FINAL_MAX_PARTICLE_RESIDUAL, UPIC_INFO_LOCAL_ITER_MAX, UPIC_INFO_LOCAL_ITER_MEAN,
-    UPIC_INFO_ANDERSON_STEPS, UPIC_INFO_PICARD_STEPS, UPIC_INFO_COUNT
+    UPIC_INFO_ANDERSON_STEPS, UPIC_INFO_PICARD_STEPS,
+    /* Picard errors of the last iteration (picard_step_orbit,
+     * ec_pic_serial_demo.cpp:1509-1530; NaN for CN_ORBIT) and the path
+     * statistics of the accepted orbits (crossing particles, average and
+     * maximum segments per orbit), the _diagnostics.csv columns of both. */
+    UPIC_INFO_CURRENT_ERROR, UPIC_INFO_VELOCITY_ERROR, UPIC_INFO_CROSSING_PARTICLES,
+    UPIC_INFO_AVG_PATH_SEGMENTS, UPIC_INFO_MAX_PATH_SEGMENTS, UPIC_INFO_COUNT
 };
 
 /* Step diagnostics of the implicit method: StepDiagnostics of

@@ -27,7 +27,7 @@ enum {
     I_NX, I_NY, I_NZ, I_ORDER, I_NQ, I_SPLIT, I_NYQ, I_NL_MAXIT, I_AND_MEM, I_AND_START,
     I_LOC_MAXIT, I_SOLVER, I_NSTEPS, I_MODE, I_COUNT
 };
-constexpr int kDiag = 22;
+constexpr int kDiag = 23;
 constexpr int kInfo = 8;
 constexpr int kStepDiag = 17;
 
@@ -70,7 +70,7 @@ void store_diag(const Diagnostics& d, double* o) {
                              d.gauge_normalization_rms, d.gauge_relative, d.field_energy,
                              d.kinetic_energy, d.total_energy, d.rho_mode, d.E_mode_re,
                              d.E_mode_im, d.E_mode_abs, d.Bz_y_mode_re, d.Bz_y_mode_im,
-                             d.Bz_y_mode_abs};
+                             d.Bz_y_mode_abs, d.mean_rho};
     std::memcpy(o, v, sizeof(v));
 }
 

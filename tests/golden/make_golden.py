@@ -1,17 +1,20 @@
 """Regenerate the golden fixtures in tests/golden/ from the reference's own code.
 
-Runs the reference solvers Project2/spectral_pic_part3.cpp and
-Project3/ec_pic_nyquist_projected.cpp through the C-ABI harnesses
-oracle/_ref/libref_p2.so and oracle/_ref/libref_p3.so (built by `make -C
-oracle` from the reference sources) on small seeded inputs and saves inputs
-and outputs, and copies the published validation numbers of
-Project2/docs/validation_summary.json.  The
+Runs the reference solvers Project2/spectral_pic_part3.cpp,
+Project3/ec_pic_nyquist_projected.cpp and Project1/ec_pic_serial_demo.cpp
+through the C-ABI harnesses oracle/_ref/libref_p2.so, libref_p3.so and
+libref_p1.so (built by `make -C oracle` from the reference sources) on small
+seeded inputs and saves inputs and outputs, and copies the published
+validation numbers of Project2/docs/validation_summary.json and the columns
+of the shipped Project1/output/landau_weak run.  The
 fixtures let the oracle and the GPU path be checked where the reference
 sources are absent.
 
     python tests/golden/make_golden.py        # all fixtures
     python tests/golden/make_golden.py p3     # the implicit-method runs only
+    python tests/golden/make_golden.py p1     # the non-relativistic implicit runs only
 """
+import csv
 import ctypes
 import json
 import os
@@ -101,6 +104,7 @@ def main():
     with open(os.path.join(HERE, "p2_weibel_published.json"), "w") as fh:
         json.dump({"source": "Project2/docs/validation_summary.json", "runs": runs}, fh, indent=1)
     p3_main()
+    p1_main()
     print("fixtures written")
 
 
@@ -199,8 +203,89 @@ def p3_main():
         print(name, "iterations", out["info"][:, 0].tolist())
 
 
+# Non-relativistic implicit (Project1) runs: (name, problem keywords,
+# particle source).  "ref": the reference's own initializer (two_stream or
+# Landau); ("thermal", vth, nonuniform): seeded particles with thermal
+# velocities in all three components, per-particle charges when nonuniform.
+P1_CASES = [
+    ("p1_run_landau_weak", dict(nx=32, ny=1, Lx=12.566370614359172, Ly=1.0, Lz=1.0, dt=0.1, order=1, nq=12,
+                                picard_tol=1e-10, picard_maxit=24, n_steps=60, ppc=32, case="landau_weak",
+                                landau_alpha=0.01, vth=1.0), "ref"),
+    ("p1_run_landau_strong_o3", dict(nx=16, ny=2, Lx=12.566370614359172, Ly=1.0, Lz=1.0, dt=0.1, order=3,
+                                     nq=12, picard_tol=1e-10, picard_maxit=30, n_steps=8, ppc=16,
+                                     case="landau_strong", landau_alpha=0.5, vth=1.0), "ref"),
+    ("p1_run_two_stream_o2", dict(nx=16, ny=8, Lx=2 * np.pi, Ly=2 * np.pi, Lz=2 * np.pi, dt=0.025, order=2,
+                                  nq=16, n_steps=6, ppc=4, case="two_stream"), "ref"),
+    ("p1_run_thermal_o2_nosplit", dict(nx=16, ny=16, Lx=2 * np.pi, Ly=2 * np.pi, Lz=1.0, dt=0.1, order=2,
+                                       nq=8, split=False, n_steps=4),
+     ("thermal", (0.1, 0.1, 0.05), False)),
+    ("p1_run_thermal_o1_weights", dict(nx=16, ny=16, Lx=2 * np.pi, Ly=np.pi, Lz=0.5, dt=0.1, order=1, nq=6,
+                                       n_steps=4), ("thermal", (0.2, 0.1, 0.1), True)),
+    ("p1_run_o4_capped", dict(nx=8, ny=16, Lx=2 * np.pi, Ly=2 * np.pi, Lz=2 * np.pi, dt=0.1, order=4, nq=8,
+                              picard_maxit=3, sweep=False, n_steps=3), ("thermal", (0.05, 0.05, 0.0), False)),
+]
+# The reference embeds these 2D runs in 3D with nz = 1 and also splits orbits
+# at z knots; the z spline is constant there, so that changes no integral,
+# only the path statistics.  Runs with both knot splitting and z motion use
+# orders whose z knots the particles do not reach (1 and 3), or vz = 0.
+
+
+def p1_particles(rng, prob, vth, nonuniform, ppc=8):
+    """Seeded particles on the Project1 box [-L/2, L/2) (z = 0): thermal
+    velocities, charges summing to -n0 Lx Ly Lz, m = |q|."""
+    n = prob.nx * prob.ny * ppc
+    x = np.zeros((n, 3))
+    x[:, 0] = rng.uniform(-prob.Lx / 2, prob.Lx / 2, n)
+    x[:, 1] = rng.uniform(-prob.Ly / 2, prob.Ly / 2, n)
+    p3_edge_positions(x, prob.Lx, prob.Ly, prob.nx, prob.ny)
+    v = rng.normal(size=(n, 3)) * np.asarray(vth)
+    w = rng.uniform(0.5, 1.5, n) if nonuniform else np.ones(n)
+    q = -prob.n0 * prob.Lx * prob.Ly * prob.Lz * w / w.sum()
+    return x, v, q, np.abs(q)
+
+
+def p1_main():
+    """Fixtures of the non-relativistic implicit Picard step from
+    oracle/_ref/libref_p1.so, and the columns of the reference's shipped
+    landau_weak run (Project1/output) that the harness reproduces."""
+    lib = ol.ref_p1()
+    if lib is None:
+        raise SystemExit("oracle/_ref/libref_p1.so missing: run make -C oracle")
+    for k, (name, kw, src) in enumerate(P1_CASES):
+        prob = ol.P1Problem(**kw)
+        if src == "ref":
+            x, v, q, m = ol.p1_init(lib, prob)
+        else:
+            x, v, q, m = p1_particles(np.random.default_rng(20261210 + k), prob, src[1], src[2])
+        out = ol.p1_run(lib.ref_p1_run, prob, x, v, q, m)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), dparams=prob.dparams(), iparams=prob.iparams(),
+                            in_x=x, in_v=v, in_q=q, in_m=m,
+                            **{"out_" + c: out[c] for c in ("x", "v", "P", "v_prev")},
+                            diag=out["diag"], info=out["info"], fields=out["fields"], step_diag=out["step_diag"])
+        print(name, len(q), "particles, iterations", out["info"][:, 0].astype(int).tolist())
+    shipped = os.path.join(REF, "Project1", "output", "landau_weak")
+    with open(shipped + "_diagnostics.csv") as fh:
+        rows = list(csv.reader(fh))
+    with open(shipped + "_step_diagnostics.csv") as fh:
+        srows = list(csv.reader(fh))
+    # the shipped run is 300 steps long; the deck's first 60 are kept
+    hdr, data = rows[0], rows[1:62]
+    srows = srows[:61]
+    info_cols = ["picard_iterations", "picard_current_error", "picard_velocity_error", "crossing_particles",
+                 "avg_path_segments", "max_path_segments"]
+    diag = np.array([[float(r[hdr.index(c)]) for c in ol.P1_DIAG_NAMES] for r in data])
+    info = np.array([[float(r[hdr.index(c)]) for c in info_cols] for r in data[1:]])
+    sdiag = np.array([[float(v) for v in r[2:]] for r in srows[1:]])
+    np.savez_compressed(os.path.join(HERE, "p1_landau_weak_shipped.npz"), diag=diag, info=info,
+                        step_diag=sdiag, diag_columns=np.array(ol.P1_DIAG_NAMES),
+                        info_columns=np.array(info_cols), step_diag_columns=np.array(srows[0][2:]))
+    print("p1_landau_weak_shipped written")
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "p3":
         p3_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "p1":
+        p1_main()
     else:
         main()

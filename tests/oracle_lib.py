@@ -100,14 +100,14 @@ def init_weibel(lib_fn, nx, ny, Lx, Ly, ppc, c=1.0, n0=1.0, vx=0.5, vy_max=0.01,
 # Project3 (implicit GM-HC-CN) runs: dparams / iparams layout of
 # oracle/ref/ref_p3_harness.cpp and oracle/p3_oracle.c.
 REF_P3_SO = os.path.join(ROOT, "oracle", "_ref", "libref_p3.so")
-P3_NDIAG = 22
+P3_NDIAG = 23
 P3_NINFO = 8
 P3_NSTEPDIAG = 17
 P3_DIAG_NAMES = ["gauss_rms", "gauss_max", "divE_rms", "sigma1_rho_rms", "gauss_normalization_rms",
                  "gauss_relative", "gauge_rms", "gauge_max", "psi_over_kappa2_rms", "divA_rms",
                  "gauge_normalization_rms", "gauge_relative", "field_energy", "kinetic_energy",
                  "total_energy", "rho_mode", "E_mode_re", "E_mode_im", "E_mode_abs", "Bz_y_mode_re",
-                 "Bz_y_mode_im", "Bz_y_mode_abs"]
+                 "Bz_y_mode_im", "Bz_y_mode_abs", "mean_rho"]
 
 
 def ref_p3():
@@ -176,3 +176,73 @@ def p3_particles(rng, nx, ny, ppc, Lx, Ly, uth=(0.02, 0.2, 0.0), n0=1.0, Lz=1.0)
     v = u / gam[:, None]
     q = np.full(n, -n0 * Lx * Ly * Lz / n)
     return x, v, q, np.abs(q)
+
+
+# Project1 (non-relativistic implicit Picard) runs: dparams / iparams layout
+# of oracle/ref/ref_p1_harness.cpp.
+REF_P1_SO = os.path.join(ROOT, "oracle", "_ref", "libref_p1.so")
+P1_NDIAG = 11
+P1_NINFO = 6
+P1_DIAG_NAMES = ["gauss_rms", "gauss_max", "gauge_rms", "field_energy", "kinetic_energy", "total_energy",
+                 "rho_mode", "E_mode_re", "E_mode_im", "E_mode_abs", "mean_rho"]
+
+
+def ref_p1():
+    return _load(REF_P1_SO)
+
+
+class P1Problem:
+    def __init__(self, nx, ny, Lx, Ly, dt, nz=1, Lz=1.0, c=1.0, eps0=1.0, mu0=1.0, n0=1.0, order=2, nq=16,
+                 split=True, picard_tol=1e-11, picard_maxit=16, sweep=True, n_steps=1, mode=1, ppc=4,
+                 case="two_stream", v0=0.3, perturbation=0.02, landau_alpha=-1.0, vth=1.0):
+        self.__dict__.update(locals())
+        del self.__dict__["self"]
+
+    def dparams(self):
+        return np.array([self.Lx, self.Ly, self.Lz, self.dt, self.c, self.eps0, self.mu0, self.n0,
+                         self.picard_tol, self.v0, self.perturbation, self.landau_alpha, self.vth])
+
+    def iparams(self):
+        return np.array([self.nx, self.ny, self.nz, self.order, self.nq, int(self.split), self.picard_maxit,
+                         int(self.sweep), self.n_steps, self.mode, self.ppc,
+                         1 if self.case.startswith("landau") else 0], dtype=np.int32)
+
+
+def p1_init(lib, prob, cap=10_000_000):
+    """Particles of the reference's own initial condition: x, v (np, 3), q, m."""
+    x = np.zeros((cap, 3))
+    v = np.zeros((cap, 3))
+    q = np.zeros(cap)
+    m = np.zeros(cap)
+    lib.ref_p1_init.restype = ctypes.c_long
+    n = lib.ref_p1_init(ptr(prob.dparams()), ptr(prob.iparams()), ctypes.c_long(cap), ptr(x), ptr(v), ptr(q),
+                        ptr(m))
+    if n < 0:
+        raise RuntimeError("p1 init failed")
+    return x[:n].copy(), v[:n].copy(), q[:n].copy(), m[:n].copy()
+
+
+def p1_run(fn, prob, x, v, q, m, want_fields=True):
+    """Run fn (ref_p1_run) on copies: x, v (np, 3).  Returns dict with x, v,
+    P, v_prev, diag (n_steps+1, 11), info (n_steps, 6), step_diag (n_steps,
+    17), fields (12, nx, ny*nz) and seconds."""
+    n = len(q)
+    out = {"x": np.ascontiguousarray(x, dtype=np.float64).copy(),
+           "v": np.ascontiguousarray(v, dtype=np.float64).copy(),
+           "P": np.zeros((n, 3)), "v_prev": np.zeros((n, 3))}
+    diag = np.full((prob.n_steps + 1, P1_NDIAG), np.nan)
+    info = np.full((max(prob.n_steps, 1), P1_NINFO), np.nan)
+    sdiag = np.full((max(prob.n_steps, 1), 17), np.nan)
+    N = prob.nx * prob.ny * prob.nz
+    fields = np.zeros((12, N)) if want_fields else None
+    secs = np.zeros(1)
+    rc = fn(ptr(prob.dparams()), ptr(prob.iparams()), ctypes.c_long(n), ptr(out["x"]), ptr(out["v"]),
+            ptr(out["P"]), ptr(out["v_prev"]), ptr(np.ascontiguousarray(q, dtype=np.float64)),
+            ptr(np.ascontiguousarray(m, dtype=np.float64)), ptr(diag), ptr(info), ptr(sdiag), ptr(fields),
+            ptr(secs))
+    if rc != 0:
+        raise RuntimeError("p1 run failed")
+    out.update(diag=diag, info=info[:prob.n_steps], step_diag=sdiag[:prob.n_steps], seconds=float(secs[0]))
+    if fields is not None:
+        out["fields"] = fields.reshape(12, prob.nx, prob.ny * prob.nz)
+    return out

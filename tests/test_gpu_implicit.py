@@ -82,7 +82,7 @@ def compare_diag(row, ref, nyquist, tol):
     for k, name in enumerate(names):
         a, b = row[k], ref[k]
         roundoff = name in ("gauss_rms", "gauss_max", "gauge_rms", "gauge_max", "gauss_relative",
-                            "gauge_relative")
+                            "gauge_relative", "mean_rho")
         if roundoff and (nyquist or abs(b) < 1e-9):
             assert abs(a - b) < TOL_ROUNDOFF * max(1.0, abs(b)) or abs(a) < 1e-11, (name, a, b)
         else:

@@ -139,3 +139,43 @@ def test_orbit_fixtures_regenerate_from_reference_build(tmp_path, monkeypatch):
     assert a.keys() == b.keys()
     for k in a:
         assert np.array_equal(a[k], b[k]), k
+
+
+def test_p1_landau_weak_fixture_is_the_shipped_run():
+    """tests/golden/p1_run_landau_weak.npz (the reference's landau_weak deck
+    through oracle/_ref/libref_p1.so) carries the very numbers of the run the
+    reference ships in Project1/output/landau_weak_*.csv (extracted into
+    tests/golden/p1_landau_weak_shipped.npz): every diagnostics, Picard and
+    step-diagnostics column of all 60 steps agrees to the last printed digit
+    (17 significant digits, so bit for bit)."""
+    g = dict(np.load(os.path.join(GOLD, "p1_run_landau_weak.npz")))
+    s = dict(np.load(os.path.join(GOLD, "p1_landau_weak_shipped.npz")))
+    assert list(s["diag_columns"]) == ol.P1_DIAG_NAMES
+    assert np.array_equal(g["diag"], s["diag"], equal_nan=True)
+    assert np.array_equal(g["info"], s["info"], equal_nan=True)
+    assert np.array_equal(g["step_diag"], s["step_diag"], equal_nan=True)
+
+
+@pytest.mark.parametrize("case", [0, 3, 5])
+def test_p1_fixtures_regenerate_from_reference_build(case):
+    """The committed non-relativistic fixtures (tests/golden/p1_run_*.npz)
+    are outputs of the reference's own solver (Project1/ec_pic_serial_demo.cpp):
+    rerunning the reference build on the stored inputs reproduces them bit
+    for bit.  Skipped where oracle/_ref/libref_p1.so is absent."""
+    ref = ol.ref_p1()
+    if ref is None:
+        pytest.skip("reference harness not built (no reference sources)")
+    from golden.make_golden import P1_CASES
+    name, kw, src = P1_CASES[case]
+    g = dict(np.load(os.path.join(GOLD, name + ".npz")))
+    prob = ol.P1Problem(**kw)
+    assert np.array_equal(prob.dparams(), g["dparams"]) and np.array_equal(prob.iparams(), g["iparams"])
+    if src == "ref":
+        x, v, q, m = ol.p1_init(ref, prob)
+        assert np.array_equal(x, g["in_x"]) and np.array_equal(v, g["in_v"]) and np.array_equal(q, g["in_q"])
+    out = ol.p1_run(ref.ref_p1_run, prob, g["in_x"], g["in_v"], g["in_q"], g["in_m"])
+    for k in ("x", "v", "P", "v_prev"):
+        assert np.array_equal(out[k], g["out_" + k]), k
+    for k in ("diag", "info", "step_diag"):
+        assert np.array_equal(out[k], g[k], equal_nan=True), k
+    assert np.array_equal(out["fields"], g["fields"])

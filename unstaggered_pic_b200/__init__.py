@@ -13,11 +13,12 @@ import numpy as np
 
 from ._native import UPIC_ERR, UpicConfig, c_dp, lib
 
-__all__ = ["UpicError", "Config", "ImplicitConfig", "Simulation", "generate_bimaxwellian",
-           "DIAG_COLUMNS", "IMPLICIT_DIAG_COLUMNS", "SOLVE_INFO_COLUMNS", "STEP_DIAG_COLUMNS", "METHODS",
+__all__ = ["UpicError", "Config", "ImplicitConfig", "NonrelConfig", "Simulation", "generate_bimaxwellian",
+           "DIAG_COLUMNS", "IMPLICIT_DIAG_COLUMNS", "NONREL_DIAG_COLUMNS", "SOLVE_INFO_COLUMNS",
+           "STEP_DIAG_COLUMNS", "METHODS",
            "FIELDS"]
 
-METHODS = {"bdf1": 1, "bdf2": 2, "cn_orbit": 3}
+METHODS = {"bdf1": 1, "bdf2": 2, "cn_orbit": 3, "cn_orbit_nonrel": 4}
 CHARGE_UPDATES = {"conserving": 0, "naive": 1}
 NONLINEAR_SOLVERS = {"anderson_quasi_newton": 0, "anderson": 0, "picard": 1}
 FIELDS = {"phi": 0, "Ax": 1, "Ay": 2, "Az": 3, "rho": 4, "Jx": 5, "Jy": 6, "Jz": 7,
@@ -32,7 +33,11 @@ IMPLICIT_DIAG_COLUMNS = [
     "gauss_relative", "gauge_rms", "gauge_max", "psi_over_kappa2_rms", "divA_rms",
     "gauge_normalization_rms", "gauge_relative", "field_energy", "kinetic_energy", "total_energy",
     "rho_mode", "E_mode_re", "E_mode_im", "E_mode_abs", "Bz_y_mode_re", "Bz_y_mode_im",
-    "Bz_y_mode_abs"]
+    "Bz_y_mode_abs", "mean_rho"]
+# Diagnostics of the non-relativistic method (Diagnostics, Project1/ec_pic_serial_demo.cpp:1037-1055),
+# taken from the implicit row by name.
+NONREL_DIAG_COLUMNS = ["gauss_rms", "gauss_max", "gauge_rms", "field_energy", "kinetic_energy",
+                       "total_energy", "rho_mode", "E_mode_re", "E_mode_im", "E_mode_abs", "mean_rho"]
 # Step diagnostics of the implicit method (StepDiagnostics, ec_pic_nyquist_projected.cpp:4303-4321),
 # the column order of its _step_diagnostics.csv.
 STEP_DIAG_COLUMNS = ["A_chain_abs_rms", "A_chain_rel_rms", "A_chain_max_norm", "A_chain_mean_norm",
@@ -43,7 +48,9 @@ STEP_DIAG_COLUMNS = ["A_chain_abs_rms", "A_chain_rel_rms", "A_chain_max_norm", "
 # Per-step outer-solve report (NonlinearSolveInfo, ec_pic_nyquist_projected.cpp:5493-5533).
 SOLVE_INFO_COLUMNS = ["iterations", "converged", "final_rms_residual", "final_max_particle_residual",
                       "local_particle_iterations_max", "local_particle_iterations_mean",
-                      "anderson_steps", "picard_fallback_steps"]
+                      "anderson_steps", "picard_fallback_steps", "picard_current_error",
+                      "picard_velocity_error", "crossing_particles", "avg_path_segments",
+                      "max_path_segments"]
 
 
 class UpicError(RuntimeError):
@@ -143,6 +150,41 @@ class ImplicitConfig:
         return cfg
 
 
+class NonrelConfig:
+    """Deck of the non-relativistic implicit orbit-averaged method with
+    Picard iteration on the particle velocities, with the keys and defaults
+    of the reference Config (Project1/ec_pic_serial_demo.cpp:232-301), 2D
+    (nz = 1; Lz sets the cell volume).  Positions live in [-L/2, L/2)."""
+
+    def __init__(self, nx=4, ny=4, Lx=2 * np.pi, Ly=2 * np.pi, Lz=2 * np.pi, dt=0.00625, c=1.0, eps0=1.0,
+                 mu0=1.0, n0=1.0, spline_order=2, orbit_quad_order=16, split_orbit_at_knots=True,
+                 picard_tol=1.0e-11, picard_max_iter=16, final_consistency_sweep=True, perturbation_mode=1,
+                 tile=0, guard=-1):
+        self.method = "cn_orbit_nonrel"
+        self.nx, self.ny, self.Lx, self.Ly, self.Lz, self.dt = nx, ny, Lx, Ly, Lz, dt
+        self.c, self.eps0, self.mu0, self.n0 = c, eps0, mu0, n0
+        self.spline_order, self.orbit_quad_order = spline_order, orbit_quad_order
+        self.split_orbit_at_knots = split_orbit_at_knots
+        self.picard_tol, self.picard_max_iter = picard_tol, picard_max_iter
+        self.final_consistency_sweep = final_consistency_sweep
+        self.perturbation_mode, self.tile, self.guard = perturbation_mode, tile, guard
+
+    def to_c(self):
+        cfg = UpicConfig()
+        lib().upic_config_default(ctypes.byref(cfg))
+        cfg.nx, cfg.ny = int(self.nx), int(self.ny)
+        cfg.Lx, cfg.Ly, cfg.Lz, cfg.dt = float(self.Lx), float(self.Ly), float(self.Lz), float(self.dt)
+        cfg.method = METHODS["cn_orbit_nonrel"]
+        cfg.c, cfg.eps0, cfg.mu0, cfg.n0 = float(self.c), float(self.eps0), float(self.mu0), float(self.n0)
+        cfg.spline_order, cfg.orbit_quad_order = int(self.spline_order), int(self.orbit_quad_order)
+        cfg.split_orbit_at_knots = int(bool(self.split_orbit_at_knots))
+        cfg.picard_tol, cfg.picard_max_iter = float(self.picard_tol), int(self.picard_max_iter)
+        cfg.final_consistency_sweep = int(bool(self.final_consistency_sweep))
+        cfg.perturbation_mode = int(self.perturbation_mode)
+        cfg.tile, cfg.guard = int(self.tile), int(self.guard)
+        return cfg
+
+
 class Simulation:
     """One device context: particles + field state of the explicit BDF/IAEM
     step (Config) or of the implicit orbit-averaged GM-HC-CN step
@@ -157,7 +199,7 @@ class Simulation:
             raise UpicError(rc, lib().upic_last_error(None).decode())
         self.np = 0
         self.N = config.nx * config.ny
-        self.implicit = cfg.method == METHODS["cn_orbit"]
+        self.implicit = cfg.method in (METHODS["cn_orbit"], METHODS["cn_orbit_nonrel"])
 
     def _check(self, rc):
         if rc != 0:

@@ -82,6 +82,8 @@ class UpicConfig(ctypes.Structure):
         ("local_rtol", ctypes.c_double), ("local_atol", ctypes.c_double),
         ("local_damping", ctypes.c_double),
         ("perturbation_mode", ctypes.c_int),
+        ("picard_tol", ctypes.c_double), ("picard_max_iter", ctypes.c_int),
+        ("final_consistency_sweep", ctypes.c_int),
     ]
 
 

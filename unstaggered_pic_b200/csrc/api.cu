@@ -56,8 +56,15 @@ void dfree(upic_ctx* c, void* p) {
 
 bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
-int mode_number(int i, int n) {
-    // spectral_pic_part3.cpp:320-330: Nyquist wave number zeroed.
+// Integer Fourier mode of FFT index i on an n-point axis.
+enum ModeConvention {
+    kModesP2,        // spectral_pic_part3.cpp:320-330: Nyquist zeroed (n = 1 gives -1)
+    kModesP3,        // ec_pic_nyquist_projected.cpp:1485-1504: Nyquist zeroed, n = 1 gives 0
+    kModesKeepNyq    // ec_pic_serial_demo.cpp:385-391: Nyquist kept as +n/2, n = 1 gives 0
+};
+int mode_number(int i, int n, ModeConvention conv = kModesP2) {
+    if (conv != kModesP2 && n == 1) return 0;
+    if (conv == kModesKeepNyq) return (i <= n / 2) ? i : i - n;
     if (n > 1 && i == n / 2) return 0;
     return (i < n / 2) ? i : i - n;
 }
@@ -422,6 +429,10 @@ int upic_config_default(upic_config* cfg) {
     cfg->local_atol = 1.0e-13;
     cfg->local_damping = 1.0;
     cfg->perturbation_mode = 1;
+    // non-relativistic implicit method: ec_pic_serial_demo.cpp:232-301
+    cfg->picard_tol = 1.0e-11;
+    cfg->picard_max_iter = 16;
+    cfg->final_consistency_sweep = 1;
     return UPIC_OK;
 }
 
@@ -436,10 +447,23 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
     if (!pow2(cfg->nx) || !pow2(cfg->ny) || cfg->nx > 8192 || cfg->ny > 8192)
         return fail(nullptr, UPIC_ERR_CONFIG,
                     "the radix-2 FFT requires nx and ny to be powers of two (<= 8192)");
-    const bool implicit = cfg->method == UPIC_METHOD_CN_ORBIT;
+    const bool nonrel = cfg->method == UPIC_METHOD_CN_ORBIT_NONREL;
+    const bool implicit = cfg->method == UPIC_METHOD_CN_ORBIT || nonrel;
     if (!is_bdf(cfg->method) && !implicit)
-        return fail(nullptr, UPIC_ERR_CONFIG, "method must be bdf1, bdf2 or cn_orbit");
-    if (implicit) {
+        return fail(nullptr, UPIC_ERR_CONFIG, "method must be bdf1, bdf2, cn_orbit or cn_orbit_nonrel");
+    if (nonrel) {
+        // Config of ec_pic_serial_demo.cpp:232-301 and the checks of make_grid
+        // / bspline (:396, :565)
+        if (!(cfg->Lx > 0) || !(cfg->Ly > 0) || !(cfg->Lz > 0) || !(cfg->dt > 0) || !(cfg->c > 0) ||
+            !(cfg->eps0 > 0) || !(cfg->mu0 > 0))
+            return fail(nullptr, UPIC_ERR_CONFIG, "Lx, Ly, Lz, dt, c, eps0, mu0 must be positive");
+        if (cfg->spline_order < 1 || cfg->spline_order > 4)
+            return fail(nullptr, UPIC_ERR_CONFIG, "spline_order must be 1, 2, 3 or 4");
+        if (cfg->orbit_quad_order < 1 || cfg->orbit_quad_order > 32)
+            return fail(nullptr, UPIC_ERR_CONFIG, "orbit_quad_order must be in 1..32");
+        if (cfg->picard_max_iter < 1) return fail(nullptr, UPIC_ERR_CONFIG, "picard_max_iter must be positive");
+        if (!(cfg->picard_tol >= 0)) return fail(nullptr, UPIC_ERR_CONFIG, "picard_tol must be non-negative");
+    } else if (implicit) {
         // validation of ec_pic_nyquist_projected.cpp read_config / make_grid
         if (!(cfg->Lx > 0) || !(cfg->Ly > 0) || !(cfg->Lz > 0) || !(cfg->dt > 0) || !(cfg->kappa > 0) ||
             !(cfg->sigma1 > 0) || !(cfg->sigma2 > 0))
@@ -521,14 +545,22 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
     if (cudaMallocHost(&c->h_row, sizeof(double) * UPIC_DIAG_COUNT) != cudaSuccess)
         return bail(fail(c, UPIC_ERR_NOMEM, "cudaMallocHost failed"));
     std::vector<double> kx(N), ky(N), k2(N);
+    const ModeConvention dconv = implicit ? kModesP3 : kModesP2;
+    const ModeConvention lconv = nonrel ? kModesKeepNyq : dconv;
     for (int i = 0; i < c->nx; ++i) {
-        const double kxi = 2.0 * kPi * (double)mode_number(i, c->nx) / cfg->Lx;
+        const double kxi = 2.0 * kPi * (double)mode_number(i, c->nx, dconv) / cfg->Lx;
+        const double kxf = 2.0 * kPi * (double)mode_number(i, c->nx, lconv) / cfg->Lx;
         for (int j = 0; j < c->ny; ++j) {
-            const double kyj = 2.0 * kPi * (double)mode_number(j, c->ny) / cfg->Ly;
+            const double kyj = 2.0 * kPi * (double)mode_number(j, c->ny, dconv) / cfg->Ly;
+            const double kyf = 2.0 * kPi * (double)mode_number(j, c->ny, lconv) / cfg->Ly;
             const int id = i * c->ny + j;
+            // First derivatives take the zeroed Nyquist wave number in every
+            // method: Project1 keeps +n/2 but returns the real part of each
+            // inverse transform, which removes the i k_Nyquist component.
+            // Its k^2 (Poisson, wave step) keeps the Nyquist value.
             kx[id] = kxi;
             ky[id] = kyj;
-            k2[id] = kxi * kxi + kyj * kyj;
+            k2[id] = kxf * kxf + kyf * kyf;
         }
     }
     if (cudaMemcpy(c->d_twx, tw_x.data(), sizeof(double2) * tw_x.size(), cudaMemcpyHostToDevice) ||

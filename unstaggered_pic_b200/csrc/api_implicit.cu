@@ -91,6 +91,13 @@ struct ImplicitState {
     // field and kinetic energy of the current state, when known
     bool energy_valid = false;
     double energy_W = 0.0, energy_K = 0.0;
+    // non-relativistic Picard method (UPIC_METHOD_CN_ORBIT_NONREL)
+    bool picard = false;
+    double *gx = nullptr, *gy = nullptr, *gz = nullptr;  // velocity guess (sorted order)
+    double* Jprev = nullptr;                              // 3 x N
+    unsigned long long* pstat = nullptr;                  // path statistics counters (4)
+    int* perr = nullptr;
+    double vb_limit = 0.0;  // bound on |vbar| components of the fixed-point deposit
     bool loaded = false;  // upic_set_particles has succeeded
     bool ready = false;   // upic_init_fields has succeeded
 };
@@ -187,6 +194,9 @@ int alloc_particles(upic_ctx* c, ImplicitState& s, long cap, bool with_qm) {
         if ((rc = dalloc(c, &s.bx[k], cap)) || (rc = dalloc(c, &s.by[k], cap)) || (rc = dalloc(c, &s.bz[k], cap)))
             return rc;
     }
+    if (s.picard &&
+        ((rc = dalloc(c, &s.gx, cap)) || (rc = dalloc(c, &s.gy, cap)) || (rc = dalloc(c, &s.gz, cap))))
+        return rc;
     if ((rc = alloc_sortwork(c, s.sw, cap, s.tg))) return rc;
     s.cap = cap;
     return ensure_tmp3(c, cap);
@@ -200,6 +210,10 @@ void free_particles(upic_ctx* c, ImplicitState& s) {
         dfree(c, s.bz[k]);
         s.bx[k] = s.by[k] = s.bz[k] = nullptr;
     }
+    dfree(c, s.gx);
+    dfree(c, s.gy);
+    dfree(c, s.gz);
+    s.gx = s.gy = s.gz = nullptr;
     free_sortwork(c, s.sw);
     s.cap = 0;
 }
@@ -322,6 +336,194 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
         return fail(c, UPIC_ERR_LOCAL_PARTICLE, buf);
     }
     return 0;
+}
+
+int path_stats(upic_ctx* c, ImplicitState& s, double* out3);
+
+// relative_rms_error_vec_particles / relative_rms_error_vecfield
+// (ec_pic_serial_demo.cpp:188, :196) from double-double sums over `count`
+// components: r2 = |a - b|^2, map2 = |a|^2, guess2 = |b|^2.
+double relative_rms(const NormSums& h, double count) {
+    const double cnt = std::max(1.0, count);
+    const double rd = std::sqrt((h.r2[0] + h.r2[1]) / cnt);
+    const double ra = std::sqrt((h.map2[0] + h.map2[1]) / cnt);
+    const double rb = std::sqrt((h.guess2[0] + h.guess2[1]) / cnt);
+    return rd / (0.5 * (ra + rb) + 1.0e-300);
+}
+
+// One evaluation of the Picard map at the velocity guess (s.gx, s.gy, s.gz):
+// evaluate_picard_map_orbit (ec_pic_serial_demo.cpp:1455).  Jbar lands in
+// s.map, the trial state in the spare particle set and spec_out; vel: the
+// velocity-change sums.
+int picard_eval(upic_ctx* c, ImplicitState& s, NormSums& vel) {
+    const upic_config& cf = c->cfg;
+    const int N = c->N;
+    const ParticleSoA& p = s.P[s.cur];
+    const ParticleSoA& o = s.P[1 - s.cur];
+    // Jbar: orbit-averaged deposit of vbar = (v_guess + v^n) / 2 (:1468-1472)
+    UPIC_CUDA(c, cudaMemsetAsync(s.acc, 0, sizeof(unsigned long long) * 6 * (size_t)N, c->st));
+    UPIC_CUDA(c, cudaMemsetAsync(s.dstats, 0, sizeof(MapStats), c->st));
+    UPIC_CUDA(c, cudaMemsetAsync(&s.dstats->first_fail_key, 0xff, sizeof(unsigned long long), c->st));
+    UPIC_CUDA(c, cudaMemsetAsync(s.perr, 0, sizeof(int), c->st));
+    if (s.np > 0) {
+        ImplicitMapArgs a{};
+        a.x = p.x; a.y = p.y; a.vx = p.vx; a.vy = p.vy; a.vz = p.vz;
+        a.q = p.q; a.q0 = s.q0; a.id = p.id;
+        a.gx = s.gx; a.gy = s.gy; a.gz = s.gz;
+        a.vb_limit = s.vb_limit;
+        a.np = s.np;
+        a.Lx = cf.Lx; a.Ly = cf.Ly; a.inv_dx = 1.0 / s.dx; a.inv_dy = 1.0 / s.dy; a.inv_dV = 1.0 / s.dV;
+        a.dt = cf.dt; a.kappa = cf.kappa;
+        a.split = cf.split_orbit_at_knots;
+        a.chunks = s.sw.chunks;
+        a.nchunks = s.sw.nchunks;
+        a.acc = s.acc;
+        for (int d = 0; d < 3; ++d) a.scale[d] = s.scaleJ[d];
+        a.stats = s.dstats;
+        a.qtab = s.qtab;
+        a.nq = s.nq;
+        a.mnq = s.mnq;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (c->profiling) {
+            UPIC_CUDA(c, cudaEventCreate(&e0));
+            UPIC_CUDA(c, cudaEventCreate(&e1));
+            UPIC_CUDA(c, cudaEventRecord(e0, c->st));
+        }
+        UPIC_CUDA(c, launch_implicit_map(s.order, s.uniform, a.split != 0, s.tg, a, s.grid, c->st, true));
+        if (c->profiling) {
+            UPIC_CUDA(c, cudaEventRecord(e1, c->st));
+            c->prof_events.emplace_back(e0, e1);
+        }
+    }
+    UPIC_CUDA(c, launch_convert_acc(s.acc, N, s.scaleJ, s.map, nullptr, 0.0, 1, c->st));
+    // continuity, CN update of the potentials (:1474-1482)
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.Jhat, 3, 0, c->st, s.map));
+    CnArgs k{};
+    k.nx = c->nx; k.ny = c->ny; k.N = N;
+    k.kx = c->d_kx; k.ky = c->d_ky; k.k2 = c->d_k2;
+    k.excl = nullptr;
+    k.Jhat = s.Jhat;
+    k.st = s.spec;
+    k.out = s.spec_out;
+    k.gspec = s.gspec;
+    k.dt = cf.dt; k.kappa = cf.kappa; k.sigma1 = cf.sigma1; k.sigma2 = cf.sigma2;
+    UPIC_CUDA(c, launch_cn_kspace(k, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.gspec, 2, 1, c->st, nullptr, 2, s.rec, kIRec, kIRecGpm));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.gspec + 2 * (size_t)N, 3, 1, c->st, nullptr, 2, s.rec, kIRec, kIRecAe));
+    // push (:1484-1505)
+    PicardPushArgs q{};
+    q.x = p.x; q.y = p.y; q.Px = p.Px; q.Py = p.Py; q.Pz = p.Pz; q.vx = p.vx; q.vy = p.vy; q.vz = p.vz;
+    q.gx = s.gx; q.gy = s.gy; q.gz = s.gz;
+    q.q = p.q; q.m = p.m; q.q0 = s.q0; q.m0 = s.m0;
+    q.np = s.np;
+    q.ox = o.x; q.oy = o.y; q.oPx = o.Px; q.oPy = o.Py; q.oPz = o.Pz; q.ovx = o.vx; q.ovy = o.vy; q.ovz = o.vz;
+    q.nx = c->nx; q.ny = c->ny;
+    q.Lx = cf.Lx; q.Ly = cf.Ly; q.inv_dx = 1.0 / s.dx; q.inv_dy = 1.0 / s.dy; q.dt = cf.dt;
+    q.rec = s.rec;
+    q.split = cf.split_orbit_at_knots;
+    q.nq = s.nq;
+    q.mnq = s.mnq;
+    q.qtab = s.qtab;
+    q.partials = s.partials;
+    q.err = s.perr;
+    UPIC_CUDA(c, launch_picard_push(s.order, s.uniform, q.split != 0, q, kNormGrid, s.dnorm, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hstats, s.dstats, sizeof(MapStats), cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hnorm, s.dnorm, sizeof(NormSums), cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hflag, s.perr, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    int rc = sync(c);
+    if (rc) return rc;
+    if (s.hstats->failures > 0 && (int)(s.hstats->first_fail_key & 0xffu) == kLocalNonfiniteIterate)
+        return fail(c, UPIC_ERR_NONCONVERGED,
+                    "Picard iterate velocity is not finite or exceeds 16 times the initial bound max(|v|, c)");
+    if (s.hstats->failures > 0 || *s.hflag > 0)
+        return fail(c, UPIC_ERR_TOO_LARGE, "an orbit crosses more spline knots than the kernel holds (38)");
+    vel = *s.hnorm;
+    return 0;
+}
+
+// One step of the non-relativistic method: picard_step_orbit
+// (ec_pic_serial_demo.cpp:1509-1559).  The iteration count is a fixed upper
+// limit; the reference accepts the last iterate when it is reached.
+int picard_one_step(upic_ctx* c, ImplicitState& s, double* info) {
+    const upic_config& cf = c->cfg;
+    const int N = c->N, n3 = 3 * N;
+    int rc;
+    if (s.np > 0 && (rc = sort_active(c, s))) return rc;
+    // A^n records for D_A and the start-point gathers
+    UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec + 3 * (size_t)N, sizeof(double2) * 3 * N,
+                                 cudaMemcpyDeviceToDevice, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 3, 1, c->st, nullptr, 2, s.rec, kIRec, kIRecAn));
+    const ParticleSoA& p = s.P[s.cur];
+    const ParticleSoA& o = s.P[1 - s.cur];
+    // v_guess = 2 v^n - v^{n-1} (:1514)
+    if (s.np > 0) {
+        UPIC_CUDA(c, launch_extrapolate((int)s.np, p.vx, p.wx, s.gx, c->st));
+        UPIC_CUDA(c, launch_extrapolate((int)s.np, p.vy, p.wy, s.gy, c->st));
+        UPIC_CUDA(c, launch_extrapolate((int)s.np, p.vz, p.wz, s.gz, c->st));
+    }
+    const size_t pb = sizeof(double) * s.np;
+    auto guess_from_trial = [&]() -> int {
+        if (s.np == 0) return 0;
+        UPIC_CUDA(c, cudaMemcpyAsync(s.gx, o.vx, pb, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.gy, o.vy, pb, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.gz, o.vz, pb, cudaMemcpyDeviceToDevice, c->st));
+        return 0;
+    };
+    bool have_prev = false, converged = false;
+    int iters = 0;
+    double cur_err = NAN, vel_err = NAN;
+    for (int it = 0; it < cf.picard_max_iter; ++it) {
+        NormSums vel;
+        if ((rc = picard_eval(c, s, vel))) return rc;
+        vel_err = relative_rms(vel, 3.0 * (double)s.np);
+        cur_err = INFINITY;
+        if (have_prev) {
+            UPIC_CUDA(c, launch_residual_norms(N, s.map, s.Jprev, 1.0, 0.0, 1.0, s.partials, kNormGrid, s.dnorm,
+                                               c->st));
+            UPIC_CUDA(c, cudaMemcpyAsync(s.hnorm, s.dnorm, sizeof(NormSums), cudaMemcpyDeviceToHost, c->st));
+            if ((rc = sync(c))) return rc;
+            cur_err = relative_rms(*s.hnorm, (double)n3);
+        }
+        iters = it + 1;
+        if (it > 0 && std::max(cur_err, vel_err) < cf.picard_tol) {
+            converged = true;
+            break;
+        }
+        UPIC_CUDA(c, cudaMemcpyAsync(s.Jprev, s.map, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
+        have_prev = true;
+        if ((rc = guess_from_trial())) return rc;
+    }
+    if (cf.final_consistency_sweep) {
+        // tr = evaluate_picard_map_orbit(tr.v_next, ...) (:1537-1539)
+        if ((rc = guess_from_trial())) return rc;
+        NormSums vel;
+        if ((rc = picard_eval(c, s, vel))) return rc;
+    }
+    // accept: x, P, v from the trial set; v_prev = v^n; fields from spec_out
+    ParticleSoA& nw = s.P[1 - s.cur];
+    if (s.np > 0) {
+        UPIC_CUDA(c, cudaMemcpyAsync(nw.wx, p.vx, pb, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(nw.wy, p.vy, pb, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(nw.wz, p.vz, pb, cudaMemcpyDeviceToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(nw.id, p.id, sizeof(int) * s.np, cudaMemcpyDeviceToDevice, c->st));
+        if (!s.uniform) {
+            UPIC_CUDA(c, cudaMemcpyAsync(nw.q, p.q, pb, cudaMemcpyDeviceToDevice, c->st));
+            UPIC_CUDA(c, cudaMemcpyAsync(nw.m, p.m, pb, cudaMemcpyDeviceToDevice, c->st));
+        }
+    }
+    s.cur = 1 - s.cur;
+    std::swap(s.spec, s.spec_out);
+    UPIC_CUDA(c, cudaMemcpyAsync(s.J, s.map, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
+    if (info) {
+        for (int k = 0; k < UPIC_INFO_COUNT; ++k) info[k] = NAN;
+        info[UPIC_INFO_ITERATIONS] = iters;
+        info[UPIC_INFO_CONVERGED] = converged ? 1.0 : 0.0;
+        info[UPIC_INFO_CURRENT_ERROR] = cur_err;
+        info[UPIC_INFO_VELOCITY_ERROR] = vel_err;
+        if ((rc = path_stats(c, s, info + UPIC_INFO_CROSSING_PARTICLES))) return rc;
+    }
+    ++s.steps;
+    return sync(c);
 }
 
 // finite_node_vector (:5051) of a 3 x N node vector.
@@ -457,7 +659,7 @@ int state_diagnostics(upic_ctx* c, ImplicitState& s, double* row, const double2*
     UPIC_CUDA(c, launch_implicit_diag(d, s.ddots, c->st));
     const ParticleSoA& p = s.P[pset];
     UPIC_CUDA(c, launch_kinetic(s.np, p.vx, p.vy, p.vz, s.uniform ? nullptr : p.m, s.m0, cf.kappa,
-                                s.partials + 32 * kNormGrid, kNormGrid, s.ddots + 20, c->st));
+                                s.partials + 32 * kNormGrid, kNormGrid, s.ddots + 20, c->st, s.picard));
     UPIC_CUDA(c, cudaMemcpyAsync(s.hdots, s.ddots, sizeof(double) * 22, cudaMemcpyDeviceToHost, c->st));
     int rc = sync(c);
     if (rc) return rc;
@@ -488,6 +690,48 @@ int state_diagnostics(upic_ctx* c, ImplicitState& s, double* row, const double2*
     r[UPIC_P3_BZ_Y_MODE_RE] = modes[2].x * invN;
     r[UPIC_P3_BZ_Y_MODE_IM] = modes[2].y * invN;
     r[UPIC_P3_BZ_Y_MODE_ABS] = std::hypot(modes[2].x, modes[2].y) * invN;
+    r[UPIC_P3_MEAN_RHO] = tot(8) / (double)N;
+    return 0;
+}
+
+// Knot-crossing statistics of the step just accepted (the orbits from the
+// spare set's positions): crossing particles, average and maximum segments
+// per orbit (PathStats, ec_pic_nyquist_projected.cpp and
+// ec_pic_serial_demo.cpp:835).  Orbit velocity: the stored vbar, or for the
+// Picard method (v^{n+1} + v^n) / 2 as Project1's main loop forms it.
+int path_stats(upic_ctx* c, ImplicitState& s, double* out3) {
+    const upic_config& cf = c->cfg;
+    const ParticleSoA& p0 = s.P[1 - s.cur];
+    const ParticleSoA& p1 = s.P[s.cur];
+    PathStatsArgs a{};
+    a.x = p0.x;
+    a.y = p0.y;
+    if (s.picard) {
+        a.v1x = p1.vx;
+        a.v1y = p1.vy;
+        a.v0x = p0.vx;
+        a.v0y = p0.vy;
+    } else {
+        a.bx = s.bx[s.cur];
+        a.by = s.by[s.cur];
+    }
+    a.np = s.np;
+    a.nx = c->nx;
+    a.ny = c->ny;
+    a.Lx = cf.Lx;
+    a.Ly = cf.Ly;
+    a.dt = cf.dt;
+    a.split = cf.split_orbit_at_knots;
+    a.counts = s.pstat;
+    unsigned long long h[4];
+    UPIC_CUDA(c, cudaMemsetAsync(s.pstat, 0, sizeof(unsigned long long) * 4, c->st));
+    if (s.np > 0) UPIC_CUDA(c, launch_path_stats(s.order, a, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(h, s.pstat, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+    const int rc = sync(c);
+    if (rc) return rc;
+    out3[0] = (double)h[2];
+    out3[1] = s.np ? (double)h[0] / (double)s.np : (s.picard ? 0.0 : 1.0);
+    out3[2] = (double)(s.np ? h[3] : 1);
     return 0;
 }
 
@@ -624,6 +868,10 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
         info[UPIC_INFO_LOCAL_ITER_MEAN] = s.np > 0 ? (double)ms.iter_total / (double)s.np : 0.0;
         info[UPIC_INFO_ANDERSON_STEPS] = anderson_steps;
         info[UPIC_INFO_PICARD_STEPS] = picard_steps;
+        info[UPIC_INFO_CURRENT_ERROR] = NAN;
+        info[UPIC_INFO_VELOCITY_ERROR] = NAN;
+        int rc2 = path_stats(c, s, info + UPIC_INFO_CROSSING_PARTICLES);
+        if (rc2) return rc2;
     }
     ++s.steps;
     return sync(c);
@@ -644,9 +892,18 @@ __global__ void wrap_positions_kernel(double* x, double* y, long n, double Lx, d
 
 // ---------------------------------------------------------------------------
 int implicit_create(upic_ctx* c) {
-    const upic_config& cf = c->cfg;
     auto* s = new ImplicitState();
     c->imp = s;
+    if (c->cfg.method == UPIC_METHOD_CN_ORBIT_NONREL) {
+        // Project1's constants in the roles of Project3's: light speed c,
+        // scalar source 1/eps0, vector source mu0; no Nyquist projection
+        c->cfg.kappa = c->cfg.c;
+        c->cfg.sigma1 = 1.0 / c->cfg.eps0;
+        c->cfg.sigma2 = c->cfg.mu0;
+        c->cfg.nyquist_projection = 0;
+        s->picard = true;
+    }
+    const upic_config& cf = c->cfg;
     s->order = cf.spline_order;
     s->nq = cf.orbit_quad_order;
     s->dx = cf.Lx / c->nx;
@@ -656,7 +913,7 @@ int implicit_create(upic_ctx* c) {
     // window guard: the orbit reaches kappa*dt from its start; sorting every
     // step leaves no drift on top of that
     const double reach = cf.kappa * cf.dt / std::min(s->dx, s->dy);
-    const int guard = cf.guard >= 0 ? cf.guard : (int)std::ceil(reach) + 1;
+    const int guard = cf.guard >= 0 ? cf.guard : (s->picard ? 2 : (int)std::ceil(reach) + 1);
     const int tile = cf.tile > 0 ? cf.tile : 8;
     s->tg = make_tiles(c->nx, c->ny, tile, guard, s->order / 2, s->order / 2 + 1);
     s->tg.key_origin_x = 0.5 * cf.Lx;
@@ -664,9 +921,9 @@ int implicit_create(upic_ctx* c) {
     s->tg.key_shift = 0.0;
     s->tg.chunk = 1024;
     const bool split = cf.split_orbit_at_knots != 0;
-    if (implicit_configure_smem(s->tg, s->order, split) != cudaSuccess)
+    if (implicit_configure_smem(s->tg, s->order, split, s->picard) != cudaSuccess)
         return fail(c, UPIC_ERR_CUDA, "cudaFuncSetAttribute (implicit map) failed");
-    const int occ = implicit_map_occupancy(s->tg, s->order, split);
+    const int occ = implicit_map_occupancy(s->tg, s->order, split, s->picard);
     s->grid = c->nsm * (occ > 0 ? occ : 1);
     // Gauss rules: the deck's nq points, and for segment moments (order <= 2
     // with knot splitting) the (order+1)-point rule.  Within a knot-split
@@ -701,8 +958,9 @@ int implicit_create(upic_ctx* c) {
         (rc = dalloc(c, &s->trial_map, 3 * (size_t)N)) || (rc = dalloc(c, &s->cand, 3 * (size_t)N)) ||
         (rc = dalloc(c, &s->resid, 3 * (size_t)N)) || (rc = dalloc(c, &s->partials, 64 * (size_t)kNormGrid)) ||
         (rc = dalloc(c, &s->dnorm, 1)) || (rc = dalloc(c, &s->dstats, 1)) || (rc = dalloc(c, &s->ddots, 32)) ||
-        (rc = dalloc(c, &s->dflag, 1)))
+        (rc = dalloc(c, &s->dflag, 1)) || (rc = dalloc(c, &s->pstat, 4)) || (rc = dalloc(c, &s->perr, 1)))
         return rc;
+    if (s->picard && (rc = dalloc(c, &s->Jprev, 3 * (size_t)N))) return rc;
     for (int k = 0; k < kHist; ++k)
         if ((rc = dalloc(c, &s->hx[k], 3 * (size_t)N)) || (rc = dalloc(c, &s->hr[k], 3 * (size_t)N))) return rc;
     if (cudaMallocHost(&s->hnorm, sizeof(NormSums)) != cudaSuccess ||
@@ -743,7 +1001,7 @@ int implicit_set_particles(upic_ctx* c, long np, const double* x, const double* 
             !std::isfinite(vp[2]))
             return fail(c, UPIC_ERR_NONFINITE, "non-finite particle position or velocity");
         // gamma_from_v (:623)
-        if ((vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]) / (c->cfg.kappa * c->cfg.kappa) >= 1.0)
+        if (!s.picard && (vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]) / (c->cfg.kappa * c->cfg.kappa) >= 1.0)
             return fail(c, UPIC_ERR_SUPERLUMINAL, "relativistic initial velocity must satisfy |v| < kappa");
         if (!(m[p] > 0.0)) return fail(c, UPIC_ERR_ARGUMENT, "particle masses must be positive");
     }
@@ -777,8 +1035,15 @@ int implicit_set_particles(upic_ctx* c, long np, const double* x, const double* 
         }
         if ((rc = iota(c, d.id, np))) return rc;
     }
-    // fixed-point bound of the orbit-averaged current: |v| < kappa
-    const double bJ = qabs * c->cfg.kappa / s.dV;
+    // fixed-point bound of the orbit-averaged current: |v| < kappa; for the
+    // non-relativistic method 16 times the larger of the initial speeds and c
+    double bJ = qabs * c->cfg.kappa / s.dV;
+    if (s.picard) {
+        double vmax = c->cfg.c;
+        for (long p = 0; p < 3 * np; ++p) vmax = std::max(vmax, std::fabs(v[p]));
+        bJ = qabs * 16.0 * vmax / s.dV;
+        s.vb_limit = 16.0 * vmax;
+    }
     s.scaleJ[0] = s.scaleJ[1] = s.scaleJ[2] = fixed_scale(bJ);
     s.scaleJ[3] = fixed_scale(qabs / s.dV);
     s.ready = false;
@@ -840,10 +1105,18 @@ int implicit_init_fields(upic_ctx* c, double* diag_row) {
     UPIC_CUDA(c, fft2d_batched(c->plan, s.spec + 2 * (size_t)N, 1, 0, c->st, rho));
     UPIC_CUDA(c, launch_kspace_mask(s.spec + 2 * (size_t)N, 1, N, cf.nyquist_projection ? s.excl : nullptr, 1,
                                     c->st));
-    UPIC_CUDA(c, launch_poisson_kspace(N, c->d_k2, s.spec + 2 * (size_t)N, 1.0 / cf.sigma1, s.spec, c->st));
+    UPIC_CUDA(c, launch_poisson_kspace(N, c->d_k2, s.spec + 2 * (size_t)N, s.picard ? cf.eps0 : 1.0 / cf.sigma1,
+                                       s.spec, c->st));
     UPIC_CUDA(c, launch_kspace_mask(s.spec, 1, N, cf.nyquist_projection ? s.excl : nullptr, 1, c->st));
     // P = m gamma v (A = 0); v_prev from one backward Lorentz step; vbar = v
-    if (s.np > 0) {
+    if (s.np > 0 && s.picard) {
+        // P = m v, v_prev = v - dt (q/m) E (ec_pic_serial_demo.cpp:1200-1210)
+        UPIC_CUDA(c, launch_diag_spectra(N, c->d_kx, c->d_ky, s.spec, s.dspec, c->st));
+        UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 3, 1, c->st, nullptr, 1, s.dreal));
+        UPIC_CUDA(c, launch_picard_startup(s.order, c->nx, c->ny, cf.Lx, cf.Ly, s.dreal, s.np, p.x, p.y, p.vx, p.vy,
+                                           p.vz, s.uniform ? nullptr : p.q, s.q0, s.uniform ? nullptr : p.m, s.m0,
+                                           cf.dt, p.Px, p.Py, p.Pz, p.wx, p.wy, p.wz, c->st));
+    } else if (s.np > 0) {
         UPIC_CUDA(c, launch_momentum_from_v(s.np, p.vx, p.vy, p.vz, s.uniform ? nullptr : p.m, s.m0, cf.kappa,
                                             p.Px, p.Py, p.Pz, c->st));
         UPIC_CUDA(c, launch_diag_spectra(N, c->d_kx, c->d_ky, s.spec, s.dspec, c->st));
@@ -909,6 +1182,39 @@ int step_diagnostics(upic_ctx* c, ImplicitState& s, double W0, double K0, double
             (rc = dalloc(c, &s.sd_counts, 4)))
             return rc;
     }
+    const double* Jgrid = s.J;
+    if (s.picard && s.np > 0) {
+        // Project1 (compute_step_diagnostics, ec_pic_serial_demo.cpp:1384):
+        // vbar = (v^{n+1} + v^n) / 2 and the grid work of its re-deposited
+        // orbit current
+        const ParticleSoA& v1 = s.P[s.cur];
+        const ParticleSoA& v0 = s.P[1 - s.cur];
+        UPIC_CUDA(c, launch_half_sum((int)s.np, v1.vx, v0.vx, s.bx[s.cur], c->st));
+        UPIC_CUDA(c, launch_half_sum((int)s.np, v1.vy, v0.vy, s.by[s.cur], c->st));
+        UPIC_CUDA(c, launch_half_sum((int)s.np, v1.vz, v0.vz, s.bz[s.cur], c->st));
+        UPIC_CUDA(c, cudaMemsetAsync(s.acc, 0, sizeof(unsigned long long) * 6 * (size_t)N, c->st));
+        UPIC_CUDA(c, cudaMemsetAsync(s.dstats, 0, sizeof(MapStats), c->st));
+        ImplicitMapArgs a{};
+        a.x = v0.x; a.y = v0.y; a.vx = v0.vx; a.vy = v0.vy; a.vz = v0.vz;
+        a.q = v0.q; a.q0 = s.q0; a.id = v0.id;
+        a.gx = v1.vx; a.gy = v1.vy; a.gz = v1.vz;
+        a.vb_limit = INFINITY;
+        a.np = s.np;
+        a.Lx = cf.Lx; a.Ly = cf.Ly; a.inv_dx = 1.0 / s.dx; a.inv_dy = 1.0 / s.dy; a.inv_dV = 1.0 / s.dV;
+        a.dt = cf.dt; a.kappa = cf.kappa;
+        a.split = cf.split_orbit_at_knots;
+        a.chunks = s.sw.chunks;
+        a.nchunks = s.sw.nchunks;
+        a.acc = s.acc;
+        for (int d = 0; d < 3; ++d) a.scale[d] = s.scaleJ[d];
+        a.stats = s.dstats;
+        a.qtab = s.qtab;
+        a.nq = s.nq;
+        a.mnq = s.mnq;
+        UPIC_CUDA(c, launch_implicit_map(s.order, s.uniform, a.split != 0, s.tg, a, s.grid, c->st, true));
+        UPIC_CUDA(c, launch_convert_acc(s.acc, N, s.scaleJ, s.trial, nullptr, 0.0, 1, c->st));
+        Jgrid = s.trial;
+    }
     UPIC_CUDA(c, launch_step_diag_spectra(N, c->d_kx, c->d_ky, s.spec_out, s.spec, s.sd_spec, c->st));
     UPIC_CUDA(c, fft2d_batched(c->plan, s.sd_spec, 12, 1, c->st, nullptr, 2, s.sd_rec, 12, 0));
     UPIC_CUDA(c, cudaMemsetAsync(s.sd_counts, 0, sizeof(unsigned long long) * 4, c->st));
@@ -936,7 +1242,7 @@ int step_diagnostics(upic_ctx* c, ImplicitState& s, double W0, double K0, double
     a.partials = s.partials;
     a.counts = s.sd_counts;
     UPIC_CUDA(c, launch_step_diag(s.order, a, kNormGrid, s.ddots, c->st));
-    UPIC_CUDA(c, launch_grid_work(N, s.J, s.sd_rec, s.partials + 16 * kNormGrid, kNormGrid, s.ddots + 14, c->st));
+    UPIC_CUDA(c, launch_grid_work(N, Jgrid, s.sd_rec, s.partials + 16 * kNormGrid, kNormGrid, s.ddots + 14, c->st));
     unsigned long long cnt[4];
     UPIC_CUDA(c, cudaMemcpyAsync(s.hdots, s.ddots, sizeof(double) * 16, cudaMemcpyDeviceToHost, c->st));
     UPIC_CUDA(c, cudaMemcpyAsync(cnt, s.sd_counts, sizeof(cnt), cudaMemcpyDeviceToHost, c->st));
@@ -1100,7 +1406,8 @@ extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double*
         }
         const double W0 = s.energy_W, K0 = s.energy_K;
         s.energy_valid = false;
-        rc = implicit_one_step(c, s, info ? info + (size_t)k * UPIC_INFO_COUNT : nullptr);
+        double* ik = info ? info + (size_t)k * UPIC_INFO_COUNT : nullptr;
+        rc = s.picard ? picard_one_step(c, s, ik) : implicit_one_step(c, s, ik);
         if (rc) return rc;
         c->steps = s.steps;
         if (diag || step_diag) {

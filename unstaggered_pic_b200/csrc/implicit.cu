@@ -263,23 +263,17 @@ struct LocalOut {
     double x1, y1;
 };
 
-// One evaluation of the particle map at guess vbar (evaluate_local_particle_substep
-// :4843 with h = dt, theta0 = 0, theta1 = 1).  b/nb: breakpoints of the orbit.
+// Orbit averages along x0 + s (dxx, dxy), s in [0, 1] split at the
+// breakpoints b[0..nb): gp = <grad phi_mid> and D[c][d] = <d A_c / d x_d>
+// with A = (1-s) A^n + s A^{n+1} (path_average_gather_vector_one :2738,
+// orbit_discrete_gradient_A_interval :2958), the deck's Gauss rule point by
+// point.
 template <int ORDER>
-UPIC_D bool evaluate(const Geo& g, const double* __restrict__ rec, double dt, double kappa, int split,
-                     const LocalIn& in, const double* guess, LocalOut& o, double* b, int& nb) {
-    const double dxx = dt * guess[0], dxy = dt * guess[1];
-    o.x1 = wrap1(in.x0 + dxx, g.Lx);
-    o.y1 = wrap1(in.y0 + dxy, g.Ly);
-    double A1p[3];
-    gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, A1p);
-    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
-                           0.5 * (in.A0p[2] + A1p[2])};
-    nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
-    if (nb < 0) return false;
-    // orbit averages: grad phi_mid along the path and D_A (:2738, :2958)
+UPIC_D void orbit_integrals_points(const Geo& g, const double* __restrict__ rec, double x0, double y0, double dxx,
+                                   double dxy, const double* b, int nb, double gp[2], double D[3][2]) {
     double gp0 = 0.0, gp1 = 0.0;
-    double D[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) D[c][0] = D[c][1] = 0.0;
     const int nq = g.nq;
     for (int k = 0; k + 1 < nb; ++k) {
         const double sa = b[k], len = b[k + 1] - b[k];
@@ -287,8 +281,8 @@ UPIC_D bool evaluate(const Geo& g, const double* __restrict__ rec, double dt, do
         for (int iq = 0; iq < nq; ++iq) {
             const double s = sa + len * g.qs[iq];
             const double wq = len * g.qw[iq];
-            const double xs = wrap1(in.x0 + s * dxx, g.Lx);
-            const double ys = wrap1(in.y0 + s * dxy, g.Ly);
+            const double xs = wrap1(x0 + s * dxx, g.Lx);
+            const double ys = wrap1(y0 + s * dxy, g.Ly);
             Stencil<ORDER> sx, sy;
             stencil_xy<ORDER>(g, xs, ys, sx, sy);
             double g0 = 0.0, g1 = 0.0;
@@ -326,6 +320,27 @@ UPIC_D bool evaluate(const Geo& g, const double* __restrict__ rec, double dt, do
             }
         }
     }
+    gp[0] = gp0;
+    gp[1] = gp1;
+}
+
+// One evaluation of the particle map at guess vbar (evaluate_local_particle_substep
+// :4843 with h = dt, theta0 = 0, theta1 = 1).  b/nb: breakpoints of the orbit.
+template <int ORDER>
+UPIC_D bool evaluate(const Geo& g, const double* __restrict__ rec, double dt, double kappa, int split,
+                     const LocalIn& in, const double* guess, LocalOut& o, double* b, int& nb) {
+    const double dxx = dt * guess[0], dxy = dt * guess[1];
+    o.x1 = wrap1(in.x0 + dxx, g.Lx);
+    o.y1 = wrap1(in.y0 + dxy, g.Ly);
+    double A1p[3];
+    gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, A1p);
+    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
+                           0.5 * (in.A0p[2] + A1p[2])};
+    nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
+    if (nb < 0) return false;
+    double gpv[2], D[3][2];
+    orbit_integrals_points<ORDER>(g, rec, in.x0, in.y0, dxx, dxy, b, nb, gpv, D);
+    const double gp0 = gpv[0], gp1 = gpv[1];
     // D vbar and the skew part K = D^T - D as B_eff (:4585-4620); the z
     // columns of D vanish in 2D.
     const double Dv[3] = {D[0][0] * guess[0] + D[0][1] * guess[1], D[1][0] * guess[0] + D[1][1] * guess[1],
@@ -416,27 +431,20 @@ UPIC_D void segment_moments(const Geo& g, double x0, double y0, double dxx, doub
     }
 }
 
-// evaluate() for ORDER <= 2 with knot splitting on, through segment moments.
+// orbit_integrals_points through segment moments (ORDER <= 2, knot splitting
+// on, so that each segment has one stencil).
 template <int ORDER>
-UPIC_D bool evaluate_moments(const Geo& g, const double* __restrict__ rec, double dt, double kappa, int split,
-                             const LocalIn& in, const double* guess, LocalOut& o, double* b, int& nb) {
+UPIC_D void orbit_integrals_moments(const Geo& g, const double* __restrict__ rec, double x0, double y0, double dxx,
+                                    double dxy, const double* b, int nb, double gp[2], double D[3][2]) {
     constexpr int S = ORDER + 1;
-    const double dxx = dt * guess[0], dxy = dt * guess[1];
-    o.x1 = wrap1(in.x0 + dxx, g.Lx);
-    o.y1 = wrap1(in.y0 + dxy, g.Ly);
-    double A1p[3];
-    gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, A1p);
-    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
-                           0.5 * (in.A0p[2] + A1p[2])};
-    nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
-    if (nb < 0) return false;
     double gp0 = 0.0, gp1 = 0.0;
-    double D[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) D[c][0] = D[c][1] = 0.0;
     for (int k = 0; k + 1 < nb; ++k) {
         const double len = b[k + 1] - b[k];
         if (len <= 0.0) continue;
         SegMoments<ORDER> M;
-        segment_moments<ORDER, true>(g, in.x0, in.y0, dxx, dxy, b[k], len, M);
+        segment_moments<ORDER, true>(g, x0, y0, dxx, dxy, b[k], len, M);
 #pragma unroll
         for (int a = 0; a < S; ++a) {
             const int gx = wrap_index(M.ilx + a, g.nx);
@@ -459,6 +467,26 @@ UPIC_D bool evaluate_moments(const Geo& g, const double* __restrict__ rec, doubl
             }
         }
     }
+    gp[0] = gp0;
+    gp[1] = gp1;
+}
+
+// evaluate() for ORDER <= 2 with knot splitting on, through segment moments.
+template <int ORDER>
+UPIC_D bool evaluate_moments(const Geo& g, const double* __restrict__ rec, double dt, double kappa, int split,
+                             const LocalIn& in, const double* guess, LocalOut& o, double* b, int& nb) {
+    const double dxx = dt * guess[0], dxy = dt * guess[1];
+    o.x1 = wrap1(in.x0 + dxx, g.Lx);
+    o.y1 = wrap1(in.y0 + dxy, g.Ly);
+    double A1p[3];
+    gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, A1p);
+    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
+                           0.5 * (in.A0p[2] + A1p[2])};
+    nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
+    if (nb < 0) return false;
+    double gpv[2], D[3][2];
+    orbit_integrals_moments<ORDER>(g, rec, in.x0, in.y0, dxx, dxy, b, nb, gpv, D);
+    const double gp0 = gpv[0], gp1 = gpv[1];
     const double Dv[3] = {D[0][0] * guess[0] + D[0][1] * guess[1], D[1][0] * guess[0] + D[1][1] * guess[1],
                           D[2][0] * guess[0] + D[2][1] * guess[1]};
     const double B[3] = {D[2][1], -D[2][0], D[1][0] - D[0][1]};
@@ -493,8 +521,12 @@ UPIC_D int window_coord(int s, int origin, int n, int w, int span) {
 }
 
 // MOM: segment moments (ORDER <= 2 with knot splitting on); otherwise the
-// orbit integrals are gathered point by point.
-template <int ORDER, bool UNIFORM, bool MOM>
+// orbit integrals are gathered point by point.  PICARD: the deposit of the
+// non-relativistic Picard map (evaluate_picard_map_orbit,
+// Project1/ec_pic_serial_demo.cpp:1455-1474): the orbit velocity is
+// vbar = (v_guess + v^n) / 2 with no local solve, followed by the same
+// orbit-averaged deposit.
+template <int ORDER, bool UNIFORM, bool MOM, bool PICARD>
 __global__ void __launch_bounds__(kMapThreads, kMapMinBlocks)
 implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
     constexpr int S = ORDER + 1;
@@ -577,7 +609,28 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
             double bk[kMaxBreaks];
             int nb = 0;
             LocalIn in;
-            if (active) {
+            if (PICARD && active) {
+                in.x0 = a.x[p];
+                in.y0 = a.y[p];
+                in.q = UNIFORM ? a.q0 : a.q[p];
+                vb[0] = 0.5 * (a.gx[p] + a.vx[p]);
+                vb[1] = 0.5 * (a.gy[p] + a.vy[p]);
+                vb[2] = 0.5 * (a.gz[p] + a.vz[p]);
+                int reason = kLocalOk;
+                if (!(fabs(vb[0]) <= a.vb_limit && fabs(vb[1]) <= a.vb_limit && fabs(vb[2]) <= a.vb_limit)) {
+                    reason = kLocalNonfiniteIterate;
+                } else {
+                    nb = breakpoints<ORDER>(g, in.x0, in.y0, a.dt * vb[0], a.dt * vb[1], a.split, bk);
+                    if (nb < 0) reason = kLocalTooManyCrossings;
+                }
+                ok = reason == kLocalOk;
+                if (!ok) {
+                    nb = 0;
+                    ++nfail;
+                    const unsigned long long key = ((unsigned long long)(unsigned)a.id[p] << 8) | (unsigned)reason;
+                    first_fail = key < first_fail ? key : first_fail;
+                }
+            } else if (active) {
                 in.x0 = a.x[p];
                 in.y0 = a.y[p];
                 in.P0[0] = a.Px[p];
@@ -1308,6 +1361,16 @@ __global__ void nonfinite_kernel(int n, const double* v, int* flag) {
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
+__global__ void extrapolate_kernel(int n, const double* v, const double* w, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = 2.0 * v[i] - w[i];
+}
+
+__global__ void half_sum_kernel(int n, const double* a, const double* b, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = 0.5 * (a[i] + b[i]);
+}
+
 __global__ void lerp_kernel(int n, const double* a, const double* b, double s, double* out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         out[i] = a[i] + s * (b[i] - a[i]);
@@ -1501,6 +1564,166 @@ __global__ void __launch_bounds__(kRed) grid_work_kernel(int N, const double* J,
     }
 }
 
+// ---- non-relativistic Picard push (evaluate_picard_map_orbit,
+// Project1/ec_pic_serial_demo.cpp:1455-1506) ---------------------------------
+// Per particle: vbar = (v_guess + v^n)/2, x_end = wrap(x + dt vbar), orbit
+// averages of grad phi_mid and D_A (A time-interpolated), A^{n+1} at x_end,
+// P_end = P + dt (-q <grad phi> + q D_A^T vbar), v_next = (P_end - q A)/m.
+// Writes the trial state (sorted order) and per-CTA double-double partials of
+// |v_next - v_guess|^2, |v_next|^2, |v_guess|^2 in the residual-norm layout.
+template <int ORDER, bool UNIFORM, bool MOM>
+__global__ void __launch_bounds__(kRed) picard_push_kernel(PicardPushArgs a) {
+    Geo g{a.nx, a.ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    g.qs = a.qtab;
+    g.qw = a.qtab + kMaxQuad;
+    g.ms = a.qtab + 2 * kMaxQuad;
+    g.mw = a.qtab + 3 * kMaxQuad;
+    g.nq = a.nq;
+    g.mnq = a.mnq;
+    DD d2{0, 0}, n2{0, 0}, g2{0, 0};
+    int nfail = 0;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < a.np; p += (long)gridDim.x * blockDim.x) {
+        const double x0 = a.x[p], y0 = a.y[p];
+        const double vg[3] = {a.gx[p], a.gy[p], a.gz[p]};
+        const double vb[3] = {0.5 * (vg[0] + a.vx[p]), 0.5 * (vg[1] + a.vy[p]), 0.5 * (vg[2] + a.vz[p])};
+        const double q = UNIFORM ? a.q0 : a.q[p];
+        const double m = UNIFORM ? a.m0 : a.m[p];
+        const double dxx = a.dt * vb[0], dxy = a.dt * vb[1];
+        const double x1 = wrap1(x0 + dxx, g.Lx), y1 = wrap1(y0 + dxy, g.Ly);
+        double b[kMaxBreaks];
+        const int nb = breakpoints<ORDER>(g, x0, y0, dxx, dxy, a.split, b);
+        double gp[2] = {0.0, 0.0}, D[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+        if (nb < 0) {
+            ++nfail;
+        } else if constexpr (MOM) {
+            orbit_integrals_moments<ORDER>(g, a.rec, x0, y0, dxx, dxy, b, nb, gp, D);
+        } else {
+            orbit_integrals_points<ORDER>(g, a.rec, x0, y0, dxx, dxy, b, nb, gp, D);
+        }
+        double A1p[3];
+        gather_rec3<ORDER>(g, a.rec, kIRecAe, x1, y1, A1p);
+        // D_A^T vbar (the z derivatives vanish in 2D)
+        const double DATv[3] = {D[0][0] * vb[0] + D[1][0] * vb[1] + D[2][0] * vb[2],
+                                D[0][1] * vb[0] + D[1][1] * vb[1] + D[2][1] * vb[2], 0.0};
+        const double gpb[3] = {gp[0], gp[1], 0.0};
+        const double P0[3] = {a.Px[p], a.Py[p], a.Pz[p]};
+        double Pe[3], vn[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double f = (-q) * gpb[c] + q * DATv[c];
+            Pe[c] = P0[c] + a.dt * f;
+            vn[c] = (Pe[c] - q * A1p[c]) / m;
+            const double dv = vn[c] - vg[c];
+            d2 = dd_add_dd(d2, dd_sq(dv));
+            n2 = dd_add_dd(n2, dd_sq(vn[c]));
+            g2 = dd_add_dd(g2, dd_sq(vg[c]));
+        }
+        a.ox[p] = x1;
+        a.oy[p] = y1;
+        a.oPx[p] = Pe[0];
+        a.oPy[p] = Pe[1];
+        a.oPz[p] = Pe[2];
+        a.ovx[p] = vn[0];
+        a.ovy[p] = vn[1];
+        a.ovz[p] = vn[2];
+    }
+    if (nfail) atomicAdd(a.err, nfail);
+    d2 = warp_sum_dd(d2);
+    n2 = warp_sum_dd(n2);
+    g2 = warp_sum_dd(g2);
+    __shared__ double red[kRed / kWarp][6];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[w][0] = d2.hi; red[w][1] = d2.lo; red[w][2] = n2.hi; red[w][3] = n2.lo;
+        red[w][4] = g2.hi; red[w][5] = g2.lo;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD A{0, 0}, B{0, 0}, C{0, 0};
+        for (int k = 0; k < kRed / kWarp; ++k) {
+            A = dd_add_dd(A, DD{red[k][0], red[k][1]});
+            B = dd_add_dd(B, DD{red[k][2], red[k][3]});
+            C = dd_add_dd(C, DD{red[k][4], red[k][5]});
+        }
+        double* o = a.partials + (size_t)blockIdx.x * 8;
+        o[0] = A.hi; o[1] = A.lo; o[2] = B.hi; o[3] = B.lo; o[4] = C.hi; o[5] = C.lo; o[6] = 0.0; o[7] = 0.0;
+    }
+}
+
+// v_prev = v - dt (q/m) E(x) and P = m v: the Taylor start-up of
+// Project1's initializers (ec_pic_serial_demo.cpp:1200-1210).
+template <int ORDER>
+__global__ void picard_startup_kernel(int nx, int ny, double Lx, double Ly, const double* E3, long np,
+                                      const double* x, const double* y, const double* vx, const double* vy,
+                                      const double* vz, const double* qa, double q0, const double* ma, double m0,
+                                      double dt, double* Px, double* Py, double* Pz, double* wx, double* wy,
+                                      double* wz) {
+    const Geo g{nx, ny, Lx, Ly, nx / Lx, ny / Ly};
+    const int N = nx * ny;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
+        Stencil<ORDER> sx, sy;
+        stencil_xy<ORDER>(g, x[p], y[p], sx, sy);
+        double E[3] = {0.0, 0.0, 0.0};
+        for (int ia = 0; ia <= ORDER; ++ia) {
+            const int gx = wrap_index(sx.il + ia, nx);
+            for (int ib = 0; ib <= ORDER; ++ib) {
+                const int node = gx * ny + wrap_index(sy.il + ib, ny);
+                const double w = sx.w[ia] * sy.w[ib];
+                for (int c = 0; c < 3; ++c) E[c] = fma(E3[(size_t)c * N + node], w, E[c]);
+            }
+        }
+        const double q = qa ? qa[p] : q0, m = ma ? ma[p] : m0;
+        const double v[3] = {vx[p], vy[p], vz[p]};
+        const double qm = q / m;
+        Px[p] = m * v[0];
+        Py[p] = m * v[1];
+        Pz[p] = m * v[2];
+        wx[p] = v[0] - dt * (qm * E[0]);
+        wy[p] = v[1] - dt * (qm * E[1]);
+        wz[p] = v[2] - dt * (qm * E[2]);
+    }
+}
+
+// Knot-crossing statistics of the orbits x + dt vbar (compute_path_stats,
+// ec_pic_serial_demo.cpp:835; PathStats of Project3): vbar from (bx, by)
+// or, with vbar null arrays, (v1 + v0) / 2.  counts: total segments,
+// crossings, crossing particles, max segments.
+template <int ORDER>
+__global__ void path_stats_kernel(PathStatsArgs a) {
+    const Geo g{a.nx, a.ny, a.Lx, a.Ly, a.nx / a.Lx, a.ny / a.Ly};
+    unsigned long long segs = 0, cross = 0, cpart = 0;
+    int maxseg = 1;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < a.np; p += (long)gridDim.x * blockDim.x) {
+        double vbx, vby;
+        if (a.bx) {
+            vbx = a.bx[p];
+            vby = a.by[p];
+        } else {
+            vbx = 0.5 * (a.v1x[p] + a.v0x[p]);
+            vby = 0.5 * (a.v1y[p] + a.v0y[p]);
+        }
+        double b[kMaxBreaks];
+        const int nb = breakpoints<ORDER>(g, a.x[p], a.y[p], a.dt * vbx, a.dt * vby, a.split, b);
+        const int nseg = nb - 1 > 1 ? nb - 1 : 1;
+        segs += (unsigned long long)nseg;
+        cross += (unsigned long long)(nseg - 1);
+        cpart += nseg > 1 ? 1ull : 0ull;
+        maxseg = max(maxseg, nseg);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        segs += __shfl_xor_sync(0xffffffffu, segs, o);
+        cross += __shfl_xor_sync(0xffffffffu, cross, o);
+        cpart += __shfl_xor_sync(0xffffffffu, cpart, o);
+        maxseg = max(maxseg, __shfl_xor_sync(0xffffffffu, maxseg, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&a.counts[0], segs);
+        atomicAdd(&a.counts[1], cross);
+        atomicAdd(&a.counts[2], cpart);
+        atomicMax(&a.counts[3], (unsigned long long)maxseg);
+    }
+}
+
 // ---- diagnostics ----------------------------------------------------------------
 constexpr int kDiagSums = 9;
 
@@ -1580,17 +1803,23 @@ __global__ void implicit_diag_final_kernel(const double* partials, int grid, dou
     }
 }
 
+// Relativistic m kappa^2 (gamma - 1) (compute_kinetic_energy, Project3 :3457)
+// or, with nonrel, m v^2 / 2 (Project1 :1031).
 __global__ void __launch_bounds__(kRed)
 kinetic_kernel(long np, const double* vx, const double* vy, const double* vz, const double* m, double m0,
-               double kappa, double* partials) {
+               double kappa, double* partials, int nonrel) {
     DD s{0, 0};
     const double k2 = kappa * kappa;
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
         const double v[3] = {vx[p], vy[p], vz[p]};
-        const double beta2 = dot3(v, v) / k2;
-        const double gam = 1.0 / sqrt(fmax(1.0e-300, 1.0 - beta2));
         const double mm = m ? m[p] : m0;
-        s = dd_add(s, mm * kappa * kappa * (gam - 1.0));
+        if (nonrel) {
+            s = dd_add(s, 0.5 * mm * dot3(v, v));
+        } else {
+            const double beta2 = dot3(v, v) / k2;
+            const double gam = 1.0 / sqrt(fmax(1.0e-300, 1.0 - beta2));
+            s = dd_add(s, mm * kappa * kappa * (gam - 1.0));
+        }
     }
     s = warp_sum_dd(s);
     __shared__ double red[kRed / kWarp][2];
@@ -1625,10 +1854,12 @@ int gsize(long n, int threads = 256) {
 
 using MapKernel = void (*)(ImplicitMapArgs, TileGeom);
 
-// The map kernel instance of (order, uniform q/m, knot splitting).
-MapKernel map_kernel(int order, bool uniform, bool split) {
+// The map kernel instance of (order, uniform q/m, knot splitting, Picard
+// deposit).
+template <bool PICARD>
+MapKernel map_kernel_of(int order, bool uniform, bool split) {
     const bool mom = split && order <= 2;
-#define UPIC_K(O, U, M) &implicit_map_kernel<O, U, M>
+#define UPIC_K(O, U, M) &implicit_map_kernel<O, U, M, PICARD>
     switch (order) {
         case 1:
             return mom ? (uniform ? UPIC_K(1, true, true) : UPIC_K(1, false, true))
@@ -1643,6 +1874,10 @@ MapKernel map_kernel(int order, bool uniform, bool split) {
     return nullptr;
 }
 
+MapKernel map_kernel(int order, bool uniform, bool split, bool picard) {
+    return picard ? map_kernel_of<true>(order, uniform, split) : map_kernel_of<false>(order, uniform, split);
+}
+
 }  // namespace
 
 int implicit_map_smem_bytes(const TileGeom& tg, int order) {
@@ -1651,10 +1886,10 @@ int implicit_map_smem_bytes(const TileGeom& tg, int order) {
     return 2 * 3 * tg.wx * tg.wy * 8 + kMapWarps * (32 * RW * 8 + 32 * 4) + 4 * kMaxQuad * 8;
 }
 
-cudaError_t implicit_configure_smem(const TileGeom& tg, int order, bool split) {
+cudaError_t implicit_configure_smem(const TileGeom& tg, int order, bool split, bool picard) {
     const int b = implicit_map_smem_bytes(tg, order);
     for (int u = 0; u < 2; ++u) {
-        MapKernel k = map_kernel(order, u != 0, split);
+        MapKernel k = map_kernel(order, u != 0, split, picard);
         if (!k) return cudaErrorInvalidValue;
         const cudaError_t e =
             cudaFuncSetAttribute(reinterpret_cast<const void*>(k), cudaFuncAttributeMaxDynamicSharedMemorySize, b);
@@ -1663,17 +1898,17 @@ cudaError_t implicit_configure_smem(const TileGeom& tg, int order, bool split) {
     return cudaSuccess;
 }
 
-int implicit_map_occupancy(const TileGeom& tg, int order, bool split) {
+int implicit_map_occupancy(const TileGeom& tg, int order, bool split, bool picard) {
     int n = 0;
-    MapKernel k = map_kernel(order, true, split);
+    MapKernel k = map_kernel(order, true, split, picard);
     if (!k) return 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kMapThreads, implicit_map_smem_bytes(tg, order));
     return n;
 }
 
 cudaError_t launch_implicit_map(int order, bool uniform, bool split, const TileGeom& tg,
-                                const ImplicitMapArgs& a, int grid, cudaStream_t st) {
-    MapKernel k = map_kernel(order, uniform, split);
+                                const ImplicitMapArgs& a, int grid, cudaStream_t st, bool picard) {
+    MapKernel k = map_kernel(order, uniform, split, picard);
     if (!k) return cudaErrorInvalidValue;
     k<<<grid, kMapThreads, implicit_map_smem_bytes(tg, order), st>>>(a, tg);
     count_launches(1);
@@ -1731,6 +1966,62 @@ cudaError_t launch_grid_work(int N, const double* J, const double* rec12, double
     grid_work_kernel<<<grid, kRed, 0, st>>>(N, J, rec12, partials);
     pair_final_kernel<<<1, 32, 0, st>>>(partials, grid, out2);
     count_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_picard_push(int order, bool uniform, bool split, const PicardPushArgs& a, int grid,
+                              NormSums* out, cudaStream_t st) {
+    const bool mom = split && order <= 2;
+#define UPIC_PP(O, U, M) picard_push_kernel<O, U, M><<<grid, kRed, 0, st>>>(a)
+    switch (order) {
+        case 1:
+            if (mom) { if (uniform) UPIC_PP(1, true, true); else UPIC_PP(1, false, true); }
+            else { if (uniform) UPIC_PP(1, true, false); else UPIC_PP(1, false, false); }
+            break;
+        case 2:
+            if (mom) { if (uniform) UPIC_PP(2, true, true); else UPIC_PP(2, false, true); }
+            else { if (uniform) UPIC_PP(2, true, false); else UPIC_PP(2, false, false); }
+            break;
+        case 3: if (uniform) UPIC_PP(3, true, false); else UPIC_PP(3, false, false); break;
+        case 4: if (uniform) UPIC_PP(4, true, false); else UPIC_PP(4, false, false); break;
+        default: return cudaErrorInvalidValue;
+    }
+#undef UPIC_PP
+    residual_final_kernel<<<1, 32, 0, st>>>(a.partials, grid, out);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_picard_startup(int order, int nx, int ny, double Lx, double Ly, const double* E3, long np,
+                                  const double* x, const double* y, const double* vx, const double* vy,
+                                  const double* vz, const double* q, double q0, const double* m, double m0,
+                                  double dt, double* Px, double* Py, double* Pz, double* wx, double* wy, double* wz,
+                                  cudaStream_t st) {
+    const int g = gsize(np);
+#define UPIC_PS(O) picard_startup_kernel<O><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, E3, np, x, y, vx, vy, vz, q, q0, m, \
+                                                               m0, dt, Px, Py, Pz, wx, wy, wz)
+    switch (order) {
+        case 1: UPIC_PS(1); break;
+        case 2: UPIC_PS(2); break;
+        case 3: UPIC_PS(3); break;
+        case 4: UPIC_PS(4); break;
+        default: return cudaErrorInvalidValue;
+    }
+#undef UPIC_PS
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_path_stats(int order, const PathStatsArgs& a, cudaStream_t st) {
+    const int g = gsize(a.np);
+    switch (order) {
+        case 1: path_stats_kernel<1><<<g, 256, 0, st>>>(a); break;
+        case 2: path_stats_kernel<2><<<g, 256, 0, st>>>(a); break;
+        case 3: path_stats_kernel<3><<<g, 256, 0, st>>>(a); break;
+        case 4: path_stats_kernel<4><<<g, 256, 0, st>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -1860,6 +2151,18 @@ cudaError_t launch_nonfinite_flag(int n, const double* v, int* flag, cudaStream_
     return cudaGetLastError();
 }
 
+cudaError_t launch_extrapolate(int n, const double* v, const double* w, double* out, cudaStream_t st) {
+    extrapolate_kernel<<<gsize(n), 256, 0, st>>>(n, v, w, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_half_sum(int n, const double* a, const double* b, double* out, cudaStream_t st) {
+    half_sum_kernel<<<gsize(n), 256, 0, st>>>(n, a, b, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_lerp(int n, const double* a, const double* b, double s, double* out, cudaStream_t st) {
     lerp_kernel<<<gsize(n), 256, 0, st>>>(n, a, b, s, out);
     count_launches(1);
@@ -1880,8 +2183,9 @@ cudaError_t launch_implicit_diag(const ImplicitDiagArgs& a, double* out20, cudaS
 }
 
 cudaError_t launch_kinetic(long np, const double* vx, const double* vy, const double* vz, const double* m,
-                           double m0, double kappa, double* partials, int grid, double* out, cudaStream_t st) {
-    kinetic_kernel<<<grid, kRed, 0, st>>>(np, vx, vy, vz, m, m0, kappa, partials);
+                           double m0, double kappa, double* partials, int grid, double* out, cudaStream_t st,
+                           bool nonrel) {
+    kinetic_kernel<<<grid, kRed, 0, st>>>(np, vx, vy, vz, m, m0, kappa, partials, nonrel ? 1 : 0);
     pair_final_kernel<<<1, 32, 0, st>>>(partials, grid, out);
     count_launches(2);
     return cudaGetLastError();

@@ -69,15 +69,21 @@ struct ImplicitMapArgs {
     // for segment moments)
     const double* qtab;
     int nq, mnq;
+    // Picard deposit (picard = true): guess velocities, orbit vbar = (guess + v) / 2;
+    // a particle with a component of vbar above vb_limit (or not finite) is
+    // counted as a failure, since its deposit could leave the fixed-point range
+    const double *gx, *gy, *gz;
+    double vb_limit;
 };
 
-// split: knot splitting of the orbit (ImplicitMapArgs::split), which selects
-// the kernel instance.
+// split: knot splitting of the orbit (ImplicitMapArgs::split); picard: the
+// non-relativistic Picard deposit instead of the local GM-HC solve.  Both
+// select the kernel instance.
 cudaError_t launch_implicit_map(int order, bool uniform, bool split, const TileGeom& tg,
-                                const ImplicitMapArgs& a, int grid, cudaStream_t st);
+                                const ImplicitMapArgs& a, int grid, cudaStream_t st, bool picard = false);
 int implicit_map_smem_bytes(const TileGeom& tg, int order);
-cudaError_t implicit_configure_smem(const TileGeom& tg, int order, bool split);
-int implicit_map_occupancy(const TileGeom& tg, int order, bool split);
+cudaError_t implicit_configure_smem(const TileGeom& tg, int order, bool split, bool picard = false);
+int implicit_map_occupancy(const TileGeom& tg, int order, bool split, bool picard = false);
 
 // Point deposit of rho (q S / dV, slot 3) and J (q v S / dV, slots 0..2) at
 // the particle positions (deposit_scalar_to_mesh :2117, deposit_current_to_mesh
@@ -194,6 +200,10 @@ cudaError_t launch_anderson_candidate(int N3, const double* const* x, const doub
 // *flag |= 1 when any of v[0..n) is not finite (finite_node_vector :5051);
 // the caller clears *flag.
 cudaError_t launch_nonfinite_flag(int n, const double* v, int* flag, cudaStream_t st);
+// out = 2 v - w (Picard predictor, ec_pic_serial_demo.cpp:1514)
+cudaError_t launch_extrapolate(int n, const double* v, const double* w, double* out, cudaStream_t st);
+// out = (a + b) / 2
+cudaError_t launch_half_sum(int n, const double* a, const double* b, double* out, cudaStream_t st);
 // out = a + s (b - a)
 cudaError_t launch_lerp(int n, const double* a, const double* b, double s, double* out, cudaStream_t st);
 // out = a + s b
@@ -217,10 +227,49 @@ struct ImplicitDiagArgs {
 // sums: [0..1] gauss^2, [2..3] divE^2, [4..5] rho^2, [6..7] gauge^2, [8..9] psi^2,
 // [10..11] divA^2, [12..13] E^2, [14..15] B^2, [16..17] rho; [18] gauss max, [19] gauge max
 cudaError_t launch_implicit_diag(const ImplicitDiagArgs& a, double* out20, cudaStream_t st);
-// kinetic energy and gamma sum over particles (double-double): out[0..1] kinetic
+// kinetic energy over particles (double-double): out[0..1]; relativistic
+// m kappa^2 (gamma - 1), or m v^2 / 2 with nonrel
 cudaError_t launch_kinetic(long np, const double* vx, const double* vy, const double* vz,
                            const double* m, double m0, double kappa, double* partials, int grid,
-                           double* out, cudaStream_t st);
+                           double* out, cudaStream_t st, bool nonrel = false);
+
+// Non-relativistic Picard push (picard_push_kernel, Project1
+// evaluate_picard_map_orbit :1455): trial state and the double-double sums
+// |v_next - v_guess|^2 (r2), |v_next|^2 (map2), |v_guess|^2 (guess2).
+struct PicardPushArgs {
+    const double *x, *y, *Px, *Py, *Pz, *vx, *vy, *vz;   // state n (sorted order)
+    const double *gx, *gy, *gz;                          // velocity guess
+    const double *q, *m;
+    double q0, m0;
+    long np;
+    double *ox, *oy, *oPx, *oPy, *oPz, *ovx, *ovy, *ovz;  // trial end state
+    int nx, ny;
+    double Lx, Ly, inv_dx, inv_dy, dt;
+    const double* rec;
+    int split, nq, mnq;
+    const double* qtab;
+    double* partials;  // grid x 8
+    int* err;          // += particles whose orbit crosses too many knots
+};
+cudaError_t launch_picard_push(int order, bool uniform, bool split, const PicardPushArgs& a, int grid,
+                              NormSums* out, cudaStream_t st);
+// P = m v, v_prev = v - dt (q/m) E(x) (Project1 start-up).
+cudaError_t launch_picard_startup(int order, int nx, int ny, double Lx, double Ly, const double* E3, long np,
+                                  const double* x, const double* y, const double* vx, const double* vy,
+                                  const double* vz, const double* q, double q0, const double* m, double m0,
+                                  double dt, double* Px, double* Py, double* Pz, double* wx, double* wy, double* wz,
+                                  cudaStream_t st);
+struct PathStatsArgs {
+    const double *x, *y;                  // orbit starts
+    const double *bx, *by;                // orbit velocity, or null: (v1 + v0) / 2
+    const double *v1x, *v1y, *v0x, *v0y;
+    long np;
+    int nx, ny;
+    double Lx, Ly, dt;
+    int split;
+    unsigned long long* counts;           // segments, crossings, crossing particles, max segments
+};
+cudaError_t launch_path_stats(int order, const PathStatsArgs& a, cudaStream_t st);
 
 // Lorentz backward start-up of v_prev (initialize_relativistic_history_velocity :3423)
 cudaError_t launch_history_velocity(int order, int nx, int ny, double Lx, double Ly, const double* E3,
