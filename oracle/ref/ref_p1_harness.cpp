@@ -189,4 +189,15 @@ int ref_p1_run(const double* d, const int* ip, long np, double* x, double* v, do
     }
 }
 
+// The reference's own command-line program on a deck file (main :1768):
+// returns its exit code; output files go where the deck's output_prefix says.
+int ref_p1_run_deck(const char* deck) {
+    char prog[] = "ec_pic_serial_demo";
+    std::string d(deck);
+    std::vector<char> arg(d.begin(), d.end());
+    arg.push_back('\0');
+    char* argv[] = {prog, arg.data(), nullptr};
+    return upic_ref_p1_cli_main(2, argv);
+}
+
 }  // extern "C"

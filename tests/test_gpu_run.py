@@ -142,3 +142,163 @@ def test_deck_matches_reference_cli(tmp_path, example, charge):
     ea = [ln for ln in open(str(tmp_path / "gpu_config_echo.txt")) if not ln.startswith("output_prefix")]
     eb = [ln for ln in open(str(tmp_path / "ref_config_echo.txt")) if not ln.startswith("output_prefix")]
     assert ea == eb
+
+
+# ---- Project1 decks: upic_run --nonrel -------------------------------------
+
+def write_p1_deck(path, prefix, **kw):
+    """A Project1 deck: the keys of Project1/examples/input_landau_weak.txt
+    (1D Landau damping, 32x1x1) unless overridden."""
+    keys = dict(test_case="landau_weak", nx=32, ny=1, nz=1, Lx=12.566370614359172, Ly=1.0, Lz=1.0, n_steps=60,
+                dt=0.1, particles_per_cell=32, spline_order=1, orbit_quad_order=12, split_orbit_at_knots="true",
+                c=1.0, eps0=1.0, mu0=1.0, n0=1.0, thermal_velocity=1.0, landau_alpha=0.01, perturbation_mode=1,
+                theory_omega=1.4156618886, theory_gamma=-0.1533594669, picard_tol=1.0e-10, picard_max_iter=24,
+                final_consistency_sweep="true", run_unit_tests="false")
+    keys.update(kw)
+    with open(path, "w") as fh:
+        fh.write("# Project1 deck written by the test\n")
+        for k, v in keys.items():
+            fh.write(f"{k} = {v}\n")
+        fh.write(f"output_prefix = {prefix}\n")
+
+
+def run_nonrel(deck):
+    r = subprocess.run([RUN, "--nonrel", deck], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r
+
+
+P1_DIAG_TEXT = {0}                 # step
+P1_DIAG_ROUNDOFF = {2, 3, 4, 14}   # gauss_rms, gauss_max, gauge_rms, mean_rho
+
+
+def compare_p1_diagnostics(ra, rb, tol, picard_tol):
+    assert len(ra) == len(rb)
+    cols = len(ra[0])
+    for k in range(cols):
+        a = np.array([float(r[k]) for r in ra])
+        b = np.array([float(r[k]) for r in rb])
+        if k in P1_DIAG_TEXT:
+            assert [r[k] for r in ra] == [r[k] for r in rb]
+        elif k == 1:  # time, same arithmetic
+            assert np.array_equal(a, b)
+        elif k in P1_DIAG_ROUNDOFF:
+            assert np.max(np.abs(a - b)) < 1e-12, k
+        elif k == 15:  # Picard iterations
+            assert np.max(np.abs(a - b)) <= 1
+        elif k in (16, 17):  # last Picard errors: both below the tolerance
+            assert np.all(np.isnan(a[:1])) and np.all(np.isnan(b[:1]))
+            assert np.all(a[1:] < picard_tol) and np.all(b[1:] < picard_tol), k
+        elif k == 18:  # crossing particles
+            assert np.max(np.abs(a - b)) <= 1
+        elif k == 20:
+            assert np.array_equal(a, b)
+        else:
+            both_nan = np.isnan(a) & np.isnan(b)
+            assert np.array_equal(np.isnan(a), np.isnan(b)), k
+            scale = max(np.max(np.abs(b[~both_nan])) if (~both_nan).any() else 0.0, 1e-300)
+            d = np.abs(a - b)[~both_nan]
+            assert d.size == 0 or np.max(d) <= tol * scale + 1e-15, (k, np.max(d) / scale)
+
+
+def test_nonrel_usage_and_errors(tmp_path):
+    deck = str(tmp_path / "d.txt")
+    write_p1_deck(deck, str(tmp_path / "x"), nz=16)
+    r = subprocess.run([RUN, "--nonrel", deck], capture_output=True, text=True)
+    assert r.returncode == 1 and "nz = 1" in r.stderr
+    write_p1_deck(deck, str(tmp_path / "x"), nx=12)
+    r = subprocess.run([RUN, "--nonrel", deck], capture_output=True, text=True)
+    assert r.returncode == 1 and "powers of two" in r.stderr
+    write_p1_deck(deck, str(tmp_path / "x"), test_case="bump_on_tail", n_steps=1)
+    r = subprocess.run([RUN, "--nonrel", deck], capture_output=True, text=True)
+    assert r.returncode == 1 and "unknown test_case" in r.stderr
+    write_p1_deck(deck, str(tmp_path / "x"), landau_alpha=1.5, n_steps=1)
+    r = subprocess.run([RUN, "--nonrel", deck], capture_output=True, text=True)
+    assert r.returncode == 1 and "|alpha| < 1" in r.stderr
+
+
+@pytest.mark.skipif(not os.path.exists(ol.REF_P1_SO), reason="oracle/_ref/libref_p1.so not built")
+def test_nonrel_initial_particles_match_reference_cli(tmp_path):
+    """With n_steps = 0 both programs write the start state: the two-stream
+    and Landau initializers give the very same particles (all 17 digits)."""
+    ref = ol.ref_p1()
+    ref.ref_p1_run_deck.argtypes = [ctypes.c_char_p]
+    for case, kw in (("landau_strong", dict(landau_alpha=0.5, nx=16, ny=2)),
+                     ("two_stream", dict(nx=16, ny=8, Lx=6.283185307179586, Ly=6.283185307179586,
+                                         Lz=6.283185307179586, particles_per_cell=3, spline_order=2))):
+        g, r = str(tmp_path / f"g_{case}"), str(tmp_path / f"r_{case}")
+        write_p1_deck(g + ".txt", g, test_case=case, n_steps=0, **kw)
+        write_p1_deck(r + ".txt", r, test_case=case, n_steps=0, **kw)
+        run_nonrel(g + ".txt")
+        assert ref.ref_p1_run_deck((r + ".txt").encode()) == 0
+        assert open(g + "_particle_sample.csv").read() == open(r + "_particle_sample.csv").read(), case
+        assert open(g + "_config_echo.txt").read() == open(r + "_config_echo.txt").read(), case
+        ha, ra = read_csv(g + "_diagnostics.csv")
+        hb, rb = read_csv(r + "_diagnostics.csv")
+        assert ha == hb and len(ra) == 1
+        compare_p1_diagnostics(ra, rb, 1e-12, 1e-10)
+
+
+@pytest.mark.skipif(not os.path.exists(ol.REF_P1_SO), reason="oracle/_ref/libref_p1.so not built")
+@pytest.mark.parametrize("case", ["landau_weak", "two_stream_2d"])
+def test_nonrel_deck_matches_reference_cli(tmp_path, case):
+    """A Project1 deck through upic_run --nonrel and through the reference's
+    own main(): every file, header and column."""
+    kw = {}
+    if case == "two_stream_2d":
+        kw = dict(test_case="two_stream", nx=16, ny=8, Lx=6.283185307179586, Ly=6.283185307179586,
+                  Lz=6.283185307179586, particles_per_cell=4, spline_order=2, orbit_quad_order=16, n_steps=8,
+                  dt=0.025, picard_tol=1e-11, picard_max_iter=16, theory_omega=0.0, theory_gamma=0.0)
+    g, r = str(tmp_path / "gpu"), str(tmp_path / "ref")
+    write_p1_deck(g + ".txt", g, **kw)
+    write_p1_deck(r + ".txt", r, **kw)
+    out = run_nonrel(g + ".txt").stdout
+    assert "Final total energy" in out
+    ref = ol.ref_p1()
+    ref.ref_p1_run_deck.argtypes = [ctypes.c_char_p]
+    assert ref.ref_p1_run_deck((r + ".txt").encode()) == 0
+    ha, ra = read_csv(g + "_diagnostics.csv")
+    hb, rb = read_csv(r + "_diagnostics.csv")
+    assert ha == hb
+    nsteps = len(rb) - 1
+    compare_p1_diagnostics(ra, rb, 2e-10 * nsteps, 1e-10 if case == "landau_weak" else 1e-11)
+    ha, ra = read_csv(g + "_step_diagnostics.csv")
+    hb, rb = read_csv(r + "_step_diagnostics.csv")
+    assert ha == hb and len(ra) == len(rb) == nsteps
+    for k in range(len(ha)):
+        a = np.array([float(x[k]) for x in ra])
+        b = np.array([float(x[k]) for x in rb])
+        name = ha[k]
+        if name in ("step", "time", "max_path_segments"):
+            assert np.array_equal(a, b), name
+        elif name in ("crossing_particles", "total_crossings"):
+            assert np.max(np.abs(a - b)) <= 1, name
+        elif name == "avg_path_segments":
+            assert np.max(np.abs(a - b)) <= 1.5 / 1024, name
+        elif np.max(np.abs(b)) < 1e-10:
+            assert np.max(np.abs(a - b)) < 1e-12, name
+        else:
+            assert np.max(np.abs(a - b)) <= 2e-10 * nsteps * np.abs(b).max() + 1e-12, name
+    ha, ra = read_csv(g + "_particle_sample.csv")
+    hb, rb = read_csv(r + "_particle_sample.csv")
+    assert ha == hb and len(ra) == len(rb)
+    assert [x[0] for x in ra] == [x[0] for x in rb]
+    for k in range(1, len(ha)):
+        a = np.array([float(x[k]) for x in ra])
+        b = np.array([float(x[k]) for x in rb])
+        assert np.max(np.abs(a - b)) <= 1e-9 * max(np.abs(b).max(), 1.0), ha[k]
+    assert open(g + "_config_echo.txt").read() == open(r + "_config_echo.txt").read()
+
+
+def test_nonrel_unit_tests_pass(tmp_path):
+    """run_unit_tests = true: the 2D start-up checks pass, with the
+    reference's messages, on the console and in _unit_tests.txt."""
+    g = str(tmp_path / "u")
+    write_p1_deck(g + ".txt", g, n_steps=2, run_unit_tests="true")
+    out = run_nonrel(g + ".txt").stdout
+    log = open(g + "_unit_tests.txt").read()
+    for line in ("R_A,p chain-rule unit test: abs_rms=", "R_A,p crossing unit test: split_abs_rms=",
+                 "Initial Gauss-law unit test: gauss_rms=", "One-step Gauss-law unit test: gauss_rms=",
+                 "One-step R_A,p unit test: A_chain_abs_rms=", "One-step deposit/gather work residual="):
+        assert line in log and line in out, line
+    assert "FAILED" not in log and "Unit tests passed." in out

@@ -66,9 +66,9 @@ def build(verbose=False, ptxas_info=False):
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
     # upic_run: the deck-driven driver (host C++ over the C ABI)
-    src = os.path.join(CSRC, "upic_run.cpp")
-    if not _newer(RUN, [src, OUT, os.path.join(ROOT, "include", "upic.h")]):
-        cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), src, "-o", RUN,
+    srcs = [os.path.join(CSRC, "upic_run.cpp"), os.path.join(CSRC, "run_nonrel.cpp")]
+    if not _newer(RUN, srcs + [OUT, os.path.join(ROOT, "include", "upic.h")]):
+        cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include")] + srcs + ["-o", RUN,
                "-L", HERE, "-lupic", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))

@@ -877,14 +877,20 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
     return sync(c);
 }
 
+// wrap1 of positions outside [-L/2, L/2); positions inside are kept as
+// given (a second wrap of a wrapped value can move it by an ulp).
 __global__ void wrap_positions_kernel(double* x, double* y, long n, double Lx, double Ly) {
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
-        double a = fmod(x[p] + 0.5 * Lx, Lx);
-        if (a < 0.0) a += Lx;
-        x[p] = a - 0.5 * Lx;
-        double b = fmod(y[p] + 0.5 * Ly, Ly);
-        if (b < 0.0) b += Ly;
-        y[p] = b - 0.5 * Ly;
+        if (!(x[p] >= -0.5 * Lx && x[p] < 0.5 * Lx)) {
+            double a = fmod(x[p] + 0.5 * Lx, Lx);
+            if (a < 0.0) a += Lx;
+            x[p] = a - 0.5 * Lx;
+        }
+        if (!(y[p] >= -0.5 * Ly && y[p] < 0.5 * Ly)) {
+            double b = fmod(y[p] + 0.5 * Ly, Ly);
+            if (b < 0.0) b += Ly;
+            y[p] = b - 0.5 * Ly;
+        }
     }
 }
 

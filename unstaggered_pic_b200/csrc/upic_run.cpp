@@ -5,9 +5,11 @@
 // <output_prefix>_diagnostics.csv, _particle_sample.csv and _config_echo.txt
 // in its formats.
 //
-//     upic_run deck.txt
+//     upic_run deck.txt              Project2 decks (spectral_pic_part3)
+//     upic_run --nonrel deck.txt     Project1 decks (ec_pic_serial_demo), run_nonrel.cpp
 //
-// Exit codes as the reference: 0 ok, 1 error (message on stderr), 2 usage.
+// Exit codes as the reference: 0 ok, 1 error (message on stderr), 2 usage,
+// 3 failed start-up unit tests (Project1 decks).
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -365,12 +367,16 @@ void run(const Deck& d) {
 
 }  // namespace
 
+int run_nonrel(const std::string& path);
+
 int main(int argc, char** argv) {
     try {
-        if (argc != 2) {
-            std::cerr << "usage: " << argv[0] << " input_file.txt\n";
+        const bool nonrel = argc == 3 && std::string(argv[1]) == "--nonrel";
+        if (argc != 2 && !nonrel) {
+            std::cerr << "usage: " << argv[0] << " [--nonrel] input_file.txt\n";
             return 2;
         }
+        if (nonrel) return run_nonrel(argv[2]);
         run(read_deck(argv[1]));
         return 0;
     } catch (const std::exception& ex) {
