@@ -131,6 +131,9 @@ P3_CASES = [
                        n_steps=2), 16, (0.05, 0.05, 0.05), False),
     ("p3_run_two_species", dict(nx=16, ny=8, Lx=2 * np.pi, Ly=np.pi, dt=0.1, order=2, nq=8,
                                 nyquist=True, n_steps=2, Lz=0.5), 16, (0.1, 0.05, 0.02), True),
+    # 1D-2V (ny = nz = 1), cubic splines
+    ("p3_run_1d_o3", dict(nx=64, ny=1, Lx=4 * np.pi, Ly=1.0, dt=0.1, order=3, nq=8, nyquist=True,
+                          n_steps=3), 32, (0.1, 0.05, 0.0), False),
 ]
 
 

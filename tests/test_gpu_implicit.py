@@ -23,7 +23,7 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 TOL_STEP = 2e-10      # relative difference per step, fields and particle state
 TOL_ROUNDOFF = 1e-12  # absolute, residual diagnostics at round-off level
 CASES = ["p3_run_o2_anderson", "p3_run_o3_picard", "p3_run_o1_nosplit", "p3_run_o4",
-         "p3_run_two_species"]
+         "p3_run_two_species", "p3_run_1d_o3"]
 FIELD_ORDER = ["phi", "psi", "rho", "Ax", "Ay", "Az", "Ux", "Uy", "Uz", "Jx", "Jy", "Jz"]
 
 
