@@ -441,14 +441,22 @@ def measure(args, name, steps, warmup, world, rank, dist, dev):
     # ---- end to end through the public API from pinned host buffers
     e2e = None
     if not args.no_e2e:
+        # the step's result is read back into pinned host buffers, as the inputs come from them
+        res = {k: torch.empty((np_total,) if k in ("x", "y") else (np_total, 3), dtype=torch.float64,
+                              pin_memory=True).numpy() for k in ("x", "y", "P", "v", "v_prev")}
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         load()
+        t1 = time.perf_counter()
         sim.init_fields(True)
+        t2 = time.perf_counter()
         advance(sim, w, steps, 1)
-        out = sim.get_particles()
-        t_e2e = allmax(time.perf_counter() - t0)
+        t3 = time.perf_counter()
+        out = sim.get_particles(out=res)
+        t4 = time.perf_counter()
+        t_e2e = allmax(t4 - t0)
+        phases = {"set_particles": t1 - t0, "init_fields": t2 - t1, "steps": t3 - t2, "get_particles": t4 - t3}
         del out
         ncol = len(up.IMPLICIT_DIAG_COLUMNS) + len(up.SOLVE_INFO_COLUMNS) if implicit else len(up.DIAG_COLUMNS)
         h2d = np_total * 13 * 8 / steps
@@ -456,6 +464,7 @@ def measure(args, name, steps, warmup, world, rank, dist, dev):
         api = "upic_step_implicit(K)" if implicit else "upic_step(K, diagnostics every step)"
         e2e = {"value": world * np_total * steps / t_e2e, "unit": METRIC,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "seconds": t_e2e,
+               "phase_seconds": phases,
                "what": f"upic_set_particles + upic_init_fields + {api} with a diagnostics row per "
                        "step + upic_get_particles, host wall clock, max over ranks"}
     sim.close()

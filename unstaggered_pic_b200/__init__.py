@@ -236,10 +236,19 @@ class Simulation:
         self._check(lib().upic_set_particles(self._ctx, n, *[_p(a) for a in arrs]))
         self.np = n
 
-    def get_particles(self):
+    def get_particles(self, out=None):
+        """Particle state in load order.  out: optional dict of preallocated
+        float64 arrays x, y (n,) and P, v, v_prev (n, 3), e.g. views of
+        pinned host memory, filled in place."""
         n = self.np
-        out = {"x": np.empty(n), "y": np.empty(n), "P": np.empty((n, 3)), "v": np.empty((n, 3)),
-               "v_prev": np.empty((n, 3))}
+        if out is None:
+            out = {"x": np.empty(n), "y": np.empty(n), "P": np.empty((n, 3)), "v": np.empty((n, 3)),
+                   "v_prev": np.empty((n, 3))}
+        else:
+            for k, shape in (("x", (n,)), ("y", (n,)), ("P", (n, 3)), ("v", (n, 3)), ("v_prev", (n, 3))):
+                a = out[k]
+                if a.dtype != np.float64 or a.shape != shape or not a.flags.c_contiguous:
+                    raise ValueError(f"out[{k!r}] must be a C-contiguous float64 array of shape {shape}")
         self._check(lib().upic_get_particles(self._ctx, n, _p(out["x"]), _p(out["y"]), _p(out["P"]),
                                              _p(out["v"]), _p(out["v_prev"])))
         return out

@@ -13,7 +13,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "upic_common.cuh"
@@ -246,6 +248,50 @@ int download3(upic_ctx* c, double* host, long n, const double* a, const double* 
     UPIC_CUDA(c, cudaGetLastError());
     UPIC_CUDA(c, cudaMemcpyAsync(host, c->d_tmp3, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
     return 0;
+}
+
+HostScan scan_particles(long np, const double* x, const double* y, const double* v, const double* q,
+                        const double* m) {
+    constexpr int kChunks = 64;
+    HostScan part[kChunks];
+    if (np <= 0) return HostScan{};
+    const double q0 = q[0], m0 = m[0];
+    auto run = [&](int k) {
+        HostScan& h = part[k];
+        const long b = np * k / kChunks, e = np * (k + 1) / kChunks;
+        for (long p = b; p < e; ++p) {
+            if (q[p] != q0 || m[p] != m0) h.uniform = false;
+            if (!(m[p] > 0.0)) h.positive_m = false;
+            h.qabs += std::fabs(q[p]);
+            const double* vp = v + 3 * p;
+            const double s = std::sqrt(vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]);
+            if (!std::isfinite(s) || !std::isfinite(x[p]) || !std::isfinite(y[p])) h.finite = false;
+            h.speed_max = std::max(h.speed_max, s);
+            h.comp_max = std::max(h.comp_max, std::max(std::fabs(vp[0]), std::max(std::fabs(vp[1]), std::fabs(vp[2]))));
+        }
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = np < (1L << 20) ? 1 : (int)std::min<unsigned>(16u, hw ? hw : 1u);
+    if (nt <= 1) {
+        for (int k = 0; k < kChunks; ++k) run(k);
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t)
+            th.emplace_back([&, t] {
+                for (int k = t; k < kChunks; k += nt) run(k);
+            });
+        for (auto& t : th) t.join();
+    }
+    HostScan r;
+    for (int k = 0; k < kChunks; ++k) {
+        r.finite = r.finite && part[k].finite;
+        r.uniform = r.uniform && part[k].uniform;
+        r.positive_m = r.positive_m && part[k].positive_m;
+        r.qabs += part[k].qabs;
+        r.speed_max = std::max(r.speed_max, part[k].speed_max);
+        r.comp_max = std::max(r.comp_max, part[k].comp_max);
+    }
+    return r;
 }
 
 int ensure_tmp3(upic_ctx* c, long n) {
@@ -614,41 +660,47 @@ int upic_set_particles(upic_ctx* c, long np, const double* x, const double* y, c
         }
         return rc;
     }
-    // uniform charge/mass (the reference stores them per particle)
-    bool uniform = true;
-    double qabs = 0.0, vmax = 0.0;
-    for (long p = 0; p < np; ++p) {
-        if (q[p] != q[0] || m[p] != m[0]) uniform = false;
-        qabs += std::fabs(q[p]);
-        const double s = std::sqrt(v[3 * p] * v[3 * p] + v[3 * p + 1] * v[3 * p + 1] + v[3 * p + 2] * v[3 * p + 2]);
-        if (!std::isfinite(s) || !std::isfinite(x[p]) || !std::isfinite(y[p]))
-            return fail(c, UPIC_ERR_NONFINITE, "non-finite particle position or velocity");
-        if (s > vmax) vmax = s;
-    }
     int rc;
-    if (np > c->cap || (!uniform && !c->P[0].q)) {
+    c->fields_ready = false;
+    if (np > c->cap) {
+        const bool had_qm = c->P[0].q != nullptr;
         free_soa(c, c->P[0]);
         free_soa(c, c->P[1]);
         free_sortwork(c, c->sw);
-        const long cap = np > c->cap ? np : c->cap;
-        if ((rc = alloc_soa(c, c->P[0], cap, true, !uniform)) || (rc = alloc_soa(c, c->P[1], cap, true, !uniform)) ||
-            (rc = alloc_sortwork(c, c->sw, cap, c->tg)))
+        if ((rc = alloc_soa(c, c->P[0], np, true, had_qm)) || (rc = alloc_soa(c, c->P[1], np, true, had_qm)) ||
+            (rc = alloc_sortwork(c, c->sw, np, c->tg)))
             return rc;
-        c->cap = cap;
+        c->cap = np;
     }
     if ((rc = ensure_tmp3(c, np))) return rc;
-    c->np = np;
-    c->cur = 0;
-    c->uniform_qm = uniform;
-    c->q0 = np ? q[0] : 0.0;
-    c->m0 = np ? m[0] : 0.0;
     ParticleSoA& s = c->P[0];
+    // the state copies run while the host validates the set
     if (np > 0) {
         UPIC_CUDA(c, cudaMemcpyAsync(s.x, x, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
         UPIC_CUDA(c, cudaMemcpyAsync(s.y, y, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
         if ((rc = upload3(c, P, np, s.Px, s.Py, s.Pz))) return rc;
         if ((rc = upload3(c, v, np, s.vx, s.vy, s.vz))) return rc;
         if ((rc = upload3(c, v_prev, np, s.wx, s.wy, s.wz))) return rc;
+    }
+    // uniform charge/mass (the reference stores them per particle)
+    const HostScan hs = scan_particles(np, x, y, v, q, m);
+    if (!hs.finite) {
+        c->np = 0;  // the context holds no particle set until a valid one is loaded
+        sync(c);
+        return fail(c, UPIC_ERR_NONFINITE, "non-finite particle position or velocity");
+    }
+    const bool uniform = hs.uniform;
+    const double qabs = hs.qabs, vmax = hs.speed_max;
+    if (!uniform && !s.q) {
+        for (int k = 0; k < 2; ++k)
+            if ((rc = dalloc(c, &c->P[k].q, c->cap + 2)) || (rc = dalloc(c, &c->P[k].m, c->cap + 2))) return rc;
+    }
+    c->np = np;
+    c->cur = 0;
+    c->uniform_qm = uniform;
+    c->q0 = np ? q[0] : 0.0;
+    c->m0 = np ? m[0] : 0.0;
+    if (np > 0) {
         if (!uniform) {
             UPIC_CUDA(c, cudaMemcpyAsync(s.q, q, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
             UPIC_CUDA(c, cudaMemcpyAsync(s.m, m, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
@@ -676,10 +728,10 @@ int upic_get_particles(upic_ctx* c, long np, double* x, double* y, double* P, do
     int rc;
     if (x) UPIC_CUDA(c, cudaMemcpyAsync(x, d.x, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
     if (y) UPIC_CUDA(c, cudaMemcpyAsync(y, d.y, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    // the staging buffer is reused in stream order: each join waits for the
+    // previous copy out of it
     if (P && (rc = download3(c, P, np, d.Px, d.Py, d.Pz))) return rc;
-    if (P) { if ((rc = sync(c))) return rc; }
     if (v && (rc = download3(c, v, np, d.vx, d.vy, d.vz))) return rc;
-    if (v) { if ((rc = sync(c))) return rc; }
     if (v_prev && (rc = download3(c, v_prev, np, d.wx, d.wy, d.wz))) return rc;
     return sync(c);
 }

@@ -997,20 +997,14 @@ void implicit_destroy(upic_ctx* c) {
 int implicit_set_particles(upic_ctx* c, long np, const double* x, const double* y, const double* P,
                            const double* v, const double* v_prev, const double* q, const double* m) {
     ImplicitState& s = *c->imp;
-    bool uniform = true;
-    double qabs = 0.0;
-    for (long p = 0; p < np; ++p) {
-        if (q[p] != q[0] || m[p] != m[0]) uniform = false;
-        qabs += std::fabs(q[p]);
-        const double* vp = v + 3 * p;
-        if (!std::isfinite(x[p]) || !std::isfinite(y[p]) || !std::isfinite(vp[0]) || !std::isfinite(vp[1]) ||
-            !std::isfinite(vp[2]))
-            return fail(c, UPIC_ERR_NONFINITE, "non-finite particle position or velocity");
-        // gamma_from_v (:623)
-        if (!s.picard && (vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]) / (c->cfg.kappa * c->cfg.kappa) >= 1.0)
-            return fail(c, UPIC_ERR_SUPERLUMINAL, "relativistic initial velocity must satisfy |v| < kappa");
-        if (!(m[p] > 0.0)) return fail(c, UPIC_ERR_ARGUMENT, "particle masses must be positive");
-    }
+    const HostScan hs = scan_particles(np, x, y, v, q, m);
+    if (!hs.finite) return fail(c, UPIC_ERR_NONFINITE, "non-finite particle position or velocity");
+    // gamma_from_v (:623)
+    if (!s.picard && hs.speed_max >= c->cfg.kappa)
+        return fail(c, UPIC_ERR_SUPERLUMINAL, "relativistic initial velocity must satisfy |v| < kappa");
+    if (!hs.positive_m) return fail(c, UPIC_ERR_ARGUMENT, "particle masses must be positive");
+    const bool uniform = hs.uniform;
+    const double qabs = hs.qabs;
     int rc;
     if (np > s.cap || (!uniform && !s.P[0].q)) {
         free_particles(c, s);
@@ -1045,8 +1039,7 @@ int implicit_set_particles(upic_ctx* c, long np, const double* x, const double* 
     // non-relativistic method 16 times the larger of the initial speeds and c
     double bJ = qabs * c->cfg.kappa / s.dV;
     if (s.picard) {
-        double vmax = c->cfg.c;
-        for (long p = 0; p < 3 * np; ++p) vmax = std::max(vmax, std::fabs(v[p]));
+        const double vmax = std::max(c->cfg.c, hs.comp_max);
         bJ = qabs * 16.0 * vmax / s.dV;
         s.vb_limit = 16.0 * vmax;
     }

@@ -118,6 +118,17 @@ int gridn(long n);
 int upload3(upic_ctx* c, const double* host, long n, double* a, double* b, double* d);
 int download3(upic_ctx* c, double* host, long n, const double* a, const double* b, const double* d);
 int ensure_tmp3(upic_ctx* c, long n);
+// Validation scan of a host particle set (positions x, y; velocities v as
+// xyz triples; q, m): finiteness, uniform q/m, sum |q|, largest speed and
+// largest velocity component, positive masses.  Runs in 64 fixed chunks on
+// up to 16 host threads; partial sums combine in chunk order, so the result
+// does not depend on the thread count.
+struct HostScan {
+    bool finite = true, uniform = true, positive_m = true;
+    double qabs = 0.0, speed_max = 0.0, comp_max = 0.0;
+};
+HostScan scan_particles(long np, const double* x, const double* y, const double* v, const double* q,
+                        const double* m);
 double fixed_scale(double bound);
 TileGeom make_tiles(int nx, int ny, int tile, int guard, int lo, int hi);
 int alloc_soa(upic_ctx* c, ParticleSoA& s, long cap, bool with_state, bool with_qm);
