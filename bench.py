@@ -50,6 +50,10 @@ WORKLOADS = {
     # profiling case: same grid and physics, 16 e-/cell (370 MB of particle state)
     "weibel512_ppc16": dict(nx=512, ny=512, ppc=16, L=2 * np.pi / 0.3, dt=0.05, method="bdf1",
                             charge_update="conserving", uth=(0.02, 0.2, 0.0), seed=2026),
+    # profiling case with the bench workload's cell occupancy pattern (several
+    # warps per cell): 256x256 grid, 64 e-/cell (4,194,304 particles, 370 MB)
+    "weibel256_ppc64": dict(nx=256, ny=256, ppc=64, L=2 * np.pi / 0.3, dt=0.05, method="bdf1",
+                            charge_update="conserving", uth=(0.02, 0.2, 0.0), seed=2026),
     # the same Weibel decks advanced by the implicit orbit-averaged GM-HC-CN step
     "weibel512_implicit": dict(nx=512, ny=512, ppc=256, L=2 * np.pi / 0.3, dt=0.05, method="cn_orbit",
                                charge_update="-", uth=(0.02, 0.2, 0.0), seed=2026),
