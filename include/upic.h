@@ -234,6 +234,18 @@ int upic_get_particles(upic_ctx* ctx, long np, double* x, double* y, double* P, 
  * before upic_init_fields. */
 int upic_set_background(upic_ctx* ctx, const double* rho_bg);
 
+/* Checkpoint / restart -- no counterpart in the reference, which writes CSV
+ * field snapshots only (ec_pic_nyquist_projected.cpp write_field_grid_snapshot
+ * :8160) and cannot resume a run.  upic_save_state writes everything the next
+ * step of the context reads (particles in their current order, field
+ * spectra and histories, deposit accumulators, step counters) to a binary
+ * file; upic_load_state restores it into a context created with the same
+ * configuration (UPIC_ERR_CONFIG otherwise), after which the run continues
+ * bit for bit as the saved one would have.  The file holds device-order
+ * state of this library version; it is not a portable exchange format. */
+int upic_save_state(upic_ctx* ctx, const char* path);
+int upic_load_state(upic_ctx* ctx, const char* path);
+
 /* Start-up fields: rho0 = n0 + deposited electron charge, J0 = deposited
  * current, phi0 from Poisson, A0 = 0, all BDF histories filled with copies
  * (spectral_pic_part3.cpp:1100-1111).  If diag_row is not NULL it receives
@@ -275,6 +287,8 @@ int upic_profile_read(upic_ctx* ctx, double* push_ms, long* push_launches, long*
 
 /* Number of steps taken since upic_init_fields. */
 int upic_step_count(const upic_ctx* ctx, long* steps);
+/* Number of particles the context holds (upic_set_particles or a restored state). */
+int upic_particle_count(const upic_ctx* ctx, long* np);
 
 /* Fields of the current time level (phi, A, rho, J; implicit method also
  * psi = d phi/dt and U = dA/dt), nx*ny doubles. */

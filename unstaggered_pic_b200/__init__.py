@@ -259,6 +259,18 @@ class Simulation:
         arr = None if rho_bg is None else _f64(rho_bg).ravel()
         self._check(lib().upic_set_background(self._ctx, _p(arr)))
 
+    def save_state(self, path):
+        """Checkpoint everything the next step reads to a binary file."""
+        self._check(lib().upic_save_state(self._ctx, str(path).encode()))
+
+    def load_state(self, path):
+        """Restore a checkpoint written by a context of the same configuration;
+        the run then continues as the saved one would have."""
+        self._check(lib().upic_load_state(self._ctx, str(path).encode()))
+        n = ctypes.c_long()
+        self._check(lib().upic_particle_count(self._ctx, ctypes.byref(n)))
+        self.np = n.value
+
     def init_fields(self, diagnostics=True):
         ncol = len(IMPLICIT_DIAG_COLUMNS) if self.implicit else len(DIAG_COLUMNS)
         row = np.empty(ncol) if diagnostics else None

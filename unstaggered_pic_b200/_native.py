@@ -30,9 +30,12 @@ SYMBOLS = {
     "upic_get_particles": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 5),
     "upic_init_fields": (ctypes.c_int, [ctypes.c_void_p, c_dp]),
     "upic_set_background": (ctypes.c_int, [ctypes.c_void_p, c_dp]),
+    "upic_save_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    "upic_load_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     "upic_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
     "upic_step_implicit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, c_dp, c_dp]),
     "upic_step_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]),
+    "upic_particle_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]),
     "upic_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "upic_profile_read": (ctypes.c_int, [ctypes.c_void_p, c_dp, ctypes.POINTER(ctypes.c_long),
                                          ctypes.POINTER(ctypes.c_long)]),

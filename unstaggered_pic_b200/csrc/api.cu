@@ -625,6 +625,182 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
     return UPIC_OK;
 }
 
+}  // extern "C"
+
+// ---- state files -------------------------------------------------------------
+
+namespace upic_host {
+
+int state_bytes(upic_ctx* c, StateIO& io, void* host, size_t n) {
+    if (n == 0) return 0;
+    const size_t done = io.writing ? std::fwrite(host, 1, n, io.f) : std::fread(host, 1, n, io.f);
+    if (done != n) return fail(c, UPIC_ERR_ARGUMENT, io.writing ? "state file write failed" : "state file truncated");
+    return 0;
+}
+
+int state_device(upic_ctx* c, StateIO& io, void* dev, size_t n) {
+    constexpr size_t kPiece = size_t(64) << 20;
+    if (io.buf.size() < std::min(n, kPiece)) io.buf.resize(std::min(n, kPiece));
+    char* d = static_cast<char*>(dev);
+    for (size_t off = 0; off < n; off += kPiece) {
+        const size_t k = std::min(kPiece, n - off);
+        int rc;
+        if (io.writing) {
+            UPIC_CUDA(c, cudaMemcpyAsync(io.buf.data(), d + off, k, cudaMemcpyDeviceToHost, c->st));
+            if ((rc = sync(c)) || (rc = state_bytes(c, io, io.buf.data(), k))) return rc;
+        } else {
+            if ((rc = state_bytes(c, io, io.buf.data(), k))) return rc;
+            UPIC_CUDA(c, cudaMemcpyAsync(d + off, io.buf.data(), k, cudaMemcpyHostToDevice, c->st));
+            if ((rc = sync(c))) return rc;
+        }
+    }
+    return 0;
+}
+
+}  // namespace upic_host
+
+namespace {
+
+constexpr char kStateMagic[8] = {'U', 'P', 'I', 'C', 'S', 'T', 'A', 'T'};
+constexpr unsigned kStateVersion = 1;
+
+// Every configuration field that shapes the state or its evolution, as
+// doubles (struct padding never enters the comparison).
+std::vector<double> config_signature(const upic_config& f) {
+    return {(double)f.nx, (double)f.ny, f.Lx, f.Ly, f.dt, (double)f.method, (double)f.charge_update, f.c, f.eps0,
+            f.mu0, f.n0, (double)f.precision, (double)f.sort_interval, (double)f.tile, (double)f.guard, f.Lz,
+            f.kappa, f.sigma1, f.sigma2, (double)f.spline_order, (double)f.orbit_quad_order,
+            (double)f.split_orbit_at_knots, (double)f.nyquist_projection, (double)f.nonlinear_solver,
+            (double)f.nonlinear_max_iter, (double)f.anderson_memory, (double)f.anderson_start,
+            (double)f.local_max_iter, f.nonlinear_rtol, f.nonlinear_atol, f.anderson_damping,
+            f.anderson_regularization, f.anderson_growth_limit, f.local_rtol, f.local_atol, f.local_damping,
+            (double)f.perturbation_mode, f.picard_tol, (double)f.picard_max_iter,
+            (double)f.final_consistency_sweep};
+}
+
+// Everything the next explicit step reads: the particle set in its current
+// (sorted) order with the chunk list of the last sort, the field spectra and
+// BDF histories, the gathered field records, the deposit accumulators of the
+// next step's current, the charge and current, and the step counters.
+int explicit_state_io(upic_ctx* c, StateIO& io) {
+    int rc;
+    long np = c->np;
+    int uniform = c->uniform_qm ? 1 : 0, ready = c->fields_ready ? 1 : 0, has_bg = c->d_bg ? 1 : 0;
+    if ((rc = state_value(c, io, np)) || (rc = state_value(c, io, uniform)) || (rc = state_value(c, io, ready)) ||
+        (rc = state_value(c, io, has_bg)) || (rc = state_value(c, io, c->q0)) || (rc = state_value(c, io, c->m0)) ||
+        (rc = state_bytes(c, io, c->scale, sizeof(c->scale))) || (rc = state_value(c, io, c->head)) ||
+        (rc = state_value(c, io, c->steps)) || (rc = state_value(c, io, c->steps_since_sort)))
+        return rc;
+    if (!io.writing) {
+        if (np < 0 || np > 0x7fffffffL) return fail(c, UPIC_ERR_ARGUMENT, "state file: bad particle count");
+        if (np > c->cap || (!uniform && !c->P[0].q)) {
+            free_soa(c, c->P[0]);
+            free_soa(c, c->P[1]);
+            free_sortwork(c, c->sw);
+            const long cap = std::max(np, c->cap);
+            if ((rc = alloc_soa(c, c->P[0], cap, true, !uniform)) ||
+                (rc = alloc_soa(c, c->P[1], cap, true, !uniform)) || (rc = alloc_sortwork(c, c->sw, cap, c->tg)))
+                return rc;
+            c->cap = cap;
+        }
+        if ((rc = ensure_tmp3(c, np))) return rc;
+        if (has_bg && !c->d_bg && (rc = dalloc(c, &c->d_bg, c->N))) return rc;
+        c->cur = 0;
+        c->np = np;
+        c->uniform_qm = uniform != 0;
+        c->fields_ready = ready != 0;
+    }
+    ParticleSoA& p = c->P[c->cur];
+    const size_t pb = sizeof(double) * np;
+    double* arrs[] = {p.x, p.y, p.Px, p.Py, p.Pz, p.vx, p.vy, p.vz, p.wx, p.wy, p.wz};
+    for (double* a : arrs)
+        if ((rc = state_device(c, io, a, pb))) return rc;
+    if ((rc = state_device(c, io, p.id, sizeof(int) * np))) return rc;
+    if (!uniform && ((rc = state_device(c, io, p.q, pb)) || (rc = state_device(c, io, p.m, pb)))) return rc;
+    int nch = 0;
+    if (io.writing && np > 0) {
+        UPIC_CUDA(c, cudaMemcpy(&nch, c->sw.nchunks, sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    if ((rc = state_value(c, io, nch))) return rc;
+    if (nch > 0) {
+        const long chunk_cap = c->cap / c->tg.chunk + c->tg.ntx * c->tg.nty + 1;
+        if (nch > chunk_cap) return fail(c, UPIC_ERR_ARGUMENT, "state file: chunk list larger than the context's");
+        if ((rc = state_device(c, io, c->sw.chunks, sizeof(Chunk) * nch))) return rc;
+        if (!io.writing) UPIC_CUDA(c, cudaMemcpy(c->sw.nchunks, &nch, sizeof(int), cudaMemcpyHostToDevice));
+    }
+    const size_t N = (size_t)c->N;
+    if ((rc = state_device(c, io, c->d_spec, sizeof(double2) * 16 * N)) ||
+        (rc = state_device(c, io, c->d_hist, sizeof(double2) * 5 * kHistSlots * N)) ||
+        (rc = state_device(c, io, c->d_gf, sizeof(double) * kGFStride * N)) ||
+        (rc = state_device(c, io, c->d_acc, sizeof(unsigned long long) * 8 * N)) ||
+        (rc = state_device(c, io, c->d_J, sizeof(double) * 3 * N)) ||
+        (rc = state_device(c, io, c->d_rho, sizeof(double) * N)))
+        return rc;
+    if (has_bg && (rc = state_device(c, io, c->d_bg, sizeof(double) * N))) return rc;
+    return 0;
+}
+
+int state_file(upic_ctx* c, const char* path, bool writing) {
+    if (!c || !path) return UPIC_ERR_ARGUMENT;
+    StateIO io;
+    io.writing = writing;
+    io.f = std::fopen(path, writing ? "wb" : "rb");
+    if (!io.f) return fail(c, UPIC_ERR_ARGUMENT, std::string("cannot open state file ") + path);
+    int rc = 0;
+    char magic[8];
+    unsigned version = kStateVersion;
+    std::vector<double> sig = config_signature(c->cfg);
+    long nsig = (long)sig.size();
+    if (writing) std::memcpy(magic, kStateMagic, 8);
+    if ((rc = state_bytes(c, io, magic, 8)) || (rc = state_value(c, io, version)) || (rc = state_value(c, io, nsig))) {
+        std::fclose(io.f);
+        return rc;
+    }
+    if (!writing && (std::memcmp(magic, kStateMagic, 8) != 0 || version != kStateVersion ||
+                     nsig != (long)sig.size())) {
+        std::fclose(io.f);
+        return fail(c, UPIC_ERR_ARGUMENT, "not a state file of this library version");
+    }
+    std::vector<double> file_sig(sig);
+    if ((rc = state_bytes(c, io, file_sig.data(), sizeof(double) * sig.size()))) {
+        std::fclose(io.f);
+        return rc;
+    }
+    if (!writing && std::memcmp(file_sig.data(), sig.data(), sizeof(double) * sig.size()) != 0) {
+        std::fclose(io.f);
+        return fail(c, UPIC_ERR_CONFIG, "state file was written by a context with a different configuration");
+    }
+    rc = c->imp ? implicit_state_io(c, io) : explicit_state_io(c, io);
+    if (std::fclose(io.f) != 0 && rc == 0) rc = fail(c, UPIC_ERR_ARGUMENT, "state file close failed");
+    if (rc && !writing) {
+        // a partly read state is unusable: the context waits for particles again
+        c->np = 0;
+        c->fields_ready = false;
+        if (c->imp) implicit_mark_unloaded(c);
+    }
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int upic_save_state(upic_ctx* ctx, const char* path) {
+    if (ctx && ctx->st) {
+        const cudaError_t e = cudaStreamSynchronize(ctx->st);
+        if (e != cudaSuccess) return fail(ctx, UPIC_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return state_file(ctx, path, true);
+}
+
+int upic_load_state(upic_ctx* ctx, const char* path) {
+    if (ctx && ctx->st) {
+        const cudaError_t e = cudaStreamSynchronize(ctx->st);
+        if (e != cudaSuccess) return fail(ctx, UPIC_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return state_file(ctx, path, false);
+}
+
 int upic_destroy(upic_ctx* c) {
     if (!c) return UPIC_OK;
     if (c->st) cudaStreamSynchronize(c->st);
@@ -896,6 +1072,12 @@ int upic_set_background(upic_ctx* c, const double* rho_bg) {
 int upic_step_count(const upic_ctx* c, long* steps) {
     if (!c || !steps) return UPIC_ERR_ARGUMENT;
     *steps = c->steps;
+    return UPIC_OK;
+}
+
+int upic_particle_count(const upic_ctx* c, long* np) {
+    if (!c || !np) return UPIC_ERR_ARGUMENT;
+    *np = c->np;
     return UPIC_OK;
 }
 

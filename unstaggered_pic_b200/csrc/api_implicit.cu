@@ -1052,6 +1052,62 @@ int implicit_set_particles(upic_ctx* c, long np, const double* x, const double* 
     return sync(c);
 }
 
+void implicit_mark_unloaded(upic_ctx* c) {
+    ImplicitState& s = *c->imp;
+    s.np = 0;
+    s.loaded = false;
+    s.ready = false;
+    s.energy_valid = false;
+}
+
+// Everything the next implicit step reads: the particle set with its orbit
+// velocities, the state spectra, the state current (the next step's first
+// current guess), scales and counters.
+int implicit_state_io(upic_ctx* c, StateIO& io) {
+    ImplicitState& s = *c->imp;
+    int rc;
+    long np = s.np;
+    int uniform = s.uniform ? 1 : 0, loaded = s.loaded ? 1 : 0, ready = s.ready ? 1 : 0,
+        evalid = s.energy_valid ? 1 : 0;
+    if ((rc = state_value(c, io, np)) || (rc = state_value(c, io, uniform)) || (rc = state_value(c, io, loaded)) ||
+        (rc = state_value(c, io, ready)) || (rc = state_value(c, io, evalid)) ||
+        (rc = state_value(c, io, s.energy_W)) || (rc = state_value(c, io, s.energy_K)) ||
+        (rc = state_value(c, io, s.q0)) || (rc = state_value(c, io, s.m0)) || (rc = state_value(c, io, s.qabs)) ||
+        (rc = state_value(c, io, s.vb_limit)) || (rc = state_bytes(c, io, s.scaleJ, sizeof(s.scaleJ))) ||
+        (rc = state_value(c, io, s.steps)))
+        return rc;
+    if (!io.writing) {
+        if (np < 0 || np > 0x7fffffffL) return fail(c, UPIC_ERR_ARGUMENT, "state file: bad particle count");
+        if (np > s.cap || (!uniform && !s.P[0].q)) {
+            free_particles(c, s);
+            if ((rc = alloc_particles(c, s, std::max(np, s.cap), !uniform))) return rc;
+        }
+        if ((rc = ensure_tmp3(c, np))) return rc;
+        s.cur = 0;
+        s.np = np;
+        s.uniform = uniform != 0;
+        s.loaded = loaded != 0;
+        s.ready = ready != 0;
+        s.energy_valid = evalid != 0;
+        c->np = np;
+        c->fields_ready = s.ready;
+        c->steps = s.steps;
+    }
+    ParticleSoA& p = s.P[s.cur];
+    const size_t pb = sizeof(double) * np;
+    double* arrs[] = {p.x, p.y, p.Px, p.Py, p.Pz, p.vx, p.vy, p.vz, p.wx, p.wy, p.wz,
+                      s.bx[s.cur], s.by[s.cur], s.bz[s.cur]};
+    for (double* a : arrs)
+        if ((rc = state_device(c, io, a, pb))) return rc;
+    if ((rc = state_device(c, io, p.id, sizeof(int) * np))) return rc;
+    if (!uniform && ((rc = state_device(c, io, p.q, pb)) || (rc = state_device(c, io, p.m, pb)))) return rc;
+    const size_t N = (size_t)c->N;
+    if ((rc = state_device(c, io, s.spec, sizeof(double2) * 9 * N)) ||
+        (rc = state_device(c, io, s.J, sizeof(double) * 3 * N)))
+        return rc;
+    return 0;
+}
+
 int implicit_get_particles(upic_ctx* c, long np, double* x, double* y, double* P, double* v, double* v_prev) {
     ImplicitState& s = *c->imp;
     if (np != s.np) return fail(c, UPIC_ERR_ARGUMENT, "particle count does not match the context");

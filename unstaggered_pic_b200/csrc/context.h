@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdio>
 #include <string>
 #include <utility>
 #include <vector>
@@ -127,6 +128,23 @@ struct HostScan {
     bool finite = true, uniform = true, positive_m = true;
     double qabs = 0.0, speed_max = 0.0, comp_max = 0.0;
 };
+// State files (upic_save_state / upic_load_state).  One routine per state
+// serialises in both directions: with writing set it writes host/device
+// bytes to the file, otherwise it reads them back into the same places.
+struct StateIO {
+    FILE* f = nullptr;
+    bool writing = false;
+    std::vector<char> buf;  // host staging of device ranges
+};
+int state_bytes(upic_ctx* c, StateIO& io, void* host, size_t n);
+int state_device(upic_ctx* c, StateIO& io, void* dev, size_t n);
+template <typename T>
+int state_value(upic_ctx* c, StateIO& io, T& v) {
+    return state_bytes(c, io, &v, sizeof(T));
+}
+int implicit_state_io(upic_ctx* c, StateIO& io);
+void implicit_mark_unloaded(upic_ctx* c);
+
 HostScan scan_particles(long np, const double* x, const double* y, const double* v, const double* q,
                         const double* m);
 double fixed_scale(double bound);
