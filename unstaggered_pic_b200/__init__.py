@@ -20,6 +20,9 @@ __all__ = ["UpicError", "Config", "ImplicitConfig", "NonrelConfig", "Simulation"
 
 METHODS = {"bdf1": 1, "bdf2": 2, "cn_orbit": 3, "cn_orbit_nonrel": 4}
 CHARGE_UPDATES = {"conserving": 0, "naive": 1}
+# FP64 throughout, or the mixed form of the explicit step (FP32 particles with
+# cell-relative offsets, FP64 field solve and diagnostics)
+PRECISIONS = {"fp64": 0, "mixed": 1}
 NONLINEAR_SOLVERS = {"anderson_quasi_newton": 0, "anderson": 0, "picard": 1}
 FIELDS = {"phi": 0, "Ax": 1, "Ay": 2, "Az": 3, "rho": 4, "Jx": 5, "Jy": 6, "Jz": 7,
           "psi": 8, "Ux": 9, "Uy": 10, "Uz": 11}
@@ -76,11 +79,12 @@ class Config:
 
     def __init__(self, nx=32, ny=32, Lx=2 * np.pi, Ly=2 * np.pi, dt=0.05, method="bdf1",
                  charge_update="conserving", c=1.0, eps0=1.0, mu0=1.0, n0=1.0,
-                 sort_interval=0, tile=0, guard=-1):
+                 sort_interval=0, tile=0, guard=-1, precision="fp64"):
         self.nx, self.ny, self.Lx, self.Ly, self.dt = nx, ny, Lx, Ly, dt
         self.method, self.charge_update = method, charge_update
         self.c, self.eps0, self.mu0, self.n0 = c, eps0, mu0, n0
         self.sort_interval, self.tile, self.guard = sort_interval, tile, guard
+        self.precision = precision
 
     def to_c(self):
         cfg = UpicConfig()
@@ -92,6 +96,8 @@ class Config:
         cfg.charge_update = CHARGE_UPDATES[cu] if isinstance(cu, str) else int(cu)
         cfg.c, cfg.eps0, cfg.mu0, cfg.n0 = float(self.c), float(self.eps0), float(self.mu0), float(self.n0)
         cfg.sort_interval, cfg.tile, cfg.guard = int(self.sort_interval), int(self.tile), int(self.guard)
+        pr = self.precision
+        cfg.precision = PRECISIONS[pr] if isinstance(pr, str) else int(pr)
         return cfg
 
 

@@ -18,7 +18,7 @@ OUT = os.path.join(HERE, "libupic.so")
 RUN = os.path.join(HERE, "upic_run")
 BUILD = os.path.join(ROOT, "_build")
 
-SOURCES = ["fft.cu", "sort.cu", "explicit.cu", "implicit.cu", "api.cu", "api_implicit.cu", "noalloc.cu",
+SOURCES = ["fft.cu", "sort.cu", "explicit.cu", "mixed.cu", "implicit.cu", "api.cu", "api_implicit.cu", "noalloc.cu",
            "generate.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

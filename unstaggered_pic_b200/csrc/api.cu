@@ -141,6 +141,34 @@ void free_soa(upic_ctx* c, ParticleSoA& s) {
     s = ParticleSoA{};
 }
 
+int alloc_mixed(upic_ctx* c, MixedSoA& s, long cap, bool with_qm) {
+    int rc;
+    float** arrs[] = {&s.rx, &s.ry, &s.Px, &s.Py, &s.Pz, &s.vx, &s.vy, &s.vz, &s.wx, &s.wy, &s.wz};
+    for (float** a : arrs)
+        if ((rc = dalloc(c, a, cap))) return rc;
+    if (with_qm && ((rc = dalloc(c, &s.q, cap)) || (rc = dalloc(c, &s.m, cap)))) return rc;
+    if ((rc = dalloc(c, &s.cell, cap))) return rc;
+    return dalloc(c, &s.id, cap);
+}
+
+void free_mixed(upic_ctx* c, MixedSoA& s) {
+    void* ps[] = {s.cell, s.rx, s.ry, s.Px, s.Py, s.Pz, s.vx, s.vy, s.vz, s.wx, s.wy, s.wz, s.q, s.m, s.id};
+    for (void* p : ps) dfree(c, p);
+    s = MixedSoA{};
+}
+
+// Single-word fixed-point scale: 2^F with |sum| * 2^F < 2^59 for any sum
+// bounded by `bound` (four bits of headroom in the int64).
+double fixed_scale1(double bound) {
+    if (!(bound > 0.0) || !std::isfinite(bound)) return 1.0;
+    int e = 0;
+    std::frexp(bound, &e);
+    int F = 59 - e;
+    if (F > 1000) F = 1000;
+    if (F < -1000) F = -1000;
+    return std::ldexp(1.0, F);
+}
+
 int alloc_sortwork(upic_ctx* c, SortWork& w, long cap, const TileGeom& tg) {
     int rc;
     if ((rc = dalloc(c, &w.keys, cap))) return rc;
@@ -387,6 +415,14 @@ int run_diag(upic_ctx* c, int slot_new, int slot_prev0, int na, const double* ac
 // Sort the active particle set by the cell of wrap(x + shift v) and make the
 // sorted copy active.
 int sort_active(upic_ctx* c, double shift) {
+    if (c->mixed) {
+        const float sx = (float)(shift / c->dx), sy = (float)(shift / c->dy);
+        UPIC_CUDA(c, sort_mixed_by_tile(c->tg, c->M[c->cur], c->np, c->lny, sx, sy, c->sw, c->st));
+        UPIC_CUDA(c, permute_mixed(c->M[c->cur], c->M[1 - c->cur], c->np, c->sw, c->st));
+        c->cur = 1 - c->cur;
+        c->steps_since_sort = 0;
+        return 0;
+    }
     ParticleSoA& src = c->P[c->cur];
     ParticleSoA& dst = c->P[1 - c->cur];
     UPIC_CUDA(c, sort_particles_by_tile(c->tg, src, c->np, c->cfg.Lx, c->cfg.Ly, shift, c->sw, c->st));
@@ -396,8 +432,47 @@ int sort_active(upic_ctx* c, double shift) {
     return 0;
 }
 
+int launch_push_mixed_ctx(upic_ctx* c, int mode, int ncomp, long np, bool uniform, const SortWork& w,
+                          double* pdiag) {
+    MixedPushArgs a{};
+    a.p = c->M[c->cur];
+    a.np = np;
+    a.q0f = (float)c->q0;
+    a.m0f = (float)c->m0;
+    a.m0 = c->m0;
+    a.dt = (float)c->cfg.dt;
+    a.dt_dx = (float)(c->cfg.dt / c->dx);
+    a.dt_dy = (float)(c->cfg.dt / c->dy);
+    a.c = (float)c->cfg.c;
+    a.c2 = (float)(c->cfg.c * c->cfg.c);
+    a.inv_dA = (float)(1.0 / c->dA);
+    a.cd = c->cfg.c;
+    a.inv_c2d = 1.0 / (c->cfg.c * c->cfg.c);
+    a.lny = c->lny;
+    a.gf = c->d_gf32;
+    a.chunks = w.chunks;
+    a.nchunks = w.nchunks;
+    a.acc = c->d_acc;
+    for (int k = 0; k < 4; ++k) a.scale[k] = c->scale[k];
+    a.diag_part = pdiag;
+    const bool prof = c->profiling && mode == kModePush;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof) {
+        UPIC_CUDA(c, cudaEventCreate(&e0));
+        UPIC_CUDA(c, cudaEventCreate(&e1));
+        UPIC_CUDA(c, cudaEventRecord(e0, c->st));
+    }
+    UPIC_CUDA(c, launch_push_mixed(mode, ncomp, uniform, c->tg, a, c->push_grid, c->st));
+    if (prof) {
+        UPIC_CUDA(c, cudaEventRecord(e1, c->st));
+        c->prof_events.emplace_back(e0, e1);
+    }
+    return 0;
+}
+
 int launch_push(upic_ctx* c, int mode, int ncomp, const ParticleSoA& p, long np, bool uniform,
                 const SortWork& w, double* pdiag) {
+    if (c->mixed) return launch_push_mixed_ctx(c, mode, ncomp, np, uniform, w, pdiag);
     PushArgs a = push_args(c, p, np, uniform);
     a.chunks = w.chunks;
     a.nchunks = w.nchunks;
@@ -538,8 +613,9 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
             !(cfg->mu0 > 0))
             return fail(nullptr, UPIC_ERR_CONFIG, "Lx, Ly, dt, c, eps0, mu0 must be positive");
     }
-    if (cfg->precision != UPIC_PRECISION_FP64)
-        return fail(nullptr, UPIC_ERR_CONFIG, "this build supports precision = fp64 only");
+    if (cfg->precision != UPIC_PRECISION_FP64 && !(cfg->precision == UPIC_PRECISION_MIXED && !implicit))
+        return fail(nullptr, UPIC_ERR_CONFIG,
+                    "precision must be fp64, or mixed with the explicit methods (bdf1, bdf2)");
 
     upic_ctx* c = new upic_ctx();
     c->cfg = *cfg;
@@ -568,10 +644,14 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
     if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(c, UPIC_ERR_CUDA, "cudaStreamCreate failed"));
     c->st = c->own;
-    if (fft_configure_smem() != cudaSuccess || push_configure_smem(c->tg) != cudaSuccess)
+    c->mixed = cfg->precision == UPIC_PRECISION_MIXED;
+    while ((1 << c->lny) < c->ny) ++c->lny;
+    if (fft_configure_smem() != cudaSuccess || push_configure_smem(c->tg) != cudaSuccess ||
+        (c->mixed && push_mixed_configure_smem(c->tg) != cudaSuccess))
         return bail(fail(c, UPIC_ERR_CUDA, "cudaFuncSetAttribute failed"));
     // persistent grid: as many push CTAs as fit on the GPU at once
-    const int occ = push_occupancy(c->tg, cfg->charge_update == UPIC_CHARGE_NAIVE ? 4 : 3);
+    const int ncomp_step = cfg->charge_update == UPIC_CHARGE_NAIVE ? 4 : 3;
+    const int occ = c->mixed ? push_mixed_occupancy(c->tg, ncomp_step) : push_occupancy(c->tg, ncomp_step);
     c->push_grid = c->nsm * (occ > 0 ? occ : 1);
 
     const int N = c->N;
@@ -586,7 +666,8 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
         (rc = dalloc(c, &c->d_dreal, (size_t)kDiagFields * N)) ||
         (rc = dalloc(c, &c->d_partials, (size_t)kRedGrid * 16)) ||
         (rc = dalloc(c, &c->d_pdiag, (size_t)c->push_grid * kDiagPart)) ||
-        (rc = dalloc(c, &c->d_row, UPIC_DIAG_COUNT)))
+        (rc = dalloc(c, &c->d_row, UPIC_DIAG_COUNT)) ||
+        (c->mixed && (rc = dalloc(c, &c->d_gf32, (size_t)kGFStride * N))))
         return bail(rc);
     if (cudaMallocHost(&c->h_row, sizeof(double) * UPIC_DIAG_COUNT) != cudaSuccess)
         return bail(fail(c, UPIC_ERR_NOMEM, "cudaMallocHost failed"));
@@ -693,7 +774,16 @@ int explicit_state_io(upic_ctx* c, StateIO& io) {
         return rc;
     if (!io.writing) {
         if (np < 0 || np > 0x7fffffffL) return fail(c, UPIC_ERR_ARGUMENT, "state file: bad particle count");
-        if (np > c->cap || (!uniform && !c->P[0].q)) {
+        if (c->mixed && (np > c->cap || (!uniform && !c->M[0].q))) {
+            free_mixed(c, c->M[0]);
+            free_mixed(c, c->M[1]);
+            free_sortwork(c, c->sw);
+            const long cap = std::max(np, c->cap);
+            if ((rc = alloc_mixed(c, c->M[0], cap + 2, !uniform)) || (rc = alloc_mixed(c, c->M[1], cap + 2, !uniform)) ||
+                (rc = alloc_sortwork(c, c->sw, cap, c->tg)))
+                return rc;
+            c->cap = cap;
+        } else if (!c->mixed && (np > c->cap || (!uniform && !c->P[0].q))) {
             free_soa(c, c->P[0]);
             free_soa(c, c->P[1]);
             free_sortwork(c, c->sw);
@@ -710,13 +800,24 @@ int explicit_state_io(upic_ctx* c, StateIO& io) {
         c->uniform_qm = uniform != 0;
         c->fields_ready = ready != 0;
     }
-    ParticleSoA& p = c->P[c->cur];
-    const size_t pb = sizeof(double) * np;
-    double* arrs[] = {p.x, p.y, p.Px, p.Py, p.Pz, p.vx, p.vy, p.vz, p.wx, p.wy, p.wz};
-    for (double* a : arrs)
-        if ((rc = state_device(c, io, a, pb))) return rc;
-    if ((rc = state_device(c, io, p.id, sizeof(int) * np))) return rc;
-    if (!uniform && ((rc = state_device(c, io, p.q, pb)) || (rc = state_device(c, io, p.m, pb)))) return rc;
+    if (c->mixed) {
+        MixedSoA& p = c->M[c->cur];
+        const size_t fb = sizeof(float) * np;
+        float* arrs[] = {p.rx, p.ry, p.Px, p.Py, p.Pz, p.vx, p.vy, p.vz, p.wx, p.wy, p.wz};
+        for (float* a : arrs)
+            if ((rc = state_device(c, io, a, fb))) return rc;
+        if ((rc = state_device(c, io, p.cell, sizeof(int) * np)) || (rc = state_device(c, io, p.id, sizeof(int) * np)))
+            return rc;
+        if (!uniform && ((rc = state_device(c, io, p.q, fb)) || (rc = state_device(c, io, p.m, fb)))) return rc;
+    } else {
+        ParticleSoA& p = c->P[c->cur];
+        const size_t pb = sizeof(double) * np;
+        double* arrs[] = {p.x, p.y, p.Px, p.Py, p.Pz, p.vx, p.vy, p.vz, p.wx, p.wy, p.wz};
+        for (double* a : arrs)
+            if ((rc = state_device(c, io, a, pb))) return rc;
+        if ((rc = state_device(c, io, p.id, sizeof(int) * np))) return rc;
+        if (!uniform && ((rc = state_device(c, io, p.q, pb)) || (rc = state_device(c, io, p.m, pb)))) return rc;
+    }
     int nch = 0;
     if (io.writing && np > 0) {
         UPIC_CUDA(c, cudaMemcpy(&nch, c->sw.nchunks, sizeof(int), cudaMemcpyDeviceToHost));
@@ -731,7 +832,8 @@ int explicit_state_io(upic_ctx* c, StateIO& io) {
     const size_t N = (size_t)c->N;
     if ((rc = state_device(c, io, c->d_spec, sizeof(double2) * 16 * N)) ||
         (rc = state_device(c, io, c->d_hist, sizeof(double2) * 5 * kHistSlots * N)) ||
-        (rc = state_device(c, io, c->d_gf, sizeof(double) * kGFStride * N)) ||
+        (c->mixed ? (rc = state_device(c, io, c->d_gf32, sizeof(float) * kGFStride * N))
+                  : (rc = state_device(c, io, c->d_gf, sizeof(double) * kGFStride * N))) ||
         (rc = state_device(c, io, c->d_acc, sizeof(unsigned long long) * 8 * N)) ||
         (rc = state_device(c, io, c->d_J, sizeof(double) * 3 * N)) ||
         (rc = state_device(c, io, c->d_rho, sizeof(double) * N)))
@@ -821,6 +923,91 @@ int upic_set_stream(upic_ctx* c, void* stream) {
     return UPIC_OK;
 }
 
+// Mixed precision: the host set in the reference's layout becomes nearest
+// nodes, FP32 offsets and FP32 momenta and velocities (the conversions run
+// on the device from the FP64 staging buffer).
+static int set_particles_mixed(upic_ctx* c, long np, const double* x, const double* y, const double* P,
+                               const double* v, const double* v_prev, const double* q, const double* m) {
+    int rc;
+    c->fields_ready = false;
+    if (np > c->cap) {
+        const bool had_qm = c->M[0].q != nullptr;
+        free_mixed(c, c->M[0]);
+        free_mixed(c, c->M[1]);
+        free_sortwork(c, c->sw);
+        if ((rc = alloc_mixed(c, c->M[0], np + 2, had_qm)) || (rc = alloc_mixed(c, c->M[1], np + 2, had_qm)) ||
+            (rc = alloc_sortwork(c, c->sw, np, c->tg)))
+            return rc;
+        c->cap = np;
+    }
+    if ((rc = ensure_tmp3(c, np))) return rc;
+    MixedSoA& s = c->M[0];
+    double* t = c->d_tmp3;
+    if (np > 0) {
+        UPIC_CUDA(c, cudaMemcpyAsync(t, x, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(t + np, y, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, mixed_from_positions(np, t, t + np, 1.0 / c->dx, 1.0 / c->dy, c->nx, c->ny, c->lny, s.cell,
+                                          s.rx, s.ry, c->st));
+        const double* trip[3] = {P, v, v_prev};
+        float* dst[3][3] = {{s.Px, s.Py, s.Pz}, {s.vx, s.vy, s.vz}, {s.wx, s.wy, s.wz}};
+        for (int k = 0; k < 3; ++k) {
+            UPIC_CUDA(c, cudaMemcpyAsync(t, trip[k], sizeof(double) * 3 * np, cudaMemcpyHostToDevice, c->st));
+            UPIC_CUDA(c, mixed_split3(np, t, dst[k][0], dst[k][1], dst[k][2], c->st));
+        }
+    }
+    const HostScan hs = scan_particles(np, x, y, v, q, m);
+    if (!hs.finite) {
+        c->np = 0;
+        sync(c);
+        return fail(c, UPIC_ERR_NONFINITE, "non-finite particle position or velocity");
+    }
+    const bool uniform = hs.uniform;
+    if (!uniform && !s.q) {
+        for (int k = 0; k < 2; ++k)
+            if ((rc = dalloc(c, &c->M[k].q, c->cap + 2)) || (rc = dalloc(c, &c->M[k].m, c->cap + 2))) return rc;
+    }
+    c->np = np;
+    c->cur = 0;
+    c->uniform_qm = uniform;
+    c->q0 = np ? q[0] : 0.0;
+    c->m0 = np ? m[0] : 0.0;
+    if (np > 0) {
+        if (!uniform) {
+            UPIC_CUDA(c, cudaMemcpyAsync(t, q, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+            UPIC_CUDA(c, mixed_from_doubles(np, t, c->M[0].q, c->st));
+            UPIC_CUDA(c, cudaMemcpyAsync(t + np, m, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+            UPIC_CUDA(c, mixed_from_doubles(np, t + np, c->M[0].m, c->st));
+        }
+        if ((rc = iota(c, c->M[0].id, np))) return rc;
+    }
+    const double vb = hs.speed_max > c->cfg.c ? hs.speed_max : c->cfg.c;
+    c->scale[0] = c->scale[1] = c->scale[2] = fixed_scale1(hs.qabs * vb / c->dA);
+    c->scale[3] = fixed_scale1(hs.qabs / c->dA);
+    c->steps = 0;
+    return sync(c);
+}
+
+static int get_particles_mixed(upic_ctx* c, long np, double* x, double* y, double* P, double* v, double* v_prev) {
+    if (np == 0) return UPIC_OK;
+    MixedSoA& s = c->M[c->cur];
+    MixedSoA& d = c->M[1 - c->cur];
+    UPIC_CUDA(c, unpermute_mixed(s, d, np, c->st));
+    double* t = c->d_tmp3;
+    UPIC_CUDA(c, mixed_to_positions(np, d.cell, d.rx, d.ry, c->dx, c->dy, c->cfg.Lx, c->cfg.Ly, c->lny, c->ny, t,
+                                    t + np, c->st));
+    if (x) UPIC_CUDA(c, cudaMemcpyAsync(x, t, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    if (y) UPIC_CUDA(c, cudaMemcpyAsync(y, t + np, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    double* out[3] = {P, v, v_prev};
+    const float* src[3][3] = {{d.Px, d.Py, d.Pz}, {d.vx, d.vy, d.vz}, {d.wx, d.wy, d.wz}};
+    for (int k = 0; k < 3; ++k) {
+        if (!out[k]) continue;
+        // the staging buffer is reused in stream order
+        UPIC_CUDA(c, mixed_join3(np, src[k][0], src[k][1], src[k][2], t, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(out[k], t, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost, c->st));
+    }
+    return sync(c);
+}
+
 int upic_set_particles(upic_ctx* c, long np, const double* x, const double* y, const double* P,
                        const double* v, const double* v_prev, const double* q, const double* m) {
     if (!c) return UPIC_ERR_ARGUMENT;
@@ -836,6 +1023,7 @@ int upic_set_particles(upic_ctx* c, long np, const double* x, const double* y, c
         }
         return rc;
     }
+    if (c->mixed) return set_particles_mixed(c, np, x, y, P, v, v_prev, q, m);
     int rc;
     c->fields_ready = false;
     if (np > c->cap) {
@@ -897,6 +1085,7 @@ int upic_get_particles(upic_ctx* c, long np, double* x, double* y, double* P, do
     if (!c) return UPIC_ERR_ARGUMENT;
     if (np != c->np) return fail(c, UPIC_ERR_ARGUMENT, "particle count does not match the context");
     if (c->imp) return implicit_get_particles(c, np, x, y, P, v, v_prev);
+    if (c->mixed) return get_particles_mixed(c, np, x, y, P, v, v_prev);
     if (np == 0) return UPIC_OK;
     ParticleSoA& s = c->P[c->cur];
     ParticleSoA& d = c->P[1 - c->cur];
@@ -927,7 +1116,10 @@ int upic_init_fields(upic_ctx* c, double* diag_row) {
     } else {
         UPIC_CUDA(c, cudaMemsetAsync(c->d_pdiag, 0, sizeof(double) * c->push_grid * kDiagPart, c->st));
     }
-    UPIC_CUDA(c, launch_convert_acc(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0, 3, c->st, c->d_bg));
+    if (c->mixed)
+        UPIC_CUDA(c, launch_convert_acc1(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0, 3, c->st, c->d_bg));
+    else
+        UPIC_CUDA(c, launch_convert_acc(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0, 3, c->st, c->d_bg));
     // phi0 from Poisson (:1104, :819-827), histories (:1107-1111)
     double2* sp = c->d_spec;
     UPIC_CUDA(c, fft2d_batched(c->plan, sp + 3 * (size_t)N, 1, 0, c->st, c->d_rho));
@@ -979,8 +1171,12 @@ int upic_step(upic_ctx* c, int nsteps, int diag_stride, double* diag) {
             if ((rc = sort_active(c, c->cfg.dt))) return rc;
         }
         // J^n (and rho^n) were deposited by the previous particle kernel
-        UPIC_CUDA(c, launch_convert_acc(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0,
-                                        naive ? 3 : 1, c->st, c->d_bg));
+        if (c->mixed)
+            UPIC_CUDA(c, launch_convert_acc1(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0, naive ? 3 : 1,
+                                             c->st, c->d_bg));
+        else
+            UPIC_CUDA(c, launch_convert_acc(c->d_acc, N, c->scale, c->d_J, c->d_rho, c->cfg.n0, naive ? 3 : 1,
+                                            c->st, c->d_bg));
         UPIC_CUDA(c, fft2d_batched(c->plan, sp, 3, 0, c->st, c->d_J));
         if (naive) UPIC_CUDA(c, fft2d_batched(c->plan, sp + 3 * (size_t)N, 1, 0, c->st, c->d_rho));
         KspaceArgs k{};
@@ -1004,8 +1200,12 @@ int upic_step(upic_ctx* c, int nsteps, int diag_stride, double* diag) {
         k.conserving = naive ? 0 : 1;
         k.gspec = sp + 4 * (size_t)N;
         UPIC_CUDA(c, launch_bdf_kspace(k, c->st));
-        UPIC_CUDA(c, fft2d_batched(c->plan, sp + 4 * (size_t)N, kGF, 1, c->st, nullptr, 2, c->d_gf,
-                                   kGFStride, 0));
+        if (c->mixed)
+            UPIC_CUDA(c, fft2d_batched(c->plan, sp + 4 * (size_t)N, kGF, 1, c->st, nullptr, 3,
+                                       reinterpret_cast<double*>(c->d_gf32), kGFStride, 0));
+        else
+            UPIC_CUDA(c, fft2d_batched(c->plan, sp + 4 * (size_t)N, kGF, 1, c->st, nullptr, 2, c->d_gf,
+                                       kGFStride, 0));
         if (c->np > 0) {
             if ((rc = launch_push(c, kModePush, grid_ncomp(c), c->P[c->cur], c->np, c->uniform_qm, c->sw,
                                   c->d_pdiag)))

@@ -24,6 +24,7 @@ struct ImplicitState;  // api_implicit.cu
 }  // namespace upic_host
 
 using upic::FftPlan;
+using upic::MixedSoA;
 using upic::ParticleSoA;
 using upic::SortWork;
 using upic::TileGeom;
@@ -49,6 +50,14 @@ struct upic_ctx {
     double q0 = 0, m0 = 0;
     double scale[4] = {1, 1, 1, 1};
     double* d_tmp3 = nullptr;  // 3*cap staging for xyz triples
+
+    // mixed precision (UPIC_PRECISION_MIXED): the particle state lives in
+    // M[cur] instead of P[cur]; scale[] then holds single-word fixed-point
+    // scales; d_gf32 holds the FP32 node records
+    bool mixed = false;
+    MixedSoA M[2];
+    float* d_gf32 = nullptr;
+    int lny = 0;  // log2(ny)
 
     // kernel-level entry points use their own particle buffers
     long kcap = 0;
@@ -92,6 +101,7 @@ struct upic_ctx {
 
 namespace upic_host {
 
+using upic::MixedSoA;
 using upic::ParticleSoA;
 using upic::SortWork;
 using upic::TileGeom;

@@ -91,7 +91,8 @@ fft_y_kernel(double2* __restrict__ data, const double* __restrict__ rin, int in_
 // column j lives at c*N + i*ny + j.  out_mode 0: complex in place;
 // 1: real part to rout[(c*N + node) ...] planar (rout_comp_stride = N,
 // rout_node_stride = 1); 2: real part to interleaved records
-// rout[node*rec_stride + comp_offset + c].
+// rout[node*rec_stride + comp_offset + c]; 3: the same records in FP32 (rout
+// then points to floats).
 __global__ void __launch_bounds__(kFftThreads)
 fft_x_kernel(double2* __restrict__ data, int ncomp, int nx, int ny, int log2nx, int cols_per_cta,
              const double2* __restrict__ tw, int inverse, int out_mode, double* __restrict__ rout,
@@ -118,7 +119,8 @@ fft_x_kernel(double2* __restrict__ data, int ncomp, int nx, int ny, int log2nx, 
         const size_t node = (size_t)i * ny + j0 + cc;
         if (out_mode == 0) d[node] = v;
         else if (out_mode == 1) rout[c * N + node] = v.x;
-        else rout[node * rec_stride + comp_offset + c] = v.x;
+        else if (out_mode == 2) rout[node * rec_stride + comp_offset + c] = v.x;
+        else reinterpret_cast<float*>(rout)[node * rec_stride + comp_offset + c] = (float)v.x;
     }
 }
 

@@ -23,7 +23,8 @@ struct FftPlan {
 // real_in != NULL: the input is the real planar array real_in (imag 0), the
 // transform result lands in data.  out_mode 0: complex result in data;
 // 1: real part to real_out planar (component stride nx*ny); 2: real part to
-// interleaved records real_out[node*rec_stride + comp_offset + c].
+// interleaved records real_out[node*rec_stride + comp_offset + c]; 3: the
+// same records as floats (real_out then points to float storage).
 cudaError_t fft2d_batched(const FftPlan& p, double2* data, int ncomp, int inverse, cudaStream_t st,
                           const double* real_in = nullptr, int out_mode = 0,
                           double* real_out = nullptr, int rec_stride = 0, int comp_offset = 0);
@@ -93,6 +94,42 @@ cudaError_t permute_particles(const ParticleSoA& src, const ParticleSoA& dst, lo
 // dst[id[k]] = src[k] for the arrays x..wz (restores the caller's order).
 cudaError_t unpermute_particles(const ParticleSoA& src, const ParticleSoA& dst, long np,
                                 cudaStream_t st);
+// The radix sort of w.keys (with w.vals) and the chunk table, after the keys
+// are made (shared by both particle formats).
+cudaError_t sort_keys_to_chunks(const TileGeom& tg, long np, SortWork& w, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Mixed-precision particle state of the explicit step (UPIC_PRECISION_MIXED,
+// mixed.cu): per particle the nearest node cell = ix * ny + iy and the
+// cell-relative offsets r = x / dx - ix in [-1/2, 1/2), FP32 momenta and
+// velocities.
+struct MixedSoA {
+    int* cell = nullptr;
+    float *rx = nullptr, *ry = nullptr;
+    float *Px = nullptr, *Py = nullptr, *Pz = nullptr;
+    float *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    float *wx = nullptr, *wy = nullptr, *wz = nullptr;  // previous velocity
+    float *q = nullptr, *m = nullptr;                    // per particle, or null (uniform)
+    int* id = nullptr;
+};
+
+// Keys of the nearest-node cell after advancing the offsets by (sx vx, sy vy)
+// (sx = shift / dx), then sort_keys_to_chunks.
+cudaError_t sort_mixed_by_tile(const TileGeom& tg, const MixedSoA& p, long np, int lny, float sx, float sy,
+                               SortWork& w, cudaStream_t st);
+cudaError_t permute_mixed(const MixedSoA& src, const MixedSoA& dst, long np, const SortWork& w,
+                          cudaStream_t st);
+// Host layout -> mixed: x, y in [0, L) (doubles), P, v, v_prev as xyz triples
+// (doubles, in tmp3 staging on the device) -> the mixed arrays.
+cudaError_t mixed_from_positions(long np, const double* x, const double* y, double inv_dx, double inv_dy, int nx,
+                                 int ny, int lny, int* cell, float* rx, float* ry, cudaStream_t st);
+cudaError_t mixed_split3(long np, const double* aos, float* a, float* b, float* c, cudaStream_t st);
+cudaError_t mixed_from_doubles(long np, const double* src, float* dst, cudaStream_t st);
+// Mixed (sorted order) -> caller order in dst, then positions / triples as doubles.
+cudaError_t unpermute_mixed(const MixedSoA& src, const MixedSoA& dst, long np, cudaStream_t st);
+cudaError_t mixed_to_positions(long np, const int* cell, const float* rx, const float* ry, double dx, double dy,
+                               double Lx, double Ly, int lny, int ny, double* x, double* y, cudaStream_t st);
+cudaError_t mixed_join3(long np, const float* a, const float* b, const float* c, double* aos, cudaStream_t st);
 
 // ---------------------------------------------------------------------------
 // Explicit BDF/IAEM step (explicit.cu)
@@ -121,6 +158,34 @@ int push_deposit_smem_bytes(const TileGeom& tg, int ncomp);
 cudaError_t push_configure_smem(const TileGeom& tg);
 // Resident CTAs per SM of the step's push kernel (ncomp 3 or 4).
 int push_occupancy(const TileGeom& tg, int ncomp);
+
+// Mixed-precision step kernel (mixed.cu): the FP32 counterpart of
+// push_deposit_kernel with single-word fixed-point deposits.
+struct MixedPushArgs {
+    MixedSoA p;
+    long np;
+    float q0f, m0f;          // uniform charge and mass (FP32 arithmetic)
+    double m0;               // uniform mass for the FP64 diagnostics
+    float dt, dt_dx, dt_dy;  // dt and dt / dx, dt / dy (offsets advance in cells)
+    float c, c2, inv_dA;
+    double cd, inv_c2d;      // c and 1 / c^2 of the FP64 diagnostics
+    int lny;                 // log2(ny)
+    const float* gf;         // FP32 node records, kGFStride floats
+    const Chunk* chunks;
+    const int* nchunks;
+    unsigned long long* acc; // [slot][2][N]: the single-word sums go to the first word of a slot
+    double scale[4];         // single-word fixed-point scale per slot
+    double* diag_part;       // per-CTA particle reductions (kDiagPart doubles)
+};
+cudaError_t launch_push_mixed(int mode, int ncomp, bool uniform_qm, const TileGeom& tg, const MixedPushArgs& a,
+                              int grid, cudaStream_t st);
+int push_mixed_smem_bytes(const TileGeom& tg, int ncomp);
+cudaError_t push_mixed_configure_smem(const TileGeom& tg);
+int push_mixed_occupancy(const TileGeom& tg, int ncomp);
+// Single-word accumulators -> J (slots 0..2, mask & 1) and rho = background +
+// slot 3 (mask & 2); clears the converted slots.
+cudaError_t launch_convert_acc1(unsigned long long* acc, int N, const double* scale, double* J, double* rho,
+                                double n0, int ncomp_mask, cudaStream_t st, const double* bg);
 
 // acc -> real fields: J (3 x N) from slots 0..2 when ncomp_mask & 1;
 // rho = background + slot 3 when ncomp_mask & 2, the background being bg[id]

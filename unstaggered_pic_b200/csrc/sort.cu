@@ -258,6 +258,14 @@ cudaError_t sort_particles_by_tile(const TileGeom& tg, const ParticleSoA& p, lon
     make_keys_kernel<<<grid_for(np), 256, 0, st>>>(tg, p, np, Lx, Ly, inv_dx, inv_dy, shift, w.keys,
                                                    w.vals);
     count_launches(1);
+    return sort_keys_to_chunks(tg, np, w, st);
+}
+
+cudaError_t sort_keys_to_chunks(const TileGeom& tg, long np, SortWork& w, cudaStream_t st) {
+    if (np <= 0) {
+        cudaMemsetAsync(w.nchunks, 0, sizeof(int), st);
+        return cudaGetLastError();
+    }
     const long ncells = (long)tg.nx * tg.ny;
     int bits = 0;
     while ((1L << bits) < ncells) ++bits;
