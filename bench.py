@@ -75,6 +75,11 @@ IMPLICIT_DECK = dict(Lz=1.0, kappa=1.0, sigma1=1.0, sigma2=1.0, n0=1.0, spline_o
 # Algorithmic HBM bytes per particle per step of the fused push kernel: the
 # FP64 particle state x, y, P(3), v(3), v_prev(3) read once and written once.
 ALG_BYTES_PER_PARTICLE = 176
+# The mixed form's push kernel: cell (int32), offsets (2), P (3), v (3),
+# v_prev (3) in FP32 read (48 B), the same less P_z written (44 B).
+ALG_BYTES_PER_PARTICLE_MIXED = 92
+# Diagnostics columns whose mixed-vs-FP64 difference the bench line reports.
+MIXED_ERROR_COLUMNS = ("field_energy", "kinetic_energy", "total_energy", "Bz_l2", "E_l2", "J_l2", "rho_l2")
 # Reference CPU sample: same grid, 16 electrons per cell, timed step loop.
 REF_SAMPLE_PPC = 16
 REF_SAMPLE_STEPS = 2
@@ -90,6 +95,8 @@ def parse():
     ap.add_argument("--diag-stride", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision companion run of an explicit workload")
     ap.add_argument("--implicit-workload", default="weibel512_implicit",
                     help="implicit-method workload reported beside an explicit headline ('none' skips)")
     ap.add_argument("--implicit-steps", type=int, default=3,
@@ -323,22 +330,22 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
-def make_simulation(up, w):
+def make_simulation(up, w, precision="fp64"):
     if w["method"] == "cn_orbit":
         cfg = up.ImplicitConfig(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], **IMPLICIT_DECK)
     else:
         cfg = up.Config(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], method=w["method"],
-                        charge_update=w["charge_update"])
+                        charge_update=w["charge_update"], precision=precision)
     return up.Simulation(cfg)
 
 
 def advance(sim, w, steps, diag_stride):
-    """K steps of the workload's method; returns the implicit solve reports."""
+    """K steps of the workload's method; returns the implicit solve reports,
+    or the explicit diagnostics rows."""
     if w["method"] == "cn_orbit":
         _, info = sim.step_implicit(steps, diagnostics=diag_stride > 0)
         return info
-    sim.step(steps, diag_stride)
-    return None
+    return sim.step(steps, diag_stride)
 
 
 # Implicit map kernel: per launch it streams x, y, P(3), v(3) of every
@@ -406,6 +413,7 @@ def measure(args, name, steps, warmup, world, rank, dist, dev):
     e0.record(stream)
     info = advance(sim, w, steps, args.diag_stride)
     e1.record(stream)
+    rows64 = None if implicit else info
     torch.cuda.synchronize()
     clk = clocks.stop()
     t_ms = allmax(e0.elapsed_time(e1))
@@ -473,6 +481,44 @@ def measure(args, name, steps, warmup, world, rank, dist, dev):
                        "step + upic_get_particles, host wall clock, max over ranks"}
     sim.close()
 
+    # ---- mixed-precision form of the explicit step on the same input
+    mixed = None
+    if not implicit and not args.no_mixed:
+        torch.cuda.empty_cache()
+        msim = make_simulation(up, w, "mixed")
+        msim.set_stream(stream.cuda_stream)
+        msim.set_particles(host["x"], host["y"], host["P"], host["v"], host["v_prev"], host["q"], host["m"])
+        msim.init_fields(False)
+        advance(msim, w, warmup, args.diag_stride)
+        torch.cuda.synchronize()
+        barrier()
+        msim.profile_enable(True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        rows32 = advance(msim, w, steps, args.diag_stride)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tm_ms = allmax(e0.elapsed_time(e1))
+        mk_ms, mk_n, _ = msim.profile_read()
+        msim.close()
+        mpush_s = mk_ms / max(mk_n, 1) / 1e3
+        mach = ALG_BYTES_PER_PARTICLE_MIXED * np_total / mpush_s / 1e9
+        err = {}
+        for col in MIXED_ERROR_COLUMNS:
+            k = up.DIAG_COLUMNS.index(col)
+            a, b = rows32[:, k], rows64[:, k]
+            ok = np.isfinite(a) & np.isfinite(b)
+            scale = float(np.max(np.abs(b[ok]))) if ok.any() else 0.0
+            err[col] = float(np.max(np.abs(a[ok] - b[ok])) / scale) if scale > 0 else None
+        mixed = {"value": replica_throughput(world, np_total, steps, tm_ms), "unit": METRIC,
+                 "ms_per_step": tm_ms / steps, "dtype": "f32 particles, f64 field solve and energies",
+                 "roofline": {"bound": "hbm", "achieved": mach, "peak": peak, "unit": "GB/s", "frac": mach / peak,
+                              "kernel": "push_deposit_mixed_kernel", "kernel_ms": mpush_s * 1e3,
+                              "algorithmic_bytes_per_particle": ALG_BYTES_PER_PARTICLE_MIXED},
+                 "max_rel_diff_vs_fp64": err,
+                 "what": f"same plasma, same {warmup} warm-up and {steps} timed steps as the FP64 run; "
+                         "differences over the timed steps, relative to each column's largest FP64 value"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -489,6 +535,8 @@ def measure(args, name, steps, warmup, world, rank, dist, dev):
            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk}
     if solve is not None:
         out["implicit_solve"] = solve
+    if mixed is not None:
+        out["mixed"] = mixed
     return out
 
 
@@ -521,7 +569,7 @@ def run_upic(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": main["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic"}
-    for k in ("config", "roofline", "cpu_baseline", "e2e", "gpu_launches", "clocks", "implicit_solve"):
+    for k in ("config", "roofline", "cpu_baseline", "e2e", "gpu_launches", "clocks", "implicit_solve", "mixed"):
         if k in main:
             line[k] = main[k]
     if companion is not None:
