@@ -80,7 +80,7 @@ UPIC_D void fold_window1(const unsigned long long* win, int WN, const TileGeom& 
 }
 
 template <int MODE, int NCOMP, bool UNIFORM>
-__global__ void __launch_bounds__(kMThreads, 3) push_deposit_mixed_kernel(MixedPushArgs a, TileGeom tg) {
+__global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedPushArgs a, TileGeom tg) {
     constexpr int NV = MStage<NCOMP>::kNV;
     constexpr int RW = MStage<NCOMP>::kRow;
     constexpr int NPER = (NV + 31) / 32;
