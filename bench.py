@@ -330,9 +330,10 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
-def make_simulation(up, w, precision="fp64"):
+def make_simulation(up, w, precision="fp64", predictor="previous"):
     if w["method"] == "cn_orbit":
-        cfg = up.ImplicitConfig(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], **IMPLICIT_DECK)
+        cfg = up.ImplicitConfig(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], current_predictor=predictor,
+                                **IMPLICIT_DECK)
     else:
         cfg = up.Config(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], method=w["method"],
                         charge_update=w["charge_update"], precision=precision)
@@ -355,7 +356,7 @@ IMPLICIT_READ_BYTES = 64
 IMPLICIT_WRITE_BYTES = 88
 
 
-def measure(args, name, steps, warmup, world, rank, dist, dev):
+def measure(args, name, steps, warmup, world, rank, dist, dev, predictor="previous", extras=True):
     """Device-resident and end-to-end throughput of workload `name` (one
     replica per rank), the dominant kernel's roofline and the reference CPU
     sample; returns the bench-line fields."""
@@ -383,7 +384,7 @@ def measure(args, name, steps, warmup, world, rank, dist, dev):
         pinned[k] = t
     del p
     host = {k: t.numpy() for k, t in pinned.items()}
-    sim = make_simulation(up, w)
+    sim = make_simulation(up, w, predictor=predictor)
     stream = torch.cuda.current_stream()
     sim.set_stream(stream.cuda_stream)
 
@@ -452,7 +453,7 @@ def measure(args, name, steps, warmup, world, rank, dist, dev):
 
     # ---- end to end through the public API from pinned host buffers
     e2e = None
-    if not args.no_e2e:
+    if extras and not args.no_e2e:
         # the step's result is read back into pinned host buffers, as the inputs come from them
         res = {k: torch.empty((np_total,) if k in ("x", "y") else (np_total, 3), dtype=torch.float64,
                               pin_memory=True).numpy() for k in ("x", "y", "P", "v", "v_prev")}
@@ -483,7 +484,7 @@ def measure(args, name, steps, warmup, world, rank, dist, dev):
 
     # ---- mixed-precision form of the explicit step on the same input
     mixed = None
-    if not implicit and not args.no_mixed:
+    if extras and not implicit and not args.no_mixed:
         torch.cuda.empty_cache()
         msim = make_simulation(up, w, "mixed")
         msim.set_stream(stream.cuda_stream)
@@ -520,7 +521,7 @@ def measure(args, name, steps, warmup, world, rank, dist, dev):
                          "differences over the timed steps, relative to each column's largest FP64 value"}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if extras and rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             ref_ppc, ref_steps = (4, 2) if implicit else (REF_SAMPLE_PPC, REF_SAMPLE_STEPS)
             v, kind, n, secs, what = reference_sample(w, ref_ppc, ref_steps, 0, 7)
@@ -561,6 +562,14 @@ def run_upic(args):
         torch.cuda.empty_cache()
         companion = measure(args, args.implicit_workload, min(args.steps, args.implicit_steps),
                             args.warmup, world, rank, dist, dev)
+        # the same run with the extrapolated first current guess (opt-in; not in the reference)
+        torch.cuda.empty_cache()
+        extrap = measure(args, args.implicit_workload, min(args.steps, args.implicit_steps), args.warmup, world,
+                         rank, dist, dev, predictor="extrapolated", extras=False)
+        companion["predictor_extrapolated"] = {
+            "value": extrap["value"], "unit": METRIC, "ms_per_step": extrap["ms_per_step"],
+            "implicit_solve": extrap.get("implicit_solve"),
+            "what": "current_predictor = extrapolated (2 J^n - J^(n-1)); same tolerances, same plasma"}
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:

@@ -63,6 +63,14 @@ enum {
  * The implicit methods run in 2D (nz = 1). */
 enum { UPIC_METHOD_BDF1 = 1, UPIC_METHOD_BDF2 = 2, UPIC_METHOD_CN_ORBIT = 3, UPIC_METHOD_CN_ORBIT_NONREL = 4 };
 
+/* First guess of the implicit step's outer current iteration.  PREVIOUS:
+ * the last accepted current, as the reference does
+ * (nonlinear_step_uniform_subcycled, ec_pic_nyquist_projected.cpp:5887).
+ * EXTRAPOLATED: 2 J^n - J^{n-1} (the previous current on the first step
+ * after upic_init_fields); not in the reference.  The iteration still runs
+ * to the same tolerances, so only the iteration count changes. */
+enum { UPIC_PREDICTOR_PREVIOUS = 0, UPIC_PREDICTOR_EXTRAPOLATED = 1 };
+
 /* Outer nonlinear solver of the implicit method (Config::nonlinear_solver,
  * ec_pic_nyquist_projected.cpp:891). */
 enum { UPIC_SOLVER_ANDERSON = 0, UPIC_SOLVER_PICARD = 1 };
@@ -148,6 +156,9 @@ typedef struct upic_config {
     double picard_tol;
     int picard_max_iter;
     int final_consistency_sweep;
+    /* First outer-iteration guess of the implicit GM-HC-CN step's mesh
+     * current (UPIC_PREDICTOR_*). */
+    int current_predictor;
 } upic_config;
 
 typedef struct upic_ctx upic_ctx;

@@ -278,3 +278,33 @@ def test_step_diagnostics_match_reference(case):
                     assert abs(a - b) <= TOL_STEP * (s + 1) * abs(b) + TOL_ROUNDOFF, (s, name, a, b)
     finally:
         sim.close()
+
+
+def test_extrapolated_predictor_same_solution():
+    """current_predictor = extrapolated (2 J^n - J^(n-1)) converges to the
+    reference's solution at the same tolerances, in no more outer
+    iterations over the run than the reference's previous-current guess."""
+    g = dict(np.load(os.path.join(GOLD, "p3_run_o2_anderson.npz")))
+    nsteps = int(g["iparams"][12])
+    nyq = bool(g["iparams"][6])
+    iters = {}
+    for pred in ("previous", "extrapolated"):
+        cfg = config_from(g["dparams"], g["iparams"])
+        cfg.current_predictor = pred
+        sim = up.Simulation(cfg)
+        x, v = g["in_x"], g["in_v"]
+        n = len(g["in_q"])
+        sim.set_particles(x[:, 0], x[:, 1], np.zeros((n, 3)), v, v, g["in_q"], g["in_m"])
+        try:
+            sim.init_fields()
+            diag, info = sim.step_implicit(nsteps)
+            for s in range(nsteps):
+                compare_diag(diag[s], g["diag"][s + 1], nyq, TOL_STEP * (s + 1))
+            fields = np.stack([sim.field(f) for f in FIELD_ORDER])
+            for k, f in enumerate(FIELD_ORDER):
+                assert family_err(fields, g["fields"], k) < TOL_STEP * nsteps, f
+            iters[pred] = info[:, 0]
+        finally:
+            sim.close()
+    assert iters["extrapolated"][0] == iters["previous"][0]  # no history on the first step
+    assert iters["extrapolated"].sum() <= iters["previous"].sum(), iters

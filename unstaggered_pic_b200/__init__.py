@@ -23,6 +23,8 @@ CHARGE_UPDATES = {"conserving": 0, "naive": 1}
 # FP64 throughout, or the mixed form of the explicit step (FP32 particles with
 # cell-relative offsets, FP64 field solve and diagnostics)
 PRECISIONS = {"fp64": 0, "mixed": 1}
+# first guess of the implicit step's outer current iteration
+PREDICTORS = {"previous": 0, "extrapolated": 1}
 NONLINEAR_SOLVERS = {"anderson_quasi_newton": 0, "anderson": 0, "picard": 1}
 FIELDS = {"phi": 0, "Ax": 1, "Ay": 2, "Az": 3, "rho": 4, "Jx": 5, "Jy": 6, "Jz": 7,
           "psi": 8, "Ux": 9, "Uy": 10, "Uz": 11}
@@ -113,8 +115,9 @@ class ImplicitConfig:
                  nonlinear_atol=1.0e-13, nonlinear_max_iter=32, anderson_memory=4, anderson_start=2,
                  anderson_damping=0.7, anderson_regularization=1.0e-12, anderson_growth_limit=1.2,
                  uniform_local_rtol=1.0e-11, uniform_local_atol=1.0e-13, uniform_local_max_iter=24,
-                 uniform_local_damping=1.0, perturbation_mode=1, tile=0, guard=-1):
+                 uniform_local_damping=1.0, perturbation_mode=1, tile=0, guard=-1, current_predictor="previous"):
         self.method = "cn_orbit"
+        self.current_predictor = current_predictor
         self.nx, self.ny, self.Lx, self.Ly, self.Lz, self.dt = nx, ny, Lx, Ly, Lz, dt
         self.kappa, self.sigma1, self.sigma2, self.n0 = kappa, sigma1, sigma2, n0
         self.spline_order, self.orbit_quad_order = spline_order, orbit_quad_order
@@ -153,6 +156,8 @@ class ImplicitConfig:
         cfg.local_damping = float(self.uniform_local_damping)
         cfg.perturbation_mode = int(self.perturbation_mode)
         cfg.tile, cfg.guard = int(self.tile), int(self.guard)
+        cp = self.current_predictor
+        cfg.current_predictor = PREDICTORS[cp] if isinstance(cp, str) else int(cp)
         return cfg
 
 

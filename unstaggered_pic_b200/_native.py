@@ -87,6 +87,7 @@ class UpicConfig(ctypes.Structure):
         ("perturbation_mode", ctypes.c_int),
         ("picard_tol", ctypes.c_double), ("picard_max_iter", ctypes.c_int),
         ("final_consistency_sweep", ctypes.c_int),
+        ("current_predictor", ctypes.c_int),
     ]
 
 

@@ -554,6 +554,7 @@ int upic_config_default(upic_config* cfg) {
     cfg->picard_tol = 1.0e-11;
     cfg->picard_max_iter = 16;
     cfg->final_consistency_sweep = 1;
+    cfg->current_predictor = UPIC_PREDICTOR_PREVIOUS;
     return UPIC_OK;
 }
 
@@ -606,6 +607,8 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
         if (!(cfg->anderson_damping > 0) || !(cfg->local_damping > 0) || !(cfg->anderson_growth_limit > 0) ||
             !(cfg->anderson_regularization >= 0))
             return fail(nullptr, UPIC_ERR_CONFIG, "damping and growth limits must be positive");
+        if (cfg->current_predictor != UPIC_PREDICTOR_PREVIOUS && cfg->current_predictor != UPIC_PREDICTOR_EXTRAPOLATED)
+            return fail(nullptr, UPIC_ERR_CONFIG, "current_predictor must be previous or extrapolated");
     } else {
         if (cfg->charge_update != UPIC_CHARGE_CONSERVING && cfg->charge_update != UPIC_CHARGE_NAIVE)
             return fail(nullptr, UPIC_ERR_CONFIG, "charge_update must be conserving or naive");
@@ -756,7 +759,7 @@ std::vector<double> config_signature(const upic_config& f) {
             (double)f.local_max_iter, f.nonlinear_rtol, f.nonlinear_atol, f.anderson_damping,
             f.anderson_regularization, f.anderson_growth_limit, f.local_rtol, f.local_atol, f.local_damping,
             (double)f.perturbation_mode, f.picard_tol, (double)f.picard_max_iter,
-            (double)f.final_consistency_sweep};
+            (double)f.final_consistency_sweep, (double)f.current_predictor};
 }
 
 // Everything the next explicit step reads: the particle set in its current

@@ -95,6 +95,9 @@ struct ImplicitState {
     bool picard = false;
     double *gx = nullptr, *gy = nullptr, *gz = nullptr;  // velocity guess (sorted order)
     double* Jprev = nullptr;                              // 3 x N
+    // current of the step before the last (UPIC_PREDICTOR_EXTRAPOLATED)
+    double* Jold = nullptr;                               // 3 x N
+    bool have_Jold = false;
     unsigned long long* pstat = nullptr;                  // path statistics counters (4)
     int* perr = nullptr;
     double vb_limit = 0.0;  // bound on |vbar| components of the fixed-point deposit
@@ -746,7 +749,10 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
     UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec + 3 * (size_t)N, sizeof(double2) * 3 * N,
                                  cudaMemcpyDeviceToDevice, c->st));
     UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 3, 1, c->st, nullptr, 2, s.rec, kIRec, kIRecAn));
-    UPIC_CUDA(c, cudaMemcpyAsync(s.guess, s.J, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
+    if (cf.current_predictor == UPIC_PREDICTOR_EXTRAPOLATED && s.have_Jold)
+        UPIC_CUDA(c, launch_extrapolate(n3, s.J, s.Jold, s.guess, c->st));
+    else
+        UPIC_CUDA(c, cudaMemcpyAsync(s.guess, s.J, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
     bool finite = true;
     if ((rc = all_finite(c, s, s.guess, finite))) return rc;
     if (!finite) return fail(c, UPIC_ERR_NONFINITE, "nonfinite initial macro-current predictor");
@@ -858,6 +864,10 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
     }
     s.cur = 1 - s.cur;
     std::swap(s.spec, s.spec_out);
+    if (cf.current_predictor == UPIC_PREDICTOR_EXTRAPOLATED) {
+        UPIC_CUDA(c, cudaMemcpyAsync(s.Jold, s.J, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
+        s.have_Jold = true;
+    }
     UPIC_CUDA(c, cudaMemcpyAsync(s.J, s.map, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
     if (info) {
         info[UPIC_INFO_ITERATIONS] = iterations;
@@ -967,6 +977,8 @@ int implicit_create(upic_ctx* c) {
         (rc = dalloc(c, &s->dflag, 1)) || (rc = dalloc(c, &s->pstat, 4)) || (rc = dalloc(c, &s->perr, 1)))
         return rc;
     if (s->picard && (rc = dalloc(c, &s->Jprev, 3 * (size_t)N))) return rc;
+    if (c->cfg.current_predictor == UPIC_PREDICTOR_EXTRAPOLATED && (rc = dalloc(c, &s->Jold, 3 * (size_t)N)))
+        return rc;
     for (int k = 0; k < kHist; ++k)
         if ((rc = dalloc(c, &s->hx[k], 3 * (size_t)N)) || (rc = dalloc(c, &s->hr[k], 3 * (size_t)N))) return rc;
     if (cudaMallocHost(&s->hnorm, sizeof(NormSums)) != cudaSuccess ||
@@ -1105,6 +1117,11 @@ int implicit_state_io(upic_ctx* c, StateIO& io) {
     if ((rc = state_device(c, io, s.spec, sizeof(double2) * 9 * N)) ||
         (rc = state_device(c, io, s.J, sizeof(double) * 3 * N)))
         return rc;
+    if (s.Jold) {
+        int have = s.have_Jold ? 1 : 0;
+        if ((rc = state_value(c, io, have)) || (rc = state_device(c, io, s.Jold, sizeof(double) * 3 * N))) return rc;
+        s.have_Jold = have != 0;
+    }
     return 0;
 }
 
@@ -1187,6 +1204,7 @@ int implicit_init_fields(upic_ctx* c, double* diag_row) {
     }
     s.ready = true;
     s.steps = 0;
+    s.have_Jold = false;
     c->steps = 0;
     c->fields_ready = true;
     if ((rc = sync(c))) return rc;
