@@ -159,6 +159,13 @@ typedef struct upic_config {
     /* First outer-iteration guess of the implicit GM-HC-CN step's mesh
      * current (UPIC_PREDICTOR_*). */
     int current_predictor;
+    /* Implicit GM-HC-CN step: with 1, each particle's local fixed point starts
+     * from its orbit velocity of the previous current-map evaluation of the
+     * same step instead of from v^n (the reference's start,
+     * solve_local_particle_substep, ec_pic_nyquist_projected.cpp:4930).  The
+     * local and outer tolerances are unchanged; results agree with the
+     * reference to those tolerances, not bit for bit.  Default 0. */
+    int local_warm_start;
 } upic_config;
 
 typedef struct upic_ctx upic_ctx;

@@ -308,3 +308,36 @@ def test_extrapolated_predictor_same_solution():
             sim.close()
     assert iters["extrapolated"][0] == iters["previous"][0]  # no history on the first step
     assert iters["extrapolated"].sum() <= iters["previous"].sum(), iters
+
+
+@pytest.mark.parametrize("case", ["p3_run_o2_anderson", "p3_run_o3_picard", "p3_run_two_species"])
+def test_local_warm_start_same_solution(case):
+    """local_warm_start = 1 (each local fixed point starts from the previous
+    map evaluation's orbit velocity) converges to the reference's solution at
+    the same tolerances with fewer local iterations."""
+    g = dict(np.load(os.path.join(GOLD, case + ".npz")))
+    nsteps = int(g["iparams"][12])
+    nyq = bool(g["iparams"][6])
+    local = {}
+    for warm in (False, True):
+        cfg = config_from(g["dparams"], g["iparams"])
+        cfg.local_warm_start = warm
+        sim = up.Simulation(cfg)
+        x, v = g["in_x"], g["in_v"]
+        n = len(g["in_q"])
+        sim.set_particles(x[:, 0], x[:, 1], np.zeros((n, 3)), v, v, g["in_q"], g["in_m"])
+        try:
+            sim.init_fields()
+            diag, info = sim.step_implicit(nsteps)
+            for s in range(nsteps):
+                compare_diag(diag[s], g["diag"][s + 1], nyq, TOL_STEP * (s + 1))
+            fields = np.stack([sim.field(f) for f in FIELD_ORDER])
+            for k, f in enumerate(FIELD_ORDER):
+                assert family_err(fields, g["fields"], k) < TOL_STEP * nsteps, f
+            p = sim.get_particles()
+            assert relerr(p["v"], g["out_v"]) < TOL_STEP * nsteps
+            local[warm] = info[:, up.SOLVE_INFO_COLUMNS.index("local_particle_iterations_mean")]
+        finally:
+            sim.close()
+    # the final consistency evaluation's mean local iterations drop
+    assert np.all(local[True] < local[False]), local

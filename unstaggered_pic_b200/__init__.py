@@ -115,9 +115,10 @@ class ImplicitConfig:
                  nonlinear_atol=1.0e-13, nonlinear_max_iter=32, anderson_memory=4, anderson_start=2,
                  anderson_damping=0.7, anderson_regularization=1.0e-12, anderson_growth_limit=1.2,
                  uniform_local_rtol=1.0e-11, uniform_local_atol=1.0e-13, uniform_local_max_iter=24,
-                 uniform_local_damping=1.0, perturbation_mode=1, tile=0, guard=-1, current_predictor="previous"):
+                 uniform_local_damping=1.0, perturbation_mode=1, tile=0, guard=-1, current_predictor="previous",
+                 local_warm_start=False):
         self.method = "cn_orbit"
-        self.current_predictor = current_predictor
+        self.current_predictor, self.local_warm_start = current_predictor, local_warm_start
         self.nx, self.ny, self.Lx, self.Ly, self.Lz, self.dt = nx, ny, Lx, Ly, Lz, dt
         self.kappa, self.sigma1, self.sigma2, self.n0 = kappa, sigma1, sigma2, n0
         self.spline_order, self.orbit_quad_order = spline_order, orbit_quad_order
@@ -158,6 +159,7 @@ class ImplicitConfig:
         cfg.tile, cfg.guard = int(self.tile), int(self.guard)
         cp = self.current_predictor
         cfg.current_predictor = PREDICTORS[cp] if isinstance(cp, str) else int(cp)
+        cfg.local_warm_start = int(bool(self.local_warm_start))
         return cfg
 
 

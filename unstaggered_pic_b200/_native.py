@@ -88,6 +88,7 @@ class UpicConfig(ctypes.Structure):
         ("picard_tol", ctypes.c_double), ("picard_max_iter", ctypes.c_int),
         ("final_consistency_sweep", ctypes.c_int),
         ("current_predictor", ctypes.c_int),
+        ("local_warm_start", ctypes.c_int),
     ]
 
 

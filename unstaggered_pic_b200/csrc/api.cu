@@ -555,6 +555,7 @@ int upic_config_default(upic_config* cfg) {
     cfg->picard_max_iter = 16;
     cfg->final_consistency_sweep = 1;
     cfg->current_predictor = UPIC_PREDICTOR_PREVIOUS;
+    cfg->local_warm_start = 0;
     return UPIC_OK;
 }
 
@@ -759,7 +760,7 @@ std::vector<double> config_signature(const upic_config& f) {
             (double)f.local_max_iter, f.nonlinear_rtol, f.nonlinear_atol, f.anderson_damping,
             f.anderson_regularization, f.anderson_growth_limit, f.local_rtol, f.local_atol, f.local_damping,
             (double)f.perturbation_mode, f.picard_tol, (double)f.picard_max_iter,
-            (double)f.final_consistency_sweep, (double)f.current_predictor};
+            (double)f.final_consistency_sweep, (double)f.current_predictor, (double)f.local_warm_start};
 }
 
 // Everything the next explicit step reads: the particle set in its current

@@ -98,6 +98,9 @@ struct ImplicitState {
     // current of the step before the last (UPIC_PREDICTOR_EXTRAPOLATED)
     double* Jold = nullptr;                               // 3 x N
     bool have_Jold = false;
+    // local_warm_start: gx/gy/gz keep the orbit velocities of the last map
+    // evaluation of the current step
+    bool warm_valid = false;
     unsigned long long* pstat = nullptr;                  // path statistics counters (4)
     int* perr = nullptr;
     double vb_limit = 0.0;  // bound on |vbar| components of the fixed-point deposit
@@ -197,7 +200,7 @@ int alloc_particles(upic_ctx* c, ImplicitState& s, long cap, bool with_qm) {
         if ((rc = dalloc(c, &s.bx[k], cap)) || (rc = dalloc(c, &s.by[k], cap)) || (rc = dalloc(c, &s.bz[k], cap)))
             return rc;
     }
-    if (s.picard &&
+    if ((s.picard || c->cfg.local_warm_start) &&
         ((rc = dalloc(c, &s.gx, cap)) || (rc = dalloc(c, &s.gy, cap)) || (rc = dalloc(c, &s.gz, cap))))
         return rc;
     if ((rc = alloc_sortwork(c, s.sw, cap, s.tg))) return rc;
@@ -301,6 +304,16 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
     a.qtab = s.qtab;
     a.nq = s.nq;
     a.mnq = s.mnq;
+    if (cf.local_warm_start) {
+        if (s.warm_valid) {
+            a.warm_x = s.gx;
+            a.warm_y = s.gy;
+            a.warm_z = s.gz;
+        }
+        a.keep_x = s.gx;
+        a.keep_y = s.gy;
+        a.keep_z = s.gz;
+    }
     if (s.np > 0) {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (c->profiling) {
@@ -338,6 +351,7 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
                       s.hstats->failures, key >> 8, reason < 7 ? names[reason] : "?", cf.local_max_iter);
         return fail(c, UPIC_ERR_LOCAL_PARTICLE, buf);
     }
+    if (cf.local_warm_start) s.warm_valid = true;
     return 0;
 }
 
@@ -745,6 +759,7 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
     const int N = c->N, n3 = 3 * N;
     int rc;
     if (s.np > 0 && (rc = sort_active(c, s))) return rc;
+    s.warm_valid = false;  // the sort reorders the particles
     // A^n records for the orbit D_A and the start-point gather
     UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec + 3 * (size_t)N, sizeof(double2) * 3 * N,
                                  cudaMemcpyDeviceToDevice, c->st));

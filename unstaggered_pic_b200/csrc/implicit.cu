@@ -642,6 +642,11 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
 #pragma unroll
                 for (int c = 0; c < 3; ++c) in.pstart[c] = in.P0[c] - in.q * in.A0p[c];
                 double guess[3] = {a.vx[p], a.vy[p], a.vz[p]};
+                if (a.warm_x) {
+                    guess[0] = a.warm_x[p];
+                    guess[1] = a.warm_y[p];
+                    guess[2] = a.warm_z[p];
+                }
                 // solve_local_particle_substep (:4930)
                 int reason = kLocalMaxIter;
                 int iters = 0;
@@ -697,6 +702,11 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                     vb[0] = guess[0];
                     vb[1] = guess[1];
                     vb[2] = guess[2];
+                    if (a.keep_x) {
+                        a.keep_x[p] = guess[0];
+                        a.keep_y[p] = guess[1];
+                        a.keep_z[p] = guess[2];
+                    }
                     if (a.write_state) {
                         a.ox[p] = o.x1;
                         a.oy[p] = o.y1;

@@ -74,6 +74,10 @@ struct ImplicitMapArgs {
     // counted as a failure, since its deposit could leave the fixed-point range
     const double *gx, *gy, *gz;
     double vb_limit;
+    // local fixed point of the relativistic map: start guesses (null: v^n)
+    // and where to keep each particle's converged orbit velocity (null: not kept)
+    const double *warm_x, *warm_y, *warm_z;
+    double *keep_x, *keep_y, *keep_z;
 };
 
 // split: knot splitting of the orbit (ImplicitMapArgs::split); picard: the
