@@ -166,6 +166,14 @@ typedef struct upic_config {
      * local and outer tolerances are unchanged; results agree with the
      * reference to those tolerances, not bit for bit.  Default 0. */
     int local_warm_start;
+    /* Implicit GM-HC-CN step: selective particle sub-cycling fallback
+     * (Config::selective_particle_fallback / selective_particle_max_substeps,
+     * nonlinear_step_selective_particle_fallback, ec_pic_nyquist_projected.cpp
+     * :6328).  When a particle's local solve fails over the full dt, failing
+     * particles are advanced in 2, 4, ... up to max_substeps (a power of two
+     * <= 64) chained substeps and the outer current solve restarts. */
+    int selective_particle_fallback;
+    int selective_particle_max_substeps;
 } upic_config;
 
 typedef struct upic_ctx upic_ctx;
@@ -198,7 +206,11 @@ enum {
      * statistics of the accepted orbits (crossing particles, average and
      * maximum segments per orbit), the _diagnostics.csv columns of both. */
     UPIC_INFO_CURRENT_ERROR, UPIC_INFO_VELOCITY_ERROR, UPIC_INFO_CROSSING_PARTICLES,
-    UPIC_INFO_AVG_PATH_SEGMENTS, UPIC_INFO_MAX_PATH_SEGMENTS, UPIC_INFO_COUNT
+    UPIC_INFO_AVG_PATH_SEGMENTS, UPIC_INFO_MAX_PATH_SEGMENTS,
+    /* selective sub-cycling (NonlinearSolveInfo::selective_*): fallback used,
+     * refinement restarts, refined particles, total particle substeps */
+    UPIC_INFO_SELECTIVE_FALLBACK_USED, UPIC_INFO_SELECTIVE_RESTARTS, UPIC_INFO_SELECTIVE_REFINED,
+    UPIC_INFO_SELECTIVE_SUBSTEPS, UPIC_INFO_COUNT
 };
 
 /* Step diagnostics of the implicit method: StepDiagnostics of

@@ -28,6 +28,12 @@ enum {
     I_LOC_MAXIT, I_SOLVER, I_NSTEPS, I_MODE, I_COUNT
 };
 constexpr int kDiag = 23;
+// selective particle sub-cycling fallback of the next ref_p3_run
+// (ref_p3_set_fallback) and its per-step report (ref_p3_selective_info)
+bool g_fallback = false;
+int g_fallback_max = 64;
+std::vector<double> g_selective;  // per step: used, restarts, refined, total substeps
+
 constexpr int kInfo = 8;
 constexpr int kStepDiag = 17;
 
@@ -56,7 +62,8 @@ Config make_cfg(const double* d, const int* ip) {
     c.uniform_local_max_iter = ip[I_LOC_MAXIT];
     c.uniform_local_damping = d[D_LOC_DAMP];
     c.uniform_particle_subcycling = false;
-    c.selective_particle_fallback = false;
+    c.selective_particle_fallback = g_fallback;
+    c.selective_particle_max_substeps = g_fallback_max;
     c.adaptive_dt = false;
     c.run_unit_tests = false;
     c.output_prefix = "/tmp/upic_ref_p3";
@@ -93,6 +100,22 @@ void copy_vec3(const std::vector<Vec3>& a, double* out) {
 }  // namespace
 
 extern "C" {
+
+// Enable the reference's selective particle sub-cycling fallback
+// (nonlinear_step_selective_particle_fallback, :6328) for later runs.
+int ref_p3_set_fallback(int enable, int max_substeps) {
+    g_fallback = enable != 0;
+    g_fallback_max = max_substeps;
+    return 0;
+}
+
+// Per step of the last ref_p3_run: selective_fallback_used,
+// selective_refinement_restarts, selective_refined_particles,
+// selective_total_particle_substeps (NonlinearSolveInfo).
+int ref_p3_selective_info(double* out, int nsteps) {
+    for (int k = 0; k < 4 * nsteps && k < (int)g_selective.size(); ++k) out[k] = g_selective[k];
+    return 0;
+}
 
 // Gauss-Legendre nodes and weights on [0,1] (gauss_legendre_01, :2479).
 int ref_p3_gauss_legendre(int n, double* s, double* w) {
@@ -197,6 +220,7 @@ int ref_p3_run(const double* d, const int* ip, long np, double* x, double* v, do
         const int mode = ip[I_MODE];
         if (diag) store_diag(compute_diagnostics(st, g, c.sigma1, c.sigma2, c.kappa, mode), diag);
         const auto t0 = std::chrono::steady_clock::now();
+        g_selective.assign(4 * (std::size_t)std::max(ip[I_NSTEPS], 0), 0.0);
         for (int s = 1; s <= ip[I_NSTEPS]; ++s) {
             std::vector<NonlinearHistoryEntry> hist;
             NonlinearSolveInfo si;
@@ -215,6 +239,11 @@ int ref_p3_run(const double* d, const int* ip, long np, double* x, double* v, do
                 o[5] = si.local_particle_iterations_mean; o[6] = si.anderson_steps;
                 o[7] = si.picard_fallback_steps;
             }
+            double* sl = g_selective.data() + 4 * (std::size_t)(s - 1);
+            sl[0] = si.selective_fallback_used ? 1.0 : 0.0;
+            sl[1] = si.selective_refinement_restarts;
+            sl[2] = (double)si.selective_refined_particles;
+            sl[3] = (double)si.selective_total_particle_substeps;
         }
         const auto t1 = std::chrono::steady_clock::now();
         if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();

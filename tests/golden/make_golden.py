@@ -137,6 +137,20 @@ P3_CASES = [
 ]
 
 
+# Implicit runs that need the selective particle sub-cycling fallback (a
+# small particle_local_max_iter makes some local solves fail over the full
+# dt): (name, problem keywords, particles per cell, thermal spreads,
+# fallback max_substeps).
+P3_FALLBACK_CASES = [
+    ("p3_fallback_few", dict(nx=16, ny=16, Lx=2 * np.pi, Ly=2 * np.pi, dt=0.2, order=2, nq=8, nyquist=True,
+                             n_steps=2, loc_maxit=5), 8, (0.3, 0.3, 0.0), 64),
+    ("p3_fallback_some", dict(nx=16, ny=16, Lx=2 * np.pi, Ly=2 * np.pi, dt=0.1, order=2, nq=8, nyquist=True,
+                              n_steps=2, loc_maxit=4), 8, (0.5, 0.5, 0.0), 64),
+    ("p3_fallback_many_o3", dict(nx=16, ny=16, Lx=2 * np.pi, Ly=2 * np.pi, dt=0.3, order=3, nq=8, nyquist=True,
+                                 n_steps=2, loc_maxit=5), 8, (0.3, 0.3, 0.1), 64),
+]
+
+
 # Orbit kernels: (order, knot splitting, Gauss points)
 P3_ORBIT_CASES = [(2, True, 8), (2, False, 8), (1, True, 4), (3, True, 6)]
 
@@ -204,6 +218,23 @@ def p3_main():
                             diag=out["diag"], info=out["info"], fields=out["fields"],
                             step_diag=out["step_diag"])
         print(name, "iterations", out["info"][:, 0].tolist())
+    for k, (name, kw, ppc, uth, max_sub) in enumerate(P3_FALLBACK_CASES):
+        rng = np.random.default_rng(20261220 + k)
+        prob = ol.P3Problem(**kw)
+        x, v, q, m = ol.p3_particles(rng, prob.nx, prob.ny, ppc, prob.Lx, prob.Ly, uth=uth, Lz=prob.Lz)
+        lib.ref_p3_set_fallback(1, max_sub)
+        try:
+            out = ol.p3_run(lib.ref_p3_run, prob, x, v, q, m)
+            sel = np.zeros(4 * prob.n_steps)
+            lib.ref_p3_selective_info(ol.ptr(sel), prob.n_steps)
+        finally:
+            lib.ref_p3_set_fallback(0, 64)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), dparams=prob.dparams(), iparams=prob.iparams(),
+                            in_x=x, in_v=v, in_q=q, in_m=m, max_substeps=max_sub,
+                            **{"out_" + c: out[c] for c in ("x", "v", "P", "v_prev", "vbar")},
+                            diag=out["diag"], info=out["info"], fields=out["fields"],
+                            selective=sel.reshape(prob.n_steps, 4))
+        print(name, "iterations", out["info"][:, 0].tolist(), "selective", sel.tolist())
 
 
 # Non-relativistic implicit (Project1) runs: (name, problem keywords,

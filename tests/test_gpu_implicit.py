@@ -341,3 +341,74 @@ def test_local_warm_start_same_solution(case):
             sim.close()
     # the final consistency evaluation's mean local iterations drop
     assert np.all(local[True] < local[False]), local
+
+
+FALLBACK_CASES = ["p3_fallback_few", "p3_fallback_some", "p3_fallback_many_o3"]
+
+
+@pytest.mark.parametrize("case", FALLBACK_CASES)
+def test_selective_fallback_matches_reference(case):
+    """Runs where some particles' local solves fail over the full dt: with
+    selective_particle_fallback the failing particles are sub-cycled (2, 4,
+    ... substeps) and the outer solve restarts, as the reference's
+    nonlinear_step_selective_particle_fallback does; the same particles are
+    refined the same number of times and the state agrees to the solver
+    tolerance."""
+    g = dict(np.load(os.path.join(GOLD, case + ".npz")))
+    cfg = config_from(g["dparams"], g["iparams"])
+    cfg.selective_particle_fallback = True
+    cfg.selective_particle_max_substeps = int(g["max_substeps"])
+    nsteps = int(g["iparams"][12])
+    sim, _ = None, None
+    sim = up.Simulation(cfg)
+    x, v = g["in_x"], g["in_v"]
+    n = len(g["in_q"])
+    sim.set_particles(x[:, 0], x[:, 1], np.zeros((n, 3)), v, v, g["in_q"], g["in_m"])
+    cols = up.SOLVE_INFO_COLUMNS
+    try:
+        sim.init_fields()
+        diag, info, sd = sim.step_implicit(nsteps, step_diagnostics=True)
+        for s in range(nsteps):
+            compare_diag(diag[s], g["diag"][s + 1], True, TOL_STEP * (s + 1))
+        sel = g["selective"]
+        got = info[:, [cols.index(c) for c in ("selective_fallback_used", "selective_refinement_restarts",
+                                               "selective_refined_particles", "selective_total_particle_substeps")]]
+        assert np.array_equal(got, sel), (got, sel)
+        assert np.all(np.abs(info[:, 0] - g["info"][:, 0]) <= 1), (info[:, 0], g["info"][:, 0])
+        assert np.all(np.isnan(sd))  # sub-cycled particles: single-orbit balances do not apply
+        tol = TOL_STEP * nsteps
+        fields = np.stack([sim.field(f) for f in FIELD_ORDER])
+        for k, f in enumerate(FIELD_ORDER):
+            assert family_err(fields, g["fields"], k) < tol, (f, family_err(fields, g["fields"], k))
+        p = sim.get_particles()
+        assert periodic_err(p["x"], g["out_x"][:, 0], cfg.Lx) < tol * cfg.Lx
+        assert periodic_err(p["y"], g["out_x"][:, 1], cfg.Ly) < tol * cfg.Ly
+        assert relerr(p["v"], g["out_v"]) < tol
+        assert relerr(p["P"], g["out_P"]) < tol
+        assert relerr(p["v_prev"], g["out_v_prev"]) < tol
+    finally:
+        sim.close()
+
+
+def test_selective_fallback_limits():
+    """Without the fallback a failing local solve ends the step
+    (UPIC_ERR_LOCAL_PARTICLE); with max_substeps = 1 nothing can be refined
+    and the step fails as the reference's exhausted fallback does."""
+    g = dict(np.load(os.path.join(GOLD, "p3_fallback_some.npz")))
+    x, v = g["in_x"], g["in_v"]
+    n = len(g["in_q"])
+    for fallback, maxsub, code, text in ((False, 64, -7, "local particle solve failed"),
+                                         (True, 1, -6, "selective particle fallback reached h=dt/1")):
+        cfg = config_from(g["dparams"], g["iparams"])
+        cfg.selective_particle_fallback = fallback
+        cfg.selective_particle_max_substeps = maxsub
+        with up.Simulation(cfg) as sim:
+            sim.set_particles(x[:, 0], x[:, 1], np.zeros((n, 3)), v, v, g["in_q"], g["in_m"])
+            sim.init_fields()
+            with pytest.raises(up.UpicError) as e:
+                sim.step_implicit(1)
+            assert e.value.code == code and text in str(e.value), str(e.value)
+    with pytest.raises(up.UpicError) as e:
+        up.Simulation(up.ImplicitConfig(nx=8, ny=8, selective_particle_fallback=True,
+                                        selective_particle_max_substeps=3))
+    assert e.value.code == -1

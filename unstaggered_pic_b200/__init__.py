@@ -55,7 +55,8 @@ SOLVE_INFO_COLUMNS = ["iterations", "converged", "final_rms_residual", "final_ma
                       "local_particle_iterations_max", "local_particle_iterations_mean",
                       "anderson_steps", "picard_fallback_steps", "picard_current_error",
                       "picard_velocity_error", "crossing_particles", "avg_path_segments",
-                      "max_path_segments"]
+                      "max_path_segments", "selective_fallback_used", "selective_refinement_restarts",
+                      "selective_refined_particles", "selective_total_particle_substeps"]
 
 
 class UpicError(RuntimeError):
@@ -116,9 +117,11 @@ class ImplicitConfig:
                  anderson_damping=0.7, anderson_regularization=1.0e-12, anderson_growth_limit=1.2,
                  uniform_local_rtol=1.0e-11, uniform_local_atol=1.0e-13, uniform_local_max_iter=24,
                  uniform_local_damping=1.0, perturbation_mode=1, tile=0, guard=-1, current_predictor="previous",
-                 local_warm_start=False):
+                 local_warm_start=False, selective_particle_fallback=False, selective_particle_max_substeps=64):
         self.method = "cn_orbit"
         self.current_predictor, self.local_warm_start = current_predictor, local_warm_start
+        self.selective_particle_fallback = selective_particle_fallback
+        self.selective_particle_max_substeps = selective_particle_max_substeps
         self.nx, self.ny, self.Lx, self.Ly, self.Lz, self.dt = nx, ny, Lx, Ly, Lz, dt
         self.kappa, self.sigma1, self.sigma2, self.n0 = kappa, sigma1, sigma2, n0
         self.spline_order, self.orbit_quad_order = spline_order, orbit_quad_order
@@ -160,6 +163,8 @@ class ImplicitConfig:
         cp = self.current_predictor
         cfg.current_predictor = PREDICTORS[cp] if isinstance(cp, str) else int(cp)
         cfg.local_warm_start = int(bool(self.local_warm_start))
+        cfg.selective_particle_fallback = int(bool(self.selective_particle_fallback))
+        cfg.selective_particle_max_substeps = int(self.selective_particle_max_substeps)
         return cfg
 
 

@@ -89,6 +89,7 @@ class UpicConfig(ctypes.Structure):
         ("final_consistency_sweep", ctypes.c_int),
         ("current_predictor", ctypes.c_int),
         ("local_warm_start", ctypes.c_int),
+        ("selective_particle_fallback", ctypes.c_int), ("selective_particle_max_substeps", ctypes.c_int),
     ]
 
 

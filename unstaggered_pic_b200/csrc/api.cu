@@ -556,6 +556,8 @@ int upic_config_default(upic_config* cfg) {
     cfg->final_consistency_sweep = 1;
     cfg->current_predictor = UPIC_PREDICTOR_PREVIOUS;
     cfg->local_warm_start = 0;
+    cfg->selective_particle_fallback = 0;
+    cfg->selective_particle_max_substeps = 64;
     return UPIC_OK;
 }
 
@@ -610,6 +612,12 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
             return fail(nullptr, UPIC_ERR_CONFIG, "damping and growth limits must be positive");
         if (cfg->current_predictor != UPIC_PREDICTOR_PREVIOUS && cfg->current_predictor != UPIC_PREDICTOR_EXTRAPOLATED)
             return fail(nullptr, UPIC_ERR_CONFIG, "current_predictor must be previous or extrapolated");
+        {
+            const int ms = cfg->selective_particle_max_substeps;
+            if (ms < 1 || ms > 64 || (ms & (ms - 1)) != 0)
+                return fail(nullptr, UPIC_ERR_CONFIG,
+                            "selective particle fallback requires a power-of-two max_substeps in [1,64]");
+        }
     } else {
         if (cfg->charge_update != UPIC_CHARGE_CONSERVING && cfg->charge_update != UPIC_CHARGE_NAIVE)
             return fail(nullptr, UPIC_ERR_CONFIG, "charge_update must be conserving or naive");
@@ -760,7 +768,8 @@ std::vector<double> config_signature(const upic_config& f) {
             (double)f.local_max_iter, f.nonlinear_rtol, f.nonlinear_atol, f.anderson_damping,
             f.anderson_regularization, f.anderson_growth_limit, f.local_rtol, f.local_atol, f.local_damping,
             (double)f.perturbation_mode, f.picard_tol, (double)f.picard_max_iter,
-            (double)f.final_consistency_sweep, (double)f.current_predictor, (double)f.local_warm_start};
+            (double)f.final_consistency_sweep, (double)f.current_predictor, (double)f.local_warm_start,
+            (double)f.selective_particle_fallback, (double)f.selective_particle_max_substeps};
 }
 
 // Everything the next explicit step reads: the particle set in its current

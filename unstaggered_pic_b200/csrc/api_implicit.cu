@@ -101,6 +101,14 @@ struct ImplicitState {
     // local_warm_start: gx/gy/gz keep the orbit velocities of the last map
     // evaluation of the current step
     bool warm_valid = false;
+    // selective particle sub-cycling (selective_particle_fallback): substeps
+    // per sorted particle (device and host), the refined list, the failing
+    // particles of the last map evaluation
+    int *nsub = nullptr, *refined = nullptr, *failed = nullptr, *nfailed = nullptr;
+    std::vector<int> h_nsub;
+    bool layout_active = false;
+    int nref = 0, last_refined = 0;
+    long total_substeps = 0;
     unsigned long long* pstat = nullptr;                  // path statistics counters (4)
     int* perr = nullptr;
     double vb_limit = 0.0;  // bound on |vbar| components of the fixed-point deposit
@@ -203,6 +211,10 @@ int alloc_particles(upic_ctx* c, ImplicitState& s, long cap, bool with_qm) {
     if ((s.picard || c->cfg.local_warm_start) &&
         ((rc = dalloc(c, &s.gx, cap)) || (rc = dalloc(c, &s.gy, cap)) || (rc = dalloc(c, &s.gz, cap))))
         return rc;
+    if (c->cfg.selective_particle_fallback &&
+        ((rc = dalloc(c, &s.nsub, cap)) || (rc = dalloc(c, &s.refined, cap)) || (rc = dalloc(c, &s.failed, cap)) ||
+         (rc = dalloc(c, &s.nfailed, 1))))
+        return rc;
     if ((rc = alloc_sortwork(c, s.sw, cap, s.tg))) return rc;
     s.cap = cap;
     return ensure_tmp3(c, cap);
@@ -220,6 +232,11 @@ void free_particles(upic_ctx* c, ImplicitState& s) {
     dfree(c, s.gy);
     dfree(c, s.gz);
     s.gx = s.gy = s.gz = nullptr;
+    dfree(c, s.nsub);
+    dfree(c, s.refined);
+    dfree(c, s.failed);
+    dfree(c, s.nfailed);
+    s.nsub = s.refined = s.failed = s.nfailed = nullptr;
     free_sortwork(c, s.sw);
     s.cap = 0;
 }
@@ -304,6 +321,16 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
     a.qtab = s.qtab;
     a.nq = s.nq;
     a.mnq = s.mnq;
+    if (s.layout_active) {
+        a.nsub = s.nsub;
+        a.refined = s.refined;
+        a.nref = s.nref;
+        a.grid_nx = c->nx;
+        a.grid_ny = c->ny;
+        a.failed = s.failed;
+        a.nfailed = s.nfailed;
+        UPIC_CUDA(c, cudaMemsetAsync(s.nfailed, 0, sizeof(int), c->st));
+    }
     if (cf.local_warm_start) {
         if (s.warm_valid) {
             a.warm_x = s.gx;
@@ -326,6 +353,7 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
             UPIC_CUDA(c, cudaEventRecord(e1, c->st));
             c->prof_events.emplace_back(e0, e1);
         }
+        if (s.layout_active && s.nref > 0) UPIC_CUDA(c, launch_refined_map(s.order, s.uniform, a, c->st));
     }
     UPIC_CUDA(c, launch_convert_acc(s.acc, N, s.scaleJ, out, nullptr, 0.0, 1, c->st));
     if (cf.nyquist_projection) UPIC_CUDA(c, launch_project_nyquist(out, 3, c->nx, c->ny, c->st));
@@ -754,16 +782,24 @@ int path_stats(upic_ctx* c, ImplicitState& s, double* out3) {
 
 // One implicit step (nonlinear_step_uniform_subcycled :5878); info: the
 // UPIC_INFO_* entries.
-int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
+// Result of one outer current solve (from the first guess to the accepted
+// final evaluation).
+struct OuterResult {
+    int iterations = 0, anderson_steps = 0, picard_steps = 0;
+    Norms fin;
+    MapStats ms{};
+};
+
+// The outer current iteration of nonlinear_step_uniform_subcycled (:5878) at
+// the current particle layout: first guess, Anderson / damped Picard updates
+// with backtracking, the final consistency evaluation (:6160) that writes the
+// trial state.  Returns UPIC_ERR_LOCAL_PARTICLE when a local particle solve
+// fails in any evaluation (SelectiveParticleRefinementNeeded).
+int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
     const upic_config& cf = c->cfg;
     const int N = c->N, n3 = 3 * N;
     int rc;
-    if (s.np > 0 && (rc = sort_active(c, s))) return rc;
-    s.warm_valid = false;  // the sort reorders the particles
-    // A^n records for the orbit D_A and the start-point gather
-    UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec + 3 * (size_t)N, sizeof(double2) * 3 * N,
-                                 cudaMemcpyDeviceToDevice, c->st));
-    UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 3, 1, c->st, nullptr, 2, s.rec, kIRec, kIRecAn));
+    s.warm_valid = false;
     if (cf.current_predictor == UPIC_PREDICTOR_EXTRAPOLATED && s.have_Jold)
         UPIC_CUDA(c, launch_extrapolate(n3, s.J, s.Jold, s.guess, c->st));
     else
@@ -863,6 +899,97 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
     if (!(fin.rms_scaled <= 1.0 && fin.max_scaled <= 1.0))
         return fail(c, UPIC_ERR_NONCONVERGED,
                     "final outer macro-current consistency evaluation failed at the prescribed macro dt");
+    out.iterations = iterations;
+    out.anderson_steps = anderson_steps;
+    out.picard_steps = picard_steps;
+    out.fin = fin;
+    out.ms = ms;
+    return 0;
+}
+
+// Upload the particle layout (substeps per sorted particle) and the compact
+// list of refined particles.
+int upload_layout(upic_ctx* c, ImplicitState& s) {
+    std::vector<int> refined;
+    long total = 0;
+    for (long p = 0; p < s.np; ++p) {
+        total += s.h_nsub[p];
+        if (s.h_nsub[p] > 1) refined.push_back((int)p);
+    }
+    s.nref = (int)refined.size();
+    s.total_substeps = total;
+    UPIC_CUDA(c, cudaMemcpyAsync(s.nsub, s.h_nsub.data(), sizeof(int) * s.np, cudaMemcpyHostToDevice, c->st));
+    if (s.nref > 0)
+        UPIC_CUDA(c, cudaMemcpyAsync(s.refined, refined.data(), sizeof(int) * s.nref, cudaMemcpyHostToDevice, c->st));
+    return sync(c);
+}
+
+// One implicit step (nonlinear_step_orbit :6477): the full-dt solve, and when
+// a local particle solve fails and selective_particle_fallback is set, the
+// selective sub-cycling fallback (nonlinear_step_selective_particle_fallback
+// :6328): every failing particle's substep count doubles (up to
+// selective_particle_max_substeps) and the outer solve restarts from its
+// first guess, until it succeeds.
+int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
+    const upic_config& cf = c->cfg;
+    const int N = c->N, n3 = 3 * N;
+    int rc;
+    if (s.np > 0 && (rc = sort_active(c, s))) return rc;
+    // A^n records for the orbit D_A and the start-point gather
+    UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec + 3 * (size_t)N, sizeof(double2) * 3 * N,
+                                 cudaMemcpyDeviceToDevice, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 3, 1, c->st, nullptr, 2, s.rec, kIRec, kIRecAn));
+    s.layout_active = false;
+    s.nref = 0;
+    s.total_substeps = s.np;
+    OuterResult r;
+    rc = outer_solve(c, s, r);
+    int restarts = 0;
+    bool fallback_used = false;
+    if (rc == UPIC_ERR_LOCAL_PARTICLE && cf.selective_particle_fallback && s.np > 0) {
+        fallback_used = true;
+        const std::string direct = c->err;
+        s.h_nsub.assign(s.np, 1);
+        if ((rc = upload_layout(c, s))) return rc;
+        s.layout_active = true;
+        for (;;) {
+            rc = outer_solve(c, s, r);
+            if (rc != UPIC_ERR_LOCAL_PARTICLE) break;
+            int nf = 0;
+            UPIC_CUDA(c, cudaMemcpy(&nf, s.nfailed, sizeof(int), cudaMemcpyDeviceToHost));
+            std::vector<int> failed(nf);
+            if (nf > 0)
+                UPIC_CUDA(c, cudaMemcpy(failed.data(), s.failed, sizeof(int) * nf, cudaMemcpyDeviceToHost));
+            long exhausted = 0;
+            for (int p : failed)
+                if (s.h_nsub[p] >= cf.selective_particle_max_substeps) ++exhausted;
+            if (exhausted > 0) {
+                char buf[400];
+                std::snprintf(buf, sizeof(buf),
+                              "direct macro solve failed (%s); selective particle fallback reached h=dt/%d with %ld "
+                              "particles still unconverged; macro dt=%g was not changed",
+                              direct.c_str(), cf.selective_particle_max_substeps, exhausted, cf.dt);
+                rc = fail(c, UPIC_ERR_NONCONVERGED, buf);
+                break;
+            }
+            for (int p : failed) s.h_nsub[p] = std::min(cf.selective_particle_max_substeps, 2 * s.h_nsub[p]);
+            ++restarts;
+            if ((rc = upload_layout(c, s))) return rc;
+        }
+        s.layout_active = false;
+        if (rc == UPIC_ERR_NONCONVERGED && c->err.find("selective particle fallback") == std::string::npos) {
+            const std::string inner = c->err;
+            rc = fail(c, UPIC_ERR_NONCONVERGED,
+                      "direct macro solve failed (" + direct +
+                          "); selective outer current solve also failed without a refinable local-particle set (" +
+                          inner + ")");
+        }
+    }
+    if (rc) return rc;
+    s.last_refined = s.nref;
+    const int iterations = r.iterations, anderson_steps = r.anderson_steps, picard_steps = r.picard_steps;
+    const Norms& fin = r.fin;
+    const MapStats& ms = r.ms;
     // accept: particles from the trial set, v_prev = v^n, fields from the trial spectra
     ParticleSoA& old = s.P[s.cur];
     ParticleSoA& nw = s.P[1 - s.cur];
@@ -890,13 +1017,17 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
         info[UPIC_INFO_FINAL_RMS_RESIDUAL] = fin.rms_relative;
         info[UPIC_INFO_FINAL_MAX_PARTICLE_RESIDUAL] = fin.max_relative;
         info[UPIC_INFO_LOCAL_ITER_MAX] = ms.iter_max;
-        info[UPIC_INFO_LOCAL_ITER_MEAN] = s.np > 0 ? (double)ms.iter_total / (double)s.np : 0.0;
+        info[UPIC_INFO_LOCAL_ITER_MEAN] = s.np > 0 ? (double)ms.iter_total / (double)s.total_substeps : 0.0;
         info[UPIC_INFO_ANDERSON_STEPS] = anderson_steps;
         info[UPIC_INFO_PICARD_STEPS] = picard_steps;
         info[UPIC_INFO_CURRENT_ERROR] = NAN;
         info[UPIC_INFO_VELOCITY_ERROR] = NAN;
         int rc2 = path_stats(c, s, info + UPIC_INFO_CROSSING_PARTICLES);
         if (rc2) return rc2;
+        info[UPIC_INFO_SELECTIVE_FALLBACK_USED] = fallback_used ? 1.0 : 0.0;
+        info[UPIC_INFO_SELECTIVE_RESTARTS] = restarts;
+        info[UPIC_INFO_SELECTIVE_REFINED] = s.nref;
+        info[UPIC_INFO_SELECTIVE_SUBSTEPS] = (double)s.total_substeps;
     }
     ++s.steps;
     return sync(c);
@@ -1505,9 +1636,15 @@ extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double*
             s.energy_K = r[UPIC_P3_KINETIC_ENERGY];
             s.energy_valid = true;
         }
-        if (step_diag &&
-            (rc = step_diagnostics(c, s, W0, K0, s.energy_W, s.energy_K, step_diag + (size_t)k * UPIC_SD_COUNT)))
+        if (step_diag && !s.picard && s.last_refined > 0) {
+            // sub-cycled particles: the single-orbit work balances do not
+            // apply (the reference switches to compute_subcycled_step_diagnostics)
+            for (int j = 0; j < UPIC_SD_COUNT; ++j) step_diag[(size_t)k * UPIC_SD_COUNT + j] = NAN;
+        } else if (step_diag &&
+                   (rc = step_diagnostics(c, s, W0, K0, s.energy_W, s.energy_K,
+                                          step_diag + (size_t)k * UPIC_SD_COUNT))) {
             return rc;
+        }
     }
     return UPIC_OK;
 }

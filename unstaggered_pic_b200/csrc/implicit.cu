@@ -270,7 +270,8 @@ struct LocalOut {
 // point.
 template <int ORDER>
 UPIC_D void orbit_integrals_points(const Geo& g, const double* __restrict__ rec, double x0, double y0, double dxx,
-                                   double dxy, const double* b, int nb, double gp[2], double D[3][2]) {
+                                   double dxy, const double* b, int nb, double gp[2], double D[3][2],
+                                   double th0 = 0.0, double th1 = 1.0) {
     double gp0 = 0.0, gp1 = 0.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) D[c][0] = D[c][1] = 0.0;
@@ -287,7 +288,10 @@ UPIC_D void orbit_integrals_points(const Geo& g, const double* __restrict__ rec,
             stencil_xy<ORDER>(g, xs, ys, sx, sy);
             double g0 = 0.0, g1 = 0.0;
             double d[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-            const double s1 = 1.0 - s;
+            // A at the orbit's time: (1 - th) A^n + th A^{n+1} with th running
+            // over [th0, th1] (orbit_discrete_gradient_A_interval :2958)
+            const double th = th0 + s * (th1 - th0);
+            const double s1 = 1.0 - th;
 #pragma unroll
             for (int a = 0; a <= ORDER; ++a) {
                 const int gx = wrap_index(sx.il + a, g.nx);
@@ -303,7 +307,7 @@ UPIC_D void orbit_integrals_points(const Geo& g, const double* __restrict__ rec,
                     const double dsy = sx.w[a] * sy.dw[bb];
                     g0 = fma(r01.x, sh, g0);
                     g1 = fma(r01.y, sh, g1);
-                    const double av[3] = {s1 * r23.x + s * r45.y, s1 * r23.y + s * r67.x, s1 * r45.x + s * r67.y};
+                    const double av[3] = {s1 * r23.x + th * r45.y, s1 * r23.y + th * r67.x, s1 * r45.x + th * r67.y};
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         d[c][0] = fma(av[c], dsx, d[c][0]);
@@ -352,6 +356,54 @@ UPIC_D bool evaluate(const Geo& g, const double* __restrict__ rec, double dt, do
 #pragma unroll
     for (int c = 0; c < 3; ++c) pm[c] = ((in.P0[c] - q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
     hc_rotate(pm, B, q, m, kappa, dt, pp);
+    double pend[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        o.P_end[c] = ((pp[c] + q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
+        pend[c] = o.P_end[c] - q * A1p[c];
+    }
+    const double gam = gamma_p(pend, m * kappa);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.v_end[c] = pend[c] * (1.0 / (m * gam));
+    double vm[3], vp[3];
+    secant(pm, in.pstart, m, kappa, vm);
+    secant(pend, pp, m, kappa, vp);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.vbar_map[c] = 0.5 * (vm[c] + vp[c]);
+    return true;
+}
+
+// One evaluation of the particle map of a substep: h = dt / n over the step
+// fraction [th0, th1] (evaluate_local_particle_substep :4843): A at the orbit
+// ends and along the orbit is interpolated in time between A^n and A^{n+1};
+// grad phi_mid is the step's.
+template <int ORDER>
+UPIC_D bool evaluate_sub(const Geo& g, const double* __restrict__ rec, double h, double th0, double th1,
+                         double kappa, int split, const LocalIn& in, const double* guess, LocalOut& o, double* b,
+                         int& nb) {
+    const double dxx = h * guess[0], dxy = h * guess[1];
+    o.x1 = wrap1(in.x0 + dxx, g.Lx);
+    o.y1 = wrap1(in.y0 + dxy, g.Ly);
+    double An1[3], Ae1[3], A1p[3];
+    gather_rec3<ORDER>(g, rec, kIRecAn, o.x1, o.y1, An1);
+    gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, Ae1);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) A1p[c] = (1.0 - th1) * An1[c] + th1 * Ae1[c];
+    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
+                           0.5 * (in.A0p[2] + A1p[2])};
+    nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
+    if (nb < 0) return false;
+    double gpv[2], D[3][2];
+    orbit_integrals_points<ORDER>(g, rec, in.x0, in.y0, dxx, dxy, b, nb, gpv, D, th0, th1);
+    const double Dv[3] = {D[0][0] * guess[0] + D[0][1] * guess[1], D[1][0] * guess[0] + D[1][1] * guess[1],
+                          D[2][0] * guess[0] + D[2][1] * guess[1]};
+    const double B[3] = {D[2][1], -D[2][0], D[1][0] - D[0][1]};
+    const double q = in.q, m = in.m, hq = 0.5 * q * h;
+    const double gpb[3] = {gpv[0], gpv[1], 0.0};
+    double pm[3], pp[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pm[c] = ((in.P0[c] - q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
+    hc_rotate(pm, B, q, m, kappa, h, pp);
     double pend[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -630,7 +682,7 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                     const unsigned long long key = ((unsigned long long)(unsigned)a.id[p] << 8) | (unsigned)reason;
                     first_fail = key < first_fail ? key : first_fail;
                 }
-            } else if (active) {
+            } else if (active && !(a.nsub && a.nsub[p] > 1)) {
                 in.x0 = a.x[p];
                 in.y0 = a.y[p];
                 in.P0[0] = a.Px[p];
@@ -698,6 +750,7 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                     ++nfail;
                     const unsigned long long key = ((unsigned long long)(unsigned)a.id[p] << 8) | (unsigned)reason;
                     first_fail = key < first_fail ? key : first_fail;
+                    if (a.failed) a.failed[atomicAdd(a.nfailed, 1)] = p;
                 } else {
                     vb[0] = guess[0];
                     vb[1] = guess[1];
@@ -892,6 +945,177 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
         }
         atomicMax(&st->worst_scaled_bits, (unsigned long long)__double_as_longlong(worst));
     }
+}
+
+// ---- selective particle sub-cycling ------------------------------------------
+// One thread per refined particle (push_particle of
+// evaluate_selective_current_map_at_layout, ec_pic_nyquist_projected.cpp:5235):
+// n = nsub[p] chained substeps of h = dt / n, each a local fixed point started
+// from the particle's current velocity over [k/n, (k+1)/n] of the step; each
+// accepted sub-orbit deposits q/n of the particle's current.  A failing
+// particle is appended to the failed list and leaves the evaluation (which
+// is then discarded and refined again).
+template <int ORDER, bool UNIFORM>
+__global__ void __launch_bounds__(128) refined_map_kernel(ImplicitMapArgs a, int nx, int ny) {
+    constexpr int S = ORDER + 1;
+    Geo g{nx, ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    g.qs = a.qtab;
+    g.qw = a.qtab + kMaxQuad;
+    g.ms = a.qtab + 2 * kMaxQuad;
+    g.mw = a.qtab + 3 * kMaxQuad;
+    g.nq = a.nq;
+    g.mnq = a.mnq;
+    const int N = nx * ny;
+    unsigned long long it_total = 0;
+    int it_max = 0, nfail = 0;
+    unsigned long long first_fail = ~0ull;
+    double worst = 0.0;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.nref) {
+        const int p = a.refined[i];
+        const int n = a.nsub[p];
+        const double h = a.dt / (double)n;
+        const double q = UNIFORM ? a.q0 : a.q[p];
+        const double m = UNIFORM ? a.m0 : a.m[p];
+        double x = a.x[p], y = a.y[p];
+        double P[3] = {a.Px[p], a.Py[p], a.Pz[p]};
+        double v[3] = {a.vx[p], a.vy[p], a.vz[p]};
+        double vmacro[3] = {0.0, 0.0, 0.0};
+        double bk[kMaxBreaks];
+        bool alive = true;
+        for (int k = 0; k < n && alive; ++k) {
+            const double th0 = (double)k / (double)n, th1 = (double)(k + 1) / (double)n;
+            LocalIn in;
+            in.x0 = x;
+            in.y0 = y;
+            in.q = q;
+            in.m = m;
+            double An0[3], Ae0[3];
+            gather_rec3<ORDER>(g, a.rec, kIRecAn, x, y, An0);
+            gather_rec3<ORDER>(g, a.rec, kIRecAe, x, y, Ae0);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                in.P0[c] = P[c];
+                in.A0p[c] = (1.0 - th0) * An0[c] + th0 * Ae0[c];
+                in.pstart[c] = P[c] - q * in.A0p[c];
+            }
+            double guess[3] = {v[0], v[1], v[2]};
+            int reason = kLocalMaxIter, iters = 0, nb = 0;
+            double scaled = INFINITY;
+            LocalOut o;
+            for (int it = 0; it < a.loc_maxit; ++it) {
+                if (!evaluate_sub<ORDER>(g, a.rec, h, th0, th1, a.kappa, a.split, in, guess, o, bk, nb)) {
+                    reason = kLocalTooManyCrossings;
+                    break;
+                }
+                ++iters;
+                if (!finite3(o.vbar_map)) {
+                    reason = kLocalNonfiniteMap;
+                    break;
+                }
+                if (norm3(o.vbar_map) >= a.kappa) {
+                    reason = kLocalSuperluminalMap;
+                    break;
+                }
+                const double res[3] = {o.vbar_map[0] - guess[0], o.vbar_map[1] - guess[1],
+                                       o.vbar_map[2] - guess[2]};
+                const double sc = 0.5 * (norm3(o.vbar_map) + norm3(guess));
+                scaled = norm3(res) / (a.loc_atol + a.loc_rtol * sc);
+                if (scaled <= 1.0) {
+                    reason = kLocalOk;
+                    break;
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) guess[c] += a.loc_damp * res[c];
+                if (!finite3(guess)) {
+                    reason = kLocalNonfiniteIterate;
+                    break;
+                }
+                if (norm3(guess) >= a.kappa) {
+                    reason = kLocalSuperluminalIterate;
+                    break;
+                }
+            }
+            it_total += (unsigned long long)iters;
+            it_max = max(it_max, iters);
+            worst = fmax(worst, isfinite(scaled) ? scaled : 1.0e300);
+            if (reason != kLocalOk) {
+                ++nfail;
+                const unsigned long long key = ((unsigned long long)(unsigned)a.id[p] << 8) | (unsigned)reason;
+                first_fail = key < first_fail ? key : first_fail;
+                if (a.failed) a.failed[atomicAdd(a.nfailed, 1)] = p;
+                alive = false;
+                break;
+            }
+            // this sub-orbit's share of the orbit-averaged current (:2784, weight q/n)
+            const double dxx = h * guess[0], dxy = h * guess[1];
+            const double qa = q / (double)n * a.inv_dV;
+            const double val[3] = {qa * guess[0], qa * guess[1], qa * guess[2]};
+            for (int kk = 0; kk + 1 < nb; ++kk) {
+                const double sa = bk[kk], len = bk[kk + 1] - bk[kk];
+                if (len <= 0.0) continue;
+                for (int iq = 0; iq < g.nq; ++iq) {
+                    const double s = sa + len * g.qs[iq];
+                    const double wq = len * g.qw[iq];
+                    Stencil<ORDER> sx, sy;
+                    stencil_xy<ORDER>(g, wrap1(x + s * dxx, g.Lx), wrap1(y + s * dxy, g.Ly), sx, sy);
+#pragma unroll
+                    for (int ia = 0; ia < S; ++ia) {
+                        const int gx = wrap_index(sx.il + ia, nx);
+#pragma unroll
+                        for (int ib = 0; ib < S; ++ib) {
+                            const int node = gx * ny + wrap_index(sy.il + ib, ny);
+                            const double w = wq * sx.w[ia] * sy.w[ib];
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                const double dv = val[c] * w;
+                                if (dv != 0.0) {
+                                    const Fixed2 f = to_fixed(dv, a.scale[c]);
+                                    atomicAdd(&a.acc[(size_t)(2 * c) * N + node], f.hi);
+                                    atomicAdd(&a.acc[(size_t)(2 * c + 1) * N + node], f.lo);
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            x = o.x1;
+            y = o.y1;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                P[c] = o.P_end[c];
+                v[c] = o.v_end[c];
+                vmacro[c] += (1.0 / (double)n) * guess[c];
+            }
+        }
+        if (alive && a.write_state) {
+            a.ox[p] = x;
+            a.oy[p] = y;
+            a.oPx[p] = P[0];
+            a.oPy[p] = P[1];
+            a.oPz[p] = P[2];
+            a.ovx[p] = v[0];
+            a.ovy[p] = v[1];
+            a.ovz[p] = v[2];
+            a.obx[p] = vmacro[0];
+            a.oby[p] = vmacro[1];
+            a.obz[p] = vmacro[2];
+        }
+    }
+    MapStats* st = a.stats;
+    if (i < a.nref) {
+        if (it_total) atomicAdd(&st->iter_total, it_total);
+        atomicMax(&st->iter_max, it_max);
+        if (nfail) {
+            atomicAdd(&st->failures, nfail);
+            atomicMin(&st->first_fail_key, first_fail);
+        }
+        atomicMax(&st->worst_scaled_bits, (unsigned long long)__double_as_longlong(worst));
+    }
+}
+
+__global__ void fill_int_kernel(int n, int value, int* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = value;
 }
 
 // ---- start-up point deposit -------------------------------------------------
@@ -1921,6 +2145,31 @@ cudaError_t launch_implicit_map(int order, bool uniform, bool split, const TileG
     MapKernel k = map_kernel(order, uniform, split, picard);
     if (!k) return cudaErrorInvalidValue;
     k<<<grid, kMapThreads, implicit_map_smem_bytes(tg, order), st>>>(a, tg);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_refined_map(int order, bool uniform, const ImplicitMapArgs& a, cudaStream_t st) {
+    if (a.nref <= 0) return cudaSuccess;
+    const int g = (a.nref + 127) / 128;
+    const int nx = a.grid_nx, ny = a.grid_ny;
+#define UPIC_RM(O) \
+    if (uniform) refined_map_kernel<O, true><<<g, 128, 0, st>>>(a, nx, ny); \
+    else refined_map_kernel<O, false><<<g, 128, 0, st>>>(a, nx, ny);
+    switch (order) {
+        case 1: UPIC_RM(1) break;
+        case 2: UPIC_RM(2) break;
+        case 3: UPIC_RM(3) break;
+        case 4: UPIC_RM(4) break;
+        default: return cudaErrorInvalidValue;
+    }
+#undef UPIC_RM
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_int(int n, int value, int* out, cudaStream_t st) {
+    fill_int_kernel<<<gsize(n), 256, 0, st>>>(n, value, out);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -78,7 +78,24 @@ struct ImplicitMapArgs {
     // and where to keep each particle's converged orbit velocity (null: not kept)
     const double *warm_x, *warm_y, *warm_z;
     double *keep_x, *keep_y, *keep_z;
+    // selective particle sub-cycling (ec_pic_nyquist_projected.cpp:5235,
+    // :6328): nsub[p] substeps of dt / nsub[p] per particle (null: all 1).
+    // The map kernel skips particles with nsub > 1; the refined kernel
+    // advances the compact list refined[0..nref).  Failing particles are
+    // appended to failed[] (count in *nfailed) when failed is not null.
+    const int* nsub;
+    const int* refined;
+    int nref;
+    int grid_nx, grid_ny;  // grid of the refined kernel (the map kernel takes it from its tile geometry)
+    int* failed;
+    int* nfailed;
 };
+// The refined particles of a sub-cycled map evaluation: chained local
+// solves over [k/n, (k+1)/n] of the step with time-interpolated fields, each
+// sub-orbit deposited with weight q/n (point quadrature, fixed-point grid adds).
+cudaError_t launch_refined_map(int order, bool uniform, const ImplicitMapArgs& a, cudaStream_t st);
+// nsub[p] = 1 for p < n
+cudaError_t launch_fill_int(int n, int value, int* out, cudaStream_t st);
 
 // split: knot splitting of the orbit (ImplicitMapArgs::split); picard: the
 // non-relativistic Picard deposit instead of the local GM-HC solve.  Both
