@@ -218,13 +218,23 @@ def p3_main():
                             diag=out["diag"], info=out["info"], fields=out["fields"],
                             step_diag=out["step_diag"])
         print(name, "iterations", out["info"][:, 0].tolist())
+    p3_fallback_main(lib)
+
+
+def p3_fallback_main(lib=None):
+    """Fixtures of implicit runs through the reference's selective particle
+    sub-cycling fallback, with the sub-cycled step diagnostics
+    (compute_subcycled_step_diagnostics) of each step."""
+    lib = lib or ol.ref_p3()
+    if lib is None:
+        raise SystemExit("oracle/_ref/libref_p3.so missing: run make -C oracle")
     for k, (name, kw, ppc, uth, max_sub) in enumerate(P3_FALLBACK_CASES):
         rng = np.random.default_rng(20261220 + k)
         prob = ol.P3Problem(**kw)
         x, v, q, m = ol.p3_particles(rng, prob.nx, prob.ny, ppc, prob.Lx, prob.Ly, uth=uth, Lz=prob.Lz)
         lib.ref_p3_set_fallback(1, max_sub)
         try:
-            out = ol.p3_run(lib.ref_p3_run, prob, x, v, q, m)
+            out = ol.p3_run(lib.ref_p3_run, prob, x, v, q, m, want_step_diag=True)
             sel = np.zeros(4 * prob.n_steps)
             lib.ref_p3_selective_info(ol.ptr(sel), prob.n_steps)
         finally:
@@ -233,7 +243,7 @@ def p3_main():
                             in_x=x, in_v=v, in_q=q, in_m=m, max_substeps=max_sub,
                             **{"out_" + c: out[c] for c in ("x", "v", "P", "v_prev", "vbar")},
                             diag=out["diag"], info=out["info"], fields=out["fields"],
-                            selective=sel.reshape(prob.n_steps, 4))
+                            selective=sel.reshape(prob.n_steps, 4), step_diag=out["step_diag"])
         print(name, "iterations", out["info"][:, 0].tolist(), "selective", sel.tolist())
 
 
@@ -319,6 +329,8 @@ def p1_main():
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "p3":
         p3_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "p3_fallback":
+        p3_fallback_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "p1":
         p1_main()
     else:

@@ -249,6 +249,25 @@ def test_orbit_kernels_match_reference(k):
         assert np.all(Z == 0.0)
 
 
+def compare_step_diag(sd, ref, np_):
+    """Step diagnostics rows against the reference's: crossing counts within
+    one (a path exactly on a knot), the largest path exactly, round-off
+    residuals absolutely, the rest to the step tolerance."""
+    for s in range(len(ref)):
+        for k, name in enumerate(up.STEP_DIAG_COLUMNS):
+            a, b = sd[s, k], ref[s, k]
+            if name in ("crossing_particles", "total_crossings"):
+                assert abs(a - b) <= 1, (s, name, a, b)
+            elif name == "avg_path_segments":
+                assert abs(a - b) <= 1.0 / np_ + 1e-15, (s, name, a, b)
+            elif name == "max_path_segments":
+                assert a == b, (s, name, a, b)
+            elif abs(b) < 1e-10:
+                assert abs(a - b) < TOL_ROUNDOFF, (s, name, a, b)  # round-off residuals
+            else:
+                assert abs(a - b) <= TOL_STEP * (s + 1) * abs(b) + TOL_ROUNDOFF, (s, name, a, b)
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_step_diagnostics_match_reference(case):
     """upic_step_implicit's step diagnostics against the reference's
@@ -258,24 +277,11 @@ def test_step_diagnostics_match_reference(case):
     sim, cfg = load_sim(g)
     nsteps = int(g["iparams"][12])
     np_ = len(g["in_q"])
-    names = up.STEP_DIAG_COLUMNS
     try:
         sim.init_fields(diagnostics=False)  # energies of the start state computed on demand
         _, info, sd = sim.step_implicit(nsteps, diagnostics=False, step_diagnostics=True)
-        ref = g["step_diag"]
-        for s in range(nsteps):
-            for k, name in enumerate(names):
-                a, b = sd[s, k], ref[s, k]
-                if name in ("crossing_particles", "total_crossings"):
-                    assert abs(a - b) <= 1, (s, name, a, b)
-                elif name == "avg_path_segments":
-                    assert abs(a - b) <= 1.0 / np_ + 1e-15, (s, name, a, b)
-                elif name == "max_path_segments":
-                    assert a == b, (s, name, a, b)
-                elif abs(b) < 1e-10:
-                    assert abs(a - b) < TOL_ROUNDOFF, (s, name, a, b)  # round-off residuals
-                else:
-                    assert abs(a - b) <= TOL_STEP * (s + 1) * abs(b) + TOL_ROUNDOFF, (s, name, a, b)
+        assert sd.shape == (nsteps, len(up.STEP_DIAG_COLUMNS))
+        compare_step_diag(sd, g["step_diag"], np_)
     finally:
         sim.close()
 
@@ -352,8 +358,9 @@ def test_selective_fallback_matches_reference(case):
     selective_particle_fallback the failing particles are sub-cycled (2, 4,
     ... substeps) and the outer solve restarts, as the reference's
     nonlinear_step_selective_particle_fallback does; the same particles are
-    refined the same number of times and the state agrees to the solver
-    tolerance."""
+    refined the same number of times, the state agrees to the solver
+    tolerance, and the step diagnostics follow the reference's sub-cycled
+    form (one A-chain term per sub-orbit, grid work of the accepted current)."""
     g = dict(np.load(os.path.join(GOLD, case + ".npz")))
     cfg = config_from(g["dparams"], g["iparams"])
     cfg.selective_particle_fallback = True
@@ -375,7 +382,7 @@ def test_selective_fallback_matches_reference(case):
                                                "selective_refined_particles", "selective_total_particle_substeps")]]
         assert np.array_equal(got, sel), (got, sel)
         assert np.all(np.abs(info[:, 0] - g["info"][:, 0]) <= 1), (info[:, 0], g["info"][:, 0])
-        assert np.all(np.isnan(sd))  # sub-cycled particles: single-orbit balances do not apply
+        compare_step_diag(sd, g["step_diag"], n)
         tol = TOL_STEP * nsteps
         fields = np.stack([sim.field(f) for f in FIELD_ORDER])
         for k, f in enumerate(FIELD_ORDER):

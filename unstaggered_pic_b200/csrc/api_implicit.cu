@@ -108,6 +108,12 @@ struct ImplicitState {
     std::vector<int> h_nsub;
     bool layout_active = false;
     int nref = 0, last_refined = 0;
+    // sub-orbit records (x0, y0, vbar) of the refined particles, written by
+    // the final map evaluation of a sub-cycled step and read by its step
+    // diagnostics; roff[i] is refined particle i's first record
+    int* roff = nullptr;
+    double* sub_rec = nullptr;
+    long sub_cap = 0;
     long total_substeps = 0;
     unsigned long long* pstat = nullptr;                  // path statistics counters (4)
     int* perr = nullptr;
@@ -213,7 +219,7 @@ int alloc_particles(upic_ctx* c, ImplicitState& s, long cap, bool with_qm) {
         return rc;
     if (c->cfg.selective_particle_fallback &&
         ((rc = dalloc(c, &s.nsub, cap)) || (rc = dalloc(c, &s.refined, cap)) || (rc = dalloc(c, &s.failed, cap)) ||
-         (rc = dalloc(c, &s.nfailed, 1))))
+         (rc = dalloc(c, &s.nfailed, 1)) || (rc = dalloc(c, &s.roff, cap))))
         return rc;
     if ((rc = alloc_sortwork(c, s.sw, cap, s.tg))) return rc;
     s.cap = cap;
@@ -236,7 +242,11 @@ void free_particles(upic_ctx* c, ImplicitState& s) {
     dfree(c, s.refined);
     dfree(c, s.failed);
     dfree(c, s.nfailed);
-    s.nsub = s.refined = s.failed = s.nfailed = nullptr;
+    dfree(c, s.roff);
+    dfree(c, s.sub_rec);
+    s.nsub = s.refined = s.failed = s.nfailed = s.roff = nullptr;
+    s.sub_rec = nullptr;
+    s.sub_cap = 0;
     free_sortwork(c, s.sw);
     s.cap = 0;
 }
@@ -329,6 +339,8 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
         a.grid_ny = c->ny;
         a.failed = s.failed;
         a.nfailed = s.nfailed;
+        a.roff = s.roff;
+        a.sub_rec = s.sub_rec;
         UPIC_CUDA(c, cudaMemsetAsync(s.nfailed, 0, sizeof(int), c->st));
     }
     if (cf.local_warm_start) {
@@ -907,20 +919,36 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
     return 0;
 }
 
-// Upload the particle layout (substeps per sorted particle) and the compact
-// list of refined particles.
+// Upload the particle layout (substeps per sorted particle), the compact
+// list of refined particles and their sub-orbit record offsets; grow the
+// sub-orbit record buffer to the refined particles' substeps.
 int upload_layout(upic_ctx* c, ImplicitState& s) {
-    std::vector<int> refined;
-    long total = 0;
+    std::vector<int> refined, roff;
+    long total = 0, rtotal = 0;
     for (long p = 0; p < s.np; ++p) {
         total += s.h_nsub[p];
-        if (s.h_nsub[p] > 1) refined.push_back((int)p);
+        if (s.h_nsub[p] > 1) {
+            refined.push_back((int)p);
+            roff.push_back((int)rtotal);
+            rtotal += s.h_nsub[p];
+        }
     }
     s.nref = (int)refined.size();
     s.total_substeps = total;
+    if (rtotal > s.sub_cap) {
+        int rc;
+        if ((rc = sync(c))) return rc;
+        dfree(c, s.sub_rec);
+        s.sub_rec = nullptr;
+        s.sub_cap = 0;
+        if ((rc = dalloc(c, &s.sub_rec, 5 * (size_t)rtotal))) return rc;
+        s.sub_cap = rtotal;
+    }
     UPIC_CUDA(c, cudaMemcpyAsync(s.nsub, s.h_nsub.data(), sizeof(int) * s.np, cudaMemcpyHostToDevice, c->st));
-    if (s.nref > 0)
+    if (s.nref > 0) {
         UPIC_CUDA(c, cudaMemcpyAsync(s.refined, refined.data(), sizeof(int) * s.nref, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, cudaMemcpyAsync(s.roff, roff.data(), sizeof(int) * s.nref, cudaMemcpyHostToDevice, c->st));
+    }
     return sync(c);
 }
 
@@ -1460,6 +1488,18 @@ int step_diagnostics(upic_ctx* c, ImplicitState& s, double W0, double K0, double
     a.rec = s.sd_rec;
     a.partials = s.partials;
     a.counts = s.sd_counts;
+    if (!s.picard && s.last_refined > 0) {
+        // sub-cycled particles (compute_subcycled_step_diagnostics :4363):
+        // one A-chain term per recorded sub-orbit
+        a.nsub = s.nsub;
+        a.refined = s.refined;
+        a.nref = s.last_refined;
+        a.roff = s.roff;
+        a.sub = s.sub_rec;
+        // partials hold 64 x kNormGrid doubles: the main kernel's 16 x kNormGrid,
+        // then up to 16 x 2 kNormGrid for the refined blocks
+        a.refined_grid_max = 2 * kNormGrid;
+    }
     UPIC_CUDA(c, launch_step_diag(s.order, a, kNormGrid, s.ddots, c->st));
     UPIC_CUDA(c, launch_grid_work(N, Jgrid, s.sd_rec, s.partials + 16 * kNormGrid, kNormGrid, s.ddots + 14, c->st));
     unsigned long long cnt[4];
@@ -1636,15 +1676,9 @@ extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double*
             s.energy_K = r[UPIC_P3_KINETIC_ENERGY];
             s.energy_valid = true;
         }
-        if (step_diag && !s.picard && s.last_refined > 0) {
-            // sub-cycled particles: the single-orbit work balances do not
-            // apply (the reference switches to compute_subcycled_step_diagnostics)
-            for (int j = 0; j < UPIC_SD_COUNT; ++j) step_diag[(size_t)k * UPIC_SD_COUNT + j] = NAN;
-        } else if (step_diag &&
-                   (rc = step_diagnostics(c, s, W0, K0, s.energy_W, s.energy_K,
-                                          step_diag + (size_t)k * UPIC_SD_COUNT))) {
+        if (step_diag && (rc = step_diagnostics(c, s, W0, K0, s.energy_W, s.energy_K,
+                                                step_diag + (size_t)k * UPIC_SD_COUNT)))
             return rc;
-        }
     }
     return UPIC_OK;
 }

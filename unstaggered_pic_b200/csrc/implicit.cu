@@ -1047,6 +1047,14 @@ __global__ void __launch_bounds__(128) refined_map_kernel(ImplicitMapArgs a, int
                 alive = false;
                 break;
             }
+            if (a.write_state && a.sub_rec) {
+                double* so = a.sub_rec + (size_t)(a.roff[i] + k) * 5;
+                so[0] = x;
+                so[1] = y;
+                so[2] = guess[0];
+                so[3] = guess[1];
+                so[4] = guess[2];
+            }
             // this sub-orbit's share of the orbit-averaged current (:2784, weight q/n)
             const double dxx = h * guess[0], dxy = h * guess[1];
             const double qa = q / (double)n * a.inv_dV;
@@ -1642,6 +1650,53 @@ __global__ void step_diag_spectra_kernel(int N, const double* kx, const double* 
     }
 }
 
+struct DDSix {
+    DD v[6];
+};
+
+// Block reduction of the step-diagnostics sums: six double-double sums and
+// the max into out[0..12], path counts into counts by integer atomics.
+UPIC_D void sd_block_finish(DDSix sums, double nmax, unsigned long long segs, unsigned long long cross,
+                            unsigned long long cpart, int maxseg, unsigned long long* counts, double* out) {
+    __shared__ double red[kRed / kWarp][kSdPart];
+    const int w = threadIdx.x >> 5;
+    for (int k = 0; k < 6; ++k) {
+        const DD v = warp_sum_dd(sums.v[k]);
+        if ((threadIdx.x & 31) == 0) {
+            red[w][2 * k] = v.hi;
+            red[w][2 * k + 1] = v.lo;
+        }
+    }
+    nmax = warp_max(nmax);
+    if ((threadIdx.x & 31) == 0) red[w][12] = nmax;
+    for (int o = 16; o > 0; o >>= 1) {
+        segs += __shfl_xor_sync(0xffffffffu, segs, o);
+        cross += __shfl_xor_sync(0xffffffffu, cross, o);
+        cpart += __shfl_xor_sync(0xffffffffu, cpart, o);
+        maxseg = max(maxseg, __shfl_xor_sync(0xffffffffu, maxseg, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&counts[0], segs);
+        atomicAdd(&counts[1], cross);
+        atomicAdd(&counts[2], cpart);
+        atomicMax(&counts[3], (unsigned long long)maxseg);
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        const int k = threadIdx.x;
+        if (k < 6) {
+            DD t{0, 0};
+            for (int q = 0; q < kRed / kWarp; ++q) t = dd_add_dd(t, DD{red[q][2 * k], red[q][2 * k + 1]});
+            out[2 * k] = t.hi;
+            out[2 * k + 1] = t.lo;
+        } else {
+            double mx = 0.0;
+            for (int q = 0; q < kRed / kWarp; ++q) mx = fmax(mx, red[q][12]);
+            out[12] = mx;
+        }
+    }
+}
+
 template <int ORDER>
 __global__ void __launch_bounds__(kRed) step_diag_kernel(StepDiagArgs a) {
     constexpr int S = ORDER + 1;
@@ -1653,6 +1708,7 @@ __global__ void __launch_bounds__(kRed) step_diag_kernel(StepDiagArgs a) {
     unsigned long long segs = 0, cross = 0, cpart = 0;
     int maxseg = 1;
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < a.np; p += (long)gridDim.x * blockDim.x) {
+        if (a.nsub && a.nsub[p] > 1) continue;  // sub-cycled: step_diag_refined_kernel
         const double x0 = a.x[p], y0 = a.y[p];
         const double vb[3] = {a.bx[p], a.by[p], a.bz[p]};
         const double q = a.q ? a.q[p] : a.q0;
@@ -1711,45 +1767,103 @@ __global__ void __launch_bounds__(kRed) step_diag_kernel(StepDiagArgs a) {
         cpart += nseg > 1 ? 1ull : 0ull;
         maxseg = max(maxseg, nseg);
     }
-    DD v[6] = {r2, a2, rhs2, nsum, wdef, pw};
-    __shared__ double red[kRed / kWarp][kSdPart];
-    const int w = threadIdx.x >> 5;
-    for (int k = 0; k < 6; ++k) {
-        v[k] = warp_sum_dd(v[k]);
-        if ((threadIdx.x & 31) == 0) {
-            red[w][2 * k] = v[k].hi;
-            red[w][2 * k + 1] = v[k].lo;
+    sd_block_finish(DDSix{r2, a2, rhs2, nsum, wdef, pw}, nmax, segs, cross, cpart, maxseg, a.counts,
+                    a.partials + (size_t)blockIdx.x * kSdPart);
+}
+
+// Step diagnostics of the refined (sub-cycled) particles
+// (compute_subcycled_step_diagnostics :4340): per recorded sub-orbit of
+// h = dt/n over [k/n, (k+1)/n], the A-chain defect with time-interpolated A
+// (weights 1/n in the rms sums), the work defect and the particle work; path
+// segments summed per particle.  Block partials go to a.partials + block.
+template <int ORDER>
+__global__ void __launch_bounds__(kRed) step_diag_refined_kernel(StepDiagArgs a) {
+    constexpr int S = ORDER + 1;
+    Geo g{a.nx, a.ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    const double* qs = a.qtab;
+    const double* qw = a.qtab + kMaxQuad;
+    DD r2{0, 0}, a2{0, 0}, rhs2{0, 0}, nsum{0, 0}, wdef{0, 0}, pw{0, 0};
+    double nmax = 0.0;
+    unsigned long long segs = 0, cross = 0, cpart = 0;
+    int maxseg = 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nref; i += gridDim.x * blockDim.x) {
+        const int p = a.refined[i];
+        const int n = a.nsub[p];
+        const double q = a.q ? a.q[p] : a.q0;
+        const double h = a.dt / (double)n, wgt = 1.0 / (double)n;
+        int psegs = 0;
+        bool crossed = false;
+        for (int k = 0; k < n; ++k) {
+            const double* so = a.sub + (size_t)(a.roff[i] + k) * 5;
+            const double x0 = so[0], y0 = so[1];
+            const double vb[3] = {so[2], so[3], so[4]};
+            const double th0 = (double)k / (double)n, th1 = (double)(k + 1) / (double)n;
+            const double dxx = h * vb[0], dxy = h * vb[1];
+            const double x1 = wrap1(x0 + dxx, g.Lx), y1 = wrap1(y0 + dxy, g.Ly);
+            double An0[3], Ae0[3], An1[3], Ae1[3], A0p[3], A1p[3];
+            gather_rec3<ORDER, kSdRec>(g, a.rec, 0, x0, y0, An0);
+            gather_rec3<ORDER, kSdRec>(g, a.rec, 3, x0, y0, Ae0);
+            gather_rec3<ORDER, kSdRec>(g, a.rec, 0, x1, y1, An1);
+            gather_rec3<ORDER, kSdRec>(g, a.rec, 3, x1, y1, Ae1);
+            for (int c = 0; c < 3; ++c) {
+                A0p[c] = (1.0 - th0) * An0[c] + th0 * Ae0[c];
+                A1p[c] = (1.0 - th1) * An1[c] + th1 * Ae1[c];
+            }
+            double b[kMaxBreaks];
+            const int nb = breakpoints<ORDER>(g, x0, y0, dxx, dxy, a.split, b);
+            double Ub[3] = {0.0, 0.0, 0.0}, Eb[3] = {0.0, 0.0, 0.0};
+            double D[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+            for (int kk = 0; kk + 1 < nb; ++kk) {
+                const double sa = b[kk], len = b[kk + 1] - b[kk];
+                if (len <= 0.0) continue;
+                for (int iq = 0; iq < a.nq; ++iq) {
+                    const double s = sa + len * qs[iq];
+                    const double wq = len * qw[iq];
+                    const double th = th0 + s * (th1 - th0);
+                    Stencil<ORDER> sx, sy;
+                    stencil_xy<ORDER>(g, wrap1(x0 + s * dxx, g.Lx), wrap1(y0 + s * dxy, g.Ly), sx, sy);
+                    for (int ia = 0; ia < S; ++ia) {
+                        const int gx = wrap_index(sx.il + ia, a.nx);
+                        for (int ib = 0; ib < S; ++ib) {
+                            const double* r = a.rec + (size_t)(gx * a.ny + wrap_index(sy.il + ib, a.ny)) * kSdRec;
+                            const double shape = sx.w[ia] * sy.w[ib];
+                            const double dsx = sx.dw[ia] * sy.w[ib], dsy = sx.w[ia] * sy.dw[ib];
+                            for (int c = 0; c < 3; ++c) {
+                                Ub[c] += wq * r[6 + c] * shape;
+                                Eb[c] += wq * r[9 + c] * shape;
+                                const double av = (1.0 - th) * r[c] + th * r[3 + c];
+                                D[c][0] += wq * av * dsx;
+                                D[c][1] += wq * av * dsy;
+                            }
+                        }
+                    }
+                }
+            }
+            double Rv[3], Ad[3], rhs[3];
+            for (int c = 0; c < 3; ++c) {
+                Ad[c] = A1p[c] - A0p[c];
+                rhs[c] = h * (Ub[c] + (D[c][0] * vb[0] + D[c][1] * vb[1]));
+                Rv[c] = Ad[c] - rhs[c];
+            }
+            r2 = dd_add(r2, wgt * dot3(Rv, Rv));
+            a2 = dd_add(a2, wgt * dot3(Ad, Ad));
+            rhs2 = dd_add(rhs2, wgt * dot3(rhs, rhs));
+            const double nr = norm3(Rv);
+            nmax = fmax(nmax, nr);
+            nsum = dd_add(nsum, wgt * nr);
+            wdef = dd_add(wdef, -q * dot3(vb, Rv));
+            pw = dd_add(pw, (h * q) * dot3(vb, Eb));
+            const int nseg = nb - 1 > 1 ? nb - 1 : 1;
+            psegs += nseg;
+            cross += (unsigned long long)(nseg - 1);
+            crossed = crossed || nseg > 1;
         }
+        segs += (unsigned long long)psegs;
+        cpart += crossed ? 1ull : 0ull;
+        maxseg = max(maxseg, psegs);
     }
-    nmax = warp_max(nmax);
-    if ((threadIdx.x & 31) == 0) red[w][12] = nmax;
-    for (int o = 16; o > 0; o >>= 1) {
-        segs += __shfl_xor_sync(0xffffffffu, segs, o);
-        cross += __shfl_xor_sync(0xffffffffu, cross, o);
-        cpart += __shfl_xor_sync(0xffffffffu, cpart, o);
-        maxseg = max(maxseg, __shfl_xor_sync(0xffffffffu, maxseg, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&a.counts[0], segs);
-        atomicAdd(&a.counts[1], cross);
-        atomicAdd(&a.counts[2], cpart);
-        atomicMax(&a.counts[3], (unsigned long long)maxseg);
-    }
-    __syncthreads();
-    if (threadIdx.x < 7) {
-        const int k = threadIdx.x;
-        double* o = a.partials + (size_t)blockIdx.x * kSdPart;
-        if (k < 6) {
-            DD t{0, 0};
-            for (int q = 0; q < kRed / kWarp; ++q) t = dd_add_dd(t, DD{red[q][2 * k], red[q][2 * k + 1]});
-            o[2 * k] = t.hi;
-            o[2 * k + 1] = t.lo;
-        } else {
-            double mx = 0.0;
-            for (int q = 0; q < kRed / kWarp; ++q) mx = fmax(mx, red[q][12]);
-            o[12] = mx;
-        }
-    }
+    sd_block_finish(DDSix{r2, a2, rhs2, nsum, wdef, pw}, nmax, segs, cross, cpart, maxseg, a.counts,
+                    a.partials + (size_t)blockIdx.x * kSdPart);
 }
 
 // One warp per quantity: out[0..11] the six double-double sums, out[12] max.
@@ -2215,7 +2329,22 @@ cudaError_t launch_step_diag(int order, const StepDiagArgs& a, int grid, double*
         case 4: step_diag_kernel<4><<<grid, kRed, 0, st>>>(a); break;
         default: return cudaErrorInvalidValue;
     }
-    step_diag_final_kernel<<<1, 32 * 7, 0, st>>>(a.partials, grid, out13);
+    int g2 = 0;
+    if (a.nref > 0) {
+        // refined particles: their block partials follow the main kernel's
+        g2 = std::min((a.nref + kRed - 1) / kRed, a.refined_grid_max);
+        StepDiagArgs b = a;
+        b.partials = a.partials + (size_t)grid * kSdPart;
+        switch (order) {
+            case 1: step_diag_refined_kernel<1><<<g2, kRed, 0, st>>>(b); break;
+            case 2: step_diag_refined_kernel<2><<<g2, kRed, 0, st>>>(b); break;
+            case 3: step_diag_refined_kernel<3><<<g2, kRed, 0, st>>>(b); break;
+            case 4: step_diag_refined_kernel<4><<<g2, kRed, 0, st>>>(b); break;
+            default: return cudaErrorInvalidValue;
+        }
+        count_launches(1);
+    }
+    step_diag_final_kernel<<<1, 32 * 7, 0, st>>>(a.partials, grid + g2, out13);
     count_launches(2);
     return cudaGetLastError();
 }

@@ -87,6 +87,10 @@ struct ImplicitMapArgs {
     const int* refined;
     int nref;
     int grid_nx, grid_ny;  // grid of the refined kernel (the map kernel takes it from its tile geometry)
+    // sub-orbit records of the refined particles (x0, y0, vbar from roff[i]),
+    // written by the final evaluation (write_state), or null
+    const int* roff;
+    double* sub_rec;
     int* failed;
     int* nfailed;
 };
@@ -154,8 +158,17 @@ struct StepDiagArgs {
     int split, nq;
     const double* qtab;
     const double* rec;                // 12 doubles per node: An, Ae, U_mid, E_mid
-    double* partials;                 // grid x 16
+    double* partials;                 // grid x 16 (then the refined kernel's blocks)
     unsigned long long* counts;       // segments, crossings, crossing particles, max segments
+    // sub-cycled particles of the step: nsub per particle (null: none), the
+    // refined list, their sub-orbit records (x0, y0, vbar; 5 doubles) from
+    // roff[i], and the most blocks the refined kernel may use
+    const int* nsub;
+    const int* refined;
+    int nref;
+    const int* roff;
+    const double* sub;
+    int refined_grid_max;
 };
 // Spectra (12 x N) of A^n, A^{n+1}, U_mid, E_mid from the two states' spectra.
 cudaError_t launch_step_diag_spectra(int N, const double* kx, const double* ky, const double2* s0,
