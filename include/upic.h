@@ -67,9 +67,16 @@ enum { UPIC_METHOD_BDF1 = 1, UPIC_METHOD_BDF2 = 2, UPIC_METHOD_CN_ORBIT = 3, UPI
  * the last accepted current, as the reference does
  * (nonlinear_step_uniform_subcycled, ec_pic_nyquist_projected.cpp:5887).
  * EXTRAPOLATED: 2 J^n - J^{n-1} (the previous current on the first step
- * after upic_init_fields); not in the reference.  The iteration still runs
- * to the same tolerances, so only the iteration count changes. */
-enum { UPIC_PREDICTOR_PREVIOUS = 0, UPIC_PREDICTOR_EXTRAPOLATED = 1 };
+ * after upic_init_fields); not in the reference.  LEARNED (CN_ORBIT only):
+ * the extrapolation plus the correction predicted by a small conv net
+ * (4 layers of 3x3 periodic convolutions, 32 channels, BF16 on the tensor
+ * cores) from the last three steps' J, A and phi, trained online on the
+ * accepted currents of the first learned_train_steps steps; a step uses it
+ * only when on the step before the learned prediction was closer to the
+ * accepted current than the extrapolation, else the extrapolation.  The
+ * iteration still runs to the same tolerances, so only the iteration count
+ * changes. */
+enum { UPIC_PREDICTOR_PREVIOUS = 0, UPIC_PREDICTOR_EXTRAPOLATED = 1, UPIC_PREDICTOR_LEARNED = 2 };
 
 /* Outer nonlinear solver of the implicit method (Config::nonlinear_solver,
  * ec_pic_nyquist_projected.cpp:891). */
@@ -174,6 +181,14 @@ typedef struct upic_config {
      * <= 64) chained substeps and the outer current solve restarts. */
     int selective_particle_fallback;
     int selective_particle_max_substeps;
+    /* UPIC_PREDICTOR_LEARNED: training steps (accepted steps whose current
+     * trains the net, from the third step on; default 200), Adam iterations
+     * per training step (default 4), Adam learning rate (default 1e-3),
+     * weight-initialisation seed. */
+    int learned_train_steps;
+    int learned_train_iters;
+    double learned_rate;
+    unsigned long long learned_seed;
 } upic_config;
 
 typedef struct upic_ctx upic_ctx;
@@ -210,7 +225,16 @@ enum {
     /* selective sub-cycling (NonlinearSolveInfo::selective_*): fallback used,
      * refinement restarts, refined particles, total particle substeps */
     UPIC_INFO_SELECTIVE_FALLBACK_USED, UPIC_INFO_SELECTIVE_RESTARTS, UPIC_INFO_SELECTIVE_REFINED,
-    UPIC_INFO_SELECTIVE_SUBSTEPS, UPIC_INFO_COUNT
+    UPIC_INFO_SELECTIVE_SUBSTEPS,
+    /* first guess of the outer current iteration (CN_ORBIT): the predictor
+     * used (UPIC_PREDICTOR_*), and the relative rms distances |J - J^{n+1}| /
+     * |J^{n+1}| from the accepted current of the guess used, of the
+     * extrapolation 2 J^n - J^{n-1} and of the learned prediction (NaN when
+     * not formed), and the learned predictor's training loss on this step
+     * (mean squared error in units of the rms second difference of J; NaN
+     * when it did not train) */
+    UPIC_INFO_PREDICTOR_USED, UPIC_INFO_GUESS_ERROR, UPIC_INFO_EXTRAPOLATION_ERROR, UPIC_INFO_LEARNED_ERROR,
+    UPIC_INFO_LEARNED_LOSS, UPIC_INFO_COUNT
 };
 
 /* Step diagnostics of the implicit method: StepDiagnostics of
@@ -373,6 +397,20 @@ int upic_orbit_deposit(upic_ctx* ctx, long np, const double* x, const double* y,
 int upic_orbit_gather(upic_ctx* ctx, long np, const double* x, const double* y, const double* dx,
                       const double* mesh, const double* An, const double* Anp1, double* gathered,
                       double* grad);
+
+/* Kernel-level pieces of the learned predictor's network (any context; no
+ * counterpart in the reference).  Activations are nx*ny x 32 bf16 (raw
+ * uint16 bits), pixel p = ix*ny + iy; w is 32 x 288 bf16, row = output
+ * channel, column = tap*32 + input channel, tap = (dx+1)*3 + (dy+1).
+ * upic_guess_conv: out[p][n] = sum_{t,c} x[wrap(p + sign*d_t)][c] w[n][t*32+c]
+ * (+ bias[n] when bias != NULL) on the tensor cores; mode 0: ReLU, bf16 out
+ * (nx*ny x 32 uint16); 1: linear, fp32 out (nx*ny x 32 float); 2: times
+ * (mask[p][n] > 0), bf16 out.  sign is +1 or -1.
+ * upic_guess_wgrad: grad[n*288 + t*32 + c] = sum_p dz[p][n] x[wrap(p + d_t)][c]
+ * and grad[9216 + n] = sum_p dz[p][n] (fp32, 9248 floats). */
+int upic_guess_conv(upic_ctx* ctx, int nx, int ny, const uint16_t* x, const uint16_t* w, const float* bias,
+                    const uint16_t* mask, int mode, int sign, void* out);
+int upic_guess_wgrad(upic_ctx* ctx, int nx, int ny, const uint16_t* dz, const uint16_t* x, float* grad);
 
 /* Largest grid (nx*ny nodes) upic_deposit_current_noalloc accepts: its
  * scratch is a fixed 6*UPIC_NOALLOC_MAX_NODES+2 uint64 array (3 MiB). */

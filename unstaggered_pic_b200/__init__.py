@@ -24,7 +24,7 @@ CHARGE_UPDATES = {"conserving": 0, "naive": 1}
 # cell-relative offsets, FP64 field solve and diagnostics)
 PRECISIONS = {"fp64": 0, "mixed": 1}
 # first guess of the implicit step's outer current iteration
-PREDICTORS = {"previous": 0, "extrapolated": 1}
+PREDICTORS = {"previous": 0, "extrapolated": 1, "learned": 2}
 NONLINEAR_SOLVERS = {"anderson_quasi_newton": 0, "anderson": 0, "picard": 1}
 FIELDS = {"phi": 0, "Ax": 1, "Ay": 2, "Az": 3, "rho": 4, "Jx": 5, "Jy": 6, "Jz": 7,
           "psi": 8, "Ux": 9, "Uy": 10, "Uz": 11}
@@ -56,7 +56,9 @@ SOLVE_INFO_COLUMNS = ["iterations", "converged", "final_rms_residual", "final_ma
                       "anderson_steps", "picard_fallback_steps", "picard_current_error",
                       "picard_velocity_error", "crossing_particles", "avg_path_segments",
                       "max_path_segments", "selective_fallback_used", "selective_refinement_restarts",
-                      "selective_refined_particles", "selective_total_particle_substeps"]
+                      "selective_refined_particles", "selective_total_particle_substeps",
+                      # first guess of the outer current iteration (not in the reference)
+                      "predictor_used", "guess_error", "extrapolation_error", "learned_error", "learned_loss"]
 
 
 class UpicError(RuntimeError):
@@ -117,8 +119,11 @@ class ImplicitConfig:
                  anderson_damping=0.7, anderson_regularization=1.0e-12, anderson_growth_limit=1.2,
                  uniform_local_rtol=1.0e-11, uniform_local_atol=1.0e-13, uniform_local_max_iter=24,
                  uniform_local_damping=1.0, perturbation_mode=1, tile=0, guard=-1, current_predictor="previous",
-                 local_warm_start=False, selective_particle_fallback=False, selective_particle_max_substeps=64):
+                 local_warm_start=False, selective_particle_fallback=False, selective_particle_max_substeps=64,
+                 learned_train_steps=200, learned_train_iters=4, learned_rate=1.0e-3, learned_seed=20261203):
         self.method = "cn_orbit"
+        self.learned_train_steps, self.learned_train_iters = learned_train_steps, learned_train_iters
+        self.learned_rate, self.learned_seed = learned_rate, learned_seed
         self.current_predictor, self.local_warm_start = current_predictor, local_warm_start
         self.selective_particle_fallback = selective_particle_fallback
         self.selective_particle_max_substeps = selective_particle_max_substeps
@@ -165,6 +170,8 @@ class ImplicitConfig:
         cfg.local_warm_start = int(bool(self.local_warm_start))
         cfg.selective_particle_fallback = int(bool(self.selective_particle_fallback))
         cfg.selective_particle_max_substeps = int(self.selective_particle_max_substeps)
+        cfg.learned_train_steps, cfg.learned_train_iters = int(self.learned_train_steps), int(self.learned_train_iters)
+        cfg.learned_rate, cfg.learned_seed = float(self.learned_rate), int(self.learned_seed)
         return cfg
 
 
@@ -388,6 +395,33 @@ class Simulation:
         arrs = [_f64(x), _f64(y), _f64(dx, (n, 3)), _f64(mesh).ravel(), _f64(An).ravel(), _f64(Anp1).ravel()]
         self._check(lib().upic_orbit_gather(self._ctx, n, *[_p(a) for a in arrs], _p(gat), _p(grad)))
         return gat, grad
+
+    def guess_conv(self, x, w, bias=None, mask=None, mode="relu", sign=1):
+        """One periodic 3x3 conv of the learned predictor's network on the
+        tensor cores.  x, mask: (nx, ny, 32) bf16 bit patterns (uint16); w:
+        (32, 288) uint16; bias: 32 float32.  mode relu / mask return uint16
+        (nx, ny, 32), linear returns float32 (nx, ny, 32)."""
+        nx, ny = x.shape[0], x.shape[1]
+        modes = {"relu": 0, "linear": 1, "mask": 2}
+        x = np.ascontiguousarray(x, dtype=np.uint16)
+        w = np.ascontiguousarray(w, dtype=np.uint16)
+        b = None if bias is None else np.ascontiguousarray(bias, dtype=np.float32)
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint16)
+        out = np.empty((nx, ny, 32), dtype=np.float32 if mode == "linear" else np.uint16)
+        vp = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+        self._check(lib().upic_guess_conv(self._ctx, nx, ny, vp(x), vp(w), vp(b), vp(m), modes[mode], int(sign),
+                                          vp(out)))
+        return out
+
+    def guess_wgrad(self, dz, x):
+        """Weight (32, 288) and bias (32) gradients of one conv, float32."""
+        nx, ny = x.shape[0], x.shape[1]
+        dz = np.ascontiguousarray(dz, dtype=np.uint16)
+        x = np.ascontiguousarray(x, dtype=np.uint16)
+        g = np.empty(32 * 288 + 32, dtype=np.float32)
+        self._check(lib().upic_guess_wgrad(self._ctx, nx, ny, dz.ctypes.data_as(ctypes.c_void_p),
+                                           x.ctypes.data_as(ctypes.c_void_p), g.ctypes.data_as(ctypes.c_void_p)))
+        return g[:32 * 288].reshape(32, 288), g[32 * 288:]
 
     def solve_bdf(self, source, hist):
         out = np.empty(self.N)

@@ -49,6 +49,9 @@ SYMBOLS = {
     "upic_solve_bdf": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp, c_dp]),
     "upic_orbit_deposit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 6),
     "upic_orbit_gather": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 8),
+    "upic_guess_conv": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 4
+                        + [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "upic_guess_wgrad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 3),
     "upic_deposit_current_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                     ctypes.c_double, ctypes.c_long, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -90,6 +93,8 @@ class UpicConfig(ctypes.Structure):
         ("current_predictor", ctypes.c_int),
         ("local_warm_start", ctypes.c_int),
         ("selective_particle_fallback", ctypes.c_int), ("selective_particle_max_substeps", ctypes.c_int),
+        ("learned_train_steps", ctypes.c_int), ("learned_train_iters", ctypes.c_int),
+        ("learned_rate", ctypes.c_double), ("learned_seed", ctypes.c_ulonglong),
     ]
 
 

@@ -558,6 +558,10 @@ int upic_config_default(upic_config* cfg) {
     cfg->local_warm_start = 0;
     cfg->selective_particle_fallback = 0;
     cfg->selective_particle_max_substeps = 64;
+    cfg->learned_train_steps = 200;
+    cfg->learned_train_iters = 4;
+    cfg->learned_rate = 1.0e-3;
+    cfg->learned_seed = 20261203ull;
     return UPIC_OK;
 }
 
@@ -576,6 +580,8 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
     const bool implicit = cfg->method == UPIC_METHOD_CN_ORBIT || nonrel;
     if (!is_bdf(cfg->method) && !implicit)
         return fail(nullptr, UPIC_ERR_CONFIG, "method must be bdf1, bdf2, cn_orbit or cn_orbit_nonrel");
+    if (cfg->current_predictor == UPIC_PREDICTOR_LEARNED && cfg->method != UPIC_METHOD_CN_ORBIT)
+        return fail(nullptr, UPIC_ERR_CONFIG, "the learned predictor needs method cn_orbit");
     if (nonrel) {
         // Config of ec_pic_serial_demo.cpp:232-301 and the checks of make_grid
         // / bspline (:396, :565)
@@ -610,8 +616,14 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
         if (!(cfg->anderson_damping > 0) || !(cfg->local_damping > 0) || !(cfg->anderson_growth_limit > 0) ||
             !(cfg->anderson_regularization >= 0))
             return fail(nullptr, UPIC_ERR_CONFIG, "damping and growth limits must be positive");
-        if (cfg->current_predictor != UPIC_PREDICTOR_PREVIOUS && cfg->current_predictor != UPIC_PREDICTOR_EXTRAPOLATED)
-            return fail(nullptr, UPIC_ERR_CONFIG, "current_predictor must be previous or extrapolated");
+        if (cfg->current_predictor != UPIC_PREDICTOR_PREVIOUS && cfg->current_predictor != UPIC_PREDICTOR_EXTRAPOLATED &&
+            cfg->current_predictor != UPIC_PREDICTOR_LEARNED)
+            return fail(nullptr, UPIC_ERR_CONFIG, "current_predictor must be previous, extrapolated or learned");
+        if (cfg->current_predictor == UPIC_PREDICTOR_LEARNED) {
+            if (cfg->learned_train_steps < 0 || cfg->learned_train_iters < 1 || !(cfg->learned_rate > 0))
+                return fail(nullptr, UPIC_ERR_CONFIG,
+                            "learned_train_steps >= 0, learned_train_iters >= 1 and learned_rate > 0 required");
+        }
         {
             const int ms = cfg->selective_particle_max_substeps;
             if (ms < 1 || ms > 64 || (ms & (ms - 1)) != 0)
@@ -769,7 +781,9 @@ std::vector<double> config_signature(const upic_config& f) {
             f.anderson_regularization, f.anderson_growth_limit, f.local_rtol, f.local_atol, f.local_damping,
             (double)f.perturbation_mode, f.picard_tol, (double)f.picard_max_iter,
             (double)f.final_consistency_sweep, (double)f.current_predictor, (double)f.local_warm_start,
-            (double)f.selective_particle_fallback, (double)f.selective_particle_max_substeps};
+            (double)f.selective_particle_fallback, (double)f.selective_particle_max_substeps,
+            (double)f.learned_train_steps, (double)f.learned_train_iters, f.learned_rate,
+            (double)(f.learned_seed >> 32), (double)(f.learned_seed & 0xFFFFFFFFull)};
 }
 
 // Everything the next explicit step reads: the particle set in its current

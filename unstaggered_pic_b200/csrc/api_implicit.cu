@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "context.h"
+#include "guess_net.h"
 #include "implicit_kernels.h"
 #include "upic_common.cuh"
 
@@ -115,6 +116,19 @@ struct ImplicitState {
     double* sub_rec = nullptr;
     long sub_cap = 0;
     long total_substeps = 0;
+    // first guess of the outer current iteration: J0 the guess of the
+    // current step; Jx = 2 J^n - J^(n-1) (extrapolated and learned
+    // predictors); Jl the learned prediction and the network with its field
+    // frames (learned predictor; fbuf: A and phi of the accepted state)
+    double *J0 = nullptr, *Jx = nullptr, *Jl = nullptr, *fbuf = nullptr;
+    bool have_Jx = false, have_Jl = false, use_learned = false;
+    int predictor_used = UPIC_PREDICTOR_PREVIOUS;
+    long trained_steps = 0;
+    upic::gnet::Net* net = nullptr;
+    double* dloss = nullptr;
+    NormSums* dnorm3 = nullptr;
+    NormSums* hnorm3 = nullptr;  // pinned (3)
+    double* hloss = nullptr;     // pinned
     unsigned long long* pstat = nullptr;                  // path statistics counters (4)
     int* perr = nullptr;
     double vb_limit = 0.0;  // bound on |vbar| components of the fixed-point deposit
@@ -812,10 +826,7 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
     const int N = c->N, n3 = 3 * N;
     int rc;
     s.warm_valid = false;
-    if (cf.current_predictor == UPIC_PREDICTOR_EXTRAPOLATED && s.have_Jold)
-        UPIC_CUDA(c, launch_extrapolate(n3, s.J, s.Jold, s.guess, c->st));
-    else
-        UPIC_CUDA(c, cudaMemcpyAsync(s.guess, s.J, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.guess, s.J0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
     bool finite = true;
     if ((rc = all_finite(c, s, s.guess, finite))) return rc;
     if (!finite) return fail(c, UPIC_ERR_NONFINITE, "nonfinite initial macro-current predictor");
@@ -952,6 +963,95 @@ int upload_layout(upic_ctx* c, ImplicitState& s) {
     return sync(c);
 }
 
+// Append the accepted state's J, A and phi to the learned predictor's
+// frames (A and phi transformed back from the state spectra).
+int push_frame(upic_ctx* c, ImplicitState& s) {
+    const size_t N = (size_t)c->N;
+    UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec + 3 * N, sizeof(double2) * 3 * N, cudaMemcpyDeviceToDevice, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 3, 1, c->st, nullptr, 1, s.fbuf));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec, sizeof(double2) * N, cudaMemcpyDeviceToDevice, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 1, 1, c->st, nullptr, 1, s.fbuf + 3 * N));
+    UPIC_CUDA(c, gnet::net_push_frame(s.net, s.J, s.fbuf, s.fbuf + 3 * N, c->st));
+    return 0;
+}
+
+// First guess J0 of this step's outer current iteration (UPIC_PREDICTOR_*),
+// with the extrapolation Jx and the learned prediction Jl it was chosen from.
+int form_guess(upic_ctx* c, ImplicitState& s) {
+    const upic_config& cf = c->cfg;
+    const int n3 = 3 * c->N;
+    s.have_Jx = s.have_Jl = false;
+    if (cf.current_predictor == UPIC_PREDICTOR_EXTRAPOLATED && s.have_Jold) {
+        UPIC_CUDA(c, launch_extrapolate(n3, s.J, s.Jold, s.Jx, c->st));
+        s.have_Jx = true;
+    } else if (cf.current_predictor == UPIC_PREDICTOR_LEARNED && gnet::net_frames(s.net) >= 2) {
+        UPIC_CUDA(c, gnet::net_extrapolate(s.net, s.Jx, c->st));
+        s.have_Jx = true;
+        if (gnet::net_frames(s.net) >= gnet::kFrames && s.trained_steps > 0) {
+            UPIC_CUDA(c, gnet::net_predict(s.net, s.Jl, c->st));
+            s.have_Jl = true;
+        }
+    }
+    const double* g = s.J;
+    s.predictor_used = UPIC_PREDICTOR_PREVIOUS;
+    if (s.have_Jl && s.use_learned) {
+        g = s.Jl;
+        s.predictor_used = UPIC_PREDICTOR_LEARNED;
+    } else if (s.have_Jx) {
+        g = s.Jx;
+        s.predictor_used = UPIC_PREDICTOR_EXTRAPOLATED;
+    }
+    UPIC_CUDA(c, cudaMemcpyAsync(s.J0, g, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
+    return 0;
+}
+
+// After the accepted current J^{n+1} is in s.J: distances of the guess, the
+// extrapolation and the learned prediction from it (into info), and for the
+// learned predictor the choice of the next step's guess, a training step on
+// this step's sample and the new frame.
+int predictor_update(upic_ctx* c, ImplicitState& s, double* info) {
+    const upic_config& cf = c->cfg;
+    const int N = c->N;
+    const bool learned = cf.current_predictor == UPIC_PREDICTOR_LEARNED;
+    if (!info && !learned) return 0;
+    const double* cand[3] = {s.J0, s.have_Jx ? s.Jx : nullptr, s.have_Jl ? s.Jl : nullptr};
+    for (int k = 0; k < 3; ++k)
+        if (cand[k])
+            UPIC_CUDA(c, launch_residual_norms(N, s.J, cand[k], 1.0, 0.0, 1.0, s.partials, kNormGrid, s.dnorm3 + k,
+                                               c->st));
+    bool trained = false;
+    if (learned && gnet::net_frames(s.net) >= gnet::kFrames && s.trained_steps < cf.learned_train_steps) {
+        UPIC_CUDA(c, gnet::net_train(s.net, s.J, cf.learned_train_iters, (float)cf.learned_rate, s.dloss, c->st));
+        ++s.trained_steps;
+        trained = true;
+    }
+    UPIC_CUDA(c, cudaMemcpyAsync(s.hnorm3, s.dnorm3, sizeof(NormSums) * 3, cudaMemcpyDeviceToHost, c->st));
+    if (trained) UPIC_CUDA(c, cudaMemcpyAsync(s.hloss, s.dloss, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    int rc;
+    if (learned && (rc = push_frame(c, s))) return rc;
+    int nerr = 0;
+    if (learned) UPIC_CUDA(c, cudaMemcpyAsync(&nerr, gnet::net_error_flag(s.net), sizeof(int), cudaMemcpyDeviceToHost,
+                                              c->st));
+    if ((rc = sync(c))) return rc;
+    if (nerr) return fail(c, UPIC_ERR_CUDA, "learned predictor: a tensor-core wait timed out");
+    double err[3] = {NAN, NAN, NAN};
+    for (int k = 0; k < 3; ++k)
+        if (cand[k]) {
+            const NormSums& h = s.hnorm3[k];
+            const double m2 = h.map2[0] + h.map2[1];
+            err[k] = std::sqrt((h.r2[0] + h.r2[1]) / (m2 > 0.0 ? m2 : 1.0e-300));
+        }
+    if (learned) s.use_learned = s.have_Jl && s.have_Jx && err[2] < err[1];
+    if (info) {
+        info[UPIC_INFO_PREDICTOR_USED] = s.predictor_used;
+        info[UPIC_INFO_GUESS_ERROR] = err[0];
+        info[UPIC_INFO_EXTRAPOLATION_ERROR] = err[1];
+        info[UPIC_INFO_LEARNED_ERROR] = err[2];
+        info[UPIC_INFO_LEARNED_LOSS] = trained ? *s.hloss : NAN;
+    }
+    return 0;
+}
+
 // One implicit step (nonlinear_step_orbit :6477): the full-dt solve, and when
 // a local particle solve fails and selective_particle_fallback is set, the
 // selective sub-cycling fallback (nonlinear_step_selective_particle_fallback
@@ -970,6 +1070,7 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
     s.layout_active = false;
     s.nref = 0;
     s.total_substeps = s.np;
+    if ((rc = form_guess(c, s))) return rc;
     OuterResult r;
     rc = outer_solve(c, s, r);
     int restarts = 0;
@@ -1057,6 +1158,7 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
         info[UPIC_INFO_SELECTIVE_REFINED] = s.nref;
         info[UPIC_INFO_SELECTIVE_SUBSTEPS] = (double)s.total_substeps;
     }
+    if ((rc = predictor_update(c, s, info))) return rc;
     ++s.steps;
     return sync(c);
 }
@@ -1153,12 +1255,24 @@ int implicit_create(upic_ctx* c) {
     if (s->picard && (rc = dalloc(c, &s->Jprev, 3 * (size_t)N))) return rc;
     if (c->cfg.current_predictor == UPIC_PREDICTOR_EXTRAPOLATED && (rc = dalloc(c, &s->Jold, 3 * (size_t)N)))
         return rc;
+    if ((rc = dalloc(c, &s->J0, 3 * (size_t)N)) || (rc = dalloc(c, &s->dnorm3, 3))) return rc;
+    if (c->cfg.current_predictor != UPIC_PREDICTOR_PREVIOUS && (rc = dalloc(c, &s->Jx, 3 * (size_t)N))) return rc;
+    if (c->cfg.current_predictor == UPIC_PREDICTOR_LEARNED) {
+        if ((rc = dalloc(c, &s->Jl, 3 * (size_t)N)) || (rc = dalloc(c, &s->fbuf, 4 * (size_t)N)) ||
+            (rc = dalloc(c, &s->dloss, 1)))
+            return rc;
+        const cudaError_t e = gnet::net_create(&s->net, c->nx, c->ny, c->cfg.learned_seed, c->nsm);
+        if (e != cudaSuccess)
+            return fail(c, UPIC_ERR_NOMEM, std::string("learned predictor: ") + cudaGetErrorString(e));
+    }
     for (int k = 0; k < kHist; ++k)
         if ((rc = dalloc(c, &s->hx[k], 3 * (size_t)N)) || (rc = dalloc(c, &s->hr[k], 3 * (size_t)N))) return rc;
     if (cudaMallocHost(&s->hnorm, sizeof(NormSums)) != cudaSuccess ||
         cudaMallocHost(&s->hstats, sizeof(MapStats)) != cudaSuccess ||
         cudaMallocHost(&s->hdots, sizeof(double) * 32) != cudaSuccess ||
-        cudaMallocHost(&s->hflag, sizeof(int)) != cudaSuccess)
+        cudaMallocHost(&s->hflag, sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&s->hnorm3, sizeof(NormSums) * 3) != cudaSuccess ||
+        cudaMallocHost(&s->hloss, sizeof(double)) != cudaSuccess)
         return fail(c, UPIC_ERR_NOMEM, "cudaMallocHost failed");
     std::vector<unsigned char> ex(N, 0);
     for (int i = 0; i < c->nx; ++i)
@@ -1176,6 +1290,9 @@ void implicit_destroy(upic_ctx* c) {
     if (s->hstats) cudaFreeHost(s->hstats);
     if (s->hdots) cudaFreeHost(s->hdots);
     if (s->hflag) cudaFreeHost(s->hflag);
+    if (s->hnorm3) cudaFreeHost(s->hnorm3);
+    if (s->hloss) cudaFreeHost(s->hloss);
+    gnet::net_destroy(s->net);
     delete s;
     c->imp = nullptr;
 }
@@ -1296,6 +1413,25 @@ int implicit_state_io(upic_ctx* c, StateIO& io) {
         if ((rc = state_value(c, io, have)) || (rc = state_device(c, io, s.Jold, sizeof(double) * 3 * N))) return rc;
         s.have_Jold = have != 0;
     }
+    if (s.net) {
+        int newest = 0, count = 0, use = s.use_learned ? 1 : 0;
+        long t = 0;
+        gnet::net_host_state(s.net, &newest, &count, &t, false);
+        if ((rc = state_value(c, io, newest)) || (rc = state_value(c, io, count)) || (rc = state_value(c, io, t)) ||
+            (rc = state_value(c, io, use)) || (rc = state_value(c, io, s.trained_steps)))
+            return rc;
+        if (!io.writing) {
+            if (newest < -1 || newest >= gnet::kFrames || count < 0 || count > gnet::kFrames || t < 0)
+                return fail(c, UPIC_ERR_ARGUMENT, "state file: bad learned-predictor state");
+            gnet::net_host_state(s.net, &newest, &count, &t, true);
+            s.use_learned = use != 0;
+        }
+        void* ptrs[16];
+        size_t sizes[16];
+        const size_t k = gnet::net_state_ranges(s.net, ptrs, sizes, 16);
+        for (size_t i = 0; i < k; ++i)
+            if ((rc = state_device(c, io, ptrs[i], sizes[i]))) return rc;
+    }
     return 0;
 }
 
@@ -1381,6 +1517,18 @@ int implicit_init_fields(upic_ctx* c, double* diag_row) {
     s.have_Jold = false;
     c->steps = 0;
     c->fields_ready = true;
+    if (s.net) {
+        // the learned predictor's frames restart from this state; its
+        // weights keep what they learned
+        int newest = -1, count = 0;
+        long t = 0;
+        gnet::net_host_state(s.net, &newest, &count, &t, false);
+        newest = -1;
+        count = 0;
+        gnet::net_host_state(s.net, &newest, &count, &t, true);
+        s.use_learned = false;
+        if ((rc = push_frame(c, s))) return rc;
+    }
     if ((rc = sync(c))) return rc;
     s.energy_valid = false;
     if (diag_row) {
@@ -1646,6 +1794,86 @@ extern "C" int upic_orbit_gather(upic_ctx* c, long np, const double* x, const do
         UPIC_CUDA(c, cudaMemcpyAsync(grad, s.ograd, sizeof(double) * 9 * np, cudaMemcpyDeviceToHost, c->st));
     }
     return orbit_check(c, s);
+}
+
+namespace {
+// Device scratch of one kernel-level call, freed on every return path.
+struct Scratch {
+    std::vector<void*> p;
+    ~Scratch() {
+        for (void* q : p) cudaFree(q);
+    }
+    template <typename T>
+    T* get(size_t n) {
+        void* v = nullptr;
+        if (cudaMalloc(&v, n * sizeof(T) + 16) != cudaSuccess) return nullptr;
+        p.push_back(v);
+        return reinterpret_cast<T*>(v);
+    }
+};
+}  // namespace
+
+extern "C" int upic_guess_conv(upic_ctx* c, int nx, int ny, const uint16_t* x, const uint16_t* w, const float* bias,
+                               const uint16_t* mask, int mode, int sign, void* out) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (nx < 1 || ny < 1 || (long)nx * ny > (1L << 26) || !x || !w || !out || (sign != 1 && sign != -1) ||
+        mode < gnet::kConvRelu || mode > gnet::kConvMask || (mode == gnet::kConvMask && !mask))
+        return fail(c, UPIC_ERR_ARGUMENT, "upic_guess_conv: bad grid, mode, sign or null array");
+    const size_t P = (size_t)nx * ny, act = P * gnet::kC;
+    Scratch sc;
+    uint16_t *dx = sc.get<uint16_t>(act), *dw = sc.get<uint16_t>(gnet::kW), *dm = nullptr, *dob = nullptr;
+    float *db = nullptr, *dof = nullptr;
+    int* derr = sc.get<int>(1);
+    if (!dx || !dw || !derr) return fail(c, UPIC_ERR_NOMEM, "upic_guess_conv: device allocation failed");
+    if (bias && !(db = sc.get<float>(gnet::kC))) return fail(c, UPIC_ERR_NOMEM, "upic_guess_conv: allocation");
+    if (mask && !(dm = sc.get<uint16_t>(act))) return fail(c, UPIC_ERR_NOMEM, "upic_guess_conv: allocation");
+    if (mode == gnet::kConvLinear ? !(dof = sc.get<float>(act)) : !(dob = sc.get<uint16_t>(act)))
+        return fail(c, UPIC_ERR_NOMEM, "upic_guess_conv: allocation");
+    UPIC_CUDA(c, cudaMemcpyAsync(dx, x, sizeof(uint16_t) * act, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(dw, w, sizeof(uint16_t) * gnet::kW, cudaMemcpyHostToDevice, c->st));
+    if (db) UPIC_CUDA(c, cudaMemcpyAsync(db, bias, sizeof(float) * gnet::kC, cudaMemcpyHostToDevice, c->st));
+    if (dm) UPIC_CUDA(c, cudaMemcpyAsync(dm, mask, sizeof(uint16_t) * act, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemsetAsync(derr, 0, sizeof(int), c->st));
+    gnet::ConvArgs a{};
+    a.in = dx;
+    a.w = dw;
+    a.bias = db;
+    a.mask = dm;
+    a.out_bf = dob;
+    a.out_f = dof;
+    a.nx = nx;
+    a.ny = ny;
+    a.P = (int)P;
+    a.sign = sign;
+    a.mode = mode;
+    a.err = derr;
+    UPIC_CUDA(c, mode == gnet::kConvLinear ? gnet::launch_conv_tc_full(a, c->nsm, c->st)
+                                           : gnet::launch_conv_tc(a, c->nsm, c->st));
+    if (dof) UPIC_CUDA(c, cudaMemcpyAsync(out, dof, sizeof(float) * act, cudaMemcpyDeviceToHost, c->st));
+    else UPIC_CUDA(c, cudaMemcpyAsync(out, dob, sizeof(uint16_t) * act, cudaMemcpyDeviceToHost, c->st));
+    int herr = 0;
+    UPIC_CUDA(c, cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    int rc;
+    if ((rc = sync(c))) return rc;
+    if (herr) return fail(c, UPIC_ERR_CUDA, "upic_guess_conv: a tensor-core wait timed out");
+    return UPIC_OK;
+}
+
+extern "C" int upic_guess_wgrad(upic_ctx* c, int nx, int ny, const uint16_t* dz, const uint16_t* x, float* grad) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (nx < 1 || ny < 1 || (long)nx * ny > (1L << 26) || !dz || !x || !grad)
+        return fail(c, UPIC_ERR_ARGUMENT, "upic_guess_wgrad: bad grid or null array");
+    const size_t P = (size_t)nx * ny, act = P * gnet::kC;
+    const int grid = std::max(1, std::min(2 * c->nsm, (int)((P + 255) / 256)));
+    Scratch sc;
+    uint16_t *ddz = sc.get<uint16_t>(act), *dx = sc.get<uint16_t>(act);
+    float *part = sc.get<float>((size_t)grid * gnet::kParams), *dg = sc.get<float>(gnet::kParams);
+    if (!ddz || !dx || !part || !dg) return fail(c, UPIC_ERR_NOMEM, "upic_guess_wgrad: device allocation failed");
+    UPIC_CUDA(c, cudaMemcpyAsync(ddz, dz, sizeof(uint16_t) * act, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(dx, x, sizeof(uint16_t) * act, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, gnet::launch_conv_wgrad(ddz, dx, nx, ny, part, grid, dg, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(grad, dg, sizeof(float) * gnet::kParams, cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
 }
 
 extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double* info, double* step_diag) {
