@@ -101,6 +101,10 @@ def parse():
                     help="implicit-method workload reported beside an explicit headline ('none' skips)")
     ap.add_argument("--implicit-steps", type=int, default=3,
                     help="timed steps of the implicit companion run (at most --steps)")
+    ap.add_argument("--learned-steps", type=int, default=260,
+                    help="steps of the learned-vs-extrapolated first-guess comparison (0 skips; one GPU only)")
+    ap.add_argument("--learned-train", type=int, default=200,
+                    help="training steps of the learned first guess")
     return ap.parse_args()
 
 
@@ -330,6 +334,77 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+# Learned vs extrapolated first guess of the implicit outer iteration: a
+# 256x256 periodic plasma, 128 e-/cell (8,388,608 electrons), isotropic
+# Maxwellian vth = 0.05 c with a density perturbation of amplitude 0.01 at
+# k = (1, 1), solved to a 1e-10 relative residual.
+LEARNED_CASE = dict(nx=256, ny=256, ppc=128, L=2 * np.pi / 0.3, dt=0.05, vth=0.05, amp=0.01, seed=404)
+
+
+def learned_particles(up, c):
+    p = up.generate_bimaxwellian(c["nx"], c["ny"], c["L"], c["L"], c["ppc"], (c["vth"],) * 3, seed=c["seed"])
+    # displacement xi = -amp k / |k|^2 sin(k.x): n = n0 (1 + amp cos(k.x)) to first order
+    k = 2 * np.pi / c["L"]
+    ph = k * p["x"] + k * p["y"]
+    d = -c["amp"] * np.sin(ph) / (2 * k)
+    p["x"] = p["x"] + d
+    p["y"] = p["y"] + d
+    return p
+
+
+def learned_comparison(args):
+    """Both first guesses on the same plasma: outer iterations per step,
+    wall time per step (host clock around the solver calls, which synchronise
+    every step), and the distance between the two final states."""
+    import unstaggered_pic_b200 as up
+
+    c = LEARNED_CASE
+    steps, train = args.learned_steps, min(args.learned_train, max(0, args.learned_steps - 3))
+    window = steps - min(steps, train + 2)
+    p = learned_particles(up, c)
+    deck = dict(IMPLICIT_DECK)
+    deck["nonlinear_rtol"] = 1e-10
+    res = {}
+    for pred in ("extrapolated", "learned"):
+        cfg = up.ImplicitConfig(nx=c["nx"], ny=c["ny"], Lx=c["L"], Ly=c["L"], dt=c["dt"], current_predictor=pred,
+                                learned_train_steps=train, **deck)
+        with up.Simulation(cfg) as sim:
+            sim.set_particles(p["x"], p["y"], p["P"], p["v"], p["v_prev"], p["q"], p["m"])
+            sim.init_fields(False)
+            t0 = time.perf_counter()
+            _, info_a = sim.step_implicit(steps - window, diagnostics=False)
+            t1 = time.perf_counter()
+            _, info_b = (sim.step_implicit(window, diagnostics=False) if window > 0
+                         else (None, np.zeros((0, info_a.shape[1]))))
+            t2 = time.perf_counter()
+            fields = np.stack([sim.field(f) for f in ("phi", "Ax", "Ay", "Az", "Jx", "Jy", "Jz")])
+        info = np.concatenate([info_a, info_b])
+        res[pred] = (info, fields, t1 - t0, t2 - t1)
+    cols = up.SOLVE_INFO_COLUMNS
+    out = {"workload": f"maxwellian_perturbed_{c['nx']}x{c['ny']}_ppc{c['ppc']}",
+           "particles": c["nx"] * c["ny"] * c["ppc"], "steps": steps, "training_steps": train,
+           "nonlinear_rtol": 1e-10, "data": "synthetic (seeded Maxwellian, vth 0.05, density perturbation 0.01 at "
+                                              "k = (1, 1))"}
+    for pred, (info, _, ta, tb) in res.items():
+        it = info[:, cols.index("iterations")]
+        after = info[len(info) - window:] if window > 0 else info[:0]
+        used = info[:, cols.index("predictor_used")]
+        out[pred] = {
+            "outer_iterations_per_step": float(it.mean()),
+            "outer_iterations_per_step_after_training": float(after[:, 0].mean()) if window > 0 else None,
+            "ms_per_step_training_window": 1e3 * ta / max(1, steps - window),
+            "ms_per_step_after_training": 1e3 * tb / window if window > 0 else None,
+            "guess_error_median_after_training": (float(np.median(after[:, cols.index("guess_error")]))
+                                                  if window > 0 else None),
+            "steps_using_learned_guess": int((used == 2).sum()),
+            "final_rms_residual_max": float(info[:, cols.index("final_rms_residual")].max()),
+        }
+    fe, fl = res["extrapolated"][1], res["learned"][1]
+    out["final_state_max_rel_diff"] = float(max(np.max(np.abs(fl[k] - fe[k])) / (np.max(np.abs(fe[k])) + 1e-300)
+                                                for k in range(len(fe))))
+    return out
+
+
 def make_simulation(up, w, precision="fp64", predictor="previous", warm=False):
     if w["method"] == "cn_orbit":
         cfg = up.ImplicitConfig(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], current_predictor=predictor,
@@ -572,6 +647,10 @@ def run_upic(args):
             "implicit_solve": opt.get("implicit_solve"),
             "what": "current_predictor = extrapolated (2 J^n - J^(n-1)) and local_warm_start = 1; "
                     "same tolerances, same plasma"}
+    learned = None
+    if args.learned_steps > 0 and world == 1 and WORKLOADS[args.workload]["method"] != "cn_orbit":
+        torch.cuda.empty_cache()
+        learned = learned_comparison(args)
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
@@ -587,6 +666,8 @@ def run_upic(args):
         companion.update({"metric": METRIC, "unit": METRIC, "n_gpus": world, "dtype": "f64",
                           "method": "implicit orbit-averaged GM-HC-CN step on the same plasma"})
         line["implicit"] = companion
+    if learned is not None:
+        line["learned_guess"] = learned
     print(json.dumps(line))
     return 0
 
