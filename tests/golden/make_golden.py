@@ -151,6 +151,46 @@ P3_FALLBACK_CASES = [
 ]
 
 
+# Long implicit run for the linear growth rate: 1D-2V (ny = nz = 1) cold
+# relativistic two-stream instability, beams at +-0.2 c, 1024 electrons per
+# beam on a quiet start with a 1e-3 density perturbation of mode 1, cubic
+# splines, 250 steps of dt = 0.1 (about ten e-foldings, into saturation).
+P3_LONG_CASE = ("p3_two_stream_long", dict(nx=64, ny=1, Lx=2 * np.pi / 3.0, Ly=1.0, dt=0.1, order=3, nq=8,
+                                           nyquist=True, n_steps=250), 1024, 0.2, 1e-3)
+
+
+def two_stream_particles(Lx, Ly, Lz, nb, v0, eps, n0=1.0):
+    """Quiet-start cold beams at +-v0 on the same displaced positions:
+    n = n0 (1 + eps cos(k (x + L/2))) to first order."""
+    k = 2 * np.pi / Lx
+    x0 = -Lx / 2 + (np.arange(nb) + 0.5) * Lx / nb
+    xi = -(eps / k) * np.sin(k * (x0 + Lx / 2))
+    n = 2 * nb
+    x = np.zeros((n, 3))
+    x[:, 0] = np.concatenate([x0 + xi, x0 + xi])
+    v = np.zeros((n, 3))
+    v[:nb, 0], v[nb:, 0] = v0, -v0
+    q = np.full(n, -n0 * Lx * Ly * Lz / n)
+    return x, v, q, np.abs(q)
+
+
+def p3_long_main(lib=None):
+    """Fixture of a long reference run (diagnostics of every step) whose
+    linear growth rate, energy drift and gauge residual the GPU run must
+    reproduce."""
+    lib = lib or ol.ref_p3()
+    if lib is None:
+        raise SystemExit("oracle/_ref/libref_p3.so missing: run make -C oracle")
+    name, kw, nb, v0, eps = P3_LONG_CASE
+    prob = ol.P3Problem(**kw)
+    x, v, q, m = two_stream_particles(prob.Lx, prob.Ly, prob.Lz, nb, v0, eps)
+    out = ol.p3_run(lib.ref_p3_run, prob, x, v, q, m)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), dparams=prob.dparams(), iparams=prob.iparams(),
+                        in_x=x, in_v=v, in_q=q, in_m=m, diag=out["diag"], info=out["info"],
+                        fields=out["fields"], seconds=out["seconds"])
+    print(name, "seconds", out["seconds"], "iterations", out["info"][:, 0].sum())
+
+
 # Orbit kernels: (order, knot splitting, Gauss points)
 P3_ORBIT_CASES = [(2, True, 8), (2, False, 8), (1, True, 4), (3, True, 6)]
 
@@ -331,6 +371,8 @@ if __name__ == "__main__":
         p3_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "p3_fallback":
         p3_fallback_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "p3_long":
+        p3_long_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "p1":
         p1_main()
     else:

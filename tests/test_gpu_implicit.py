@@ -419,3 +419,58 @@ def test_selective_fallback_limits():
         up.Simulation(up.ImplicitConfig(nx=8, ny=8, selective_particle_fallback=True,
                                         selective_particle_max_substeps=3))
     assert e.value.code == -1
+
+
+def growth_fit(amp, dt, lo, hi):
+    """Least-squares slope of log(amp) against time over the steps where
+    lo <= amp <= hi (the linear phase), and that window."""
+    idx = np.nonzero((amp >= lo) & (amp <= hi))[0]
+    t = idx * dt
+    return np.polyfit(t, np.log(amp[idx]), 1)[0], idx
+
+
+def test_two_stream_growth_matches_reference():
+    """A long run (250 steps, about ten e-foldings into saturation) of the
+    1D-2V cold relativistic two-stream instability against the reference's
+    run on the same quiet start: the linear growth rate of |E_x(k_x = 1)|
+    within 2%, the mode amplitude through the linear phase, and the energy
+    drift and gauge residual of every step at the reference's level."""
+    g = dict(np.load(os.path.join(GOLD, "p3_two_stream_long.npz")))
+    sim, cfg = load_sim(g)
+    nsteps = int(g["iparams"][12])
+    cols = up.IMPLICIT_DIAG_COLUMNS
+    try:
+        row0 = sim.init_fields()
+        diag, info = sim.step_implicit(nsteps)
+    finally:
+        sim.close()
+    assert np.all(info[:, 1] == 1.0)
+    ours = np.vstack([row0, diag])
+    ref = g["diag"]
+    k = cols.index("E_mode_abs")
+    a_ref, a_gpu = ref[:, k], ours[:, k]
+    # linear phase: from 4x the seeded amplitude (past the beat of the
+    # excited modes) to half the final amplitude (before saturation)
+    lo, hi = 4 * a_ref[0], 0.5 * a_ref.max()
+    rate_ref, idx = growth_fit(a_ref, cfg.dt, lo, hi)
+    rate_gpu, idx_gpu = growth_fit(a_gpu, cfg.dt, lo, hi)
+    assert len(idx) >= 50 and np.all(np.diff(idx) == 1), idx
+    assert np.array_equal(idx, idx_gpu)
+    assert abs(rate_gpu - rate_ref) <= 0.02 * abs(rate_ref), (rate_gpu, rate_ref)
+    # and the cold-beam dispersion relation 1 = wb^2/(w - k v0)^2 + wb^2/(w + k v0)^2,
+    # wb^2 = (n0/2)/gamma0^3 (longitudinal mass), is met to 3%
+    v0, k = 0.2, 2 * np.pi / cfg.Lx
+    wb2, kv = 0.5 * (1 - v0 * v0) ** 1.5, k * v0
+    w2 = np.roots([1.0, -(2 * kv * kv + 2 * wb2), kv ** 4 - 2 * wb2 * kv * kv])
+    rate_theory = np.sqrt(-np.min(w2.real))
+    assert abs(rate_gpu - rate_theory) <= 0.03 * rate_theory, (rate_gpu, rate_theory)
+    # through the linear phase the amplitudes themselves agree closely
+    lin = np.arange(idx[-1] + 1)
+    assert np.max(np.abs(a_gpu[lin] - a_ref[lin]) / a_ref[lin]) < 1e-6
+    # energy drift and gauge residual of every step at the reference's level
+    e = cols.index("total_energy")
+    drift_ref = np.abs(ref[:, e] - ref[0, e]) / ref[0, e]
+    drift_gpu = np.abs(ours[:, e] - ours[0, e]) / ours[0, e]
+    assert drift_gpu.max() <= max(10 * drift_ref.max(), 1e-12), (drift_gpu.max(), drift_ref.max())
+    gg = cols.index("gauge_relative")
+    assert np.max(ours[:, gg]) <= max(10 * np.max(ref[:, gg]), 1e-12), (np.max(ours[:, gg]), np.max(ref[:, gg]))
