@@ -105,6 +105,10 @@ def parse():
                     help="steps of the learned-vs-extrapolated first-guess comparison (0 skips; one GPU only)")
     ap.add_argument("--learned-train", type=int, default=200,
                     help="training steps of the learned first guess")
+    ap.add_argument("--ensemble-runs", type=int, default=256,
+                    help="independent runs of the ensemble comparison (0 skips; one GPU only)")
+    ap.add_argument("--ensemble-steps", type=int, default=80,
+                    help="steps of the ensemble comparison")
     return ap.parse_args()
 
 
@@ -405,6 +409,103 @@ def learned_comparison(args):
     return out
 
 
+# Ensemble of independent explicit runs of uneven sizes (the BASELINE's
+# batched-ensemble form, on the explicit 2D method): per run the node count
+# is drawn from {128, 256, 512, 1024} (grids 16x8, 16x16, 32x16, 32x32) and
+# the particle count log-uniformly from [1e4, 1e5]; Weibel bi-Maxwellian
+# plasma, dt 0.05.  Tile size and re-sort interval are autotuned per grid
+# bucket on the bucket's median run.
+ENSEMBLE_GRIDS = [(16, 8), (16, 16), (32, 16), (32, 32)]
+
+
+def ensemble_comparison(args):
+    """The runs advanced one after another with upic_step, then the same
+    runs from the same start advanced together with upic_ensemble_step (one
+    CUDA graph per period); particle-steps/s of both (host clock around the
+    calls, which return when the work is complete) and the largest state
+    difference between the two (they are bit-for-bit equal by design)."""
+    import unstaggered_pic_b200 as up
+
+    rng = np.random.default_rng(707)
+    nruns, steps = args.ensemble_runs, args.ensemble_steps
+    L0 = 2 * np.pi / 0.3
+    runs = []
+    for r in range(nruns):
+        nx, ny = ENSEMBLE_GRIDS[rng.integers(len(ENSEMBLE_GRIDS))]
+        npart = int(round(np.exp(rng.uniform(np.log(1e4), np.log(1e5)))))
+        ppc = max(1, npart // (nx * ny))
+        runs.append((nx, ny, ppc, 1000 + r))
+    t0 = time.perf_counter()
+    tuned = {}
+    for nx, ny in ENSEMBLE_GRIDS:
+        members = sorted(ppc for gx, gy, ppc, _ in runs if (gx, gy) == (nx, ny))
+        if not members:
+            continue
+        ppc = members[len(members) // 2]
+        Lx, Ly = L0 * nx / 32, L0 * ny / 32
+        p = up.generate_bimaxwellian(nx, ny, Lx, Ly, ppc, (0.02, 0.2, 0.0), seed=5)
+        make = lambda tile, si: up.Config(nx=nx, ny=ny, Lx=Lx, Ly=Ly, dt=0.05, method="bdf1", tile=tile,
+                                          sort_interval=si)
+        tile, si, _ = up.autotune_explicit(make, p, tiles=(4, 8), sort_intervals=(2, 4), steps=8)
+        tuned[f"{nx}x{ny}"] = {"tile": tile, "sort_interval": si}
+    t_tune = time.perf_counter() - t0
+
+    def start_all():
+        sims = []
+        for nx, ny, ppc, seed in runs:
+            Lx, Ly = L0 * nx / 32, L0 * ny / 32
+            t = tuned[f"{nx}x{ny}"]
+            sim = up.Simulation(up.Config(nx=nx, ny=ny, Lx=Lx, Ly=Ly, dt=0.05, method="bdf1", tile=t["tile"],
+                                          sort_interval=t["sort_interval"]))
+            p = up.generate_bimaxwellian(nx, ny, Lx, Ly, ppc, (0.02, 0.2, 0.0), seed=seed)
+            sim.set_particles(p["x"], p["y"], p["P"], p["v"], p["v_prev"], p["q"], p["m"])
+            sim.init_fields(False)
+            sims.append(sim)
+        return sims
+
+    total = sum(nx * ny * ppc for nx, ny, ppc, _ in runs)
+    seq = start_all()
+    for sim in seq:
+        sim.step(3, 0)
+    t0 = time.perf_counter()
+    for sim in seq:
+        sim.step(steps, 0)
+    t_seq = time.perf_counter() - t0
+    ens_sims = start_all()
+    for sim in ens_sims:
+        sim.step(3, 0)
+    ens = up.Ensemble(ens_sims)
+    t0 = time.perf_counter()
+    ens.step(ens.period)  # records the graph
+    t_first = time.perf_counter() - t0
+    left = steps - ens.period
+    t0 = time.perf_counter()
+    if left > 0:
+        ens.step(left)
+    t_ens = time.perf_counter() - t0
+    diff = 0.0
+    for a, b in zip(seq, ens_sims):
+        pa, pb = a.get_particles(), b.get_particles()
+        diff = max(diff, float(np.max(np.abs(pa["v"] - pb["v"]))))
+    # the sequential runs took `steps` steps, the ensemble `steps` too
+    ens.close()
+    for sim in seq + ens_sims:
+        sim.close()
+    return {"workload": f"{nruns} independent explicit Weibel runs, grids {ENSEMBLE_GRIDS}, "
+                        f"1e4-1e5 particles each (log-uniform)",
+            "runs": nruns, "particles": total, "steps": steps, "period": ens.period,
+            "tuned": tuned, "autotune_seconds": t_tune,
+            "sequential": {"value": total * steps / t_seq, "unit": METRIC, "ms_per_step": 1e3 * t_seq / steps,
+                           "what": "upic_step(run, K) for each run in turn"},
+            "ensemble": {"value": total * left / t_ens if left > 0 else None, "unit": METRIC,
+                         "ms_per_step": 1e3 * t_ens / left if left > 0 else None,
+                         "first_period_seconds_with_capture": t_first,
+                         "what": "upic_ensemble_step: one CUDA graph launch per period, every run on its own "
+                                 "stream; timed after the period that records the graph"},
+            "max_abs_velocity_difference": diff,
+            "data": "synthetic (seeded bi-Maxwellian per run)"}
+
+
 def make_simulation(up, w, precision="fp64", predictor="previous", warm=False):
     if w["method"] == "cn_orbit":
         cfg = up.ImplicitConfig(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], current_predictor=predictor,
@@ -647,6 +748,10 @@ def run_upic(args):
             "implicit_solve": opt.get("implicit_solve"),
             "what": "current_predictor = extrapolated (2 J^n - J^(n-1)) and local_warm_start = 1; "
                     "same tolerances, same plasma"}
+    ensemble = None
+    if args.ensemble_runs > 0 and world == 1 and WORKLOADS[args.workload]["method"] != "cn_orbit":
+        torch.cuda.empty_cache()
+        ensemble = ensemble_comparison(args)
     learned = None
     if args.learned_steps > 0 and world == 1 and WORKLOADS[args.workload]["method"] != "cn_orbit":
         torch.cuda.empty_cache()
@@ -668,6 +773,8 @@ def run_upic(args):
         line["implicit"] = companion
     if learned is not None:
         line["learned_guess"] = learned
+    if ensemble is not None:
+        line["ensemble"] = ensemble
     print(json.dumps(line))
     return 0
 

@@ -398,6 +398,27 @@ int upic_orbit_gather(upic_ctx* ctx, long np, const double* x, const double* y, 
                       const double* mesh, const double* An, const double* Anp1, double* gathered,
                       double* grad);
 
+/* Ensembles of independent runs of the explicit methods (no counterpart in
+ * the reference, whose runs are one process each).  Each run is a context
+ * created, loaded and started as usual (upic_create, upic_set_particles,
+ * upic_init_fields) with its own grid, particle count, tiling and re-sort
+ * interval; upic_ensemble_step advances every run by nsteps with the same
+ * result as upic_step(run, nsteps, 0, NULL) on each, but records `period`
+ * steps of all runs (period: the least common multiple of 5 and twice every
+ * run's sort_interval, upic_ensemble_period) into one CUDA graph, each run's
+ * kernels on its own stream, and replays it: one launch advances all runs
+ * by `period` steps.  Steps beyond a multiple of the period run with
+ * ordinary launches.  No diagnostics rows are produced (call upic_step on a
+ * run for those).  The runs stay owned by the caller and must not be used
+ * by other calls while upic_ensemble_step runs; the call returns when every
+ * run's work is complete.  Errors are reported on the first run's context
+ * (upic_last_error(runs[0])), or on NULL for upic_ensemble_create. */
+typedef struct upic_ensemble upic_ensemble;
+int upic_ensemble_create(upic_ctx* const* runs, int nruns, upic_ensemble** ens);
+int upic_ensemble_period(const upic_ensemble* ens, int* period);
+int upic_ensemble_step(upic_ensemble* ens, int nsteps);
+int upic_ensemble_destroy(upic_ensemble* ens);
+
 /* Kernel-level pieces of the learned predictor's network (any context; no
  * counterpart in the reference).  Activations are nx*ny x 32 bf16 (raw
  * uint16 bits), pixel p = ix*ny + iy; w is 32 x 288 bf16, row = output

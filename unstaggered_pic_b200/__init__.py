@@ -13,7 +13,8 @@ import numpy as np
 
 from ._native import UPIC_ERR, UpicConfig, c_dp, lib
 
-__all__ = ["UpicError", "Config", "ImplicitConfig", "NonrelConfig", "Simulation", "generate_bimaxwellian",
+__all__ = ["UpicError", "Config", "ImplicitConfig", "NonrelConfig", "Simulation", "Ensemble", "autotune_explicit",
+           "generate_bimaxwellian",
            "DIAG_COLUMNS", "IMPLICIT_DIAG_COLUMNS", "NONREL_DIAG_COLUMNS", "SOLVE_INFO_COLUMNS",
            "STEP_DIAG_COLUMNS", "METHODS",
            "FIELDS"]
@@ -428,6 +429,69 @@ class Simulation:
         h = _f64(hist).ravel()
         self._check(lib().upic_solve_bdf(self._ctx, _p(_f64(source).ravel()), _p(h), _p(out)))
         return out.reshape(self.config.nx, self.config.ny)
+
+
+class Ensemble:
+    """Independent explicit-method runs (loaded and started Simulations,
+    each with its own grid, particles, tiling and re-sort interval) advanced
+    together: `period` steps of all runs are recorded into one CUDA graph and
+    replayed (upic_ensemble_*).  The Simulations stay usable afterwards."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        arr = (ctypes.c_void_p * len(self.sims))(*[s._ctx.value for s in self.sims])
+        self._e = ctypes.c_void_p()
+        rc = lib().upic_ensemble_create(arr, len(self.sims), ctypes.byref(self._e))
+        if rc != 0:
+            raise UpicError(rc, lib().upic_last_error(None).decode())
+        p = ctypes.c_int()
+        lib().upic_ensemble_period(self._e, ctypes.byref(p))
+        self.period = p.value
+
+    def step(self, nsteps):
+        rc = lib().upic_ensemble_step(self._e, int(nsteps))
+        if rc != 0:
+            raise UpicError(rc, lib().upic_last_error(self.sims[0]._ctx).decode())
+
+    def close(self):
+        if self._e:
+            lib().upic_ensemble_destroy(self._e)
+            self._e = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def autotune_explicit(make_config, particles, tiles=(4, 8, 16), sort_intervals=(2, 4, 8), steps=8, warmup=3):
+    """Pick the deposit tile edge and re-sort interval of an explicit run by
+    timing each candidate on the run's own particles: make_config(tile,
+    sort_interval) returns a Config; particles is the dict of
+    generate_bimaxwellian.  Returns (tile, sort_interval, {candidate: ms per
+    step}), steps timed by the host clock around upic_step (which returns
+    when its work is complete)."""
+    import time
+    times = {}
+    for tile in tiles:
+        for si in sort_intervals:
+            with Simulation(make_config(tile, si)) as sim:
+                p = particles
+                sim.set_particles(p["x"], p["y"], p["P"], p["v"], p["v_prev"], p["q"], p["m"])
+                sim.init_fields(False)
+                sim.step(warmup, 0)
+                t0 = time.perf_counter()
+                sim.step(steps, 0)
+                times[(tile, si)] = 1e3 * (time.perf_counter() - t0) / steps
+    best = min(times, key=times.get)
+    return best[0], best[1], times
 
 
 def generate_bimaxwellian(nx, ny, Lx, Ly, ppc, uth, udrift=(0.0, 0.0, 0.0), c=1.0, n0=1.0, seed=1):

@@ -52,6 +52,11 @@ SYMBOLS = {
     "upic_guess_conv": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 4
                         + [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "upic_guess_wgrad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 3),
+    "upic_ensemble_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "upic_ensemble_period": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "upic_ensemble_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "upic_ensemble_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "upic_deposit_current_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                     ctypes.c_double, ctypes.c_long, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

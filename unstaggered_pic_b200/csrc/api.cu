@@ -923,6 +923,7 @@ int upic_save_state(upic_ctx* ctx, const char* path) {
 }
 
 int upic_load_state(upic_ctx* ctx, const char* path) {
+    if (ctx) ++ctx->generation;
     if (ctx && ctx->st) {
         const cudaError_t e = cudaStreamSynchronize(ctx->st);
         if (e != cudaSuccess) return fail(ctx, UPIC_ERR_CUDA, cudaGetErrorString(e));
@@ -945,6 +946,7 @@ int upic_destroy(upic_ctx* c) {
 
 int upic_set_stream(upic_ctx* c, void* stream) {
     if (!c) return UPIC_ERR_ARGUMENT;
+    ++c->generation;
     UPIC_CUDA(c, cudaStreamSynchronize(c->st));
     c->st = stream ? reinterpret_cast<cudaStream_t>(stream) : c->own;
     return UPIC_OK;
@@ -1038,6 +1040,7 @@ static int get_particles_mixed(upic_ctx* c, long np, double* x, double* y, doubl
 int upic_set_particles(upic_ctx* c, long np, const double* x, const double* y, const double* P,
                        const double* v, const double* v_prev, const double* q, const double* m) {
     if (!c) return UPIC_ERR_ARGUMENT;
+    ++c->generation;
     if (np < 0 || np > 0x7fffffffL) return fail(c, UPIC_ERR_ARGUMENT, "particle count out of range");
     if (np > 0 && (!x || !y || !P || !v || !v_prev || !q || !m))
         return fail(c, UPIC_ERR_ARGUMENT, "null particle array");
@@ -1129,6 +1132,7 @@ int upic_get_particles(upic_ctx* c, long np, double* x, double* y, double* P, do
 }
 
 int upic_init_fields(upic_ctx* c, double* diag_row) {
+    if (c) ++c->generation;
     if (!c) return UPIC_ERR_ARGUMENT;
     if (c->imp) return implicit_init_fields(c, diag_row);
     if (c->cap == 0 && c->np == 0) return fail(c, UPIC_ERR_STATE, "upic_set_particles first");
@@ -1184,6 +1188,17 @@ int upic_step(upic_ctx* c, int nsteps, int diag_stride, double* diag) {
     if (c->imp) return fail(c, UPIC_ERR_STATE, "the implicit method advances with upic_step_implicit");
     if (!c->fields_ready) return fail(c, UPIC_ERR_STATE, "upic_init_fields first");
     if (nsteps < 0) return fail(c, UPIC_ERR_ARGUMENT, "nsteps < 0");
+    return upic_host::explicit_advance(c, nsteps, diag_stride, diag, true);
+}
+
+}  // extern "C"
+
+namespace upic_host {
+
+// The explicit step loop of upic_step.  Without diagnostics rows and with
+// final_sync false it only queues work on the context's stream (no host
+// synchronisation, no allocation), so it can be captured into a CUDA graph.
+int explicit_advance(upic_ctx* c, int nsteps, int diag_stride, double* diag, bool final_sync) {
     const int N = c->N;
     int na, nb;
     double a[3], b[5];
@@ -1252,8 +1267,12 @@ int upic_step(upic_ctx* c, int nsteps, int diag_stride, double* diag) {
         c->steps = step;
         c->steps_since_sort++;
     }
-    return sync(c);
+    return final_sync ? sync(c) : 0;
 }
+
+}  // namespace upic_host
+
+extern "C" {
 
 int upic_profile_enable(upic_ctx* c, int on) {
     if (!c) return UPIC_ERR_ARGUMENT;
@@ -1279,6 +1298,7 @@ int upic_profile_read(upic_ctx* c, double* push_ms, long* push_launches, long* k
 }
 
 int upic_set_background(upic_ctx* c, const double* rho_bg) {
+    if (c) ++c->generation;
     if (!c) return UPIC_ERR_ARGUMENT;
     if (c->imp) return fail(c, UPIC_ERR_STATE, "the implicit method has a uniform background (n0)");
     if (!rho_bg) {

@@ -80,6 +80,10 @@ struct upic_ctx {
 
     int head = 0;
     long steps = 0;
+    // bumped by every call that may reallocate or reset the state (particle
+    // upload, start-up, state load, stream or background change): a CUDA
+    // graph recorded before such a call is stale
+    long generation = 0;
     bool fields_ready = false;
     int steps_since_sort = 0;
     int sort_interval = 4;
@@ -153,6 +157,7 @@ int state_value(upic_ctx* c, StateIO& io, T& v) {
     return state_bytes(c, io, &v, sizeof(T));
 }
 int implicit_state_io(upic_ctx* c, StateIO& io);
+int explicit_advance(upic_ctx* c, int nsteps, int diag_stride, double* diag, bool final_sync);
 void implicit_mark_unloaded(upic_ctx* c);
 
 HostScan scan_particles(long np, const double* x, const double* y, const double* v, const double* q,

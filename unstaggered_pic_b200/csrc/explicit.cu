@@ -10,6 +10,9 @@
 // already deposits the NEXT step's current J^{n+1} at wrap(x^n + dt v^n) with
 // v^n (what the reference's next iteration deposits).  The field work of a
 // step is a handful of grid kernels in k-space (histories kept as spectra).
+#include <map>
+#include <mutex>
+#include <utility>
 #include "kernels.h"
 #include "upic_common.cuh"
 
@@ -711,11 +714,24 @@ cudaError_t launch_one(const TileGeom& tg, const PushArgs& a, int grid, cudaStre
 
 template <int MODE, int NCOMP, bool UNIFORM>
 cudaError_t set_smem_one(int bytes) {
-    return cudaFuncSetAttribute(push_deposit_kernel<MODE, NCOMP, UNIFORM>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return raise_smem_limit(reinterpret_cast<const void*>(push_deposit_kernel<MODE, NCOMP, UNIFORM>), bytes);
 }
 
 }  // namespace
+
+cudaError_t raise_smem_limit(const void* func, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    int& cur = limit[{func, dev}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
 
 static long g_launches = 0;
 void count_launches(long n) { __atomic_fetch_add(&g_launches, n, __ATOMIC_RELAXED); }

@@ -2239,8 +2239,7 @@ cudaError_t implicit_configure_smem(const TileGeom& tg, int order, bool split, b
     for (int u = 0; u < 2; ++u) {
         MapKernel k = map_kernel(order, u != 0, split, picard);
         if (!k) return cudaErrorInvalidValue;
-        const cudaError_t e =
-            cudaFuncSetAttribute(reinterpret_cast<const void*>(k), cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), b);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

@@ -10,6 +10,11 @@ namespace upic {
 // upic_profile_read.  Each launcher adds the kernels it starts.
 void count_launches(long n);
 long launches_total();
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device.  The limit belongs to the function, not to a context, so
+// it only ever grows: contexts with different tile windows in one process
+// each keep room for their own launches.
+cudaError_t raise_smem_limit(const void* func, int bytes);
 
 // ---------------------------------------------------------------------------
 // FFT (fft.cu)

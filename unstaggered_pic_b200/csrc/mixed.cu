@@ -485,8 +485,7 @@ cudaError_t launch_mixed_one(const TileGeom& tg, const MixedPushArgs& a, int gri
 
 template <int MODE, int NCOMP, bool UNIFORM>
 cudaError_t set_mixed_smem(int bytes) {
-    return cudaFuncSetAttribute(push_deposit_mixed_kernel<MODE, NCOMP, UNIFORM>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return raise_smem_limit(reinterpret_cast<const void*>(push_deposit_mixed_kernel<MODE, NCOMP, UNIFORM>), bytes);
 }
 
 }  // namespace
