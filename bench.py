@@ -109,6 +109,10 @@ def parse():
                     help="independent runs of the ensemble comparison (0 skips; one GPU only)")
     ap.add_argument("--ensemble-steps", type=int, default=80,
                     help="steps of the ensemble comparison")
+    ap.add_argument("--implicit-ensemble-runs", type=int, default=64,
+                    help="1D-2V two-stream runs of the implicit ensemble comparison (0 skips; one GPU only)")
+    ap.add_argument("--implicit-ensemble-steps", type=int, default=10,
+                    help="steps of the implicit ensemble comparison")
     return ap.parse_args()
 
 
@@ -506,6 +510,75 @@ def ensemble_comparison(args):
             "data": "synthetic (seeded bi-Maxwellian per run)"}
 
 
+# Implicit ensemble (BASELINE's batched-ensemble configuration): 1D-2V
+# periodic two-stream runs, Nx from {128, 256, 512, 1024}, particle count
+# log-uniform in [1e4, 1e5] (the configuration's upper bound is 1e6),
+# counter-drifting Maxwellian beams at +-v0, v0 uniform in [0.05, 0.3] c,
+# vth 0.01 c, cubic splines, dt 0.1.
+def implicit_ensemble_comparison(args):
+    """The runs advanced one after another with upic_step_implicit, then
+    the same runs together with upic_ensemble_step (a pool of host threads,
+    each run on its own stream); particle-steps/s of both and the largest
+    state difference (bit-for-bit equal by design)."""
+    import unstaggered_pic_b200 as up
+
+    rng = np.random.default_rng(909)
+    nruns, steps = args.implicit_ensemble_runs, args.implicit_ensemble_steps
+    deck = dict(IMPLICIT_DECK)
+    deck["spline_order"] = 3
+    runs = []
+    for r in range(nruns):
+        nx = int(rng.choice([128, 256, 512, 1024]))
+        npart = 2 * int(round(np.exp(rng.uniform(np.log(1e4), np.log(1e5))) / 2))
+        v0 = float(rng.uniform(0.05, 0.3))
+        runs.append((nx, npart, v0, 3000 + r))
+
+    def start_all():
+        sims = []
+        for nx, npart, v0, seed in runs:
+            g = np.random.default_rng(seed)
+            Lx = 2 * np.pi * v0 / 0.6 * 4  # four wavelengths of the fastest-growing cold mode
+            nb = npart // 2
+            x = g.uniform(-Lx / 2, Lx / 2, npart)
+            v = np.zeros((npart, 3))
+            v[:nb, 0], v[nb:, 0] = v0, -v0
+            v[:, :2] += 0.01 * g.normal(size=(npart, 2))
+            q = np.full(npart, -Lx / npart)
+            cfg = up.ImplicitConfig(nx=nx, ny=1, Lx=Lx, Ly=1.0, dt=0.1, **deck)
+            sim = up.Simulation(cfg)
+            sim.set_particles(x, np.zeros(npart), np.zeros((npart, 3)), v, v, q, np.abs(q))
+            sim.init_fields(False)
+            sims.append(sim)
+        return sims
+
+    total = sum(n for _, n, _, _ in runs)
+    seq = start_all()
+    t0 = time.perf_counter()
+    for sim in seq:
+        sim.step_implicit(steps, diagnostics=False)
+    t_seq = time.perf_counter() - t0
+    par = start_all()
+    ens = up.Ensemble(par)
+    t0 = time.perf_counter()
+    ens.step(steps)
+    t_ens = time.perf_counter() - t0
+    diff = 0.0
+    for a, b in zip(seq, par):
+        diff = max(diff, float(np.max(np.abs(a.get_particles()["v"] - b.get_particles()["v"]))))
+    ens.close()
+    for sim in seq + par:
+        sim.close()
+    return {"workload": f"{nruns} independent 1D-2V two-stream runs (implicit GM-HC-CN, cubic), Nx from "
+                        "{128, 256, 512, 1024}, 1e4-1e5 particles each (log-uniform), v0 in [0.05, 0.3] c",
+            "runs": nruns, "particles": total, "steps": steps,
+            "sequential": {"value": total * steps / t_seq, "unit": METRIC, "ms_per_step": 1e3 * t_seq / steps,
+                           "what": "upic_step_implicit(run, K) for each run in turn"},
+            "ensemble": {"value": total * steps / t_ens, "unit": METRIC, "ms_per_step": 1e3 * t_ens / steps,
+                         "what": "upic_ensemble_step: runs on a pool of host threads, each on its own stream"},
+            "max_abs_velocity_difference": diff,
+            "data": "synthetic (seeded beams per run)"}
+
+
 def make_simulation(up, w, precision="fp64", predictor="previous", warm=False):
     if w["method"] == "cn_orbit":
         cfg = up.ImplicitConfig(nx=w["nx"], ny=w["ny"], Lx=w["L"], Ly=w["L"], dt=w["dt"], current_predictor=predictor,
@@ -752,6 +825,10 @@ def run_upic(args):
     if args.ensemble_runs > 0 and world == 1 and WORKLOADS[args.workload]["method"] != "cn_orbit":
         torch.cuda.empty_cache()
         ensemble = ensemble_comparison(args)
+    implicit_ensemble = None
+    if args.implicit_ensemble_runs > 0 and world == 1 and WORKLOADS[args.workload]["method"] != "cn_orbit":
+        torch.cuda.empty_cache()
+        implicit_ensemble = implicit_ensemble_comparison(args)
     learned = None
     if args.learned_steps > 0 and world == 1 and WORKLOADS[args.workload]["method"] != "cn_orbit":
         torch.cuda.empty_cache()
@@ -775,6 +852,8 @@ def run_upic(args):
         line["learned_guess"] = learned
     if ensemble is not None:
         line["ensemble"] = ensemble
+    if implicit_ensemble is not None:
+        line["implicit_ensemble"] = implicit_ensemble
     print(json.dumps(line))
     return 0
 

@@ -398,8 +398,8 @@ int upic_orbit_gather(upic_ctx* ctx, long np, const double* x, const double* y, 
                       const double* mesh, const double* An, const double* Anp1, double* gathered,
                       double* grad);
 
-/* Ensembles of independent runs of the explicit methods (no counterpart in
- * the reference, whose runs are one process each).  Each run is a context
+/* Ensembles of independent runs (no counterpart in the reference, whose
+ * runs are one process each).  Each run is a context
  * created, loaded and started as usual (upic_create, upic_set_particles,
  * upic_init_fields) with its own grid, particle count, tiling and re-sort
  * interval; upic_ensemble_step advances every run by nsteps with the same
@@ -412,7 +412,13 @@ int upic_orbit_gather(upic_ctx* ctx, long np, const double* x, const double* y, 
  * run for those).  The runs stay owned by the caller and must not be used
  * by other calls while upic_ensemble_step runs; the call returns when every
  * run's work is complete.  Errors are reported on the first run's context
- * (upic_last_error(runs[0])), or on NULL for upic_ensemble_create. */
+ * (upic_last_error(runs[0])), or on NULL for upic_ensemble_create.
+ * An ensemble of implicit-method runs (all CN_ORBIT or CN_ORBIT_NONREL;
+ * methods of the two kinds cannot be mixed) cannot be recorded, since each
+ * step's iteration count is decided on the host: upic_ensemble_step then
+ * advances every run with upic_step_implicit(run, nsteps, NULL, NULL, NULL)
+ * on a pool of host threads, each run on its own stream, and the period is
+ * 1. */
 typedef struct upic_ensemble upic_ensemble;
 int upic_ensemble_create(upic_ctx* const* runs, int nruns, upic_ensemble** ens);
 int upic_ensemble_period(const upic_ensemble* ens, int* period);

@@ -125,3 +125,62 @@ def test_contexts_with_different_windows_coexist():
     finally:
         for sim in sims:
             sim.close()
+
+
+IMPLICIT_DECK = dict(Lz=1.0, kappa=1.0, sigma1=1.0, sigma2=1.0, n0=1.0, orbit_quad_order=8,
+                     split_orbit_at_knots=True, nyquist_projection=True, nonlinear_rtol=1e-10,
+                     nonlinear_atol=1e-13, nonlinear_max_iter=80, anderson_damping=0.5,
+                     uniform_local_rtol=1e-12, uniform_local_atol=1e-14, uniform_local_max_iter=64)
+
+
+def two_stream_1d(nx, nb, v0, eps=1e-3):
+    """1D-2V (ny = 1) cold beams at +-v0 on a quiet start, Project3 coordinates."""
+    Lx = 2 * np.pi * v0 / 0.6
+    k = 2 * np.pi / Lx
+    x0 = -Lx / 2 + (np.arange(nb) + 0.5) * Lx / nb
+    x0 = x0 - (eps / k) * np.sin(k * (x0 + Lx / 2))
+    x = np.concatenate([x0, x0])
+    v = np.zeros((2 * nb, 3))
+    v[:nb, 0], v[nb:, 0] = v0, -v0
+    q = np.full(2 * nb, -Lx / (2 * nb))
+    return Lx, x, v, q, np.abs(q)
+
+
+def test_implicit_ensemble_matches_runs_alone():
+    """Implicit runs (1D-2V two-stream of uneven sizes, cubic splines, and a
+    2D non-relativistic run) advanced on the ensemble's thread pool equal the
+    same runs advanced alone, bit for bit."""
+    specs = []
+    for nx, nb, v0 in ((64, 512, 0.2), (128, 1500, 0.15), (32, 300, 0.3)):
+        Lx, x, v, q, m = two_stream_1d(nx, nb, v0)
+        cfg = dict(nx=nx, ny=1, Lx=Lx, Ly=1.0, dt=0.1, spline_order=3, **IMPLICIT_DECK)
+        specs.append((up.ImplicitConfig, cfg, (np.stack([x, np.zeros_like(x), np.zeros_like(x)], 1), None, v, q, m)))
+    L = 2 * np.pi
+    p = up.generate_bimaxwellian(16, 16, L, L, 8, (0.05, 0.05, 0.0), seed=6)
+    specs.append((up.NonrelConfig, dict(nx=16, ny=16, Lx=L, Ly=L, dt=0.05),
+                  (np.stack([p["x"], p["y"], np.zeros_like(p["x"])], 1), None, p["v"], p["q"], p["m"])))
+
+    def start_impl(cls, kw, parts):
+        sim = up.Simulation(cls(**kw))
+        x, _, v, q, m = parts
+        sim.set_particles(x[:, 0], x[:, 1], np.zeros_like(v), v, v, q, m)
+        sim.init_fields(False)
+        return sim
+
+    alone = [start_impl(*s) for s in specs]
+    together = [start_impl(*s) for s in specs]
+    try:
+        with up.Ensemble(together) as ens:
+            assert ens.period == 1
+            ens.step(4)
+        for sim in alone:
+            sim.step_implicit(4, diagnostics=False)
+        for a, b in zip(alone, together):
+            sa, sb = state(a), state(b)
+            for k in sa:
+                assert np.array_equal(sa[k], sb[k]), k
+        with pytest.raises(up.UpicError):
+            up.Ensemble([alone[0], start(*run_specs()[0])])
+    finally:
+        for s in alone + together:
+            s.close()

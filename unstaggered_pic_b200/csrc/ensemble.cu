@@ -12,10 +12,19 @@
 // the graph was captured at and no call has since reallocated or reset it
 // (the context's generation count), otherwise the next step call captures
 // again.
+//
+// Implicit-method runs (CN_ORBIT, CN_ORBIT_NONREL) decide their outer
+// iteration count on the host after every map evaluation, so their steps
+// cannot be recorded; an ensemble of them advances each run on a pool of
+// host threads instead (every run on its own stream), so that the small
+// kernels and synchronisations of different runs overlap on the GPU.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "context.h"
@@ -30,6 +39,7 @@ struct upic_ensemble {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int period = 0;
+    bool implicit = false;
     // per run: history head, re-sort counter and current particle buffer
     // where the graph starts and where it ends
     std::vector<int> head0, count0, cur0, head1, count1, cur1;
@@ -129,6 +139,42 @@ int sync_all(upic_ensemble* e) {
 
 }  // namespace
 
+extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double* info, double* step_diag);
+
+namespace {
+
+// Implicit runs: a pool of host threads, each taking the next run and
+// advancing it by nsteps with upic_step_implicit.
+int step_threads(upic_ensemble* e, int nsteps) {
+    const int n = (int)e->runs.size();
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int T = std::max(1, std::min({n, hw, 64}));
+    std::atomic<int> next{0};
+    std::vector<int> rc(n, 0);
+    auto work = [&]() {
+        for (int i = next++; i < n; i = next++) {
+            upic_ctx* c = e->runs[i];
+            if (cudaSetDevice(c->device) != cudaSuccess) {
+                rc[i] = UPIC_ERR_CUDA;
+                continue;
+            }
+            rc[i] = upic_step_implicit(c, nsteps, nullptr, nullptr, nullptr);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; ++t) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    for (int i = 0; i < n; ++i)
+        if (rc[i]) {
+            if (i == 0) return rc[0];
+            return ens_fail(e, rc[i], "ensemble run " + std::to_string(i) + ": " + e->runs[i]->err);
+        }
+    return 0;
+}
+
+}  // namespace
+
 extern "C" {
 
 int upic_ensemble_create(upic_ctx* const* runs, int nruns, upic_ensemble** out) {
@@ -143,9 +189,9 @@ int upic_ensemble_create(upic_ctx* const* runs, int nruns, upic_ensemble** out) 
         if (!c) return fail(nullptr, UPIC_ERR_ARGUMENT, "upic_ensemble_create: null run");
         for (int q = 0; q < r; ++q)
             if (v[q] == c) return fail(nullptr, UPIC_ERR_ARGUMENT, "upic_ensemble_create: a run appears twice");
-        if (c->imp)
+        if ((c->imp != nullptr) != (v[0]->imp != nullptr))
             return fail(nullptr, UPIC_ERR_ARGUMENT,
-                        "upic_ensemble_create: ensembles advance the explicit methods (bdf1, bdf2) only");
+                        "upic_ensemble_create: runs of explicit and implicit methods cannot share an ensemble");
         if (!c->fields_ready) return fail(nullptr, UPIC_ERR_STATE, "upic_ensemble_create: upic_init_fields first");
         if (c->profiling) return fail(nullptr, UPIC_ERR_STATE, "upic_ensemble_create: a run has profiling enabled");
         if (c->device != dev) return fail(nullptr, UPIC_ERR_ARGUMENT, "upic_ensemble_create: runs on another device");
@@ -154,7 +200,8 @@ int upic_ensemble_create(upic_ctx* const* runs, int nruns, upic_ensemble** out) 
     }
     upic_ensemble* e = new upic_ensemble();
     e->runs = v;
-    e->period = (int)period;
+    e->implicit = v[0]->imp != nullptr;
+    e->period = e->implicit ? 1 : (int)period;
     e->join.assign(nruns, nullptr);
     e->head0.assign(nruns, 0);
     e->count0.assign(nruns, 0);
@@ -185,8 +232,9 @@ int upic_ensemble_step(upic_ensemble* e, int nsteps) {
     if (!e) return UPIC_ERR_ARGUMENT;
     if (nsteps < 0) return ens_fail(e, UPIC_ERR_ARGUMENT, "upic_ensemble_step: nsteps < 0");
     for (upic_ctx* c : e->runs)
-        if (!c->fields_ready || c->profiling || c->imp)
+        if (!c->fields_ready || c->profiling || (c->imp != nullptr) != e->implicit)
             return ens_fail(e, UPIC_ERR_STATE, "upic_ensemble_step: a run was reset or has profiling enabled");
+    if (e->implicit) return step_threads(e, nsteps);
     int rc, left = nsteps;
     // work queued before on the runs' own streams is complete: every API
     // call that queues work on a run synchronises before it returns
