@@ -115,6 +115,14 @@ TileGeom make_tiles(int nx, int ny, int tile, int guard, int lo, int hi) {
 
 int iota(upic_ctx* c, int* id, long n);
 
+int choose_chunk(long np, int grid, int max_chunk) {
+    long t = (np + grid - 1) / (grid > 0 ? grid : 1);
+    t = (t + kMinChunk - 1) / kMinChunk * kMinChunk;
+    if (t < kMinChunk) t = kMinChunk;
+    if (t > max_chunk) t = max_chunk;
+    return (int)t;
+}
+
 int alloc_soa(upic_ctx* c, ParticleSoA& s, long cap, bool with_state, bool with_qm) {
     int rc = 0;
     // two elements of padding: bulk prefetches widen their ranges to 16-byte
@@ -184,7 +192,8 @@ int alloc_sortwork(upic_ctx* c, SortWork& w, long cap, const TileGeom& tg) {
     if ((rc = dalloc(c, &w.tile_count, ntiles))) return rc;
     if ((rc = dalloc(c, &w.tile_start, ntiles + 1))) return rc;
     if ((rc = dalloc(c, &w.tile_chunks, ntiles))) return rc;
-    const long chunks = cap / tg.chunk + ntiles + 1;
+    // chunk table for the smallest chunk size choose_chunk picks
+    const long chunks = cap / kMinChunk + ntiles + 1;
     if ((rc = dalloc(c, &w.chunks, chunks))) return rc;
     if ((rc = dalloc(c, &w.nchunks, 1))) return rc;
     w.cap = cap;
@@ -851,7 +860,7 @@ int explicit_state_io(upic_ctx* c, StateIO& io) {
     }
     if ((rc = state_value(c, io, nch))) return rc;
     if (nch > 0) {
-        const long chunk_cap = c->cap / c->tg.chunk + c->tg.ntx * c->tg.nty + 1;
+        const long chunk_cap = c->cap / kMinChunk + c->tg.ntx * c->tg.nty + 1;
         if (nch > chunk_cap) return fail(c, UPIC_ERR_ARGUMENT, "state file: chunk list larger than the context's");
         if ((rc = state_device(c, io, c->sw.chunks, sizeof(Chunk) * nch))) return rc;
         if (!io.writing) UPIC_CUDA(c, cudaMemcpy(c->sw.nchunks, &nch, sizeof(int), cudaMemcpyHostToDevice));

@@ -32,6 +32,7 @@ namespace upic_host {
 
 constexpr int kHist = 5;         // Anderson memory + 1 (memory <= 4)
 constexpr int kNormGrid = 296;
+constexpr int kMaxImplicitChunk = 1024;
 
 struct ImplicitState {
     int order = 2, nq = 8, mnq = 8;
@@ -1211,7 +1212,7 @@ int implicit_create(upic_ctx* c) {
     s->tg.key_origin_x = 0.5 * cf.Lx;
     s->tg.key_origin_y = 0.5 * cf.Ly;
     s->tg.key_shift = 0.0;
-    s->tg.chunk = 1024;
+    s->tg.chunk = kMaxImplicitChunk;
     const bool split = cf.split_orbit_at_knots != 0;
     if (implicit_configure_smem(s->tg, s->order, split, s->picard) != cudaSuccess)
         return fail(c, UPIC_ERR_CUDA, "cudaFuncSetAttribute (implicit map) failed");
@@ -1315,6 +1316,7 @@ int implicit_set_particles(upic_ctx* c, long np, const double* x, const double* 
     }
     if ((rc = ensure_tmp3(c, np))) return rc;
     s.np = np;
+    s.tg.chunk = choose_chunk(np, s.grid, kMaxImplicitChunk);
     s.cur = 0;
     s.uniform = uniform;
     s.q0 = np ? q[0] : 0.0;
@@ -1388,6 +1390,7 @@ int implicit_state_io(upic_ctx* c, StateIO& io) {
         if ((rc = ensure_tmp3(c, np))) return rc;
         s.cur = 0;
         s.np = np;
+        s.tg.chunk = choose_chunk(np, s.grid, kMaxImplicitChunk);
         s.uniform = uniform != 0;
         s.loaded = loaded != 0;
         s.ready = ready != 0;

@@ -164,6 +164,15 @@ HostScan scan_particles(long np, const double* x, const double* y, const double*
                         const double* m);
 double fixed_scale(double bound);
 TileGeom make_tiles(int nx, int ny, int tile, int guard, int lo, int hi);
+// Particles per deposit chunk of the implicit map kernel: enough chunks for
+// every resident CTA of a `grid`-CTA launch (a small particle set would
+// otherwise keep most SMs idle behind a few long per-particle solves), a
+// multiple of kMinChunk in [kMinChunk, max_chunk].  The explicit push keeps
+// 2048-particle chunks: its per-particle work is short, and many small
+// explicit runs are better served by an ensemble.  Chunk tables are
+// allocated for kMinChunk.
+constexpr int kMinChunk = 128;
+int choose_chunk(long np, int grid, int max_chunk);
 int alloc_soa(upic_ctx* c, ParticleSoA& s, long cap, bool with_state, bool with_qm);
 void free_soa(upic_ctx* c, ParticleSoA& s);
 int alloc_sortwork(upic_ctx* c, SortWork& w, long cap, const TileGeom& tg);
