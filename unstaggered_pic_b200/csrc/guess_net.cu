@@ -127,21 +127,44 @@ __global__ void __launch_bounds__(kConvThreads) conv_tc_kernel(ConvArgs a, int f
     const int ntiles = (a.P + kTileM - 1) / kTileM;
     uint32_t parity = 0;
     bool ok = true;
+    // im2col mapping: thread tid fills channel quarter q = tid % 4 of rows
+    // r_j = tid / 4 + 32 j (j < 4) for all 9 taps; the loads of three taps
+    // (12 x 16 B) are issued before any of their shared-memory stores
+    const int q = tid & 3;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        // im2col rows: i -> channel quarter q (fastest), row r, tap t
-        for (int i = tid; i < kTileM * kChunks; i += kConvThreads) {
-            const int q = i & 3;
-            const int r = (i >> 2) & (kTileM - 1);
-            const int t = i >> 9;
-            const int p = tile * kTileM + r;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (p < a.P) {
-                const int ix = p / a.ny, iy = p - (p / a.ny) * a.ny;
-                const int jx = wrapi(ix + a.sign * (t / 3 - 1), a.nx);
-                const int jy = wrapi(iy + a.sign * (t % 3 - 1), a.ny);
-                v = *reinterpret_cast<const uint4*>(a.in + ((size_t)jx * a.ny + jy) * kC + q * 8);
+        int ixs[4], iys[4];
+        bool valid[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int p = tile * kTileM + (tid >> 2) + 32 * j;
+            valid[j] = p < a.P;
+            ixs[j] = valid[j] ? p / a.ny : 0;
+            iys[j] = valid[j] ? p - ixs[j] * a.ny : 0;
+        }
+#pragma unroll
+        for (int t0 = 0; t0 < kTaps; t0 += 3) {
+            uint4 v[3][4];
+#pragma unroll
+            for (int dt = 0; dt < 3; ++dt) {
+                const int t = t0 + dt;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    v[dt][j] = make_uint4(0u, 0u, 0u, 0u);
+                    if (valid[j]) {
+                        const int jx = wrapi(ixs[j] + a.sign * (t / 3 - 1), a.nx);
+                        const int jy = wrapi(iys[j] + a.sign * (t % 3 - 1), a.ny);
+                        v[dt][j] = __ldg(reinterpret_cast<const uint4*>(a.in + ((size_t)jx * a.ny + jy) * kC + q * 8));
+                    }
+                }
             }
-            *reinterpret_cast<uint4*>(sA + (r >> 3) * kGroupBytes + (t * 4 + q) * 128 + (r & 7) * 16) = v;
+#pragma unroll
+            for (int dt = 0; dt < 3; ++dt)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int r = (tid >> 2) + 32 * j;
+                    *reinterpret_cast<uint4*>(sA + (r >> 3) * kGroupBytes + ((t0 + dt) * 4 + q) * 128 + (r & 7) * 16) =
+                        v[dt][j];
+                }
         }
         // make the generic-proxy stores visible to the tensor core
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -214,19 +237,23 @@ __global__ void __launch_bounds__(kConvThreads) conv_tc_kernel(ConvArgs a, int f
 }
 
 constexpr int kWgThreads = 256;
-constexpr int kWgBatch = 16;
+constexpr int kWgBatch = 32;
 
 // Weight gradient partials of one block's pixel range (CUDA cores, FP32):
-// thread (co = tid % 32, row group rg = tid / 32) owns rows k = rg + 8 i.
+// thread tid owns the 4 x 9 block of outputs co = 4 (tid % 8) + c, k =
+// 9 (tid / 8) + kk, so each pixel costs it 13 shared-memory loads for 36
+// fused multiply-adds.
 __global__ void __launch_bounds__(kWgThreads)
     wgrad_kernel(const uint16_t* dz, const uint16_t* x, int nx, int ny, int P, float* partials) {
-    __shared__ float sdz[kWgBatch][kC];
+    __shared__ __align__(16) float sdz[kWgBatch][kC];
     __shared__ float sx[kWgBatch][kK];
-    const int tid = threadIdx.x, co = tid & 31, rg = tid >> 5;
-    float acc[kK / 8];
+    const int tid = threadIdx.x, cb = (tid & 7) * 4, kb = (tid >> 3) * 9;
+    float acc[4][9];
 #pragma unroll
-    for (int i = 0; i < kK / 8; ++i) acc[i] = 0.0f;
-    float bacc = 0.0f;
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) acc[c][k] = 0.0f;
+    float bacc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     const int per = (P + gridDim.x - 1) / gridDim.x;
     const int p0 = blockIdx.x * per, p1 = min(P, p0 + per);
     for (int pb = p0; pb < p1; pb += kWgBatch) {
@@ -241,7 +268,7 @@ __global__ void __launch_bounds__(kWgThreads)
             if (p < p1) {
                 const int ix = p / ny, iy = p - (p / ny) * ny;
                 const int jx = wrapi(ix + t / 3 - 1, nx), jy = wrapi(iy + t % 3 - 1, ny);
-                v = *reinterpret_cast<const uint4*>(x + ((size_t)jx * ny + jy) * kC + qq * 8);
+                v = __ldg(reinterpret_cast<const uint4*>(x + ((size_t)jx * ny + jy) * kC + qq * 8));
             }
             const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
             float* d = &sx[q][t * kC + qq * 8];
@@ -252,18 +279,30 @@ __global__ void __launch_bounds__(kWgThreads)
             }
         }
         __syncthreads();
+#pragma unroll 4
         for (int q = 0; q < kWgBatch; ++q) {
-            const float g = sdz[q][co];
-            bacc += g;
+            const float4 g = *reinterpret_cast<const float4*>(&sdz[q][cb]);
+            const float gv[4] = {g.x, g.y, g.z, g.w};
+            float xv[9];
 #pragma unroll
-            for (int i = 0; i < kK / 8; ++i) acc[i] = fmaf(g, sx[q][rg + 8 * i], acc[i]);
+            for (int k = 0; k < 9; ++k) xv[k] = sx[q][kb + k];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                bacc[c] += gv[c];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) acc[c][k] = fmaf(gv[c], xv[k], acc[c][k]);
+            }
         }
         __syncthreads();
     }
     float* o = partials + (size_t)blockIdx.x * kParams;
 #pragma unroll
-    for (int i = 0; i < kK / 8; ++i) o[co * kK + rg + 8 * i] = acc[i];
-    if (rg == 0) o[kW + co] = bacc;
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) o[(cb + c) * kK + kb + k] = acc[c][k];
+    if (kb == 0)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) o[kW + cb + c] = bacc[c];
 }
 
 // grad[j] = sum_b partials[b][j] in block order
@@ -454,13 +493,8 @@ uint16_t host_bf16(float f) {
 }  // namespace
 
 cudaError_t launch_conv_tc(const ConvArgs& a, int nsm, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   kSmemConv);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(conv_tc_kernel), kSmemConv);
+    if (e != cudaSuccess) return e;
     const int ntiles = (a.P + kTileM - 1) / kTileM;
     const int grid = std::min(ntiles, 2 * nsm);
     if (grid <= 0) return cudaSuccess;
@@ -471,13 +505,8 @@ cudaError_t launch_conv_tc(const ConvArgs& a, int nsm, cudaStream_t st) {
 
 // Test form: linear outputs of all 32 channels (out_f: P x 32).
 cudaError_t launch_conv_tc_full(const ConvArgs& a, int nsm, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   kSmemConv);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(conv_tc_kernel), kSmemConv);
+    if (e != cudaSuccess) return e;
     const int ntiles = (a.P + kTileM - 1) / kTileM;
     const int grid = std::min(ntiles, 2 * nsm);
     if (grid <= 0) return cudaSuccess;
