@@ -409,9 +409,13 @@ int upic_orbit_gather(upic_ctx* ctx, long np, const double* x, const double* y, 
  * kernels on its own stream, and replays it: one launch advances all runs
  * by `period` steps.  Steps beyond a multiple of the period run with
  * ordinary launches.  No diagnostics rows are produced (call upic_step on a
- * run for those).  The runs stay owned by the caller and must not be used
- * by other calls while upic_ensemble_step runs; the call returns when every
- * run's work is complete.  Errors are reported on the first run's context
+ * run for those).  The runs stay owned by the caller, must outlive the
+ * ensemble and must not be used by other calls while upic_ensemble_step
+ * runs; the call returns when every run's work is complete.  Calls on a run
+ * between ensemble steps are allowed: one that reloads or restarts it
+ * (upic_set_particles, upic_init_fields, upic_load_state, upic_set_stream,
+ * upic_set_background) or steps it makes the next ensemble step record a
+ * new graph.  Errors are reported on the first run's context
  * (upic_last_error(runs[0])), or on NULL for upic_ensemble_create.
  * An ensemble of implicit-method runs (all CN_ORBIT or CN_ORBIT_NONREL;
  * methods of the two kinds cannot be mixed) cannot be recorded, since each
