@@ -412,10 +412,10 @@ int upic_orbit_gather(upic_ctx* ctx, long np, const double* x, const double* y, 
  * run for those).  The runs stay owned by the caller, must outlive the
  * ensemble and must not be used by other calls while upic_ensemble_step
  * runs; the call returns when every run's work is complete.  Calls on a run
- * between ensemble steps are allowed: one that reloads or restarts it
- * (upic_set_particles, upic_init_fields, upic_load_state, upic_set_stream,
- * upic_set_background) or steps it makes the next ensemble step record a
- * new graph.  Errors are reported on the first run's context
+ * between ensemble steps are allowed (stepping it, or reloading or
+ * restarting it with upic_set_particles, upic_init_fields, upic_load_state,
+ * upic_set_stream or upic_set_background): the next ensemble step records a
+ * new graph whenever the recorded one no longer matches a run's state.  Errors are reported on the first run's context
  * (upic_last_error(runs[0])), or on NULL for upic_ensemble_create.
  * An ensemble of implicit-method runs (all CN_ORBIT or CN_ORBIT_NONREL;
  * methods of the two kinds cannot be mixed) cannot be recorded, since each
