@@ -474,3 +474,29 @@ def test_two_stream_growth_matches_reference():
     assert drift_gpu.max() <= max(10 * drift_ref.max(), 1e-12), (drift_gpu.max(), drift_ref.max())
     gg = cols.index("gauge_relative")
     assert np.max(ours[:, gg]) <= max(10 * np.max(ref[:, gg]), 1e-12), (np.max(ours[:, gg]), np.max(ref[:, gg]))
+
+
+@pytest.mark.parametrize("order,split", [(1, True), (2, True), (2, False), (3, True), (4, True)])
+def test_orbit_deposit_gather_adjoint(order, split):
+    """The orbit current deposit and the orbit field gather use the same
+    weights, so the particle power sum_p q vbar . <E S> equals the mesh
+    power dV sum_nodes J . E to round-off (the reference's known-answer test
+    test_orbit_deposit_gather_adjointness, threshold 5e-14)."""
+    rng = np.random.default_rng(23 + order)
+    nx = ny = 8
+    L, dt, n = 2 * np.pi, 0.2, 64
+    cfg = up.ImplicitConfig(nx=nx, ny=ny, Lx=L, Ly=L, Lz=L, dt=dt, spline_order=order, orbit_quad_order=18,
+                            split_orbit_at_knots=split, nyquist_projection=False)
+    x0 = rng.uniform(-0.5, 0.5, (n, 2)) * L
+    vbar = rng.normal(size=(n, 3)) * np.array([0.35, 0.2, 0.15])
+    dx = dt * vbar
+    q = 0.1 * rng.normal(size=n)
+    E = rng.normal(size=(3, nx * ny))
+    with up.Simulation(cfg) as sim:
+        J = sim.orbit_deposit(x0[:, 0], x0[:, 1], dx, vbar, q).reshape(3, -1)
+        Ebar, _ = sim.orbit_gather(x0[:, 0], x0[:, 1], dx, E, E, E)
+    dV = (L / nx) * (L / ny) * L
+    particle = float(np.sum(q * np.sum(vbar * Ebar, axis=1)))
+    mesh = float(np.sum(J * E)) * dV
+    scale = abs(particle) + abs(mesh) + 1.0
+    assert abs(particle - mesh) / scale < 5e-14, (particle, mesh)
