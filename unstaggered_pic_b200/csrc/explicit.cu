@@ -20,7 +20,15 @@ namespace upic {
 
 namespace {
 
-constexpr int kPushThreads = 256;
+// Threads per CTA and resident CTAs per SM the push kernel is compiled for
+// (register budget 65536 / (threads * CTAs) per thread).
+#ifndef UPIC_PUSH_THREADS
+#define UPIC_PUSH_THREADS 256
+#endif
+#ifndef UPIC_PUSH_MIN_BLOCKS
+#define UPIC_PUSH_MIN_BLOCKS 3
+#endif
+constexpr int kPushThreads = UPIC_PUSH_THREADS;
 constexpr int kPushWarps = kPushThreads / kWarp;
 constexpr int kKeyNone = -1;
 constexpr int kKeyEscape = -2;
@@ -111,7 +119,7 @@ UPIC_D void prefetch_next_batch(const PushArgs& a, const Chunk& ch, int base, in
 }
 
 template <int MODE, int NCOMP, bool UNIFORM>
-__global__ void __launch_bounds__(kPushThreads, 3)
+__global__ void __launch_bounds__(kPushThreads, UPIC_PUSH_MIN_BLOCKS)
 push_deposit_kernel(PushArgs a, TileGeom tg) {
     constexpr int NV = StageLayout<NCOMP>::kNV;
     constexpr int RW = StageLayout<NCOMP>::kRow;
