@@ -28,6 +28,12 @@ namespace {
 #ifndef UPIC_PUSH_MIN_BLOCKS
 #define UPIC_PUSH_MIN_BLOCKS 3
 #endif
+// 1: the step push stages its tile window's field records in shared memory
+// and gathers from there (the same sums in the same order as the global
+// gather, which remains for stencils outside the window)
+#ifndef UPIC_PUSH_SMEM_GATHER
+#define UPIC_PUSH_SMEM_GATHER 1
+#endif
 constexpr int kPushThreads = UPIC_PUSH_THREADS;
 constexpr int kPushWarps = kPushThreads / kWarp;
 constexpr int kKeyNone = -1;
@@ -132,6 +138,14 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
     double* sprod = reinterpret_cast<double*>(wlo + NCOMP * WN) + warp * StageLayout<NCOMP>::kDoubles;
     int* sgk = reinterpret_cast<int*>(reinterpret_cast<double*>(wlo + NCOMP * WN) +
                                       kPushWarps * StageLayout<NCOMP>::kDoubles) + warp * 32;
+#if UPIC_PUSH_SMEM_GATHER
+    // field records of the tile's window (kModePush): the gathers of
+    // particles whose stencil lies in the window read them from here
+    double2* srec = reinterpret_cast<double2*>(
+        (reinterpret_cast<uintptr_t>(reinterpret_cast<int*>(reinterpret_cast<double*>(wlo + NCOMP * WN) +
+                                                            kPushWarps * StageLayout<NCOMP>::kDoubles) +
+                                     kPushWarps * 32) + 15) & ~uintptr_t(15));
+#endif
 
     const int nx = tg.nx, ny = tg.ny;
     const int N = nx * ny;
@@ -174,6 +188,18 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
             const int tx = cur_tile / tg.nty, ty = cur_tile - tx * tg.nty;
             ox = tg.full_x ? 0 : tx * tg.tile_x - tg.guard - 1;
             oy = tg.full_y ? 0 : ty * tg.tile_y - tg.guard - 1;
+#if UPIC_PUSH_SMEM_GATHER
+            if (MODE == kModePush) {
+                const double2* g2 = reinterpret_cast<const double2*>(a.gfields);
+                for (int idx = threadIdx.x; idx < WN * (kGFStride / 2); idx += blockDim.x) {
+                    const int node = idx / (kGFStride / 2), f = idx - node * (kGFStride / 2);
+                    const int lx = node / tg.wy, ly = node - lx * tg.wy;
+                    const int gx = tg.full_x ? lx : ((ox + lx) & (nx - 1));
+                    const int gy = tg.full_y ? ly : ((oy + ly) & (ny - 1));
+                    srec[idx] = __ldg(g2 + (size_t)(gx * ny + gy) * (kGFStride / 2) + f);
+                }
+            }
+#endif
             __syncthreads();
         }
         for (int base = ch.start; base < ch.end; base += kPushThreads) {
@@ -198,6 +224,28 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                     double G[12];
 #pragma unroll
                     for (int f = 0; f < 12; ++f) G[f] = 0.0;
+#if UPIC_PUSH_SMEM_GATHER
+                    const int lx0 = tg.full_x ? 0 : window_coord(qx.ic - 1, ox, nx, tg.wx);
+                    const int ly0 = tg.full_y ? 0 : window_coord(qy.ic - 1, oy, ny, tg.wy);
+                    if (lx0 >= 0 && ly0 >= 0) {
+#pragma unroll
+                        for (int ia = 0; ia < 3; ++ia) {
+                            const int wxi = tg.full_x ? wrap_index(qx.ic - 1 + ia, nx) : lx0 + ia;
+#pragma unroll
+                            for (int ib = 0; ib < 3; ++ib) {
+                                const int wyi = tg.full_y ? wrap_index(qy.ic - 1 + ib, ny) : ly0 + ib;
+                                const double w = wxs[ia] * wys[ib];
+                                const double2* rec = srec + (wxi * tg.wy + wyi) * (kGFStride / 2);
+#pragma unroll
+                                for (int f2 = 0; f2 < kGFStride / 2; ++f2) {
+                                    const double2 r = rec[f2];
+                                    G[2 * f2] = fma(r.x, w, G[2 * f2]);
+                                    G[2 * f2 + 1] = fma(r.y, w, G[2 * f2 + 1]);
+                                }
+                            }
+                        }
+                    } else
+#endif
 #pragma unroll
                     for (int ia = 0; ia < 3; ++ia) {
                         const int gx = wrap_index(qx.ic - 1 + ia, nx);
@@ -749,7 +797,10 @@ int push_deposit_smem_bytes(const TileGeom& tg, int ncomp) {
     const int WN = tg.wx * tg.wy;
     const int window = 2 * ncomp * WN * 8;
     const int stage = kPushWarps * (32 * (9 + ncomp) * 8 + 32 * 4);
-    const int bytes = window + stage;
+    int bytes = window + stage;
+#if UPIC_PUSH_SMEM_GATHER
+    bytes += 16 + WN * kGFStride * 8;
+#endif
     const int red = kPushWarps * 5 * 8;
     return bytes > red ? bytes : red;
 }
