@@ -91,6 +91,12 @@ __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedP
     float* sprod = reinterpret_cast<float*>(win + NCOMP * WN) + warp * MStage<NCOMP>::kFloats;
     int* sgk = reinterpret_cast<int*>(reinterpret_cast<float*>(win + NCOMP * WN) +
                                       kMWarps * MStage<NCOMP>::kFloats) + warp * 32;
+    // FP32 field records of the tile's window (kModePush): gathers of
+    // stencils inside the window read them from here
+    float4* srec = reinterpret_cast<float4*>(
+        (reinterpret_cast<uintptr_t>(reinterpret_cast<int*>(reinterpret_cast<float*>(win + NCOMP * WN) +
+                                                            kMWarps * MStage<NCOMP>::kFloats) +
+                                     kMWarps * 32) + 15) & ~uintptr_t(15));
 
     const int nx = tg.nx, ny = tg.ny;
     const int N = nx * ny;
@@ -115,6 +121,16 @@ __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedP
             const int tx = cur_tile / tg.nty, ty = cur_tile - tx * tg.nty;
             ox = tg.full_x ? 0 : tx * tg.tile_x - tg.guard - 1;
             oy = tg.full_y ? 0 : ty * tg.tile_y - tg.guard - 1;
+            if (MODE == kModePush) {
+                const float4* g4 = reinterpret_cast<const float4*>(a.gf);
+                for (int idx = threadIdx.x; idx < WN * (kGFStride / 4); idx += blockDim.x) {
+                    const int node = idx / (kGFStride / 4), f = idx - node * (kGFStride / 4);
+                    const int lx = node / tg.wy, ly = node - lx * tg.wy;
+                    const int gx = tg.full_x ? lx : ((ox + lx) & (nx - 1));
+                    const int gy = tg.full_y ? ly : ((oy + ly) & (ny - 1));
+                    srec[idx] = __ldg(g4 + (size_t)(gx * ny + gy) * (kGFStride / 4) + f);
+                }
+            }
             __syncthreads();
         }
         for (int base = ch.start; base < ch.end; base += kMThreads) {
@@ -139,6 +155,28 @@ __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedP
                     float G[12];
 #pragma unroll
                     for (int f = 0; f < 12; ++f) G[f] = 0.0f;
+                    const int lx0 = tg.full_x ? 0 : mwindow_coord(ix - 1, ox, nx, tg.wx);
+                    const int ly0 = tg.full_y ? 0 : mwindow_coord(iy - 1, oy, ny, tg.wy);
+                    if (lx0 >= 0 && ly0 >= 0) {
+#pragma unroll
+                        for (int ia = 0; ia < 3; ++ia) {
+                            const int wxi = tg.full_x ? wrap_index(ix - 1 + ia, nx) : lx0 + ia;
+#pragma unroll
+                            for (int ib = 0; ib < 3; ++ib) {
+                                const int wyi = tg.full_y ? wrap_index(iy - 1 + ib, ny) : ly0 + ib;
+                                const float w = wxs[ia] * wys[ib];
+                                const float4* rec = srec + (wxi * tg.wy + wyi) * (kGFStride / 4);
+#pragma unroll
+                                for (int f4 = 0; f4 < kGFStride / 4; ++f4) {
+                                    const float4 r = rec[f4];
+                                    G[4 * f4] = fmaf(r.x, w, G[4 * f4]);
+                                    G[4 * f4 + 1] = fmaf(r.y, w, G[4 * f4 + 1]);
+                                    G[4 * f4 + 2] = fmaf(r.z, w, G[4 * f4 + 2]);
+                                    G[4 * f4 + 3] = fmaf(r.w, w, G[4 * f4 + 3]);
+                                }
+                            }
+                        }
+                    } else
 #pragma unroll
                     for (int ia = 0; ia < 3; ++ia) {
                         const int gx = wrap_index(ix - 1 + ia, nx);
@@ -493,7 +531,7 @@ cudaError_t set_mixed_smem(int bytes) {
 int push_mixed_smem_bytes(const TileGeom& tg, int ncomp) {
     const int window = ncomp * tg.wx * tg.wy * 8;
     const int stage = kMWarps * (32 * (9 + ncomp) * 4 + 32 * 4);
-    const int bytes = window + stage;
+    const int bytes = window + stage + 16 + tg.wx * tg.wy * kGFStride * 4;
     const int red = kMWarps * 5 * 8;
     return bytes > red ? bytes : red;
 }
