@@ -113,6 +113,10 @@ def parse():
                     help="1D-2V two-stream runs of the implicit ensemble comparison (0 skips; one GPU only)")
     ap.add_argument("--implicit-ensemble-steps", type=int, default=10,
                     help="steps of the implicit ensemble comparison")
+    ap.add_argument("--large-mixed-check", action="store_true",
+                    help="instead of the bench line: the 2048x2048, 64 e-/cell Weibel + beam run in FP64 and in "
+                         "mixed precision (energy drift and gauge residual of both), one JSON line")
+    ap.add_argument("--large-steps", type=int, default=500, help="steps of --large-mixed-check")
     return ap.parse_args()
 
 
@@ -858,10 +862,64 @@ def run_upic(args):
     return 0
 
 
+def large_mixed_check(args):
+    """The large mixed-precision configuration on the explicit step: a
+    2048x2048 periodic grid with the cell size of the 512x512 bench workload
+    (L = 4 * 2 pi / 0.3), 58 electrons per cell of Weibel bi-Maxwellian
+    plasma (vth 0.02, 0.2, 0 c) plus 6 per cell of a beam of density 0.1
+    drifting at 0.5 c along x (268,435,456 particles), fixed ion background
+    1.1, dt 0.05, run in FP64 and in mixed precision from the same seed;
+    energy drift and gauge / Gauss residuals of both, every 10 steps."""
+    import torch
+    import unstaggered_pic_b200 as up
+
+    torch.cuda.set_device(0)
+    n, L, steps = 2048, 4 * 2 * np.pi / 0.3, args.large_steps
+    u_beam = 0.5 / np.sqrt(1 - 0.25)
+    a = up.generate_bimaxwellian(n, n, L, L, 58, (0.02, 0.2, 0.0), n0=1.0, seed=55)
+    b = up.generate_bimaxwellian(n, n, L, L, 6, (0.02, 0.02, 0.02), udrift=(u_beam, 0.0, 0.0), n0=0.1, seed=56)
+    p = {k: np.concatenate([a[k], b[k]]) for k in a}
+    del a, b
+    npart = len(p["x"])
+    names = up.DIAG_COLUMNS
+    out = {"workload": f"weibel_beam_{n}x{n}_ppc64", "particles": npart, "steps": steps, "L": L, "dt": 0.05,
+           "shape": "quadratic B-spline (the explicit method's)", "data": "synthetic (seeded)"}
+    rows = {}
+    for prec in ("fp64", "mixed"):
+        cfg = up.Config(nx=n, ny=n, Lx=L, Ly=L, dt=0.05, method="bdf1", n0=1.1, precision=prec)
+        with up.Simulation(cfg) as sim:
+            sim.set_particles(p["x"], p["y"], p["P"], p["v"], p["v_prev"], p["q"], p["m"])
+            row0 = sim.init_fields(True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            d = sim.step(steps, 10)
+            el = time.perf_counter() - t0
+        d = np.vstack([row0, d[9::10]])
+        rows[prec] = d
+        e = d[:, names.index("total_energy")]
+        out[prec] = {"value": npart * steps / el, "unit": METRIC, "ms_per_step": 1e3 * el / steps,
+                     "energy_drift_max": float(np.max(np.abs(e - e[0]) / abs(e[0]))),
+                     "gauge_rms_max": float(np.max(d[:, names.index("gauge_rms")])),
+                     "gauss_rms_max": float(np.max(d[:, names.index("gauss_rms")])),
+                     "continuity_rms_start": float(d[0, names.index("continuity_rms")]),
+                     "continuity_rms_max_after_start": float(np.max(d[1:, names.index("continuity_rms")])),
+                     "final_field_energy": float(d[-1, names.index("field_energy")]),
+                     "final_Bz_l2": float(d[-1, names.index("Bz_l2")])}
+    r64, r32 = rows["fp64"], rows["mixed"]
+    out["mixed_vs_fp64_max_rel_diff"] = {
+        c: float(np.max(np.abs(r32[:, names.index(c)] - r64[:, names.index(c)])) /
+                 (np.max(np.abs(r64[:, names.index(c)])) + 1e-300))
+        for c in ("total_energy", "field_energy", "kinetic_energy", "Bz_l2", "E_l2", "J_l2")}
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.large_mixed_check:
+        return large_mixed_check(args)
     return run_upic(args)
 
 
