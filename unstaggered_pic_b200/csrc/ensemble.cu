@@ -75,6 +75,26 @@ int ens_fail(upic_ensemble* e, int code, const std::string& msg) {
 int capture(upic_ensemble* e) {
     drop_graph(e);
     const size_t n = e->runs.size();
+    // host counters before recording: restored if the recording fails, so
+    // that no run counts steps that never ran
+    struct Saved {
+        int head, cur, since;
+        long steps;
+    };
+    std::vector<Saved> saved(n);
+    for (size_t r = 0; r < n; ++r) {
+        const upic_ctx* c = e->runs[r];
+        saved[r] = {c->head, c->cur, c->steps_since_sort, c->steps};
+    }
+    auto restore = [&]() {
+        for (size_t r = 0; r < n; ++r) {
+            upic_ctx* c = e->runs[r];
+            c->head = saved[r].head;
+            c->cur = saved[r].cur;
+            c->steps_since_sort = saved[r].since;
+            c->steps = saved[r].steps;
+        }
+    };
     for (size_t r = 0; r < n; ++r) {
         e->head0[r] = e->runs[r]->head;
         e->count0[r] = phase_count(e->runs[r]);
@@ -100,6 +120,7 @@ int capture(upic_ensemble* e) {
     const cudaError_t ee = cudaStreamEndCapture(e->master, &g);
     if (rc || ee != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
+        restore();
         if (rc == UPIC_ERR_CUDA || rc == 0)
             return ens_fail(e, UPIC_ERR_CUDA,
                             std::string("ensemble capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee));
@@ -108,6 +129,7 @@ int capture(upic_ensemble* e) {
     e->graph = g;
     if ((ce = cudaGraphInstantiate(&e->exec, e->graph, 0)) != cudaSuccess) {
         drop_graph(e);
+        restore();
         return ens_fail(e, UPIC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce));
     }
     for (size_t r = 0; r < n; ++r) {
