@@ -18,8 +18,11 @@ TOL_50 = 1e-10
 
 
 def relerr(a, b):
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if not (np.iscomplexobj(a) or np.iscomplexobj(b)):
+        a = a.astype(np.float64)
+        b = b.astype(np.float64)
     scale = np.max(np.abs(b))
     if scale == 0.0:
         return float(np.max(np.abs(a)))
