@@ -223,6 +223,27 @@ __global__ void gather_array_kernel(const T* __restrict__ src, T* __restrict__ d
         dst[q] = src[idx[q]];
 }
 
+// All payload arrays of the particle set gathered by one pass over the
+// sorted index: dst_k[q] = src_k[idx[q]] for the double arrays present (and
+// the original index); the index is read once instead of once per array.
+struct GatherSet {
+    const double* src[13];
+    double* dst[13];
+    int narr;
+    const int* sid;
+    int* did;
+};
+
+__global__ void gather_set_kernel(GatherSet g, const int* __restrict__ idx, long n) {
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+        const int i = idx[q];
+#pragma unroll
+        for (int k = 0; k < 13; ++k)
+            if (k < g.narr) g.dst[k][q] = g.src[k][i];
+        if (g.did) g.did[q] = g.sid[i];
+    }
+}
+
 __global__ void unpermute_kernel(ParticleSoA s, ParticleSoA d, long n) {
     for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
         const int o = s.id[k];
@@ -312,13 +333,19 @@ cudaError_t permute_particles(const ParticleSoA& s, const ParticleSoA& d, long n
     const int g = grid_for(np);
     double* const src[13] = {s.x, s.y, s.Px, s.Py, s.Pz, s.vx, s.vy, s.vz, s.wx, s.wy, s.wz, s.q, s.m};
     double* const dst[13] = {d.x, d.y, d.Px, d.Py, d.Pz, d.vx, d.vy, d.vz, d.wx, d.wy, d.wz, d.q, d.m};
+    GatherSet gs{};
     for (int k = 0; k < 13; ++k)
         if (src[k] && dst[k]) {
-            gather_array_kernel<double><<<g, 256, 0, st>>>(src[k], dst[k], w.vals, np);
-            count_launches(1);
+            gs.src[gs.narr] = src[k];
+            gs.dst[gs.narr] = dst[k];
+            ++gs.narr;
         }
     if (s.id && d.id) {
-        gather_array_kernel<int><<<g, 256, 0, st>>>(s.id, d.id, w.vals, np);
+        gs.sid = s.id;
+        gs.did = d.id;
+    }
+    if (np > 0) {
+        gather_set_kernel<<<g, 256, 0, st>>>(gs, w.vals, np);
         count_launches(1);
     }
     return cudaGetLastError();
