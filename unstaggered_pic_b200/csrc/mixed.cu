@@ -593,18 +593,45 @@ cudaError_t sort_mixed_by_tile(const TileGeom& tg, const MixedSoA& p, long np, i
     return sort_keys_to_chunks(tg, np, w, st);
 }
 
+// Every payload array of the mixed set in one pass over the sorted index.
+struct MGatherSet {
+    const float* src[13];
+    float* dst[13];
+    int narr;
+    const int *scell, *sid;
+    int *dcell, *did;
+};
+
+__global__ void mgather_set_kernel(MGatherSet g, const int* __restrict__ idx, long n) {
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+        const int i = idx[q];
+#pragma unroll
+        for (int k = 0; k < 13; ++k)
+            if (k < g.narr) g.dst[k][q] = g.src[k][i];
+        g.dcell[q] = g.scell[i];
+        g.did[q] = g.sid[i];
+    }
+}
+
 cudaError_t permute_mixed(const MixedSoA& s, const MixedSoA& d, long np, const SortWork& w, cudaStream_t st) {
     const int g = mgrid(np);
     float* const src[13] = {s.rx, s.ry, s.Px, s.Py, s.Pz, s.vx, s.vy, s.vz, s.wx, s.wy, s.wz, s.q, s.m};
     float* const dst[13] = {d.rx, d.ry, d.Px, d.Py, d.Pz, d.vx, d.vy, d.vz, d.wx, d.wy, d.wz, d.q, d.m};
+    MGatherSet gs{};
     for (int k = 0; k < 13; ++k)
         if (src[k] && dst[k]) {
-            mgather_kernel<float><<<g, 256, 0, st>>>(src[k], dst[k], w.vals, np);
-            count_launches(1);
+            gs.src[gs.narr] = src[k];
+            gs.dst[gs.narr] = dst[k];
+            ++gs.narr;
         }
-    mgather_kernel<int><<<g, 256, 0, st>>>(s.cell, d.cell, w.vals, np);
-    mgather_kernel<int><<<g, 256, 0, st>>>(s.id, d.id, w.vals, np);
-    count_launches(2);
+    gs.scell = s.cell;
+    gs.dcell = d.cell;
+    gs.sid = s.id;
+    gs.did = d.id;
+    if (np > 0) {
+        mgather_set_kernel<<<g, 256, 0, st>>>(gs, w.vals, np);
+        count_launches(1);
+    }
     return cudaGetLastError();
 }
 
