@@ -417,8 +417,8 @@ def learned_comparison(args):
     return out
 
 
-# Ensemble of independent explicit runs of uneven sizes (the BASELINE's
-# batched-ensemble form, on the explicit 2D method): per run the node count
+# Ensemble of independent explicit runs of uneven sizes (the batched
+# ensemble on the explicit 2D method): per run the node count
 # is drawn from {128, 256, 512, 1024} (grids 16x8, 16x16, 32x16, 32x32) and
 # the particle count log-uniformly from [1e4, 1e5]; Weibel bi-Maxwellian
 # plasma, dt 0.05.  Tile size and re-sort interval are autotuned per grid
@@ -514,9 +514,9 @@ def ensemble_comparison(args):
             "data": "synthetic (seeded bi-Maxwellian per run)"}
 
 
-# Implicit ensemble (BASELINE's batched-ensemble configuration): 1D-2V
+# Implicit ensemble of 1024-style batched two-stream runs, reduced: 1D-2V
 # periodic two-stream runs, Nx from {128, 256, 512, 1024}, particle count
-# log-uniform in [1e4, 1e5] (the configuration's upper bound is 1e6),
+# log-uniform in [1e4, 1e5] (up to 1e6 in the full-size form),
 # counter-drifting Maxwellian beams at +-v0, v0 uniform in [0.05, 0.3] c,
 # vth 0.01 c, cubic splines, dt 0.1.
 def implicit_ensemble_comparison(args):
