@@ -514,9 +514,9 @@ def ensemble_comparison(args):
             "data": "synthetic (seeded bi-Maxwellian per run)"}
 
 
-# Implicit ensemble of 1024-style batched two-stream runs, reduced: 1D-2V
-# periodic two-stream runs, Nx from {128, 256, 512, 1024}, particle count
-# log-uniform in [1e4, 1e5] (up to 1e6 in the full-size form),
+# Implicit ensemble: 1D-2V periodic two-stream runs (64 by default; the
+# full-size batch is 1024 runs of up to 1e6 particles), Nx from
+# {128, 256, 512, 1024}, particle count log-uniform in [1e4, 1e5],
 # counter-drifting Maxwellian beams at +-v0, v0 uniform in [0.05, 0.3] c,
 # vth 0.01 c, cubic splines, dt 0.1.
 def implicit_ensemble_comparison(args):
