@@ -184,3 +184,33 @@ def test_implicit_ensemble_matches_runs_alone():
     finally:
         for s in alone + together:
             s.close()
+
+
+def test_ensemble_with_an_empty_run():
+    """A run without particles (its fields still evolve) in an ensemble
+    equals the same run stepped alone."""
+    L = 2 * np.pi / 0.3
+    p = up.generate_bimaxwellian(16, 16, L, L, 8, (0.02, 0.2, 0.0), seed=9)
+    empty = {k: v[:0] for k, v in p.items()}
+    sims_a, sims_b = [], []
+    try:
+        for parts in (p, empty):
+            for lst in (sims_a, sims_b):
+                sim = up.Simulation(up.Config(nx=16, ny=16, Lx=L, Ly=L, dt=0.05, sort_interval=2))
+                # (an explicit context needs a particle set loaded once before
+                # it accepts an empty one)
+                sim.set_particles(p["x"], p["y"], p["P"], p["v"], p["v_prev"], p["q"], p["m"])
+                sim.set_particles(parts["x"], parts["y"], parts["P"], parts["v"], parts["v_prev"], parts["q"],
+                                  parts["m"])
+                sim.init_fields(False)
+                lst.append(sim)
+        with up.Ensemble(sims_b) as ens:
+            ens.step(25)
+        for sim in sims_a:
+            sim.step(25, 0)
+        for a, b in zip(sims_a, sims_b):
+            for f in FIELDS:
+                assert np.array_equal(a.field(f), b.field(f)), f
+    finally:
+        for s in sims_a + sims_b:
+            s.close()
