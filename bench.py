@@ -240,7 +240,9 @@ def reference_sample(w, ppc, steps, warmup, seed):
     per-particle cost of the implicit step does not depend on the box)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as ol
-    import unstaggered_pic_b200 as up
+    # inputs from the oracle's restatement of the workload generator (bit for
+    # bit the product's), so this arm loads none of the product's code
+    gen = ol.generate_bimaxwellian
     if w["method"] == "cn_orbit":
         lib = ol.ref_p3()
         if lib is None:
@@ -248,7 +250,7 @@ def reference_sample(w, ppc, steps, warmup, seed):
         nsub = 64
         Ls = w["L"] * nsub / w["nx"]
         d = IMPLICIT_DECK
-        p = up.generate_bimaxwellian(nsub, nsub, Ls, Ls, ppc, w["uth"], seed=seed)
+        p = gen(nsub, nsub, Ls, Ls, ppc, w["uth"], seed=seed)
         x = np.zeros((len(p["x"]), 3))
         x[:, 0] = p["x"] - Ls / 2
         x[:, 1] = p["y"] - Ls / 2
@@ -277,7 +279,7 @@ def reference_sample(w, ppc, steps, warmup, seed):
     if fn is None:
         fn = ol.oracle().o2_simulate
         kind = "port"
-    p = up.generate_bimaxwellian(w["nx"], w["ny"], w["L"], w["L"], ppc, w["uth"], seed=seed)
+    p = gen(w["nx"], w["ny"], w["L"], w["L"], ppc, w["uth"], seed=seed)
     parts = {"x": p["x"], "y": p["y"], "P": p["P"], "v": p["v"], "vprev": p["v_prev"], "q": p["q"],
              "m": p["m"]}
     if warmup > 0:
@@ -296,7 +298,7 @@ def _ref_worker(args):
     return reference_sample(WORKLOADS[name], ppc, steps, warmup, seed)
 
 
-def reference_pool(name, steps, warmup):
+def reference_pool(name, steps, warmup, diag_stride=1):
     """The reference's CPU step on all host cores (one serial reference
     process per core, each on its own sample of workload `name`)."""
     import multiprocessing as mp
@@ -317,7 +319,7 @@ def reference_pool(name, steps, warmup):
     sample = (f"{cores} concurrent processes, each a {res[0][4]}; value = total particle-steps / "
               f"slowest process time")
     return {"value": value, "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * slowest / steps,
-            "config": config_desc(w, {"reference_sample": sample}),
+            "config": config_desc(w, {"diag_stride": diag_stride}),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": res[0][1],
                              "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -330,7 +332,7 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    main = reference_pool(args.workload, args.steps, args.warmup)
+    main = reference_pool(args.workload, args.steps, args.warmup, args.diag_stride)
     line = {"metric": METRIC, "value": main["value"], "unit": METRIC, "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": main["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -338,7 +340,8 @@ def run_reference_arm(args):
     for k in ("config", "cpu_baseline", "e2e", "wall_s"):
         line[k] = main[k]
     if args.implicit_workload != "none" and WORKLOADS[args.workload]["method"] != "cn_orbit":
-        imp = reference_pool(args.implicit_workload, min(args.steps, args.implicit_steps), args.warmup)
+        imp = reference_pool(args.implicit_workload, min(args.steps, args.implicit_steps), args.warmup,
+                             args.diag_stride)
         imp.update({"metric": METRIC, "unit": METRIC, "impl": "reference", "dtype": "f64"})
         line["implicit"] = imp
     print(json.dumps(line))

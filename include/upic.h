@@ -444,7 +444,7 @@ int upic_guess_conv(upic_ctx* ctx, int nx, int ny, const uint16_t* x, const uint
 int upic_guess_wgrad(upic_ctx* ctx, int nx, int ny, const uint16_t* dz, const uint16_t* x, float* grad);
 
 /* Largest grid (nx*ny nodes) upic_deposit_current_noalloc accepts: its
- * scratch is a fixed 6*UPIC_NOALLOC_MAX_NODES+2 uint64 array (3 MiB). */
+ * scratch is a fixed 6*UPIC_NOALLOC_MAX_NODES+3 uint64 array (3 MiB). */
 #define UPIC_NOALLOC_MAX_NODES 65536
 
 /* Current deposit that allocates nothing -- no counterpart in the reference.
@@ -454,14 +454,20 @@ int upic_guess_wgrad(upic_ctx* ctx, int nx, int ny, const uint16_t* dz, const ui
  * loops that cannot risk the device synchronization an allocation may
  * cause.  x, y (np), v (3*np xyz triples), q (np) and J (3*nx*ny) are DEVICE
  * pointers owned by the caller; work is queued on `stream` (a cudaStream_t,
- * NULL = default stream) and J is complete when the stream reaches it.
+ * NULL = default stream), and the call returns once that work has finished
+ * (it reads back one status word), so J is complete on return.
  * Scratch lives in one fixed __device__ array per GPU (3 MiB, held by every
  * GPU that loads the library until exit).  The first call on a device
- * resolves that array's device address, so make the first call on each
- * device before any stream capture.  Every call uses the same array and
- * clears it first: calls that overlap on the GPU (different streams, or
- * host threads sharing a device) race and must be serialized by the caller.
- * Returns UPIC_ERR_TOO_LARGE when nx*ny > UPIC_NOALLOC_MAX_NODES. */
+ * resolves that array's device address and keeps it for the life of the
+ * process, so make the first call on each device before any stream capture,
+ * and do not call it again after a cudaDeviceReset of that device.  Every
+ * call uses the same array and clears it first: calls that overlap on the
+ * GPU (different streams, or host threads sharing a device) race and must
+ * be serialized by the caller.
+ * Returns UPIC_ERR_TOO_LARGE when nx*ny > UPIC_NOALLOC_MAX_NODES,
+ * UPIC_ERR_NONFINITE (with J set to NaN) when a position, velocity or charge
+ * is not finite, and UPIC_ERR_CUDA, without launching, when a CUDA error
+ * from the caller's earlier work is pending (that error is left in place). */
 int upic_deposit_current_noalloc(int nx, int ny, double Lx, double Ly, long np, const double* x,
                                  const double* y, const double* v, const double* q, double* J,
                                  void* stream);

@@ -62,6 +62,13 @@ long o2_init_weibel(int nx, int ny, double Lx, double Ly, int ppc, double c, dou
                     long np_capacity, double* x, double* y, double* P, double* v,
                     double* vprev, double* q, double* m);
 
+/* Seeded bi-Maxwellian plasma of the benchmark workloads (splitmix64 streams
+ * per particle + Box-Muller); the same arrays as upic_generate_bimaxwellian.
+ * Returns 0, or -2 on a bad argument. */
+int o_generate_bimaxwellian(int nx, int ny, double Lx, double Ly, int ppc, double c, double n0,
+                            const double* uth, const double* udrift, uint64_t seed, double* x,
+                            double* y, double* P, double* v, double* v_prev, double* q, double* m);
+
 /* std::mt19937 restated (C++ [rand.eng.mers] parameters). */
 typedef struct {
     uint32_t mt[624];

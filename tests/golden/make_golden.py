@@ -10,9 +10,12 @@ of the shipped Project1/output/landau_weak run.  The
 fixtures let the oracle and the GPU path be checked where the reference
 sources are absent.
 
-    python tests/golden/make_golden.py        # all fixtures
-    python tests/golden/make_golden.py p3     # the implicit-method runs only
-    python tests/golden/make_golden.py p1     # the non-relativistic implicit runs only
+    UPIC_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py        # all fixtures
+    UPIC_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py p3     # implicit runs only
+    UPIC_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py p1     # Project1 runs only
+
+UPIC_REFERENCE_DIR is needed only by the fixtures that copy shipped reference
+files (the published validation numbers and the shipped Project1 output).
 """
 import csv
 import ctypes
@@ -26,7 +29,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 import oracle_lib as ol  # noqa: E402
 
-REF = "/root/reference"
+
+
+def ref_path(*parts):
+    """Path of a file of the reference checkout named by UPIC_REFERENCE_DIR."""
+    root = os.environ.get("UPIC_REFERENCE_DIR")
+    if not root or not os.path.isdir(root):
+        raise SystemExit("set UPIC_REFERENCE_DIR to the reference checkout")
+    return os.path.join(root, *parts)
 
 
 def seeded_particles(rng, n, Lx, Ly, vth=(0.02, 0.2, 0.05), edge=True):
@@ -98,7 +108,7 @@ def main():
                                 **{"out_" + k: v for k, v in out.items()}, diag=diag, fields=fields)
 
     # published validation numbers of the four Weibel decks
-    with open(os.path.join(REF, "Project2/docs/validation_summary.json")) as fh:
+    with open(ref_path("Project2", "docs", "validation_summary.json")) as fh:
         summ = json.load(fh)
     runs = {k: v for k, v in summ["runs"].items() if k.startswith("weibel")}
     with open(os.path.join(HERE, "p2_weibel_published.json"), "w") as fh:
@@ -347,7 +357,7 @@ def p1_main():
                             **{"out_" + c: out[c] for c in ("x", "v", "P", "v_prev")},
                             diag=out["diag"], info=out["info"], fields=out["fields"], step_diag=out["step_diag"])
         print(name, len(q), "particles, iterations", out["info"][:, 0].astype(int).tolist())
-    shipped = os.path.join(REF, "Project1", "output", "landau_weak")
+    shipped = ref_path("Project1", "output", "landau_weak")
     with open(shipped + "_diagnostics.csv") as fh:
         rows = list(csv.reader(fh))
     with open(shipped + "_step_diagnostics.csv") as fh:

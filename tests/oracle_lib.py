@@ -37,6 +37,24 @@ def oracle():
     return lib
 
 
+def generate_bimaxwellian(nx, ny, Lx, Ly, ppc, uth, udrift=(0.0, 0.0, 0.0), c=1.0, n0=1.0, seed=1):
+    """The benchmark workloads' seeded plasma from the oracle's restatement
+    (o_generate_bimaxwellian): the same dict of x, y, P, v, v_prev, q, m as
+    the product's generator, without loading the product library."""
+    n = nx * ny * ppc
+    out = {"x": np.empty(n), "y": np.empty(n), "P": np.empty((n, 3)), "v": np.empty((n, 3)),
+           "v_prev": np.empty((n, 3)), "q": np.empty(n), "m": np.empty(n)}
+    uth = np.ascontiguousarray(uth, dtype=np.float64)
+    ud = np.ascontiguousarray(udrift, dtype=np.float64)
+    rc = oracle().o_generate_bimaxwellian(int(nx), int(ny), ctypes.c_double(Lx), ctypes.c_double(Ly), int(ppc),
+                                          ctypes.c_double(c), ctypes.c_double(n0), ptr(uth), ptr(ud),
+                                          ctypes.c_uint64(seed),
+                                          *[ptr(out[k]) for k in ("x", "y", "P", "v", "v_prev", "q", "m")])
+    if rc != 0:
+        raise ValueError("o_generate_bimaxwellian: bad argument")
+    return out
+
+
 def ref_p2():
     """The reference's own code; None when it was not built (no sources)."""
     return _load(REF_P2_SO)

@@ -179,3 +179,21 @@ def test_p1_fixtures_regenerate_from_reference_build(case):
     for k in ("diag", "info", "step_diag"):
         assert np.array_equal(out[k], g[k], equal_nan=True), k
     assert np.array_equal(out["fields"], g["fields"])
+
+
+@pytest.mark.parametrize("args", [
+    (16, 8, 20.94, 10.47, 5, (0.02, 0.2, 0.0), (0.0, 0.0, 0.0), 1.0, 1.0, 2026),
+    (32, 32, 3.0, 5.0, 3, (0.1, 0.05, 0.02), (0.577, 0.0, -0.1), 1.0, 0.1, 56),
+    (256, 128, 20.94, 10.47, 3, (0.02, 0.2, 0.0), (0.0, 0.0, 0.0), 2.0, 1.0, 1000),
+])
+def test_oracle_generator_equals_product_generator(args):
+    """The oracle's restatement of the workloads' seeded plasma gives the
+    product generator's arrays bit for bit (the reference arm of bench.py
+    builds its inputs from the oracle, without the product library; the
+    largest case runs the product on several host threads)."""
+    import unstaggered_pic_b200 as up
+    nx, ny, Lx, Ly, ppc, uth, ud, c, n0, seed = args
+    a = ol.generate_bimaxwellian(nx, ny, Lx, Ly, ppc, uth, udrift=ud, c=c, n0=n0, seed=seed)
+    b = up.generate_bimaxwellian(nx, ny, Lx, Ly, ppc, uth, udrift=ud, c=c, n0=n0, seed=seed)
+    for k in a:
+        assert a[k].tobytes() == b[k].tobytes(), k

@@ -5,7 +5,7 @@
 // their own allocator and forbid raw allocations, or latency-critical loops
 // that must not risk the implicit device synchronization a cudaMalloc or
 // cudaFree can cause.  For them this entry point keeps its scratch -- the
-// fixed-point accumulators of the grid and two reduction words -- in one
+// fixed-point accumulators of the grid and three status words -- in one
 // file-scope __device__ array of fixed size, which every GPU that loads
 // this library holds until the process exits.  The caller passes device
 // pointers for the particles and for the output current.
@@ -27,29 +27,38 @@ namespace {
 using namespace upic;
 
 constexpr long kNoAllocMaxNodes = UPIC_NOALLOC_MAX_NODES;
-constexpr long kScratchWords = 6 * kNoAllocMaxNodes + 2;
+constexpr long kScratchWords = 6 * kNoAllocMaxNodes + 3;
 
 // Accumulators (hi, lo) x (J_x, J_y, J_z) x nodes, then the bit patterns of
-// max|q| and max|v| (non-negative doubles order like their bits).
+// max|q| and max|v| (non-negative doubles order like their bits), then a
+// flag word that is non-zero when a particle value is not finite.
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kScratchWords];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 unsigned long long* g_scratch_ptr[kMaxDevices] = {};
 
-__global__ void noalloc_bound_kernel(long np, const double* __restrict__ v, const double* __restrict__ q,
+// Bounds max|q|, max|v| and the non-finite flag.  fmax drops a NaN operand,
+// so non-finite values are caught by an explicit test, not by the bound.
+__global__ void noalloc_bound_kernel(long np, const double* __restrict__ x, const double* __restrict__ y,
+                                     const double* __restrict__ v, const double* __restrict__ q,
                                      unsigned long long* words) {
     double mq = 0.0, mv = 0.0;
+    bool bad = false;
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
-        mq = fmax(mq, fabs(q[p]));
         const double a = v[3 * p], b = v[3 * p + 1], c = v[3 * p + 2];
-        mv = fmax(mv, sqrt(a * a + b * b + c * c));
+        const double qp = q[p], sp = sqrt(a * a + b * b + c * c);
+        bad |= !(isfinite(qp) && isfinite(sp) && isfinite(x[p]) && isfinite(y[p]));
+        mq = fmax(mq, fabs(qp));
+        mv = fmax(mv, sp);
     }
     mq = warp_max(mq);
     mv = warp_max(mv);
+    const unsigned any_bad = __ballot_sync(0xffffffffu, bad);
     if ((threadIdx.x & 31) == 0) {
         atomicMax(&words[0], (unsigned long long)__double_as_longlong(mq));
         atomicMax(&words[1], (unsigned long long)__double_as_longlong(mv));
+        if (any_bad) atomicOr(&words[2], 1ull);
     }
 }
 
@@ -58,6 +67,7 @@ __global__ void noalloc_deposit_kernel(int nx, int ny, double inv_dx, double inv
                                        const double* __restrict__ v, const double* __restrict__ q,
                                        unsigned long long* acc, const unsigned long long* words) {
     const int N = nx * ny;
+    if (words[2]) return;  // non-finite input: nothing is deposited, J becomes NaN
     // fixed-point scale from the bound np * max|q| * max|v| / dA on any node
     // value (2^(91 - ceil(log2 bound)), as the context-based deposit uses)
     const double bound = (double)np * __longlong_as_double((long long)words[0]) *
@@ -102,10 +112,12 @@ __global__ void noalloc_convert_kernel(int N, long np, double inv_dA, const unsi
         frexp(bound, &e);
         inv_scale = ldexp(1.0, -max(-1000, min(1000, 91 - e)));
     }
+    const bool bad = words[2] != 0ull;
     for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < N; id += gridDim.x * blockDim.x)
         for (int c = 0; c < 3; ++c)
-            J[(size_t)c * N + id] = from_fixed(acc[(size_t)(2 * c) * N + id],
-                                               acc[(size_t)(2 * c + 1) * N + id], inv_scale);
+            J[(size_t)c * N + id] = bad ? __longlong_as_double(0x7ff8000000000000ll)
+                                        : from_fixed(acc[(size_t)(2 * c) * N + id],
+                                                     acc[(size_t)(2 * c + 1) * N + id], inv_scale);
 }
 
 bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
@@ -125,6 +137,9 @@ extern "C" int upic_deposit_current_noalloc(int nx, int ny, double Lx, double Ly
         (np > 0 && (!x || !y || !v || !q)))
         return UPIC_ERR_ARGUMENT;
     if ((long)nx * ny > kNoAllocMaxNodes) return UPIC_ERR_TOO_LARGE;  // grid larger than the scratch
+    // an error left pending by the caller's own earlier launches is not this
+    // call's to consume: report it and leave it in place
+    if (cudaPeekAtLastError() != cudaSuccess) return UPIC_ERR_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return UPIC_ERR_CUDA;
     unsigned long long* scratch = nullptr;
@@ -144,17 +159,24 @@ extern "C" int upic_deposit_current_noalloc(int nx, int ny, double Lx, double Ly
     unsigned long long* acc = scratch;
     unsigned long long* words = scratch + 6 * (size_t)N;
     // the array keeps the previous call's contents: clear what this call sums into
-    if (cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * (6 * (size_t)N + 2), st) != cudaSuccess)
+    if (cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * (6 * (size_t)N + 3), st) != cudaSuccess)
         return UPIC_ERR_CUDA;
     const double dx = Lx / nx, dy = Ly / ny;
     const double inv_dA = 1.0 / (dx * dy);
     if (np > 0) {
-        noalloc_bound_kernel<<<grid_blocks(np), 256, 0, st>>>(np, v, q, words);
+        noalloc_bound_kernel<<<grid_blocks(np), 256, 0, st>>>(np, x, y, v, q, words);
         noalloc_deposit_kernel<<<grid_blocks(np), 256, 0, st>>>(nx, ny, 1.0 / dx, 1.0 / dy, inv_dA, np, x, y,
                                                                 v, q, acc, words);
         count_launches(2);
     }
     noalloc_convert_kernel<<<grid_blocks(N), 256, 0, st>>>(N, np, inv_dA, acc, words, J);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? UPIC_OK : UPIC_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return UPIC_ERR_CUDA;
+    // the non-finite flag decides the return code, so the call waits for its
+    // own kernels on `stream` (one 8-byte read into host stack memory)
+    unsigned long long flag = 0;
+    if (cudaMemcpyAsync(&flag, words + 2, sizeof(flag), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return UPIC_ERR_CUDA;
+    return flag ? UPIC_ERR_NONFINITE : UPIC_OK;
 }
