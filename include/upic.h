@@ -88,7 +88,12 @@ enum { UPIC_CHARGE_CONSERVING = 0, UPIC_CHARGE_NAIVE = 1 };
 
 enum { UPIC_PRECISION_FP64 = 0, UPIC_PRECISION_MIXED = 1 };
 
-/* Field selectors for upic_get_field / upic_set_field. */
+/* Field selectors for upic_get_field.  E and B are derived on request from
+ * the resident state: explicit methods E = -grad phi - dA/dt with the step's
+ * BDF derivative and B = curl A (compute_diagnostics,
+ * Project2/spectral_pic_part3.cpp:918-944); implicit methods E = -grad phi - U
+ * and B = curl A (compute_E, spectral_curl,
+ * Project3/ec_pic_nyquist_projected.cpp:3338, :1780). */
 enum {
     UPIC_FIELD_PHI = 0,
     UPIC_FIELD_AX = 1,
@@ -102,7 +107,13 @@ enum {
     UPIC_FIELD_UX = 9,
     UPIC_FIELD_UY = 10,
     UPIC_FIELD_UZ = 11,
-    UPIC_FIELD_COUNT = 12
+    UPIC_FIELD_EX = 12,
+    UPIC_FIELD_EY = 13,
+    UPIC_FIELD_EZ = 14,
+    UPIC_FIELD_BX = 15,
+    UPIC_FIELD_BY = 16,
+    UPIC_FIELD_BZ = 17,
+    UPIC_FIELD_COUNT = 18
 };
 
 /* Diagnostics row, the column order of the reference's _diagnostics.csv after
@@ -347,6 +358,16 @@ int upic_particle_count(const upic_ctx* ctx, long* np);
 /* Fields of the current time level (phi, A, rho, J; implicit method also
  * psi = d phi/dt and U = dA/dt), nx*ny doubles. */
 int upic_get_field(upic_ctx* ctx, int which, double* host);
+
+/* Field snapshot of the implicit methods' accepted state in the columns of
+ * Project3's _field_grid_snapshots.csv (write_field_grid_header :8137-8140,
+ * write_field_grid_snapshot :8160): step,time,spline_order,ix,iy,iz,x,y,z,
+ * phi,psi,rho,Ax,Ay,Az,Ux,Uy,Uz,Jx,Jy,Jz,Ex,Ey,Ez,Bx,By,Bz, one row per node
+ * (x-major; x = -Lx/2 + ix*dx as in Project3's box, iz = 0, z = -Lz/2),
+ * values at 17 significant digits.  append = 0 creates the file with the
+ * header, append != 0 adds rows to it.  UPIC_ERR_STATE for explicit
+ * methods, whose state has no psi or U. */
+int upic_write_field_snapshot(upic_ctx* ctx, const char* path, int append, long step, double time);
 
 /* ---- Kernel-level entry points (host arrays in and out).  Each runs the
  * same device kernels as upic_step on the context's grid. ------------- */

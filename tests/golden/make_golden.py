@@ -201,6 +201,70 @@ def p3_long_main(lib=None):
     print(name, "seconds", out["seconds"], "iterations", out["info"][:, 0].sum())
 
 
+# Full-length run of the CPU-runnable explicit configuration: 2D Weibel on a
+# 64x64 grid over [0, 2 pi / 0.3)^2, 64 electrons per cell (262,144) from the
+# workloads' seeded bi-Maxwellian (vth 0.02 c in x, 0.2 c in y), quadratic
+# splines, BDF1 with the conserving charge update, dt 0.05, 1000 steps.  Only
+# the diagnostics rows (energy history, gauge / Gauss / continuity residuals,
+# |B_z|) and the final fields are kept; the particles are regenerated from
+# the seed (the generator is checked bit for bit in the CPU tests).
+P2_LONG_CASE = dict(nx=64, ny=64, L=2 * np.pi / 0.3, ppc=64, uth=(0.02, 0.2, 0.0), seed=2026, dt=0.05,
+                    n_steps=1000)
+
+
+def p2_long_main():
+    lib = ol.ref_p2()
+    if lib is None:
+        raise SystemExit("oracle/_ref/libref_p2.so missing: run make -C oracle")
+    c = P2_LONG_CASE
+    p = ol.generate_bimaxwellian(c["nx"], c["ny"], c["L"], c["L"], c["ppc"], c["uth"], seed=c["seed"])
+    parts = {"x": p["x"], "y": p["y"], "P": p["P"], "v": p["v"], "vprev": p["v_prev"], "q": p["q"], "m": p["m"]}
+    prob = ol.P2Problem(c["nx"], c["ny"], c["L"], c["L"], c["dt"], 1, True, n_steps=c["n_steps"])
+    out, diag, fields, secs = ol.simulate(lib.ref_p2_simulate, prob, parts)
+    np.savez_compressed(os.path.join(HERE, "p2_weibel64_long.npz"), params=prob.params(), iparams=prob.iparams(),
+                        ppc=c["ppc"], uth=np.array(c["uth"]), seed=c["seed"], diag=diag, fields=fields,
+                        out_v_checksum=np.array([out["v"].sum(), np.abs(out["v"]).sum()]), seconds=secs)
+    print("p2_weibel64_long seconds", secs)
+
+
+# Long implicit 2D Weibel run for the growth rate: a bi-Maxwellian hot along x
+# (u_th = 0.3 c in x, 0.03 c in y, seeded), so that the Weibel modes have k
+# along y (B_z(k_y), the mode Project3's diagnostics record); 16x16 grid over
+# [0, 2 pi)^2, 64 electrons per cell (16,384); the manuscript deck's solver
+# settings in 2D with its dt = 0.2, 200 steps: the magnetic field grows from
+# the particle noise by about 30x in field energy between t = 10 and t = 24,
+# then saturates.  Run on the OpenMP build of the reference
+# (oracle/_ref/libref_p3_omp.so, the reference's own -fopenmp recipe) when it
+# is present.
+P3_WEIBEL_CASE = dict(nx=16, ny=16, L=2 * np.pi, ppc=64, uth=(0.3, 0.03, 0.0), seed=77, dt=0.2, n_steps=200)
+
+
+def p3_weibel_particles(c):
+    """Particles of P3_WEIBEL_CASE in Project3's box [-L/2, L/2): x (n, 3), v (n, 3), q, m."""
+    p = ol.generate_bimaxwellian(c["nx"], c["ny"], c["L"], c["L"], c["ppc"], c["uth"], seed=c["seed"])
+    n = len(p["x"])
+    x = np.zeros((n, 3))
+    x[:, 0] = p["x"] - c["L"] / 2
+    x[:, 1] = p["y"] - c["L"] / 2
+    return x, p["v"], p["q"], np.abs(p["q"])
+
+
+def p3_weibel_main():
+    omp = os.path.join(os.path.dirname(ol.REF_P3_SO), "libref_p3_omp.so")
+    lib = ctypes.CDLL(omp) if os.path.exists(omp) else ol.ref_p3()
+    if lib is None:
+        raise SystemExit("oracle/_ref/libref_p3.so missing: run make -C oracle")
+    c = P3_WEIBEL_CASE
+    x, v, q, m = p3_weibel_particles(c)
+    prob = ol.P3Problem(c["nx"], c["ny"], c["L"], c["L"], c["dt"], order=2, nq=8, n_steps=c["n_steps"])
+    out = ol.p3_run(lib.ref_p3_run, prob, x, v, q, m)
+    np.savez_compressed(os.path.join(HERE, "p3_weibel16_long.npz"), dparams=prob.dparams(), iparams=prob.iparams(),
+                        ppc=c["ppc"], uth=np.array(c["uth"]), seed=c["seed"],
+                        diag=out["diag"], info=out["info"], fields=out["fields"], seconds=out["seconds"],
+                        threads=os.cpu_count() if os.path.exists(omp) else 1)
+    print("p3_weibel16_long seconds", out["seconds"], "iterations", out["info"][:, 0].sum())
+
+
 # Orbit kernels: (order, knot splitting, Gauss points)
 P3_ORBIT_CASES = [(2, True, 8), (2, False, 8), (1, True, 4), (3, True, 6)]
 
@@ -383,6 +447,10 @@ if __name__ == "__main__":
         p3_fallback_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "p3_long":
         p3_long_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "p2_long":
+        p2_long_main()
+    elif len(sys.argv) > 1 and sys.argv[1] == "p3_weibel":
+        p3_weibel_main()
     elif len(sys.argv) > 1 and sys.argv[1] == "p1":
         p1_main()
     else:

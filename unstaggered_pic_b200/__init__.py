@@ -8,6 +8,7 @@ velocity v, previous velocity v_prev, charge q and mass m; grids are nx*ny
 doubles with node id = i*ny + j.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -28,7 +29,7 @@ PRECISIONS = {"fp64": 0, "mixed": 1}
 PREDICTORS = {"previous": 0, "extrapolated": 1, "learned": 2}
 NONLINEAR_SOLVERS = {"anderson_quasi_newton": 0, "anderson": 0, "picard": 1}
 FIELDS = {"phi": 0, "Ax": 1, "Ay": 2, "Az": 3, "rho": 4, "Jx": 5, "Jy": 6, "Jz": 7,
-          "psi": 8, "Ux": 9, "Uy": 10, "Uz": 11}
+          "psi": 8, "Ux": 9, "Uy": 10, "Uz": 11, "Ex": 12, "Ey": 13, "Ez": 14, "Bx": 15, "By": 16, "Bz": 17}
 # Diagnostics columns of the reference's _diagnostics.csv (spectral_pic_part3.cpp:1117-1119).
 DIAG_COLUMNS = ["gauge_rms", "gauss_rms", "continuity_rms", "Bz_l2", "B_l2", "E_l2", "rho_l2",
                 "J_l2", "field_energy", "kinetic_energy", "total_energy", "max_speed",
@@ -338,6 +339,12 @@ class Simulation:
         out = np.empty(self.N)
         self._check(lib().upic_get_field(self._ctx, FIELDS[name], _p(out)))
         return out.reshape(self.config.nx, self.config.ny)
+
+    def write_field_snapshot(self, path, step, time, append=False):
+        """Project3's field grid snapshot CSV rows of the accepted state
+        (upic_write_field_snapshot)."""
+        self._check(lib().upic_write_field_snapshot(self._ctx, os.fsencode(path), int(bool(append)), int(step),
+                                                    float(time)))
 
     # ---- kernel-level entry points (include/upic.h) -----------------------
     def deposit_current(self, x, y, v, q):

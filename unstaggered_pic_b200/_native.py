@@ -40,6 +40,8 @@ SYMBOLS = {
     "upic_profile_read": (ctypes.c_int, [ctypes.c_void_p, c_dp, ctypes.POINTER(ctypes.c_long),
                                          ctypes.POINTER(ctypes.c_long)]),
     "upic_get_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp]),
+    "upic_write_field_snapshot": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_long,
+                                                 ctypes.c_double]),
     "upic_deposit_current": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 5),
     "upic_deposit_charge": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 4),
     "upic_gather": (ctypes.c_int, [ctypes.c_void_p, c_dp, ctypes.c_long, c_dp, c_dp, c_dp]),

@@ -1347,6 +1347,43 @@ int upic_get_field(upic_ctx* c, int which, double* host) {
                                      cudaMemcpyDeviceToHost, c->st));
         return sync(c);
     }
+    if (which >= UPIC_FIELD_EX && which <= UPIC_FIELD_BZ) {
+        // E = -grad phi - dA/dt (the BDF derivative of the last step, or zero
+        // at start-up as in the step-0 diagnostics row) and B = curl A, from
+        // the history spectra (compute_diagnostics :918-944)
+        int na, nb;
+        double a[3], b[5];
+        int prev = c->head;
+        if (c->steps == 0) {
+            na = 2;
+            a[0] = 1.0, a[1] = -1.0, a[2] = 0.0;
+        } else {
+            bdf_coeffs(c->cfg.method, na, a, nb, b);
+            prev = (c->head + 1) % kHistSlots;
+        }
+        DiagKArgs d{};
+        d.N = N;
+        d.kx = c->d_kx;
+        d.ky = c->d_ky;
+        d.k2 = c->d_k2;
+        d.Jhat = c->d_spec;
+        d.hist = c->d_hist;
+        d.R = kHistSlots;
+        d.slot_new = c->head;
+        d.slot_prev0 = prev;
+        d.na = na;
+        for (int k = 0; k < 3; ++k) d.a[k] = a[k];
+        d.dt = c->cfg.dt;
+        d.c = c->cfg.c;
+        d.eps0 = c->cfg.eps0;
+        d.out = c->d_dspec;
+        UPIC_CUDA(c, launch_diag_kspace(d, c->st));
+        // diag_kspace output slots: E 1..3, B 6..8
+        const int slot = which <= UPIC_FIELD_EZ ? 1 + which - UPIC_FIELD_EX : 6 + which - UPIC_FIELD_BX;
+        UPIC_CUDA(c, fft2d_batched(c->plan, c->d_dspec + (size_t)slot * N, 1, 1, c->st, nullptr, 1, c->d_dreal));
+        UPIC_CUDA(c, cudaMemcpyAsync(host, c->d_dreal, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
+        return sync(c);
+    }
     if (which < 0 || which > UPIC_FIELD_RHO) return fail(c, UPIC_ERR_ARGUMENT, "unknown field");
     const int f = which;  // phi 0, A 1..3, rho 4 share the history field index
     const double2* src = c->d_hist + ((size_t)f * kHistSlots + c->head) * N;

@@ -15,6 +15,7 @@
 // node: grad phi_mid, A^n, A^{n+1}); node currents J, J_field, guesses,
 // map values and the Anderson history (3 doubles per node each).
 #include <cfloat>
+#include <cstdio>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -1551,6 +1552,15 @@ int implicit_get_field(upic_ctx* c, int which, double* host) {
                                      cudaMemcpyDeviceToHost, c->st));
         return sync(c);
     }
+    if (which >= UPIC_FIELD_EX && which <= UPIC_FIELD_BZ) {
+        // E = -grad phi - U, B = curl A of the accepted state (compute_E
+        // :3338, spectral_curl :1780): diag_spectra slots E 0..2, B 3..5
+        UPIC_CUDA(c, launch_diag_spectra(N, c->d_kx, c->d_ky, s.spec, s.dspec, c->st));
+        const int slot = which - UPIC_FIELD_EX;
+        UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec + (size_t)slot * N, 1, 1, c->st, nullptr, 1, s.dreal));
+        UPIC_CUDA(c, cudaMemcpyAsync(host, s.dreal, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
+        return sync(c);
+    }
     // spectra slot of each field: phi 0, psi 1, rho 2, A 3..5, U 6..8
     int slot;
     switch (which) {
@@ -1912,4 +1922,55 @@ extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double*
             return rc;
     }
     return UPIC_OK;
+}
+
+// write_field_grid_header / write_field_grid_snapshot (:8137-8140, :8160):
+// one row per node, x-major, with the coordinates of Project3's box
+// [-L/2, L/2) and every value at 17 significant digits.
+extern "C" int upic_write_field_snapshot(upic_ctx* c, const char* path, int append, long step, double time) {
+    if (!c || !path) return UPIC_ERR_ARGUMENT;
+    if (!c->imp) return fail(c, UPIC_ERR_STATE, "field snapshots carry psi and U: implicit methods only");
+    if (!c->imp->ready) return fail(c, UPIC_ERR_STATE, "upic_init_fields first");
+    // column order of the snapshot after the coordinates
+    static const int kCols[18] = {UPIC_FIELD_PHI, UPIC_FIELD_PSI, UPIC_FIELD_RHO, UPIC_FIELD_AX, UPIC_FIELD_AY,
+                                  UPIC_FIELD_AZ,  UPIC_FIELD_UX,  UPIC_FIELD_UY,  UPIC_FIELD_UZ, UPIC_FIELD_JX,
+                                  UPIC_FIELD_JY,  UPIC_FIELD_JZ,  UPIC_FIELD_EX,  UPIC_FIELD_EY, UPIC_FIELD_EZ,
+                                  UPIC_FIELD_BX,  UPIC_FIELD_BY,  UPIC_FIELD_BZ};
+    const int N = c->N;
+    std::vector<double> f((size_t)18 * N);
+    for (int k = 0; k < 18; ++k) {
+        const int rc = implicit_get_field(c, kCols[k], f.data() + (size_t)k * N);
+        if (rc) return rc;
+    }
+    FILE* out = std::fopen(path, append ? "a" : "w");
+    if (!out) return fail(c, UPIC_ERR_ARGUMENT, std::string("cannot open ") + path);
+    if (!append)
+        std::fputs("step,time,spline_order,ix,iy,iz,x,y,z,phi,psi,rho,"
+                   "Ax,Ay,Az,Ux,Uy,Uz,Jx,Jy,Jz,Ex,Ey,Ez,Bx,By,Bz\n",
+                   out);
+    const upic_config& cf = c->cfg;
+    const double hx = cf.Lx / c->nx, hy = cf.Ly / c->ny;
+    const double z = -0.5 * cf.Lz;
+    std::string line;
+    char buf[64];
+    for (int i = 0; i < c->nx; ++i) {
+        for (int j = 0; j < c->ny; ++j) {
+            const int id = i * c->ny + j;
+            line.clear();
+            std::snprintf(buf, sizeof(buf), "%ld,%.17g,%d,%d,%d,0,", step, time, cf.spline_order, i, j);
+            line += buf;
+            const double xy[3] = {-0.5 * cf.Lx + (double)i * hx, -0.5 * cf.Ly + (double)j * hy, z};
+            for (double v : xy) {
+                std::snprintf(buf, sizeof(buf), "%.17g,", v);
+                line += buf;
+            }
+            for (int k = 0; k < 18; ++k) {
+                std::snprintf(buf, sizeof(buf), k < 17 ? "%.17g," : "%.17g\n", f[(size_t)k * N + id]);
+                line += buf;
+            }
+            std::fputs(line.c_str(), out);
+        }
+    }
+    const bool ok = std::fclose(out) == 0;
+    return ok ? UPIC_OK : fail(c, UPIC_ERR_ARGUMENT, std::string("write failed: ") + path);
 }
