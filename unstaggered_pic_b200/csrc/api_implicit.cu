@@ -97,6 +97,9 @@ struct ImplicitState {
     // non-relativistic Picard method (UPIC_METHOD_CN_ORBIT_NONREL)
     bool picard = false;
     double *gx = nullptr, *gy = nullptr, *gz = nullptr;  // velocity guess (sorted order)
+    // orbit velocities handed from the solve launch to the deposit launch of
+    // a map evaluation (ImplicitMapArgs::vbar_*; relativistic method only)
+    double *hvx = nullptr, *hvy = nullptr, *hvz = nullptr;
     double* Jprev = nullptr;                              // 3 x N
     // current of the step before the last (UPIC_PREDICTOR_EXTRAPOLATED)
     double* Jold = nullptr;                               // 3 x N
@@ -233,6 +236,9 @@ int alloc_particles(upic_ctx* c, ImplicitState& s, long cap, bool with_qm) {
     if ((s.picard || c->cfg.local_warm_start) &&
         ((rc = dalloc(c, &s.gx, cap)) || (rc = dalloc(c, &s.gy, cap)) || (rc = dalloc(c, &s.gz, cap))))
         return rc;
+    if (!s.picard &&
+        ((rc = dalloc(c, &s.hvx, cap)) || (rc = dalloc(c, &s.hvy, cap)) || (rc = dalloc(c, &s.hvz, cap))))
+        return rc;
     if (c->cfg.selective_particle_fallback &&
         ((rc = dalloc(c, &s.nsub, cap)) || (rc = dalloc(c, &s.refined, cap)) || (rc = dalloc(c, &s.failed, cap)) ||
          (rc = dalloc(c, &s.nfailed, 1)) || (rc = dalloc(c, &s.roff, cap))))
@@ -254,6 +260,10 @@ void free_particles(upic_ctx* c, ImplicitState& s) {
     dfree(c, s.gy);
     dfree(c, s.gz);
     s.gx = s.gy = s.gz = nullptr;
+    dfree(c, s.hvx);
+    dfree(c, s.hvy);
+    dfree(c, s.hvz);
+    s.hvx = s.hvy = s.hvz = nullptr;
     dfree(c, s.nsub);
     dfree(c, s.refined);
     dfree(c, s.failed);
@@ -359,6 +369,9 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
         a.sub_rec = s.sub_rec;
         UPIC_CUDA(c, cudaMemsetAsync(s.nfailed, 0, sizeof(int), c->st));
     }
+    a.vbar_x = s.hvx;
+    a.vbar_y = s.hvy;
+    a.vbar_z = s.hvz;
     if (cf.local_warm_start) {
         if (s.warm_valid) {
             a.warm_x = s.gx;

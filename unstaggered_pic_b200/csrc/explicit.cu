@@ -141,10 +141,14 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
 #if UPIC_PUSH_SMEM_GATHER
     // field records of the tile's window (kModePush): the gathers of
     // particles whose stencil lies in the window read them from here
-    double2* srec = reinterpret_cast<double2*>(
-        (reinterpret_cast<uintptr_t>(reinterpret_cast<int*>(reinterpret_cast<double*>(wlo + NCOMP * WN) +
-                                                            kPushWarps * StageLayout<NCOMP>::kDoubles) +
-                                     kPushWarps * 32) + 15) & ~uintptr_t(15));
+    // (16-byte aligned; the offset is taken from the shared base so that the
+    // pointer keeps the shared state space and the gathers are LDS, not
+    // generic loads)
+    unsigned char* const sbytes = reinterpret_cast<unsigned char*>(smem_u64);
+    const unsigned char* const sgk_end = reinterpret_cast<const unsigned char*>(
+        reinterpret_cast<int*>(reinterpret_cast<double*>(wlo + NCOMP * WN) +
+                               kPushWarps * StageLayout<NCOMP>::kDoubles) + kPushWarps * 32);
+    double2* srec = reinterpret_cast<double2*>(sbytes + (((sgk_end - sbytes) + 15) & ~ptrdiff_t(15)));
 #endif
 
     const int nx = tg.nx, ny = tg.ny;
@@ -171,7 +175,7 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
     }
 
     DD kin{0.0, 0.0}, gsum{0.0, 0.0};
-    double vmax = 0.0;
+    double vmax2 = 0.0;  // largest |v|^2 (sqrt taken once: sqrt is monotonic and correctly rounded)
     const double c2 = a.c * a.c;
 
     int cur_tile = -1, ox = 0, oy = 0;
@@ -301,7 +305,7 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                     const double gam = rsqrt(one_m > 1.0e-14 ? one_m : 1.0e-14);
                     gsum = dd_add(gsum, gam);
                     kin = dd_add(kin, (gam - 1.0) * m * a.c * a.c);
-                    vmax = fmax(vmax, sqrt(sp2));
+                    vmax2 = fmax(vmax2, sp2);
                 }
                 // deposit position: stored x (kModeDeposit) or one step ahead
                 if (MODE != kModeDeposit) {
@@ -408,13 +412,15 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                         const int t = lane + 32 * r;
                         if (t < NV) {
                             double s0 = 0.0, s1 = 0.0;
-                            int j = rs;
-                            const int iw = t_ab[r], iv = 9 + t_c[r];
-                            for (; j + 1 < re; j += 2) {
-                                s0 = fma(sprod[j * RW + iv], sprod[j * RW + iw], s0);
-                                s1 = fma(sprod[(j + 1) * RW + iv], sprod[(j + 1) * RW + iw], s1);
+                            // rows rs..re-1, two interleaved partial sums
+                            const double* pv = sprod + rs * RW + 9 + t_c[r];
+                            const double* pw = sprod + rs * RW + t_ab[r];
+                            const double* const pe = sprod + re * RW + 9 + t_c[r];
+                            for (; pv + RW < pe; pv += 2 * RW, pw += 2 * RW) {
+                                s0 = fma(pv[0], pw[0], s0);
+                                s1 = fma(pv[RW], pw[RW], s1);
                             }
-                            if (j < re) s0 = fma(sprod[j * RW + iv], sprod[j * RW + iw], s0);
+                            if (pv < pe) s0 = fma(pv[0], pw[0], s0);
                             const double sum = s0 + s1;
                             if (sum != 0.0) {
                                 int widx;
@@ -444,7 +450,7 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
     if (a.diag_part) {
         kin = warp_sum_dd(kin);
         gsum = warp_sum_dd(gsum);
-        vmax = warp_max(vmax);
+        const double vmax = warp_max(sqrt(vmax2));
         __syncthreads();
         double* red = reinterpret_cast<double*>(smem_u64);
         if (lane == 0) {

@@ -28,6 +28,24 @@ constexpr int kMapThreads = 128;
 #define UPIC_MAP_MIN_BLOCKS 3
 #endif
 constexpr int kMapMinBlocks = UPIC_MAP_MIN_BLOCKS;
+// A map evaluation runs as one fused launch (kPartFused), or as a local-solve
+// launch followed by a deposit launch (kPartSolve, kPartDeposit) that hands
+// the orbit velocities over through global memory.  The split keeps the
+// solve's code and registers free of the deposit machinery and gives the
+// deposit its own occupancy; the sums are the same bit for bit.
+#ifndef UPIC_MAP_SPLIT
+#define UPIC_MAP_SPLIT 1
+#endif
+#ifndef UPIC_SOLVE_MIN_BLOCKS
+#define UPIC_SOLVE_MIN_BLOCKS 3
+#endif
+#ifndef UPIC_DEPOSIT_MIN_BLOCKS
+#define UPIC_DEPOSIT_MIN_BLOCKS 6
+#endif
+constexpr int kPartFused = 0, kPartSolve = 1, kPartDeposit = 2;
+constexpr int map_min_blocks(int part) {
+    return part == kPartSolve ? UPIC_SOLVE_MIN_BLOCKS : part == kPartDeposit ? UPIC_DEPOSIT_MIN_BLOCKS : kMapMinBlocks;
+}
 constexpr int kMapWarps = kMapThreads / kWarp;
 constexpr int kKeyNone = -1;
 constexpr int kKeyEscape = -2;
@@ -578,9 +596,14 @@ UPIC_D int window_coord(int s, int origin, int n, int w, int span) {
 // Project1/ec_pic_serial_demo.cpp:1455-1474): the orbit velocity is
 // vbar = (v_guess + v^n) / 2 with no local solve, followed by the same
 // orbit-averaged deposit.
-template <int ORDER, bool UNIFORM, bool MOM, bool PICARD>
-__global__ void __launch_bounds__(kMapThreads, kMapMinBlocks)
+// PART: kPartFused (solve and deposit in one launch), kPartSolve (local
+// solves only; writes each particle's orbit velocity to vbar_*) or
+// kPartDeposit (the deposit of the orbits in vbar_*).
+template <int ORDER, bool UNIFORM, bool MOM, bool PICARD, int PART = kPartFused>
+__global__ void __launch_bounds__(kMapThreads, map_min_blocks(PART))
 implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
+    constexpr bool kSolve = PART != kPartDeposit;
+    constexpr bool kDeposit = PART != kPartSolve;
     constexpr int S = ORDER + 1;
     constexpr int SS = S * S;
     constexpr int NV = 3 * SS;
@@ -631,7 +654,7 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
     int cur_tile = -1, ox = 0, oy = 0;
     for (int ci = c_begin; ci < c_end; ++ci) {
         const Chunk ch = a.chunks[ci];
-        if (ch.tile != cur_tile) {
+        if (kDeposit && ch.tile != cur_tile) {
             __syncthreads();
             if (cur_tile >= 0) {
                 for (int idx = threadIdx.x; idx < 3 * WN; idx += blockDim.x) {
@@ -661,7 +684,23 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
             double bk[kMaxBreaks];
             int nb = 0;
             LocalIn in;
-            if (PICARD && active) {
+            if (PART == kPartDeposit) {
+                // the orbit velocity the solve launch accepted (NaN: none)
+                if (active) {
+                    vb[0] = a.vbar_x[p];
+                    vb[1] = a.vbar_y[p];
+                    vb[2] = a.vbar_z[p];
+                    ok = finite3(vb);
+                    if (ok) {
+                        in.x0 = a.x[p];
+                        in.y0 = a.y[p];
+                        in.q = UNIFORM ? a.q0 : a.q[p];
+                        nb = breakpoints<ORDER>(g, in.x0, in.y0, a.dt * vb[0], a.dt * vb[1], a.split, bk);
+                        ok = nb >= 0;
+                    }
+                    if (!ok) nb = 0;
+                }
+            } else if (PICARD && active) {
                 in.x0 = a.x[p];
                 in.y0 = a.y[p];
                 in.q = UNIFORM ? a.q0 : a.q[p];
@@ -774,6 +813,15 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                         a.obz[p] = guess[2];
                     }
                 }
+            }
+            if constexpr (PART == kPartSolve) {
+                if (active) {
+                    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+                    a.vbar_x[p] = ok ? vb[0] : nan;
+                    a.vbar_y[p] = ok ? vb[1] : nan;
+                    a.vbar_z[p] = ok ? vb[2] : nan;
+                }
+                continue;
             }
             // Orbit-averaged deposit of the accepted orbit (:2784).  Item k of
             // a particle is its k-th segment (MOM: the segment's shape sums,
@@ -913,19 +961,22 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
             }
         }
     }
-    __syncthreads();
-    if (cur_tile >= 0) {
-        for (int idx = threadIdx.x; idx < 3 * WN; idx += blockDim.x) {
-            const unsigned long long hi = whi[idx], lo = wlo[idx];
-            if ((hi | lo) == 0ull) continue;
-            const int cc = idx / WN, widx = idx - cc * WN;
-            const int lx = widx / tg.wy, ly = widx - lx * tg.wy;
-            const int gx = tg.full_x ? lx : wrap_index(ox + lx, nx);
-            const int gy = tg.full_y ? ly : wrap_index(oy + ly, ny);
-            atomicAdd(&a.acc[(size_t)(2 * cc) * N + gx * ny + gy], hi);
-            atomicAdd(&a.acc[(size_t)(2 * cc + 1) * N + gx * ny + gy], lo);
+    if (kDeposit) {
+        __syncthreads();
+        if (cur_tile >= 0) {
+            for (int idx = threadIdx.x; idx < 3 * WN; idx += blockDim.x) {
+                const unsigned long long hi = whi[idx], lo = wlo[idx];
+                if ((hi | lo) == 0ull) continue;
+                const int cc = idx / WN, widx = idx - cc * WN;
+                const int lx = widx / tg.wy, ly = widx - lx * tg.wy;
+                const int gx = tg.full_x ? lx : wrap_index(ox + lx, nx);
+                const int gy = tg.full_y ? ly : wrap_index(oy + ly, ny);
+                atomicAdd(&a.acc[(size_t)(2 * cc) * N + gx * ny + gy], hi);
+                atomicAdd(&a.acc[(size_t)(2 * cc + 1) * N + gx * ny + gy], lo);
+            }
         }
     }
+    if (!kSolve) return;
     // statistics (integer atomics and max over bit patterns: order independent)
     MapStats* st = a.stats;
     for (int o = 16; o > 0; o >>= 1) {
@@ -2203,11 +2254,11 @@ int gsize(long n, int threads = 256) {
 using MapKernel = void (*)(ImplicitMapArgs, TileGeom);
 
 // The map kernel instance of (order, uniform q/m, knot splitting, Picard
-// deposit).
-template <bool PICARD>
+// deposit, part).
+template <bool PICARD, int PART>
 MapKernel map_kernel_of(int order, bool uniform, bool split) {
     const bool mom = split && order <= 2;
-#define UPIC_K(O, U, M) &implicit_map_kernel<O, U, M, PICARD>
+#define UPIC_K(O, U, M) &implicit_map_kernel<O, U, M, PICARD, PART>
     switch (order) {
         case 1:
             return mom ? (uniform ? UPIC_K(1, true, true) : UPIC_K(1, false, true))
@@ -2222,8 +2273,19 @@ MapKernel map_kernel_of(int order, bool uniform, bool split) {
     return nullptr;
 }
 
-MapKernel map_kernel(int order, bool uniform, bool split, bool picard) {
-    return picard ? map_kernel_of<true>(order, uniform, split) : map_kernel_of<false>(order, uniform, split);
+MapKernel map_kernel(int order, bool uniform, bool split, bool picard, int part = kPartFused) {
+    if (picard) return map_kernel_of<true, kPartFused>(order, uniform, split);
+    switch (part) {
+        case kPartSolve: return map_kernel_of<false, kPartSolve>(order, uniform, split);
+        case kPartDeposit: return map_kernel_of<false, kPartDeposit>(order, uniform, split);
+        default: return map_kernel_of<false, kPartFused>(order, uniform, split);
+    }
+}
+
+// Split launches for the relativistic map when the caller supplied the
+// hand-over buffers.
+bool use_split(const ImplicitMapArgs& a, bool picard) {
+    return UPIC_MAP_SPLIT && !picard && a.vbar_x && a.vbar_y && a.vbar_z;
 }
 
 }  // namespace
@@ -2237,10 +2299,12 @@ int implicit_map_smem_bytes(const TileGeom& tg, int order) {
 cudaError_t implicit_configure_smem(const TileGeom& tg, int order, bool split, bool picard) {
     const int b = implicit_map_smem_bytes(tg, order);
     for (int u = 0; u < 2; ++u) {
-        MapKernel k = map_kernel(order, u != 0, split, picard);
-        if (!k) return cudaErrorInvalidValue;
-        const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), b);
-        if (e != cudaSuccess) return e;
+        for (int part = kPartFused; part <= (picard ? kPartFused : kPartDeposit); ++part) {
+            MapKernel k = map_kernel(order, u != 0, split, picard, part);
+            if (!k) return cudaErrorInvalidValue;
+            const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), b);
+            if (e != cudaSuccess) return e;
+        }
     }
     return cudaSuccess;
 }
@@ -2255,9 +2319,23 @@ int implicit_map_occupancy(const TileGeom& tg, int order, bool split, bool picar
 
 cudaError_t launch_implicit_map(int order, bool uniform, bool split, const TileGeom& tg,
                                 const ImplicitMapArgs& a, int grid, cudaStream_t st, bool picard) {
+    const int smem = implicit_map_smem_bytes(tg, order);
+    if (use_split(a, picard)) {
+        MapKernel ks = map_kernel(order, uniform, split, picard, kPartSolve);
+        MapKernel kd = map_kernel(order, uniform, split, picard, kPartDeposit);
+        if (!ks || !kd) return cudaErrorInvalidValue;
+        // grid is sized for the fused kernel's resident CTAs; each part is
+        // given as many CTAs as it keeps resident
+        const int gs = grid / kMapMinBlocks * UPIC_SOLVE_MIN_BLOCKS;
+        const int gd = grid / kMapMinBlocks * UPIC_DEPOSIT_MIN_BLOCKS;
+        ks<<<gs > 0 ? gs : grid, kMapThreads, smem, st>>>(a, tg);
+        kd<<<gd > 0 ? gd : grid, kMapThreads, smem, st>>>(a, tg);
+        count_launches(2);
+        return cudaGetLastError();
+    }
     MapKernel k = map_kernel(order, uniform, split, picard);
     if (!k) return cudaErrorInvalidValue;
-    k<<<grid, kMapThreads, implicit_map_smem_bytes(tg, order), st>>>(a, tg);
+    k<<<grid, kMapThreads, smem, st>>>(a, tg);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -93,6 +93,10 @@ struct ImplicitMapArgs {
     double* sub_rec;
     int* failed;
     int* nfailed;
+    // orbit velocities handed from the local-solve launch to the deposit
+    // launch of a split map evaluation (NaN for a particle that deposits
+    // nothing), or null: one fused launch
+    double *vbar_x, *vbar_y, *vbar_z;
 };
 // The refined particles of a sub-cycled map evaluation: chained local
 // solves over [k/n, (k+1)/n] of the step with time-interpolated fields, each

@@ -93,10 +93,13 @@ __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedP
                                       kMWarps * MStage<NCOMP>::kFloats) + warp * 32;
     // FP32 field records of the tile's window (kModePush): gathers of
     // stencils inside the window read them from here
-    float4* srec = reinterpret_cast<float4*>(
-        (reinterpret_cast<uintptr_t>(reinterpret_cast<int*>(reinterpret_cast<float*>(win + NCOMP * WN) +
-                                                            kMWarps * MStage<NCOMP>::kFloats) +
-                                     kMWarps * 32) + 15) & ~uintptr_t(15));
+    // (16-byte aligned; offset from the shared base, so the pointer keeps the
+    // shared state space: LDS, not generic loads)
+    unsigned char* const sbytes = reinterpret_cast<unsigned char*>(msmem);
+    const unsigned char* const sgk_end = reinterpret_cast<const unsigned char*>(
+        reinterpret_cast<int*>(reinterpret_cast<float*>(win + NCOMP * WN) + kMWarps * MStage<NCOMP>::kFloats) +
+        kMWarps * 32);
+    float4* srec = reinterpret_cast<float4*>(sbytes + (((sgk_end - sbytes) + 15) & ~ptrdiff_t(15)));
 
     const int nx = tg.nx, ny = tg.ny;
     const int N = nx * ny;
@@ -105,7 +108,7 @@ __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedP
     const int c_end = (int)(((long long)(blockIdx.x + 1) * nch) / gridDim.x);
 
     DD kin{0.0, 0.0}, gsum{0.0, 0.0};
-    double vmax = 0.0;
+    double vmax2 = 0.0;  // largest |v|^2 (sqrt taken once: monotonic, correctly rounded)
 
     int cur_tile = -1, ox = 0, oy = 0;
     for (int ci = c_begin; ci < c_end; ++ci) {
@@ -235,7 +238,7 @@ __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedP
                     const double gam = rsqrt(one_m > 1.0e-14 ? one_m : 1.0e-14);
                     gsum = dd_add(gsum, gam);
                     kin = dd_add(kin, (gam - 1.0) * m * a.cd * a.cd);
-                    vmax = fmax(vmax, sqrt(sp2));
+                    vmax2 = fmax(vmax2, sp2);
                 }
                 // deposit position: stored x (kModeDeposit) or one step ahead
                 if (MODE != kModeDeposit) {
@@ -363,7 +366,7 @@ __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedP
     if (a.diag_part) {
         kin = warp_sum_dd(kin);
         gsum = warp_sum_dd(gsum);
-        vmax = warp_max(vmax);
+        const double vmax = warp_max(sqrt(vmax2));
         __syncthreads();
         double* red = reinterpret_cast<double*>(msmem);
         if (lane == 0) {
