@@ -728,7 +728,9 @@ def measure(args, name, steps, warmup, world, rank, dist, dev, predictor="previo
         phases = {"set_particles": t1 - t0, "init_fields": t2 - t1, "steps": t3 - t2, "get_particles": t4 - t3}
         del out
         ncol = len(up.IMPLICIT_DIAG_COLUMNS) + len(up.SOLVE_INFO_COLUMNS) if implicit else len(up.DIAG_COLUMNS)
-        h2d = np_total * 13 * 8 / steps
+        # x, y, P, v, v_prev (11 doubles); q and m cross only when they are
+        # not uniform (this plasma's are: one species)
+        h2d = np_total * 11 * 8 / steps
         d2h = (ncol * 8 * (steps + 1) + np_total * 11 * 8) / steps
         api = "upic_step_implicit(K)" if implicit else "upic_step(K, diagnostics every step)"
         e2e = {"value": world * np_total * steps / t_e2e, "unit": METRIC,

@@ -233,10 +233,9 @@ UPIC_D double gamma_p(const double* p, double mk) { return sqrt(1.0 + dot3(p, p)
 
 // Higuera-Cary rotation by B_eff (higuera_cary_rotate_with_K :4636,
 // beff_from_skew_K :4605).
-UPIC_D void hc_rotate(const double* pm, const double* B, double q, double m, double kappa, double dt,
-                      double* out) {
-    const double mk = m * kappa;
-    double u[3] = {pm[0] * (1.0 / mk), pm[1] * (1.0 / mk), pm[2] * (1.0 / mk)};
+UPIC_D double hc_rotate(const double* pm, const double* B, double q, double m, double mk, double inv_mk,
+                        double dt, double* out) {
+    double u[3] = {pm[0] * inv_mk, pm[1] * inv_mk, pm[2] * inv_mk};
     const double gm = sqrt(1.0 + dot3(u, u));
     const double c = q * dt / (2.0 * m);
     const double tau[3] = {c * B[0], c * B[1], c * B[2]};
@@ -244,8 +243,8 @@ UPIC_D void hc_rotate(const double* pm, const double* B, double q, double m, dou
     const double udt = dot3(u, tau);
     const double sigma = gm * gm - tau2;
     const double ghc2 = 0.5 * (sigma + sqrt(sigma * sigma + 4.0 * (tau2 + udt * udt)));
-    const double ghc = sqrt(fmax(ghc2, 1.0));
-    const double t[3] = {tau[0] / ghc, tau[1] / ghc, tau[2] / ghc};
+    const double inv_ghc = 1.0 / sqrt(fmax(ghc2, 1.0));
+    const double t[3] = {tau[0] * inv_ghc, tau[1] * inv_ghc, tau[2] * inv_ghc};
     const double sf = 2.0 / (1.0 + dot3(t, t));
     const double sv[3] = {sf * t[0], sf * t[1], sf * t[2]};
     const double up[3] = {u[0] + (u[1] * t[2] - u[2] * t[1]), u[1] + (u[2] * t[0] - u[0] * t[2]),
@@ -255,15 +254,7 @@ UPIC_D void hc_rotate(const double* pm, const double* B, double q, double m, dou
     out[0] = mk * upl[0];
     out[1] = mk * upl[1];
     out[2] = mk * upl[2];
-}
-
-// kinetic_secant_velocity (:682)
-UPIC_D void secant(const double* a, const double* b, double m, double kappa, double* v) {
-    const double mk = m * kappa;
-    const double s = 1.0 / (m * (gamma_p(a, mk) + gamma_p(b, mk)));
-    v[0] = s * (a[0] + b[0]);
-    v[1] = s * (a[1] + b[1]);
-    v[2] = s * (a[2] + b[2]);
+    return gm;  // gamma of pm
 }
 
 struct LocalIn {
@@ -272,6 +263,9 @@ struct LocalIn {
     double A0p[3];
     double pstart[3];
     double q, m;
+    // per-particle constants of the local solve: m kappa, 1 / (m kappa) and
+    // gamma(pstart) (set by set_local_constants)
+    double mk, inv_mk, gstart;
 };
 
 struct LocalOut {
@@ -280,6 +274,56 @@ struct LocalOut {
     double v_end[3];
     double x1, y1;
 };
+
+// gamma_from_p (:584) with the particle's 1 / (m kappa)
+UPIC_D double gamma_p_inv(const double* p, double inv_mk) {
+    return sqrt(1.0 + dot3(p, p) * (inv_mk * inv_mk));
+}
+
+UPIC_D void set_local_constants(LocalIn& in, double kappa) {
+    in.mk = in.m * kappa;
+    in.inv_mk = 1.0 / in.mk;
+    in.gstart = gamma_p_inv(in.pstart, in.inv_mk);
+}
+
+// The kick-rotate-kick of one local map evaluation over a step h
+// (evaluate_local_particle_substep :4843-4929): the orbit averages gp =
+// <grad phi_mid> and D = <dA/dx>, A' at the orbit's end (A1p) and at its
+// midpoint ((A0p + A1p) / 2) give P_end, v_end and the secant orbit
+// velocity vbar_map.  Each gamma is evaluated once (the rotation's gamma of
+// p_minus serves its secant, gamma(pstart) is a particle constant, gamma of
+// p_end serves both v_end and its secant).
+UPIC_D void kick_rotate_kick(const LocalIn& in, const double* guess, double gp0, double gp1, const double (&D)[3][2],
+                             const double* A1p, double h, LocalOut& o) {
+    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
+                           0.5 * (in.A0p[2] + A1p[2])};
+    // D vbar and the skew part K = D^T - D as B_eff (:4585-4620); the z
+    // columns of D vanish in 2D.
+    const double Dv[3] = {D[0][0] * guess[0] + D[0][1] * guess[1], D[1][0] * guess[0] + D[1][1] * guess[1],
+                          D[2][0] * guess[0] + D[2][1] * guess[1]};
+    const double B[3] = {D[2][1], -D[2][0], D[1][0] - D[0][1]};
+    const double q = in.q, m = in.m, hq = 0.5 * q * h;
+    const double gpb[3] = {gp0, gp1, 0.0};
+    double pm[3], pp[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pm[c] = ((in.P0[c] - q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
+    const double gm = hc_rotate(pm, B, q, m, in.mk, in.inv_mk, h, pp);
+    double pend[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        o.P_end[c] = ((pp[c] + q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
+        pend[c] = o.P_end[c] - q * A1p[c];
+    }
+    const double gam = gamma_p_inv(pend, in.inv_mk);
+    const double inv_mgam = 1.0 / (m * gam);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.v_end[c] = pend[c] * inv_mgam;
+    // kinetic_secant_velocity (:682) of (p_minus, pstart) and (p_end, p_plus)
+    const double sm = 1.0 / (m * (gm + in.gstart));
+    const double sp = 1.0 / (m * (gam + gamma_p_inv(pp, in.inv_mk)));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o.vbar_map[c] = 0.5 * (sm * (pm[c] + in.pstart[c]) + sp * (pend[c] + pp[c]));
+}
 
 // Orbit averages along x0 + s (dxx, dxy), s in [0, 1] split at the
 // breakpoints b[0..nb): gp = <grad phi_mid> and D[c][d] = <d A_c / d x_d>
@@ -356,38 +400,11 @@ UPIC_D bool evaluate(const Geo& g, const double* __restrict__ rec, double dt, do
     o.y1 = wrap1(in.y0 + dxy, g.Ly);
     double A1p[3];
     gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, A1p);
-    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
-                           0.5 * (in.A0p[2] + A1p[2])};
     nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
     if (nb < 0) return false;
     double gpv[2], D[3][2];
     orbit_integrals_points<ORDER>(g, rec, in.x0, in.y0, dxx, dxy, b, nb, gpv, D);
-    const double gp0 = gpv[0], gp1 = gpv[1];
-    // D vbar and the skew part K = D^T - D as B_eff (:4585-4620); the z
-    // columns of D vanish in 2D.
-    const double Dv[3] = {D[0][0] * guess[0] + D[0][1] * guess[1], D[1][0] * guess[0] + D[1][1] * guess[1],
-                          D[2][0] * guess[0] + D[2][1] * guess[1]};
-    const double B[3] = {D[2][1], -D[2][0], D[1][0] - D[0][1]};
-    const double q = in.q, m = in.m, hq = 0.5 * q * dt;
-    const double gpb[3] = {gp0, gp1, 0.0};
-    double pm[3], pp[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) pm[c] = ((in.P0[c] - q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
-    hc_rotate(pm, B, q, m, kappa, dt, pp);
-    double pend[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        o.P_end[c] = ((pp[c] + q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
-        pend[c] = o.P_end[c] - q * A1p[c];
-    }
-    const double gam = gamma_p(pend, m * kappa);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) o.v_end[c] = pend[c] * (1.0 / (m * gam));
-    double vm[3], vp[3];
-    secant(pm, in.pstart, m, kappa, vm);
-    secant(pend, pp, m, kappa, vp);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) o.vbar_map[c] = 0.5 * (vm[c] + vp[c]);
+    kick_rotate_kick(in, guess, gpv[0], gpv[1], D, A1p, dt, o);
     return true;
 }
 
@@ -407,35 +424,11 @@ UPIC_D bool evaluate_sub(const Geo& g, const double* __restrict__ rec, double h,
     gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, Ae1);
 #pragma unroll
     for (int c = 0; c < 3; ++c) A1p[c] = (1.0 - th1) * An1[c] + th1 * Ae1[c];
-    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
-                           0.5 * (in.A0p[2] + A1p[2])};
     nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
     if (nb < 0) return false;
     double gpv[2], D[3][2];
     orbit_integrals_points<ORDER>(g, rec, in.x0, in.y0, dxx, dxy, b, nb, gpv, D, th0, th1);
-    const double Dv[3] = {D[0][0] * guess[0] + D[0][1] * guess[1], D[1][0] * guess[0] + D[1][1] * guess[1],
-                          D[2][0] * guess[0] + D[2][1] * guess[1]};
-    const double B[3] = {D[2][1], -D[2][0], D[1][0] - D[0][1]};
-    const double q = in.q, m = in.m, hq = 0.5 * q * h;
-    const double gpb[3] = {gpv[0], gpv[1], 0.0};
-    double pm[3], pp[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) pm[c] = ((in.P0[c] - q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
-    hc_rotate(pm, B, q, m, kappa, h, pp);
-    double pend[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        o.P_end[c] = ((pp[c] + q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
-        pend[c] = o.P_end[c] - q * A1p[c];
-    }
-    const double gam = gamma_p(pend, m * kappa);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) o.v_end[c] = pend[c] * (1.0 / (m * gam));
-    double vm[3], vp[3];
-    secant(pm, in.pstart, m, kappa, vm);
-    secant(pend, pp, m, kappa, vp);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) o.vbar_map[c] = 0.5 * (vm[c] + vp[c]);
+    kick_rotate_kick(in, guess, gpv[0], gpv[1], D, A1p, h, o);
     return true;
 }
 
@@ -550,36 +543,11 @@ UPIC_D bool evaluate_moments(const Geo& g, const double* __restrict__ rec, doubl
     o.y1 = wrap1(in.y0 + dxy, g.Ly);
     double A1p[3];
     gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, A1p);
-    const double Aep[3] = {0.5 * (in.A0p[0] + A1p[0]), 0.5 * (in.A0p[1] + A1p[1]),
-                           0.5 * (in.A0p[2] + A1p[2])};
     nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
     if (nb < 0) return false;
     double gpv[2], D[3][2];
     orbit_integrals_moments<ORDER>(g, rec, in.x0, in.y0, dxx, dxy, b, nb, gpv, D);
-    const double gp0 = gpv[0], gp1 = gpv[1];
-    const double Dv[3] = {D[0][0] * guess[0] + D[0][1] * guess[1], D[1][0] * guess[0] + D[1][1] * guess[1],
-                          D[2][0] * guess[0] + D[2][1] * guess[1]};
-    const double B[3] = {D[2][1], -D[2][0], D[1][0] - D[0][1]};
-    const double q = in.q, m = in.m, hq = 0.5 * q * dt;
-    const double gpb[3] = {gp0, gp1, 0.0};
-    double pm[3], pp[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) pm[c] = ((in.P0[c] - q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
-    hc_rotate(pm, B, q, m, kappa, dt, pp);
-    double pend[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        o.P_end[c] = ((pp[c] + q * Aep[c]) - hq * gpb[c]) + hq * Dv[c];
-        pend[c] = o.P_end[c] - q * A1p[c];
-    }
-    const double gam = gamma_p(pend, m * kappa);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) o.v_end[c] = pend[c] * (1.0 / (m * gam));
-    double vm[3], vp[3];
-    secant(pm, in.pstart, m, kappa, vm);
-    secant(pend, pp, m, kappa, vp);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) o.vbar_map[c] = 0.5 * (vm[c] + vp[c]);
+    kick_rotate_kick(in, guess, gpv[0], gpv[1], D, A1p, dt, o);
     return true;
 }
 
@@ -732,6 +700,7 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                 gather_rec3<ORDER>(g, a.rec, kIRecAn, in.x0, in.y0, in.A0p);
 #pragma unroll
                 for (int c = 0; c < 3; ++c) in.pstart[c] = in.P0[c] - in.q * in.A0p[c];
+                set_local_constants(in, a.kappa);
                 double guess[3] = {a.vx[p], a.vy[p], a.vz[p]};
                 if (a.warm_x) {
                     guess[0] = a.warm_x[p];
@@ -1050,6 +1019,7 @@ __global__ void __launch_bounds__(128) refined_map_kernel(ImplicitMapArgs a, int
                 in.A0p[c] = (1.0 - th0) * An0[c] + th0 * Ae0[c];
                 in.pstart[c] = P[c] - q * in.A0p[c];
             }
+            set_local_constants(in, a.kappa);
             double guess[3] = {v[0], v[1], v[2]};
             int reason = kLocalMaxIter, iters = 0, nb = 0;
             double scaled = INFINITY;
