@@ -105,6 +105,8 @@ def parse():
                     help="steps of the learned-vs-extrapolated first-guess comparison (0 skips; one GPU only)")
     ap.add_argument("--learned-train", type=int, default=200,
                     help="training steps of the learned first guess")
+    ap.add_argument("--learned-dt", type=float, default=None,
+                    help="time step of the learned-guess comparison (default: the case's 0.05)")
     ap.add_argument("--ensemble-runs", type=int, default=256,
                     help="independent runs of the ensemble comparison (0 skips; one GPU only)")
     ap.add_argument("--ensemble-steps", type=int, default=80,
@@ -373,7 +375,9 @@ def learned_comparison(args):
     every step), and the distance between the two final states."""
     import unstaggered_pic_b200 as up
 
-    c = LEARNED_CASE
+    c = dict(LEARNED_CASE)
+    if args.learned_dt:
+        c["dt"] = args.learned_dt
     steps, train = args.learned_steps, min(args.learned_train, max(0, args.learned_steps - 3))
     window = steps - min(steps, train + 2)
     p = learned_particles(up, c)
@@ -398,7 +402,7 @@ def learned_comparison(args):
     cols = up.SOLVE_INFO_COLUMNS
     out = {"workload": f"maxwellian_perturbed_{c['nx']}x{c['ny']}_ppc{c['ppc']}",
            "particles": c["nx"] * c["ny"] * c["ppc"], "steps": steps, "training_steps": train,
-           "nonlinear_rtol": 1e-10, "data": "synthetic (seeded Maxwellian, vth 0.05, density perturbation 0.01 at "
+           "dt": c["dt"], "nonlinear_rtol": 1e-10, "data": "synthetic (seeded Maxwellian, vth 0.05, density perturbation 0.01 at "
                                               "k = (1, 1))"}
     for pred, (info, _, ta, tb) in res.items():
         it = info[:, cols.index("iterations")]

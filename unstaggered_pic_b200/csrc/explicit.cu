@@ -39,16 +39,13 @@ constexpr int kPushWarps = kPushThreads / kWarp;
 constexpr int kKeyNone = -1;
 constexpr int kKeyEscape = -2;
 
-// Per-warp staging, column-major: column k < 9 holds the tensor-product
-// stencil weight S_ab (k = 3a + b) of each of the warp's 32 rows (particles),
-// column 9 + c its deposit value c (q v_c / dA, or q / dA).  A particle's
-// writes land in 32 consecutive doubles per column (no bank conflicts), and
-// the reduction reads two rows of a column with one 16-byte load.
+// Per-warp staging: one row per particle with its 9 tensor-product stencil
+// weights S_ab and its NCOMP deposit values (q v_c / dA, or q / dA).
 template <int NCOMP>
 struct StageLayout {
     static constexpr int kNV = 9 * NCOMP;   // values reduced per particle
-    static constexpr int kCols = 9 + NCOMP;  // doubles staged per particle
-    static constexpr int kDoubles = 32 * kCols;
+    static constexpr int kRow = 9 + NCOMP;  // doubles staged per particle
+    static constexpr int kDoubles = 32 * kRow;
 };
 
 UPIC_D int acc_slot(int ncomp, int c) { return ncomp == 1 ? 3 : c; }
@@ -131,6 +128,7 @@ template <int MODE, int NCOMP, bool UNIFORM>
 __global__ void __launch_bounds__(kPushThreads, UPIC_PUSH_MIN_BLOCKS)
 push_deposit_kernel(PushArgs a, TileGeom tg) {
     constexpr int NV = StageLayout<NCOMP>::kNV;
+    constexpr int RW = StageLayout<NCOMP>::kRow;
     constexpr int NPER = (NV + 31) / 32;
     extern __shared__ unsigned long long smem_u64[];
     const int WN = tg.wx * tg.wy;
@@ -362,13 +360,13 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
             if (key == kKeyEscape) row = nvalid + __popc(esc & lt);
             if (row >= 0) {
                 // stage S_ab and q v_c / dA of this particle in its row
-                double* mine = sprod + row;
+                double* mine = sprod + row * RW;
 #pragma unroll
                 for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
-                    for (int ib = 0; ib < 3; ++ib) mine[(ia * 3 + ib) * 32] = dwx[ia] * dwy[ib];
+                    for (int ib = 0; ib < 3; ++ib) mine[ia * 3 + ib] = dwx[ia] * dwy[ib];
 #pragma unroll
-                for (int cc = 0; cc < NCOMP; ++cc) mine[(9 + cc) * 32] = dval[cc];
+                for (int cc = 0; cc < NCOMP; ++cc) mine[9 + cc] = dval[cc];
             }
             __syncwarp();
             // Particles whose stencil leaves the window (rare): exact fixed-point
@@ -385,7 +383,7 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                     for (int r = 0; r < NPER; ++r) {
                         const int t = lane + 32 * r;
                         if (t < NV) {
-                            const double v = sprod[(9 + t_c[r]) * 32 + erow] * sprod[t_ab[r] * 32 + erow];
+                            const double v = sprod[erow * RW + 9 + t_c[r]] * sprod[erow * RW + t_ab[r]];
                             if (v != 0.0) {
                                 const int g = wrap_index(gxj + t_a[r], nx) * ny + wrap_index(gyj + t_b[r], ny);
                                 const int sl = acc_slot(NCOMP, t_c[r]);
@@ -414,23 +412,15 @@ push_deposit_kernel(PushArgs a, TileGeom tg) {
                         const int t = lane + 32 * r;
                         if (t < NV) {
                             double s0 = 0.0, s1 = 0.0;
-                            // rows rs..re-1 of columns S_ab and v_c: an odd first
-                            // row alone, then row pairs by 16-byte loads into two
-                            // interleaved partial sums (fixed order)
-                            const double* pw = sprod + t_ab[r] * 32;
-                            const double* pv = sprod + (9 + t_c[r]) * 32;
-                            int j = rs;
-                            if (j & 1) {
-                                s0 = fma(pv[j], pw[j], s0);
-                                ++j;
+                            // rows rs..re-1, two interleaved partial sums
+                            const double* pv = sprod + rs * RW + 9 + t_c[r];
+                            const double* pw = sprod + rs * RW + t_ab[r];
+                            const double* const pe = sprod + re * RW + 9 + t_c[r];
+                            for (; pv + RW < pe; pv += 2 * RW, pw += 2 * RW) {
+                                s0 = fma(pv[0], pw[0], s0);
+                                s1 = fma(pv[RW], pw[RW], s1);
                             }
-                            for (; j + 1 < re; j += 2) {
-                                const double2 w2 = *reinterpret_cast<const double2*>(pw + j);
-                                const double2 v2 = *reinterpret_cast<const double2*>(pv + j);
-                                s0 = fma(v2.x, w2.x, s0);
-                                s1 = fma(v2.y, w2.y, s1);
-                            }
-                            if (j < re) s0 = fma(pv[j], pw[j], s0);
+                            if (pv < pe) s0 = fma(pv[0], pw[0], s0);
                             const double sum = s0 + s1;
                             if (sum != 0.0) {
                                 int widx;

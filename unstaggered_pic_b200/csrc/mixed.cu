@@ -27,19 +27,12 @@ constexpr int kMWarps = kMThreads / kWarp;
 constexpr int kKeyNone = -1;
 constexpr int kKeyEscape = -2;
 
-// Per-warp staging, column-major (column k < 9: stencil weights S_ab of the
-// warp's 32 rows; column 9 + c: deposit value c): a particle's writes land in
-// consecutive floats of each column, and the reduction reads four rows of a
-// column with one 16-byte load.  The staging starts 16-byte aligned.
 template <int NCOMP>
 struct MStage {
-    static constexpr int kNV = 9 * NCOMP;    // values reduced per particle
-    static constexpr int kCols = 9 + NCOMP;  // floats staged per particle
-    static constexpr int kFloats = 32 * kCols;
+    static constexpr int kNV = 9 * NCOMP;   // values reduced per particle
+    static constexpr int kRow = 9 + NCOMP;  // floats staged per particle
+    static constexpr int kFloats = 32 * kRow;
 };
-
-// u64 words of the window accumulators, rounded up to whole 16-byte units
-__host__ __device__ inline int mixed_window_words(int ncomp, int wn) { return (ncomp * wn + 1) & ~1; }
 
 UPIC_D int slot_of(int ncomp, int c) { return ncomp == 1 ? 3 : c; }
 
@@ -89,21 +82,23 @@ UPIC_D void fold_window1(const unsigned long long* win, int WN, const TileGeom& 
 template <int MODE, int NCOMP, bool UNIFORM>
 __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedPushArgs a, TileGeom tg) {
     constexpr int NV = MStage<NCOMP>::kNV;
+    constexpr int RW = MStage<NCOMP>::kRow;
     constexpr int NPER = (NV + 31) / 32;
     extern __shared__ unsigned long long msmem[];
     const int WN = tg.wx * tg.wy;
     unsigned long long* win = msmem;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* const sstage = reinterpret_cast<float*>(win + mixed_window_words(NCOMP, WN));
-    float* sprod = sstage + warp * MStage<NCOMP>::kFloats;
-    int* sgk = reinterpret_cast<int*>(sstage + kMWarps * MStage<NCOMP>::kFloats) + warp * 32;
+    float* sprod = reinterpret_cast<float*>(win + NCOMP * WN) + warp * MStage<NCOMP>::kFloats;
+    int* sgk = reinterpret_cast<int*>(reinterpret_cast<float*>(win + NCOMP * WN) +
+                                      kMWarps * MStage<NCOMP>::kFloats) + warp * 32;
     // FP32 field records of the tile's window (kModePush): gathers of
     // stencils inside the window read them from here
     // (16-byte aligned; offset from the shared base, so the pointer keeps the
     // shared state space: LDS, not generic loads)
     unsigned char* const sbytes = reinterpret_cast<unsigned char*>(msmem);
     const unsigned char* const sgk_end = reinterpret_cast<const unsigned char*>(
-        reinterpret_cast<int*>(sstage + kMWarps * MStage<NCOMP>::kFloats) + kMWarps * 32);
+        reinterpret_cast<int*>(reinterpret_cast<float*>(win + NCOMP * WN) + kMWarps * MStage<NCOMP>::kFloats) +
+        kMWarps * 32);
     float4* srec = reinterpret_cast<float4*>(sbytes + (((sgk_end - sbytes) + 15) & ~ptrdiff_t(15)));
 
     const int nx = tg.nx, ny = tg.ny;
@@ -289,13 +284,13 @@ __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedP
             }
             if (key == kKeyEscape) row = nvalid + __popc(esc & lt);
             if (row >= 0) {
-                float* mine = sprod + row;
+                float* mine = sprod + row * RW;
 #pragma unroll
                 for (int ia = 0; ia < 3; ++ia)
 #pragma unroll
-                    for (int ib = 0; ib < 3; ++ib) mine[(ia * 3 + ib) * 32] = dwx[ia] * dwy[ib];
+                    for (int ib = 0; ib < 3; ++ib) mine[ia * 3 + ib] = dwx[ia] * dwy[ib];
 #pragma unroll
-                for (int cc = 0; cc < NCOMP; ++cc) mine[(9 + cc) * 32] = dval[cc];
+                for (int cc = 0; cc < NCOMP; ++cc) mine[9 + cc] = dval[cc];
             }
             __syncwarp();
             // particles whose stencil leaves the window: fixed-point adds to the grid
@@ -312,7 +307,7 @@ __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedP
                         const int t = lane + 32 * r;
                         if (t < NV) {
                             const int tab = t / NCOMP, tc = t - tab * NCOMP;
-                            const float v = sprod[(9 + tc) * 32 + erow] * sprod[tab * 32 + erow];
+                            const float v = sprod[erow * RW + 9 + tc] * sprod[erow * RW + tab];
                             if (v != 0.0f) {
                                 const int g = wrap_index(gxj + tab / 3, nx) * ny + wrap_index(gyj + tab % 3, ny);
                                 const int sl = slot_of(NCOMP, tc);
@@ -339,22 +334,12 @@ __global__ void __launch_bounds__(kMThreads, 4) push_deposit_mixed_kernel(MixedP
                         if (t < NV) {
                             const int tab = t / NCOMP, tc = t - tab * NCOMP;
                             float s0 = 0.0f, s1 = 0.0f;
-                            // rows rs..re-1 of columns S_ab and v_c: single rows up
-                            // to a multiple of four, then four rows per 16-byte
-                            // load into two interleaved partial sums (fixed order)
-                            const float* pw = sprod + tab * 32;
-                            const float* pv = sprod + (9 + tc) * 32;
                             int j = rs;
-                            for (; j < re && (j & 3); ++j) s0 = fmaf(pv[j], pw[j], s0);
-                            for (; j + 3 < re; j += 4) {
-                                const float4 w4 = *reinterpret_cast<const float4*>(pw + j);
-                                const float4 v4 = *reinterpret_cast<const float4*>(pv + j);
-                                s0 = fmaf(v4.x, w4.x, s0);
-                                s1 = fmaf(v4.y, w4.y, s1);
-                                s0 = fmaf(v4.z, w4.z, s0);
-                                s1 = fmaf(v4.w, w4.w, s1);
+                            for (; j + 1 < re; j += 2) {
+                                s0 = fmaf(sprod[j * RW + 9 + tc], sprod[j * RW + tab], s0);
+                                s1 = fmaf(sprod[(j + 1) * RW + 9 + tc], sprod[(j + 1) * RW + tab], s1);
                             }
-                            for (; j < re; ++j) s0 = fmaf(pv[j], pw[j], s0);
+                            if (j < re) s0 = fmaf(sprod[j * RW + 9 + tc], sprod[j * RW + tab], s0);
                             const float sum = s0 + s1;
                             if (sum != 0.0f) {
                                 int widx;
@@ -547,7 +532,7 @@ cudaError_t set_mixed_smem(int bytes) {
 }  // namespace
 
 int push_mixed_smem_bytes(const TileGeom& tg, int ncomp) {
-    const int window = mixed_window_words(ncomp, tg.wx * tg.wy) * 8;
+    const int window = ncomp * tg.wx * tg.wy * 8;
     const int stage = kMWarps * (32 * (9 + ncomp) * 4 + 32 * 4);
     const int bytes = window + stage + 16 + tg.wx * tg.wy * kGFStride * 4;
     const int red = kMWarps * 5 * 8;
