@@ -302,8 +302,14 @@ int sort_active(upic_ctx* c, ImplicitState& s) {
 // trial spectra to spec_out.  Returns UPIC_ERR_LOCAL_PARTICLE when a local
 // solve fails (the step then fails, as SelectiveParticleRefinementNeeded
 // propagates in the reference), with the failure described in c->err.
+int launch_residual_sums(upic_ctx* c, ImplicitState& s, const double* map, const double* guess);
+void norms_from_sums(upic_ctx* c, ImplicitState& s, Norms& n);
+
+// One evaluation of the outer map at `guess` into `out`.  With norms set, the
+// residual norms of (out, guess) are formed in the same round trip to the
+// host as the map's statistics.
 int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bool write_state,
-             MapStats* stats_out, bool* map_finite = nullptr) {
+             MapStats* stats_out, bool* map_finite = nullptr, Norms* norms = nullptr) {
     const upic_config& cf = c->cfg;
     const int N = c->N;
     // J_field = projected guess (:5264-5265), its spectra
@@ -404,10 +410,15 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
         UPIC_CUDA(c, launch_nonfinite_flag(3 * N, out, s.dflag, c->st));
         UPIC_CUDA(c, cudaMemcpyAsync(s.hflag, s.dflag, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     }
+    if (norms) {
+        const int rn = launch_residual_sums(c, s, out, guess);
+        if (rn) return rn;
+    }
     int rc = sync(c);
     if (rc) return rc;
     if (stats_out) *stats_out = *s.hstats;
     if (map_finite) *map_finite = *s.hflag == 0;
+    if (norms) norms_from_sums(c, s, *norms);
     if (s.hstats->failures > 0) {
         static const char* names[] = {"none", "nonfinite_map", "superluminal_map", "nonfinite_iterate",
                                       "superluminal_iterate", "maximum_iterations", "too_many_knot_crossings"};
@@ -623,15 +634,21 @@ int all_finite(upic_ctx* c, ImplicitState& s, const double* v, bool& finite) {
     return 0;
 }
 
-// nonlinear_residual_norms (:5576) on node vectors.
-int residual_norms(upic_ctx* c, ImplicitState& s, const double* map, const double* guess, Norms& n) {
+// nonlinear_residual_norms (:5576) on node vectors: the device sums and their
+// copy to the host, queued on the context's stream ...
+int launch_residual_sums(upic_ctx* c, ImplicitState& s, const double* map, const double* guess) {
     const upic_config& cf = c->cfg;
     const double floor_rel = 64.0 * DBL_EPSILON * cf.kappa;
     UPIC_CUDA(c, launch_residual_norms(c->N, map, guess, floor_rel, cf.nonlinear_atol, cf.nonlinear_rtol,
                                        s.partials, kNormGrid, s.dnorm, c->st));
     UPIC_CUDA(c, cudaMemcpyAsync(s.hnorm, s.dnorm, sizeof(NormSums), cudaMemcpyDeviceToHost, c->st));
-    int rc = sync(c);
-    if (rc) return rc;
+    return 0;
+}
+
+// ... and the norms from the sums once the stream has reached them.
+void norms_from_sums(upic_ctx* c, ImplicitState& s, Norms& n) {
+    const upic_config& cf = c->cfg;
+    const double floor_rel = 64.0 * DBL_EPSILON * cf.kappa;
     const double cnt = 3.0 * c->N;
     const NormSums& h = *s.hnorm;
     n.rms_absolute = std::sqrt((h.r2[0] + h.r2[1]) / cnt);
@@ -642,8 +659,8 @@ int residual_norms(upic_ctx* c, ImplicitState& s, const double* map, const doubl
     n.rms_scaled = n.rms_absolute / (cf.nonlinear_atol + cf.nonlinear_rtol * vrms);
     n.max_relative = h.max_rel;
     n.max_scaled = h.max_scaled;
-    return 0;
 }
+
 
 // anderson_type2_candidate (:5763) over the last m+1 history entries.
 int anderson_candidate(upic_ctx* c, ImplicitState& s, bool& ok) {
@@ -850,17 +867,18 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
     double prev_rms = INFINITY;
     bool have_prefetched = false, converged = false;
     int iterations = 0, anderson_steps = 0, picard_steps = 0;
-    Norms norms;
+    Norms norms, prefetched_norms;
     MapStats ms{};
     for (int it = 0; it < cf.nonlinear_max_iter; ++it) {
         if (!have_prefetched) {
-            if ((rc = eval_map(c, s, s.guess, s.map, false, &ms, &finite))) return rc;
+            if ((rc = eval_map(c, s, s.guess, s.map, false, &ms, &finite, &norms))) return rc;
             if (!finite)
                 return fail(c, UPIC_ERR_NONCONVERGED, "uniform particle map returned a nonfinite macro current");
+        } else {
+            norms = prefetched_norms;  // the accepted trial's norms: the same (map, guess) pair
         }
         have_prefetched = false;
         UPIC_CUDA(c, launch_axpy(n3, s.map, s.guess, -1.0, s.resid, c->st));
-        if ((rc = residual_norms(c, s, s.map, s.guess, norms))) return rc;
         iterations = it + 1;
         if (norms.rms_scaled <= 1.0 && norms.max_scaled <= 1.0) {
             converged = true;
@@ -880,23 +898,27 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
         }
         const double cur_rms = norms.rms_scaled, cur_max = norms.max_scaled;
         // backtracking line search on the candidate (:6044-6084)
-        auto try_update = [&](bool& accepted) -> int {
+        // cand_finite: the candidate is known to be finite, and so is every
+        // trial between it and the (finite) current guess
+        auto try_update = [&](bool& accepted, bool cand_finite) -> int {
             accepted = false;
             for (int bt = 0; bt <= 6; ++bt) {
                 const double alpha = std::ldexp(1.0, -bt);
                 UPIC_CUDA(c, launch_lerp(n3, s.guess, s.cand, alpha, s.trial, c->st));
-                bool tf = true;
-                int r2 = all_finite(c, s, s.trial, tf);
-                if (r2) return r2;
-                if (!tf) continue;
-                r2 = eval_map(c, s, s.trial, s.trial_map, false, &ms);
-                if (r2) return r2;
+                int r2;
+                if (!cand_finite) {
+                    bool tf = true;
+                    if ((r2 = all_finite(c, s, s.trial, tf))) return r2;
+                    if (!tf) continue;
+                }
                 Norms tn;
-                if ((r2 = residual_norms(c, s, s.trial_map, s.trial, tn))) return r2;
+                r2 = eval_map(c, s, s.trial, s.trial_map, false, &ms, nullptr, &tn);
+                if (r2) return r2;
                 if (!std::isfinite(tn.rms_scaled)) continue;
                 const bool dec = tn.rms_scaled <= (1.0 - 1.0e-4 * alpha) * cur_rms;
                 const bool safe = tn.max_scaled <= cf.anderson_growth_limit * cur_max;
                 if (dec && safe) {
+                    prefetched_norms = tn;
                     accepted = true;
                     return 0;
                 }
@@ -905,14 +927,14 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
         };
         bool accepted = false, as_anderson = false;
         if (used_anderson) {
-            if ((rc = try_update(accepted))) return rc;
+            if ((rc = try_update(accepted, true))) return rc;
             as_anderson = accepted;
             if (!accepted) reset_history(c, s, s.guess, s.resid);
         }
         if (!accepted) {
             const double damping = anderson ? cf.anderson_damping : 1.0;
             UPIC_CUDA(c, launch_axpy(n3, s.guess, s.resid, damping, s.cand, c->st));
-            if ((rc = try_update(accepted))) return rc;
+            if ((rc = try_update(accepted, false))) return rc;
         }
         if (!accepted)
             return fail(c, UPIC_ERR_NONCONVERGED,
@@ -931,9 +953,8 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
         return fail(c, UPIC_ERR_NONCONVERGED, buf);
     }
     // final consistency evaluation (:6160) produces the accepted state
-    if ((rc = eval_map(c, s, s.guess, s.map, true, &ms))) return rc;
     Norms fin;
-    if ((rc = residual_norms(c, s, s.map, s.guess, fin))) return rc;
+    if ((rc = eval_map(c, s, s.guess, s.map, true, &ms, nullptr, &fin))) return rc;
     if (!(fin.rms_scaled <= 1.0 && fin.max_scaled <= 1.0))
         return fail(c, UPIC_ERR_NONCONVERGED,
                     "final outer macro-current consistency evaluation failed at the prescribed macro dt");
