@@ -115,6 +115,10 @@ def parse():
                     help="1D-2V two-stream runs of the implicit ensemble comparison (0 skips; one GPU only)")
     ap.add_argument("--implicit-ensemble-steps", type=int, default=10,
                     help="steps of the implicit ensemble comparison")
+    ap.add_argument("--implicit-ensemble-max-particles", type=float, default=1e5,
+                    help="largest particle count of an implicit ensemble run (log-uniform from 1e4)")
+    ap.add_argument("--implicit-ensemble-check-runs", type=int, default=0,
+                    help="runs stepped alone for the sequential rate and the bitwise check (0: all)")
     ap.add_argument("--large-mixed-check", action="store_true",
                     help="instead of the bench line: the 2048x2048, 64 e-/cell Weibel + beam run in FP64 and in "
                          "mixed precision (energy drift and gauge residual of both), one JSON line")
@@ -535,18 +539,22 @@ def implicit_ensemble_comparison(args):
 
     rng = np.random.default_rng(909)
     nruns, steps = args.implicit_ensemble_runs, args.implicit_ensemble_steps
+    pmax = float(args.implicit_ensemble_max_particles)
     deck = dict(IMPLICIT_DECK)
     deck["spline_order"] = 3
     runs = []
     for r in range(nruns):
         nx = int(rng.choice([128, 256, 512, 1024]))
-        npart = 2 * int(round(np.exp(rng.uniform(np.log(1e4), np.log(1e5))) / 2))
+        npart = 2 * int(round(np.exp(rng.uniform(np.log(1e4), np.log(pmax))) / 2))
         v0 = float(rng.uniform(0.05, 0.3))
         runs.append((nx, npart, v0, 3000 + r))
+    # the runs stepped alone: all of them, or every k-th for a large ensemble
+    ncheck = args.implicit_ensemble_check_runs or nruns
+    checked = list(range(0, nruns, max(1, nruns // ncheck)))[:ncheck]
 
-    def start_all():
+    def start_all(which=None):
         sims = []
-        for nx, npart, v0, seed in runs:
+        for nx, npart, v0, seed in (runs if which is None else [runs[i] for i in which]):
             g = np.random.default_rng(seed)
             Lx = 2 * np.pi * v0 / 0.6 * 4  # four wavelengths of the fastest-growing cold mode
             nb = npart // 2
@@ -563,7 +571,8 @@ def implicit_ensemble_comparison(args):
         return sims
 
     total = sum(n for _, n, _, _ in runs)
-    seq = start_all()
+    total_checked = sum(runs[i][1] for i in checked)
+    seq = start_all(checked)
     t0 = time.perf_counter()
     for sim in seq:
         sim.step_implicit(steps, diagnostics=False)
@@ -574,16 +583,19 @@ def implicit_ensemble_comparison(args):
     ens.step(steps)
     t_ens = time.perf_counter() - t0
     diff = 0.0
-    for a, b in zip(seq, par):
-        diff = max(diff, float(np.max(np.abs(a.get_particles()["v"] - b.get_particles()["v"]))))
+    for i, a in zip(checked, seq):
+        diff = max(diff, float(np.max(np.abs(a.get_particles()["v"] - par[i].get_particles()["v"]))))
     ens.close()
     for sim in seq + par:
         sim.close()
     return {"workload": f"{nruns} independent 1D-2V two-stream runs (implicit GM-HC-CN, cubic), Nx from "
-                        "{128, 256, 512, 1024}, 1e4-1e5 particles each (log-uniform), v0 in [0.05, 0.3] c",
+                        f"{{128, 256, 512, 1024}}, 1e4-{pmax:.0e} particles each (log-uniform), v0 in [0.05, 0.3] c",
             "runs": nruns, "particles": total, "steps": steps,
-            "sequential": {"value": total * steps / t_seq, "unit": METRIC, "ms_per_step": 1e3 * t_seq / steps,
-                           "what": "upic_step_implicit(run, K) for each run in turn"},
+            "sequential": {"value": total_checked * steps / t_seq, "unit": METRIC,
+                           "ms_per_step": 1e3 * t_seq / steps, "runs": len(checked),
+                           "what": "upic_step_implicit(run, K) for each run in turn"
+                                   + ("" if len(checked) == nruns else
+                                      f" (every {max(1, nruns // ncheck)}-th run; rate over those runs)")},
             "ensemble": {"value": total * steps / t_ens, "unit": METRIC, "ms_per_step": 1e3 * t_ens / steps,
                          "what": "upic_ensemble_step: runs on a pool of host threads, each on its own stream"},
             "max_abs_velocity_difference": diff,

@@ -493,6 +493,55 @@ int upic_deposit_current_noalloc(int nx, int ny, double Lx, double Ly, long np, 
                                  const double* y, const double* v, const double* q, double* J,
                                  void* stream);
 
+/* ---- Project3's cold-instability initial states (2D, nz = 1) ------------
+ * initialize_two_stream_3d_linear_x (Project3/ec_pic_nyquist_projected.cpp
+ * :3689) and initialize_weibel_filamentation_3d (:3961): two cold electron
+ * streams at +-v0 along x on the same quiet-start positions (cell-centred,
+ * particles_per_cell_pair per cell along x), seeded with the growing
+ * cold-fluid eigenmode (the Config keys of the same names, defaults as the
+ * reference's Config).  upic_p3_initial_state fills x, y (in [-L/2, L/2)),
+ * v (xyz triples), q, m (upic_p3_case_particles entries) and the initial
+ * A, U (3 x nx*ny each; zero for the two-stream case), and the cold-fluid
+ * growth rate of the seeded mode (cold_two_stream_growth_rate :4160,
+ * cold_weibel_growth_rate :4197) when growth_rate is not NULL.  Host code;
+ * the arrays are the reference's bit for bit.  Start a run from them with
+ * upic_set_particles (P and v_prev are recomputed), upic_set_initial_potential
+ * and upic_init_fields. */
+enum { UPIC_P3_TWO_STREAM = 0, UPIC_P3_WEIBEL = 1 };
+typedef struct upic_p3_case {
+    int kind;                       /* UPIC_P3_TWO_STREAM or UPIC_P3_WEIBEL */
+    int nx, ny;
+    double Lx, Ly, Lz;
+    double kappa, sigma1, n0;
+    int spline_order;
+    int perturbation_mode;          /* mode along x (two-stream) or y (Weibel) */
+    int particles_per_cell_pair;
+    double v0;                      /* stream speed, |v0| < kappa */
+    double perturbation;            /* legacy two-stream velocity seed; Weibel B0 when weibel_B0 < 0 */
+    double two_stream_density_alpha;/* density eigenmode amplitude; < 0: legacy velocity seed */
+    int two_stream_eigenmode;
+    int two_stream_finite_grid_theory;
+    double tsi_transverse_seed;     /* common v_x seed amplitude along y */
+    int tsi_transverse_mode;
+    double weibel_B0;               /* B_z seed amplitude; < 0: perturbation */
+    int weibel_eigenmode;
+    int weibel_finite_grid_theory;
+} upic_p3_case;
+int upic_p3_case_default(upic_p3_case* c);
+long upic_p3_case_particles(const upic_p3_case* c);
+int upic_p3_initial_state(const upic_p3_case* c, long capacity, double* x, double* y, double* v, double* q,
+                          double* m, double* A, double* U, double* growth_rate);
+
+/* Initial vector potential A and its time derivative U (3 x nx*ny each,
+ * host arrays, reference index order) for the next upic_init_fields of an
+ * implicit-method context, which then uses them instead of A = U = 0: they
+ * are Nyquist-projected with the rest of the start state, the canonical
+ * momenta become P = m gamma v + q A(x), and the history velocities see
+ * E = -grad phi - U and B = curl A (project_initial_state :3398,
+ * initialize_relativistic_history_velocity :3423).  NULL, NULL clears them.
+ * UPIC_ERR_STATE for explicit methods. */
+int upic_set_initial_potential(upic_ctx* ctx, const double* A, const double* U);
+
 /* Seeded synthetic plasma generator (splitmix64 + Box-Muller, independent of
  * any C++ library's distributions): np_per_cell electrons per cell at uniform
  * random positions in [0,Lx)x[0,Ly) with a drifting bi-Maxwellian in

@@ -15,7 +15,7 @@ import numpy as np
 from ._native import UPIC_ERR, UpicConfig, c_dp, lib
 
 __all__ = ["UpicError", "Config", "ImplicitConfig", "NonrelConfig", "Simulation", "Ensemble", "autotune_explicit",
-           "generate_bimaxwellian",
+           "generate_bimaxwellian", "p3_initial_state", "P3_CASES",
            "DIAG_COLUMNS", "IMPLICIT_DIAG_COLUMNS", "NONREL_DIAG_COLUMNS", "SOLVE_INFO_COLUMNS",
            "STEP_DIAG_COLUMNS", "METHODS",
            "FIELDS"]
@@ -340,6 +340,15 @@ class Simulation:
         self._check(lib().upic_get_field(self._ctx, FIELDS[name], _p(out)))
         return out.reshape(self.config.nx, self.config.ny)
 
+    def set_initial_potential(self, A, U):
+        """Initial A and U (3 x nx x ny) for the next init_fields of an
+        implicit-method run (upic_set_initial_potential); None, None clears."""
+        if A is None and U is None:
+            self._check(lib().upic_set_initial_potential(self._ctx, None, None))
+            return
+        a, u = _f64(A, (3 * self.N,)), _f64(U, (3 * self.N,))
+        self._check(lib().upic_set_initial_potential(self._ctx, _p(a), _p(u)))
+
     def write_field_snapshot(self, path, step, time, append=False):
         """Project3's field grid snapshot CSV rows of the accepted state
         (upic_write_field_snapshot)."""
@@ -499,6 +508,40 @@ def autotune_explicit(make_config, particles, tiles=(4, 8, 16), sort_intervals=(
                 times[(tile, si)] = 1e3 * (time.perf_counter() - t0) / steps
     best = min(times, key=times.get)
     return best[0], best[1], times
+
+
+P3_CASES = {"two_stream": 0, "weibel": 1}
+
+
+def p3_initial_state(case, **keys):
+    """Project3's cold-instability start (upic_p3_initial_state): case
+    "two_stream" or "weibel" with Config keys (nx, ny, Lx, Ly, Lz, kappa,
+    sigma1, n0, spline_order, perturbation_mode, particles_per_cell_pair, v0,
+    perturbation, two_stream_*, tsi_transverse_*, weibel_*; the reference's
+    defaults otherwise).  Returns a dict of x, y, v, q, m (particles in
+    [-L/2, L/2)), A, U (3 x nx x ny) and growth_rate."""
+    from ._native import UpicP3Case
+    c = UpicP3Case()
+    lib().upic_p3_case_default(ctypes.byref(c))
+    c.kind = P3_CASES[case]
+    for k, v in keys.items():
+        if not hasattr(c, k):
+            raise KeyError(k)
+        setattr(c, k, int(v) if isinstance(getattr(c, k), int) else float(v))
+    n = lib().upic_p3_case_particles(ctypes.byref(c))
+    if n < 0:
+        raise UpicError(-1, "invalid instability case")
+    N = c.nx * c.ny
+    out = {"x": np.empty(n), "y": np.empty(n), "v": np.empty((n, 3)), "q": np.empty(n), "m": np.empty(n),
+           "A": np.empty((3, c.nx, c.ny)), "U": np.empty((3, c.nx, c.ny))}
+    rate = np.zeros(1)
+    rc = lib().upic_p3_initial_state(ctypes.byref(c), n, *[_p(out[k]) for k in ("x", "y", "v", "q", "m", "A", "U")],
+                                     _p(rate))
+    if rc != 0:
+        raise UpicError(rc, "p3_initial_state failed")
+    out["growth_rate"] = float(rate[0])
+    assert out["A"].size == 3 * N
+    return out
 
 
 def generate_bimaxwellian(nx, ny, Lx, Ly, ppc, uth, udrift=(0.0, 0.0, 0.0), c=1.0, n0=1.0, seed=1):

@@ -63,11 +63,32 @@ SYMBOLS = {
                                                     ctypes.c_double, ctypes.c_long, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p]),
+    "upic_p3_case_default": (ctypes.c_int, [ctypes.c_void_p]),
+    "upic_p3_case_particles": (ctypes.c_long, [ctypes.c_void_p]),
+    "upic_p3_initial_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 8),
+    "upic_set_initial_potential": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp]),
     "upic_generate_bimaxwellian": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                                   ctypes.c_double, c_dp, c_dp, ctypes.c_uint64]
                                    + [c_dp] * 7),
 }
+
+
+class UpicP3Case(ctypes.Structure):
+    """Mirror of struct upic_p3_case (include/upic.h)."""
+    _fields_ = [
+        ("kind", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("Lx", ctypes.c_double), ("Ly", ctypes.c_double), ("Lz", ctypes.c_double),
+        ("kappa", ctypes.c_double), ("sigma1", ctypes.c_double), ("n0", ctypes.c_double),
+        ("spline_order", ctypes.c_int), ("perturbation_mode", ctypes.c_int),
+        ("particles_per_cell_pair", ctypes.c_int),
+        ("v0", ctypes.c_double), ("perturbation", ctypes.c_double),
+        ("two_stream_density_alpha", ctypes.c_double), ("two_stream_eigenmode", ctypes.c_int),
+        ("two_stream_finite_grid_theory", ctypes.c_int),
+        ("tsi_transverse_seed", ctypes.c_double), ("tsi_transverse_mode", ctypes.c_int),
+        ("weibel_B0", ctypes.c_double), ("weibel_eigenmode", ctypes.c_int),
+        ("weibel_finite_grid_theory", ctypes.c_int),
+    ]
 
 
 class UpicConfig(ctypes.Structure):

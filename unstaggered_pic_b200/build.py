@@ -19,7 +19,7 @@ RUN = os.path.join(HERE, "upic_run")
 BUILD = os.path.join(ROOT, "_build")
 
 SOURCES = ["fft.cu", "sort.cu", "explicit.cu", "mixed.cu", "implicit.cu", "guess_net.cu", "api.cu", "api_implicit.cu",
-           "ensemble.cu", "noalloc.cu", "generate.cpp"]
+           "ensemble.cu", "noalloc.cu", "generate.cpp", "p3_init.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

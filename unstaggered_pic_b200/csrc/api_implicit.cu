@@ -100,6 +100,9 @@ struct ImplicitState {
     // orbit velocities handed from the solve launch to the deposit launch of
     // a map evaluation (ImplicitMapArgs::vbar_*; relativistic method only)
     double *hvx = nullptr, *hvy = nullptr, *hvz = nullptr;
+    // initial A and U (6 x N) for the next start-up (upic_set_initial_potential)
+    double* init_AU = nullptr;
+    bool init_AU_set = false;
     double* Jprev = nullptr;                              // 3 x N
     // current of the step before the last (UPIC_PREDICTOR_EXTRAPOLATED)
     double* Jold = nullptr;                               // 3 x N
@@ -1528,7 +1531,16 @@ int implicit_init_fields(upic_ctx* c, double* diag_row) {
     UPIC_CUDA(c, launch_poisson_kspace(N, c->d_k2, s.spec + 2 * (size_t)N, s.picard ? cf.eps0 : 1.0 / cf.sigma1,
                                        s.spec, c->st));
     UPIC_CUDA(c, launch_kspace_mask(s.spec, 1, N, cf.nyquist_projection ? s.excl : nullptr, 1, c->st));
-    // P = m gamma v (A = 0); v_prev from one backward Lorentz step; vbar = v
+    const bool with_AU = s.init_AU_set && !s.picard;
+    if (with_AU) {
+        // A, U of upic_set_initial_potential, Nyquist-projected with the rest
+        // of the start state (project_initial_state :3398)
+        UPIC_CUDA(c, fft2d_batched(c->plan, s.spec + 3 * (size_t)N, 3, 0, c->st, s.init_AU));
+        UPIC_CUDA(c, fft2d_batched(c->plan, s.spec + 6 * (size_t)N, 3, 0, c->st, s.init_AU + 3 * (size_t)N));
+        if (cf.nyquist_projection) UPIC_CUDA(c, launch_kspace_mask(s.spec + 3 * (size_t)N, 6, N, s.excl, 0, c->st));
+        s.init_AU_set = false;
+    }
+    // P = m gamma v + q A (A = 0 unless set); v_prev from one backward Lorentz step; vbar = v
     if (s.np > 0 && s.picard) {
         // P = m v, v_prev = v - dt (q/m) E (ec_pic_serial_demo.cpp:1200-1210)
         UPIC_CUDA(c, launch_diag_spectra(N, c->d_kx, c->d_ky, s.spec, s.dspec, c->st));
@@ -1539,6 +1551,14 @@ int implicit_init_fields(upic_ctx* c, double* diag_row) {
     } else if (s.np > 0) {
         UPIC_CUDA(c, launch_momentum_from_v(s.np, p.vx, p.vy, p.vz, s.uniform ? nullptr : p.m, s.m0, cf.kappa,
                                             p.Px, p.Py, p.Pz, c->st));
+        if (with_AU) {
+            // the projected A in real space, gathered at the particles
+            UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec + 3 * (size_t)N, sizeof(double2) * 3 * N,
+                                         cudaMemcpyDeviceToDevice, c->st));
+            UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 3, 1, c->st, nullptr, 1, s.dreal));
+            UPIC_CUDA(c, launch_add_qA(s.order, c->nx, c->ny, cf.Lx, cf.Ly, s.dreal, s.np, p.x, p.y,
+                                       s.uniform ? nullptr : p.q, s.q0, p.Px, p.Py, p.Pz, c->st));
+        }
         UPIC_CUDA(c, launch_diag_spectra(N, c->d_kx, c->d_ky, s.spec, s.dspec, c->st));
         UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 6, 1, c->st, nullptr, 1, s.dreal));
         UPIC_CUDA(c, launch_history_velocity(s.order, c->nx, c->ny, cf.Lx, cf.Ly, s.dreal, s.dreal + 3 * (size_t)N,
@@ -1955,6 +1975,29 @@ extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double*
                                                 step_diag + (size_t)k * UPIC_SD_COUNT)))
             return rc;
     }
+    return UPIC_OK;
+}
+
+extern "C" int upic_set_initial_potential(upic_ctx* c, const double* A, const double* U) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (!c->imp) return fail(c, UPIC_ERR_STATE, "an initial potential needs an implicit method");
+    ImplicitState& s = *c->imp;
+    if (!A && !U) {
+        s.init_AU_set = false;
+        return UPIC_OK;
+    }
+    if (!A || !U) return fail(c, UPIC_ERR_ARGUMENT, "A and U are both needed");
+    if (s.picard) return fail(c, UPIC_ERR_STATE, "the non-relativistic method starts from A = U = 0");
+    const int N = c->N;
+    int rc;
+    if (!s.init_AU && (rc = dalloc(c, &s.init_AU, 6 * (size_t)N))) return rc;
+    for (long k = 0; k < 3L * N; ++k)
+        if (!std::isfinite(A[k]) || !std::isfinite(U[k])) return fail(c, UPIC_ERR_NONFINITE, "non-finite A or U");
+    UPIC_CUDA(c, cudaMemcpyAsync(s.init_AU, A, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.init_AU + 3 * (size_t)N, U, sizeof(double) * 3 * N, cudaMemcpyHostToDevice,
+                                 c->st));
+    if ((rc = sync(c))) return rc;
+    s.init_AU_set = true;
     return UPIC_OK;
 }
 

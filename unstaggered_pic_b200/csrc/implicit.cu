@@ -1296,6 +1296,30 @@ __global__ void gather3_kernel(int nx, int ny, double Lx, double Ly, const doubl
 }
 
 template <int ORDER>
+__global__ void add_qA_kernel(int nx, int ny, double Lx, double Ly, const double* A3, long np, const double* x,
+                              const double* y, const double* q, double q0, double* Px, double* Py, double* Pz) {
+    const Geo g{nx, ny, Lx, Ly, nx / Lx, ny / Ly};
+    const int N = nx * ny;
+    double* const P[3] = {Px, Py, Pz};
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
+        Stencil<ORDER> sx, sy;
+        stencil_xy<ORDER>(g, x[p], y[p], sx, sy);
+        double o[3] = {0.0, 0.0, 0.0};
+        for (int ia = 0; ia <= ORDER; ++ia) {
+            const int gx = wrap_index(sx.il + ia, nx);
+            for (int ib = 0; ib <= ORDER; ++ib) {
+                const int node = gx * ny + wrap_index(sy.il + ib, ny);
+                const double w = sx.w[ia] * sy.w[ib];
+                for (int c = 0; c < 3; ++c) o[c] = fma(A3[(size_t)c * N + node], w, o[c]);
+            }
+        }
+        const double qp = q ? q[p] : q0;
+        // m gamma v + q A, the product rounded before the sum as the reference's
+        for (int c = 0; c < 3; ++c) P[c][p] = __dadd_rn(P[c][p], __dmul_rn(qp, o[c]));
+    }
+}
+
+template <int ORDER>
 __global__ void history_velocity_kernel(int nx, int ny, double Lx, double Ly, const double* E3,
                                         const double* B3, long np, const double* x, const double* y,
                                         const double* vx, const double* vy, const double* vz,
@@ -2467,6 +2491,21 @@ cudaError_t launch_point_deposit(int order, const PointDepositArgs& a, cudaStrea
         case 2: point_deposit_kernel<2><<<g, 256, 0, st>>>(a); break;
         case 3: point_deposit_kernel<3><<<g, 256, 0, st>>>(a); break;
         case 4: point_deposit_kernel<4><<<g, 256, 0, st>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_add_qA(int order, int nx, int ny, double Lx, double Ly, const double* A3, long np,
+                          const double* x, const double* y, const double* q, double q0, double* Px, double* Py,
+                          double* Pz, cudaStream_t st) {
+    const int g = gsize(np);
+    switch (order) {
+        case 1: add_qA_kernel<1><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, A3, np, x, y, q, q0, Px, Py, Pz); break;
+        case 2: add_qA_kernel<2><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, A3, np, x, y, q, q0, Px, Py, Pz); break;
+        case 3: add_qA_kernel<3><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, A3, np, x, y, q, q0, Px, Py, Pz); break;
+        case 4: add_qA_kernel<4><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, A3, np, x, y, q, q0, Px, Py, Pz); break;
         default: return cudaErrorInvalidValue;
     }
     count_launches(1);

@@ -189,6 +189,12 @@ cudaError_t launch_gather3(int order, int nx, int ny, double Lx, double Ly, cons
                            long np, const double* x, const double* y, double* out3,
                            cudaStream_t st);
 
+// P += q A(x) with A a planar 3-vector field (the canonical momentum of a
+// start state with a non-zero A, :4113-4117); q per particle or q0.
+cudaError_t launch_add_qA(int order, int nx, int ny, double Lx, double Ly, const double* A3, long np,
+                          const double* x, const double* y, const double* q, double q0, double* Px, double* Py,
+                          double* Pz, cudaStream_t st);
+
 // k-space map step: J_field spectra -> rho_end, rho_mid, CN (phi, psi), (A, U)
 // and the spectra of grad phi_mid and A_end (continuity_charge_update :3288,
 // cn_potential_update :3249, cn_fft_wave_step_from_spectra :3131).
