@@ -174,6 +174,29 @@ int ref_p3_orbit_gather(const double* d, const int* ip, long np, const double* x
     return 0;
 }
 
+// Config of an instability case: case_d = {v0, perturbation,
+// two_stream_density_alpha, tsi_transverse_seed, weibel_B0}, case_i = {kind
+// (0 two-stream, 1 Weibel), particles_per_cell_pair, two_stream_eigenmode,
+// two_stream_finite_grid_theory, tsi_transverse_mode, weibel_eigenmode,
+// weibel_finite_grid_theory}; the mode is iparams' I_MODE.
+Config make_case_cfg(const double* d, const int* ip, const double* cd, const int* ci) {
+    Config c = make_cfg(d, ip);
+    c.test_case = ci[0] == 1 ? "cold_relativistic_weibel" : "cold_relativistic_two_stream";
+    c.perturbation_mode = ip[I_MODE];
+    c.particles_per_cell_pair = ci[1];
+    c.two_stream_eigenmode = ci[2] != 0;
+    c.two_stream_finite_grid_theory = ci[3] != 0;
+    c.tsi_transverse_mode = ci[4];
+    c.weibel_eigenmode = ci[5] != 0;
+    c.weibel_finite_grid_theory = ci[6] != 0;
+    c.v0 = cd[0];
+    c.perturbation = cd[1];
+    c.two_stream_density_alpha = cd[2];
+    c.tsi_transverse_seed = cd[3];
+    c.weibel_B0 = cd[4];
+    return c;
+}
+
 // Injected start-up state (the tail of initialize_weibel_filamentation_3d,
 // :4061-4123, with the caller's particles, A = U = 0) followed by n_steps of
 // nonlinear_step_orbit (:6477) and compute_diagnostics (:3521) per step.
@@ -261,6 +284,80 @@ int ref_p3_run(const double* d, const int* ip, long np, double* x, double* v, do
         return 0;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "ref_p3_run: %s\n", e.what());
+        return -1;
+    }
+}
+
+// The reference's own start state of an instability case (initialize_state
+// :4125, after project_initial_state and the history velocities): x, v, P,
+// v_prev (3*np), q, m (np), A, U (3 x N), growth (1): the case's cold-fluid
+// rate (selected_theory_growth_rate).  Returns np, or -1 (error, message on
+// stderr) or -2 (cap too small).
+long ref_p3_case_state(const double* d, const int* ip, const double* cd, const int* ci, long cap, double* x,
+                       double* v, double* P, double* v_prev, double* q, double* m, double* A, double* U,
+                       double* growth) {
+    try {
+        Config c = make_case_cfg(d, ip, cd, ci);
+        Grid g = make_grid(c);
+        State st = initialize_state(c, g);
+        const long np = (long)st.x.size();
+        if (np > cap) return -2;
+        copy_vec3(st.x, x);
+        copy_vec3(st.v, v);
+        copy_vec3(st.P, P);
+        copy_vec3(st.v_prev, v_prev);
+        std::memcpy(q, st.q.data(), sizeof(double) * np);
+        std::memcpy(m, st.m.data(), sizeof(double) * np);
+        for (int k = 0; k < 3; ++k) {
+            std::memcpy(A + (std::size_t)k * g.N, st.A[k].data(), sizeof(double) * g.N);
+            std::memcpy(U + (std::size_t)k * g.N, st.U[k].data(), sizeof(double) * g.N);
+        }
+        if (growth) *growth = selected_theory_growth_rate(c, g);
+        return np;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_p3_case_state: %s\n", e.what());
+        return -1;
+    }
+}
+
+// An instability case run from the reference's own start state: n_steps of
+// nonlinear_step_orbit (:6477) with compute_diagnostics (:3521) per step;
+// diag (n_steps+1) x 23, info n_steps x 8, fields 12 x N after the last step
+// (the layouts of ref_p3_run).
+int ref_p3_case_run(const double* d, const int* ip, const double* cd, const int* ci, double* diag, double* info,
+                    double* fields, double* seconds) {
+    try {
+        Config c = make_case_cfg(d, ip, cd, ci);
+        Grid g = make_grid(c);
+        Quadrature quad = gauss_legendre_01(c.orbit_quad_order);
+        State st = initialize_state(c, g);
+        const int mode = ip[I_MODE];
+        if (diag) store_diag(compute_diagnostics(st, g, c.sigma1, c.sigma2, c.kappa, mode), diag);
+        const auto t0 = std::chrono::steady_clock::now();
+        for (int s = 1; s <= ip[I_NSTEPS]; ++s) {
+            std::vector<NonlinearHistoryEntry> hist;
+            NonlinearSolveInfo si;
+            st = nonlinear_step_orbit(st, g, c, quad, hist, &si, (s - 1) * c.dt);
+            if (diag) store_diag(compute_diagnostics(st, g, c.sigma1, c.sigma2, c.kappa, mode),
+                                 diag + (std::size_t)kDiag * s);
+            if (info) {
+                double* o = info + (std::size_t)kInfo * (s - 1);
+                o[0] = si.iterations; o[1] = si.converged; o[2] = si.final_rms_residual;
+                o[3] = si.final_max_particle_residual; o[4] = si.local_particle_iterations_max;
+                o[5] = si.local_particle_iterations_mean; o[6] = si.anderson_steps;
+                o[7] = si.picard_fallback_steps;
+            }
+        }
+        if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (fields) {
+            const Field* f[12] = {&st.phi, &st.psi, &st.rho, &st.A[0], &st.A[1], &st.A[2],
+                                  &st.U[0], &st.U[1], &st.U[2], &st.J[0], &st.J[1], &st.J[2]};
+            for (int k = 0; k < 12; ++k)
+                std::memcpy(fields + (std::size_t)k * g.N, f[k]->data(), sizeof(double) * g.N);
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_p3_case_run: %s\n", e.what());
         return -1;
     }
 }

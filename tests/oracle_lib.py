@@ -182,6 +182,64 @@ def p3_run(fn, prob, x, v, q, m, want_fields=True, want_step_diag=False):
     return out
 
 
+# Instability cases of the reference's initialize_state (ref_p3_case_state /
+# ref_p3_case_run): the case keys of upic_p3_case.
+P3_CASE_DEFAULTS = dict(v0=0.3, perturbation=0.02, two_stream_density_alpha=-1.0, tsi_transverse_seed=0.0,
+                        weibel_B0=-1.0, particles_per_cell_pair=4, two_stream_eigenmode=1,
+                        two_stream_finite_grid_theory=1, tsi_transverse_mode=1, weibel_eigenmode=1,
+                        weibel_finite_grid_theory=1)
+
+
+def p3_case_arrays(case, keys):
+    k = dict(P3_CASE_DEFAULTS)
+    k.update({a: b for a, b in keys.items() if a in k})
+    cd = np.array([k["v0"], k["perturbation"], k["two_stream_density_alpha"], k["tsi_transverse_seed"],
+                   k["weibel_B0"]], dtype=np.float64)
+    ci = np.array([1 if case == "weibel" else 0, k["particles_per_cell_pair"], k["two_stream_eigenmode"],
+                   k["two_stream_finite_grid_theory"], k["tsi_transverse_mode"], k["weibel_eigenmode"],
+                   k["weibel_finite_grid_theory"]], dtype=np.int32)
+    return cd, ci
+
+
+def p3_case_state(lib, prob, case, keys, cap=2_000_000):
+    """The reference's start state of an instability case: dict of x, v, P,
+    v_prev (np, 3), q, m (np), A, U (3, nx, ny), growth_rate."""
+    cd, ci = p3_case_arrays(case, keys)
+    N = prob.nx * prob.ny * prob.nz
+    out = {k: np.zeros((cap, 3)) for k in ("x", "v", "P", "v_prev")}
+    out.update(q=np.zeros(cap), m=np.zeros(cap), A=np.zeros(3 * N), U=np.zeros(3 * N))
+    g = np.zeros(1)
+    lib.ref_p3_case_state.restype = ctypes.c_long
+    n = lib.ref_p3_case_state(ptr(prob.dparams()), ptr(prob.iparams()), ptr(cd), ptr(ci), ctypes.c_long(cap),
+                              ptr(out["x"]), ptr(out["v"]), ptr(out["P"]), ptr(out["v_prev"]), ptr(out["q"]),
+                              ptr(out["m"]), ptr(out["A"]), ptr(out["U"]), ptr(g))
+    if n < 0:
+        raise RuntimeError("ref_p3_case_state failed")
+    for k in ("x", "v", "P", "v_prev", "q", "m"):
+        out[k] = out[k][:n]
+    out["A"] = out["A"].reshape(3, prob.nx, prob.ny * prob.nz)
+    out["U"] = out["U"].reshape(3, prob.nx, prob.ny * prob.nz)
+    out["growth_rate"] = float(g[0])
+    return out
+
+
+def p3_case_run(lib, prob, case, keys):
+    """An instability case run by the reference from its own start state:
+    dict of diag (n_steps+1, 23), info (n_steps, 8), fields (12, nx, ny), seconds."""
+    cd, ci = p3_case_arrays(case, keys)
+    N = prob.nx * prob.ny * prob.nz
+    diag = np.full((prob.n_steps + 1, P3_NDIAG), np.nan)
+    info = np.full((max(prob.n_steps, 1), P3_NINFO), np.nan)
+    fields = np.zeros((12, N))
+    secs = np.zeros(1)
+    rc = lib.ref_p3_case_run(ptr(prob.dparams()), ptr(prob.iparams()), ptr(cd), ptr(ci), ptr(diag), ptr(info),
+                             ptr(fields), ptr(secs))
+    if rc != 0:
+        raise RuntimeError("ref_p3_case_run failed")
+    return {"diag": diag, "info": info[:prob.n_steps], "fields": fields.reshape(12, prob.nx, prob.ny * prob.nz),
+            "seconds": float(secs[0])}
+
+
 def p3_particles(rng, nx, ny, ppc, Lx, Ly, uth=(0.02, 0.2, 0.0), n0=1.0, Lz=1.0):
     """Random electrons in [-L/2, L/2) (Project3's coordinates), normalized
     momentum u = gamma v Maxwellian with spreads uth, q/m = -1, neutralizing n0."""

@@ -197,3 +197,37 @@ def test_oracle_generator_equals_product_generator(args):
     b = up.generate_bimaxwellian(nx, ny, Lx, Ly, ppc, uth, udrift=ud, c=c, n0=n0, seed=seed)
     for k in a:
         assert a[k].tobytes() == b[k].tobytes(), k
+
+
+# Instability starts of Project3 (initialize_two_stream_3d_linear_x :3689,
+# initialize_weibel_filamentation_3d :3961) on 2D grids: the product's host
+# restatement against the reference's own initialize_state, bit for bit.
+P3_INIT_CASES = [
+    ("weibel", dict(nx=16, ny=16, Lx=2 * np.pi, Ly=2 * np.pi, v0=0.5, weibel_B0=1e-3, particles_per_cell_pair=2,
+                    spline_order=2)),
+    ("weibel", dict(nx=8, ny=32, Lx=3.0, Ly=2 * np.pi / 0.7, v0=0.3, perturbation=2e-3, particles_per_cell_pair=3,
+                    spline_order=3, perturbation_mode=2, weibel_finite_grid_theory=0)),
+    ("two_stream", dict(nx=32, ny=4, Lx=2 * np.pi / 3.0, Ly=1.0, v0=0.2, two_stream_density_alpha=1e-3,
+                        particles_per_cell_pair=8, spline_order=3)),
+    ("two_stream", dict(nx=16, ny=8, Lx=2 * np.pi, Ly=2.0, v0=0.25, perturbation=0.01, tsi_transverse_seed=1e-3,
+                        tsi_transverse_mode=2, particles_per_cell_pair=4, spline_order=2)),
+]
+
+
+@pytest.mark.parametrize("case,keys", P3_INIT_CASES)
+def test_p3_instability_start_equals_reference(case, keys):
+    lib = ol.ref_p3()
+    if lib is None:
+        pytest.skip("oracle/_ref/libref_p3.so is not built")
+    import unstaggered_pic_b200 as up
+    mine = up.p3_initial_state(case, Lz=1.0, **keys)
+    # the reference's start with its Nyquist projection off, so that A and U
+    # are the initializer's own
+    prob = ol.P3Problem(keys["nx"], keys["ny"], keys["Lx"], keys["Ly"], 0.1, Lz=1.0, order=keys["spline_order"],
+                        nyquist=False, mode=keys.get("perturbation_mode", 1))
+    ref = ol.p3_case_state(lib, prob, case, keys)
+    assert np.array_equal(mine["x"], ref["x"][:, 0]) and np.array_equal(mine["y"], ref["x"][:, 1])
+    assert np.all(ref["x"][:, 2] == 0.0)
+    for k in ("v", "q", "m", "A", "U"):
+        assert np.array_equal(mine[k], ref[k]), k
+    assert mine["growth_rate"] == ref["growth_rate"]
