@@ -245,7 +245,43 @@ enum {
      * (mean squared error in units of the rms second difference of J; NaN
      * when it did not train) */
     UPIC_INFO_PREDICTOR_USED, UPIC_INFO_GUESS_ERROR, UPIC_INFO_EXTRAPOLATION_ERROR, UPIC_INFO_LEARNED_ERROR,
-    UPIC_INFO_LEARNED_LOSS, UPIC_INFO_COUNT
+    UPIC_INFO_LEARNED_LOSS,
+    /* the rest of NonlinearSolveInfo (CN_ORBIT; NaN for CN_ORBIT_NONREL):
+     * Anderson restarts (history cleared by the growth limit, a failed or
+     * non-finite candidate, or a failed Anderson line search), the final
+     * absolute rms residual, the observed convergence rate (final / first
+     * relative rms residual)^(1/(iterations-1)) (observed_nonlinear_
+     * convergence_rate :5534; inf with fewer than 2 iterations), the secant
+     * map contraction rms(G(x_k) - G(x_{k-1})) / rms(x_k - x_{k-1}) of the
+     * last iterate pair with rms(x_k - x_{k-1}) > 64 eps (:5990-5996; inf
+     * when none), updates accepted with alpha < 1 and the smallest such
+     * alpha (1 when none), the method code of the last accepted update
+     * (UPIC_METHOD_CODE_*, upic_convergence_method_name), the largest
+     * substep count of the particle layout, the outer iterations of the
+     * failed direct attempt before a selective fallback, the selective
+     * work ratio (particle substeps / particles) and the particles at 1,
+     * 2, 4, ..., 64 substeps */
+    UPIC_INFO_ANDERSON_RESTARTS, UPIC_INFO_FINAL_ABS_RMS_RESIDUAL, UPIC_INFO_OBSERVED_RATE,
+    UPIC_INFO_MAP_CONTRACTION, UPIC_INFO_BACKTRACKED_STEPS, UPIC_INFO_MIN_UPDATE_ALPHA,
+    UPIC_INFO_CONVERGENCE_METHOD, UPIC_INFO_SUBSTEPS_USED, UPIC_INFO_DIRECT_ATTEMPT_ITERATIONS,
+    UPIC_INFO_SELECTIVE_WORK_RATIO, UPIC_INFO_SELECTIVE_N1, UPIC_INFO_SELECTIVE_N2, UPIC_INFO_SELECTIVE_N4,
+    UPIC_INFO_SELECTIVE_N8, UPIC_INFO_SELECTIVE_N16, UPIC_INFO_SELECTIVE_N32, UPIC_INFO_SELECTIVE_N64,
+    UPIC_INFO_COUNT
+};
+
+/* Method code of UPIC_INFO_CONVERGENCE_METHOD: base + 8 * form.  Bases
+ * (the update_method strings of nonlinear_step_uniform_subcycled :5878):
+ * none, picard, picard_fallback (converged before any update),
+ * current_anderson, current_anderson_backtracked, current_picard,
+ * current_picard_backtracked.  Forms (the prefix nonlinear_step_orbit
+ * :6477 and the selective fallback :6328 put in front): plain, the
+ * direct full-dt solve ("nested_full_dt_"), the selective fallback
+ * ("selective_"). */
+enum {
+    UPIC_METHOD_CODE_NONE = 0, UPIC_METHOD_CODE_PICARD, UPIC_METHOD_CODE_PICARD_FALLBACK,
+    UPIC_METHOD_CODE_ANDERSON, UPIC_METHOD_CODE_ANDERSON_BACKTRACKED, UPIC_METHOD_CODE_CURRENT_PICARD,
+    UPIC_METHOD_CODE_CURRENT_PICARD_BACKTRACKED,
+    UPIC_METHOD_FORM_DIRECT = 8, UPIC_METHOD_FORM_SELECTIVE = 16
 };
 
 /* Step diagnostics of the implicit method: StepDiagnostics of
@@ -368,6 +404,49 @@ int upic_get_field(upic_ctx* ctx, int which, double* host);
  * header, append != 0 adds rows to it.  UPIC_ERR_STATE for explicit
  * methods, whose state has no psi or U. */
 int upic_write_field_snapshot(upic_ctx* ctx, const char* path, int append, long step, double time);
+
+/* Time step of the next implicit steps (CN_ORBIT, CN_ORBIT_NONREL): the
+ * reference's run loop shortens the last step to the remaining time,
+ * dt_try = min(dt, n_steps*dt - time) (main, ec_pic_nyquist_projected.cpp
+ * :8702).  0 < dt <= the dt the context was created with (its deposit
+ * window covers kappa*dt of travel); UPIC_ERR_STATE for explicit methods,
+ * whose BDF coefficients are fixed at creation. */
+int upic_set_time_step(upic_ctx* ctx, double dt);
+
+/* The reference's string for a UPIC_INFO_CONVERGENCE_METHOD code
+ * ("nested_full_dt_current_anderson", ...); NULL for an unknown code. */
+const char* upic_convergence_method_name(int code);
+
+/* Map evaluations of the last upic_step_implicit call (CN_ORBIT), the rows
+ * of Project3's _particle_inner_history.csv after its time_n,dt columns
+ * (nonlinear_step_uniform_subcycled :5918-5945): step of the call (0 ..
+ * nsteps-1), map_evaluation (1, 2, ... within one outer solve; a selective
+ * fallback restarts the count), particles_converged (1 when every local
+ * particle solve converged, else 0), failed_particles,
+ * max_scaled_particle_residual (inf when non-finite),
+ * local_iterations_mean (NaN when particles failed), local_iterations_max.
+ * *nrows receives the number of rows; min(capacity, *nrows) rows of
+ * UPIC_MAPLOG_COUNT doubles are copied to rows. */
+enum {
+    UPIC_MAPLOG_STEP = 0, UPIC_MAPLOG_EVALUATION, UPIC_MAPLOG_CONVERGED, UPIC_MAPLOG_FAILED,
+    UPIC_MAPLOG_MAX_SCALED_RESIDUAL, UPIC_MAPLOG_ITER_MEAN, UPIC_MAPLOG_ITER_MAX, UPIC_MAPLOG_COUNT
+};
+int upic_map_log(upic_ctx* ctx, int capacity, double* rows, int* nrows);
+
+/* Point probes of the implicit method's accepted fields with the particle
+ * shape (evaluate_reconstructed_field_probe, ec_pic_nyquist_projected.cpp
+ * :7924-7945): for each point (x[p], y[p]) the B-spline gathers of phi,
+ * psi, rho, A, U, J, of the grid fields E = -grad phi - U and B = curl A
+ * (compute_E :3338, spectral_curl :1780), the shape gradient grad(S phi)
+ * (gather_shape_gradient_scalar_at) and grad(S A) (gradA[c][d] =
+ * dA_c/dx_d); z derivatives are 0 on the 2D grid.  out: np x
+ * UPIC_PROBE_COUNT doubles.  CN_ORBIT contexts. */
+enum {
+    UPIC_PROBE_PHI = 0, UPIC_PROBE_PSI = 1, UPIC_PROBE_RHO = 2, UPIC_PROBE_A = 3, UPIC_PROBE_U = 6,
+    UPIC_PROBE_J = 9, UPIC_PROBE_E = 12, UPIC_PROBE_B = 15, UPIC_PROBE_GRAD_PHI = 18, UPIC_PROBE_GRAD_A = 21,
+    UPIC_PROBE_COUNT = 30
+};
+int upic_probe_fields(upic_ctx* ctx, long np, const double* x, const double* y, double* out);
 
 /* ---- Kernel-level entry points (host arrays in and out).  Each runs the
  * same device kernels as upic_step on the context's grid. ------------- */
@@ -506,8 +585,14 @@ int upic_deposit_current_noalloc(int nx, int ny, double Lx, double Ly, long np, 
  * cold_weibel_growth_rate :4197) when growth_rate is not NULL.  Host code;
  * the arrays are the reference's bit for bit.  Start a run from them with
  * upic_set_particles (P and v_prev are recomputed), upic_set_initial_potential
- * and upic_init_fields. */
-enum { UPIC_P3_TWO_STREAM = 0, UPIC_P3_WEIBEL = 1 };
+ * and upic_init_fields.  UPIC_P3_LANDAU is Project3's retained Landau
+ * example (initialize_landau_damping_1d3d :3853): particles_per_cell_pair
+ * quiet-start velocities (thermal_velocity times Acklam's inverse normal
+ * CDF at (j + 1/2)/nv) along x at every cell centre, charges q0 (1 + alpha
+ * cos(k x)) with alpha = landau_alpha (perturbation when negative), A = U
+ * = 0, growth rate 0; UPIC_ERR_CONFIG for fewer than 2 velocities or
+ * |alpha| >= 1. */
+enum { UPIC_P3_TWO_STREAM = 0, UPIC_P3_WEIBEL = 1, UPIC_P3_LANDAU = 2 };
 typedef struct upic_p3_case {
     int kind;                       /* UPIC_P3_TWO_STREAM or UPIC_P3_WEIBEL */
     int nx, ny;
@@ -526,6 +611,8 @@ typedef struct upic_p3_case {
     double weibel_B0;               /* B_z seed amplitude; < 0: perturbation */
     int weibel_eigenmode;
     int weibel_finite_grid_theory;
+    double landau_alpha;            /* Landau density amplitude; < 0: perturbation */
+    double thermal_velocity;        /* Landau Maxwellian thermal speed */
 } upic_p3_case;
 int upic_p3_case_default(upic_p3_case* c);
 long upic_p3_case_particles(const upic_p3_case* c);

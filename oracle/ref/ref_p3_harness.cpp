@@ -181,7 +181,7 @@ int ref_p3_orbit_gather(const double* d, const int* ip, long np, const double* x
 // weibel_finite_grid_theory}; the mode is iparams' I_MODE.
 Config make_case_cfg(const double* d, const int* ip, const double* cd, const int* ci) {
     Config c = make_cfg(d, ip);
-    c.test_case = ci[0] == 1 ? "cold_relativistic_weibel" : "cold_relativistic_two_stream";
+    c.test_case = ci[0] == 2 ? "landau" : (ci[0] == 1 ? "cold_relativistic_weibel" : "cold_relativistic_two_stream");
     c.perturbation_mode = ip[I_MODE];
     c.particles_per_cell_pair = ci[1];
     c.two_stream_eigenmode = ci[2] != 0;
@@ -194,6 +194,8 @@ Config make_case_cfg(const double* d, const int* ip, const double* cd, const int
     c.two_stream_density_alpha = cd[2];
     c.tsi_transverse_seed = cd[3];
     c.weibel_B0 = cd[4];
+    c.landau_alpha = cd[5];
+    c.thermal_velocity = cd[6];
     return c;
 }
 
@@ -360,6 +362,17 @@ int ref_p3_case_run(const double* d, const int* ip, const double* cd, const int*
         std::fprintf(stderr, "ref_p3_case_run: %s\n", e.what());
         return -1;
     }
+}
+
+// The reference's own command-line program on a deck file (main :8336):
+// returns its exit code; output files go where the deck's output_prefix says.
+int ref_p3_run_deck(const char* deck) {
+    char prog[] = "ec_pic_nyquist_projected";
+    std::string d(deck);
+    std::vector<char> arg(d.begin(), d.end());
+    arg.push_back('\0');
+    char* argv[] = {prog, arg.data(), nullptr};
+    return upic_ref_p3_cli_main(2, argv);
 }
 
 }  // extern "C"

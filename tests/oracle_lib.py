@@ -187,15 +187,16 @@ def p3_run(fn, prob, x, v, q, m, want_fields=True, want_step_diag=False):
 P3_CASE_DEFAULTS = dict(v0=0.3, perturbation=0.02, two_stream_density_alpha=-1.0, tsi_transverse_seed=0.0,
                         weibel_B0=-1.0, particles_per_cell_pair=4, two_stream_eigenmode=1,
                         two_stream_finite_grid_theory=1, tsi_transverse_mode=1, weibel_eigenmode=1,
-                        weibel_finite_grid_theory=1)
+                        weibel_finite_grid_theory=1, landau_alpha=-1.0, thermal_velocity=1.0)
 
 
 def p3_case_arrays(case, keys):
     k = dict(P3_CASE_DEFAULTS)
     k.update({a: b for a, b in keys.items() if a in k})
     cd = np.array([k["v0"], k["perturbation"], k["two_stream_density_alpha"], k["tsi_transverse_seed"],
-                   k["weibel_B0"]], dtype=np.float64)
-    ci = np.array([1 if case == "weibel" else 0, k["particles_per_cell_pair"], k["two_stream_eigenmode"],
+                   k["weibel_B0"], k["landau_alpha"], k["thermal_velocity"]], dtype=np.float64)
+    ci = np.array([{"two_stream": 0, "weibel": 1, "landau": 2}[case], k["particles_per_cell_pair"],
+                   k["two_stream_eigenmode"],
                    k["two_stream_finite_grid_theory"], k["tsi_transverse_mode"], k["weibel_eigenmode"],
                    k["weibel_finite_grid_theory"]], dtype=np.int32)
     return cd, ci

@@ -302,3 +302,158 @@ def test_nonrel_unit_tests_pass(tmp_path):
                  "One-step R_A,p unit test: A_chain_abs_rms=", "One-step deposit/gather work residual="):
         assert line in log and line in out, line
     assert "FAILED" not in log and "Unit tests passed." in out
+
+
+# ---- Project3 decks: upic_run --p3 -------------------------------------------
+
+def write_p3_deck(path, prefix, **kw):
+    """A 2D Project3 deck (two-stream eigenmode, 16x4, five steps of dt 0.1,
+    the last one shortened to the remaining time) unless overridden."""
+    keys = dict(test_case="cold_relativistic_two_stream", nx=16, ny=4, nz=1, Lx=2.0943951023931953, Ly=1.0, Lz=1.0,
+                n_steps=5, dt=0.1, particles_per_cell_pair=4, spline_order=2, orbit_quad_order=8, v0=0.2,
+                two_stream_density_alpha=0.001, nyquist_projection="true", run_unit_tests="false")
+    keys.update(kw)
+    with open(path, "w") as fh:
+        fh.write("# Project3 deck written by the test\n")
+        for k, v in keys.items():
+            fh.write(f"{k} = {v}\n")
+        fh.write(f"output_prefix = {prefix}\n")
+
+
+def run_p3(deck, check=True):
+    r = subprocess.run([RUN, "--p3", deck], capture_output=True, text=True, timeout=900)
+    if check:
+        assert r.returncode == 0, r.stdout + r.stderr
+    return r
+
+
+# columns of the step records: integer counters of the outer solve (one
+# iteration more or less is the solver tolerance's reach), the method text,
+# residual-level columns (their values are differences of converged
+# iterates, known to ~1e-5 relative), wall-clock columns
+P3_COUNTERS = {"nonlinear_iterations", "anderson_restarts", "anderson_steps", "picard_fallback_steps",
+               "backtracked_steps", "local_particle_iterations_max", "local_iterations_max"}
+P3_RESIDUALS = {"nonlinear_rms_residual", "nonlinear_max_particle_residual", "nonlinear_absolute_rms_residual",
+                "observed_convergence_rate", "estimated_map_contraction", "max_scaled_particle_residual",
+                "local_particle_iterations_mean", "local_iterations_mean"}
+P3_TEXT = {"convergence_method", "outcome", "wavevector_class", "probe_axis"}
+P3_WALL = {"elapsed_wall_seconds"}
+
+
+def compare_p3_csv(a_path, b_path, tol):
+    """Every column of two Project3 CSV files by its kind: counters within
+    one, text equal, residual-level columns to 1e-3 on rows whose iteration
+    counts agree, knot jumps (differences of nearly equal probes) to 1e-6,
+    physical values to tol relative to the column's scale, round-off-level
+    columns (scale below 1e-9) by level."""
+    ha, ra = read_csv(a_path)
+    hb, rb = read_csv(b_path)
+    assert ha == hb, a_path
+    assert len(ra) == len(rb), (a_path, len(ra), len(rb))
+    if "nonlinear_iterations" in ha:
+        it = ha.index("nonlinear_iterations")
+        same = np.array([r1[it] == r2[it] for r1, r2 in zip(ra, rb)])
+    else:
+        same = np.ones(len(ra), dtype=bool)
+    for k, name in enumerate(ha):
+        if name in P3_WALL:
+            continue
+        if name in P3_TEXT:
+            for r1, r2, s in zip(ra, rb, same):
+                assert r1[k] == r2[k] or (name == "convergence_method" and not s), (a_path, name)
+            continue
+        a = np.array([float(r[k]) for r in ra])
+        b = np.array([float(r[k]) for r in rb])
+        assert np.array_equal(np.isnan(a), np.isnan(b)), (a_path, name)
+        assert np.array_equal(np.isinf(a), np.isinf(b)), (a_path, name)
+        fin = np.isfinite(b)
+        if not fin.any():
+            continue
+        d = np.abs(a - b)
+        if name in P3_COUNTERS:
+            assert np.max(d[fin]) <= 1, (a_path, name)
+        elif name in P3_RESIDUALS:
+            m = fin & same
+            assert np.all(d[m] <= 1e-3 * np.abs(b[m]) + 1e-14), (a_path, name)
+        else:
+            scale = np.max(np.abs(b[fin]))
+            rel = 1e-6 if name.endswith("_jump") else tol
+            if scale < 1e-9:
+                assert np.max(np.abs(a[fin])) < 1e-9, (a_path, name)
+            else:
+                assert np.max(d[fin]) <= rel * scale, (a_path, name, np.max(d[fin]) / scale)
+    return ha, ra, rb
+
+
+P3_DECKS = {
+    # two-stream eigenmode with a transverse seed: Nyquist projection, field
+    # line probes, grid snapshots, transverse diagnostics, particle snapshots
+    "two_stream": dict(field_grid_snapshots="true", field_diagnostics_interval=0.2, transverse_diagnostics="true",
+                       transverse_spectrum_interval=0.25, tsi_transverse_seed=0.001,
+                       particle_snapshot_times="0.1, 0.3"),
+    # Weibel eigenmode, cubic splines, probes along y; local iteration limit 2
+    # forces the selective sub-cycling fallback on every step
+    "weibel_selective": dict(test_case="cold_relativistic_weibel", nx=16, ny=16, Lx=6.283185307179586,
+                             Ly=6.283185307179586, n_steps=4, dt=0.2, particles_per_cell_pair=2, spline_order=3,
+                             v0=0.5, weibel_B0=0.001, two_stream_density_alpha=-1, nyquist_projection="false",
+                             field_probe_points_per_cell=4, field_diagnostics_interval=0.4,
+                             selective_particle_fallback="true", particle_local_max_iter=2),
+    # Project3's Landau example with the damped-Picard outer solver and a
+    # theory envelope
+    "landau_picard": dict(test_case="landau", nx=32, ny=2, Lx=12.566370614359172, n_steps=6, particles_per_cell_pair=16,
+                          thermal_velocity=0.1, landau_alpha=0.05, spline_order=1, orbit_quad_order=12,
+                          nonlinear_solver="picard", theory_gamma=-0.01, theory_omega=1.0, field_diagnostics="false",
+                          two_stream_density_alpha=-1, nyquist_projection="false"),
+}
+
+
+@pytest.mark.skipif(not os.path.exists(ol.REF_P3_SO), reason="oracle/_ref/libref_p3.so not built")
+@pytest.mark.parametrize("case", sorted(P3_DECKS))
+def test_p3_deck_matches_reference_cli(tmp_path, case):
+    """A 2D Project3 deck through upic_run --p3 and through the reference's
+    own main(): every output file, header and column."""
+    kw = P3_DECKS[case]
+    g, r = str(tmp_path / "gpu"), str(tmp_path / "ref")
+    write_p3_deck(g + ".txt", g, **kw)
+    write_p3_deck(r + ".txt", r, **kw)
+    out = run_p3(g + ".txt").stdout
+    assert "Final total energy" in out
+    ref = ol.ref_p3()
+    ref.ref_p3_run_deck.argtypes = [ctypes.c_char_p]
+    assert ref.ref_p3_run_deck((r + ".txt").encode()) == 0
+    assert open(g + "_config_echo.txt").read() == open(r + "_config_echo.txt").read()
+    nsteps = len(read_csv(r + "_step_diagnostics.csv")[1])
+    tol = 1e-9 * max(nsteps, 1)
+    h, ra, rb = compare_p3_csv(g + "_diagnostics.csv", r + "_diagnostics.csv", tol)
+    # every step converged with the reference's method and iteration count
+    assert [x[h.index("convergence_method")] for x in ra] == [x[h.index("convergence_method")] for x in rb]
+    compare_p3_csv(g + "_step_diagnostics.csv", r + "_step_diagnostics.csv", tol)
+    compare_p3_csv(g + "_adaptive_diagnostics.csv", r + "_adaptive_diagnostics.csv", tol)
+    compare_p3_csv(g + "_particle_inner_history.csv", r + "_particle_inner_history.csv", tol)
+    compare_p3_csv(g + "_particle_sample.csv", r + "_particle_sample.csv", tol)
+    assert read_csv(g + "_failed_particle_diagnostics.csv")[0] == read_csv(r + "_failed_particle_diagnostics.csv")[0]
+    names = sorted(os.path.basename(p)[len("ref"):] for p in map(str, tmp_path.glob("ref_*")))
+    assert names == sorted(os.path.basename(p)[len("gpu"):] for p in map(str, tmp_path.glob("gpu_*")))
+    for extra in ("_field_line_probe.csv", "_field_knot_jumps.csv", "_field_grid_snapshots.csv",
+                  "_velocity_moments.csv", "_field_spectrum.csv", "_particles_t0.10000000000000001.csv",
+                  "_particles_t0.29999999999999999.csv"):
+        if os.path.exists(r + extra):
+            compare_p3_csv(g + extra, r + extra, tol)
+    if case == "weibel_selective":
+        info = {n: [float(x[h.index(n)]) for x in ra[1:]] for n in ("selective_fallback_used", "selective_n4")}
+        assert all(v == 1 for v in info["selective_fallback_used"]) and max(info["selective_n4"]) > 0
+
+
+def test_p3_unit_tests_pass(tmp_path):
+    """run_unit_tests = true: the 2D start-up checks pass, with the
+    reference's messages, on the console and in _unit_tests.txt."""
+    g = str(tmp_path / "u")
+    write_p3_deck(g + ".txt", g, n_steps=1, run_unit_tests="true", field_diagnostics="false")
+    out = run_p3(g + ".txt").stdout
+    log = open(g + "_unit_tests.txt").read()
+    for line in ("Orbit deposit/gather adjoint unit test: residual=", "Initial Gauss-law unit test: gauss_rms=",
+                 "One-step Gauss-law unit test: gauss_rms=", "One-step R_A,p unit test: A_chain_abs_rms=",
+                 "Small multistep energy unit test: max_rel_drift=", "Instability IC/theory unit test: ts_gamma=",
+                 "Two-stream eigenmode growth unit test: gamma_fit="):
+        assert line in log and line in out, line
+    assert "FAILED" not in log and "Unit tests passed." in out

@@ -200,7 +200,8 @@ def test_oracle_generator_equals_product_generator(args):
 
 
 # Instability starts of Project3 (initialize_two_stream_3d_linear_x :3689,
-# initialize_weibel_filamentation_3d :3961) on 2D grids: the product's host
+# initialize_weibel_filamentation_3d :3961) and its Landau example
+# (initialize_landau_damping_1d3d :3853) on 2D grids: the product's host
 # restatement against the reference's own initialize_state, bit for bit.
 P3_INIT_CASES = [
     ("weibel", dict(nx=16, ny=16, Lx=2 * np.pi, Ly=2 * np.pi, v0=0.5, weibel_B0=1e-3, particles_per_cell_pair=2,
@@ -211,6 +212,10 @@ P3_INIT_CASES = [
                         particles_per_cell_pair=8, spline_order=3)),
     ("two_stream", dict(nx=16, ny=8, Lx=2 * np.pi, Ly=2.0, v0=0.25, perturbation=0.01, tsi_transverse_seed=1e-3,
                         tsi_transverse_mode=2, particles_per_cell_pair=4, spline_order=2)),
+    ("landau", dict(nx=32, ny=2, Lx=4 * np.pi, Ly=1.0, particles_per_cell_pair=16, landau_alpha=0.05,
+                    spline_order=1, thermal_velocity=0.1)),
+    ("landau", dict(nx=16, ny=4, Lx=2 * np.pi, Ly=3.0, particles_per_cell_pair=64, perturbation=0.3,
+                    spline_order=2, thermal_velocity=0.05, perturbation_mode=2)),
 ]
 
 

@@ -15,7 +15,8 @@ import numpy as np
 from ._native import UPIC_ERR, UpicConfig, c_dp, lib
 
 __all__ = ["UpicError", "Config", "ImplicitConfig", "NonrelConfig", "Simulation", "Ensemble", "autotune_explicit",
-           "generate_bimaxwellian", "p3_initial_state", "P3_CASES",
+           "generate_bimaxwellian", "p3_initial_state", "P3_CASES", "MAP_LOG_COLUMNS", "PROBE_COLUMNS",
+           "convergence_method_name",
            "DIAG_COLUMNS", "IMPLICIT_DIAG_COLUMNS", "NONREL_DIAG_COLUMNS", "SOLVE_INFO_COLUMNS",
            "STEP_DIAG_COLUMNS", "METHODS",
            "FIELDS"]
@@ -60,7 +61,22 @@ SOLVE_INFO_COLUMNS = ["iterations", "converged", "final_rms_residual", "final_ma
                       "max_path_segments", "selective_fallback_used", "selective_refinement_restarts",
                       "selective_refined_particles", "selective_total_particle_substeps",
                       # first guess of the outer current iteration (not in the reference)
-                      "predictor_used", "guess_error", "extrapolation_error", "learned_error", "learned_loss"]
+                      "predictor_used", "guess_error", "extrapolation_error", "learned_error", "learned_loss",
+                      # the rest of NonlinearSolveInfo
+                      "anderson_restarts", "nonlinear_absolute_rms_residual", "observed_convergence_rate",
+                      "estimated_map_contraction", "backtracked_steps", "minimum_update_alpha",
+                      "convergence_method", "uniform_substeps_used", "direct_attempt_iterations",
+                      "selective_work_ratio", "selective_n1", "selective_n2", "selective_n4", "selective_n8",
+                      "selective_n16", "selective_n32", "selective_n64"]
+# Map evaluations of the last step_implicit call (upic_map_log): the columns
+# of _particle_inner_history.csv after time_n, dt, with the step of the call.
+MAP_LOG_COLUMNS = ["step", "map_evaluation", "particles_converged", "failed_particles",
+                   "max_scaled_particle_residual", "local_iterations_mean", "local_iterations_max"]
+# Point probe columns (upic_probe_fields).
+PROBE_COLUMNS = (["phi_h", "psi_h", "rho_h", "Ax_h", "Ay_h", "Az_h", "Ux_h", "Uy_h", "Uz_h", "Jx_h", "Jy_h", "Jz_h",
+                  "Ex_grid_gather", "Ey_grid_gather", "Ez_grid_gather", "Bx_grid_gather", "By_grid_gather",
+                  "Bz_grid_gather", "dphi_dx", "dphi_dy", "dphi_dz"] +
+                 [f"dA{c}_d{d}" for c in "xyz" for d in "xyz"])
 
 
 class UpicError(RuntimeError):
@@ -349,6 +365,26 @@ class Simulation:
         a, u = _f64(A, (3 * self.N,)), _f64(U, (3 * self.N,))
         self._check(lib().upic_set_initial_potential(self._ctx, _p(a), _p(u)))
 
+    def map_log(self):
+        """Map evaluations of the last step_implicit call, one row each in
+        MAP_LOG_COLUMNS order (upic_map_log)."""
+        n = ctypes.c_int()
+        self._check(lib().upic_map_log(self._ctx, 0, None, ctypes.byref(n)))
+        rows = np.empty((n.value, len(MAP_LOG_COLUMNS)))
+        self._check(lib().upic_map_log(self._ctx, n.value, _p(rows), ctypes.byref(n)))
+        return rows
+
+    def probe_fields(self, x, y):
+        """Shape gathers and shape gradients of the accepted fields at the
+        points (x, y), one row each in PROBE_COLUMNS order (upic_probe_fields)."""
+        xa = _f64(x).ravel()
+        ya = _f64(y).ravel()
+        if ya.size != xa.size:
+            raise ValueError("x and y differ in length")
+        out = np.empty((xa.size, len(PROBE_COLUMNS)))
+        self._check(lib().upic_probe_fields(self._ctx, xa.size, _p(xa), _p(ya), _p(out)))
+        return out
+
     def write_field_snapshot(self, path, step, time, append=False):
         """Project3's field grid snapshot CSV rows of the accepted state
         (upic_write_field_snapshot)."""
@@ -510,7 +546,16 @@ def autotune_explicit(make_config, particles, tiles=(4, 8, 16), sort_intervals=(
     return best[0], best[1], times
 
 
-P3_CASES = {"two_stream": 0, "weibel": 1}
+P3_CASES = {"two_stream": 0, "weibel": 1, "landau": 2}
+
+
+def convergence_method_name(code):
+    """The reference's convergence_method string of a solve-report code
+    (upic_convergence_method_name)."""
+    name = lib().upic_convergence_method_name(int(code))
+    if name is None:
+        raise ValueError(f"unknown convergence method code {code}")
+    return name.decode()
 
 
 def p3_initial_state(case, **keys):

@@ -67,6 +67,10 @@ SYMBOLS = {
     "upic_p3_case_particles": (ctypes.c_long, [ctypes.c_void_p]),
     "upic_p3_initial_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 8),
     "upic_set_initial_potential": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp]),
+    "upic_convergence_method_name": (ctypes.c_char_p, [ctypes.c_int]),
+    "upic_set_time_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "upic_map_log": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, c_ip]),
+    "upic_probe_fields": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, c_dp, c_dp, c_dp]),
     "upic_generate_bimaxwellian": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                                   ctypes.c_double, c_dp, c_dp, ctypes.c_uint64]
@@ -88,6 +92,7 @@ class UpicP3Case(ctypes.Structure):
         ("tsi_transverse_seed", ctypes.c_double), ("tsi_transverse_mode", ctypes.c_int),
         ("weibel_B0", ctypes.c_double), ("weibel_eigenmode", ctypes.c_int),
         ("weibel_finite_grid_theory", ctypes.c_int),
+        ("landau_alpha", ctypes.c_double), ("thermal_velocity", ctypes.c_double),
     ]
 
 

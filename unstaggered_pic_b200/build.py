@@ -66,7 +66,8 @@ def build(verbose=False, ptxas_info=False):
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
     # upic_run: the deck-driven driver (host C++ over the C ABI)
-    srcs = [os.path.join(CSRC, "upic_run.cpp"), os.path.join(CSRC, "run_nonrel.cpp")]
+    srcs = [os.path.join(CSRC, "upic_run.cpp"), os.path.join(CSRC, "run_nonrel.cpp"),
+            os.path.join(CSRC, "run_p3.cpp")]
     if not _newer(RUN, srcs + [OUT, os.path.join(ROOT, "include", "upic.h")]):
         cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include")] + srcs + ["-o", RUN,
                "-L", HERE, "-lupic", "-Wl,-rpath,$ORIGIN"]

@@ -140,8 +140,22 @@ struct ImplicitState {
     unsigned long long* pstat = nullptr;                  // path statistics counters (4)
     int* perr = nullptr;
     double vb_limit = 0.0;  // bound on |vbar| components of the fixed-point deposit
+    double dt_max = 0.0;    // dt at creation: the deposit window guard covers kappa * dt_max
     bool loaded = false;  // upic_set_particles has succeeded
     bool ready = false;   // upic_init_fields has succeeded
+    // secant contraction sums of each outer iteration: |x_k - x_{k-1}|^2 at
+    // 4 k, |G(x_k) - G(x_{k-1})|^2 at 4 k + 2 (device; pinned copy)
+    double* dcon = nullptr;
+    double* hcon = nullptr;
+    // map evaluations of the current upic_step_implicit call
+    // (UPIC_MAPLOG_COUNT values each, upic_map_log)
+    std::vector<double> maplog;
+    int log_step = 0, map_eval = 0;
+    // F18: phi, psi, rho, A, U, J, E, B on the grid for upic_probe_fields;
+    // probe staging (grown on demand)
+    double* probe_grid = nullptr;
+    double *px = nullptr, *py = nullptr, *pout = nullptr;
+    long pcap = 0;
 };
 
 namespace {
@@ -311,6 +325,19 @@ void norms_from_sums(upic_ctx* c, ImplicitState& s, Norms& n);
 // One evaluation of the outer map at `guess` into `out`.  With norms set, the
 // residual norms of (out, guess) are formed in the same round trip to the
 // host as the map's statistics.
+// One row of upic_map_log for a map evaluation with statistics m
+// (nonlinear_step_uniform_subcycled's particle-history record :5918-5945).
+void log_map_evaluation(ImplicitState& s, const MapStats& m) {
+    double worst;
+    std::memcpy(&worst, &m.worst_scaled_bits, sizeof(double));
+    if (!std::isfinite(worst)) worst = INFINITY;
+    const bool ok = m.failures == 0;
+    const double mean = s.total_substeps > 0 ? (double)m.iter_total / (double)s.total_substeps : 0.0;
+    const double row[UPIC_MAPLOG_COUNT] = {(double)s.log_step, (double)++s.map_eval, ok ? 1.0 : 0.0,
+                                           (double)m.failures, worst, ok ? mean : NAN, (double)m.iter_max};
+    s.maplog.insert(s.maplog.end(), row, row + UPIC_MAPLOG_COUNT);
+}
+
 int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bool write_state,
              MapStats* stats_out, bool* map_finite = nullptr, Norms* norms = nullptr) {
     const upic_config& cf = c->cfg;
@@ -422,6 +449,7 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
     if (stats_out) *stats_out = *s.hstats;
     if (map_finite) *map_finite = *s.hflag == 0;
     if (norms) norms_from_sums(c, s, *norms);
+    log_map_evaluation(s, *s.hstats);
     if (s.hstats->failures > 0) {
         static const char* names[] = {"none", "nonfinite_map", "superluminal_map", "nonfinite_iterate",
                                       "superluminal_iterate", "maximum_iterations", "too_many_knot_crossings"};
@@ -847,6 +875,8 @@ int path_stats(upic_ctx* c, ImplicitState& s, double* out3) {
 // final evaluation).
 struct OuterResult {
     int iterations = 0, anderson_steps = 0, picard_steps = 0;
+    int restarts = 0, backtracked = 0, method = UPIC_METHOD_CODE_NONE;
+    double min_alpha = 1.0, observed_rate = INFINITY, contraction = INFINITY;
     Norms fin;
     MapStats ms{};
 };
@@ -860,6 +890,7 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
     const upic_config& cf = c->cfg;
     const int N = c->N, n3 = 3 * N;
     int rc;
+    out = OuterResult{};
     s.warm_valid = false;
     UPIC_CUDA(c, cudaMemcpyAsync(s.guess, s.J0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
     bool finite = true;
@@ -867,28 +898,46 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
     if (!finite) return fail(c, UPIC_ERR_NONFINITE, "nonfinite initial macro-current predictor");
     const bool anderson = cf.nonlinear_solver == UPIC_SOLVER_ANDERSON;
     s.hcount = 0;
-    double prev_rms = INFINITY;
+    s.map_eval = 0;
+    double prev_rms = INFINITY, first_rms = INFINITY;
     bool have_prefetched = false, converged = false;
-    int iterations = 0, anderson_steps = 0, picard_steps = 0;
+    int iterations = 0, anderson_steps = 0, picard_steps = 0, restarts = 0, backtracked = 0;
+    double min_alpha = 1.0;
+    // update_method of the last accepted update (:5902-5903, :6122-6128)
+    int method = anderson ? UPIC_METHOD_CODE_PICARD_FALLBACK : UPIC_METHOD_CODE_PICARD;
     Norms norms, prefetched_norms;
     MapStats ms{};
     for (int it = 0; it < cf.nonlinear_max_iter; ++it) {
         if (!have_prefetched) {
-            if ((rc = eval_map(c, s, s.guess, s.map, false, &ms, &finite, &norms))) return rc;
+            if ((rc = eval_map(c, s, s.guess, s.map, false, &ms, &finite, &norms))) {
+                out.iterations = it + 1;  // the iterations a failed attempt reports (:5949-5953)
+                return rc;
+            }
             if (!finite)
                 return fail(c, UPIC_ERR_NONCONVERGED, "uniform particle map returned a nonfinite macro current");
         } else {
             norms = prefetched_norms;  // the accepted trial's norms: the same (map, guess) pair
+            // secant contraction against the previous iterate, which the
+            // swap after the accepted update left in trial / trial_map
+            // (:5981-5996); read back with the final evaluation
+            const double* xs[2] = {s.trial, s.guess};
+            const double* gs[2] = {s.trial_map, s.map};
+            UPIC_CUDA(c, launch_anderson_dots(n3, xs, 1, s.partials, kNormGrid, s.dcon + 4 * (size_t)it, c->st));
+            UPIC_CUDA(c, launch_anderson_dots(n3, gs, 1, s.partials, kNormGrid, s.dcon + 4 * (size_t)it + 2,
+                                              c->st));
         }
         have_prefetched = false;
         UPIC_CUDA(c, launch_axpy(n3, s.map, s.guess, -1.0, s.resid, c->st));
         iterations = it + 1;
+        if (it == 0) first_rms = norms.rms_relative;
         if (norms.rms_scaled <= 1.0 && norms.max_scaled <= 1.0) {
             converged = true;
             break;
         }
-        if (anderson && std::isfinite(prev_rms) && norms.rms_relative > cf.anderson_growth_limit * prev_rms)
+        if (anderson && std::isfinite(prev_rms) && norms.rms_relative > cf.anderson_growth_limit * prev_rms) {
             s.hcount = 0;
+            ++restarts;
+        }
         push_history(c, s, s.guess, s.resid);
         bool used_anderson = false;
         if (anderson && it >= cf.anderson_start && s.hcount >= 2) {
@@ -897,16 +946,21 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
                 if ((rc = all_finite(c, s, s.cand, finite))) return rc;
                 used_anderson = finite;
             }
-            if (!used_anderson) reset_history(c, s, s.guess, s.resid);
+            if (!used_anderson) {
+                reset_history(c, s, s.guess, s.resid);
+                ++restarts;
+            }
         }
         const double cur_rms = norms.rms_scaled, cur_max = norms.max_scaled;
         // backtracking line search on the candidate (:6044-6084)
         // cand_finite: the candidate is known to be finite, and so is every
         // trial between it and the (finite) current guess
+        double accepted_alpha = 1.0;
         auto try_update = [&](bool& accepted, bool cand_finite) -> int {
             accepted = false;
             for (int bt = 0; bt <= 6; ++bt) {
                 const double alpha = std::ldexp(1.0, -bt);
+                accepted_alpha = alpha;
                 UPIC_CUDA(c, launch_lerp(n3, s.guess, s.cand, alpha, s.trial, c->st));
                 int r2;
                 if (!cand_finite) {
@@ -932,7 +986,10 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
         if (used_anderson) {
             if ((rc = try_update(accepted, true))) return rc;
             as_anderson = accepted;
-            if (!accepted) reset_history(c, s, s.guess, s.resid);
+            if (!accepted) {
+                reset_history(c, s, s.guess, s.resid);
+                ++restarts;
+            }
         }
         if (!accepted) {
             const double damping = anderson ? cf.anderson_damping : 1.0;
@@ -944,6 +1001,13 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
                         "outer current Anderson/Picard backtracking failed at the prescribed macro dt");
         if (as_anderson) ++anderson_steps;
         else ++picard_steps;
+        const bool bt = accepted_alpha < 1.0;
+        method = as_anderson ? (bt ? UPIC_METHOD_CODE_ANDERSON_BACKTRACKED : UPIC_METHOD_CODE_ANDERSON)
+                             : (bt ? UPIC_METHOD_CODE_CURRENT_PICARD_BACKTRACKED : UPIC_METHOD_CODE_CURRENT_PICARD);
+        if (bt) {
+            ++backtracked;
+            min_alpha = std::min(min_alpha, accepted_alpha);
+        }
         prev_rms = norms.rms_relative;
         std::swap(s.guess, s.trial);
         std::swap(s.map, s.trial_map);
@@ -955,6 +1019,10 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
                       iterations);
         return fail(c, UPIC_ERR_NONCONVERGED, buf);
     }
+    // the contraction sums of iterations 1.., read with the final evaluation
+    if (iterations > 1)
+        UPIC_CUDA(c, cudaMemcpyAsync(s.hcon, s.dcon, sizeof(double) * 4 * (size_t)iterations, cudaMemcpyDeviceToHost,
+                                     c->st));
     // final consistency evaluation (:6160) produces the accepted state
     Norms fin;
     if ((rc = eval_map(c, s, s.guess, s.map, true, &ms, nullptr, &fin))) return rc;
@@ -964,6 +1032,27 @@ int outer_solve(upic_ctx* c, ImplicitState& s, OuterResult& out) {
     out.iterations = iterations;
     out.anderson_steps = anderson_steps;
     out.picard_steps = picard_steps;
+    out.restarts = restarts;
+    out.backtracked = backtracked;
+    out.min_alpha = min_alpha;
+    out.method = method;
+    out.contraction = INFINITY;
+    for (int it = 1; it < iterations; ++it) {
+        const double dx2 = s.hcon[4 * it], dg2 = s.hcon[4 * it + 2];
+        const double dx_rms = std::sqrt(dx2 / (double)n3);
+        if (dx_rms > 64.0 * DBL_EPSILON) out.contraction = std::sqrt(dg2 / (double)n3) / dx_rms;
+    }
+    // observed_nonlinear_convergence_rate (:5534): one history entry per
+    // outer iteration, the first holding the first relative rms residual
+    out.observed_rate = INFINITY;
+    if (iterations >= 2 && first_rms > 0.0 && fin.rms_relative >= 0.0 && std::isfinite(fin.rms_relative)) {
+        if (fin.rms_relative == 0.0) {
+            out.observed_rate = 0.0;
+        } else {
+            const double ratio = fin.rms_relative / first_rms;
+            if (ratio > 0.0 && std::isfinite(ratio)) out.observed_rate = std::pow(ratio, 1.0 / (double)(iterations - 1));
+        }
+    }
     out.fin = fin;
     out.ms = ms;
     return 0;
@@ -1112,10 +1201,11 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
     if ((rc = form_guess(c, s))) return rc;
     OuterResult r;
     rc = outer_solve(c, s, r);
-    int restarts = 0;
+    int restarts = 0, direct_iterations = 0;
     bool fallback_used = false;
     if (rc == UPIC_ERR_LOCAL_PARTICLE && cf.selective_particle_fallback && s.np > 0) {
         fallback_used = true;
+        direct_iterations = r.iterations;
         const std::string direct = c->err;
         s.h_nsub.assign(s.np, 1);
         if ((rc = upload_layout(c, s))) return rc;
@@ -1196,6 +1286,31 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
         info[UPIC_INFO_SELECTIVE_RESTARTS] = restarts;
         info[UPIC_INFO_SELECTIVE_REFINED] = s.nref;
         info[UPIC_INFO_SELECTIVE_SUBSTEPS] = (double)s.total_substeps;
+        info[UPIC_INFO_ANDERSON_RESTARTS] = r.restarts;
+        info[UPIC_INFO_FINAL_ABS_RMS_RESIDUAL] = fin.rms_absolute;
+        info[UPIC_INFO_OBSERVED_RATE] = r.observed_rate;
+        info[UPIC_INFO_MAP_CONTRACTION] = r.contraction;
+        info[UPIC_INFO_BACKTRACKED_STEPS] = r.backtracked;
+        info[UPIC_INFO_MIN_UPDATE_ALPHA] = r.min_alpha;
+        info[UPIC_INFO_CONVERGENCE_METHOD] =
+            r.method + (fallback_used ? UPIC_METHOD_FORM_SELECTIVE : UPIC_METHOD_FORM_DIRECT);
+        info[UPIC_INFO_DIRECT_ATTEMPT_ITERATIONS] = fallback_used ? direct_iterations : 0;
+        // the particle layout: 1 substep each unless the fallback refined it
+        long counts[7] = {0, 0, 0, 0, 0, 0, 0};
+        int max_sub = 1;
+        if (fallback_used) {
+            for (int n : s.h_nsub) {
+                int level = 0;
+                for (int v = n; v > 1; v /= 2) ++level;
+                ++counts[std::min(level, 6)];
+                max_sub = std::max(max_sub, n);
+            }
+        } else {
+            counts[0] = s.np;
+        }
+        info[UPIC_INFO_SUBSTEPS_USED] = s.np > 0 ? max_sub : 0;
+        info[UPIC_INFO_SELECTIVE_WORK_RATIO] = s.np > 0 ? (double)s.total_substeps / (double)s.np : 0.0;
+        for (int k = 0; k < 7; ++k) info[UPIC_INFO_SELECTIVE_N1 + k] = (double)counts[k];
     }
     if ((rc = predictor_update(c, s, info))) return rc;
     ++s.steps;
@@ -1244,6 +1359,7 @@ int implicit_create(upic_ctx* c) {
     // window guard: the orbit reaches kappa*dt from its start; sorting every
     // step leaves no drift on top of that
     const double reach = cf.kappa * cf.dt / std::min(s->dx, s->dy);
+    s->dt_max = cf.dt;
     const int guard = cf.guard >= 0 ? cf.guard : (s->picard ? 2 : (int)std::ceil(reach) + 1);
     const int tile = cf.tile > 0 ? cf.tile : 8;
     s->tg = make_tiles(c->nx, c->ny, tile, guard, s->order / 2, s->order / 2 + 1);
@@ -1311,8 +1427,10 @@ int implicit_create(upic_ctx* c) {
         cudaMallocHost(&s->hdots, sizeof(double) * 32) != cudaSuccess ||
         cudaMallocHost(&s->hflag, sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&s->hnorm3, sizeof(NormSums) * 3) != cudaSuccess ||
-        cudaMallocHost(&s->hloss, sizeof(double)) != cudaSuccess)
+        cudaMallocHost(&s->hloss, sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&s->hcon, sizeof(double) * 4 * (size_t)std::max(1, c->cfg.nonlinear_max_iter)) != cudaSuccess)
         return fail(c, UPIC_ERR_NOMEM, "cudaMallocHost failed");
+    if ((rc = dalloc(c, &s->dcon, 4 * (size_t)std::max(1, c->cfg.nonlinear_max_iter)))) return rc;
     std::vector<unsigned char> ex(N, 0);
     for (int i = 0; i < c->nx; ++i)
         for (int j = 0; j < c->ny; ++j)
@@ -1331,6 +1449,7 @@ void implicit_destroy(upic_ctx* c) {
     if (s->hflag) cudaFreeHost(s->hflag);
     if (s->hnorm3) cudaFreeHost(s->hnorm3);
     if (s->hloss) cudaFreeHost(s->hloss);
+    if (s->hcon) cudaFreeHost(s->hcon);
     gnet::net_destroy(s->net);
     delete s;
     c->imp = nullptr;
@@ -1950,8 +2069,10 @@ extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double*
     if (!s.ready) return fail(c, UPIC_ERR_STATE, "upic_init_fields first");
     if (nsteps < 0) return fail(c, UPIC_ERR_ARGUMENT, "nsteps < 0");
     double row[UPIC_P3_DIAG_COUNT];
+    s.maplog.clear();
     for (int k = 0; k < nsteps; ++k) {
         int rc;
+        s.log_step = k;
         if (step_diag && !s.energy_valid) {
             if ((rc = state_diagnostics(c, s, row))) return rc;
             s.energy_W = row[UPIC_P3_FIELD_ENERGY];
@@ -1975,6 +2096,87 @@ extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double*
                                                 step_diag + (size_t)k * UPIC_SD_COUNT)))
             return rc;
     }
+    return UPIC_OK;
+}
+
+extern "C" const char* upic_convergence_method_name(int code) {
+    static const char* const bases[7] = {"none",
+                                         "picard",
+                                         "picard_fallback",
+                                         "current_anderson",
+                                         "current_anderson_backtracked",
+                                         "current_picard",
+                                         "current_picard_backtracked"};
+    static const char* const forms[3] = {"", "nested_full_dt_", "selective_"};
+    static char names[3][7][48];
+    static bool built = false;
+    if (!built) {
+        for (int f = 0; f < 3; ++f)
+            for (int b = 0; b < 7; ++b) std::snprintf(names[f][b], sizeof(names[f][b]), "%s%s", forms[f], bases[b]);
+        built = true;
+    }
+    const int base = code & 7, form = code >> 3;
+    if (code < 0 || base > 6 || form > 2) return nullptr;
+    return names[form][base];
+}
+
+extern "C" int upic_map_log(upic_ctx* c, int capacity, double* rows, int* nrows) {
+    if (!c || !nrows || capacity < 0 || (capacity > 0 && !rows)) return c ? fail(c, UPIC_ERR_ARGUMENT, "upic_map_log: bad arguments") : UPIC_ERR_ARGUMENT;
+    if (!c->imp) return fail(c, UPIC_ERR_STATE, "context was not created with an implicit method");
+    const ImplicitState& s = *c->imp;
+    const int n = (int)(s.maplog.size() / UPIC_MAPLOG_COUNT);
+    *nrows = n;
+    const int k = std::min(n, capacity);
+    if (k > 0) std::memcpy(rows, s.maplog.data(), sizeof(double) * UPIC_MAPLOG_COUNT * (size_t)k);
+    return UPIC_OK;
+}
+
+extern "C" int upic_probe_fields(upic_ctx* c, long np, const double* x, const double* y, double* out) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (!c->imp || c->imp->picard)
+        return fail(c, UPIC_ERR_STATE, "upic_probe_fields needs a UPIC_METHOD_CN_ORBIT context");
+    ImplicitState& s = *c->imp;
+    if (!s.ready) return fail(c, UPIC_ERR_STATE, "upic_init_fields first");
+    if (np < 0 || (np > 0 && (!x || !y || !out))) return fail(c, UPIC_ERR_ARGUMENT, "upic_probe_fields: bad arguments");
+    if (np == 0) return UPIC_OK;
+    for (long p = 0; p < np; ++p)
+        if (!std::isfinite(x[p]) || !std::isfinite(y[p])) return fail(c, UPIC_ERR_NONFINITE, "non-finite probe position");
+    const int N = c->N;
+    int rc;
+    if (!s.probe_grid && (rc = dalloc(c, &s.probe_grid, 18 * (size_t)N))) return rc;
+    if (np > s.pcap) {
+        if ((rc = sync(c))) return rc;
+        dfree(c, s.px);
+        dfree(c, s.py);
+        dfree(c, s.pout);
+        s.px = s.py = s.pout = nullptr;
+        s.pcap = 0;
+        if ((rc = dalloc(c, &s.px, (size_t)np)) || (rc = dalloc(c, &s.py, (size_t)np)) ||
+            (rc = dalloc(c, &s.pout, (size_t)np * UPIC_PROBE_COUNT)))
+            return rc;
+        s.pcap = np;
+    }
+    // phi, psi, rho, A, U from the state spectra; J; E, B from diag_spectra
+    UPIC_CUDA(c, cudaMemcpyAsync(s.dspec, s.spec, sizeof(double2) * 9 * N, cudaMemcpyDeviceToDevice, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 9, 1, c->st, nullptr, 1, s.probe_grid));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.probe_grid + 9 * (size_t)N, s.J, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice,
+                                 c->st));
+    UPIC_CUDA(c, launch_diag_spectra(N, c->d_kx, c->d_ky, s.spec, s.dspec, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, s.dspec, 6, 1, c->st, nullptr, 1, s.probe_grid + 12 * (size_t)N));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.px, x, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(s.py, y, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, launch_probe(s.order, c->nx, c->ny, c->cfg.Lx, c->cfg.Ly, s.probe_grid, np, s.px, s.py, s.pout,
+                              c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(out, s.pout, sizeof(double) * UPIC_PROBE_COUNT * np, cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+
+extern "C" int upic_set_time_step(upic_ctx* c, double dt) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (!c->imp) return fail(c, UPIC_ERR_STATE, "upic_set_time_step needs an implicit method");
+    if (!std::isfinite(dt) || !(dt > 0.0) || dt > c->imp->dt_max)
+        return fail(c, UPIC_ERR_ARGUMENT, "upic_set_time_step: dt must satisfy 0 < dt <= the dt of upic_create");
+    c->cfg.dt = dt;
     return UPIC_OK;
 }
 

@@ -1295,6 +1295,50 @@ __global__ void gather3_kernel(int nx, int ny, double Lx, double Ly, const doubl
     }
 }
 
+// Point probes (evaluate_reconstructed_field_probe :7924): F holds 18
+// planar fields phi, psi, rho, A, U, J, E, B; per point the 18 shape
+// gathers, grad(S phi) and grad(S A) (row c: dA_c/dx, dA_c/dy, 0), 30
+// values in the UPIC_PROBE_* order.
+template <int ORDER>
+__global__ void probe_kernel(int nx, int ny, double Lx, double Ly, const double* __restrict__ F, long np,
+                             const double* x, const double* y, double* out) {
+    const Geo g{nx, ny, Lx, Ly, nx / Lx, ny / Ly};
+    const int N = nx * ny;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
+        Stencil<ORDER> sx, sy;
+        stencil_xy<ORDER>(g, x[p], y[p], sx, sy);
+        double v[18], gp[2] = {0.0, 0.0}, gA[3][2] = {};
+        for (int f = 0; f < 18; ++f) v[f] = 0.0;
+        for (int ia = 0; ia <= ORDER; ++ia) {
+            const int gx = wrap_index(sx.il + ia, nx);
+            for (int ib = 0; ib <= ORDER; ++ib) {
+                const int node = gx * ny + wrap_index(sy.il + ib, ny);
+                const double w = sx.w[ia] * sy.w[ib];
+                const double wx = sx.dw[ia] * sy.w[ib], wy = sx.w[ia] * sy.dw[ib];
+                for (int f = 0; f < 18; ++f) v[f] = fma(F[(size_t)f * N + node], w, v[f]);
+                const double ph = F[node];
+                gp[0] = fma(ph, wx, gp[0]);
+                gp[1] = fma(ph, wy, gp[1]);
+                for (int c = 0; c < 3; ++c) {
+                    const double a = F[(size_t)(3 + c) * N + node];
+                    gA[c][0] = fma(a, wx, gA[c][0]);
+                    gA[c][1] = fma(a, wy, gA[c][1]);
+                }
+            }
+        }
+        double* o = out + (size_t)p * 30;
+        for (int f = 0; f < 18; ++f) o[f] = v[f];
+        o[18] = gp[0];
+        o[19] = gp[1];
+        o[20] = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            o[21 + 3 * c] = gA[c][0];
+            o[22 + 3 * c] = gA[c][1];
+            o[23 + 3 * c] = 0.0;
+        }
+    }
+}
+
 template <int ORDER>
 __global__ void add_qA_kernel(int nx, int ny, double Lx, double Ly, const double* A3, long np, const double* x,
                               const double* y, const double* q, double q0, double* Px, double* Py, double* Pz) {
@@ -2520,6 +2564,20 @@ cudaError_t launch_gather3(int order, int nx, int ny, double Lx, double Ly, cons
         case 2: gather3_kernel<2><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, f3, np, x, y, out3); break;
         case 3: gather3_kernel<3><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, f3, np, x, y, out3); break;
         case 4: gather3_kernel<4><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, f3, np, x, y, out3); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_probe(int order, int nx, int ny, double Lx, double Ly, const double* F18, long np,
+                         const double* x, const double* y, double* out30, cudaStream_t st) {
+    const int g = gsize(np, 128);
+    switch (order) {
+        case 1: probe_kernel<1><<<g, 128, 0, st>>>(nx, ny, Lx, Ly, F18, np, x, y, out30); break;
+        case 2: probe_kernel<2><<<g, 128, 0, st>>>(nx, ny, Lx, Ly, F18, np, x, y, out30); break;
+        case 3: probe_kernel<3><<<g, 128, 0, st>>>(nx, ny, Lx, Ly, F18, np, x, y, out30); break;
+        case 4: probe_kernel<4><<<g, 128, 0, st>>>(nx, ny, Lx, Ly, F18, np, x, y, out30); break;
         default: return cudaErrorInvalidValue;
     }
     count_launches(1);

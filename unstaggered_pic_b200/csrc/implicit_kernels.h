@@ -189,6 +189,12 @@ cudaError_t launch_gather3(int order, int nx, int ny, double Lx, double Ly, cons
                            long np, const double* x, const double* y, double* out3,
                            cudaStream_t st);
 
+// Point probes of 18 planar fields (phi, psi, rho, A, U, J, E, B): their
+// shape gathers, grad(S phi) and grad(S A), 30 values per point
+// (evaluate_reconstructed_field_probe :7924).
+cudaError_t launch_probe(int order, int nx, int ny, double Lx, double Ly, const double* F18, long np,
+                         const double* x, const double* y, double* out30, cudaStream_t st);
+
 // P += q A(x) with A a planar 3-vector field (the canonical momentum of a
 // start state with a non-zero A, :4113-4117); q per particle or q0.
 cudaError_t launch_add_qA(int order, int nx, int ny, double Lx, double Ly, const double* A3, long np,

@@ -4,6 +4,8 @@
 //   two-stream: initialize_two_stream_3d_linear_x
 //               (Project3/ec_pic_nyquist_projected.cpp:3689)
 //   Weibel:     initialize_weibel_filamentation_3d (:3961)
+//   Landau:     initialize_landau_damping_1d3d (:3853), the retained
+//               electrostatic teaching example
 //
 // Both put two cold counter-streaming electron populations (+-v0 along x) on
 // the same quiet-start positions -- cell-centred lines, particles_per_cell_pair
@@ -19,6 +21,7 @@
 // the arrays are the reference's bit for bit.
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "../../include/upic.h"
 
@@ -89,7 +92,8 @@ double weibel_rate(const upic_p3_case& c) {
 }
 
 bool valid(const upic_p3_case* c) {
-    return c && (c->kind == UPIC_P3_TWO_STREAM || c->kind == UPIC_P3_WEIBEL) && c->nx > 0 && c->ny > 0 &&
+    return c && (c->kind == UPIC_P3_TWO_STREAM || c->kind == UPIC_P3_WEIBEL || c->kind == UPIC_P3_LANDAU) &&
+           c->nx > 0 && c->ny > 0 &&
            c->Lx > 0.0 && c->Ly > 0.0 && c->Lz > 0.0 && c->kappa > 0.0 && c->spline_order >= 1 &&
            c->spline_order <= 4;
 }
@@ -242,6 +246,70 @@ int weibel(const upic_p3_case& c, double* x, double* y, double* v, double* q, do
     return UPIC_OK;
 }
 
+// Acklam's rational approximation of the inverse standard normal CDF (P. J.
+// Acklam, "An algorithm for computing the inverse normal cumulative
+// distribution function", 2003): a central rational function for
+// 0.02425 <= p <= 0.97575 and a tail form in sqrt(-2 log p) outside, the
+// quiet-start sampler of normal_quantile (:3623); 0 < p < 1.
+double acklam_quantile(double p) {
+    static const double a[6] = {-3.969683028665376e+01, 2.209460984245205e+02, -2.759285104469687e+02,
+                                1.383577518672690e+02, -3.066479806614716e+01, 2.506628277459239e+00};
+    static const double b[5] = {-5.447609879822406e+01, 1.615858368580409e+02, -1.556989798598866e+02,
+                                6.680131188771972e+01, -1.328068155288572e+01};
+    static const double c[6] = {-7.784894002430293e-03, -3.223964580411365e-01, -2.400758277161838e+00,
+                                -2.549732539343734e+00, 4.374664141464968e+00, 2.938163982698783e+00};
+    static const double d[4] = {7.784695709041462e-03, 3.224671290700398e-01, 2.445134137142996e+00,
+                                3.754408661907416e+00};
+    const double lo = 0.02425, hi = 1.0 - lo;
+    if (p < lo || p > hi) {
+        const double t = std::sqrt(-2.0 * std::log(p < lo ? p : 1.0 - p));
+        const double v = (((((c[0] * t + c[1]) * t + c[2]) * t + c[3]) * t + c[4]) * t + c[5]) /
+                         ((((d[0] * t + d[1]) * t + d[2]) * t + d[3]) * t + 1.0);
+        return p < lo ? v : -v;
+    }
+    const double q = p - 0.5, r = q * q;
+    return (((((a[0] * r + a[1]) * r + a[2]) * r + a[3]) * r + a[4]) * r + a[5]) * q /
+           (((((b[0] * r + b[1]) * r + b[2]) * r + b[3]) * r + b[4]) * r + 1.0);
+}
+
+double landau_alpha(const upic_p3_case& c) { return c.landau_alpha >= 0.0 ? c.landau_alpha : c.perturbation; }
+
+// initialize_landau_damping_1d3d (:3853) on the 2D grid: rows y outer, x
+// inner, nv velocities per cell centre; q = q0 (1 + alpha cos(k x)), m = |q|.
+int landau(const upic_p3_case& c, double* x, double* y, double* v, double* q, double* m, double* A, double* U,
+           double* rate) {
+    const int nv = c.particles_per_cell_pair;
+    const double alpha = landau_alpha(c);
+    if (nv < 2 || !(std::abs(alpha) < 1.0)) return UPIC_ERR_CONFIG;
+    std::vector<double> vq(nv);
+    for (int j = 0; j < nv; ++j) vq[j] = c.thermal_velocity * acklam_quantile((j + 0.5) / (double)nv);
+    const long np = (long)c.nx * c.ny * nv;
+    const double kx = 2.0 * kPi * static_cast<double>(c.perturbation_mode) / c.Lx;
+    const double q0 = -c.n0 * (c.Lx * c.Ly * c.Lz) / static_cast<double>(np);
+    long p = 0;
+    for (int j = 0; j < c.ny; ++j) {
+        const double yc = cell_center(j, c.ny, c.Ly);
+        for (int i = 0; i < c.nx; ++i) {
+            const double xc = cell_center(i, c.nx, c.Lx);
+            const double w = 1.0 + alpha * std::cos(kx * xc);
+            for (int jv = 0; jv < nv; ++jv, ++p) {
+                x[p] = wrap_centered(xc, c.Lx);
+                y[p] = wrap_centered(yc, c.Ly);
+                v[3 * p] = vq[jv];
+                v[3 * p + 1] = 0.0;
+                v[3 * p + 2] = 0.0;
+                q[p] = q0 * w;
+                m[p] = std::abs(q[p]);
+            }
+        }
+    }
+    const long N = (long)c.nx * c.ny;
+    std::fill(A, A + 3 * N, 0.0);
+    std::fill(U, U + 3 * N, 0.0);
+    if (rate) *rate = 0.0;
+    return UPIC_OK;
+}
+
 }  // namespace
 
 extern "C" int upic_p3_case_default(upic_p3_case* c) {
@@ -266,6 +334,8 @@ extern "C" int upic_p3_case_default(upic_p3_case* c) {
     c->weibel_B0 = -1.0;
     c->weibel_eigenmode = 1;
     c->weibel_finite_grid_theory = 1;
+    c->landau_alpha = -1.0;
+    c->thermal_velocity = 1.0;
     return UPIC_OK;
 }
 
@@ -273,6 +343,7 @@ extern "C" long upic_p3_case_particles(const upic_p3_case* c) {
     if (!valid(c)) return -1;
     const int per = c->kind == UPIC_P3_WEIBEL ? std::max(1, c->particles_per_cell_pair) : c->particles_per_cell_pair;
     if (per <= 0) return -1;
+    if (c->kind == UPIC_P3_LANDAU) return (long)c->nx * c->ny * per;
     return 2L * c->nx * per * c->ny;
 }
 
@@ -281,6 +352,7 @@ extern "C" int upic_p3_initial_state(const upic_p3_case* c, long capacity, doubl
     const long np = upic_p3_case_particles(c);
     if (np < 0) return UPIC_ERR_CONFIG;
     if (capacity < np || (np > 0 && (!x || !y || !v || !q || !m)) || !A || !U) return UPIC_ERR_ARGUMENT;
+    if (c->kind == UPIC_P3_LANDAU) return landau(*c, x, y, v, q, m, A, U, growth_rate);
     return c->kind == UPIC_P3_WEIBEL ? weibel(*c, x, y, v, q, m, A, U, growth_rate)
                                      : two_stream(*c, x, y, v, q, m, A, U, growth_rate);
 }

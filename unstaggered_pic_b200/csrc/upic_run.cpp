@@ -7,6 +7,7 @@
 //
 //     upic_run deck.txt              Project2 decks (spectral_pic_part3)
 //     upic_run --nonrel deck.txt     Project1 decks (ec_pic_serial_demo), run_nonrel.cpp
+//     upic_run --p3 deck.txt         Project3 decks (ec_pic_nyquist_projected), run_p3.cpp
 //
 // Exit codes as the reference: 0 ok, 1 error (message on stderr), 2 usage,
 // 3 failed start-up unit tests (Project1 decks).
@@ -368,15 +369,18 @@ void run(const Deck& d) {
 }  // namespace
 
 int run_nonrel(const std::string& path);
+int run_p3(const std::string& path);
 
 int main(int argc, char** argv) {
     try {
         const bool nonrel = argc == 3 && std::string(argv[1]) == "--nonrel";
-        if (argc != 2 && !nonrel) {
-            std::cerr << "usage: " << argv[0] << " [--nonrel] input_file.txt\n";
+        const bool p3 = argc == 3 && std::string(argv[1]) == "--p3";
+        if ((argc != 2 && !nonrel && !p3) || (argc == 2 && std::string(argv[1]).rfind("--", 0) == 0)) {
+            std::cerr << "usage: " << argv[0] << " [--nonrel | --p3] input_file.txt\n";
             return 2;
         }
         if (nonrel) return run_nonrel(argv[2]);
+        if (p3) return run_p3(argv[2]);
         run(read_deck(argv[1]));
         return 0;
     } catch (const std::exception& ex) {
