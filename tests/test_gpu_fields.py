@@ -128,3 +128,60 @@ def test_snapshot_rejects_explicit_method(tmp_path):
         sim.init_fields(False)
         with pytest.raises(up.UpicError):
             sim.write_field_snapshot(tmp_path / "x.csv", 0, 0.0)
+
+
+def bspline(r, x):
+    """Centred cardinal B-spline of degree r and its derivative (the
+    truncated-power form of the r+1-fold box convolution)."""
+    from math import comb, factorial
+
+    def B(deg, t):
+        if deg == 0:
+            return ((t >= -0.5) & (t < 0.5)).astype(np.float64)
+        s = np.zeros_like(t)
+        for k in range(deg + 2):
+            s += (-1) ** k * comb(deg + 1, k) * np.maximum(t + (deg + 1) / 2 - k, 0.0) ** deg
+        return s / factorial(deg)
+
+    return B(r, x), B(r - 1, x + 0.5) - B(r - 1, x - 0.5)
+
+
+def test_probe_fields_match_numpy():
+    """upic_probe_fields (the shape gathers and shape gradients behind
+    Project3's field line probes, evaluate_reconstructed_field_probe
+    :7924) against the same sums in numpy over the run's own fields, at
+    points inside and outside the box."""
+    g = gold("p3_run_o2_anderson.npz")
+    sim, cfg = load_sim(g)
+    sim.init_fields(True)
+    sim.step_implicit(2)
+    order = cfg.spline_order
+    nx, ny, Lx, Ly = cfg.nx, cfg.ny, cfg.Lx, cfg.Ly
+    dx, dy = Lx / nx, Ly / ny
+    names = ["phi", "psi", "rho", "Ax", "Ay", "Az", "Ux", "Uy", "Uz", "Jx", "Jy", "Jz", "Ex", "Ey", "Ez", "Bx", "By",
+             "Bz"]
+    F = np.stack([sim.field(n) for n in names])
+    rng = np.random.default_rng(5)
+    x = rng.uniform(-0.75 * Lx, 0.75 * Lx, 40)
+    y = rng.uniform(-0.75 * Ly, 0.75 * Ly, 40)
+    out = sim.probe_fields(x, y)
+    assert out.shape == (40, len(up.PROBE_COLUMNS))
+    want = np.zeros_like(out)
+    for p in range(40):
+        u, v = (x[p] + 0.5 * Lx) / dx, (y[p] + 0.5 * Ly) / dy
+        il, jl = int(np.floor(u - 0.5 * (order - 1))), int(np.floor(v - 0.5 * (order - 1)))
+        for a in range(order + 1):
+            wx, dwx = bspline(order, np.array([u - (il + a)]))
+            for b in range(order + 1):
+                wy, dwy = bspline(order, np.array([v - (jl + b)]))
+                node = F[:, (il + a) % nx, (jl + b) % ny]
+                want[p, :18] += node * wx[0] * wy[0]
+                want[p, 18] += node[0] * dwx[0] / dx * wy[0]
+                want[p, 19] += node[0] * wx[0] * dwy[0] / dy
+                for c in range(3):
+                    want[p, 21 + 3 * c] += node[3 + c] * dwx[0] / dx * wy[0]
+                    want[p, 22 + 3 * c] += node[3 + c] * wx[0] * dwy[0] / dy
+    for k, name in enumerate(up.PROBE_COLUMNS):
+        scale = max(np.max(np.abs(want[:, k])), 1e-30)
+        assert np.max(np.abs(out[:, k] - want[:, k])) <= 1e-12 * scale + 1e-300, name
+    assert np.all(out[:, [20, 23, 26, 29]] == 0.0)

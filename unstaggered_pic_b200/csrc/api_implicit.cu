@@ -330,7 +330,7 @@ void norms_from_sums(upic_ctx* c, ImplicitState& s, Norms& n);
 void log_map_evaluation(ImplicitState& s, const MapStats& m) {
     double worst;
     std::memcpy(&worst, &m.worst_scaled_bits, sizeof(double));
-    if (!std::isfinite(worst)) worst = INFINITY;
+    if (!std::isfinite(worst) || worst >= 1.0e300) worst = INFINITY;  // the kernels record non-finite as 1e300
     const bool ok = m.failures == 0;
     const double mean = s.total_substeps > 0 ? (double)m.iter_total / (double)s.total_substeps : 0.0;
     const double row[UPIC_MAPLOG_COUNT] = {(double)s.log_step, (double)++s.map_eval, ok ? 1.0 : 0.0,
