@@ -58,15 +58,27 @@ def test_instability_start_and_steps_match_reference(case, keys, run):
     for f, k in (("Ax", 0), ("Ay", 1), ("Az", 2)):
         assert np.max(np.abs(sim.field(f) - ref0["A"][k])) <= 1e-15 * max(1.0, np.max(np.abs(ref0["A"]))), f
     assert np.max(np.abs(sim.field("Ux") - ref0["U"][0])) <= 1e-15 * max(1.0, np.max(np.abs(ref0["U"])))
-    for c in ("field_energy", "kinetic_energy", "total_energy", "Bz_y_mode_abs", "E_mode_abs"):
+    # start diagnostics to rounding: the field energy of a 1e-3 perturbation
+    # carries the cancellation of rho = n0 + deposited charge (5e-12); the
+    # mode a case does not seed is rounding noise, held to 1e-13 of the seeded one
+    modes = [up.IMPLICIT_DIAG_COLUMNS.index(c) for c in ("Bz_y_mode_abs", "E_mode_abs")]
+    seeded = max(abs(ref["diag"][0, k]) for k in modes)
+    for c, tol in (("field_energy", 5e-12), ("kinetic_energy", 1e-13), ("total_energy", 1e-13),
+                   ("Bz_y_mode_abs", 1e-12), ("E_mode_abs", 1e-12)):
         k = up.IMPLICIT_DIAG_COLUMNS.index(c)
-        assert abs(d0[k] - ref["diag"][0, k]) <= 1e-13 * max(abs(ref["diag"][0, k]), 1e-30), c
+        assert abs(d0[k] - ref["diag"][0, k]) <= tol * abs(ref["diag"][0, k]) + 1e-13 * seeded, c
     # steps
     diag, info = sim.step_implicit(prob.n_steps)
     assert np.max(np.abs(info[:, 0] - ref["info"][:, 0])) <= 1
-    for c in ("field_energy", "kinetic_energy", "total_energy", "Bz_y_mode_abs", "E_mode_abs"):
+    for c in ("field_energy", "kinetic_energy", "total_energy"):
         k = up.IMPLICIT_DIAG_COLUMNS.index(c)
         assert relerr(diag[:, k], ref["diag"][1:, k]) < TOL_STEP * prob.n_steps, c
+    # the seeded mode to the step tolerance, the other one as rounding noise
+    # on the scale of the seeded one
+    ks, ko = [up.IMPLICIT_DIAG_COLUMNS.index(c) for c in
+              (("Bz_y_mode_abs", "E_mode_abs") if case == "weibel" else ("E_mode_abs", "Bz_y_mode_abs"))]
+    assert relerr(diag[:, ks], ref["diag"][1:, ks]) < TOL_STEP * prob.n_steps
+    assert np.max(np.abs(diag[:, ko] - ref["diag"][1:, ko])) <= TOL_STEP * prob.n_steps * np.max(ref["diag"][:, ks])
     names = ["phi", "psi", "rho", "Ax", "Ay", "Az", "Ux", "Uy", "Uz", "Jx", "Jy", "Jz"]
     for k, n in enumerate(names):
         scale = max(np.max(np.abs(ref["fields"][j])) for j in ((k // 3) * 3 + np.arange(3) if k >= 3 else [k]))

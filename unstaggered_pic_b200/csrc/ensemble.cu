@@ -166,15 +166,23 @@ extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double*
 namespace {
 
 // Implicit runs: a pool of host threads, each taking the next run and
-// advancing it by nsteps with upic_step_implicit.
+// advancing it by nsteps with upic_step_implicit.  Runs are handed out
+// largest first (longest-processing-time order), so that the last runs to
+// start are the short ones and the threads finish together; each run's
+// result does not depend on the order.
 int step_threads(upic_ensemble* e, int nsteps) {
     const int n = (int)e->runs.size();
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
     const int T = std::max(1, std::min({n, hw, 64}));
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return e->runs[a]->np > e->runs[b]->np; });
     std::atomic<int> next{0};
     std::vector<int> rc(n, 0);
     auto work = [&]() {
-        for (int i = next++; i < n; i = next++) {
+        for (int k = next++; k < n; k = next++) {
+            const int i = order[k];
             upic_ctx* c = e->runs[i];
             if (cudaSetDevice(c->device) != cudaSuccess) {
                 rc[i] = UPIC_ERR_CUDA;
