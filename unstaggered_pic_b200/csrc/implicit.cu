@@ -148,24 +148,36 @@ struct Geo {
     int nq = 0, mnq = 0;
 };
 
-template <int ORDER>
+// SY: nodes of the y stencil, ORDER + 1, or 1 on a grid one cell high
+// (ny = 1), where every y node wraps onto the same row: the weights of the
+// ORDER + 1 nodes then add to 1 and their derivatives to 0 (the partition
+// of unity), so the y stencil is that one row with weight 1 and
+// derivative 0.
+template <int ORDER, int SY = ORDER + 1>
 UPIC_D void stencil_xy(const Geo& g, double x, double y, Stencil<ORDER>& sx, Stencil<ORDER>& sy) {
     bspline<ORDER>((x + 0.5 * g.Lx) * g.inv_dx, g.inv_dx, sx);
-    bspline<ORDER>((y + 0.5 * g.Ly) * g.inv_dy, g.inv_dy, sy);
+    if constexpr (SY == 1) {
+        (void)y;
+        sy.il = 0;
+        sy.w[0] = 1.0;
+        sy.dw[0] = 0.0;
+    } else {
+        bspline<ORDER>((y + 0.5 * g.Ly) * g.inv_dy, g.inv_dy, sy);
+    }
 }
 
 // Sum of record component block [off, off+3) at a wrapped position.
-template <int ORDER, int STRIDE = kIRec>
+template <int ORDER, int STRIDE = kIRec, int SY = ORDER + 1>
 UPIC_D void gather_rec3(const Geo& g, const double* __restrict__ rec, int off, double x, double y,
                         double out[3]) {
     Stencil<ORDER> sx, sy;
-    stencil_xy<ORDER>(g, x, y, sx, sy);
+    stencil_xy<ORDER, SY>(g, x, y, sx, sy);
     out[0] = out[1] = out[2] = 0.0;
 #pragma unroll
     for (int a = 0; a <= ORDER; ++a) {
         const int gx = wrap_index(sx.il + a, g.nx);
 #pragma unroll
-        for (int b = 0; b <= ORDER; ++b) {
+        for (int b = 0; b < SY; ++b) {
             const double* r = rec + (size_t)(gx * g.ny + wrap_index(sy.il + b, g.ny)) * STRIDE + off;
             const double w = sx.w[a] * sy.w[b];
             out[0] = fma(__ldg(r), w, out[0]);
@@ -330,7 +342,7 @@ UPIC_D void kick_rotate_kick(const LocalIn& in, const double* guess, double gp0,
 // with A = (1-s) A^n + s A^{n+1} (path_average_gather_vector_one :2738,
 // orbit_discrete_gradient_A_interval :2958), the deck's Gauss rule point by
 // point.
-template <int ORDER>
+template <int ORDER, int SY = ORDER + 1>
 UPIC_D void orbit_integrals_points(const Geo& g, const double* __restrict__ rec, double x0, double y0, double dxx,
                                    double dxy, const double* b, int nb, double gp[2], double D[3][2],
                                    double th0 = 0.0, double th1 = 1.0) {
@@ -347,7 +359,7 @@ UPIC_D void orbit_integrals_points(const Geo& g, const double* __restrict__ rec,
             const double xs = wrap1(x0 + s * dxx, g.Lx);
             const double ys = wrap1(y0 + s * dxy, g.Ly);
             Stencil<ORDER> sx, sy;
-            stencil_xy<ORDER>(g, xs, ys, sx, sy);
+            stencil_xy<ORDER, SY>(g, xs, ys, sx, sy);
             double g0 = 0.0, g1 = 0.0;
             double d[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
             // A at the orbit's time: (1 - th) A^n + th A^{n+1} with th running
@@ -358,7 +370,7 @@ UPIC_D void orbit_integrals_points(const Geo& g, const double* __restrict__ rec,
             for (int a = 0; a <= ORDER; ++a) {
                 const int gx = wrap_index(sx.il + a, g.nx);
 #pragma unroll
-                for (int bb = 0; bb <= ORDER; ++bb) {
+                for (int bb = 0; bb < SY; ++bb) {
                     const double* r = rec + (size_t)(gx * g.ny + wrap_index(sy.il + bb, g.ny)) * kIRec;
                     const double2 r01 = __ldg(reinterpret_cast<const double2*>(r));
                     const double2 r23 = __ldg(reinterpret_cast<const double2*>(r + 2));
@@ -366,14 +378,13 @@ UPIC_D void orbit_integrals_points(const Geo& g, const double* __restrict__ rec,
                     const double2 r67 = __ldg(reinterpret_cast<const double2*>(r + 6));
                     const double sh = sx.w[a] * sy.w[bb];
                     const double dsx = sx.dw[a] * sy.w[bb];
-                    const double dsy = sx.w[a] * sy.dw[bb];
                     g0 = fma(r01.x, sh, g0);
                     g1 = fma(r01.y, sh, g1);
                     const double av[3] = {s1 * r23.x + th * r45.y, s1 * r23.y + th * r67.x, s1 * r45.x + th * r67.y};
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         d[c][0] = fma(av[c], dsx, d[c][0]);
-                        d[c][1] = fma(av[c], dsy, d[c][1]);
+                        if constexpr (SY > 1) d[c][1] = fma(av[c], sx.w[a] * sy.dw[bb], d[c][1]);
                     }
                 }
             }
@@ -392,18 +403,18 @@ UPIC_D void orbit_integrals_points(const Geo& g, const double* __restrict__ rec,
 
 // One evaluation of the particle map at guess vbar (evaluate_local_particle_substep
 // :4843 with h = dt, theta0 = 0, theta1 = 1).  b/nb: breakpoints of the orbit.
-template <int ORDER>
+template <int ORDER, int SY = ORDER + 1>
 UPIC_D bool evaluate(const Geo& g, const double* __restrict__ rec, double dt, double kappa, int split,
                      const LocalIn& in, const double* guess, LocalOut& o, double* b, int& nb) {
     const double dxx = dt * guess[0], dxy = dt * guess[1];
     o.x1 = wrap1(in.x0 + dxx, g.Lx);
     o.y1 = wrap1(in.y0 + dxy, g.Ly);
     double A1p[3];
-    gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, A1p);
+    gather_rec3<ORDER, kIRec, SY>(g, rec, kIRecAe, o.x1, o.y1, A1p);
     nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
     if (nb < 0) return false;
     double gpv[2], D[3][2];
-    orbit_integrals_points<ORDER>(g, rec, in.x0, in.y0, dxx, dxy, b, nb, gpv, D);
+    orbit_integrals_points<ORDER, SY>(g, rec, in.x0, in.y0, dxx, dxy, b, nb, gpv, D);
     kick_rotate_kick(in, guess, gpv[0], gpv[1], D, A1p, dt, o);
     return true;
 }
@@ -441,9 +452,9 @@ UPIC_D bool evaluate_sub(const Geo& g, const double* __restrict__ rec, double h,
 // The algebra is that of path_average_gather_vector_one (:2738) and
 // orbit_discrete_gradient_A_interval (:2958) with the node and quadrature
 // sums exchanged.
-template <int ORDER>
+template <int ORDER, int SY = ORDER + 1>
 struct SegMoments {
-    static constexpr int SS = (ORDER + 1) * (ORDER + 1);
+    static constexpr int SS = (ORDER + 1) * SY;
     int ilx, ily;
     double m[SS];               // sum wq Sx_a Sy_b
     double x0[SS], x1[SS];      // sum wq (1-s) dSx_a Sy_b, sum wq s dSx_a Sy_b
@@ -452,18 +463,18 @@ struct SegMoments {
 
 // Segment stencil origin and the weighted shape sums of one segment.  With
 // GRAD false only m is formed (the deposit needs no derivatives).
-template <int ORDER, bool GRAD>
+template <int ORDER, bool GRAD, int SY = ORDER + 1>
 UPIC_D void segment_moments(const Geo& g, double x0, double y0, double dxx, double dxy, double sa,
-                            double len, SegMoments<ORDER>& M) {
+                            double len, SegMoments<ORDER, SY>& M) {
     constexpr int S = ORDER + 1;
     const double off = 0.5 * (double)(ORDER - 1);
     const double ox = x0 + 0.5 * g.Lx, oy = y0 + 0.5 * g.Ly;
     const double sm = sa + 0.5 * len;
     M.ilx = (int)floor((ox + sm * dxx) * g.inv_dx - off);
-    M.ily = (int)floor((oy + sm * dxy) * g.inv_dy - off);
+    M.ily = SY == 1 ? 0 : (int)floor((oy + sm * dxy) * g.inv_dy - off);
     const double fx0 = (double)M.ilx, fy0 = (double)M.ily;
 #pragma unroll
-    for (int k = 0; k < S * S; ++k) {
+    for (int k = 0; k < S * SY; ++k) {
         M.m[k] = 0.0;
         if (GRAD) M.x0[k] = M.x1[k] = M.y0[k] = M.y1[k] = 0.0;
     }
@@ -473,21 +484,28 @@ UPIC_D void segment_moments(const Geo& g, double x0, double y0, double dxx, doub
         const double wq = len * g.mw[iq];
         double wx[S], dwx[S], wy[S], dwy[S];
         bspline_f<ORDER>((ox + s * dxx) * g.inv_dx - fx0, g.inv_dx, wx, dwx);
-        bspline_f<ORDER>((oy + s * dxy) * g.inv_dy - fy0, g.inv_dy, wy, dwy);
+        if constexpr (SY == 1) {
+            wy[0] = 1.0;
+            dwy[0] = 0.0;
+        } else {
+            bspline_f<ORDER>((oy + s * dxy) * g.inv_dy - fy0, g.inv_dy, wy, dwy);
+        }
         const double w1 = wq * s, w0 = wq * (1.0 - s);
 #pragma unroll
         for (int a = 0; a < S; ++a) {
             const double ta = wq * wx[a];
 #pragma unroll
-            for (int b = 0; b < S; ++b) M.m[a * S + b] = fma(ta, wy[b], M.m[a * S + b]);
+            for (int b = 0; b < SY; ++b) M.m[a * SY + b] = fma(ta, wy[b], M.m[a * SY + b]);
             if (GRAD) {
                 const double t0 = w0 * dwx[a], t1 = w1 * dwx[a], u0 = w0 * wx[a], u1 = w1 * wx[a];
 #pragma unroll
-                for (int b = 0; b < S; ++b) {
-                    M.x0[a * S + b] = fma(t0, wy[b], M.x0[a * S + b]);
-                    M.x1[a * S + b] = fma(t1, wy[b], M.x1[a * S + b]);
-                    M.y0[a * S + b] = fma(u0, dwy[b], M.y0[a * S + b]);
-                    M.y1[a * S + b] = fma(u1, dwy[b], M.y1[a * S + b]);
+                for (int b = 0; b < SY; ++b) {
+                    M.x0[a * SY + b] = fma(t0, wy[b], M.x0[a * SY + b]);
+                    M.x1[a * SY + b] = fma(t1, wy[b], M.x1[a * SY + b]);
+                    if constexpr (SY > 1) {  // one row: no y derivative, y0 = y1 = 0
+                        M.y0[a * SY + b] = fma(u0, dwy[b], M.y0[a * SY + b]);
+                        M.y1[a * SY + b] = fma(u1, dwy[b], M.y1[a * SY + b]);
+                    }
                 }
             }
         }
@@ -496,7 +514,7 @@ UPIC_D void segment_moments(const Geo& g, double x0, double y0, double dxx, doub
 
 // orbit_integrals_points through segment moments (ORDER <= 2, knot splitting
 // on, so that each segment has one stencil).
-template <int ORDER>
+template <int ORDER, int SY = ORDER + 1>
 UPIC_D void orbit_integrals_moments(const Geo& g, const double* __restrict__ rec, double x0, double y0, double dxx,
                                     double dxy, const double* b, int nb, double gp[2], double D[3][2]) {
     constexpr int S = ORDER + 1;
@@ -506,26 +524,26 @@ UPIC_D void orbit_integrals_moments(const Geo& g, const double* __restrict__ rec
     for (int k = 0; k + 1 < nb; ++k) {
         const double len = b[k + 1] - b[k];
         if (len <= 0.0) continue;
-        SegMoments<ORDER> M;
-        segment_moments<ORDER, true>(g, x0, y0, dxx, dxy, b[k], len, M);
+        SegMoments<ORDER, SY> M;
+        segment_moments<ORDER, true, SY>(g, x0, y0, dxx, dxy, b[k], len, M);
 #pragma unroll
         for (int a = 0; a < S; ++a) {
             const int gx = wrap_index(M.ilx + a, g.nx);
 #pragma unroll
-            for (int bb = 0; bb < S; ++bb) {
+            for (int bb = 0; bb < SY; ++bb) {
                 const double* r = rec + (size_t)(gx * g.ny + wrap_index(M.ily + bb, g.ny)) * kIRec;
                 const double2 r01 = __ldg(reinterpret_cast<const double2*>(r));
                 const double2 r23 = __ldg(reinterpret_cast<const double2*>(r + 2));
                 const double2 r45 = __ldg(reinterpret_cast<const double2*>(r + 4));
                 const double2 r67 = __ldg(reinterpret_cast<const double2*>(r + 6));
-                const int j = a * S + bb;
+                const int j = a * SY + bb;
                 gp0 = fma(r01.x, M.m[j], gp0);
                 gp1 = fma(r01.y, M.m[j], gp1);
                 const double An[3] = {r23.x, r23.y, r45.x}, Ae[3] = {r45.y, r67.x, r67.y};
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     D[c][0] = fma(An[c], M.x0[j], fma(Ae[c], M.x1[j], D[c][0]));
-                    D[c][1] = fma(An[c], M.y0[j], fma(Ae[c], M.y1[j], D[c][1]));
+                    if constexpr (SY > 1) D[c][1] = fma(An[c], M.y0[j], fma(Ae[c], M.y1[j], D[c][1]));
                 }
             }
         }
@@ -534,19 +552,20 @@ UPIC_D void orbit_integrals_moments(const Geo& g, const double* __restrict__ rec
     gp[1] = gp1;
 }
 
-// evaluate() for ORDER <= 2 with knot splitting on, through segment moments.
-template <int ORDER>
+// evaluate() with knot splitting on, through segment moments (ORDER <= 2,
+// or any order with a one-row y stencil, SY = 1).
+template <int ORDER, int SY = ORDER + 1>
 UPIC_D bool evaluate_moments(const Geo& g, const double* __restrict__ rec, double dt, double kappa, int split,
                              const LocalIn& in, const double* guess, LocalOut& o, double* b, int& nb) {
     const double dxx = dt * guess[0], dxy = dt * guess[1];
     o.x1 = wrap1(in.x0 + dxx, g.Lx);
     o.y1 = wrap1(in.y0 + dxy, g.Ly);
     double A1p[3];
-    gather_rec3<ORDER>(g, rec, kIRecAe, o.x1, o.y1, A1p);
+    gather_rec3<ORDER, kIRec, SY>(g, rec, kIRecAe, o.x1, o.y1, A1p);
     nb = breakpoints<ORDER>(g, in.x0, in.y0, dxx, dxy, split, b);
     if (nb < 0) return false;
     double gpv[2], D[3][2];
-    orbit_integrals_moments<ORDER>(g, rec, in.x0, in.y0, dxx, dxy, b, nb, gpv, D);
+    orbit_integrals_moments<ORDER, SY>(g, rec, in.x0, in.y0, dxx, dxy, b, nb, gpv, D);
     kick_rotate_kick(in, guess, gpv[0], gpv[1], D, A1p, dt, o);
     return true;
 }
@@ -567,13 +586,15 @@ UPIC_D int window_coord(int s, int origin, int n, int w, int span) {
 // PART: kPartFused (solve and deposit in one launch), kPartSolve (local
 // solves only; writes each particle's orbit velocity to vbar_*) or
 // kPartDeposit (the deposit of the orbits in vbar_*).
-template <int ORDER, bool UNIFORM, bool MOM, bool PICARD, int PART = kPartFused>
+// ONED: a grid one cell high (ny = 1): the y stencil is one row (SY = 1).
+template <int ORDER, bool UNIFORM, bool MOM, bool PICARD, int PART = kPartFused, bool ONED = false>
 __global__ void __launch_bounds__(kMapThreads, map_min_blocks(PART))
 implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
     constexpr bool kSolve = PART != kPartDeposit;
     constexpr bool kDeposit = PART != kPartSolve;
     constexpr int S = ORDER + 1;
-    constexpr int SS = S * S;
+    constexpr int SY = ONED ? 1 : S;
+    constexpr int SS = S * SY;
     constexpr int NV = 3 * SS;
     constexpr int RW = SS + 3;
     constexpr int NPER = (NV + 31) / 32;
@@ -608,8 +629,8 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
         const int t = lane + 32 * r;
         const int ab = t < NV ? t / 3 : 0;
         t_ab[r] = ab;
-        t_a[r] = ab / S;
-        t_b[r] = ab % S;
+        t_a[r] = ab / SY;
+        t_b[r] = ab % SY;
         t_c[r] = t < NV ? t - 3 * ab : 0;
         t_off[r] = t_a[r] * tg.wy + t_b[r];
     }
@@ -697,7 +718,7 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                 in.P0[2] = a.Pz[p];
                 in.q = UNIFORM ? a.q0 : a.q[p];
                 in.m = UNIFORM ? a.m0 : a.m[p];
-                gather_rec3<ORDER>(g, a.rec, kIRecAn, in.x0, in.y0, in.A0p);
+                gather_rec3<ORDER, kIRec, SY>(g, a.rec, kIRecAn, in.x0, in.y0, in.A0p);
 #pragma unroll
                 for (int c = 0; c < 3; ++c) in.pstart[c] = in.P0[c] - in.q * in.A0p[c];
                 set_local_constants(in, a.kappa);
@@ -715,9 +736,9 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                 for (int it = 0; it < a.loc_maxit; ++it) {
                     bool okev;
                     if constexpr (MOM)
-                        okev = evaluate_moments<ORDER>(g, a.rec, a.dt, a.kappa, a.split, in, guess, o, bk, nb);
+                        okev = evaluate_moments<ORDER, SY>(g, a.rec, a.dt, a.kappa, a.split, in, guess, o, bk, nb);
                     else
-                        okev = evaluate<ORDER>(g, a.rec, a.dt, a.kappa, a.split, in, guess, o, bk, nb);
+                        okev = evaluate<ORDER, SY>(g, a.rec, a.dt, a.kappa, a.split, in, guess, o, bk, nb);
                     if (!okev) {
                         reason = kLocalTooManyCrossings;
                         break;
@@ -813,8 +834,8 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                         int ilx, ily;
                         if constexpr (MOM) {
                             (void)iq;
-                            SegMoments<ORDER> M;
-                            segment_moments<ORDER, false>(g, in.x0, in.y0, dxx, dxy, sa, len, M);
+                            SegMoments<ORDER, SY> M;
+                            segment_moments<ORDER, false, SY>(g, in.x0, in.y0, dxx, dxy, sa, len, M);
                             ilx = M.ilx;
                             ily = M.ily;
 #pragma unroll
@@ -825,18 +846,18 @@ implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
                             const double xs = wrap1(in.x0 + s * dxx, g.Lx);
                             const double ys = wrap1(in.y0 + s * dxy, g.Ly);
                             Stencil<ORDER> sx, sy;
-                            stencil_xy<ORDER>(g, xs, ys, sx, sy);
+                            stencil_xy<ORDER, SY>(g, xs, ys, sx, sy);
                             ilx = sx.il;
                             ily = sy.il;
 #pragma unroll
                             for (int ia = 0; ia < S; ++ia)
 #pragma unroll
-                                for (int ib = 0; ib < S; ++ib) wgt[ia * S + ib] = wq * sx.w[ia] * sy.w[ib];
+                                for (int ib = 0; ib < SY; ++ib) wgt[ia * SY + ib] = wq * sx.w[ia] * sy.w[ib];
                         }
                         gx0 = wrap_index(ilx, nx);
                         gy0 = wrap_index(ily, ny);
                         const int lx = tg.full_x ? gx0 : window_coord(ilx, ox, nx, tg.wx, S);
-                        const int ly = tg.full_y ? gy0 : window_coord(ily, oy, ny, tg.wy, S);
+                        const int ly = tg.full_y ? gy0 : window_coord(ily, oy, ny, tg.wy, SY);
                         key = (lx < 0 || ly < 0) ? kKeyEscape : lx * tg.wy + ly;
                     }
                 }
@@ -2311,8 +2332,29 @@ MapKernel map_kernel_of(int order, bool uniform, bool split) {
     return nullptr;
 }
 
-MapKernel map_kernel(int order, bool uniform, bool split, bool picard, int part = kPartFused) {
+// The one-row (ny = 1) instances of the split launches: segment moments for
+// every order (knot splitting on; one y node leaves (ORDER + 1) moments per
+// segment).
+template <int PART>
+MapKernel map_kernel_oned(int order, bool uniform) {
+#define UPIC_K1(O) (uniform ? &implicit_map_kernel<O, true, true, false, PART, true> \
+                            : &implicit_map_kernel<O, false, true, false, PART, true>)
+    switch (order) {
+        case 1: return UPIC_K1(1);
+        case 2: return UPIC_K1(2);
+        case 3: return UPIC_K1(3);
+        case 4: return UPIC_K1(4);
+    }
+#undef UPIC_K1
+    return nullptr;
+}
+
+// oned: the grid is one cell high; its split launches (relativistic map,
+// knot splitting on) use the one-row instances.
+MapKernel map_kernel(int order, bool uniform, bool split, bool picard, int part = kPartFused, bool oned = false) {
     if (picard) return map_kernel_of<true, kPartFused>(order, uniform, split);
+    if (oned && split && part == kPartSolve) return map_kernel_oned<kPartSolve>(order, uniform);
+    if (oned && split && part == kPartDeposit) return map_kernel_oned<kPartDeposit>(order, uniform);
     switch (part) {
         case kPartSolve: return map_kernel_of<false, kPartSolve>(order, uniform, split);
         case kPartDeposit: return map_kernel_of<false, kPartDeposit>(order, uniform, split);
@@ -2338,7 +2380,7 @@ cudaError_t implicit_configure_smem(const TileGeom& tg, int order, bool split, b
     const int b = implicit_map_smem_bytes(tg, order);
     for (int u = 0; u < 2; ++u) {
         for (int part = kPartFused; part <= (picard ? kPartFused : kPartDeposit); ++part) {
-            MapKernel k = map_kernel(order, u != 0, split, picard, part);
+            MapKernel k = map_kernel(order, u != 0, split, picard, part, tg.ny == 1);
             if (!k) return cudaErrorInvalidValue;
             const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k), b);
             if (e != cudaSuccess) return e;
@@ -2359,8 +2401,8 @@ cudaError_t launch_implicit_map(int order, bool uniform, bool split, const TileG
                                 const ImplicitMapArgs& a, int grid, cudaStream_t st, bool picard) {
     const int smem = implicit_map_smem_bytes(tg, order);
     if (use_split(a, picard)) {
-        MapKernel ks = map_kernel(order, uniform, split, picard, kPartSolve);
-        MapKernel kd = map_kernel(order, uniform, split, picard, kPartDeposit);
+        MapKernel ks = map_kernel(order, uniform, split, picard, kPartSolve, tg.ny == 1);
+        MapKernel kd = map_kernel(order, uniform, split, picard, kPartDeposit, tg.ny == 1);
         if (!ks || !kd) return cudaErrorInvalidValue;
         // grid is sized for the fused kernel's resident CTAs; each part is
         // given as many CTAs as it keeps resident
