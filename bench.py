@@ -111,13 +111,13 @@ def parse():
                     help="independent runs of the ensemble comparison (0 skips; one GPU only)")
     ap.add_argument("--ensemble-steps", type=int, default=80,
                     help="steps of the ensemble comparison")
-    ap.add_argument("--implicit-ensemble-runs", type=int, default=64,
+    ap.add_argument("--implicit-ensemble-runs", type=int, default=1024,
                     help="1D-2V two-stream runs of the implicit ensemble comparison (0 skips; one GPU only)")
-    ap.add_argument("--implicit-ensemble-steps", type=int, default=10,
+    ap.add_argument("--implicit-ensemble-steps", type=int, default=5,
                     help="steps of the implicit ensemble comparison")
-    ap.add_argument("--implicit-ensemble-max-particles", type=float, default=1e5,
+    ap.add_argument("--implicit-ensemble-max-particles", type=float, default=1e6,
                     help="largest particle count of an implicit ensemble run (log-uniform from 1e4)")
-    ap.add_argument("--implicit-ensemble-check-runs", type=int, default=0,
+    ap.add_argument("--implicit-ensemble-check-runs", type=int, default=32,
                     help="runs stepped alone for the sequential rate and the bitwise check (0: all)")
     ap.add_argument("--large-mixed-check", action="store_true",
                     help="instead of the bench line: the 2048x2048, 64 e-/cell Weibel + beam run in FP64 and in "
