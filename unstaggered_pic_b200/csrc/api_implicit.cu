@@ -1372,16 +1372,20 @@ int implicit_create(upic_ctx* c) {
         return fail(c, UPIC_ERR_CUDA, "cudaFuncSetAttribute (implicit map) failed");
     const int occ = implicit_map_occupancy(s->tg, s->order, split, s->picard);
     s->grid = c->nsm * (occ > 0 ? occ : 1);
-    // Gauss rules: the deck's nq points, and for segment moments (knot
-    // splitting on; order <= 2, or any order on a grid one cell high) the
-    // (order+1)-point rule.  Within a knot-split segment every orbit
-    // integrand -- S_a S_b, (1-s) S'_a S_b, s S'_a S_b (2D), S_a, (1-s) S'_a,
-    // s S'_a (one row) -- is a polynomial of degree <= 2 order + 1 in s,
-    // which an (order+1)-point Gauss rule integrates exactly, as the deck's
-    // rule does when nq >= order+1; the two then differ by rounding only.
+    // Gauss rules.  With knot splitting, every orbit integrand within a
+    // segment -- S_a S_b, (1-s) S'_a S_b, s S'_a S_b in 2D, S_a, (1-s) S'_a,
+    // s S'_a on a grid one cell high, the time-interpolated A included -- is
+    // a polynomial of degree <= 2 order + 1 in s, which an (order+1)-point
+    // Gauss rule integrates exactly, as the deck's nq-point rule does when
+    // nq >= order+1: the two then differ by rounding only.  So with knot
+    // splitting and nq > order+1 both the point-by-point orbit integrals and
+    // the segment moments use the (order+1)-point rule; without knot
+    // splitting a segment spans several spline pieces and the deck's rule is
+    // kept.
     std::vector<double> qs, qw, ms, mw;
+    if (split && s->nq > s->order + 1) s->nq = s->order + 1;
     gauss_legendre_01(s->nq, qs, qw);
-    s->mnq = (split && (s->order <= 2 || c->ny == 1) && s->nq > s->order + 1) ? s->order + 1 : s->nq;
+    s->mnq = s->nq;
     gauss_legendre_01(s->mnq, ms, mw);
     std::vector<double> tab(4 * kMaxQuad, 0.0);
     for (int i = 0; i < s->nq; ++i) {
