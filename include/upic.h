@@ -473,6 +473,18 @@ int upic_fft2d(upic_ctx* ctx, double* re, double* im, int inverse);
  * zeroed: spectral_derivative, spectral_pic_part3.cpp:440-447. */
 int upic_spectral_derivative(upic_ctx* ctx, const double* f, int dir, double* out);
 
+/* IAEM momentum push of the explicit method on the caller's fields
+ * (push_particles_momentum_and_velocity, spectral_pic_part3.cpp:1057-1090):
+ * for particles at (x, y) -- already advanced, x^{n+1} = x^n + dt v^n
+ * (:1050) -- quadratic gathers of A, grad phi and grad A (spectral
+ * derivatives of phi and A, nx*ny and 3 x nx*ny), P += q dt (-grad phi +
+ * (grad A) . (2 v - v_prev)), v from the canonical momentum
+ * (velocity_from_canonical :602), v_prev = the old v.  P, v, v_prev (xyz
+ * triples) are updated in place.  Explicit-method contexts; the run state
+ * is not touched. */
+int upic_push_iaem(upic_ctx* ctx, long np, const double* x, const double* y, double* P, double* v, double* v_prev,
+                   const double* q, const double* m, const double* phi, const double* A);
+
 /* phi = Poisson(rho), zero-mean: solve_initial_phi_from_poisson,
  * spectral_pic_part3.cpp:819-827. */
 int upic_poisson(upic_ctx* ctx, const double* rho, double* phi);
@@ -497,6 +509,39 @@ int upic_orbit_deposit(upic_ctx* ctx, long np, const double* x, const double* y,
 int upic_orbit_gather(upic_ctx* ctx, long np, const double* x, const double* y, const double* dx,
                       const double* mesh, const double* An, const double* Anp1, double* gathered,
                       double* grad);
+
+/* One GM-HC-CN particle push of the implicit method (CN_ORBIT context: its
+ * grid, spline order, Gauss rule, knot splitting, local tolerances and dt)
+ * in the caller's fields: per particle the damped local fixed point on the
+ * orbit velocity, each iterate through the kick-rotate-kick map with the
+ * orbit averages of grad phi_mid and of D_A (solve_local_particle_substep,
+ * Project3/ec_pic_nyquist_projected.cpp:4930; evaluate_local_particle_substep
+ * :4843 with h = dt, theta0 = 0, theta1 = 1).  grad_phi_mid: 2 x nx*ny (x, y
+ * derivatives of phi at the mid level); An, Anp1: 3 x nx*ny (A^n, A^{n+1}).
+ * Per particle: x, y in [-L/2, L/2), P (canonical momentum) and v (the
+ * first guess) as xyz triples, q, m.  Out: the end position x1, y1, P_end
+ * and v_end (triples) and the accepted orbit velocity vbar (triple), NaN
+ * where the local solve failed; report[2p] = local iterations,
+ * report[2p+1] = 0 or the failure reason (1 non-finite map, 2 superluminal
+ * map, 3 non-finite iterate, 4 superluminal iterate, 5 maximum iterations,
+ * 6 too many knot crossings).  The context's run state is not touched. */
+int upic_push_gmhc(upic_ctx* ctx, long np, const double* x, const double* y, const double* P, const double* v,
+                   const double* q, const double* m, const double* grad_phi_mid, const double* An,
+                   const double* Anp1, double* x1, double* y1, double* P_end, double* v_end, double* vbar,
+                   int* report);
+
+/* The field half of one implicit map evaluation (CN_ORBIT context) on the
+ * caller's fields (nx*ny each, vectors 3 x nx*ny): the current J projected
+ * onto the Nyquist-free modes when the context projects, the continuity
+ * update rho1 = rho - dt div J (zero mean, projected;
+ * continuity_charge_update :3288), the Crank-Nicolson step of (phi, psi)
+ * with the mid-level charge and of (A, U) with J (cn_potential_update
+ * :3249 through cn_fft_wave_step_from_spectra :3131; phi1 and psi1 with
+ * zero mean), and optionally grad_phi_mid = (grad phi + grad phi1) / 2
+ * (2 x nx*ny; :5278-5285).  The context's run state is not touched. */
+int upic_fft_solve_cn(upic_ctx* ctx, const double* phi, const double* psi, const double* rho, const double* A,
+                      const double* U, const double* J, double* phi1, double* psi1, double* rho1, double* A1,
+                      double* U1, double* grad_phi_mid);
 
 /* Ensembles of independent runs (no counterpart in the reference, whose
  * runs are one process each).  Each run is a context

@@ -153,6 +153,35 @@ int ref_p2_gather(int nx, int ny, double Lx, double Ly, const double* f, long np
     return 0;
 }
 
+// IAEM momentum push (push_particles_momentum_and_velocity :1057) of the
+// given particles in the fields phi (N) and A (3N), with the reference's
+// spectral gradients (spectral_gradient_scalar / spectral_gradient_vector);
+// P, v, v_prev (3*np) updated in place.
+int ref_p2_push_iaem(int nx, int ny, double Lx, double Ly, double dt, double c, long np, const double* x,
+                     const double* y, double* P, double* v, double* v_prev, const double* q, const double* m,
+                     const double* phi, const double* A) {
+    HarnessCfg h = make_cfg(nx, ny, Lx, Ly, dt, 1, 1, c, 1.0, 1.0, 1.0);
+    std::vector<Particle> e;
+    load_particles(e, np, x, y, P, v, v_prev, q, m);
+    std::array<Field, 3> An;
+    for (int k = 0; k < 3; ++k) An[k].assign(A + (std::size_t)k * h.g.N, A + (std::size_t)(k + 1) * h.g.N);
+    const Field ph(phi, phi + h.g.N);
+    const auto grad_phi = spectral_gradient_scalar(ph, h.g);
+    const auto grad_A = spectral_gradient_vector(An, h.g);
+    push_particles_momentum_and_velocity(e, An, grad_phi, grad_A, h.cfg, h.g);
+    for (long p = 0; p < np; ++p) {
+        const Particle& pe = e[static_cast<std::size_t>(p)];
+        const Vec3* src[3] = {&pe.P, &pe.v, &pe.v_prev};
+        double* dst[3] = {P, v, v_prev};
+        for (int k = 0; k < 3; ++k) {
+            dst[k][3 * p] = src[k]->x;
+            dst[k][3 * p + 1] = src[k]->y;
+            dst[k][3 * p + 2] = src[k]->z;
+        }
+    }
+    return 0;
+}
+
 // Spectral derivative d/dx (dir=0) or d/dy (dir=1) (spectral_pic_part3.cpp:440).
 int ref_p2_spectral_derivative(int nx, int ny, double Lx, double Ly, const double* f, int dir,
                                double* out) {

@@ -174,6 +174,91 @@ int ref_p3_orbit_gather(const double* d, const int* ip, long np, const double* x
     return 0;
 }
 
+// One GM-HC local particle solve per particle (solve_local_particle_substep
+// :4930 with h = dt, theta0 = 0, theta1 = 1) in the given fields:
+// grad_phi_mid 3 x N, An (st.A) and Anp1 (A_end) 3 x N.  x0, P0, v (first
+// guess): 3*np; out: x1, P_end, v_end, vbar 3*np each (NaN on failure),
+// report: iterations, failure reason (LocalParticleFailureReason) per
+// particle.
+int ref_p3_push_gmhc(const double* d, const int* ip, long np, const double* x0, const double* P0,
+                     const double* v, const double* q, const double* m, const double* gpm, const double* An,
+                     const double* Anp1, double* x1, double* P_end, double* v_end, double* vbar, int* report) {
+    Config c = make_cfg(d, ip);
+    Grid g = make_grid(c);
+    Quadrature quad = gauss_legendre_01(c.orbit_quad_order);
+    State st;
+    VecField Ae, G;
+    for (int k = 0; k < 3; ++k) {
+        st.A[k].assign(An + (std::size_t)k * g.N, An + (std::size_t)(k + 1) * g.N);
+        Ae[k].assign(Anp1 + (std::size_t)k * g.N, Anp1 + (std::size_t)(k + 1) * g.N);
+        G[k].assign(gpm + (std::size_t)k * g.N, gpm + (std::size_t)(k + 1) * g.N);
+    }
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    for (long p = 0; p < np; ++p) {
+        const Vec3 X{x0[3 * p], x0[3 * p + 1], x0[3 * p + 2]};
+        const Vec3 P{P0[3 * p], P0[3 * p + 1], P0[3 * p + 2]};
+        const Vec3 V{v[3 * p], v[3 * p + 1], v[3 * p + 2]};
+        Vec3 vb{0.0, 0.0, 0.0};
+        LocalParticleStep mapped;
+        LocalParticleSolveReport rep;
+        const bool ok = solve_local_particle_substep(V, X, P, q[p], m[p], c.dt, 0.0, 1.0, st, Ae, G, g, c, quad,
+                                                     vb, mapped, rep);
+        const Vec3 xe = wrap_pos(add3(X, mul3(c.dt, vb)), g.L);
+        for (int k = 0; k < 3; ++k) {
+            x1[3 * p + k] = ok ? xe[k] : nan;
+            P_end[3 * p + k] = ok ? mapped.P_end[k] : nan;
+            v_end[3 * p + k] = ok ? mapped.v_end[k] : nan;
+            vbar[3 * p + k] = ok ? vb[k] : nan;
+        }
+        report[2 * p] = rep.iterations;
+        report[2 * p + 1] = (int)rep.failure_reason;
+    }
+    return 0;
+}
+
+// The field half of a map evaluation (:5265-5285) on the given fields:
+// J_field projected, rho_end (continuity_charge_update :3288), rho_mid,
+// cn_potential_update (:3249) from the state's spectra, grad_phi_mid.
+// in: phi, psi, rho (N each), A, U, J (3N each); out: phi1, psi1, rho1
+// (N), A1, U1 (3N), gpm (3N, z zero).
+int ref_p3_fft_solve_cn(const double* d, const int* ip, const double* phi, const double* psi, const double* rho,
+                        const double* A, const double* U, const double* J, double* phi1, double* psi1,
+                        double* rho1, double* A1, double* U1, double* gpm) {
+    Config c = make_cfg(d, ip);
+    Grid g = make_grid(c);
+    State st;
+    st.phi.assign(phi, phi + g.N);
+    st.psi.assign(psi, psi + g.N);
+    st.rho.assign(rho, rho + g.N);
+    VecField Jf;
+    for (int k = 0; k < 3; ++k) {
+        st.A[k].assign(A + (std::size_t)k * g.N, A + (std::size_t)(k + 1) * g.N);
+        st.U[k].assign(U + (std::size_t)k * g.N, U + (std::size_t)(k + 1) * g.N);
+        Jf[k].assign(J + (std::size_t)k * g.N, J + (std::size_t)(k + 1) * g.N);
+    }
+    const WaveSpectralState cache = make_wave_spectral_state(st.phi, st.psi, st.A, st.U, g);
+    const VecField grad_phi_n = spectral_gradient_scalar(st.phi, g);
+    project_nyquist(Jf, g);
+    const Field rho_end = continuity_charge_update(st.rho, Jf, c.dt, g);
+    Field rho_mid(g.N);
+    for (int id = 0; id < g.N; ++id) rho_mid[id] = 0.5 * (st.rho[id] + rho_end[id]);
+    Field phi_end, psi_end;
+    VecField A_end, U_end;
+    cn_potential_update(st, rho_mid, Jf, c.dt, g, c.kappa, c.sigma1, c.sigma2, phi_end, psi_end, A_end, U_end,
+                        &cache);
+    const VecField grad_phi_end = spectral_gradient_scalar(phi_end, g);
+    std::memcpy(phi1, phi_end.data(), sizeof(double) * g.N);
+    std::memcpy(psi1, psi_end.data(), sizeof(double) * g.N);
+    std::memcpy(rho1, rho_end.data(), sizeof(double) * g.N);
+    for (int k = 0; k < 3; ++k) {
+        std::memcpy(A1 + (std::size_t)k * g.N, A_end[k].data(), sizeof(double) * g.N);
+        std::memcpy(U1 + (std::size_t)k * g.N, U_end[k].data(), sizeof(double) * g.N);
+        for (int id = 0; id < g.N; ++id)
+            gpm[(std::size_t)k * g.N + id] = 0.5 * (grad_phi_n[k][id] + grad_phi_end[k][id]);
+    }
+    return 0;
+}
+
 // Config of an instability case: case_d = {v0, perturbation,
 // two_stream_density_alpha, tsi_transverse_seed, weibel_B0}, case_i = {kind
 // (0 two-stream, 1 Weibel), particles_per_cell_pair, two_stream_eigenmode,

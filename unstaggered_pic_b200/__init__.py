@@ -365,6 +365,48 @@ class Simulation:
         a, u = _f64(A, (3 * self.N,)), _f64(U, (3 * self.N,))
         self._check(lib().upic_set_initial_potential(self._ctx, _p(a), _p(u)))
 
+    def push_iaem(self, x, y, P, v, v_prev, q, m, phi, A):
+        """IAEM momentum push of the explicit method on the given fields
+        (upic_push_iaem): returns the new P, v and v_prev (n x 3)."""
+        xa, ya = _f64(x).ravel(), _f64(y).ravel()
+        n = xa.size
+        Pa, va, wa = (np.array(_f64(a, (n, 3)), copy=True) for a in (P, v, v_prev))
+        qa, ma = _f64(q).ravel(), _f64(m).ravel()
+        self._check(lib().upic_push_iaem(self._ctx, n, _p(xa), _p(ya), _p(Pa), _p(va), _p(wa), _p(qa), _p(ma),
+                                         _p(_f64(phi, (self.N,))), _p(_f64(A, (3 * self.N,)))))
+        return Pa, va, wa
+
+    def push_gmhc(self, x, y, P, v, q, m, grad_phi_mid, An, Anp1):
+        """One GM-HC-CN particle push in the given fields (upic_push_gmhc):
+        returns x1, y1, P_end, v_end, vbar (NaN where the local solve failed)
+        and the (iterations, failure reason) report per particle."""
+        xa, ya = _f64(x).ravel(), _f64(y).ravel()
+        n = xa.size
+        Pa, va = _f64(P, (n, 3)), _f64(v, (n, 3))
+        qa, ma = _f64(q).ravel(), _f64(m).ravel()
+        g = _f64(grad_phi_mid, (2 * self.N,))
+        a0, a1 = _f64(An, (3 * self.N,)), _f64(Anp1, (3 * self.N,))
+        out = {"x1": np.empty(n), "y1": np.empty(n), "P_end": np.empty((n, 3)), "v_end": np.empty((n, 3)),
+               "vbar": np.empty((n, 3))}
+        rep = np.empty((n, 2), dtype=np.int32)
+        self._check(lib().upic_push_gmhc(self._ctx, n, _p(xa), _p(ya), _p(Pa), _p(va), _p(qa), _p(ma), _p(g),
+                                         _p(a0), _p(a1), *[_p(out[k]) for k in ("x1", "y1", "P_end", "v_end", "vbar")],
+                                         rep.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        out["report"] = rep
+        return out
+
+    def fft_solve_cn(self, phi, psi, rho, A, U, J):
+        """The field half of one implicit map evaluation on the given fields
+        (upic_fft_solve_cn): dict of phi, psi, rho (nx x ny), A, U (3 x nx x ny)
+        and grad_phi_mid (2 x nx x ny) of the new level."""
+        nx, ny = self.config.nx, self.config.ny
+        ins = [_f64(f, (k * self.N,)) for f, k in ((phi, 1), (psi, 1), (rho, 1), (A, 3), (U, 3), (J, 3))]
+        out = {"phi": np.empty((nx, ny)), "psi": np.empty((nx, ny)), "rho": np.empty((nx, ny)),
+               "A": np.empty((3, nx, ny)), "U": np.empty((3, nx, ny)), "grad_phi_mid": np.empty((2, nx, ny))}
+        self._check(lib().upic_fft_solve_cn(self._ctx, *[_p(a) for a in ins],
+                                            *[_p(out[k]) for k in ("phi", "psi", "rho", "A", "U", "grad_phi_mid")]))
+        return out
+
     def map_log(self):
         """Map evaluations of the last step_implicit call, one row each in
         MAP_LOG_COLUMNS order (upic_map_log)."""

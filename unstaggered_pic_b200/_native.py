@@ -69,6 +69,9 @@ SYMBOLS = {
     "upic_set_initial_potential": (ctypes.c_int, [ctypes.c_void_p, c_dp, c_dp]),
     "upic_convergence_method_name": (ctypes.c_char_p, [ctypes.c_int]),
     "upic_set_time_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "upic_push_gmhc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 14 + [c_ip]),
+    "upic_fft_solve_cn": (ctypes.c_int, [ctypes.c_void_p] + [c_dp] * 12),
+    "upic_push_iaem": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 9),
     "upic_map_log": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, c_ip]),
     "upic_probe_fields": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, c_dp, c_dp, c_dp]),
     "upic_generate_bimaxwellian": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,

@@ -1523,6 +1523,66 @@ int upic_spectral_derivative(upic_ctx* c, const double* f, int dir, double* out)
     return sync(c);
 }
 
+int upic_push_iaem(upic_ctx* c, long np, const double* x, const double* y, double* P, double* v, double* v_prev,
+                   const double* q, const double* m, const double* phi, const double* A) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (c->imp) return fail(c, UPIC_ERR_STATE, "upic_push_iaem needs an explicit method (bdf1, bdf2)");
+    if (np < 0 || !phi || !A || (np > 0 && (!x || !y || !P || !v || !v_prev || !q || !m)))
+        return fail(c, UPIC_ERR_ARGUMENT, "upic_push_iaem: null array or negative particle count");
+    if (np == 0) return UPIC_OK;
+    for (long p = 0; p < np; ++p)
+        if (!std::isfinite(x[p]) || !std::isfinite(y[p]) || !std::isfinite(q[p]) || !(m[p] > 0.0))
+            return fail(c, UPIC_ERR_NONFINITE, "upic_push_iaem: non-finite position or charge, or mass <= 0");
+    const size_t N = (size_t)c->N, n = (size_t)np;
+    // device scratch of this call, freed on every return path
+    struct Buf {
+        std::vector<void*> p;
+        ~Buf() {
+            for (void* q : p) cudaFree(q);
+        }
+        double* get(size_t k) {
+            void* v = nullptr;
+            if (cudaMalloc(&v, k * sizeof(double) + 16) != cudaSuccess) return nullptr;
+            p.push_back(v);
+            return static_cast<double*>(v);
+        }
+    } b;
+    double* F = b.get(11 * N);
+    double* fin = b.get(N);
+    double2* spec = reinterpret_cast<double2*>(b.get(4 * N));
+    double *dx_ = b.get(n), *dy_ = b.get(n), *dP = b.get(3 * n), *dv = b.get(3 * n), *dvp = b.get(3 * n);
+    double *dq = b.get(n), *dm = b.get(n);
+    if (!F || !fin || !spec || !dx_ || !dy_ || !dP || !dv || !dvp || !dq || !dm)
+        return fail(c, UPIC_ERR_NOMEM, "upic_push_iaem: device allocation failed");
+    // F: A (3), grad phi (2), dA_c/dx, dA_c/dy (spectral_gradient_scalar,
+    // spectral_gradient_vector: spectral_derivative :440 with the Nyquist
+    // wave number zeroed)
+    UPIC_CUDA(c, cudaMemcpyAsync(F, A, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c->st));
+    const double* src[4] = {phi, A, A + N, A + 2 * N};
+    const size_t dst[4] = {3, 5, 7, 9};
+    for (int f = 0; f < 4; ++f) {
+        UPIC_CUDA(c, cudaMemcpyAsync(fin, src[f], sizeof(double) * N, cudaMemcpyHostToDevice, c->st));
+        UPIC_CUDA(c, fft2d_batched(c->plan, spec, 1, 0, c->st, fin));
+        for (int d = 0; d < 2; ++d) {
+            UPIC_CUDA(c, launch_derivative_kspace((int)N, d == 0 ? c->d_kx : c->d_ky, spec, spec + N, c->st));
+            UPIC_CUDA(c, fft2d_batched(c->plan, spec + N, 1, 1, c->st, nullptr, 1, F + (dst[f] + d) * N));
+        }
+    }
+    UPIC_CUDA(c, cudaMemcpyAsync(dx_, x, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(dy_, y, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(dP, P, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(dv, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(dvp, v_prev, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(dq, q, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(dm, m, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, launch_iaem_push(np, dx_, dy_, dP, dv, dvp, dq, dm, F, c->nx, c->ny, 1.0 / c->dx, 1.0 / c->dy,
+                                  c->cfg.dt, c->cfg.c, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(P, dP, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(v, dv, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(v_prev, dvp, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+
 int upic_poisson(upic_ctx* c, const double* rho, double* phi) {
     if (!c || !rho || !phi) return UPIC_ERR_ARGUMENT;
     const long N = c->N;

@@ -2258,3 +2258,154 @@ extern "C" int upic_write_field_snapshot(upic_ctx* c, const char* path, int appe
     const bool ok = std::fclose(out) == 0;
     return ok ? UPIC_OK : fail(c, UPIC_ERR_ARGUMENT, std::string("write failed: ") + path);
 }
+
+// ---- kernel-level GM-HC push and CN field update -------------------------------
+
+extern "C" int upic_push_gmhc(upic_ctx* c, long np, const double* x, const double* y, const double* P,
+                              const double* v, const double* q, const double* m, const double* grad_phi_mid,
+                              const double* An, const double* Anp1, double* x1, double* y1, double* P_end,
+                              double* v_end, double* vbar, int* report) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (!c->imp || c->imp->picard)
+        return fail(c, UPIC_ERR_STATE, "upic_push_gmhc needs a UPIC_METHOD_CN_ORBIT context");
+    if (np < 0 || !grad_phi_mid || !An || !Anp1 ||
+        (np > 0 && (!x || !y || !P || !v || !q || !m || !x1 || !y1 || !P_end || !v_end || !vbar || !report)))
+        return fail(c, UPIC_ERR_ARGUMENT, "upic_push_gmhc: null array or negative particle count");
+    if (np == 0) return UPIC_OK;
+    for (long p = 0; p < np; ++p)
+        if (!std::isfinite(x[p]) || !std::isfinite(y[p]) || !(m[p] > 0.0) || !std::isfinite(q[p]))
+            return fail(c, UPIC_ERR_NONFINITE, "upic_push_gmhc: non-finite position or charge, or mass <= 0");
+    ImplicitState& s = *c->imp;
+    const upic_config& cf = c->cfg;
+    const int N = c->N;
+    // node records: grad phi_mid (2), A^n (3), A^{n+1} (3)
+    std::vector<double> rec((size_t)kIRec * N), in7(7 * (size_t)np), g3(3 * (size_t)np);
+    for (int i = 0; i < N; ++i) {
+        double* r = &rec[(size_t)kIRec * i];
+        r[kIRecGpm] = grad_phi_mid[i];
+        r[kIRecGpm + 1] = grad_phi_mid[N + i];
+        for (int k = 0; k < 3; ++k) {
+            r[kIRecAn + k] = An[(size_t)k * N + i];
+            r[kIRecAe + k] = Anp1[(size_t)k * N + i];
+        }
+    }
+    for (long p = 0; p < np; ++p) {
+        in7[p] = x[p];
+        in7[np + p] = y[p];
+        for (int k = 0; k < 3; ++k) {
+            in7[(2 + k) * np + p] = P[3 * p + k];
+            g3[k * np + p] = v[3 * p + k];
+        }
+        in7[5 * np + p] = q[p];
+        in7[6 * np + p] = m[p];
+    }
+    Scratch sc;
+    double* drec = sc.get<double>(rec.size());
+    double* din = sc.get<double>(in7.size());
+    double* dg = sc.get<double>(g3.size());
+    double* dout = sc.get<double>(11 * (size_t)np);
+    int* drep = sc.get<int>(2 * (size_t)np);
+    if (!drec || !din || !dg || !dout || !drep) return fail(c, UPIC_ERR_NOMEM, "upic_push_gmhc: device allocation failed");
+    UPIC_CUDA(c, cudaMemcpyAsync(drec, rec.data(), sizeof(double) * rec.size(), cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(din, in7.data(), sizeof(double) * in7.size(), cudaMemcpyHostToDevice, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(dg, g3.data(), sizeof(double) * g3.size(), cudaMemcpyHostToDevice, c->st));
+    ImplicitMapArgs a{};
+    a.rec = drec;
+    a.Lx = cf.Lx;
+    a.Ly = cf.Ly;
+    a.inv_dx = 1.0 / s.dx;
+    a.inv_dy = 1.0 / s.dy;
+    a.dt = cf.dt;
+    a.kappa = cf.kappa;
+    a.split = cf.split_orbit_at_knots;
+    a.loc_rtol = cf.local_rtol;
+    a.loc_atol = cf.local_atol;
+    a.loc_damp = cf.local_damping;
+    a.loc_maxit = cf.local_max_iter;
+    a.qtab = s.qtab;
+    a.nq = s.nq;
+    a.mnq = s.mnq;
+    UPIC_CUDA(c, launch_gmhc_push(s.order, a, c->nx, c->ny, np, din, dg, dout, drep, c->st));
+    std::vector<double> out(11 * (size_t)np);
+    UPIC_CUDA(c, cudaMemcpyAsync(out.data(), dout, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, c->st));
+    UPIC_CUDA(c, cudaMemcpyAsync(report, drep, sizeof(int) * 2 * np, cudaMemcpyDeviceToHost, c->st));
+    int rc;
+    if ((rc = sync(c))) return rc;
+    for (long p = 0; p < np; ++p) {
+        x1[p] = out[p];
+        y1[p] = out[np + p];
+        for (int k = 0; k < 3; ++k) {
+            P_end[3 * p + k] = out[(2 + k) * np + p];
+            v_end[3 * p + k] = out[(5 + k) * np + p];
+            vbar[3 * p + k] = out[(8 + k) * np + p];
+        }
+    }
+    return UPIC_OK;
+}
+
+extern "C" int upic_fft_solve_cn(upic_ctx* c, const double* phi, const double* psi, const double* rho,
+                                 const double* A, const double* U, const double* J, double* phi1, double* psi1,
+                                 double* rho1, double* A1, double* U1, double* grad_phi_mid) {
+    if (!c) return UPIC_ERR_ARGUMENT;
+    if (!c->imp || c->imp->picard)
+        return fail(c, UPIC_ERR_STATE, "upic_fft_solve_cn needs a UPIC_METHOD_CN_ORBIT context");
+    if (!phi || !psi || !rho || !A || !U || !J || !phi1 || !psi1 || !rho1 || !A1 || !U1)
+        return fail(c, UPIC_ERR_ARGUMENT, "upic_fft_solve_cn: null array");
+    ImplicitState& s = *c->imp;
+    const upic_config& cf = c->cfg;
+    const int N = c->N;
+    const size_t n = (size_t)N;
+    Scratch sc;
+    double* dreal = sc.get<double>(9 * n);
+    double* dj = sc.get<double>(3 * n);
+    double2* sin_ = sc.get<double2>(9 * n);
+    double2* sout = sc.get<double2>(9 * n);
+    double2* jhat = sc.get<double2>(3 * n);
+    double2* gsp = sc.get<double2>(5 * n);
+    if (!dreal || !dj || !sin_ || !sout || !jhat || !gsp)
+        return fail(c, UPIC_ERR_NOMEM, "upic_fft_solve_cn: device allocation failed");
+    // state spectra in the order phi, psi, rho, A (3), U (3)
+    const double* src[5] = {phi, psi, rho, A, U};
+    const size_t cnt[5] = {n, n, n, 3 * n, 3 * n};
+    size_t off = 0;
+    for (int k = 0; k < 5; ++k) {
+        UPIC_CUDA(c, cudaMemcpyAsync(dreal + off, src[k], sizeof(double) * cnt[k], cudaMemcpyHostToDevice, c->st));
+        off += cnt[k];
+    }
+    UPIC_CUDA(c, fft2d_batched(c->plan, sin_, 9, 0, c->st, dreal));
+    // J_field: the Nyquist-projected current (:5265-5266)
+    UPIC_CUDA(c, cudaMemcpyAsync(dj, J, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->st));
+    if (cf.nyquist_projection) UPIC_CUDA(c, launch_project_nyquist(dj, 3, c->nx, c->ny, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, jhat, 3, 0, c->st, dj));
+    CnArgs k{};
+    k.nx = c->nx;
+    k.ny = c->ny;
+    k.N = N;
+    k.kx = c->d_kx;
+    k.ky = c->d_ky;
+    k.k2 = c->d_k2;
+    k.excl = cf.nyquist_projection ? s.excl : nullptr;
+    k.Jhat = jhat;
+    k.st = sin_;
+    k.out = sout;
+    k.gspec = gsp;
+    k.dt = cf.dt;
+    k.kappa = cf.kappa;
+    k.sigma1 = cf.sigma1;
+    k.sigma2 = cf.sigma2;
+    UPIC_CUDA(c, launch_cn_kspace(k, c->st));
+    UPIC_CUDA(c, fft2d_batched(c->plan, sout, 9, 1, c->st, nullptr, 1, dreal));
+    double* dst[5] = {phi1, psi1, rho1, A1, U1};
+    off = 0;
+    for (int q = 0; q < 5; ++q) {
+        UPIC_CUDA(c, cudaMemcpyAsync(dst[q], dreal + off, sizeof(double) * cnt[q], cudaMemcpyDeviceToHost, c->st));
+        off += cnt[q];
+    }
+    if (grad_phi_mid) {
+        int rc;
+        if ((rc = sync(c))) return rc;
+        UPIC_CUDA(c, fft2d_batched(c->plan, gsp, 2, 1, c->st, nullptr, 1, dreal));
+        UPIC_CUDA(c, cudaMemcpyAsync(grad_phi_mid, dreal, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, c->st));
+    }
+    return sync(c);
+}

@@ -838,6 +838,64 @@ int push_occupancy(const TileGeom& tg, int ncomp) {
     return n;
 }
 
+// IAEM momentum push of a particle list in given fields
+// (push_particles_momentum_and_velocity, spectral_pic_part3.cpp:1057-1090):
+// quadratic gathers of A, grad phi and grad A at (x, y), P += q dt
+// (-grad phi + (grad A) . v*), v* = 2 v - v_prev, then v from the canonical
+// momentum (velocity_from_canonical :602).  F: 11 planar fields A (3),
+// grad phi (2), dAx/dx, dAx/dy, dAy/dx, dAy/dy, dAz/dx, dAz/dy.  P, v,
+// v_prev: xyz triples, updated in place.
+__global__ void iaem_push_kernel(long np, const double* __restrict__ x, const double* __restrict__ y,
+                                 double* __restrict__ P, double* __restrict__ v, double* __restrict__ vp,
+                                 const double* __restrict__ q, const double* __restrict__ m,
+                                 const double* __restrict__ F, int nx, int ny, double inv_dx, double inv_dy,
+                                 double dt, double c) {
+    const int N = nx * ny;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
+        const Quad1D qx = quadratic_weights(x[p], inv_dx);
+        const Quad1D qy = quadratic_weights(y[p], inv_dy);
+        const double wx[3] = {qx.w0, qx.w1, qx.w2}, wy[3] = {qy.w0, qy.w1, qy.w2};
+        double G[11];
+        for (int f = 0; f < 11; ++f) G[f] = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            const int gx = wrap_index(qx.ic - 1 + a, nx);
+            for (int b = 0; b < 3; ++b) {
+                const int node = gx * ny + wrap_index(qy.ic - 1 + b, ny);
+                for (int f = 0; f < 11; ++f) G[f] += F[(size_t)f * N + node] * wx[a] * wy[b];
+            }
+        }
+        const double vs[3] = {2.0 * v[3 * p] - vp[3 * p], 2.0 * v[3 * p + 1] - vp[3 * p + 1],
+                              2.0 * v[3 * p + 2] - vp[3 * p + 2]};
+        const double gv[2] = {G[5] * vs[0] + G[7] * vs[1] + G[9] * vs[2], G[6] * vs[0] + G[8] * vs[1] + G[10] * vs[2]};
+        const double force[3] = {-G[3] + gv[0], -G[4] + gv[1], 0.0};
+        const double qdt = q[p] * dt;
+        double Pn[3], pm[3];
+        for (int k = 0; k < 3; ++k) {
+            Pn[k] = P[3 * p + k] + qdt * force[k];
+            pm[k] = Pn[k] - q[p] * G[k];
+        }
+        const double mc2 = m[p] * c * c;
+        const double den = sqrt(c * c * (pm[0] * pm[0] + pm[1] * pm[1] + pm[2] * pm[2]) + mc2 * mc2);
+        const double s = den == 0.0 ? 0.0 : c * c / den;
+        for (int k = 0; k < 3; ++k) {
+            vp[3 * p + k] = v[3 * p + k];
+            v[3 * p + k] = s * pm[k];
+            P[3 * p + k] = Pn[k];
+        }
+    }
+}
+
+cudaError_t launch_iaem_push(long np, const double* x, const double* y, double* P, double* v, double* vp,
+                             const double* q, const double* m, const double* F, int nx, int ny, double inv_dx,
+                             double inv_dy, double dt, double c, cudaStream_t st) {
+    long g = (np + 127) / 128;
+    if (g > 148 * 16) g = 148 * 16;
+    iaem_push_kernel<<<(int)(g < 1 ? 1 : g), 128, 0, st>>>(np, x, y, P, v, vp, q, m, F, nx, ny, inv_dx, inv_dy, dt,
+                                                           c);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_push_deposit(int mode, int ncomp, bool uniform, const TileGeom& tg,
                                 const PushArgs& a, int grid, cudaStream_t st) {
 #define UPIC_CASE(MODE, NC)                                                     \

@@ -1320,6 +1320,80 @@ __global__ void gather3_kernel(int nx, int ny, double Lx, double Ly, const doubl
 // planar fields phi, psi, rho, A, U, J, E, B; per point the 18 shape
 // gathers, grad(S phi) and grad(S A) (row c: dA_c/dx, dA_c/dy, 0), 30
 // values in the UPIC_PROBE_* order.
+// GM-HC-CN push of a particle list in given fields (upic_push_gmhc): the
+// damped local fixed point on the orbit velocity (solve_local_particle_substep
+// :4930) with the kick-rotate-kick map (evaluate_local_particle_substep
+// :4843, h = dt, theta0 = 0, theta1 = 1), one thread per particle.  rec:
+// node records (grad phi_mid, A^n, A^{n+1}; kIRec doubles per node).  in7:
+// x, y, Px, Py, Pz, q, m per particle (planar, stride np); guess3: the
+// first guesses (planar); out: x1, y1, P_end (3), v_end (3), vbar (3)
+// (planar, NaN for a failed particle); rep: iterations and failure reason.
+template <int ORDER, bool MOM>
+__global__ void gmhc_push_kernel(ImplicitMapArgs a, int nx, int ny, long np, const double* __restrict__ in7,
+                                 const double* __restrict__ guess3, double* __restrict__ out, int* __restrict__ rep) {
+    Geo g{nx, ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    g.qs = a.qtab;
+    g.qw = a.qtab + kMaxQuad;
+    g.ms = a.qtab + 2 * kMaxQuad;
+    g.mw = a.qtab + 3 * kMaxQuad;
+    g.nq = a.nq;
+    g.mnq = a.mnq;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < np; p += (long)gridDim.x * blockDim.x) {
+        LocalIn in;
+        in.x0 = in7[p];
+        in.y0 = in7[np + p];
+        for (int c = 0; c < 3; ++c) in.P0[c] = in7[(2 + c) * np + p];
+        in.q = in7[5 * np + p];
+        in.m = in7[6 * np + p];
+        gather_rec3<ORDER>(g, a.rec, kIRecAn, in.x0, in.y0, in.A0p);
+        for (int c = 0; c < 3; ++c) in.pstart[c] = in.P0[c] - in.q * in.A0p[c];
+        set_local_constants(in, a.kappa);
+        double guess[3] = {guess3[p], guess3[np + p], guess3[2 * np + p]};
+        double bk[kMaxBreaks];
+        int nb = 0, iters = 0, reason = kLocalMaxIter;
+        LocalOut o;
+        for (int it = 0; it < a.loc_maxit; ++it) {
+            const bool okev = MOM ? evaluate_moments<ORDER>(g, a.rec, a.dt, a.kappa, a.split, in, guess, o, bk, nb)
+                                  : evaluate<ORDER>(g, a.rec, a.dt, a.kappa, a.split, in, guess, o, bk, nb);
+            if (!okev) {
+                reason = kLocalTooManyCrossings;
+                break;
+            }
+            ++iters;
+            if (!finite3(o.vbar_map)) {
+                reason = kLocalNonfiniteMap;
+                break;
+            }
+            if (norm3(o.vbar_map) >= a.kappa) {
+                reason = kLocalSuperluminalMap;
+                break;
+            }
+            const double res[3] = {o.vbar_map[0] - guess[0], o.vbar_map[1] - guess[1], o.vbar_map[2] - guess[2]};
+            const double sc = 0.5 * (norm3(o.vbar_map) + norm3(guess));
+            if (norm3(res) / (a.loc_atol + a.loc_rtol * sc) <= 1.0) {
+                reason = kLocalOk;
+                break;
+            }
+            for (int c = 0; c < 3; ++c) guess[c] += a.loc_damp * res[c];
+            if (!finite3(guess)) {
+                reason = kLocalNonfiniteIterate;
+                break;
+            }
+            if (norm3(guess) >= a.kappa) {
+                reason = kLocalSuperluminalIterate;
+                break;
+            }
+        }
+        const bool ok = reason == kLocalOk;
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        const double vals[11] = {o.x1, o.y1, o.P_end[0], o.P_end[1], o.P_end[2], o.v_end[0], o.v_end[1],
+                                 o.v_end[2], guess[0], guess[1], guess[2]};
+        for (int k = 0; k < 11; ++k) out[(size_t)k * np + p] = ok ? vals[k] : nan;
+        rep[2 * p] = iters;
+        rep[2 * p + 1] = reason;
+    }
+}
+
 template <int ORDER>
 __global__ void probe_kernel(int nx, int ny, double Lx, double Ly, const double* __restrict__ F, long np,
                              const double* x, const double* y, double* out) {
@@ -2606,6 +2680,27 @@ cudaError_t launch_gather3(int order, int nx, int ny, double Lx, double Ly, cons
         case 2: gather3_kernel<2><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, f3, np, x, y, out3); break;
         case 3: gather3_kernel<3><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, f3, np, x, y, out3); break;
         case 4: gather3_kernel<4><<<g, 256, 0, st>>>(nx, ny, Lx, Ly, f3, np, x, y, out3); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gmhc_push(int order, const ImplicitMapArgs& a, int nx, int ny, long np, const double* in7,
+                             const double* guess3, double* out, int* rep, cudaStream_t st) {
+    const int gr = gsize(np, 128);
+    const bool mom = a.split && order <= 2;
+    switch (order) {
+        case 1:
+            if (mom) gmhc_push_kernel<1, true><<<gr, 128, 0, st>>>(a, nx, ny, np, in7, guess3, out, rep);
+            else gmhc_push_kernel<1, false><<<gr, 128, 0, st>>>(a, nx, ny, np, in7, guess3, out, rep);
+            break;
+        case 2:
+            if (mom) gmhc_push_kernel<2, true><<<gr, 128, 0, st>>>(a, nx, ny, np, in7, guess3, out, rep);
+            else gmhc_push_kernel<2, false><<<gr, 128, 0, st>>>(a, nx, ny, np, in7, guess3, out, rep);
+            break;
+        case 3: gmhc_push_kernel<3, false><<<gr, 128, 0, st>>>(a, nx, ny, np, in7, guess3, out, rep); break;
+        case 4: gmhc_push_kernel<4, false><<<gr, 128, 0, st>>>(a, nx, ny, np, in7, guess3, out, rep); break;
         default: return cudaErrorInvalidValue;
     }
     count_launches(1);

@@ -189,6 +189,14 @@ cudaError_t launch_gather3(int order, int nx, int ny, double Lx, double Ly, cons
                            long np, const double* x, const double* y, double* out3,
                            cudaStream_t st);
 
+// GM-HC-CN push of a particle list in the node records a.rec (grad phi_mid,
+// A^n, A^{n+1}): in7 = x, y, Px, Py, Pz, q, m (planar, stride np), guess3 =
+// first guesses (planar); out = x1, y1, P_end (3), v_end (3), vbar (3)
+// (planar; NaN where the local solve failed); rep = iterations, reason per
+// particle (solve_local_particle_substep :4930).
+cudaError_t launch_gmhc_push(int order, const ImplicitMapArgs& a, int nx, int ny, long np, const double* in7,
+                             const double* guess3, double* out, int* rep, cudaStream_t st);
+
 // Point probes of 18 planar fields (phi, psi, rho, A, U, J, E, B): their
 // shape gathers, grad(S phi) and grad(S A), 30 values per point
 // (evaluate_reconstructed_field_probe :7924).

@@ -159,6 +159,12 @@ constexpr int kDiagPart = 5;  // kinetic hi/lo, gamma-sum hi/lo, max speed
 // ncomp: 1 (charge only), 3 (current), 4 (current + charge).
 cudaError_t launch_push_deposit(int mode, int ncomp, bool uniform_qm, const TileGeom& tg,
                                 const PushArgs& a, int grid, cudaStream_t st);
+// IAEM momentum push of a particle list in given fields (kernel-level entry
+// upic_push_iaem): F = A (3), grad phi (2), grad A (6, dA_c/dx, dA_c/dy per
+// component), planar; P, v, v_prev xyz triples updated in place.
+cudaError_t launch_iaem_push(long np, const double* x, const double* y, double* P, double* v, double* vp,
+                             const double* q, const double* m, const double* F, int nx, int ny, double inv_dx,
+                             double inv_dy, double dt, double c, cudaStream_t st);
 int push_deposit_smem_bytes(const TileGeom& tg, int ncomp);
 cudaError_t push_configure_smem(const TileGeom& tg);
 // Resident CTAs per SM of the step's push kernel (ncomp 3 or 4).
