@@ -99,8 +99,12 @@ cudaError_t permute_particles(const ParticleSoA& src, const ParticleSoA& dst, lo
 // dst[id[k]] = src[k] for the arrays x..wz (restores the caller's order).
 cudaError_t unpermute_particles(const ParticleSoA& src, const ParticleSoA& dst, long np,
                                 cudaStream_t st);
-// The radix sort of w.keys (with w.vals) and the chunk table, after the keys
-// are made (shared by both particle formats).
+// The buffer a key kernel writes the unsorted cell keys into (the radix
+// passes alternate between two buffers and end in w.keys).
+unsigned* sort_key_input(const TileGeom& tg, SortWork& w);
+// The radix sort of the keys in sort_key_input(tg, w) into w.keys, with the
+// sorted source indices in w.vals, and the chunk table (shared by both
+// particle formats).
 cudaError_t sort_keys_to_chunks(const TileGeom& tg, long np, SortWork& w, cudaStream_t st);
 
 // ---------------------------------------------------------------------------
