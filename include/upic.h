@@ -433,6 +433,36 @@ enum {
 };
 int upic_map_log(upic_ctx* ctx, int capacity, double* rows, int* nrows);
 
+/* Failed-particle records of the last upic_step_implicit call (CN_ORBIT with
+ * selective_particle_fallback): one row per particle whose local solve
+ * failed in a map evaluation of the selective layout (the
+ * FailedParticleDiagnostic list of evaluate_selective_current_map_at_layout,
+ * ec_pic_nyquist_projected.cpp:5331-5350, sorted by particle index), with
+ * the columns of Project3's _failed_particle_diagnostics.csv after its
+ * time_before column (write_failed_particle_diagnostics :6234): step of the
+ * call, layout_refinement_restart, map_evaluation, event_exhausted (1 when
+ * the event left a particle at the substep limit), failed_particles_in_event,
+ * particle_index (load order), assigned_substeps, failed_substep (0-based),
+ * theta0, theta1, h, local_iterations, failure_reason (0-5 as the
+ * reference's LocalParticleFailureReason; 6 = more knot crossings than the
+ * orbit quadrature holds), first_scaled_residual, final_scaled_residual,
+ * final_absolute_residual, q, m, x0 (3; z = 0), P0 (3), initial_guess (3),
+ * last_guess (3), last_map (3).  Every failed particle of an event is
+ * listed; the reference's file keeps the worst selective_failure_diagnostic_
+ * limit of them (and the worst exhausted one), which the writer selects.
+ * *nrows receives the number of rows; min(capacity, *nrows) rows of
+ * UPIC_FAILLOG_COUNT doubles are copied to rows. */
+enum {
+    UPIC_FAILLOG_STEP = 0, UPIC_FAILLOG_RESTART, UPIC_FAILLOG_EVALUATION, UPIC_FAILLOG_EXHAUSTED,
+    UPIC_FAILLOG_IN_EVENT, UPIC_FAILLOG_PARTICLE, UPIC_FAILLOG_SUBSTEPS, UPIC_FAILLOG_FAILED_SUBSTEP,
+    UPIC_FAILLOG_THETA0, UPIC_FAILLOG_THETA1, UPIC_FAILLOG_H, UPIC_FAILLOG_ITERATIONS, UPIC_FAILLOG_REASON,
+    UPIC_FAILLOG_FIRST_SCALED, UPIC_FAILLOG_FINAL_SCALED, UPIC_FAILLOG_FINAL_ABSOLUTE, UPIC_FAILLOG_Q,
+    UPIC_FAILLOG_M, UPIC_FAILLOG_X0, UPIC_FAILLOG_P0 = UPIC_FAILLOG_X0 + 3,
+    UPIC_FAILLOG_INITIAL_GUESS = UPIC_FAILLOG_P0 + 3, UPIC_FAILLOG_LAST_GUESS = UPIC_FAILLOG_INITIAL_GUESS + 3,
+    UPIC_FAILLOG_LAST_MAP = UPIC_FAILLOG_LAST_GUESS + 3, UPIC_FAILLOG_COUNT = UPIC_FAILLOG_LAST_MAP + 3
+};
+int upic_failed_particle_log(upic_ctx* ctx, int capacity, double* rows, int* nrows);
+
 /* Point probes of the implicit method's accepted fields with the particle
  * shape (evaluate_reconstructed_field_probe, ec_pic_nyquist_projected.cpp
  * :7924-7945): for each point (x[p], y[p]) the B-spline gathers of phi,

@@ -15,7 +15,7 @@ import numpy as np
 from ._native import UPIC_ERR, UpicConfig, c_dp, lib
 
 __all__ = ["UpicError", "Config", "ImplicitConfig", "NonrelConfig", "Simulation", "Ensemble", "autotune_explicit",
-           "generate_bimaxwellian", "p3_initial_state", "P3_CASES", "MAP_LOG_COLUMNS", "PROBE_COLUMNS",
+           "generate_bimaxwellian", "p3_initial_state", "P3_CASES", "MAP_LOG_COLUMNS", "FAILED_LOG_COLUMNS", "PROBE_COLUMNS",
            "convergence_method_name",
            "DIAG_COLUMNS", "IMPLICIT_DIAG_COLUMNS", "NONREL_DIAG_COLUMNS", "SOLVE_INFO_COLUMNS",
            "STEP_DIAG_COLUMNS", "METHODS",
@@ -72,6 +72,17 @@ SOLVE_INFO_COLUMNS = ["iterations", "converged", "final_rms_residual", "final_ma
 # of _particle_inner_history.csv after time_n, dt, with the step of the call.
 MAP_LOG_COLUMNS = ["step", "map_evaluation", "particles_converged", "failed_particles",
                    "max_scaled_particle_residual", "local_iterations_mean", "local_iterations_max"]
+# Failed-particle records of the last step_implicit call
+# (upic_failed_particle_log): the columns of _failed_particle_diagnostics.csv
+# after time_before, with the step of the call; failure_reason as a code
+# (FAILURE_REASONS).
+FAILED_LOG_COLUMNS = (["step", "layout_refinement_restart", "map_evaluation", "event_exhausted",
+                       "failed_particles_in_event", "particle_index", "assigned_substeps",
+                       "failed_substep_zero_based", "theta0", "theta1", "h", "local_iterations", "failure_reason",
+                       "first_scaled_residual", "final_scaled_residual", "final_absolute_residual", "q", "m"] +
+                      [f"{v}_{c}" for v in ("x0", "P0", "initial_guess", "last_guess", "last_map") for c in "xyz"])
+FAILURE_REASONS = ["none", "nonfinite_map", "superluminal_map", "nonfinite_iterate", "superluminal_iterate",
+                   "maximum_iterations", "too_many_knot_crossings"]
 # Point probe columns (upic_probe_fields).
 PROBE_COLUMNS = (["phi_h", "psi_h", "rho_h", "Ax_h", "Ay_h", "Az_h", "Ux_h", "Uy_h", "Uz_h", "Jx_h", "Jy_h", "Jz_h",
                   "Ex_grid_gather", "Ey_grid_gather", "Ez_grid_gather", "Bx_grid_gather", "By_grid_gather",
@@ -414,6 +425,16 @@ class Simulation:
         self._check(lib().upic_map_log(self._ctx, 0, None, ctypes.byref(n)))
         rows = np.empty((n.value, len(MAP_LOG_COLUMNS)))
         self._check(lib().upic_map_log(self._ctx, n.value, _p(rows), ctypes.byref(n)))
+        return rows
+
+    def failed_particle_log(self):
+        """Failed-particle records of the last step_implicit call (selective
+        fallback), one row per failed particle in FAILED_LOG_COLUMNS order
+        (upic_failed_particle_log)."""
+        n = ctypes.c_int()
+        self._check(lib().upic_failed_particle_log(self._ctx, 0, None, ctypes.byref(n)))
+        rows = np.empty((n.value, len(FAILED_LOG_COLUMNS)))
+        self._check(lib().upic_failed_particle_log(self._ctx, n.value, _p(rows), ctypes.byref(n)))
         return rows
 
     def probe_fields(self, x, y):

@@ -73,6 +73,7 @@ SYMBOLS = {
     "upic_fft_solve_cn": (ctypes.c_int, [ctypes.c_void_p] + [c_dp] * 12),
     "upic_push_iaem": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long] + [c_dp] * 9),
     "upic_map_log": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, c_ip]),
+    "upic_failed_particle_log": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, c_ip]),
     "upic_probe_fields": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, c_dp, c_dp, c_dp]),
     "upic_generate_bimaxwellian": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_double,

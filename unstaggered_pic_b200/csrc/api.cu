@@ -287,6 +287,43 @@ int download3(upic_ctx* c, double* host, long n, const double* a, const double* 
     return 0;
 }
 
+#ifndef UPIC_DEVICE_SCAN
+#define UPIC_DEVICE_SCAN 1
+#endif
+
+// Finiteness and speed bounds of an uploaded particle state (the x, y, v
+// part of scan_particles, on the device copy): out[0] counts non-finite
+// particles, out[1] and out[2] hold the bit patterns of the largest speed
+// and velocity component (non-negative doubles order as their bits).  The
+// speed is summed without fused multiply-adds, as the host scan sums it.
+__global__ void scan_state_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                  const double* __restrict__ vx, const double* __restrict__ vy,
+                                  const double* __restrict__ vz, long n, unsigned long long* out) {
+    unsigned long long bad = 0;
+    double smax = 0.0, cmax = 0.0;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+        const double a = vx[p], b = vy[p], c = vz[p];
+        const double sp = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c)));
+        if (!isfinite(sp) || !isfinite(x[p]) || !isfinite(y[p])) {
+            ++bad;
+        } else {
+            smax = fmax(smax, sp);
+            cmax = fmax(cmax, fmax(fabs(a), fmax(fabs(b), fabs(c))));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        bad += __shfl_xor_sync(0xffffffffu, bad, o);
+        smax = fmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+        cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (bad) atomicAdd(&out[0], bad);
+        atomicMax(&out[1], (unsigned long long)__double_as_longlong(smax));
+        atomicMax(&out[2], (unsigned long long)__double_as_longlong(cmax));
+    }
+}
+
+// x == nullptr: q and m only (finite, speed_max and comp_max left as they are).
 HostScan scan_particles(long np, const double* x, const double* y, const double* v, const double* q,
                         const double* m) {
     constexpr int kChunks = 64;
@@ -300,6 +337,7 @@ HostScan scan_particles(long np, const double* x, const double* y, const double*
             if (q[p] != q0 || m[p] != m0) h.uniform = false;
             if (!(m[p] > 0.0)) h.positive_m = false;
             h.qabs += std::fabs(q[p]);
+            if (!x) continue;
             const double* vp = v + 3 * p;
             const double s = std::sqrt(vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]);
             if (!std::isfinite(s) || !std::isfinite(x[p]) || !std::isfinite(y[p])) h.finite = false;
@@ -699,10 +737,11 @@ int upic_create(const upic_config* cfg, upic_ctx** out) {
         (rc = dalloc(c, &c->d_dreal, (size_t)kDiagFields * N)) ||
         (rc = dalloc(c, &c->d_partials, (size_t)kRedGrid * 16)) ||
         (rc = dalloc(c, &c->d_pdiag, (size_t)c->push_grid * kDiagPart)) ||
-        (rc = dalloc(c, &c->d_row, UPIC_DIAG_COUNT)) ||
+        (rc = dalloc(c, &c->d_row, UPIC_DIAG_COUNT)) || (rc = dalloc(c, &c->d_scan, 3)) ||
         (c->mixed && (rc = dalloc(c, &c->d_gf32, (size_t)kGFStride * N))))
         return bail(rc);
-    if (cudaMallocHost(&c->h_row, sizeof(double) * UPIC_DIAG_COUNT) != cudaSuccess)
+    if (cudaMallocHost(&c->h_row, sizeof(double) * UPIC_DIAG_COUNT) != cudaSuccess ||
+        cudaMallocHost(&c->h_scan, 3 * sizeof(unsigned long long)) != cudaSuccess)
         return bail(fail(c, UPIC_ERR_NOMEM, "cudaMallocHost failed"));
     std::vector<double> kx(N), ky(N), k2(N);
     const ModeConvention dconv = implicit ? kModesP3 : kModesP2;
@@ -948,6 +987,7 @@ int upic_destroy(upic_ctx* c) {
     for (void* p : c->allocs)
         if (p) cudaFree(p);
     if (c->h_row) cudaFreeHost(c->h_row);
+    if (c->h_scan) cudaFreeHost(c->h_scan);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
     return UPIC_OK;
@@ -1085,8 +1125,25 @@ int upic_set_particles(upic_ctx* c, long np, const double* x, const double* y, c
         if ((rc = upload3(c, v, np, s.vx, s.vy, s.vz))) return rc;
         if ((rc = upload3(c, v_prev, np, s.wx, s.wy, s.wz))) return rc;
     }
-    // uniform charge/mass (the reference stores them per particle)
+    // uniform charge/mass (the reference stores them per particle); the
+    // device checks the uploaded positions and velocities meanwhile
+#if UPIC_DEVICE_SCAN
+    HostScan hs;
+    if (np > 0) {
+        UPIC_CUDA(c, cudaMemsetAsync(c->d_scan, 0, 3 * sizeof(unsigned long long), c->st));
+        scan_state_kernel<<<148 * 8, 256, 0, c->st>>>(s.x, s.y, s.vx, s.vy, s.vz, np, c->d_scan);
+        count_launches(1);
+        UPIC_CUDA(c, cudaMemcpyAsync(c->h_scan, c->d_scan, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                     c->st));
+        hs = scan_particles(np, nullptr, nullptr, nullptr, q, m);
+        if ((rc = sync(c))) return rc;
+        hs.finite = c->h_scan[0] == 0;
+        std::memcpy(&hs.speed_max, &c->h_scan[1], sizeof(double));
+        std::memcpy(&hs.comp_max, &c->h_scan[2], sizeof(double));
+    }
+#else
     const HostScan hs = scan_particles(np, x, y, v, q, m);
+#endif
     if (!hs.finite) {
         c->np = 0;  // the context holds no particle set until a valid one is loaded
         sync(c);

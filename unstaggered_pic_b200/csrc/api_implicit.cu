@@ -14,6 +14,7 @@
 // and their trial copies (2 x 9 complex per node); map records (8 doubles per
 // node: grad phi_mid, A^n, A^{n+1}); node currents J, J_field, guesses,
 // map values and the Anderson history (3 doubles per node each).
+#include <algorithm>
 #include <cfloat>
 #include <cstdio>
 #include <climits>
@@ -151,6 +152,15 @@ struct ImplicitState {
     // (UPIC_MAPLOG_COUNT values each, upic_map_log)
     std::vector<double> maplog;
     int log_step = 0, map_eval = 0;
+    // failed-particle records of the selective layout's failing map
+    // evaluations in the current upic_step_implicit call (UPIC_FAILLOG_COUNT
+    // values each, upic_failed_particle_log); fail_event: first row of the
+    // last event; layout_restart: the step's current layout refinement
+    std::vector<double> faillog;
+    size_t fail_event = 0;
+    int layout_restart = 0;
+    double* dfail = nullptr;  // kFailRec doubles per failed particle (grown on demand)
+    int dfail_cap = 0;
     // F18: phi, psi, rho, A, U, J, E, B on the grid for upic_probe_fields;
     // probe staging (grown on demand)
     double* probe_grid = nullptr;
@@ -257,9 +267,10 @@ int alloc_particles(upic_ctx* c, ImplicitState& s, long cap, bool with_qm) {
         ((rc = dalloc(c, &s.hvx, cap)) || (rc = dalloc(c, &s.hvy, cap)) || (rc = dalloc(c, &s.hvz, cap))))
         return rc;
     if (c->cfg.selective_particle_fallback &&
-        ((rc = dalloc(c, &s.nsub, cap)) || (rc = dalloc(c, &s.refined, cap)) || (rc = dalloc(c, &s.failed, cap)) ||
-         (rc = dalloc(c, &s.nfailed, 1)) || (rc = dalloc(c, &s.roff, cap))))
+        ((rc = dalloc(c, &s.nsub, cap)) || (rc = dalloc(c, &s.refined, cap)) || (rc = dalloc(c, &s.roff, cap))))
         return rc;
+    // the failing particles of a map evaluation, for the failed-particle log
+    if (!s.picard && ((rc = dalloc(c, &s.failed, cap)) || (rc = dalloc(c, &s.nfailed, 1)))) return rc;
     if ((rc = alloc_sortwork(c, s.sw, cap, s.tg))) return rc;
     s.cap = cap;
     return ensure_tmp3(c, cap);
@@ -338,6 +349,41 @@ void log_map_evaluation(ImplicitState& s, const MapStats& m) {
     s.maplog.insert(s.maplog.end(), row, row + UPIC_MAPLOG_COUNT);
 }
 
+// Records of the failed particles of the map evaluation just run with
+// arguments a (the selective layout's): each failing local solve is run
+// again on the evaluation's fields with its report (failure_report_kernel),
+// the rows sorted by particle index as the reference sorts its list
+// (:5402-5406) and appended to the call's failed-particle log.
+int record_failures(upic_ctx* c, ImplicitState& s, const ImplicitMapArgs& a) {
+    int nf = 0;
+    UPIC_CUDA(c, cudaMemcpyAsync(&nf, s.nfailed, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    int rc = sync(c);
+    if (rc) return rc;
+    s.fail_event = s.faillog.size();
+    if (nf <= 0) return 0;
+    if (nf > s.dfail_cap) {
+        dfree(c, s.dfail);
+        s.dfail = nullptr;
+        s.dfail_cap = 0;
+        if ((rc = dalloc(c, &s.dfail, (size_t)kFailRec * nf))) return rc;
+        s.dfail_cap = nf;
+    }
+    UPIC_CUDA(c, launch_failure_report(s.order, s.uniform, a.split != 0, s.tg, a, s.failed, nf, s.dfail, c->st));
+    std::vector<double> rows((size_t)kFailRec * nf);
+    UPIC_CUDA(c, cudaMemcpyAsync(rows.data(), s.dfail, sizeof(double) * rows.size(), cudaMemcpyDeviceToHost, c->st));
+    if ((rc = sync(c))) return rc;
+    std::vector<int> order(nf);
+    for (int i = 0; i < nf; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int i, int j) { return rows[(size_t)i * kFailRec] < rows[(size_t)j * kFailRec]; });
+    for (int i : order) {
+        const double head[5] = {(double)s.log_step, (double)s.layout_restart, (double)s.map_eval, 0.0, (double)nf};
+        s.faillog.insert(s.faillog.end(), head, head + 5);
+        const double* r = rows.data() + (size_t)i * kFailRec;
+        s.faillog.insert(s.faillog.end(), r, r + kFailRec);
+    }
+    return 0;
+}
+
 int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bool write_state,
              MapStats* stats_out, bool* map_finite = nullptr, Norms* norms = nullptr) {
     const upic_config& cf = c->cfg;
@@ -399,10 +445,12 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
         a.nref = s.nref;
         a.grid_nx = c->nx;
         a.grid_ny = c->ny;
-        a.failed = s.failed;
-        a.nfailed = s.nfailed;
         a.roff = s.roff;
         a.sub_rec = s.sub_rec;
+    }
+    if (s.failed) {
+        a.failed = s.failed;
+        a.nfailed = s.nfailed;
         UPIC_CUDA(c, cudaMemsetAsync(s.nfailed, 0, sizeof(int), c->st));
     }
     a.vbar_x = s.hvx;
@@ -451,6 +499,9 @@ int eval_map(upic_ctx* c, ImplicitState& s, const double* guess, double* out, bo
     if (norms) norms_from_sums(c, s, *norms);
     log_map_evaluation(s, *s.hstats);
     if (s.hstats->failures > 0) {
+        // the selective layout's failures, or the failures that end the step
+        // when there is no fallback (the reference's full-step layout)
+        if ((s.layout_active || !cf.selective_particle_fallback) && (rc = record_failures(c, s, a))) return rc;
         static const char* names[] = {"none", "nonfinite_map", "superluminal_map", "nonfinite_iterate",
                                       "superluminal_iterate", "maximum_iterations", "too_many_knot_crossings"};
         const unsigned long long key = s.hstats->first_fail_key;
@@ -1211,6 +1262,7 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
         if ((rc = upload_layout(c, s))) return rc;
         s.layout_active = true;
         for (;;) {
+            s.layout_restart = restarts;
             rc = outer_solve(c, s, r);
             if (rc != UPIC_ERR_LOCAL_PARTICLE) break;
             int nf = 0;
@@ -1221,6 +1273,9 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
             long exhausted = 0;
             for (int p : failed)
                 if (s.h_nsub[p] >= cf.selective_particle_max_substeps) ++exhausted;
+            if (exhausted > 0)
+                for (size_t k = s.fail_event; k < s.faillog.size(); k += UPIC_FAILLOG_COUNT)
+                    s.faillog[k + UPIC_FAILLOG_EXHAUSTED] = 1.0;
             if (exhausted > 0) {
                 char buf[400];
                 std::snprintf(buf, sizeof(buf),
@@ -1241,6 +1296,13 @@ int implicit_one_step(upic_ctx* c, ImplicitState& s, double* info) {
                       "direct macro solve failed (" + direct +
                           "); selective outer current solve also failed without a refinable local-particle set (" +
                           inner + ")");
+        }
+    }
+    if (rc == UPIC_ERR_LOCAL_PARTICLE && !cf.selective_particle_fallback) {
+        // write_failed_particle_diagnostics(..., 0, cfg, failures, true) (:6514)
+        for (size_t k = s.fail_event; k < s.faillog.size(); k += UPIC_FAILLOG_COUNT) {
+            s.faillog[k + UPIC_FAILLOG_RESTART] = 0.0;
+            s.faillog[k + UPIC_FAILLOG_EXHAUSTED] = 1.0;
         }
     }
     if (rc) return rc;
@@ -2075,6 +2137,8 @@ extern "C" int upic_step_implicit(upic_ctx* c, int nsteps, double* diag, double*
     if (nsteps < 0) return fail(c, UPIC_ERR_ARGUMENT, "nsteps < 0");
     double row[UPIC_P3_DIAG_COUNT];
     s.maplog.clear();
+    s.faillog.clear();
+    s.fail_event = 0;
     for (int k = 0; k < nsteps; ++k) {
         int rc;
         s.log_step = k;
@@ -2133,6 +2197,20 @@ extern "C" int upic_map_log(upic_ctx* c, int capacity, double* rows, int* nrows)
     *nrows = n;
     const int k = std::min(n, capacity);
     if (k > 0) std::memcpy(rows, s.maplog.data(), sizeof(double) * UPIC_MAPLOG_COUNT * (size_t)k);
+    return UPIC_OK;
+}
+
+static_assert(UPIC_FAILLOG_COUNT == 5 + kFailRec, "failed-particle log row = 5 event columns + a record");
+
+extern "C" int upic_failed_particle_log(upic_ctx* c, int capacity, double* rows, int* nrows) {
+    if (!c || !nrows || capacity < 0 || (capacity > 0 && !rows))
+        return c ? fail(c, UPIC_ERR_ARGUMENT, "upic_failed_particle_log: bad arguments") : UPIC_ERR_ARGUMENT;
+    if (!c->imp) return fail(c, UPIC_ERR_STATE, "context was not created with an implicit method");
+    const ImplicitState& s = *c->imp;
+    const int n = (int)(s.faillog.size() / UPIC_FAILLOG_COUNT);
+    *nrows = n;
+    const int k = std::min(n, capacity);
+    if (k > 0) std::memcpy(rows, s.faillog.data(), sizeof(double) * UPIC_FAILLOG_COUNT * (size_t)k);
     return UPIC_OK;
 }
 

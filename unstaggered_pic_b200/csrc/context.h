@@ -77,6 +77,10 @@ struct upic_ctx {
     double* d_row = nullptr;
     double* d_bg = nullptr;   // fixed background charge (upic_set_background) or null: uniform n0
     double* h_row = nullptr;  // pinned
+    // particle-state scan of upic_set_particles (non-finite count, largest
+    // speed and velocity component bits): device words and their pinned copy
+    unsigned long long* d_scan = nullptr;
+    unsigned long long* h_scan = nullptr;
 
     int head = 0;
     long steps = 0;

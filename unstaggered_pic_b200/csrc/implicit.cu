@@ -1164,6 +1164,198 @@ __global__ void __launch_bounds__(128) refined_map_kernel(ImplicitMapArgs a, int
     }
 }
 
+// ---- failed-particle records ---------------------------------------------------
+// The report of one local solve (LocalParticleSolveReport :4805, filled as
+// solve_local_particle_substep :4930 fills it): iteration count, reason, the
+// first and last scaled residuals, the last absolute residual, the last
+// iterate and the last map value.
+struct SolveTrace {
+    int iters = 0, reason = kLocalMaxIter;
+    double first_scaled = INFINITY, final_scaled = INFINITY, final_abs = INFINITY;
+    double last_guess[3] = {0.0, 0.0, 0.0}, last_map[3] = {0.0, 0.0, 0.0};
+};
+
+// The local fixed point of the map kernels with its report; eval(guess, o)
+// is one map evaluation (false: too many knot crossings).  The arithmetic of
+// every iterate is the map kernels', so a particle fails here exactly as it
+// failed there.
+template <class Eval>
+UPIC_D bool traced_solve(const ImplicitMapArgs& a, const double* start, Eval eval, SolveTrace& t) {
+    double guess[3] = {start[0], start[1], start[2]};
+    LocalOut o;
+    t = SolveTrace{};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) t.last_guess[c] = guess[c];
+    for (int it = 0; it < a.loc_maxit; ++it) {
+        if (!eval(guess, o)) {
+            t.reason = kLocalTooManyCrossings;
+            return false;
+        }
+        ++t.iters;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            t.last_guess[c] = guess[c];
+            t.last_map[c] = o.vbar_map[c];
+        }
+        if (!finite3(o.vbar_map)) {
+            t.reason = kLocalNonfiniteMap;
+            return false;
+        }
+        if (norm3(o.vbar_map) >= a.kappa) {
+            t.reason = kLocalSuperluminalMap;
+            return false;
+        }
+        const double res[3] = {o.vbar_map[0] - guess[0], o.vbar_map[1] - guess[1], o.vbar_map[2] - guess[2]};
+        const double sc = 0.5 * (norm3(o.vbar_map) + norm3(guess));
+        t.final_abs = norm3(res);
+        t.final_scaled = t.final_abs / (a.loc_atol + a.loc_rtol * sc);
+        if (t.iters == 1) t.first_scaled = t.final_scaled;
+        if (t.final_scaled <= 1.0) {
+            t.reason = kLocalOk;
+            return true;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            guess[c] += a.loc_damp * res[c];
+            t.last_guess[c] = guess[c];
+        }
+        if (!finite3(guess)) {
+            t.reason = kLocalNonfiniteIterate;
+            return false;
+        }
+        if (norm3(guess) >= a.kappa) {
+            t.reason = kLocalSuperluminalIterate;
+            return false;
+        }
+    }
+    t.reason = kLocalMaxIter;
+    return false;
+}
+
+// One record per failed particle of a map evaluation (failed[0..nf), sorted
+// positions; the FailedParticleDiagnostic of :5331-5350): the particle's
+// local solves are run again on the evaluation's fields, unit-step particles
+// with the map kernel's evaluation (MOM, SY as that launch), sub-cycled ones
+// substep by substep as refined_map_kernel advances them, up to the substep
+// that fails.  Record (kFailRec doubles): particle id, assigned substeps,
+// failed substep, theta0, theta1, h, iterations, reason, first / final
+// scaled residual, final absolute residual, q, m, x0 (3), P0 (3), initial
+// guess (3), last guess (3), last map (3).
+template <int ORDER, bool UNIFORM, bool MOM, int SY>
+__global__ void __launch_bounds__(128) failure_report_kernel(ImplicitMapArgs a, int nx, int ny, const int* failed,
+                                                             int nf, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nf) return;
+    Geo g{nx, ny, a.Lx, a.Ly, a.inv_dx, a.inv_dy};
+    g.qs = a.qtab;
+    g.qw = a.qtab + kMaxQuad;
+    g.ms = a.qtab + 2 * kMaxQuad;
+    g.mw = a.qtab + 3 * kMaxQuad;
+    g.nq = a.nq;
+    g.mnq = a.mnq;
+    const int p = failed[i];
+    const int n = a.nsub ? a.nsub[p] : 1;
+    const double q = UNIFORM ? a.q0 : a.q[p];
+    const double m = UNIFORM ? a.m0 : a.m[p];
+    double x = a.x[p], y = a.y[p];
+    double P[3] = {a.Px[p], a.Py[p], a.Pz[p]};
+    double v[3] = {a.vx[p], a.vy[p], a.vz[p]};
+    double bk[kMaxBreaks];
+    int nb = 0;
+    SolveTrace t;
+    int k = 0;
+    double th0 = 0.0, th1 = 1.0, h = a.dt, x0 = x, y0 = y, P0[3] = {P[0], P[1], P[2]}, start[3];
+    if (n <= 1) {
+        LocalIn in;
+        in.x0 = x;
+        in.y0 = y;
+        in.q = q;
+        in.m = m;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) in.P0[c] = P[c];
+        gather_rec3<ORDER, kIRec, SY>(g, a.rec, kIRecAn, x, y, in.A0p);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) in.pstart[c] = in.P0[c] - in.q * in.A0p[c];
+        set_local_constants(in, a.kappa);
+        start[0] = a.warm_x ? a.warm_x[p] : v[0];
+        start[1] = a.warm_x ? a.warm_y[p] : v[1];
+        start[2] = a.warm_x ? a.warm_z[p] : v[2];
+        traced_solve(a, start, [&](const double* gs, LocalOut& o) {
+            if constexpr (MOM)
+                return evaluate_moments<ORDER, SY>(g, a.rec, a.dt, a.kappa, a.split, in, gs, o, bk, nb);
+            else
+                return evaluate<ORDER, SY>(g, a.rec, a.dt, a.kappa, a.split, in, gs, o, bk, nb);
+        }, t);
+    } else {
+        h = a.dt / (double)n;
+        for (k = 0; k < n; ++k) {
+            th0 = (double)k / (double)n;
+            th1 = (double)(k + 1) / (double)n;
+            LocalIn in;
+            in.x0 = x;
+            in.y0 = y;
+            in.q = q;
+            in.m = m;
+            double An0[3], Ae0[3];
+            gather_rec3<ORDER>(g, a.rec, kIRecAn, x, y, An0);
+            gather_rec3<ORDER>(g, a.rec, kIRecAe, x, y, Ae0);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                in.P0[c] = P[c];
+                in.A0p[c] = (1.0 - th0) * An0[c] + th0 * Ae0[c];
+                in.pstart[c] = P[c] - q * in.A0p[c];
+            }
+            set_local_constants(in, a.kappa);
+            x0 = x;
+            y0 = y;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                P0[c] = P[c];
+                start[c] = v[c];
+            }
+            LocalOut last;
+            const bool ok = traced_solve(a, start, [&](const double* gs, LocalOut& o) {
+                const bool r = evaluate_sub<ORDER>(g, a.rec, h, th0, th1, a.kappa, a.split, in, gs, o, bk, nb);
+                last = o;
+                return r;
+            }, t);
+            if (!ok) break;
+            // the accepted sub-orbit's end state starts the next substep
+            x = last.x1;
+            y = last.y1;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                P[c] = last.P_end[c];
+                v[c] = last.v_end[c];
+            }
+        }
+    }
+    double* r = out + (size_t)i * kFailRec;
+    r[0] = (double)a.id[p];
+    r[1] = (double)n;
+    r[2] = (double)(n <= 1 ? 0 : k);
+    r[3] = th0;
+    r[4] = th1;
+    r[5] = h;
+    r[6] = (double)t.iters;
+    r[7] = (double)t.reason;
+    r[8] = t.first_scaled;
+    r[9] = t.final_scaled;
+    r[10] = t.final_abs;
+    r[11] = q;
+    r[12] = m;
+    r[13] = x0;
+    r[14] = y0;
+    r[15] = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        r[16 + c] = P0[c];
+        r[19 + c] = start[c];
+        r[22 + c] = t.last_guess[c];
+        r[25 + c] = t.last_map[c];
+    }
+}
+
 __global__ void fill_int_kernel(int n, int value, int* out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = value;
 }
@@ -2509,6 +2701,37 @@ cudaError_t launch_refined_map(int order, bool uniform, const ImplicitMapArgs& a
         default: return cudaErrorInvalidValue;
     }
 #undef UPIC_RM
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_failure_report(int order, bool uniform, bool split, const TileGeom& tg, const ImplicitMapArgs& a,
+                                  const int* failed, int nf, double* out, cudaStream_t st) {
+    if (nf <= 0) return cudaSuccess;
+    const int g = (nf + 127) / 128;
+    // the evaluation form of the map launch (map_kernel): one-row instances for
+    // split launches on a grid one cell high, segment moments for split
+    // orbits of order <= 2
+    const bool oned = tg.ny == 1 && split && use_split(a, false);
+    const bool mom = oned || (split && order <= 2);
+#define UPIC_FR(O, U, M, SY) failure_report_kernel<O, U, M, SY><<<g, 128, 0, st>>>(a, tg.nx, tg.ny, failed, nf, out)
+#define UPIC_FR_ORDER(O)                                                    \
+    if (oned) {                                                             \
+        if (uniform) UPIC_FR(O, true, true, 1); else UPIC_FR(O, false, true, 1); \
+    } else if (mom && O <= 2) {                                             \
+        if (uniform) UPIC_FR(O, true, (O <= 2), O + 1); else UPIC_FR(O, false, (O <= 2), O + 1); \
+    } else {                                                                \
+        if (uniform) UPIC_FR(O, true, false, O + 1); else UPIC_FR(O, false, false, O + 1); \
+    }
+    switch (order) {
+        case 1: UPIC_FR_ORDER(1) break;
+        case 2: UPIC_FR_ORDER(2) break;
+        case 3: UPIC_FR_ORDER(3) break;
+        case 4: UPIC_FR_ORDER(4) break;
+        default: return cudaErrorInvalidValue;
+    }
+#undef UPIC_FR_ORDER
+#undef UPIC_FR
     count_launches(1);
     return cudaGetLastError();
 }

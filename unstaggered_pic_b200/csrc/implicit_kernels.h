@@ -102,6 +102,12 @@ struct ImplicitMapArgs {
 // solves over [k/n, (k+1)/n] of the step with time-interpolated fields, each
 // sub-orbit deposited with weight q/n (point quadrature, fixed-point grid adds).
 cudaError_t launch_refined_map(int order, bool uniform, const ImplicitMapArgs& a, cudaStream_t st);
+// Records of the failed particles failed[0..nf) of the map evaluation whose
+// arguments are a (kFailRec doubles each, in failed order), for a grid of
+// tg's size: each particle's failing local solve run again with its report.
+constexpr int kFailRec = 28;
+cudaError_t launch_failure_report(int order, bool uniform, bool split, const TileGeom& tg, const ImplicitMapArgs& a,
+                                  const int* failed, int nf, double* out, cudaStream_t st);
 // nsub[p] = 1 for p < n
 cudaError_t launch_fill_int(int n, int value, int* out, cudaStream_t st);
 

@@ -9,7 +9,7 @@
 //
 //   _diagnostics.csv, _step_diagnostics.csv, _adaptive_diagnostics.csv,
 //   _particle_inner_history.csv, _config_echo.txt, _unit_tests.txt,
-//   _particle_sample.csv, _failed_particle_diagnostics.csv (header),
+//   _particle_sample.csv, _failed_particle_diagnostics.csv,
 //   _field_line_probe.csv, _field_knot_jumps.csv, _field_grid_snapshots.csv,
 //   _velocity_moments.csv, _field_spectrum.csv, _particles_t<time>.csv.
 //
@@ -779,6 +779,73 @@ bool unit_tests(std::ostream& os) {
 // ---- output ------------------------------------------------------------------
 
 // The NonlinearSolveInfo columns of one row.
+// _failed_particle_diagnostics.csv rows of one step (write_failed_particle_diagnostics
+// :6234): per failure event (layout restart, map evaluation) the
+// selective_failure_diagnostic_limit particles of largest final scaled
+// residual (non-finite first, the reference's sort), and in an exhausted
+// event also the worst particle at the substep limit, in particle order.
+void write_failed_particles(upic_ctx* c, const P3Deck& d, double time_before) {
+    static const char* reasons[] = {"none", "nonfinite_map", "superluminal_map", "nonfinite_iterate",
+                                    "superluminal_iterate", "maximum_iterations", "too_many_knot_crossings"};
+    int n = 0;
+    check(upic_failed_particle_log(c, 0, nullptr, &n), c);
+    if (n == 0) return;
+    std::vector<double> rows((size_t)n * UPIC_FAILLOG_COUNT);
+    check(upic_failed_particle_log(c, n, rows.data(), &n), c);
+    std::ofstream out(d.output_prefix + "_failed_particle_diagnostics.csv", std::ios::app);
+    auto at = [&](int i, int col) { return rows[(size_t)i * UPIC_FAILLOG_COUNT + col]; };
+    for (int b = 0; b < n;) {
+        int e = b;
+        while (e < n && at(e, UPIC_FAILLOG_RESTART) == at(b, UPIC_FAILLOG_RESTART) &&
+               at(e, UPIC_FAILLOG_EVALUATION) == at(b, UPIC_FAILLOG_EVALUATION) &&
+               at(e, UPIC_FAILLOG_STEP) == at(b, UPIC_FAILLOG_STEP))
+            ++e;
+        const int m = e - b;
+        std::vector<int> order(m);
+        for (int i = 0; i < m; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](int i, int j) {
+            const double x = at(b + i, UPIC_FAILLOG_FINAL_SCALED), y = at(b + j, UPIC_FAILLOG_FINAL_SCALED);
+            if (!std::isfinite(x)) return (bool)std::isfinite(y);
+            if (!std::isfinite(y)) return false;
+            return x > y;
+        });
+        std::vector<char> selected(m, 0);
+        const int limit = std::min(m, d.selective_failure_diagnostic_limit);
+        for (int i = 0; i < limit; ++i) selected[order[i]] = 1;
+        const bool exhausted = at(b, UPIC_FAILLOG_EXHAUSTED) != 0.0;
+        if (exhausted) {
+            int worst = -1;
+            for (int i = 0; i < m; ++i) {
+                if (at(b + i, UPIC_FAILLOG_SUBSTEPS) < d.selective_particle_max_substeps) continue;
+                if (worst < 0) {
+                    worst = i;
+                    continue;
+                }
+                const double cand = at(b + i, UPIC_FAILLOG_FINAL_SCALED), cur = at(b + worst, UPIC_FAILLOG_FINAL_SCALED);
+                if ((!std::isfinite(cand) && std::isfinite(cur)) ||
+                    (std::isfinite(cand) && std::isfinite(cur) && cand > cur))
+                    worst = i;
+            }
+            if (worst >= 0) selected[worst] = 1;
+        }
+        out << std::setprecision(17);
+        for (int i = 0; i < m; ++i) {
+            if (!selected[i]) continue;
+            const int r = b + i;
+            const int reason = (int)at(r, UPIC_FAILLOG_REASON);
+            out << time_before << "," << (long)at(r, UPIC_FAILLOG_RESTART) << "," << (long)at(r, UPIC_FAILLOG_EVALUATION)
+                << "," << (exhausted ? 1 : 0) << "," << (long)at(r, UPIC_FAILLOG_IN_EVENT) << ","
+                << (long)at(r, UPIC_FAILLOG_PARTICLE) << "," << (long)at(r, UPIC_FAILLOG_SUBSTEPS) << ","
+                << (long)at(r, UPIC_FAILLOG_FAILED_SUBSTEP) << "," << at(r, UPIC_FAILLOG_THETA0) << ","
+                << at(r, UPIC_FAILLOG_THETA1) << "," << at(r, UPIC_FAILLOG_H) << ","
+                << (long)at(r, UPIC_FAILLOG_ITERATIONS) << "," << (reason >= 0 && reason < 7 ? reasons[reason] : "unknown");
+            for (int col = UPIC_FAILLOG_FIRST_SCALED; col < UPIC_FAILLOG_COUNT; ++col) out << "," << at(r, col);
+            out << "\n";
+        }
+        b = e;
+    }
+}
+
 struct Solve {
     double iterations = 0, converged = 1, rms = kNaN, max_particle = kNaN, abs_rms = kNaN;
     double restarts = 0, anderson = 0, picard = 0;
@@ -1323,6 +1390,7 @@ int run_p3(const std::string& path) {
                       << m[UPIC_MAPLOG_ITER_MEAN] << "," << m[UPIC_MAPLOG_ITER_MAX] << "\n";
             }
         }
+        if (d.selective_failure_diagnostics) write_failed_particles(ctx.c, d, time);
         if (rc != UPIC_OK) {
             // the rejected attempt (:8741-8771); its solve report is not
             // returned by a failing step, so the counters keep their defaults
