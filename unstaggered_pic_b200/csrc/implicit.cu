@@ -39,12 +39,20 @@ constexpr int kMapMinBlocks = UPIC_MAP_MIN_BLOCKS;
 #ifndef UPIC_SOLVE_MIN_BLOCKS
 #define UPIC_SOLVE_MIN_BLOCKS 3
 #endif
+// resident CTAs of the deposit launch: 8 for the segment-moment instances
+// (one item per segment), 6 for the point-by-point ones (one item per
+// quadrature point), whose 8-CTA build measured slower
 #ifndef UPIC_DEPOSIT_MIN_BLOCKS
 #define UPIC_DEPOSIT_MIN_BLOCKS 6
 #endif
+#ifndef UPIC_DEPOSIT_MOM_MIN_BLOCKS
+#define UPIC_DEPOSIT_MOM_MIN_BLOCKS 8
+#endif
 constexpr int kPartFused = 0, kPartSolve = 1, kPartDeposit = 2;
-constexpr int map_min_blocks(int part) {
-    return part == kPartSolve ? UPIC_SOLVE_MIN_BLOCKS : part == kPartDeposit ? UPIC_DEPOSIT_MIN_BLOCKS : kMapMinBlocks;
+constexpr int map_min_blocks(int part, bool mom = false) {
+    return part == kPartSolve     ? UPIC_SOLVE_MIN_BLOCKS
+           : part == kPartDeposit ? (mom ? UPIC_DEPOSIT_MOM_MIN_BLOCKS : UPIC_DEPOSIT_MIN_BLOCKS)
+                                  : kMapMinBlocks;
 }
 constexpr int kMapWarps = kMapThreads / kWarp;
 constexpr int kKeyNone = -1;
@@ -588,7 +596,7 @@ UPIC_D int window_coord(int s, int origin, int n, int w, int span) {
 // kPartDeposit (the deposit of the orbits in vbar_*).
 // ONED: a grid one cell high (ny = 1): the y stencil is one row (SY = 1).
 template <int ORDER, bool UNIFORM, bool MOM, bool PICARD, int PART = kPartFused, bool ONED = false>
-__global__ void __launch_bounds__(kMapThreads, map_min_blocks(PART))
+__global__ void __launch_bounds__(kMapThreads, map_min_blocks(PART, MOM))
 implicit_map_kernel(ImplicitMapArgs a, TileGeom tg) {
     constexpr bool kSolve = PART != kPartDeposit;
     constexpr bool kDeposit = PART != kPartSolve;
@@ -2672,8 +2680,9 @@ cudaError_t launch_implicit_map(int order, bool uniform, bool split, const TileG
         if (!ks || !kd) return cudaErrorInvalidValue;
         // grid is sized for the fused kernel's resident CTAs; each part is
         // given as many CTAs as it keeps resident
+        const bool mom = (tg.ny == 1 && split) || (split && order <= 2);
         const int gs = grid / kMapMinBlocks * UPIC_SOLVE_MIN_BLOCKS;
-        const int gd = grid / kMapMinBlocks * UPIC_DEPOSIT_MIN_BLOCKS;
+        const int gd = grid / kMapMinBlocks * map_min_blocks(kPartDeposit, mom);
         ks<<<gs > 0 ? gs : grid, kMapThreads, smem, st>>>(a, tg);
         kd<<<gd > 0 ? gd : grid, kMapThreads, smem, st>>>(a, tg);
         count_launches(2);
