@@ -36,8 +36,14 @@ constexpr int kMapMinBlocks = UPIC_MAP_MIN_BLOCKS;
 #ifndef UPIC_MAP_SPLIT
 #define UPIC_MAP_SPLIT 1
 #endif
+// resident CTAs of the local-solve launch: 3 for the segment-moment
+// instances, 4 for the point-by-point ones (orders 3-4 in 2D), each the
+// faster of 2, 3 and 4 measured
 #ifndef UPIC_SOLVE_MIN_BLOCKS
 #define UPIC_SOLVE_MIN_BLOCKS 3
+#endif
+#ifndef UPIC_SOLVE_POINTS_MIN_BLOCKS
+#define UPIC_SOLVE_POINTS_MIN_BLOCKS 4
 #endif
 // resident CTAs of the deposit launch: 8 for the segment-moment instances
 // (one item per segment), 6 for the point-by-point ones (one item per
@@ -50,7 +56,7 @@ constexpr int kMapMinBlocks = UPIC_MAP_MIN_BLOCKS;
 #endif
 constexpr int kPartFused = 0, kPartSolve = 1, kPartDeposit = 2;
 constexpr int map_min_blocks(int part, bool mom = false) {
-    return part == kPartSolve     ? UPIC_SOLVE_MIN_BLOCKS
+    return part == kPartSolve     ? (mom ? UPIC_SOLVE_MIN_BLOCKS : UPIC_SOLVE_POINTS_MIN_BLOCKS)
            : part == kPartDeposit ? (mom ? UPIC_DEPOSIT_MOM_MIN_BLOCKS : UPIC_DEPOSIT_MIN_BLOCKS)
                                   : kMapMinBlocks;
 }
@@ -2681,7 +2687,7 @@ cudaError_t launch_implicit_map(int order, bool uniform, bool split, const TileG
         // grid is sized for the fused kernel's resident CTAs; each part is
         // given as many CTAs as it keeps resident
         const bool mom = (tg.ny == 1 && split) || (split && order <= 2);
-        const int gs = grid / kMapMinBlocks * UPIC_SOLVE_MIN_BLOCKS;
+        const int gs = grid / kMapMinBlocks * map_min_blocks(kPartSolve, mom);
         const int gd = grid / kMapMinBlocks * map_min_blocks(kPartDeposit, mom);
         ks<<<gs > 0 ? gs : grid, kMapThreads, smem, st>>>(a, tg);
         kd<<<gd > 0 ? gd : grid, kMapThreads, smem, st>>>(a, tg);
